@@ -1,0 +1,312 @@
+/*
+ * Typed half of the CPU oracle, included twice by stz_oracle.c with
+ * T = float / SUF = f32 and T = double / SUF = f64 (the reference's
+ * run_typed<float> / run_typed<double>, FD5:1954, 3070-3076).
+ *
+ * Test infrastructure only (see stz_oracle.h). Every arithmetic expression
+ * keeps the reference's operand order; the build disables FMA contraction and
+ * the entry points enable FTZ/DAZ as the reference main() does (FD5:3046-3047).
+ */
+#define CAT_(a, b) a##_##b
+#define CAT(a, b) CAT_(a, b)
+#define FN(name) CAT(name, SUF)
+
+/* cubic_line_pred, FD5:141-146: -(1/16)a + (9/16)b + (9/16)c - (1/16)d, left to right. */
+static inline T FN(cubic)(T a, T b, T c, T d)
+{
+    return -(1.0f / 16.0f) * a + (9.0f / 16.0f) * b + (9.0f / 16.0f) * c - (1.0f / 16.0f) * d;
+}
+
+/* cubic_line_pv_cse, FD5:163-175 (default build, PRED_NO_CSE unset). The
+ * epsilon is a float literal converted to T, as in the reference. */
+static inline void FN(line_pv)(T a, T b, T c, T d, T* p, T* v)
+{
+    const T eps = (T)1e-12f;
+    const T c0 = a - 2.0f * b + c;
+    const T c1 = b - 2.0f * c + d;
+    *v = 0.5f * (c0 * c0 + c1 * c1) + eps;
+    *p = 0.5f * (b + c) - (1.0f / 16.0f) * (c0 + c1);
+}
+
+/* blend2, FD5:178-186 (PRED_WPOW2 unset). */
+static inline T FN(blend2)(T p0, T v0, T p1, T v1)
+{
+    return (p0 * v1 + p1 * v0) / (v0 + v1);
+}
+
+/* blend4, FD5:188-203: product weights and one division. */
+static inline T FN(blend4)(T p0, T v0, T p1, T v1, T p2, T v2, T p3, T v3)
+{
+    const T w0 = v1 * v2 * v3;
+    const T w1 = v0 * v2 * v3;
+    const T w2 = v0 * v1 * v3;
+    const T w3 = v0 * v1 * v2;
+    return (w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3) / (w0 + w1 + w2 + w3);
+}
+
+/* predict_dynamic_lines_const<Block>, FD5:624-688 (no PRED_PLANE_AXIS /
+ * PRED_CUBE_AXIS): diagonal cubic lines blended by inverse variance. */
+static inline T FN(dyn_lines)(int block, const T* r, size_t i, size_t sx, size_t sy)
+{
+    T p0, v0, p1, v1, p2, v2, p3, v3;
+    if (block == 2) {
+        FN(line_pv)(r[i - sx - 1], r[i], r[i + sx + 1], r[i + 2 * sx + 2], &p0, &v0);
+        FN(line_pv)(r[i - sx + 2], r[i + 1], r[i + sx], r[i + 2 * sx - 1], &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    }
+    if (block == 4) {
+        FN(line_pv)(r[i - sy - 1], r[i], r[i + sy + 1], r[i + 2 * sy + 2], &p0, &v0);
+        FN(line_pv)(r[i - sy + 2], r[i + 1], r[i + sy], r[i + 2 * sy - 1], &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    }
+    if (block == 5) {
+        FN(line_pv)(r[i - sy - sx], r[i], r[i + sy + sx], r[i + 2 * sy + 2 * sx], &p0, &v0);
+        FN(line_pv)(r[i - sy + 2 * sx], r[i + sx], r[i + sy], r[i + 2 * sy - sx], &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    }
+    FN(line_pv)(r[i - sy - sx - 1], r[i], r[i + sy + sx + 1], r[i + 2 * sy + 2 * sx + 2], &p0, &v0);
+    FN(line_pv)(r[i - sy - sx + 2], r[i + 1], r[i + sy + sx], r[i + 2 * sy + 2 * sx - 1], &p1, &v1);
+    FN(line_pv)(r[i - sy + 2 * sx - 1], r[i + sx], r[i + sy + 1], r[i + 2 * sy - sx + 2], &p2, &v2);
+    FN(line_pv)(r[i + 2 * sy - sx - 1], r[i + sy], r[i + sx + 1], r[i - sy + 2 * sx + 2], &p3, &v3);
+    return FN(blend4)(p0, v0, p1, v1, p2, v2, p3, v3);
+}
+
+/* predict_block_const<Block>, FD5:690-748. The split kernels of FD5 use this
+ * on the boundary shells and predict_interior_const (FD5:828-840) inside; both
+ * give the same value at every point, so the oracle evaluates it pointwise. */
+static T FN(t_predict)(int block, const T* r, int x, int y, int z, int dx, int dy, int dz)
+{
+    const size_t sx = (size_t)dx, sy = (size_t)dx * (size_t)dy;
+    const size_t i = ((size_t)z * dy + y) * dx + x;
+    switch (block) {
+    case 0:
+        if (x == dx - 1) return r[i];
+        if (x == dx - 2 || x == 0) return (T)0.5f * (r[i] + r[i + 1]);
+        return FN(cubic)(r[i - 1], r[i], r[i + 1], r[i + 2]);
+    case 1:
+        if (y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0) return (T)0.5f * (r[i] + r[i + sx]);
+        return FN(cubic)(r[i - sx], r[i], r[i + sx], r[i + 2 * sx]);
+    case 2:
+        if (x == dx - 1 || y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
+            return (T)0.25f * (r[i] + r[i + sx + 1] + r[i + sx] + r[i + 1]);
+        return FN(dyn_lines)(2, r, i, sx, sy);
+    case 3:
+        if (z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0) return (T)0.5f * (r[i] + r[i + sy]);
+        return FN(cubic)(r[i - sy], r[i], r[i + sy], r[i + 2 * sy]);
+    case 4:
+        if (x == dx - 1 || z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0 || x == dx - 2 || x == 0)
+            return (T)0.25f * (r[i] + r[i + sy + 1] + r[i + 1] + r[i + sy]);
+        return FN(dyn_lines)(4, r, i, sx, sy);
+    case 5:
+        if (z == dz - 1 || y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0 || z == dz - 2 || z == 0)
+            return (T)0.25f * (r[i] + r[i + sy + sx] + r[i + sy] + r[i + sx]);
+        return FN(dyn_lines)(5, r, i, sx, sy);
+    default:
+        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0 || y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
+            return (T)0.125f * (r[i] + r[i + sy + sx + 1] + r[i + sy + sx] + r[i + sy + 1] +
+                                r[i + sx + 1] + r[i + 1] + r[i + sx] + r[i + sy]);
+        return FN(dyn_lines)(6, r, i, sx, sy);
+    }
+}
+
+/* Plain tricubic-family predictor, src/float.cpp:84-273 (templated copy in
+ * src/stz-rd.cpp:114-300): fixed stencils, boundary averages written as sums
+ * of scaled taps (0.5a + 0.5b) in that file's operand order. */
+static T FN(t_predict_plain)(int block, const T* r, int x, int y, int z, int dx, int dy, int dz)
+{
+    const size_t sx = (size_t)dx, sy = (size_t)dx * (size_t)dy;
+    const size_t i = ((size_t)z * dy + y) * dx + x;
+    switch (block) {
+    case 0:
+        if (x == dx - 1) return r[i];
+        if (x == dx - 2 || x == 0) return 0.5f * r[i] + 0.5f * r[i + 1];
+        return -(1.0f / 16.0f) * r[i - 1] + (9.0f / 16.0f) * r[i] + (9.0f / 16.0f) * r[i + 1] -
+               (1.0f / 16.0f) * r[i + 2];
+    case 1:
+        if (y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0) return 0.5f * r[i] + 0.5f * r[i + sx];
+        return -(1.0f / 16.0f) * r[i - sx] + (9.0f / 16.0f) * r[i] + (9.0f / 16.0f) * r[i + sx] -
+               (1.0f / 16.0f) * r[i + 2 * sx];
+    case 2:
+        if (x == dx - 1 || y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
+            return 0.25f * r[i] + 0.25f * r[i + sx + 1] + 0.25f * r[i + sx] + 0.25f * r[i + 1];
+        return 0.28125f * r[i] + 0.28125f * r[i + sx + 1] + 0.28125f * r[i + sx] + 0.28125f * r[i + 1] -
+               0.03125f * r[i - sx - 1] - 0.03125f * r[i + 2 * sx + 2] - 0.03125f * r[i + 2 * sx - 1] -
+               0.03125f * r[i - sx + 2];
+    case 3:
+        if (z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0) return 0.5f * r[i] + 0.5f * r[i + sy];
+        return -(1.0f / 16.0f) * r[i - sy] + (9.0f / 16.0f) * r[i] + (9.0f / 16.0f) * r[i + sy] -
+               (1.0f / 16.0f) * r[i + 2 * sy];
+    case 4:
+        if (x == dx - 1 || z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0 || x == dx - 2 || x == 0)
+            return 0.25f * r[i] + 0.25f * r[i + sy + 1] + 0.25f * r[i + 1] + 0.25f * r[i + sy];
+        return 0.28125f * r[i] + 0.28125f * r[i + sy + 1] + 0.28125f * r[i + 1] + 0.28125f * r[i + sy] -
+               0.03125f * r[i - sy - 1] - 0.03125f * r[i + 2 - sy] - 0.03125f * r[i + 2 * sy - 1] -
+               0.03125f * r[i + 2 * sy + 2];
+    case 5:
+        if (z == dz - 1 || y == dy - 1) return r[i];
+        if (y == dy - 2 || y == 0 || z == dz - 2 || z == 0)
+            return 0.25f * r[i] + 0.25f * r[i + sy + sx] + 0.25f * r[i + sy] + 0.25f * r[i + sx];
+        return 0.28125f * r[i] + 0.28125f * r[i + sy + sx] + 0.28125f * r[i + sy] + 0.28125f * r[i + sx] -
+               0.03125f * r[i - sy - sx] - 0.03125f * r[i + 2 * sy + 2 * sx] -
+               0.03125f * r[i + 2 * sy - sx] - 0.03125f * r[i + 2 * sx - sy];
+    default:
+        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return r[i];
+        if (z == dz - 2 || z == 0 || y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
+            return 0.125f * r[i] + 0.125f * r[i + sy + sx + 1] + 0.125f * r[i + sy + sx] +
+                   0.125f * r[i + sy + 1] + 0.125f * r[i + sx + 1] + 0.125f * r[i + 1] +
+                   0.125f * r[i + sx] + 0.125f * r[i + sy];
+        return 0.140625f * r[i] + 0.140625f * r[i + sy + sx + 1] + 0.140625f * r[i + sy + sx] +
+               0.140625f * r[i + sy + 1] + 0.140625f * r[i + sx + 1] + 0.140625f * r[i + 1] +
+               0.140625f * r[i + sx] + 0.140625f * r[i + sy] -
+               0.015625f * r[i - sy - sx - 1] - 0.015625f * r[i + 2 * sy + 2 * sx + 2] -
+               0.015625f * r[i + 2 * sy - sx + 2] - 0.015625f * r[i + 2 * sy + 2 * sx - 1] -
+               0.015625f * r[i - sy + 2 * sx + 2] - 0.015625f * r[i + 2 * sy - sx - 1] -
+               0.015625f * r[i - sy + 2 * sx - 1] - 0.015625f * r[i - sy - sx + 2];
+    }
+}
+
+static inline T FN(predict_any)(int predictor, int block, const T* r, int x, int y, int z, int dx, int dy,
+                                int dz)
+{
+    return predictor == 1 ? FN(t_predict_plain)(block, r, x, y, z, dx, dy, dz)
+                          : FN(t_predict)(block, r, x, y, z, dx, dy, dz);
+}
+
+/* One value of quantize_range_nodec, FD5:1216-1229 (the fallback loop
+ * FD5:1232-1249 yields the same code for every input). Returns the shifted
+ * code, 0 when unpredictable; *dec gets the decompressed residual. */
+static inline int FN(quant1)(T d, double eb, double recip, int radius, T* dec)
+{
+    const double ad = fabs((double)d) * recip;
+    const int in_range = ad < (double)(2 * radius - 1);
+    const double adc = in_range ? ad : 0.0;
+    const int half = ((int)adc + 1) >> 1;
+    const T dec_mag = (T)(2 * half * eb);
+    const T dec_k = (d < 0) ? -dec_mag : dec_mag;
+    const T derr = dec_k - d;
+    const int ok = in_range && (fabs((double)derr) <= eb);
+    if (!ok) return 0;
+    *dec = dec_k;
+    return (d < 0) ? radius - half : radius + half;
+}
+
+/* recover LUT entry, FD5:1531-1535. */
+static inline T FN(recover)(int q, double eb, int radius)
+{
+    return (T)(2 * (q - radius) * eb);
+}
+
+static long long FN(t_quantize)(const T* d, size_t n, double eb, int radius, int* q, T* unpred, size_t cap)
+{
+    ftz_on();
+    const double recip = 1.0 / eb;
+    size_t nu = 0;
+    for (size_t i = 0; i < n; ++i) {
+        T dec;
+        q[i] = FN(quant1)(d[i], eb, recip, radius, &dec);
+        if (q[i] == 0) {
+            if (nu >= cap) return -1;
+            unpred[nu++] = d[i];
+        }
+    }
+    return (long long)nu;
+}
+
+/* Level encode: residual of sub-block (block+1) against the predictor on the
+ * decoded coarse grid (FD5 preprocess + quantize, see the fd5ref shim for the
+ * reference's call sequence). The decoded fine grid uses the decoder's
+ * recover values, so it equals what the decompressor rebuilds. */
+static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, int dz, int predictor, double eb,
+                          int radius, int* q, T* unpred, size_t cap, size_t* counts, T* decoded)
+{
+    ftz_on();
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    const double recip = 1.0 / eb;
+    size_t nu = 0;
+    for (int b = 0; b < 7; ++b) {
+        const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        size_t nb = 0;
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const size_t i = ((size_t)z * dy + y) * dx + x;
+                    const size_t fi = (2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px;
+                    const T p = FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                    const T d = fine[fi] - p;
+                    T dec = 0;
+                    const int code = FN(quant1)(d, eb, recip, radius, &dec);
+                    q[(size_t)b * n + i] = code;
+                    if (code == 0) {
+                        if (nu >= cap) return -1;
+                        unpred[nu++] = d;
+                        ++nb;
+                    }
+                    if (decoded) {
+                        const T dq = code ? FN(recover)(code, eb, radius) : d;
+                        decoded[fi] = dq + p;
+                    }
+                }
+        counts[b] = nb;
+    }
+    if (decoded) {
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x)
+                    decoded[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] =
+                        coarse[((size_t)z * dy + y) * dx + x];
+    }
+    return 0;
+}
+
+/* Level decode: x' = dq + P (FD5:1049-1143), merged into the fine grid. */
+static void FN(t_level_decode)(const int* q, const T* unpred, const size_t* counts, const T* coarse, int dx, int dy,
+                           int dz, int predictor, double eb, int radius, T* out)
+{
+    ftz_on();
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    size_t u = 0;
+    for (int b = 0; b < 7; ++b) {
+        const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const size_t i = ((size_t)z * dy + y) * dx + x;
+                    const int code = q[(size_t)b * n + i];
+                    const T dq = code ? FN(recover)(code, eb, radius) : unpred[u++];
+                    out[(2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px] =
+                        dq + FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                }
+        (void)counts;
+    }
+    for (int z = 0; z < dz; ++z)
+        for (int y = 0; y < dy; ++y)
+            for (int x = 0; x < dx; ++x)
+                out[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] = coarse[((size_t)z * dy + y) * dx + x];
+}
+
+/* Subsample the field to the fine grid of one level: every s-th point. */
+static void FN(subsample)(const T* field, int nx, int ny, int nz, int s, T* out)
+{
+    const int ox = nx / s, oy = ny / s, oz = nz / s;
+    size_t o = 0;
+    for (int z = 0; z < oz; ++z)
+        for (int y = 0; y < oy; ++y)
+            for (int x = 0; x < ox; ++x)
+                out[o++] = field[((size_t)z * s * ny + (size_t)y * s) * nx + (size_t)x * s];
+}
+
+#undef FN
+#undef CAT
+#undef CAT_
