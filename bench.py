@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""STZ B200 benchmark: compress + full decompress of a 512^3 float32 field.
+
+Workload (the reference's headline config): 512x512x512 float32 lognormal field
+exp(1.5 g), g a seeded unit-variance Gaussian random field with P(k) ~ k^-3,
+value-range-relative error bound 1e-3 (pointwise max|x - x'| <= 1e-3 * range),
+zstd level 3 (the reference's final stage). One step = compress (field ->
+stream) + full decompress (stream -> field).
+
+  value : field bytes x 2 / step time, field and output resident in HBM, the
+          stream in host memory (the zstd stage runs on the host cores).
+  e2e   : the same through the host-buffer API: pinned host field in, host
+          output back, host<->device copies inside the timed region.
+
+Multi-GPU (torchrun): replicas only — every rank codes its own field, no
+collective on the data path; value = all ranks' bytes / max-over-ranks time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sc25-stz2_b200"))
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
+FALLBACK_HBM = 6650.0
+METRIC = "compress+decompress GB/s (512^3 f32 lognormal, rel eb 1e-3)"
+MULTS = (0.7, 2.7, 8.2)
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--size", type=int, default=512)
+    p.add_argument("--rel", type=float, default=1e-3)
+    p.add_argument("--zstd", type=int, default=3)
+    p.add_argument("--seed", type=int, default=2025)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+# ---- clocks ---------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---- CPU side: the reference's own code, timed on the host cores ------------------
+def cpu_reference_round_trip(field: np.ndarray, rel: float, radius: int = 32768) -> dict:
+    """One compress+decompress of `field` with the reference's functions
+    (oracle/_ref: FD5 split, predict, quantize, closed loop, recover,
+    depreprocess, merge) scheduled as FD5 schedules them, OpenMP on all host
+    cores. The SZ3-ncp Huffman/zstd stages are not available, so they are not
+    included: the CPU does strictly less work than the GPU step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    if not po.ref_available():
+        return {}
+    R = po.ref()
+    suf = "f32" if field.dtype == np.float32 else "f64"
+    enc = getattr(R, "fd5ref_level_encode_timed_" + suf)
+    enc.restype = C.c_longlong
+    enc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+    rec = getattr(R, "fd5ref_recover_parallel_" + suf)
+    rec.argtypes = [C.c_void_p, C.c_size_t, C.c_double, C.c_int, C.c_void_p]
+    nz, ny, nx = field.shape
+    K = po.num_levels(nx, ny, nz)
+    rng = float(field.max()) - float(field.min())
+    eb = rel * rng / max(MULTS)
+    ebk = [0.0] + [(MULTS[2] if k == K else MULTS[1] if k == K - 1 else MULTS[0]) * eb for k in range(1, K + 1)]
+    t0 = time.perf_counter()
+    coarse = np.ascontiguousarray(field[:: 1 << K, :: 1 << K, :: 1 << K])
+    coarsest = coarse
+    codes, unpred = [], 0
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = field if s == 1 else np.ascontiguousarray(field[::s, ::s, ::s])
+        dz, dy, dx = coarse.shape
+        q = np.empty(7 * dx * dy * dz, np.int32)
+        dec = np.empty(fine.shape, field.dtype) if k < K else None
+        unpred += enc(fine.ctypes.data, coarse.ctypes.data, dx, dy, dz, ebk[k], radius, q.ctypes.data,
+                      dec.ctypes.data if dec is not None else None)
+        codes.append(q)
+        coarse = dec
+    t1 = time.perf_counter()
+    coarse = coarsest
+    for k in range(1, K + 1):
+        q = codes[k - 1]
+        dq = np.empty(q.size, field.dtype)
+        rec(q.ctypes.data, q.size, ebk[k], radius, dq.ctypes.data)
+        coarse = po.ref_level_decode(dq, coarse, 1 if k == K else 0)
+    t2 = time.perf_counter()
+    return {"compress_s": t1 - t0, "decompress_s": t2 - t1, "unpred": int(unpred)}
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def make_field_host(n: int, seed: int) -> np.ndarray:
+    import torch
+    from stz_b200 import fields
+
+    if torch.cuda.is_available():
+        return fields.lognormal((n, n, n), seed, np.float32, device="cuda").cpu().numpy()
+    return fields.lognormal((n, n, n), seed, np.float32)
+
+
+# ---- reference arm ------------------------------------------------------------------
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    if not po.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libfd5ref.so missing"}))
+        return
+    n = args.size
+    field = make_field_host(n, args.seed)
+    sample = field
+    # size the sample so the whole run stays within a few minutes
+    first = cpu_reference_round_trip(sample, args.rel)
+    per = first["compress_s"] + first["decompress_s"]
+    while per * (args.steps + args.warmup) > 240 and sample.shape[0] > 64:
+        sample = np.ascontiguousarray(sample[: sample.shape[0] // 2])
+        r = cpu_reference_round_trip(sample, args.rel)
+        per = r["compress_s"] + r["decompress_s"]
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_reference_round_trip(sample, args.rel)
+    times = []
+    for _ in range(args.steps):
+        r = cpu_reference_round_trip(sample, args.rel)
+        times.append(r["compress_s"] + r["decompress_s"])
+    total = sum(times)
+    gbs = 2 * sample.nbytes * args.steps / total / 1e9
+    desc = (f"{sample.shape[2]}x{sample.shape[1]}x{sample.shape[0]} f32 lognormal per step: reference FD5 split/"
+            "predict/quantize/closed-loop/recover/depreprocess/merge on all host cores; SZ3-ncp Huffman+zstd "
+            "unavailable (not timed)")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": f"synthetic lognormal exp(1.5 g), g GRF k^-3, seed {args.seed}",
+        "config": {"workload": "512^3 f32 lognormal, rel eb 1e-3, compress + full decompress",
+                   "field": [n, n, n], "rel_eb": args.rel},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": cpu_cores(), "kind": "reference", "sample": desc},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+# ---- our arm ---------------------------------------------------------------------------
+def algorithmic_bytes(kernel: str, N: int, elem: int, K: int, raw_payload: int) -> float | None:
+    """Minimum HBM bytes one launch of `kernel` must move on the N-point field."""
+    fine_syms = 7 * N // 8
+    all_syms = sum(7 * (N >> (3 * j)) // 8 for j in range(K))
+    if kernel == "k_level_encode[finest]":
+        return fine_syms * elem + (N // 8) * elem + fine_syms * 2  # read 7 parities + ref grid, write codes
+    if kernel == "k_level_decode[finest]":
+        return fine_syms * 2 + (N // 8) * elem + N * elem  # read codes + ref grid, write the full field
+    if kernel == "k_decode":
+        return raw_payload + all_syms * 2  # read payload, write codes
+    if kernel == "k_encode":
+        return all_syms * 2 + raw_payload  # read codes, write payload
+    if kernel == "k_sub_bits":
+        return all_syms * 2
+    return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import stz_b200
+    from stz_b200 import fields
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    n = args.size
+    ctx = stz_b200.Context(local)
+    field = fields.lognormal((n, n, n), args.seed + rank, np.float32, device=f"cuda:{local}")
+    nbytes = field.numel() * field.element_size()
+    out = torch.empty_like(field)
+    opts = stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd)
+    stream = torch.cuda.ExternalStream(ctx.cuda_stream(), device=f"cuda:{local}")
+
+    def step():
+        s = ctx.compress(field, opts=opts)
+        ctx.decompress(s, out=out)
+        return s
+
+    for _ in range(args.warmup):
+        s = step()
+    torch.cuda.synchronize()
+    # correctness of the measured configuration
+    E = args.rel * (float(field.max()) - float(field.min()))
+    max_err = float((out.double() - field.double()).abs().max())
+    cr = nbytes / len(s)
+    info = s.info()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ctx.profile(True)
+    ctx.profile_reset()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    ev[0].record(stream)
+    for i in range(args.steps):
+        s = ctx.compress(field, opts=opts)
+        ev[2 * i + 1].record(stream)
+        ctx.decompress(s, out=out)
+        ev[2 * i + 2].record(stream)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    comp_ms = sum(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(args.steps))
+    dec_ms = sum(ev[2 * i + 1].elapsed_time(ev[2 * i + 2]) for i in range(args.steps))
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * 2 * nbytes * args.steps / (total_ms / 1e3) / 1e9
+    launches = int(sum(v[1] for v in prof.values()))
+
+    # end to end through the host-buffer API
+    e2e = None
+    if not args.no_e2e:
+        host_field = field.cpu().pin_memory()
+        host_out = np.empty((n, n, n), np.float32)
+        s = ctx.compress(host_field, opts=opts)
+        ctx.decompress(s, out=host_out)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            s = ctx.compress(host_field, opts=opts)
+            ctx.decompress(s, out=host_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        inf = s.info()
+        e2e = {"value": world * 2 * nbytes * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": nbytes + inf.raw_payload_bytes,
+               "d2h_bytes_per_step": nbytes + inf.raw_payload_bytes}
+        assert np.array_equal(host_out.view(np.uint32), out.cpu().numpy().view(np.uint32))
+
+    # roofline of the dominant kernel
+    peaks = {}
+    if os.path.exists(PEAKS_FILE):
+        peaks = json.load(open(PEAKS_FILE))
+    peak = peaks.get("hbm_gbs", FALLBACK_HBM)
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dl) = dom
+    alg = algorithmic_bytes(dname, field.numel(), 4, info.n_levels, info.raw_payload_bytes)
+    roof = None
+    if alg is not None and dl:
+        per_launch_s = dms / dl / 1e3
+        achieved = alg / per_launch_s / 1e9
+        traffic = None
+        if os.path.exists(TRAFFIC_FILE):
+            tr = json.load(open(TRAFFIC_FILE)).get(dname)
+            if tr:
+                traffic = tr.get("dram_bytes_per_launch")
+        roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
+                "ms_per_launch": dms / dl, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_round_trip(field.cpu().numpy(), args.rel)
+        if r:
+            sec = r["compress_s"] + r["decompress_s"]
+            cpu = {"value": 2 * nbytes / sec / 1e9, "unit": "GB/s", "cores": cpu_cores(), "kind": "reference",
+                   "sample": f"one full {n}^3 round trip: reference FD5 split/predict/quantize/closed-loop/recover/"
+                             "depreprocess/merge, OpenMP on all host cores; SZ3-ncp Huffman+zstd unavailable "
+                             "(not timed)",
+                   "compress_s": r["compress_s"], "decompress_s": r["decompress_s"]}
+
+    if rank == 0:
+        res = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": f"synthetic lognormal exp(1.5 g), g GRF k^-3 (FFT-filtered seeded white noise), seed {args.seed}+rank",
+            "config": {"workload": "512^3 f32 lognormal, rel eb 1e-3, compress + full decompress",
+                       "field": [n, n, n], "rel_eb": args.rel, "zstd_level": args.zstd,
+                       "l2": "inputs larger than L2 (512 MiB field per step)", "parallelism": f"replicas x{world}"},
+            "compress_gbs": world * nbytes * args.steps / (comp_ms / 1e3) / 1e9,
+            "decompress_gbs": world * nbytes * args.steps / (dec_ms / 1e3) / 1e9,
+            "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+        }
+        print(json.dumps(res))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

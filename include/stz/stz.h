@@ -1,0 +1,236 @@
+/*
+ * stz.h — C ABI of the B200-native STZ streaming compressor (libstz_b200.so).
+ *
+ * STZ ("streaming" hierarchical lossy compression of 3-D fields) splits a field
+ * into parity sub-blocks level by level, predicts each level's seven odd-parity
+ * sub-blocks from the decoded coarser grid, quantizes the residuals under an
+ * error bound, entropy-codes them per marker chunk, and finishes with zstd.
+ * Every decode mode of the reference is here: full, progressive resolution
+ * (1/2, 1/4, ... of each axis) and random-access box / slice.
+ *
+ * Reference: FabioGrosso/SC25-STZ2. The reference is a set of C++ programs
+ * whose stages are free function templates in one translation unit,
+ * src/zero_all_line_dynamic_random_access_optfast3_optcr_lb_fastdec5.cpp,
+ * cited below as FD5:<line>. Each entry point below names the reference
+ * function it replaces.
+ *
+ * Conventions
+ *   - Plain pointers and sizes, no exceptions. Every call returns stz_status;
+ *     stz_last_error() gives a thread-local message for the last failure.
+ *   - Dims are (nx, ny, nz) with x fastest (row-major z, y, x), as in the
+ *     reference (FD5:113).
+ *   - `_dev` entry points take CUDA device pointers on the context's device
+ *     and run on the context's stream; others take host pointers.
+ *   - The library owns stz_stream objects; callers own every output buffer.
+ *   - A context is used by one host thread at a time; streams are immutable
+ *     after creation and can be shared for reading.
+ */
+#ifndef STZ_B200_STZ_H
+#define STZ_B200_STZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum stz_status {
+    STZ_OK = 0,
+    STZ_ERR_ARG = 1,          /* null pointer, bad option value */
+    STZ_ERR_DIMS = 2,         /* dims not divisible as the format needs (FD5:1976-2006) */
+    STZ_ERR_CUDA = 3,         /* CUDA runtime failure (message in stz_last_error) */
+    STZ_ERR_NOMEM = 4,        /* host or device allocation failed */
+    STZ_ERR_FORMAT = 5,       /* stream bytes are not a valid container */
+    STZ_ERR_ZSTD = 6,         /* zstd reported an error */
+    STZ_ERR_RANGE = 7,        /* level / box / block index out of range */
+    STZ_ERR_UNSUPPORTED = 8   /* valid request this build does not handle */
+} stz_status;
+
+typedef enum stz_dtype { STZ_F32 = 0, STZ_F64 = 1 } stz_dtype;
+
+/* How opts.eb is interpreted. */
+typedef enum stz_eb_mode {
+    STZ_EB_ABS = 0, /* absolute */
+    STZ_EB_REL = 1  /* relative to the value range max - min (computeRange, FD5:92-104) */
+} stz_eb_mode;
+
+/* What the (absolute) bound E means. */
+typedef enum stz_bound_mode {
+    /* max |x - x'| <= E: the level multipliers are applied to E / max(mult). */
+    STZ_BOUND_POINTWISE = 0,
+    /* E is the reference CLI's eb: level k uses mult_k * E (FD5:2120-2129,
+     * 2139, 2203, 2249), so the pointwise bound is max(mult) * E. */
+    STZ_BOUND_REFERENCE = 1
+} stz_bound_mode;
+
+typedef enum stz_predictor {
+    STZ_PRED_DYNAMIC = 0, /* inverse-variance blend of cubic lines (FD5:624-748) */
+    STZ_PRED_CUBIC = 1    /* fixed tricubic-family stencils (src/float.cpp:84-273) */
+} stz_predictor;
+
+typedef struct stz_opts {
+    double eb;            /* error bound, see eb_mode / bound_mode */
+    int eb_mode;          /* stz_eb_mode */
+    int bound_mode;       /* stz_bound_mode */
+    double mult_base;     /* level multipliers, FD5 defaults 0.7 / 2.7 / 8.2 */
+    double mult_low;
+    double mult_high;
+    int radius;           /* quantizer radius (SZ3 default 32768, must be <= 32768) */
+    int chunk_high;       /* marker chunk edge of the finest level (FD5 default 32) */
+    int chunk_low;        /* marker chunk edge of the second-finest level (FD5 default 16) */
+    int zstd_level;       /* final lossless stage level (SZ3 default 3); 0 stores frames raw */
+    int predictor;        /* stz_predictor */
+    int threads;          /* host threads for zstd; 0 = all cores */
+} stz_opts;
+
+/* Reference defaults: rel eb 1e-3, pointwise, multipliers 0.7/2.7/8.2,
+ * radius 32768, chunks 32/16, zstd 3, dynamic predictor. */
+void stz_default_opts(stz_opts* opts);
+
+typedef struct stz_context stz_context;
+typedef struct stz_stream stz_stream;
+
+typedef struct stz_info {
+    int dtype;            /* stz_dtype */
+    int predictor;
+    size_t nx, ny, nz;
+    int n_levels;         /* refinement levels; decode levels 0..n_levels */
+    int radius;
+    int chunk_high, chunk_low;
+    double eb;            /* absolute eb the level multipliers were applied to */
+    double mult_base, mult_low, mult_high;
+    double max_error;     /* guaranteed max |x - x'| of a full decode */
+    size_t stream_bytes;  /* serialized size */
+    size_t raw_payload_bytes; /* entropy-coded bytes before zstd */
+} stz_info;
+
+const char* stz_status_string(stz_status s);
+/* Message of the last failing call on this thread ("" if none). */
+const char* stz_last_error(void);
+
+/* Context: one CUDA device, one CUDA stream, cached device/pinned buffers and
+ * a host thread pool for zstd. */
+stz_status stz_context_create(int device, stz_context** out);
+void stz_context_destroy(stz_context* ctx);
+/* Wait for all work queued on the context's stream. */
+stz_status stz_context_sync(stz_context* ctx);
+
+/* The CUDA stream (cudaStream_t) all of the context's work is queued on. */
+stz_status stz_context_stream(stz_context* ctx, void** stream);
+
+/* Per-kernel timing with CUDA events on the context's stream, for
+ * benchmarking. While enabled, every kernel launch is bracketed by events and
+ * its duration is accumulated under the kernel's name; launches are counted
+ * whether or not timing is enabled. */
+stz_status stz_profile_enable(stz_context* ctx, int on);
+stz_status stz_profile_reset(stz_context* ctx);
+/* Number of distinct kernel names recorded, and the totals of entry i. */
+stz_status stz_profile_count(stz_context* ctx, int* n);
+stz_status stz_profile_entry(stz_context* ctx, int i, const char** name, double* total_ms, uint64_t* launches);
+
+/* ---- whole-field codec ------------------------------------------------ */
+
+/* compress(field, dims, eb) -> stream. Replaces the compress phase of
+ * run_typed (FD5:2093-2309): split, base, low and high levels, each level's
+ * SZ_compress / SZ_compress_finish (FD5:1258-1437) and the final zstd. */
+stz_status stz_compress(stz_context* ctx, const void* field, stz_dtype dtype, size_t nx, size_t ny, size_t nz,
+                        const stz_opts* opts, stz_stream** out);
+stz_status stz_compress_dev(stz_context* ctx, const void* field_dev, stz_dtype dtype, size_t nx, size_t ny, size_t nz,
+                            const stz_opts* opts, stz_stream** out);
+
+/* Full decompress (FD5:2338-2453: base decode, SZ_decompress_separated per
+ * residual stream FD5:1466-1576, depreprocess + merge). out holds nx*ny*nz. */
+stz_status stz_decompress_full(stz_context* ctx, const stz_stream* s, void* out);
+stz_status stz_decompress_full_dev(stz_context* ctx, const stz_stream* s, void* out_dev);
+
+/* Progressive decompress: level 0 = full, 1 = half resolution (the reference's
+ * mid grid, FD5:2394), 2 = quarter (its decoded base, FD5:2339), ... up to
+ * n_levels. out holds (nx>>level)*(ny>>level)*(nz>>level) values; the
+ * resulting dims are written to out_dims when it is not null. */
+stz_status stz_decompress_level(stz_context* ctx, const stz_stream* s, int level, void* out, size_t out_dims[3]);
+stz_status stz_decompress_level_dev(stz_context* ctx, const stz_stream* s, int level, void* out_dev,
+                                    size_t out_dims[3]);
+
+/* Random-access box / slice (FD5:2460-2640): lo/hi are the inclusive corner
+ * coordinates of the query (make_query, FD5:1637: any order, clamped to the
+ * field; lo == hi on an axis makes a slice). Only the marker chunks and levels
+ * the box touches are entropy-decoded (planner FD5:1578-1839). out receives
+ * the box row-major (z, y, x); its dims are written to out_dims if not null. */
+stz_status stz_decompress_box(stz_context* ctx, const stz_stream* s, const int64_t lo[3], const int64_t hi[3],
+                              void* out, size_t out_dims[3]);
+stz_status stz_decompress_box_dev(stz_context* ctx, const stz_stream* s, const int64_t lo[3], const int64_t hi[3],
+                                  void* out_dev, size_t out_dims[3]);
+
+/* ---- stream objects --------------------------------------------------- */
+
+/* Serialized bytes (valid while the stream lives). */
+stz_status stz_stream_bytes(const stz_stream* s, const void** data, size_t* size);
+/* Parse serialized bytes (copied). */
+stz_status stz_stream_parse(stz_context* ctx, const void* data, size_t size, stz_stream** out);
+stz_status stz_stream_info(const stz_stream* s, stz_info* info);
+/* Decode the zstd frames once and keep the entropy-coded streams resident on
+ * the context's device, so later decodes skip zstd and the host->device copy. */
+stz_status stz_stream_upload(stz_context* ctx, stz_stream* s);
+void stz_stream_free(stz_stream* s);
+
+/* ---- reference function boundary (device pointers) --------------------- *
+ * The reference's own stage functions, one for one, for callers that drive
+ * the stages themselves. Block = sub_index - 1 (0..6); dims are the block's.  */
+
+/* slice_full_data (FD5:107-122): 8 sub-blocks written back to back in subs. */
+stz_status stz_split_dev(stz_context* ctx, stz_dtype dtype, const void* full, size_t nx, size_t ny, size_t nz,
+                         void* subs);
+/* merge_sub_blocks_to_full (FD5:68-90). */
+stz_status stz_merge_dev(stz_context* ctx, stz_dtype dtype, const void* subs, size_t hx, size_t hy, size_t hz,
+                         void* full);
+/* preprocess_block_zslab (FD5:1161-1175): diff = sub - P(ref) on z in [z0,z1). */
+stz_status stz_preprocess_block_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* sub,
+                                    const void* ref, void* diff, int dx, int dy, int dz, int z0, int z1);
+/* depreprocess_block_zslab (FD5:1177-1191): out = de + P(ref) on z in [z0,z1). */
+stz_status stz_depreprocess_block_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* de,
+                                      const void* ref, void* out, int dx, int dy, int dz, int z0, int z1);
+/* depreprocess_block_zslab_to_full (FD5:1145-1159): scatter into the
+ * (2dx,2dy,2dz) grid at the block's parity offsets. */
+stz_status stz_depreprocess_block_to_full_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block,
+                                              const void* de, const void* ref, void* full, int dx, int dy, int dz,
+                                              int z0, int z1);
+/* depreprocess_block with ROI bounds (FD5:978-999, 1193-1196): half-open
+ * [start, end) per axis. */
+stz_status stz_depreprocess_block_roi_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* de,
+                                          const void* ref, void* out, int dx, int dy, int dz, int end_x, int end_y,
+                                          int end_z, int start_x, int start_y, int start_z);
+/* quantize_range_nodec (FD5:1204-1253): int32 codes, unpredictable values in
+ * element order; *n_unpred receives their count. */
+stz_status stz_quantize_dev(stz_context* ctx, stz_dtype dtype, const void* data, size_t n, double eb, int radius,
+                            int32_t* q, void* unpred, size_t* n_unpred);
+/* Recover (FD5:1531-1535 and the unpredictable fallback FD5:1556-1562). */
+stz_status stz_dequantize_dev(stz_context* ctx, stz_dtype dtype, const int32_t* q, size_t n, double eb, int radius,
+                              const void* unpred, void* out);
+
+/* ROI planner (FD5:1578-1839) for a query [a, b] on a field of dims
+ * (nx,ny,nz), as a flat int64 record:
+ *   query x.b x.e y.b y.e z.b z.e is_slice,
+ *   n_high, then per high plan: block x.b x.e y.b y.e z.b z.e n_chunks chunks...,
+ *   n_regions, then per region: x.b x.e y.b y.e z.b z.e is_slice,
+ *   n_low, then per low plan: block x.b x.e y.b y.e z.b z.e n_chunks chunks...
+ * Returns the number of values written in *n_out (STZ_ERR_RANGE if cap is too
+ * small). */
+stz_status stz_plan_box(size_t nx, size_t ny, size_t nz, int chunk_high, int chunk_low, const int64_t a[3],
+                        const int64_t b[3], int64_t* out, size_t cap, size_t* n_out);
+
+/* ---- inspection (tests) --------------------------------------------------- */
+/* Quant codes of one residual stream in chunk-major order (the entropy
+ * coder's symbol order). level_from_coarse is 1..n_levels. */
+stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int level_from_coarse, int block,
+                                  uint16_t* codes, size_t cap, size_t* n_out);
+/* Canonical codebook the container format derives from a histogram of nbins
+ * code counts (host only): n_used symbols and lengths in canonical order. The
+ * reference's equivalent is SZ3-ncp HuffmanEncoder::preprocess_encode_fast
+ * (call site FD5:1401-1402), whose format is not available. */
+stz_status stz_debug_codebook(const uint32_t* hist, int nbins, uint16_t* sym, uint8_t* len, int* n_used);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STZ_B200_STZ_H */

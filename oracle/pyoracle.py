@@ -1,0 +1,258 @@
+"""ctypes bindings of the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+Two libraries:
+  * lib/libstz_oracle.so  the plain-C restatement (stz_oracle.c), built from
+    committed sources by `make -C oracle oracle` (or __graft_entry__.build()).
+  * _ref/libfd5ref.so     the reference's own FD5 translation unit compiled from
+    its sources (`make -C oracle ref`, only where the reference is mounted;
+    the built file travels with the repository snapshot).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "lib", "libstz_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libfd5ref.so")
+REFERENCE_SRC = "/root/reference/src"
+
+vp, sz, dbl, ci = C.c_void_p, C.c_size_t, C.c_double, C.c_int
+
+
+class Params(C.Structure):
+    _fields_ = [("dtype", ci), ("predictor", ci), ("radius", ci), ("chunk_high", ci), ("chunk_low", ci),
+                ("zstd_level", ci), ("eb", dbl), ("mult_base", dbl), ("mult_low", dbl), ("mult_high", dbl)]
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (and the reference shim when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref and os.path.isdir(REFERENCE_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_SRC={REFERENCE_SRC}"], check=True)
+
+
+_orc = None
+_ref = None
+
+
+def oracle() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        L = C.CDLL(ORACLE_SO)
+        L.stzo_compress.restype = C.c_longlong
+        L.stzo_compress.argtypes = [vp, ci, ci, ci, C.POINTER(Params), C.POINTER(C.POINTER(C.c_uint8))]
+        L.stzo_decompress.argtypes = [vp, sz, ci, vp, C.POINTER(ci)]
+        L.stzo_decompress_box.argtypes = [vp, sz, C.POINTER(ci), C.POINTER(ci), vp]
+        L.stzo_stream_info.argtypes = [vp, sz, C.POINTER(ci), C.POINTER(ci), C.POINTER(ci)]
+        L.stzo_debug_stream_codes.restype = C.c_longlong
+        L.stzo_debug_stream_codes.argtypes = [vp, sz, ci, ci, vp, sz]
+        L.stzo_free.argtypes = [vp]
+        L.stzo_plan.restype = C.c_longlong
+        L.stzo_plan.argtypes = [ci] * 11 + [vp, C.c_longlong]
+        L.stzo_codebook.argtypes = [vp, ci, vp, vp]
+        for suf in ("f32", "f64"):
+            getattr(L, "stzo_level_encode_" + suf).argtypes = [vp, vp, ci, ci, ci, ci, dbl, ci, vp, vp, sz, vp, vp]
+            getattr(L, "stzo_level_decode_" + suf).argtypes = [vp, vp, vp, vp, ci, ci, ci, ci, dbl, ci, vp]
+            getattr(L, "stzo_quantize_" + suf).restype = C.c_longlong
+            getattr(L, "stzo_quantize_" + suf).argtypes = [vp, sz, dbl, ci, vp, vp, sz]
+            getattr(L, "stzo_predict_" + suf).argtypes = [ci, vp, ci, ci, ci, ci, ci, ci]
+            getattr(L, "stzo_predict_plain_" + suf).argtypes = [ci, vp, ci, ci, ci, ci, ci, ci]
+        L.stzo_predict_f32.restype = C.c_float
+        L.stzo_predict_plain_f32.restype = C.c_float
+        L.stzo_predict_f64.restype = C.c_double
+        L.stzo_predict_plain_f64.restype = C.c_double
+        L.stzo_num_levels.argtypes = [ci, ci, ci]
+        L.stzo_level_chunk.argtypes = [ci] * 6
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_SO)
+        for suf in ("f32", "f64"):
+            getattr(L, "fd5ref_level_encode_" + suf).argtypes = [vp, vp, ci, ci, ci, dbl, ci, vp, vp, sz, vp, vp]
+            getattr(L, "fd5ref_level_decode_" + suf).argtypes = [vp, vp, ci, ci, ci, ci, vp]
+            getattr(L, "fd5ref_dequantize_" + suf).argtypes = [vp, sz, dbl, ci, vp, vp]
+            getattr(L, "fd5ref_quantize_range_nodec_" + suf).restype = C.c_longlong
+            getattr(L, "fd5ref_quantize_range_nodec_" + suf).argtypes = [vp, sz, dbl, ci, vp, vp, sz]
+            getattr(L, "fd5ref_preprocess_block_zslab_" + suf).argtypes = [ci, vp, vp, vp] + [ci] * 5
+            getattr(L, "fd5ref_depreprocess_block_zslab_" + suf).argtypes = [ci, vp, vp, vp] + [ci] * 5
+            getattr(L, "fd5ref_depreprocess_block_zslab_to_full_" + suf).argtypes = [ci, vp, vp, vp] + [ci] * 5
+            getattr(L, "fd5ref_depreprocess_block_roi_" + suf).argtypes = [ci, vp, vp, vp] + [ci] * 9
+            getattr(L, "fd5ref_slice_full_data_" + suf).argtypes = [vp, vp, ci, ci, ci]
+            getattr(L, "fd5ref_merge_sub_blocks_to_full_" + suf).argtypes = [vp, vp, ci, ci, ci]
+        L.fd5ref_plan.restype = C.c_longlong
+        L.fd5ref_plan.argtypes = [ci] * 11 + [vp, C.c_longlong]
+        _ref = L
+    return _ref
+
+
+def _p(a):
+    return a.ctypes.data_as(vp)
+
+
+def _suf(dtype) -> str:
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+# ---- hierarchy shape -------------------------------------------------------
+def num_levels(nx, ny, nz) -> int:
+    return oracle().stzo_num_levels(nx, ny, nz)
+
+
+def pointwise_eb(field: np.ndarray, rel: float, mults=(0.7, 2.7, 8.2)) -> float:
+    """eb the library uses for a relative, pointwise bound (value range as
+    computeRange, FD5:92-104)."""
+    rng = float(field.max()) - float(field.min())
+    E = rel * rng
+    if not (E > 0):
+        E = rel
+    return E / max(mults)
+
+
+# ---- whole-field codec -------------------------------------------------------
+def compress(field: np.ndarray, eb: float, predictor=0, radius=32768, chunk_high=32, chunk_low=16, zstd_level=3,
+             mults=(0.7, 2.7, 8.2)) -> bytes:
+    L = oracle()
+    a = np.ascontiguousarray(field)
+    nz, ny, nx = a.shape
+    p = Params(1 if a.dtype == np.float64 else 0, predictor, radius, chunk_high, chunk_low, zstd_level, eb, *mults)
+    out = C.POINTER(C.c_uint8)()
+    n = L.stzo_compress(_p(a), nx, ny, nz, C.byref(p), C.byref(out))
+    if n < 0:
+        raise ValueError(f"oracle compress failed ({n})")
+    b = C.string_at(out, n)
+    L.stzo_free(out)
+    return b
+
+
+def info(stream: bytes):
+    L = oracle()
+    dt, K = ci(), ci()
+    dims = (ci * 3)()
+    rc = L.stzo_stream_info(stream, len(stream), C.byref(dt), dims, C.byref(K))
+    if rc:
+        raise ValueError(f"bad stream ({rc})")
+    return (np.float64 if dt.value else np.float32), (dims[2], dims[1], dims[0]), K.value
+
+
+def decompress(stream: bytes, level: int = 0) -> np.ndarray:
+    L = oracle()
+    dt, (nz, ny, nx), K = info(stream)
+    out = np.empty((nz >> level, ny >> level, nx >> level), dtype=dt)
+    od = (ci * 3)()
+    rc = L.stzo_decompress(stream, len(stream), level, _p(out), od)
+    if rc:
+        raise ValueError(f"oracle decompress failed ({rc})")
+    return out
+
+
+def decompress_box(stream: bytes, lo, hi) -> np.ndarray:
+    L = oracle()
+    dt, (nz, ny, nx), K = info(stream)
+    dims = [nx, ny, nz]
+    ext = []
+    for ax in range(3):
+        a, b = int(lo[ax]), int(hi[ax])
+        if a == b:
+            ext.append(1)
+        else:
+            l_ = max(0, min(a, b))
+            h_ = min(dims[ax] - 1, max(a, b))
+            ext.append(max(h_, l_) - l_ + 1)
+    out = np.empty((ext[2], ext[1], ext[0]), dtype=dt)
+    rc = L.stzo_decompress_box(stream, len(stream), (ci * 3)(*lo), (ci * 3)(*hi), _p(out))
+    if rc:
+        raise ValueError(f"oracle box decode failed ({rc})")
+    return out
+
+
+def stream_codes(stream: bytes, k: int, block: int) -> np.ndarray:
+    L = oracle()
+    _, (nz, ny, nx), _ = info(stream)
+    buf = np.empty(nx * ny * nz, dtype=np.uint16)
+    n = L.stzo_debug_stream_codes(stream, len(stream), k, block, _p(buf), buf.size)
+    if n < 0:
+        raise ValueError(f"oracle stream decode failed ({n})")
+    return buf[:n].copy()
+
+
+def codebook(hist: np.ndarray):
+    L = oracle()
+    h = np.ascontiguousarray(hist, dtype=np.uint32)
+    sym = np.zeros(len(h), dtype=np.uint16)
+    ln = np.zeros(len(h), dtype=np.uint8)
+    n = L.stzo_codebook(_p(h), len(h), _p(sym), _p(ln))
+    return sym[:n].copy(), ln[:n].copy()
+
+
+# ---- level functions -----------------------------------------------------------
+def level_encode(fine, coarse, eb, radius=32768, predictor=0, decoded=True, use_ref=False):
+    """Codes (7, n) row-major per block, unpred values, counts, decoded fine grid."""
+    dz, dy, dx = coarse.shape
+    n = dx * dy * dz
+    q = np.zeros(7 * n, dtype=np.int32)
+    u = np.zeros(7 * n, dtype=coarse.dtype)
+    c = np.zeros(7, dtype=np.uint64)
+    d = np.zeros(fine.shape, dtype=coarse.dtype) if decoded else None
+    fine = np.ascontiguousarray(fine)
+    coarse = np.ascontiguousarray(coarse)
+    suf = _suf(coarse.dtype)
+    if use_ref:
+        if predictor != 0:
+            raise ValueError("the FD5 reference has only the dynamic predictor")
+        rc = getattr(ref(), "fd5ref_level_encode_" + suf)(_p(fine), _p(coarse), dx, dy, dz, eb, radius, _p(q), _p(u),
+                                                           u.size, _p(c), _p(d) if d is not None else None)
+    else:
+        rc = getattr(oracle(), "stzo_level_encode_" + suf)(_p(fine), _p(coarse), dx, dy, dz, predictor, eb, radius,
+                                                            _p(q), _p(u), u.size, _p(c), _p(d) if d is not None else None)
+    if rc:
+        raise ValueError("level encode failed")
+    return q.reshape(7, n), u[: int(c.sum())].copy(), c, d
+
+
+def ref_level_decode(dq7: np.ndarray, coarse: np.ndarray, mode: int) -> np.ndarray:
+    dz, dy, dx = coarse.shape
+    out = np.zeros((2 * dz, 2 * dy, 2 * dx), dtype=coarse.dtype)
+    getattr(ref(), "fd5ref_level_decode_" + _suf(coarse.dtype))(_p(np.ascontiguousarray(dq7)), _p(coarse), dx, dy, dz,
+                                                                mode, _p(out))
+    return out
+
+
+def ref_dequantize(q: np.ndarray, eb: float, radius: int, unpred: np.ndarray, dtype) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.int32)
+    out = np.zeros(q.size, dtype=dtype)
+    un = np.ascontiguousarray(unpred, dtype=dtype)
+    getattr(ref(), "fd5ref_dequantize_" + _suf(dtype))(_p(q), q.size, eb, radius, _p(un), _p(out))
+    return out
+
+
+def plan(dims_xyz, chunk_high, chunk_low, a, b, use_ref=False) -> np.ndarray:
+    out = np.zeros(1 << 20, dtype=np.int64)
+    fn = ref().fd5ref_plan if use_ref else oracle().stzo_plan
+    n = fn(*[int(v) for v in dims_xyz], chunk_high, chunk_low, *[int(v) for v in a], *[int(v) for v in b], _p(out),
+           out.size)
+    if n < 0:
+        raise ValueError("plan failed")
+    return out[:n].copy()
+
+
+def chunk_major(q_rm: np.ndarray, dims_zyx, C_: int) -> np.ndarray:
+    """Row-major block codes -> the container's chunk-major symbol order."""
+    dz, dy, dx = dims_zyx
+    a = q_rm.reshape(dz // C_, C_, dy // C_, C_, dx // C_, C_)
+    return a.transpose(0, 2, 4, 1, 3, 5).reshape(-1)

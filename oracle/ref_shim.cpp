@@ -130,6 +130,78 @@ int level_encode(const T* fine, const T* coarse, int dx, int dy, int dz, double 
     return 0;
 }
 
+// The same level step scheduled as run_typed schedules it, for timing: the
+// fine level's fused (block, 16-plane slab) task loop with a thread-local slab
+// buffer, preprocess_block_zslab + quantize_range_nodec per task and per-slab
+// unpredictable lists (FD5:2249-2296); when `decoded` is requested the
+// coarser-level tail follows: per-block writeDec emulation in parallel
+// (SZ_compress runs once per block in parallel, FD5:2199-2205), the parallel
+// depreprocess task loop and merge_sub_blocks_to_full (FD5:2207-2230).
+// Codes land in q (7 x n, row-major per block); unpredictable values are only
+// counted.
+template <typename T>
+long long level_encode_timed(const T* fine, const T* coarse, int dx, int dy, int dz, double eb, int radius, int* q,
+                             T* decoded)
+{
+    FtzGuard g;
+    const size_t n = static_cast<size_t>(dx) * dy * dz;
+    std::vector<T> subs_store(8 * n);
+    T* subs[8];
+    split8(subs_store.data(), n, subs);
+    slice_full_data(fine, subs, 2 * dx, 2 * dy, 2 * dz);
+    std::vector<T> dlut(static_cast<size_t>(radius) + 1);
+    for (size_t h = 0; h < dlut.size(); ++h) dlut[h] = static_cast<T>(2 * static_cast<int>(h) * eb);
+    const int nslab = (dz + kZChunk - 1) / kZChunk;
+    std::vector<std::array<int, 3>> tasks;
+    for (int block = 0; block < 7; ++block)
+        for (int z0 = 0; z0 < dz; z0 += kZChunk) tasks.push_back({block, z0, std::min(z0 + kZChunk, dz)});
+    const size_t plane = static_cast<size_t>(dx) * dy;
+    std::vector<std::vector<T>> unpred(7 * nslab);
+    std::vector<T> diff_store(decoded ? 7 * n : 0);
+    std::vector<std::vector<T>> slab_buf(omp_get_max_threads());
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < static_cast<int>(tasks.size()); ++t) {
+        const int block = tasks[t][0], z0 = tasks[t][1], z1 = tasks[t][2];
+        T* out;
+        if (decoded) {
+            out = diff_store.data() + block * n;
+        } else {
+            std::vector<T>& sb = slab_buf[omp_get_thread_num()];
+            if (sb.size() < static_cast<size_t>(kZChunk) * plane) sb.resize(static_cast<size_t>(kZChunk) * plane);
+            out = sb.data() - static_cast<size_t>(z0) * plane;
+        }
+        preprocess_block_zslab(block, subs[block + 1], coarse, out, dx, dy, dz, z0, z1);
+        const size_t i0 = static_cast<size_t>(z0) * plane, m = static_cast<size_t>(z1 - z0) * plane;
+        quantize_range_nodec(out + i0, m, eb, radius, dlut.data(), q + block * n + i0, unpred[block * nslab + z0 / kZChunk]);
+    }
+    long long nu = 0;
+    for (auto& u : unpred) nu += static_cast<long long>(u.size());
+    if (decoded) {
+#pragma omp parallel for
+        for (int block = 0; block < 7; ++block) {
+            const int* qb = q + block * n;
+            T* d = diff_store.data() + block * n;
+            for (size_t i = 0; i < n; ++i) {
+                if (qb[i] == 0) continue;
+                const int half = qb[i] >= radius ? qb[i] - radius : radius - qb[i];
+                d[i] = (d[i] < 0) ? -dlut[half] : dlut[half];
+            }
+        }
+        std::vector<T> de_store(7 * n);
+        T* de_sub[7];
+        split7(de_store.data(), n, de_sub);
+#pragma omp parallel for schedule(dynamic)
+        for (int t = 0; t < static_cast<int>(tasks.size()); ++t) {
+            const int block = tasks[t][0], z0 = tasks[t][1], z1 = tasks[t][2];
+            depreprocess_block_zslab(block, diff_store.data() + block * n, coarse, de_sub[block], dx, dy, dz, z0, z1);
+        }
+        T* all[8] = {const_cast<T*>(coarse), de_sub[0], de_sub[1], de_sub[2],
+                     de_sub[3], de_sub[4], de_sub[5], de_sub[6]};
+        merge_sub_blocks_to_full(all, decoded, dx, dy, dz);
+    }
+    return nu;
+}
+
 // Dequantize one residual stream exactly as SZ_decompress_separated does
 // (recover LUT FD5:1528-1535, unpredictable values consumed in row-major order
 // through LinearQuantizer::recover, FD5:1556-1562).
@@ -274,6 +346,24 @@ void push_range(std::vector<long long>& o, const AxisRange& r)
     {                                                                                                 \
         FtzGuard g;                                                                                   \
         dequantize<T>(q, n, eb, radius, unpred, out);                                                 \
+    }                                                                                                 \
+    extern "C" long long fd5ref_level_encode_timed_##SUF(const T* fine, const T* coarse, int dx,      \
+                                                         int dy, int dz, double eb, int radius,       \
+                                                         int* q, T* decoded)                          \
+    {                                                                                                 \
+        return level_encode_timed<T>(fine, coarse, dx, dy, dz, eb, radius, q, decoded);               \
+    }                                                                                                 \
+    /* recover with the LUT, chunk-parallel as the decoder's fused pass (FD5:1528-1544);             \
+       only for streams without unpredictable values */                                              \
+    extern "C" void fd5ref_recover_parallel_##SUF(const int* q, size_t n, double eb, int radius,      \
+                                                   T* out)                                            \
+    {                                                                                                 \
+        FtzGuard g;                                                                                   \
+        std::vector<T> lut(static_cast<size_t>(2 * radius) + 1);                                      \
+        for (size_t i = 0; i < lut.size(); ++i)                                                       \
+            lut[i] = static_cast<T>(2 * (static_cast<int>(i) - radius) * eb);                         \
+        _Pragma("omp parallel for") for (long long i = 0; i < static_cast<long long>(n); ++i)         \
+            out[i] = lut[q[i]];                                                                       \
     }                                                                                                 \
     extern "C" void fd5ref_level_decode_##SUF(const T* dq7, const T* coarse, int dx, int dy, int dz,  \
                                                int mode, T* out)                                      \

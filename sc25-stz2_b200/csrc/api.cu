@@ -1,0 +1,1420 @@
+// C ABI and pipeline orchestration of the STZ B200 library.
+//
+// Compress (stz_compress_dev):
+//   1. value range on the GPU when the bound is relative (computeRange,
+//      FD5:92-104);
+//   2. coarsest grid = field sampled every 2^K points (stored raw);
+//   3. one fused level-encode launch per level, coarse to fine (levels.cu);
+//   4. histogram windows to the host, canonical codebooks on the host pool;
+//   5. entropy coding on the GPU: code tables, plane bit counts, offsets scan
+//      (marker tables), encode, unpredictable-value gather, payload pack;
+//   6. per-layer zstd frames on the host pool and the container.
+// Decompress: zstd frames on the host pool into one pinned staging buffer, one
+// host->device copy, one decode launch for every chunk of every stream, then
+// one fused level-decode launch per level into the output (or an intermediate
+// grid). Box/slice queries decode only the planner's chunks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "host.h"
+#include "huffman.h"
+#include "levels.h"
+#include "roi.h"
+#include "stz/stz.h"
+#include "stz_internal.h"
+
+namespace {
+thread_local std::string g_err;
+}
+
+#define STZ_FAIL(code, msg)    \
+    do {                       \
+        g_err = (msg);         \
+        return (code);         \
+    } while (0)
+
+#define STZ_CUDA(x)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) {                                                            \
+            g_err = std::string(#x) + ": " + cudaGetErrorString(e_);                        \
+            return e_ == cudaErrorMemoryAllocation ? STZ_ERR_NOMEM : STZ_ERR_CUDA;          \
+        }                                                                                   \
+    } while (0)
+
+#define STZ_TRY(x)                  \
+    do {                            \
+        stz_status s_ = (x);        \
+        if (s_ != STZ_OK) return s_; \
+    } while (0)
+
+namespace stz {
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t b = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) cap = b;
+        else p = nullptr;
+        return e;
+    }
+    template <class T>
+    T* as() const
+    {
+        return (T*)p;
+    }
+};
+
+// Grow-only pinned host buffer.
+struct PinBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    PinBuf() = default;
+    PinBuf(const PinBuf&) = delete;
+    PinBuf& operator=(const PinBuf&) = delete;
+    ~PinBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t b = std::max<size_t>(bytes, 4096);
+        cudaError_t e = cudaHostAlloc(&p, b, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = b;
+        else p = nullptr;
+        return e;
+    }
+    template <class T>
+    T* as() const
+    {
+        return (T*)p;
+    }
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Shape of the hierarchy for given dims and options.
+struct Geometry {
+    int nx = 0, ny = 0, nz = 0, K = 0, radius = 0, chunk_high = 0, chunk_low = 0;
+    int c0[3] = {0, 0, 0};
+    std::vector<LevelGeom> lv;  // 1..K
+    std::vector<StreamDesc> sd; // stream (k-1)*7+b
+    uint64_t total_codes = 0, total_chunk_slots = 0, total_sub = 0, total_words = 0;
+    size_t n_fine_max = 0;      // largest intermediate decoded grid (elements)
+};
+
+static Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_low, int radius)
+{
+    Geometry g;
+    g.nx = nx, g.ny = ny, g.nz = nz;
+    g.radius = radius, g.chunk_high = chunk_high, g.chunk_low = chunk_low;
+    g.K = num_levels(nx, ny, nz);
+    g.c0[0] = nx >> g.K, g.c0[1] = ny >> g.K, g.c0[2] = nz >> g.K;
+    g.lv.resize(g.K + 1);
+    g.n_fine_max = (size_t)g.c0[0] * g.c0[1] * g.c0[2];
+    for (int k = 1; k <= g.K; ++k) {
+        LevelGeom& L = g.lv[k];
+        const int sh = g.K - k + 1;
+        L.dx = nx >> sh, L.dy = ny >> sh, L.dz = nz >> sh;
+        L.C = level_chunk(nx, ny, nz, g.K, k, chunk_high, chunk_low);
+        L.ncx = L.dx / L.C, L.ncy = L.dy / L.C, L.ncz = L.dz / L.C;
+        L.n = (size_t)L.dx * L.dy * L.dz;
+        if (k < g.K) g.n_fine_max = std::max(g.n_fine_max, 8 * L.n);
+        for (int b = 0; b < 7; ++b) {
+            StreamDesc s{};
+            s.code_off = g.total_codes;
+            g.total_codes += L.n;
+            s.chunk_base = g.total_chunk_slots;
+            g.total_chunk_slots += (uint64_t)L.nchunks() + 1;
+            s.sub_base = g.total_sub;
+            g.total_sub += (uint64_t)L.nchunks() * L.C;
+            s.word_base = g.total_words;
+            s.word_cap = (L.n * kMaxCodeLen + 31) / 32 + L.nchunks() + 4;
+            g.total_words += s.word_cap;
+            s.C = L.C;
+            s.ncx = L.ncx, s.ncy = L.ncy, s.ncz = L.ncz;
+            s.nchunks = L.nchunks();
+            s.radius = radius;
+            g.sd.push_back(s);
+        }
+    }
+    return g;
+}
+
+// CTA work items for chunk lists: groups of up to kCoderThreads / C chunks.
+static void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, const uint32_t* chunks,
+                     size_t n, int C)
+{
+    const size_t G = std::max(1, kCoderThreads / C);
+    for (size_t i = 0; i < n; i += G) {
+        const uint32_t cnt = (uint32_t)std::min(G, n - i);
+        work.push_back({stream, (uint32_t)ids.size(), cnt, 0});
+        ids.insert(ids.end(), chunks + i, chunks + i + cnt);
+    }
+}
+
+static void add_all_chunks(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, uint32_t nchunks,
+                           int C)
+{
+    std::vector<uint32_t> all(nchunks);
+    for (uint32_t i = 0; i < nchunks; ++i) all[i] = i;
+    add_work(work, ids, stream, all.data(), all.size(), C);
+}
+
+// Device-resident decode inputs of levels 1..kmax of one stream object.
+struct Prepared {
+    int kmax = 0;
+    std::vector<StreamDesc> sd;
+    std::vector<StreamHeader> hdr;
+    std::vector<std::vector<uint64_t>> unpred_prefix;  // per stream, per chunk: list offset
+    std::vector<uint64_t> ulist_off;                   // per stream: element offset in the unpred list
+    uint64_t total_codes = 0, total_unpred = 0;
+    DevBuf stage;
+    StreamDesc* d_sd = nullptr;
+    uint16_t* d_sym = nullptr;
+    uint8_t* d_len = nullptr;
+    uint32_t* d_sub = nullptr;
+    uint64_t* d_choff = nullptr;
+    uint8_t* d_ulist = nullptr;
+    uint32_t* d_payload = nullptr;
+    DevBuf coarsest;
+    DevBuf base;          // cached decoded base grid (level K-2 output) for box queries
+    bool base_valid = false;
+};
+
+}  // namespace stz
+
+using namespace stz;
+
+struct stz_context {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::unique_ptr<ThreadPool> pool;
+    // kernel profiling (stz_profile_*)
+    struct ProfRec {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<ProfRec> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::string> prof_names;
+    std::vector<double> prof_ms;
+    std::vector<uint64_t> prof_launches;
+    size_t prof_slot(const char* name)
+    {
+        for (size_t i = 0; i < prof_names.size(); ++i)
+            if (prof_names[i] == name) return i;
+        prof_names.emplace_back(name);
+        prof_ms.push_back(0.0);
+        prof_launches.push_back(0);
+        return prof_names.size() - 1;
+    }
+    cudaEvent_t event()
+    {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void flush_prof()
+    {
+        for (auto& r : pending) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess)
+                prof_ms[prof_slot(r.name)] += ms;
+            ev_pool.push_back(r.a);
+            ev_pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    ~stz_context()
+    {
+        flush_prof();
+        for (auto e : ev_pool) cudaEventDestroy(e);
+    }
+    DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
+        stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
+        tiles;
+    PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small;
+};
+
+struct stz_stream {
+    std::vector<uint8_t> bytes;
+    ParsedStream dir;
+    size_t raw_payload_bytes = 0;
+    std::unique_ptr<Prepared> resident;
+};
+
+namespace {
+
+// Counts the launches of one kernel and, when profiling is on, brackets them
+// with events on the context's stream.
+struct KScope {
+    stz_context* c;
+    cudaEvent_t b = nullptr;
+    KScope(stz_context* ctx, const char* name, int launches = 1) : c(ctx)
+    {
+        c->prof_launches[c->prof_slot(name)] += (uint64_t)launches;
+        if (c->prof_on) {
+            if (c->pending.size() > 4096) c->flush_prof();
+            cudaEvent_t a = c->event();
+            b = c->event();
+            cudaEventRecord(a, c->st);
+            c->pending.push_back({name, a, b});
+        }
+    }
+    ~KScope()
+    {
+        if (b) cudaEventRecord(b, c->st);
+    }
+};
+
+int pool_threads(int requested)
+{
+    if (requested > 0) return requested;
+    const unsigned h = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(h ? h : 1u, 64u));
+}
+
+stz_status check_opts(const stz_opts* o)
+{
+    if (!o) STZ_FAIL(STZ_ERR_ARG, "opts is null");
+    if (!(o->eb > 0) || !std::isfinite(o->eb)) STZ_FAIL(STZ_ERR_ARG, "eb must be a positive finite number");
+    if (o->eb_mode != STZ_EB_ABS && o->eb_mode != STZ_EB_REL) STZ_FAIL(STZ_ERR_ARG, "bad eb_mode");
+    if (o->bound_mode != STZ_BOUND_POINTWISE && o->bound_mode != STZ_BOUND_REFERENCE)
+        STZ_FAIL(STZ_ERR_ARG, "bad bound_mode");
+    if (!(o->mult_base > 0) || !(o->mult_low > 0) || !(o->mult_high > 0)) STZ_FAIL(STZ_ERR_ARG, "multipliers must be > 0");
+    if (o->radius < 1 || o->radius > 32768) STZ_FAIL(STZ_ERR_ARG, "radius must be in [1, 32768]");
+    if (o->zstd_level < 0 || o->zstd_level > 22) STZ_FAIL(STZ_ERR_ARG, "zstd_level must be in [0, 22]");
+    if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    return STZ_OK;
+}
+
+// ---- compress ----------------------------------------------------------------
+template <typename T>
+stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int nz, const stz_opts& o,
+                         stz_stream** out)
+{
+    cudaStream_t st = ctx->st;
+    const Geometry g = make_geometry(nx, ny, nz, o.chunk_high, o.chunk_low, o.radius);
+    const int K = g.K, R2 = 2 * o.radius;
+    const int nstreams = 7 * K;
+    const size_t N = (size_t)nx * ny * nz;
+    const size_t elem = sizeof(T);
+
+    // error bound: value range as computeRange (FD5:92-104)
+    STZ_CUDA(ctx->minmax.ensure(16));
+    STZ_CUDA(ctx->h_small.ensure(64));
+    {
+        KScope ks(ctx, "k_minmax");
+        launch_minmax<T>(field, N, ctx->minmax.as<double>(), st);
+    }
+    STZ_CUDA(cudaMemcpyAsync(ctx->h_small.p, ctx->minmax.p, 16, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaStreamSynchronize(st));
+    const unsigned long long* mk = ctx->h_small.as<unsigned long long>();
+    const double lo = minmax_key_to_double(mk[0]), hi = minmax_key_to_double(mk[1]);
+    double E = o.eb;
+    if (o.eb_mode == STZ_EB_REL) {
+        E = o.eb * (hi - lo);
+        if (!(E > 0) || !std::isfinite(E)) E = o.eb;  // constant (or non-finite) field: bound taken as absolute
+    }
+    // The quantizer bounds each residual by eb, but the reconstruction
+    // dq + P is rounded once more in T, so the reference overshoots its bound
+    // by up to ~1.5 ulp of the largest magnitude. The pointwise mode leaves
+    // 4 ulp of slack so that max|x - x'| <= E holds when checked in FP64.
+    double eb = E;
+    if (o.bound_mode == STZ_BOUND_POINTWISE) {
+        const double ulp = sizeof(T) == 4 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
+        const double slack = 4.0 * std::max(std::fabs(lo), std::fabs(hi)) * ulp;
+        const double Eb = (std::isfinite(slack) && E > 2.0 * slack) ? E - slack : 0.5 * E;
+        eb = Eb / std::max({o.mult_base, o.mult_low, o.mult_high});
+    }
+    std::vector<double> ebk(K + 1);
+    for (int k = 1; k <= K; ++k) ebk[k] = (k == K ? o.mult_high : k == K - 1 ? o.mult_low : o.mult_base) * eb;
+
+    // buffers
+    STZ_CUDA(ctx->grid[0].ensure(g.n_fine_max * elem));
+    STZ_CUDA(ctx->grid[1].ensure(g.n_fine_max * elem));
+    STZ_CUDA(ctx->codes.ensure(g.total_codes * 2));
+    STZ_CUDA(ctx->unpred_dense.ensure(g.total_codes * elem));
+    STZ_CUDA(ctx->unpred_cnt.ensure(g.total_chunk_slots * 4));
+    STZ_CUDA(ctx->hist.ensure((size_t)nstreams * R2 * 4));
+    STZ_CUDA(ctx->hist_out.ensure((size_t)nstreams * 4));
+    STZ_CUDA(cudaMemsetAsync(ctx->hist.p, 0, (size_t)nstreams * R2 * 4, st));
+    STZ_CUDA(cudaMemsetAsync(ctx->hist_out.p, 0, (size_t)nstreams * 4, st));
+    STZ_CUDA(cudaMemsetAsync(ctx->unpred_cnt.p, 0, g.total_chunk_slots * 4, st));
+
+    // coarsest grid
+    const size_t n0 = (size_t)g.c0[0] * g.c0[1] * g.c0[2];
+    int cur = 0;
+    {
+        KScope ks(ctx, "k_subsample");
+        launch_subsample<T>(field, nx, ny, nz, 1 << K, ctx->grid[cur].as<T>(), st);
+    }
+    std::vector<T> coarsest(n0);
+    STZ_CUDA(cudaMemcpyAsync(coarsest.data(), ctx->grid[cur].p, n0 * elem, cudaMemcpyDeviceToHost, st));
+
+    // levels, coarse to fine
+    for (int k = 1; k <= K; ++k) {
+        const StreamDesc& s0 = g.sd[(size_t)(k - 1) * 7];
+        LevelEncodeArgs<T> a;
+        a.field = field;
+        a.fsx = (size_t)nx;
+        a.fsy = (size_t)nx * ny;
+        a.stride = 1 << (K - k);
+        a.coarse = ctx->grid[cur].as<T>();
+        a.geo = g.lv[k];
+        a.predictor = o.predictor;
+        a.codes = ctx->codes.as<uint16_t>() + s0.code_off;
+        a.unpred_dense = ctx->unpred_dense.as<T>() + s0.code_off;
+        a.unpred_cnt = ctx->unpred_cnt.as<uint32_t>() + s0.chunk_base;
+        a.hist_full = ctx->hist.as<uint32_t>() + (size_t)(k - 1) * 7 * R2;
+        a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
+        a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
+        a.qp.eb = ebk[k];
+        a.qp.recip = 1.0 / ebk[k];
+        a.qp.radius = o.radius;
+        {
+            KScope ks(ctx, k == K ? "k_level_encode[finest]" : "k_level_encode[coarser]");
+            launch_level_encode<T>(a, st);
+        }
+        cur = 1 - cur;
+    }
+    STZ_CUDA(cudaGetLastError());
+
+    // histogram windows + outside counts + unpred counts to the host
+    const int wlo = std::max(0, o.radius - kHistWindow / 2);
+    const int wn = std::min(kHistWindow, R2 - wlo);
+    STZ_CUDA(ctx->h_hist.ensure((size_t)nstreams * wn * 4));
+    const size_t meta_bytes = (size_t)nstreams * 4 + g.total_chunk_slots * 4;
+    STZ_CUDA(ctx->h_meta.ensure(meta_bytes));
+    STZ_CUDA(cudaMemcpy2DAsync(ctx->h_hist.p, (size_t)wn * 4, ctx->hist.as<uint32_t>() + wlo, (size_t)R2 * 4,
+                               (size_t)wn * 4, (size_t)nstreams, cudaMemcpyDeviceToHost, st));
+    uint32_t* h_out = ctx->h_meta.as<uint32_t>();
+    uint32_t* h_ucnt = h_out + nstreams;
+    STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaStreamSynchronize(st));
+
+    // codebooks
+    std::vector<std::vector<uint16_t>> syms(nstreams);
+    std::vector<std::vector<uint8_t>> lens(nstreams);
+    std::vector<std::vector<uint32_t>> fullh(nstreams);
+    for (int s = 0; s < nstreams; ++s)
+        if (h_out[s]) {
+            fullh[s].resize(R2);
+            STZ_CUDA(cudaMemcpy(fullh[s].data(), ctx->hist.as<uint32_t>() + (size_t)s * R2, (size_t)R2 * 4,
+                                cudaMemcpyDeviceToHost));
+        }
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        if (h_out[s]) build_codebook(fullh[s].data(), R2, 0, syms[s], lens[s]);
+        else build_codebook(ctx->h_hist.as<uint32_t>() + s * (size_t)wn, wn, wlo, syms[s], lens[s]);
+    });
+    std::vector<StreamDesc> sd = g.sd;
+    uint32_t cb_total = 0;
+    for (int s = 0; s < nstreams; ++s) {
+        sd[s].cb_off = cb_total;
+        sd[s].n_used = (uint32_t)syms[s].size();
+        cb_total += sd[s].n_used;
+    }
+    // unpredictable values: per chunk list offsets
+    std::vector<UnpredWork> uwork;
+    std::vector<uint64_t> unpred_off(nstreams + 1, 0);
+    for (int s = 0; s < nstreams; ++s) {
+        uint64_t acc = unpred_off[s];
+        const uint32_t* cnt = h_ucnt + sd[s].chunk_base;
+        for (uint32_t c = 0; c < sd[s].nchunks; ++c) {
+            if (cnt[c]) uwork.push_back({(uint32_t)s, c, acc, cnt[c]});
+            acc += cnt[c];
+        }
+        unpred_off[s + 1] = acc;
+    }
+    const uint64_t total_unpred = unpred_off[nstreams];
+
+    // work list over every chunk of every stream
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+
+    // upload: sd | cb_sym | cb_len | work | ids | uwork
+    const size_t o_sd = 0, o_sym = align256(o_sd + sd.size() * sizeof(StreamDesc));
+    const size_t o_len = align256(o_sym + (size_t)cb_total * 2), o_work = align256(o_len + cb_total);
+    const size_t o_ids = align256(o_work + work.size() * sizeof(CtaWork));
+    const size_t o_uw = align256(o_ids + ids.size() * 4), up_bytes = align256(o_uw + uwork.size() * sizeof(UnpredWork));
+    STZ_CUDA(ctx->h_stage.ensure(up_bytes));
+    uint8_t* hs = ctx->h_stage.as<uint8_t>();
+    std::memcpy(hs + o_sd, sd.data(), sd.size() * sizeof(StreamDesc));
+    for (int s = 0; s < nstreams; ++s) {
+        std::memcpy(hs + o_sym + 2 * (size_t)sd[s].cb_off, syms[s].data(), 2 * syms[s].size());
+        std::memcpy(hs + o_len + sd[s].cb_off, lens[s].data(), lens[s].size());
+    }
+    std::memcpy(hs + o_work, work.data(), work.size() * sizeof(CtaWork));
+    std::memcpy(hs + o_ids, ids.data(), ids.size() * 4);
+    if (!uwork.empty()) std::memcpy(hs + o_uw, uwork.data(), uwork.size() * sizeof(UnpredWork));
+    STZ_CUDA(ctx->sd.ensure(up_bytes));
+    STZ_CUDA(cudaMemcpyAsync(ctx->sd.p, hs, up_bytes, cudaMemcpyHostToDevice, st));
+    uint8_t* dstage = ctx->sd.as<uint8_t>();
+    const StreamDesc* d_sd = (const StreamDesc*)(dstage + o_sd);
+    const uint16_t* d_sym = (const uint16_t*)(dstage + o_sym);
+    const uint8_t* d_len = (const uint8_t*)(dstage + o_len);
+    const CtaWork* d_work = (const CtaWork*)(dstage + o_work);
+    const uint32_t* d_ids = (const uint32_t*)(dstage + o_ids);
+    const UnpredWork* d_uw = (const UnpredWork*)(dstage + o_uw);
+
+    // entropy coding
+    STZ_CUDA(ctx->ctab.ensure((size_t)nstreams * R2 * 4));
+    STZ_CUDA(ctx->sub_bits.ensure(g.total_sub * 4));
+    STZ_CUDA(ctx->sub_off.ensure(g.total_sub * 4));
+    STZ_CUDA(ctx->chunk_off.ensure(g.total_chunk_slots * 8));
+    STZ_CUDA(ctx->stream_words.ensure((size_t)nstreams * 8 * 3));
+    STZ_CUDA(ctx->payload.ensure(g.total_words * 4));
+    STZ_CUDA(ctx->ulist.ensure(std::max<uint64_t>(total_unpred, 1) * elem));
+    {
+        KScope ks(ctx, "k_expand_codebook");
+        launch_expand_codebook(d_sd, nstreams, d_sym, d_len, ctx->ctab.as<uint32_t>(), st);
+    }
+    {
+        KScope ks(ctx, "k_sub_bits");
+        launch_sub_bits(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), ctx->ctab.as<uint32_t>(),
+                        ctx->sub_bits.as<uint32_t>(), st);
+    }
+    {
+        KScope ks(ctx, "k_scan_stream");
+        launch_scan_streams(d_sd, nstreams, ctx->sub_bits.as<uint32_t>(), ctx->sub_off.as<uint32_t>(),
+                            ctx->chunk_off.as<uint64_t>(), ctx->stream_words.as<uint64_t>(),
+                            ctx->payload.as<uint32_t>(), st);
+    }
+    {
+        KScope ks(ctx, "k_encode");
+        launch_encode(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), ctx->ctab.as<uint32_t>(),
+                      ctx->sub_off.as<uint32_t>(), ctx->sub_bits.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
+                      ctx->payload.as<uint32_t>(), st);
+    }
+    if (!uwork.empty()) {
+        KScope ks(ctx, "k_unpred_move");
+        launch_unpred_move<T>(true, d_uw, (int)uwork.size(), d_sd, ctx->codes.as<uint16_t>(),
+                              ctx->unpred_dense.as<T>(), ctx->ulist.as<T>(), st);
+    }
+    STZ_CUDA(cudaGetLastError());
+
+    // tables to the host
+    const size_t t_words = 0, t_choff = align256(t_words + (size_t)nstreams * 8);
+    const size_t t_sub = align256(t_choff + g.total_chunk_slots * 8);
+    const size_t t_ul = align256(t_sub + g.total_sub * 4), t_bytes = align256(t_ul + total_unpred * elem);
+    STZ_CUDA(ctx->h_io.ensure(t_bytes));
+    uint8_t* ht = ctx->h_io.as<uint8_t>();
+    STZ_CUDA(cudaMemcpyAsync(ht + t_words, ctx->stream_words.p, (size_t)nstreams * 8, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaMemcpyAsync(ht + t_choff, ctx->chunk_off.p, g.total_chunk_slots * 8, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaMemcpyAsync(ht + t_sub, ctx->sub_off.p, g.total_sub * 4, cudaMemcpyDeviceToHost, st));
+    if (total_unpred)
+        STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaStreamSynchronize(st));
+    const uint64_t* words = (const uint64_t*)(ht + t_words);
+
+    // pack payloads contiguously and copy them back
+    std::vector<uint64_t> meta(3 * (size_t)nstreams);
+    uint64_t packed_total = 0;
+    for (int s = 0; s < nstreams; ++s) {
+        meta[s] = sd[s].word_base;
+        meta[nstreams + s] = packed_total;
+        meta[2 * (size_t)nstreams + s] = words[s];
+        packed_total += words[s];
+    }
+    STZ_CUDA(ctx->pack_meta.ensure(meta.size() * 8));
+    STZ_CUDA(ctx->h_small.ensure(meta.size() * 8));
+    std::memcpy(ctx->h_small.p, meta.data(), meta.size() * 8);
+    STZ_CUDA(cudaMemcpyAsync(ctx->pack_meta.p, ctx->h_small.p, meta.size() * 8, cudaMemcpyHostToDevice, st));
+    STZ_CUDA(ctx->packed.ensure(std::max<uint64_t>(packed_total, 1) * 4));
+    const uint64_t* pm = ctx->pack_meta.as<uint64_t>();
+    {
+        KScope ks(ctx, "k_pack_payload");
+        launch_pack_payload(ctx->payload.as<uint32_t>(), pm, pm + nstreams, pm + 2 * nstreams, nstreams,
+                            ctx->packed.as<uint32_t>(), st);
+    }
+    STZ_CUDA(ctx->h_payload.ensure(std::max<uint64_t>(packed_total, 1) * 4));
+    STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.p, ctx->packed.p, packed_total * 4, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaStreamSynchronize(st));
+
+    // container
+    FileHeader h;
+    h.dtype = sizeof(T) == 8 ? 1 : 0;
+    h.predictor = o.predictor;
+    h.nx = nx, h.ny = ny, h.nz = nz, h.K = K, h.radius = o.radius;
+    h.chunk_high = o.chunk_high, h.chunk_low = o.chunk_low, h.zstd_level = o.zstd_level;
+    h.eb = eb, h.mult_base = o.mult_base, h.mult_low = o.mult_low, h.mult_high = o.mult_high;
+    h.c0[0] = g.c0[0], h.c0[1] = g.c0[1], h.c0[2] = g.c0[2];
+    std::vector<LevelDir> levels(K + 1);
+    for (int k = 1; k <= K; ++k) {
+        levels[k].dx = g.lv[k].dx, levels[k].dy = g.lv[k].dy, levels[k].dz = g.lv[k].dz;
+        levels[k].C = g.lv[k].C;
+        levels[k].eb = ebk[k];
+    }
+    std::vector<StreamParts> parts(nstreams);
+    const uint64_t* choff = (const uint64_t*)(ht + t_choff);
+    const uint32_t* subo = (const uint32_t*)(ht + t_sub);
+    const uint8_t* ul = ht + t_ul;
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        const StreamDesc& d = sd[s];
+        StreamParts& p = parts[s];
+        append_stream_header(p.hdr, syms[s].data(), lens[s].data(), d.n_used, unpred_off[s + 1] - unpred_off[s],
+                             ul + unpred_off[s] * elem, elem, h_ucnt + d.chunk_base, choff + d.chunk_base,
+                             subo + d.sub_base, (int)d.nchunks, (int)d.C);
+        p.words = ctx->h_payload.as<uint32_t>() + meta[nstreams + s];
+        p.chunk_word_off = choff + d.chunk_base;
+        p.layers = (int)d.ncz;
+        p.chunks_per_layer = (int)(d.ncx * d.ncy);
+    });
+    auto* so = new (std::nothrow) stz_stream();
+    if (!so) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
+    so->bytes = write_container(h, coarsest.data(), levels, parts, *ctx->pool);
+    so->raw_payload_bytes = packed_total * 4;
+    const std::string pe = parse_stream(so->bytes.data(), so->bytes.size(), so->dir);
+    if (!pe.empty()) {
+        delete so;
+        STZ_FAIL(STZ_ERR_FORMAT, "internal: written stream does not parse: " + pe);
+    }
+    *out = so;
+    return STZ_OK;
+}
+
+// ---- decode preparation -------------------------------------------------------
+stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
+{
+    const ParsedStream& ps = s->dir;
+    const FileHeader& h = ps.h;
+    const size_t elem = h.elem();
+    const int nstreams = 7 * kmax;
+    p.kmax = kmax;
+    p.sd.assign(nstreams, StreamDesc{});
+    p.hdr.assign(nstreams, StreamHeader{});
+    std::atomic<int> bad{0};
+    const uint8_t* bytes = s->bytes.data();
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t i) {
+        const int k = (int)i / 7 + 1, b = (int)i % 7;
+        const LevelDir& L = ps.lv[k];
+        const StreamDir& d = L.s[b];
+        std::vector<uint8_t> raw(d.hdr_raw);
+        const int nch = (L.dx / L.C) * (L.dy / L.C) * (L.dz / L.C);
+        if (!decode_frame(bytes + d.data_off, d.hdr_stored, d.hdr_raw, raw.data())) bad = 1;
+        else if (!parse_stream_header(raw.data(), raw.size(), nch, L.C, elem, p.hdr[i])) bad = 2;
+    });
+    if (bad) STZ_FAIL(STZ_ERR_FORMAT, bad == 1 ? "stream header frame does not decode" : "bad stream header");
+    // layout
+    uint64_t codes = 0, chunks = 0, subs = 0, words = 0, syms = 0, unp = 0;
+    p.ulist_off.assign(nstreams + 1, 0);
+    p.unpred_prefix.assign(nstreams, {});
+    for (int i = 0; i < nstreams; ++i) {
+        const int k = i / 7 + 1;
+        const LevelDir& L = ps.lv[k];
+        const StreamHeader& H = p.hdr[i];
+        StreamDesc& d = p.sd[i];
+        d.C = L.C;
+        d.ncx = L.dx / L.C, d.ncy = L.dy / L.C, d.ncz = L.dz / L.C;
+        d.nchunks = d.ncx * d.ncy * d.ncz;
+        d.radius = h.radius;
+        d.code_off = codes;
+        codes += (uint64_t)L.dx * L.dy * L.dz;
+        d.chunk_base = chunks;
+        chunks += d.nchunks + 1;
+        d.sub_base = subs;
+        subs += (uint64_t)d.nchunks * d.C;
+        d.cb_off = (uint32_t)syms;
+        d.n_used = (uint32_t)H.sym.size();
+        syms += d.n_used;
+        uint64_t raw = 0;
+        for (uint64_t v : L.s[i % 7].lr) raw += v;
+        if (H.chunk_word_off.back() * 4 != raw) STZ_FAIL(STZ_ERR_FORMAT, "marker table does not match payload size");
+        if (d.n_used == 0 || (d.n_used == 1 && raw != 0)) STZ_FAIL(STZ_ERR_FORMAT, "bad codebook");
+        // codebook: symbols in range, sorted canonically, Kraft sum <= 1
+        {
+            uint64_t kraft = 0;
+            for (uint32_t j = 0; j < d.n_used; ++j) {
+                if (H.sym[j] >= 2 * h.radius) STZ_FAIL(STZ_ERR_FORMAT, "codebook symbol out of range");
+                if (j && (H.len[j] < H.len[j - 1] || (H.len[j] == H.len[j - 1] && H.sym[j] <= H.sym[j - 1])))
+                    STZ_FAIL(STZ_ERR_FORMAT, "codebook not in canonical order");
+                if (d.n_used > 1) {
+                    if (H.len[j] == 0) STZ_FAIL(STZ_ERR_FORMAT, "zero-length code");
+                    kraft += 1ull << (kMaxCodeLen - H.len[j]);
+                }
+                if (H.sym[j] == 0 && H.n_unpred == 0) STZ_FAIL(STZ_ERR_FORMAT, "code 0 without unpredictable values");
+            }
+            if (kraft > (1ull << kMaxCodeLen)) STZ_FAIL(STZ_ERR_FORMAT, "codebook violates the Kraft inequality");
+        }
+        for (uint32_t c = 0; c < d.nchunks; ++c) {
+            if (H.chunk_word_off[c] > H.chunk_word_off[c + 1]) STZ_FAIL(STZ_ERR_FORMAT, "bad marker table");
+            const uint64_t cbits = 32 * (H.chunk_word_off[c + 1] - H.chunk_word_off[c]);
+            for (uint32_t lz = 0; lz < d.C; ++lz) {
+                const uint32_t v = H.sub_off[(size_t)c * d.C + lz];
+                if (v > cbits || (lz && v < H.sub_off[(size_t)c * d.C + lz - 1]))
+                    STZ_FAIL(STZ_ERR_FORMAT, "bad plane offsets");
+            }
+        }
+        d.word_base = words;
+        d.word_cap = raw / 4 + 4;
+        words += d.word_cap;
+        p.ulist_off[i] = unp;
+        auto& pre = p.unpred_prefix[i];
+        pre.resize(d.nchunks + 1);
+        uint64_t acc = 0;
+        for (uint32_t c = 0; c < d.nchunks; ++c) {
+            pre[c] = acc;
+            acc += H.unpred_count[c];
+        }
+        pre[d.nchunks] = acc;
+        if (acc != H.n_unpred) STZ_FAIL(STZ_ERR_FORMAT, "unpredictable counts do not match");
+        unp += H.n_unpred;
+    }
+    p.ulist_off[nstreams] = unp;
+    p.total_codes = codes;
+    p.total_unpred = unp;
+    const size_t o_sd = 0, o_sym = align256(nstreams * sizeof(StreamDesc)), o_len = align256(o_sym + syms * 2);
+    const size_t o_sub = align256(o_len + syms), o_ch = align256(o_sub + subs * 4), o_ul = align256(o_ch + chunks * 8);
+    const size_t o_pl = align256(o_ul + unp * elem), total = align256(o_pl + words * 4);
+    STZ_CUDA(ctx->h_stage.ensure(total));
+    uint8_t* hs = ctx->h_stage.as<uint8_t>();
+    std::memcpy(hs + o_sd, p.sd.data(), nstreams * sizeof(StreamDesc));
+    for (int i = 0; i < nstreams; ++i) {
+        const StreamHeader& H = p.hdr[i];
+        const StreamDesc& d = p.sd[i];
+        std::memcpy(hs + o_sym + 2 * (size_t)d.cb_off, H.sym.data(), 2 * H.sym.size());
+        std::memcpy(hs + o_len + d.cb_off, H.len.data(), H.len.size());
+        std::memcpy(hs + o_sub + 4 * d.sub_base, H.sub_off.data(), 4 * H.sub_off.size());
+        std::memcpy(hs + o_ch + 8 * d.chunk_base, H.chunk_word_off.data(), 8 * H.chunk_word_off.size());
+        if (H.n_unpred) std::memcpy(hs + o_ul + p.ulist_off[i] * elem, H.unpred.data(), H.unpred.size());
+    }
+    // payload frames straight into the staging buffer
+    struct Job {
+        const uint8_t* src;
+        uint64_t stored, raw;
+        uint8_t* dst;
+    };
+    std::vector<Job> jobs;
+    for (int i = 0; i < nstreams; ++i) {
+        const StreamDir& d = ps.lv[i / 7 + 1].s[i % 7];
+        const uint8_t* src = bytes + d.data_off + d.hdr_stored;
+        uint8_t* dst = hs + o_pl + 4 * p.sd[i].word_base;
+        for (uint32_t L = 0; L < d.layers; ++L) {
+            jobs.push_back({src, d.ls[L], d.lr[L], dst});
+            src += d.ls[L];
+            dst += d.lr[L];
+        }
+        std::memset(dst, 0, 16);  // read-ahead padding of the decoder
+    }
+    ctx->pool->parallel_for(jobs.size(), [&](size_t j) {
+        if (!decode_frame(jobs[j].src, jobs[j].stored, jobs[j].raw, jobs[j].dst)) bad = 3;
+    });
+    if (bad) STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
+    STZ_CUDA(p.stage.ensure(total));
+    STZ_CUDA(cudaMemcpyAsync(p.stage.p, hs, total, cudaMemcpyHostToDevice, ctx->st));
+    uint8_t* ds = p.stage.as<uint8_t>();
+    p.d_sd = (StreamDesc*)(ds + o_sd);
+    p.d_sym = (uint16_t*)(ds + o_sym);
+    p.d_len = ds + o_len;
+    p.d_sub = (uint32_t*)(ds + o_sub);
+    p.d_choff = (uint64_t*)(ds + o_ch);
+    p.d_ulist = ds + o_ul;
+    p.d_payload = (uint32_t*)(ds + o_pl);
+    const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
+    STZ_CUDA(p.coarsest.ensure(n0 * elem));
+    STZ_CUDA(cudaMemcpyAsync(p.coarsest.p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned staging buffer is reused by the next call
+    return STZ_OK;
+}
+
+// Entropy-decode the listed chunks (and scatter their unpredictable values).
+template <typename T>
+stz_status decode_chunks(stz_context* ctx, const Prepared& p, const std::vector<CtaWork>& work,
+                         const std::vector<uint32_t>& ids, const std::vector<UnpredWork>& uwork)
+{
+    const size_t o_w = 0, o_i = align256(work.size() * sizeof(CtaWork));
+    const size_t o_u = align256(o_i + ids.size() * 4), total = align256(o_u + uwork.size() * sizeof(UnpredWork));
+    STZ_CUDA(ctx->h_meta.ensure(total));
+    uint8_t* hm = ctx->h_meta.as<uint8_t>();
+    std::memcpy(hm + o_w, work.data(), work.size() * sizeof(CtaWork));
+    std::memcpy(hm + o_i, ids.data(), ids.size() * 4);
+    if (!uwork.empty()) std::memcpy(hm + o_u, uwork.data(), uwork.size() * sizeof(UnpredWork));
+    STZ_CUDA(ctx->work.ensure(total));
+    STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hm, total, cudaMemcpyHostToDevice, ctx->st));
+    const uint8_t* dw = ctx->work.as<uint8_t>();
+    STZ_CUDA(ctx->codes.ensure(p.total_codes * 2));
+    if (p.total_unpred) STZ_CUDA(ctx->unpred_dense.ensure(p.total_codes * sizeof(T)));
+    if (!work.empty()) {
+        KScope ks(ctx, "k_decode");
+        launch_decode((const CtaWork*)(dw + o_w), (const uint32_t*)(dw + o_i), (int)work.size(), p.d_sd, p.d_sym,
+                      p.d_len, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+    }
+    if (!uwork.empty()) {
+        KScope ks(ctx, "k_unpred_move");
+        launch_unpred_move<T>(false, (const UnpredWork*)(dw + o_u), (int)uwork.size(), p.d_sd,
+                              ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p.d_ulist, ctx->st);
+    }
+    STZ_CUDA(cudaGetLastError());
+    // the pinned work buffer is reused by the next call
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    return STZ_OK;
+}
+
+void add_unpred_work(const Prepared& p, uint32_t s, const uint32_t* chunks, size_t n, std::vector<UnpredWork>& uw)
+{
+    const StreamHeader& H = p.hdr[s];
+    if (!H.n_unpred) return;
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t c = chunks[i];
+        if (H.unpred_count[c]) uw.push_back({s, c, p.ulist_off[s] + p.unpred_prefix[s][c], H.unpred_count[c]});
+    }
+}
+
+QuantParams qparams(const ParsedStream& ps, int k)
+{
+    QuantParams q;
+    q.eb = ps.lv[k].eb;
+    q.recip = 1.0 / q.eb;
+    q.radius = ps.h.radius;
+    return q;
+}
+
+LevelGeom level_geom(const ParsedStream& ps, int k)
+{
+    LevelGeom g;
+    const LevelDir& L = ps.lv[k];
+    g.dx = L.dx, g.dy = L.dy, g.dz = L.dz, g.C = L.C;
+    g.ncx = L.dx / L.C, g.ncy = L.dy / L.C, g.ncz = L.dz / L.C;
+    g.n = (size_t)L.dx * L.dy * L.dz;
+    return g;
+}
+
+// Reconstruct levels 1..kdec; the last one lands in out_dev.
+template <typename T>
+stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& p, int kdec, T* out_dev)
+{
+    const ParsedStream& ps = s->dir;
+    const FileHeader& h = ps.h;
+    const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
+    if (kdec == 0) {
+        STZ_CUDA(cudaMemcpyAsync(out_dev, p.coarsest.p, n0 * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
+        return STZ_OK;
+    }
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    std::vector<UnpredWork> uw;
+    for (int i = 0; i < 7 * kdec; ++i) {
+        const StreamDesc& d = p.sd[i];
+        std::vector<uint32_t> all(d.nchunks);
+        for (uint32_t c = 0; c < d.nchunks; ++c) all[c] = c;
+        add_work(work, ids, (uint32_t)i, all.data(), all.size(), (int)d.C);
+        add_unpred_work(p, (uint32_t)i, all.data(), all.size(), uw);
+    }
+    STZ_TRY(decode_chunks<T>(ctx, p, work, ids, uw));
+    size_t gmax = n0;
+    for (int k = 1; k < kdec; ++k) gmax = std::max(gmax, 8 * (size_t)ps.lv[k].dx * ps.lv[k].dy * ps.lv[k].dz);
+    STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
+    STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
+    const T* coarse = p.coarsest.as<T>();
+    int cur = 0;
+    for (int k = 1; k <= kdec; ++k) {
+        LevelDecodeArgs<T> a;
+        a.coarse = coarse;
+        a.geo = level_geom(ps, k);
+        a.predictor = h.predictor;
+        a.qp = qparams(ps, k);
+        a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
+        a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
+        a.out = k == kdec ? out_dev : ctx->grid[cur].as<T>();
+        {
+            KScope ks(ctx, k == h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
+            launch_level_decode<T>(a, ctx->st);
+        }
+        coarse = a.out;
+        cur = 1 - cur;
+    }
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+template <typename T>
+stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level, T* out_dev)
+{
+    const int K = s->dir.h.K;
+    const int kdec = K - level;
+    if (s->resident && s->resident->kmax >= kdec) return decode_levels<T>(ctx, s, *s->resident, kdec, out_dev);
+    Prepared p;
+    STZ_TRY(prepare(ctx, s, kdec, p));
+    STZ_TRY(decode_levels<T>(ctx, s, p, kdec, out_dev));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));  // p's device buffers are freed on return
+    return STZ_OK;
+}
+
+// Box / slice: base levels in full, low and high levels only on the
+// planner's chunks.
+template <typename T>
+stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[3], const int64_t hi[3], T* out_dev,
+                              size_t odims[3])
+{
+    const ParsedStream& ps = s->dir;
+    const FileHeader& h = ps.h;
+    const int K = h.K;
+    const QueryPlan plan = plan_query(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low, lo, hi);
+    if (odims) {
+        odims[0] = (size_t)(plan.q[0].e - plan.q[0].b + 1);
+        odims[1] = (size_t)(plan.q[1].e - plan.q[1].b + 1);
+        odims[2] = (size_t)(plan.q[2].e - plan.q[2].b + 1);
+    }
+    Prepared local;
+    Prepared* p = s->resident.get();
+    if (!p || p->kmax < K) {
+        STZ_TRY(prepare(ctx, s, K, local));
+        p = &local;
+    }
+    const size_t elem = sizeof(T);
+    // decoded base (the reference decodes the whole base per query, FD5:2645-2648)
+    const LevelGeom low = level_geom(ps, K - 1), high = level_geom(ps, K);
+    const size_t nbase = low.n;
+    if (!p->base_valid) {
+        STZ_CUDA(p->base.ensure(nbase * elem));
+        STZ_TRY(decode_levels<T>(ctx, s, *p, K - 2, p->base.as<T>()));
+        p->base_valid = true;
+    }
+    // entropy-decode the planned chunks of the low and high levels
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    std::vector<UnpredWork> uw;
+    for (const BlockPlan& bp : plan.low) {
+        const uint32_t si = (uint32_t)((K - 2) * 7 + bp.block);
+        std::vector<uint32_t> cs(bp.chunks.begin(), bp.chunks.end());
+        add_work(work, ids, si, cs.data(), cs.size(), low.C);
+        add_unpred_work(*p, si, cs.data(), cs.size(), uw);
+    }
+    for (const BlockPlan& bp : plan.high) {
+        const uint32_t si = (uint32_t)((K - 1) * 7 + bp.block);
+        std::vector<uint32_t> cs(bp.chunks.begin(), bp.chunks.end());
+        add_work(work, ids, si, cs.data(), cs.size(), high.C);
+        add_unpred_work(*p, si, cs.data(), cs.size(), uw);
+    }
+    STZ_TRY(decode_chunks<T>(ctx, *p, work, ids, uw));
+    // mid grid on the reference regions
+    std::vector<RoiBox> boxes;
+    uint64_t total = 0;
+    for (const auto& r : plan.regions) {
+        if (r[0].empty() || r[1].empty() || r[2].empty()) continue;
+        RoiBox b{r[0].b, r[0].e, r[1].b, r[1].e, r[2].b, r[2].e, total};
+        total += (uint64_t)(r[0].e - r[0].b + 1) * (r[1].e - r[1].b + 1) * (r[2].e - r[2].b + 1);
+        boxes.push_back(b);
+    }
+    STZ_CUDA(ctx->mid.ensure(8 * nbase * elem));
+    STZ_CUDA(ctx->boxes.ensure(std::max<size_t>(boxes.size(), 1) * sizeof(RoiBox)));
+    STZ_CUDA(ctx->h_small.ensure(std::max<size_t>(boxes.size(), 1) * sizeof(RoiBox)));
+    if (!boxes.empty()) std::memcpy(ctx->h_small.p, boxes.data(), boxes.size() * sizeof(RoiBox));
+    STZ_CUDA(cudaMemcpyAsync(ctx->boxes.p, ctx->h_small.p, boxes.size() * sizeof(RoiBox), cudaMemcpyHostToDevice, ctx->st));
+    const T* ud = p->total_unpred ? ctx->unpred_dense.as<T>() : nullptr;
+    if (total) {
+        KScope ks(ctx, "k_roi_mid");
+        launch_roi_mid<T>(ctx->boxes.as<RoiBox>(), (int)boxes.size(), total, p->base.as<T>(), low,
+                          qparams(ps, K - 1), h.predictor, ctx->codes.as<uint16_t>() + p->sd[(size_t)(K - 2) * 7].code_off,
+                          ud ? ud + p->sd[(size_t)(K - 2) * 7].code_off : nullptr, ctx->mid.as<T>(), ctx->st);
+    }
+    const RoiBox qb{plan.q[0].b, plan.q[0].e, plan.q[1].b, plan.q[1].e, plan.q[2].b, plan.q[2].e, 0};
+    {
+        KScope ks(ctx, "k_roi_box");
+        launch_roi_box<T>(qb, ctx->mid.as<T>(), high, qparams(ps, K), h.predictor,
+                          ctx->codes.as<uint16_t>() + p->sd[(size_t)(K - 1) * 7].code_off,
+                          ud ? ud + p->sd[(size_t)(K - 1) * 7].code_off : nullptr, out_dev, ctx->st);
+    }
+    STZ_CUDA(cudaGetLastError());
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    return STZ_OK;
+}
+
+size_t dtype_size(int dtype) { return dtype == STZ_F64 ? 8 : 4; }
+
+stz_status enter(stz_context* ctx)
+{
+    if (!ctx) STZ_FAIL(STZ_ERR_ARG, "context is null");
+    g_err.clear();
+    STZ_CUDA(cudaSetDevice(ctx->device));
+    return STZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void stz_default_opts(stz_opts* o)
+{
+    if (!o) return;
+    o->eb = 1e-3;
+    o->eb_mode = STZ_EB_REL;
+    o->bound_mode = STZ_BOUND_POINTWISE;
+    o->mult_base = 0.7;
+    o->mult_low = 2.7;
+    o->mult_high = 8.2;
+    o->radius = 32768;
+    o->chunk_high = 32;
+    o->chunk_low = 16;
+    o->zstd_level = 3;
+    o->predictor = STZ_PRED_DYNAMIC;
+    o->threads = 0;
+}
+
+const char* stz_status_string(stz_status s)
+{
+    switch (s) {
+    case STZ_OK: return "ok";
+    case STZ_ERR_ARG: return "invalid argument";
+    case STZ_ERR_DIMS: return "unsupported dimensions";
+    case STZ_ERR_CUDA: return "CUDA error";
+    case STZ_ERR_NOMEM: return "out of memory";
+    case STZ_ERR_FORMAT: return "invalid stream";
+    case STZ_ERR_ZSTD: return "zstd error";
+    case STZ_ERR_RANGE: return "out of range";
+    case STZ_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+const char* stz_last_error(void) { return g_err.c_str(); }
+
+stz_status stz_context_create(int device, stz_context** out)
+{
+    g_err.clear();
+    if (!out) STZ_FAIL(STZ_ERR_ARG, "out is null");
+    int n = 0;
+    STZ_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) STZ_FAIL(STZ_ERR_ARG, "no such CUDA device");
+    STZ_CUDA(cudaSetDevice(device));
+    auto* c = new (std::nothrow) stz_context();
+    if (!c) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        STZ_FAIL(STZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    c->pool.reset(new ThreadPool(pool_threads(0)));
+    *out = c;
+    return STZ_OK;
+}
+
+void stz_context_destroy(stz_context* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->st);
+    cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+stz_status stz_context_sync(stz_context* ctx)
+{
+    STZ_TRY(enter(ctx));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    return STZ_OK;
+}
+
+stz_status stz_context_stream(stz_context* ctx, void** stream)
+{
+    if (!ctx || !stream) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    *stream = (void*)ctx->st;
+    return STZ_OK;
+}
+
+stz_status stz_profile_enable(stz_context* ctx, int on)
+{
+    STZ_TRY(enter(ctx));
+    ctx->flush_prof();
+    ctx->prof_on = on != 0;
+    return STZ_OK;
+}
+
+stz_status stz_profile_reset(stz_context* ctx)
+{
+    STZ_TRY(enter(ctx));
+    ctx->flush_prof();
+    std::fill(ctx->prof_ms.begin(), ctx->prof_ms.end(), 0.0);
+    std::fill(ctx->prof_launches.begin(), ctx->prof_launches.end(), 0);
+    return STZ_OK;
+}
+
+stz_status stz_profile_count(stz_context* ctx, int* n)
+{
+    STZ_TRY(enter(ctx));
+    if (!n) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    ctx->flush_prof();
+    *n = (int)ctx->prof_names.size();
+    return STZ_OK;
+}
+
+stz_status stz_profile_entry(stz_context* ctx, int i, const char** name, double* total_ms, uint64_t* launches)
+{
+    STZ_TRY(enter(ctx));
+    ctx->flush_prof();
+    if (i < 0 || i >= (int)ctx->prof_names.size()) STZ_FAIL(STZ_ERR_RANGE, "no such profile entry");
+    if (name) *name = ctx->prof_names[i].c_str();
+    if (total_ms) *total_ms = ctx->prof_ms[i];
+    if (launches) *launches = ctx->prof_launches[i];
+    return STZ_OK;
+}
+
+stz_status stz_compress_dev(stz_context* ctx, const void* field, stz_dtype dtype, size_t nx, size_t ny, size_t nz,
+                            const stz_opts* opts, stz_stream** out)
+{
+    STZ_TRY(enter(ctx));
+    if (!field || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (dtype != STZ_F32 && dtype != STZ_F64) STZ_FAIL(STZ_ERR_ARG, "bad dtype");
+    STZ_TRY(check_opts(opts));
+    const std::string dm = validate_dims((long long)nx, (long long)ny, (long long)nz, opts->chunk_high, opts->chunk_low);
+    if (!dm.empty()) STZ_FAIL(STZ_ERR_DIMS, dm);
+    if ((uintptr_t)field % 16) STZ_FAIL(STZ_ERR_ARG, "device field must be 16-byte aligned");
+    if (dtype == STZ_F32)
+        return compress_impl<float>(ctx, (const float*)field, (int)nx, (int)ny, (int)nz, *opts, out);
+    return compress_impl<double>(ctx, (const double*)field, (int)nx, (int)ny, (int)nz, *opts, out);
+}
+
+stz_status stz_compress(stz_context* ctx, const void* field, stz_dtype dtype, size_t nx, size_t ny, size_t nz,
+                        const stz_opts* opts, stz_stream** out)
+{
+    STZ_TRY(enter(ctx));
+    if (!field || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (dtype != STZ_F32 && dtype != STZ_F64) STZ_FAIL(STZ_ERR_ARG, "bad dtype");
+    STZ_TRY(check_opts(opts));
+    const std::string dm = validate_dims((long long)nx, (long long)ny, (long long)nz, opts->chunk_high, opts->chunk_low);
+    if (!dm.empty()) STZ_FAIL(STZ_ERR_DIMS, dm);
+    const size_t bytes = nx * ny * nz * dtype_size(dtype);
+    STZ_CUDA(ctx->field.ensure(bytes));
+    STZ_CUDA(cudaMemcpyAsync(ctx->field.p, field, bytes, cudaMemcpyHostToDevice, ctx->st));
+    return stz_compress_dev(ctx, ctx->field.p, dtype, nx, ny, nz, opts, out);
+}
+
+stz_status stz_decompress_level_dev(stz_context* ctx, const stz_stream* s, int level, void* out, size_t od[3])
+{
+    STZ_TRY(enter(ctx));
+    if (!s || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const FileHeader& h = s->dir.h;
+    if (level < 0 || level > h.K) STZ_FAIL(STZ_ERR_RANGE, "level out of range");
+    if ((uintptr_t)out % 16) STZ_FAIL(STZ_ERR_ARG, "device output must be 16-byte aligned");
+    if (od) od[0] = (size_t)(h.nx >> level), od[1] = (size_t)(h.ny >> level), od[2] = (size_t)(h.nz >> level);
+    if (h.dtype == 1) return decompress_level_dev<double>(ctx, s, level, (double*)out);
+    return decompress_level_dev<float>(ctx, s, level, (float*)out);
+}
+
+stz_status stz_decompress_level(stz_context* ctx, const stz_stream* s, int level, void* out, size_t od[3])
+{
+    STZ_TRY(enter(ctx));
+    if (!s || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const FileHeader& h = s->dir.h;
+    if (level < 0 || level > h.K) STZ_FAIL(STZ_ERR_RANGE, "level out of range");
+    const size_t n = (size_t)(h.nx >> level) * (h.ny >> level) * (h.nz >> level) * h.elem();
+    STZ_CUDA(ctx->out.ensure(n));
+    STZ_TRY(stz_decompress_level_dev(ctx, s, level, ctx->out.p, od));
+    STZ_CUDA(cudaMemcpyAsync(out, ctx->out.p, n, cudaMemcpyDeviceToHost, ctx->st));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    return STZ_OK;
+}
+
+stz_status stz_decompress_full_dev(stz_context* ctx, const stz_stream* s, void* out)
+{
+    return stz_decompress_level_dev(ctx, s, 0, out, nullptr);
+}
+
+stz_status stz_decompress_full(stz_context* ctx, const stz_stream* s, void* out)
+{
+    return stz_decompress_level(ctx, s, 0, out, nullptr);
+}
+
+stz_status stz_decompress_box_dev(stz_context* ctx, const stz_stream* s, const int64_t lo[3], const int64_t hi[3],
+                                  void* out, size_t od[3])
+{
+    STZ_TRY(enter(ctx));
+    if (!s || !lo || !hi || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    stz_stream* ms = const_cast<stz_stream*>(s);  // only the cached decoded base changes
+    if (s->dir.h.dtype == 1) return decompress_box_dev<double>(ctx, ms, lo, hi, (double*)out, od);
+    return decompress_box_dev<float>(ctx, ms, lo, hi, (float*)out, od);
+}
+
+stz_status stz_decompress_box(stz_context* ctx, const stz_stream* s, const int64_t lo[3], const int64_t hi[3],
+                              void* out, size_t od[3])
+{
+    STZ_TRY(enter(ctx));
+    if (!s || !lo || !hi || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const FileHeader& h = s->dir.h;
+    const QueryPlan plan = plan_query(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low, lo, hi);
+    const size_t n = (size_t)(plan.q[0].e - plan.q[0].b + 1) * (plan.q[1].e - plan.q[1].b + 1) *
+                     (plan.q[2].e - plan.q[2].b + 1) * h.elem();
+    STZ_CUDA(ctx->out.ensure(n));
+    STZ_TRY(stz_decompress_box_dev(ctx, s, lo, hi, ctx->out.p, od));
+    STZ_CUDA(cudaMemcpyAsync(out, ctx->out.p, n, cudaMemcpyDeviceToHost, ctx->st));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    return STZ_OK;
+}
+
+stz_status stz_stream_bytes(const stz_stream* s, const void** data, size_t* size)
+{
+    if (!s || !data || !size) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    *data = s->bytes.data();
+    *size = s->bytes.size();
+    return STZ_OK;
+}
+
+stz_status stz_stream_parse(stz_context* ctx, const void* data, size_t size, stz_stream** out)
+{
+    (void)ctx;
+    g_err.clear();
+    if (!data || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    auto* s = new (std::nothrow) stz_stream();
+    if (!s) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
+    s->bytes.assign((const uint8_t*)data, (const uint8_t*)data + size);
+    const std::string e = parse_stream(s->bytes.data(), s->bytes.size(), s->dir);
+    if (!e.empty()) {
+        delete s;
+        STZ_FAIL(STZ_ERR_FORMAT, e);
+    }
+    for (int k = 1; k <= s->dir.h.K; ++k)
+        for (int b = 0; b < 7; ++b)
+            for (uint64_t v : s->dir.lv[k].s[b].lr) s->raw_payload_bytes += v;
+    *out = s;
+    return STZ_OK;
+}
+
+stz_status stz_stream_info(const stz_stream* s, stz_info* info)
+{
+    if (!s || !info) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const FileHeader& h = s->dir.h;
+    info->dtype = h.dtype;
+    info->predictor = h.predictor;
+    info->nx = (size_t)h.nx, info->ny = (size_t)h.ny, info->nz = (size_t)h.nz;
+    info->n_levels = h.K;
+    info->radius = h.radius;
+    info->chunk_high = h.chunk_high, info->chunk_low = h.chunk_low;
+    info->eb = h.eb;
+    info->mult_base = h.mult_base, info->mult_low = h.mult_low, info->mult_high = h.mult_high;
+    info->max_error = h.eb * std::max({h.mult_base, h.mult_low, h.mult_high});
+    info->stream_bytes = s->bytes.size();
+    info->raw_payload_bytes = s->raw_payload_bytes;
+    return STZ_OK;
+}
+
+stz_status stz_stream_upload(stz_context* ctx, stz_stream* s)
+{
+    STZ_TRY(enter(ctx));
+    if (!s) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    std::unique_ptr<Prepared> p(new Prepared());
+    STZ_TRY(prepare(ctx, s, s->dir.h.K, *p));
+    s->resident = std::move(p);
+    return STZ_OK;
+}
+
+void stz_stream_free(stz_stream* s) { delete s; }
+
+// ---- reference function boundary ------------------------------------------------
+stz_status stz_split_dev(stz_context* ctx, stz_dtype dtype, const void* full, size_t nx, size_t ny, size_t nz,
+                         void* subs)
+{
+    STZ_TRY(enter(ctx));
+    if (!full || !subs) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (nx % 2 || ny % 2 || nz % 2 || !nx || !ny || !nz) STZ_FAIL(STZ_ERR_DIMS, "dims must be even and positive");
+    if ((uintptr_t)full % 16) STZ_FAIL(STZ_ERR_ARG, "full must be 16-byte aligned");
+    KScope ks(ctx, "k_split");
+    if (dtype == STZ_F64) launch_split<double>((const double*)full, (int)nx, (int)ny, (int)nz, (double*)subs, ctx->st);
+    else launch_split<float>((const float*)full, (int)nx, (int)ny, (int)nz, (float*)subs, ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+stz_status stz_merge_dev(stz_context* ctx, stz_dtype dtype, const void* subs, size_t hx, size_t hy, size_t hz,
+                         void* full)
+{
+    STZ_TRY(enter(ctx));
+    if (!full || !subs) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (!hx || !hy || !hz) STZ_FAIL(STZ_ERR_DIMS, "dims must be positive");
+    if ((uintptr_t)full % 16) STZ_FAIL(STZ_ERR_ARG, "full must be 16-byte aligned");
+    KScope ks(ctx, "k_merge");
+    if (dtype == STZ_F64) launch_merge<double>((const double*)subs, (int)hx, (int)hy, (int)hz, (double*)full, ctx->st);
+    else launch_merge<float>((const float*)subs, (int)hx, (int)hy, (int)hz, (float*)full, ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+static stz_status block_op(stz_context* ctx, int mode, stz_dtype dtype, int predictor, int block, const void* src,
+                           const void* ref, void* dst, int dx, int dy, int dz, int x0, int x1, int y0, int y1, int z0,
+                           int z1)
+{
+    STZ_TRY(enter(ctx));
+    if (!src || !ref || !dst) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (block < 0 || block > 6) STZ_FAIL(STZ_ERR_RANGE, "block must be in [0, 6]");
+    if (predictor != 0 && predictor != 1) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    if (dx <= 0 || dy <= 0 || dz <= 0) STZ_FAIL(STZ_ERR_DIMS, "dims must be positive");
+    x0 = std::max(0, x0), y0 = std::max(0, y0), z0 = std::max(0, z0);
+    x1 = std::min(dx, x1), y1 = std::min(dy, y1), z1 = std::min(dz, z1);
+    if (x0 >= x1 || y0 >= y1 || z0 >= z1) return STZ_OK;
+    KScope ks(ctx, "k_block_op");
+    if (dtype == STZ_F64)
+        launch_block_op<double>(mode, predictor, block, (const double*)src, (const double*)ref, (double*)dst, dx, dy, dz,
+                                x0, x1, y0, y1, z0, z1, ctx->st);
+    else
+        launch_block_op<float>(mode, predictor, block, (const float*)src, (const float*)ref, (float*)dst, dx, dy, dz, x0,
+                               x1, y0, y1, z0, z1, ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+stz_status stz_preprocess_block_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* sub,
+                                    const void* ref, void* diff, int dx, int dy, int dz, int z0, int z1)
+{
+    return block_op(ctx, 0, dtype, predictor, block, sub, ref, diff, dx, dy, dz, 0, dx, 0, dy, z0, z1);
+}
+
+stz_status stz_depreprocess_block_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* de,
+                                      const void* ref, void* out, int dx, int dy, int dz, int z0, int z1)
+{
+    return block_op(ctx, 1, dtype, predictor, block, de, ref, out, dx, dy, dz, 0, dx, 0, dy, z0, z1);
+}
+
+stz_status stz_depreprocess_block_to_full_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block,
+                                              const void* de, const void* ref, void* full, int dx, int dy, int dz,
+                                              int z0, int z1)
+{
+    return block_op(ctx, 2, dtype, predictor, block, de, ref, full, dx, dy, dz, 0, dx, 0, dy, z0, z1);
+}
+
+stz_status stz_depreprocess_block_roi_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* de,
+                                          const void* ref, void* out, int dx, int dy, int dz, int end_x, int end_y,
+                                          int end_z, int start_x, int start_y, int start_z)
+{
+    // roi end < 0 means "to the end of the axis" (FD5:984-986)
+    if (end_x < 0) end_x = dx;
+    if (end_y < 0) end_y = dy;
+    if (end_z < 0) end_z = dz;
+    return block_op(ctx, 1, dtype, predictor, block, de, ref, out, dx, dy, dz, start_x, end_x, start_y, end_y, start_z,
+                    end_z);
+}
+
+stz_status stz_quantize_dev(stz_context* ctx, stz_dtype dtype, const void* data, size_t n, double eb, int radius,
+                            int32_t* q, void* unpred, size_t* n_unpred)
+{
+    STZ_TRY(enter(ctx));
+    if ((!data || !q || !unpred || !n_unpred) && n) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (!(eb > 0) || radius < 1 || radius > (1 << 30)) STZ_FAIL(STZ_ERR_ARG, "bad eb or radius");
+    if (n_unpred) *n_unpred = 0;
+    if (!n) return STZ_OK;
+    const size_t tiles = (n + 1023) / 1024;
+    STZ_CUDA(ctx->tiles.ensure(align256(tiles * 4) + (tiles + 1) * 8));
+    uint32_t* cnt = ctx->tiles.as<uint32_t>();
+    uint64_t* off = (uint64_t*)(ctx->tiles.as<uint8_t>() + align256(tiles * 4));
+    QuantParams qp{eb, 1.0 / eb, radius};
+    {
+        KScope ks(ctx, "k_quantize", 3);
+        if (dtype == STZ_F64) launch_quantize<double>((const double*)data, n, qp, q, (double*)unpred, cnt, off, ctx->st);
+        else launch_quantize<float>((const float*)data, n, qp, q, (float*)unpred, cnt, off, ctx->st);
+    }
+    STZ_CUDA(cudaGetLastError());
+    uint64_t total = 0;
+    STZ_CUDA(cudaMemcpyAsync(&total, off + tiles, 8, cudaMemcpyDeviceToHost, ctx->st));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    *n_unpred = (size_t)total;
+    return STZ_OK;
+}
+
+stz_status stz_dequantize_dev(stz_context* ctx, stz_dtype dtype, const int32_t* q, size_t n, double eb, int radius,
+                              const void* unpred, void* out)
+{
+    STZ_TRY(enter(ctx));
+    if ((!q || !out) && n) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (!(eb > 0) || radius < 1 || radius > (1 << 30)) STZ_FAIL(STZ_ERR_ARG, "bad eb or radius");
+    if (!n) return STZ_OK;
+    const size_t tiles = (n + 1023) / 1024;
+    STZ_CUDA(ctx->tiles.ensure(align256(tiles * 4) + (tiles + 1) * 8));
+    uint32_t* cnt = ctx->tiles.as<uint32_t>();
+    uint64_t* off = (uint64_t*)(ctx->tiles.as<uint8_t>() + align256(tiles * 4));
+    QuantParams qp{eb, 1.0 / eb, radius};
+    KScope ks(ctx, "k_dequantize", 3);
+    if (dtype == STZ_F64) launch_dequantize<double>(q, n, qp, (const double*)unpred, (double*)out, cnt, off, ctx->st);
+    else launch_dequantize<float>(q, n, qp, (const float*)unpred, (float*)out, cnt, off, ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+stz_status stz_plan_box(size_t nx, size_t ny, size_t nz, int chunk_high, int chunk_low, const int64_t a[3],
+                        const int64_t b[3], int64_t* out, size_t cap, size_t* n_out)
+{
+    g_err.clear();
+    if (!a || !b || !n_out || (!out && cap)) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const std::string dm = validate_dims((long long)nx, (long long)ny, (long long)nz, chunk_high, chunk_low);
+    if (!dm.empty()) STZ_FAIL(STZ_ERR_DIMS, dm);
+    const QueryPlan p = plan_query((int)nx, (int)ny, (int)nz, chunk_high, chunk_low, a, b);
+    std::vector<int64_t> flat;
+    flatten_plan(p, flat);
+    *n_out = flat.size();
+    if (flat.size() > cap) STZ_FAIL(STZ_ERR_RANGE, "output capacity too small");
+    std::memcpy(out, flat.data(), flat.size() * 8);
+    return STZ_OK;
+}
+
+stz_status stz_debug_codebook(const uint32_t* hist, int nbins, uint16_t* sym, uint8_t* len, int* n_used)
+{
+    g_err.clear();
+    if (!hist || !sym || !len || !n_used || nbins <= 0 || nbins > 65536) STZ_FAIL(STZ_ERR_ARG, "bad arguments");
+    std::vector<uint16_t> s;
+    std::vector<uint8_t> l;
+    const int n = build_codebook(hist, nbins, 0, s, l);
+    std::memcpy(sym, s.data(), 2 * (size_t)n);
+    std::memcpy(len, l.data(), (size_t)n);
+    *n_used = n;
+    return STZ_OK;
+}
+
+stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int k, int block, uint16_t* codes, size_t cap,
+                                  size_t* n_out)
+{
+    STZ_TRY(enter(ctx));
+    if (!s || !codes || !n_out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const int K = s->dir.h.K;
+    if (k < 1 || k > K || block < 0 || block > 6) STZ_FAIL(STZ_ERR_RANGE, "level or block out of range");
+    const LevelDir& L = s->dir.lv[k];
+    const size_t n = (size_t)L.dx * L.dy * L.dz;
+    *n_out = n;
+    if (n > cap) STZ_FAIL(STZ_ERR_RANGE, "output capacity too small");
+    Prepared p;
+    STZ_TRY(prepare(ctx, s, k, p));
+    const uint32_t si = (uint32_t)((k - 1) * 7 + block);
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    std::vector<uint32_t> all(p.sd[si].nchunks);
+    for (uint32_t c = 0; c < all.size(); ++c) all[c] = c;
+    add_work(work, ids, si, all.data(), all.size(), (int)p.sd[si].C);
+    std::vector<UnpredWork> none;
+    STZ_TRY(decode_chunks<float>(ctx, p, work, ids, none));
+    STZ_CUDA(cudaMemcpy(codes, ctx->codes.as<uint16_t>() + p.sd[si].code_off, n * 2, cudaMemcpyDeviceToHost));
+    return STZ_OK;
+}
+
+}  // extern "C"

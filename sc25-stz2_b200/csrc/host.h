@@ -1,0 +1,134 @@
+// Host-side pieces of the STZ B200 library: canonical Huffman codebooks, the
+// stream container, the ROI planner and a small thread pool for zstd.
+#pragma once
+#include <array>
+#include <condition_variable>
+#include <cstddef>
+#include <cstdint>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace stz {
+
+// ---- thread pool ----------------------------------------------------------
+class ThreadPool {
+public:
+    explicit ThreadPool(int threads);
+    ~ThreadPool();
+    int size() const { return (int)workers_.size() + 1; }
+    // Runs fn(i) for i in [0, n) on the pool and the calling thread.
+    void parallel_for(size_t n, const std::function<void(size_t)>& fn);
+
+private:
+    void run();
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(size_t)>* job_ = nullptr;
+    size_t n_ = 0, next_ = 0, active_ = 0;
+    bool stop_ = false;
+};
+
+// ---- codebook -------------------------------------------------------------
+// Codebook of the container format for one histogram: symbols with a nonzero
+// count sorted by (count, symbol); minimum-redundancy lengths (in-place
+// algorithm of Moffat & Katajainen); lengths capped at kMaxCodeLen by
+// lengthening the least frequent code below the cap until the Kraft sum fits;
+// output in canonical (length, symbol) order. A lone symbol gets length 0.
+// `base` is added to every histogram index (windowed histograms).
+int build_codebook(const uint32_t* hist, int nbins, int base, std::vector<uint16_t>& sym, std::vector<uint8_t>& len);
+
+// ---- container ------------------------------------------------------------
+struct FileHeader {
+    int dtype = 0, predictor = 0;
+    int nx = 0, ny = 0, nz = 0;
+    int K = 0, radius = 0, chunk_high = 0, chunk_low = 0, zstd_level = 0;
+    double eb = 0, mult_base = 0, mult_low = 0, mult_high = 0;
+    int c0[3] = {0, 0, 0};
+    size_t elem() const { return dtype == 1 ? 8 : 4; }
+};
+
+struct StreamDir {
+    uint32_t layers = 0;
+    uint64_t hdr_stored = 0, hdr_raw = 0;
+    std::vector<uint64_t> ls, lr;  // stored / raw bytes per chunk z-layer
+    size_t data_off = 0;           // byte offset of the header frame
+};
+
+struct LevelDir {
+    int dx = 0, dy = 0, dz = 0, C = 0;
+    double eb = 0;
+    StreamDir s[7];
+};
+
+struct ParsedStream {
+    FileHeader h;
+    size_t coarsest_off = 0;
+    std::vector<LevelDir> lv;  // index 1..K (0 unused)
+};
+
+// Decoded (post-zstd) stream header.
+struct StreamHeader {
+    std::vector<uint16_t> sym;
+    std::vector<uint8_t> len;
+    uint64_t n_unpred = 0;
+    std::vector<uint8_t> unpred;  // n_unpred * elem bytes
+    std::vector<uint32_t> unpred_count;
+    std::vector<uint64_t> chunk_word_off;  // nchunks + 1
+    std::vector<uint32_t> sub_off;         // nchunks * C
+};
+
+// Levels of the hierarchy and chunk edge per level (shared rule with the
+// container reader).
+int num_levels(int nx, int ny, int nz);
+int level_chunk(int nx, int ny, int nz, int K, int k, int chunk_high, int chunk_low);
+
+std::string validate_dims(long long nx, long long ny, long long nz, int chunk_high, int chunk_low);
+
+// Parse the directory; returns "" on success, else an error message.
+std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out);
+bool decode_frame(const uint8_t* src, uint64_t stored, uint64_t raw, uint8_t* dst);
+bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, StreamHeader& out);
+
+// Writer input for one residual stream.
+struct StreamParts {
+    std::vector<uint8_t> hdr;        // raw stream header bytes
+    const uint32_t* words = nullptr; // payload
+    const uint64_t* chunk_word_off = nullptr;
+    int layers = 0, chunks_per_layer = 0;
+};
+
+void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const uint8_t* len, uint32_t n_used,
+                          uint64_t n_unpred, const void* unpred, size_t elem, const uint32_t* unpred_count,
+                          const uint64_t* chunk_word_off, const uint32_t* sub_off, int nchunks, int C);
+
+// Assemble the container: directory, coarsest grid, then every frame
+// (zstd-compressed in parallel on the pool).
+std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
+                                     std::vector<StreamParts>& parts, ThreadPool& pool);
+
+// ---- ROI planner (FD5:1578-1839) -------------------------------------------
+struct AxisRange {
+    int b = 1, e = 0;  // inclusive; empty when b > e
+    bool empty() const { return b > e; }
+};
+struct BlockPlan {
+    int block = 0;
+    AxisRange r[3];
+    std::vector<int64_t> chunks;  // row-major chunk ids, ascending
+};
+struct QueryPlan {
+    AxisRange q[3];
+    bool is_slice = false;
+    std::vector<BlockPlan> high;
+    std::vector<std::array<AxisRange, 3>> regions;  // high reference regions + query sub-block-0 region
+    std::vector<bool> region_slice;
+    std::vector<BlockPlan> low;
+};
+QueryPlan plan_query(int nx, int ny, int nz, int chunk_high, int chunk_low, const int64_t a[3], const int64_t b[3]);
+void flatten_plan(const QueryPlan& p, std::vector<int64_t>& out);
+
+}  // namespace stz

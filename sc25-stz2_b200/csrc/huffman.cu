@@ -1,0 +1,398 @@
+// Chunk-indexed canonical Huffman coding of the quant codes on B200.
+//
+// The reference entropy-codes each residual stream with SZ3-ncp's
+// HuffmanEncoder<int> and a per-chunk "marker" table of bit offsets
+// (encode_marked_fast / decode_marked_transform / decode_marked_chunks_fast,
+// call sites FD5:1264-1306, 1401-1413, 1512-1562, 1870-1875). That library is
+// not available, so the byte format here is this project's own; the roles are
+// the same: a codebook per stream, codes grouped in C^3 marker chunks with a
+// word offset per chunk (the marker table), so any chunk decodes on its own.
+//
+// Parallel decomposition: every z-plane of a chunk (C^2 symbols, a
+// "sub-chunk") is one thread's sequential run; its bit offset inside the chunk
+// is stored, so all planes of all chunks of all streams encode and decode
+// independently. Bits are packed MSB-first into 32-bit words; a chunk starts
+// on a word boundary.
+#include <cuda_runtime.h>
+
+#include "huffman.h"
+
+namespace stz {
+namespace {
+
+// Canonical codes from the (length, symbol)-sorted list: first code of each
+// length by the usual recurrence, then rank within the length.
+__global__ void k_expand_codebook(const StreamDesc* __restrict__ sd, const uint16_t* __restrict__ cb_sym,
+                                  const uint8_t* __restrict__ cb_len, uint32_t* __restrict__ ctab)
+{
+    const StreamDesc s = sd[blockIdx.x];
+    __shared__ uint32_t cnt[kMaxCodeLen + 1];
+    __shared__ uint32_t first_code[kMaxCodeLen + 1];
+    __shared__ uint32_t first_idx[kMaxCodeLen + 1];
+    if (threadIdx.x <= kMaxCodeLen) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) atomicAdd(&cnt[cb_len[s.cb_off + i]], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t code = 0, idx = cnt[0];
+        first_code[0] = 0;
+        first_idx[0] = 0;
+        for (int l = 1; l <= kMaxCodeLen; ++l) {
+            code = (code + (l > 1 ? cnt[l - 1] : 0)) << 1;
+            first_code[l] = code;
+            first_idx[l] = idx;
+            idx += cnt[l];
+        }
+    }
+    __syncthreads();
+    uint32_t* tab = ctab + (size_t)blockIdx.x * 2 * s.radius;
+    for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) {
+        const uint32_t l = cb_len[s.cb_off + i];
+        const uint32_t code = l ? first_code[l] + (i - first_idx[l]) : 0;
+        tab[cb_sym[s.cb_off + i]] = (code << 5) | l;
+    }
+}
+
+// Bits of every sub-chunk.
+__global__ void __launch_bounds__(kCoderThreads) k_sub_bits(const CtaWork* __restrict__ work,
+                                                            const uint32_t* __restrict__ chunk_ids,
+                                                            const StreamDesc* __restrict__ sd,
+                                                            const uint16_t* __restrict__ codes,
+                                                            const uint32_t* __restrict__ ctab,
+                                                            uint32_t* __restrict__ sub_bits)
+{
+    const CtaWork w = work[blockIdx.x];
+    const StreamDesc s = sd[w.stream];
+    const uint32_t C = s.C;
+    const uint32_t t = threadIdx.x;
+    if (t / C >= w.count) return;
+    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
+    const size_t plane = (size_t)C * C;
+    const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+    const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
+    uint32_t bits = 0;
+    for (size_t j = 0; j < plane; ++j) bits += __ldg(tab + __ldg(src + j)) & 31u;
+    sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
+}
+
+// Per stream: plane bit offsets inside each chunk, chunk word offsets (the
+// marker table) and the stream's word count; boundary words of every plane are
+// cleared for the encoder's atomic ORs.
+__global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restrict__ sd,
+                                                      const uint32_t* __restrict__ sub_bits,
+                                                      uint32_t* __restrict__ sub_off,
+                                                      uint64_t* __restrict__ chunk_word_off,
+                                                      uint64_t* __restrict__ stream_words,
+                                                      uint32_t* __restrict__ payload)
+{
+    const StreamDesc s = sd[blockIdx.x];
+    const uint32_t C = s.C;
+    __shared__ uint64_t carry;
+    __shared__ uint64_t wsum[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < s.nchunks; base += blockDim.x) {
+        const uint32_t c = base + threadIdx.x;
+        uint64_t words = 0;
+        if (c < s.nchunks) {
+            uint32_t acc = 0;
+            for (uint32_t lz = 0; lz < C; ++lz) {
+                const size_t k = s.sub_base + (size_t)c * C + lz;
+                sub_off[k] = acc;
+                acc += sub_bits[k];
+            }
+            words = (acc + 31u) / 32u;
+        }
+        uint64_t incl = words;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((threadIdx.x & 31) >= o) incl += v;
+        }
+        if ((threadIdx.x & 31) == 31) wsum[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            uint64_t v = wsum[threadIdx.x];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t u = __shfl_up_sync(0xffffffffu, v, o);
+                if (threadIdx.x >= o) v += u;
+            }
+            wsum[threadIdx.x] = v;
+        }
+        __syncthreads();
+        const uint64_t pre = carry + ((threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0) + incl - words;
+        if (c < s.nchunks) {
+            chunk_word_off[s.chunk_base + c] = pre;
+            uint32_t* w = payload + s.word_base + pre;
+            for (uint32_t lz = 0; lz < C; ++lz) {
+                const size_t k = s.sub_base + (size_t)c * C + lz;
+                const uint32_t b0 = sub_off[k], nb = sub_bits[k];
+                if (nb) {
+                    w[b0 >> 5] = 0;
+                    w[(b0 + nb - 1) >> 5] = 0;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += wsum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        chunk_word_off[s.chunk_base + s.nchunks] = carry;
+        stream_words[blockIdx.x] = carry;
+    }
+}
+
+// Encode: each thread packs one plane MSB-first. Words shared with a
+// neighbouring plane (its first and last) are merged with atomicOr; words in
+// between belong to this plane alone and are stored directly.
+__global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restrict__ work,
+                                                          const uint32_t* __restrict__ chunk_ids,
+                                                          const StreamDesc* __restrict__ sd,
+                                                          const uint16_t* __restrict__ codes,
+                                                          const uint32_t* __restrict__ ctab,
+                                                          const uint32_t* __restrict__ sub_off,
+                                                          const uint32_t* __restrict__ sub_bits,
+                                                          const uint64_t* __restrict__ chunk_word_off,
+                                                          uint32_t* __restrict__ payload)
+{
+    const CtaWork w = work[blockIdx.x];
+    const StreamDesc s = sd[w.stream];
+    const uint32_t C = s.C;
+    const uint32_t t = threadIdx.x;
+    if (t / C >= w.count) return;
+    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
+    const size_t k = s.sub_base + (size_t)c * C + lz;
+    const uint32_t nb = sub_bits[k];
+    if (nb == 0) return;
+    const size_t plane = (size_t)C * C;
+    const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+    const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
+    uint32_t* out = payload + s.word_base + chunk_word_off[s.chunk_base + c];
+    const uint32_t b0 = sub_off[k];
+    const uint32_t first_w = b0 >> 5, last_w = (b0 + nb - 1) >> 5;
+    uint32_t wi = first_w;
+    uint64_t acc = 0;      // pending bits, right-aligned
+    int nacc = b0 & 31;    // leading bits of the first word belong to the previous plane (zeros here)
+    for (size_t j = 0; j < plane; ++j) {
+        const uint32_t e = __ldg(tab + __ldg(src + j));
+        const int l = e & 31;
+        acc = (acc << l) | (e >> 5);
+        nacc += l;
+        if (nacc >= 32) {
+            const uint32_t word = (uint32_t)(acc >> (nacc - 32));
+            nacc -= 32;
+            if (wi == first_w || wi == last_w) atomicOr(out + wi, word);
+            else out[wi] = word;
+            ++wi;
+        }
+    }
+    if (nacc > 0) atomicOr(out + wi, (uint32_t)(acc << (32 - nacc)));
+}
+
+// Decode: each thread decodes one plane with a 2^kLutBits-entry table in
+// shared memory (symbol | length << 16); longer codes fall back to the
+// canonical first-code test per length.
+__global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restrict__ work,
+                                                          const uint32_t* __restrict__ chunk_ids,
+                                                          const StreamDesc* __restrict__ sd,
+                                                          const uint16_t* __restrict__ cb_sym,
+                                                          const uint8_t* __restrict__ cb_len,
+                                                          const uint32_t* __restrict__ sub_off,
+                                                          const uint64_t* __restrict__ chunk_word_off,
+                                                          const uint32_t* __restrict__ payload,
+                                                          uint16_t* __restrict__ codes)
+{
+    __shared__ uint32_t lut[1 << kLutBits];
+    __shared__ uint32_t cnt[kMaxCodeLen + 1];
+    __shared__ uint32_t first_code[kMaxCodeLen + 1];
+    __shared__ uint32_t first_idx[kMaxCodeLen + 1];
+    const CtaWork w = work[blockIdx.x];
+    const StreamDesc s = sd[w.stream];
+    for (int i = threadIdx.x; i < (1 << kLutBits); i += blockDim.x) lut[i] = 0;
+    if (threadIdx.x <= kMaxCodeLen) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) atomicAdd(&cnt[cb_len[s.cb_off + i]], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t code = 0, idx = cnt[0];
+        first_code[0] = 0;
+        first_idx[0] = 0;
+        for (int l = 1; l <= kMaxCodeLen; ++l) {
+            code = (code + (l > 1 ? cnt[l - 1] : 0)) << 1;
+            first_code[l] = code;
+            first_idx[l] = idx;
+            idx += cnt[l];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) {
+        const uint32_t l = cb_len[s.cb_off + i];
+        if (l == 0 || l > (uint32_t)kLutBits) continue;
+        const uint32_t code = first_code[l] + (i - first_idx[l]);
+        const uint32_t e = (uint32_t)cb_sym[s.cb_off + i] | (l << 16);
+        const uint32_t lo = code << (kLutBits - l), hi = (code + 1) << (kLutBits - l);
+        for (uint32_t j = lo; j < hi; ++j) lut[j] = e;
+    }
+    __syncthreads();
+
+    const uint32_t C = s.C;
+    const uint32_t t = threadIdx.x;
+    if (t / C >= w.count) return;
+    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
+    const size_t plane = (size_t)C * C;
+    uint16_t* dst = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+    if (s.n_used == 1) {
+        const uint16_t v = cb_sym[s.cb_off];
+        for (size_t j = 0; j < plane; ++j) dst[j] = v;
+        return;
+    }
+    const uint64_t cw = chunk_word_off[s.chunk_base + c];
+    const uint32_t* in = payload + s.word_base + cw;
+    // words of the stream left from this chunk's start; reads beyond read 0
+    const uint64_t lim = s.word_cap > cw ? s.word_cap - cw : 0;
+    auto rd = [&](uint64_t i) -> uint32_t { return i < lim ? __ldg(in + i) : 0u; };
+    const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
+    uint64_t wi = b0 >> 5;
+    // 64-bit window, MSB = next bit.
+    uint64_t buf = (((uint64_t)rd(wi) << 32) | rd(wi + 1)) << (b0 & 31);
+    int avail = 64 - (int)(b0 & 31);
+    wi += 2;
+    for (size_t j = 0; j < plane; ++j) {
+        if (avail < 32) {
+            buf |= (uint64_t)rd(wi) << (32 - avail);
+            avail += 32;
+            ++wi;
+        }
+        const uint32_t e = lut[buf >> (64 - kLutBits)];
+        uint32_t sym, l = e >> 16;
+        if (l) {
+            sym = e & 0xffffu;
+        } else {
+            // a corrupt stream still yields a symbol of this codebook (never
+            // code 0 unless the stream has unpredictable values)
+            sym = cb_sym[s.cb_off];
+            for (l = kLutBits + 1; l <= (uint32_t)kMaxCodeLen; ++l) {
+                const uint32_t v = (uint32_t)(buf >> (64 - l));
+                if (v - first_code[l] < cnt[l]) {
+                    sym = cb_sym[s.cb_off + first_idx[l] + (v - first_code[l])];
+                    break;
+                }
+            }
+            if (l > (uint32_t)kMaxCodeLen) l = 1;  // corrupt stream: keep going, the result is garbage
+        }
+        buf <<= l;
+        avail -= (int)l;
+        dst[j] = (uint16_t)sym;
+    }
+}
+
+// Unpredictable values: for each listed chunk, walk its codes in order and
+// move the values between the dense per-position buffer and the chunk's slot
+// of the compact list (gather on encode, scatter on decode).
+template <typename T, bool GATHER>
+__global__ void __launch_bounds__(1024) k_unpred_move(const UnpredWork* __restrict__ work,
+                                                      const StreamDesc* __restrict__ sd,
+                                                      const uint16_t* __restrict__ codes, T* __restrict__ dense,
+                                                      T* __restrict__ list)
+{
+    const UnpredWork uw = work[blockIdx.x];
+    const StreamDesc s = sd[uw.stream];
+    const size_t vol = (size_t)s.C * s.C * s.C;
+    const size_t base = s.code_off + (size_t)uw.chunk * vol;
+    __shared__ uint32_t wc[32];
+    __shared__ uint64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (size_t b = 0; b < vol; b += blockDim.x) {
+        const size_t i = b + threadIdx.x;
+        const bool f = i < vol && codes[base + i] == 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) wc[wid] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            if (k < wid) before += wc[k];
+            tot += wc[k];
+        }
+        const uint64_t r = carry + before + __popc(bal & ((1u << lane) - 1u));
+        if (f && r < uw.count) {
+            if (GATHER) list[uw.list_off + r] = dense[base + i];
+            else dense[base + i] = list[uw.list_off + r];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+}
+
+__global__ void k_pack_payload(const uint32_t* __restrict__ src, const uint64_t* __restrict__ src_base,
+                               const uint64_t* __restrict__ dst_base, const uint64_t* __restrict__ count,
+                               uint32_t* __restrict__ dst)
+{
+    const int s = blockIdx.y;
+    const uint64_t n = count[s], a = src_base[s], b = dst_base[s];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[b + i] = src[a + i];
+}
+
+}  // namespace
+
+void launch_pack_payload(const uint32_t* src, const uint64_t* src_base, const uint64_t* dst_base,
+                         const uint64_t* count, int nstreams, uint32_t* dst, cudaStream_t st)
+{
+    if (nstreams) k_pack_payload<<<dim3(64, nstreams), 256, 0, st>>>(src, src_base, dst_base, count, dst);
+}
+
+void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
+                            uint32_t* ctab, cudaStream_t st)
+{
+    if (nstreams) k_expand_codebook<<<nstreams, 256, 0, st>>>(sd, cb_sym, cb_len, ctab);
+}
+
+void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                     const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st)
+{
+    if (nwork) k_sub_bits<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
+}
+
+void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
+                         uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload, cudaStream_t st)
+{
+    if (nstreams)
+        k_scan_stream<<<nstreams, 1024, 0, st>>>(sd, sub_bits, sub_off, chunk_word_off, stream_words, payload);
+}
+
+void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint32_t* sub_bits,
+                   const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st)
+{
+    if (nwork)
+        k_encode<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_off, sub_bits, chunk_word_off,
+                                                  payload);
+}
+
+void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                   const uint16_t* cb_sym, const uint8_t* cb_len, const uint32_t* sub_off,
+                   const uint64_t* chunk_word_off, const uint32_t* payload, uint16_t* codes, cudaStream_t st)
+{
+    if (nwork)
+        k_decode<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, cb_sym, cb_len, sub_off, chunk_word_off, payload,
+                                                  codes);
+}
+
+template <typename T>
+void launch_unpred_move(bool gather, const UnpredWork* work, int nwork, const StreamDesc* sd, const uint16_t* codes,
+                        T* dense, T* list, cudaStream_t st)
+{
+    if (!nwork) return;
+    if (gather) k_unpred_move<T, true><<<nwork, 1024, 0, st>>>(work, sd, codes, dense, list);
+    else k_unpred_move<T, false><<<nwork, 1024, 0, st>>>(work, sd, codes, dense, list);
+}
+
+template void launch_unpred_move<float>(bool, const UnpredWork*, int, const StreamDesc*, const uint16_t*, float*,
+                                        float*, cudaStream_t);
+template void launch_unpred_move<double>(bool, const UnpredWork*, int, const StreamDesc*, const uint16_t*, double*,
+                                         double*, cudaStream_t);
+
+}  // namespace stz

@@ -1,0 +1,40 @@
+// Host-side launchers of the chunked canonical-Huffman kernels (huffman.cu).
+#pragma once
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "stz_internal.h"
+
+namespace stz {
+
+// A chunk holding unpredictable values and where its values sit in the
+// stream's compact list.
+struct UnpredWork {
+    uint32_t stream;
+    uint32_t chunk;
+    uint64_t list_off;
+    uint64_t count;  // values of this chunk in the list
+};
+
+// Dense code table per stream (2*radius entries): code << 5 | length.
+void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
+                            uint32_t* ctab, cudaStream_t st);
+void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                     const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st);
+void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
+                         uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload, cudaStream_t st);
+void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint32_t* sub_bits,
+                   const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st);
+void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                   const uint16_t* cb_sym, const uint8_t* cb_len, const uint32_t* sub_off,
+                   const uint64_t* chunk_word_off, const uint32_t* payload, uint16_t* codes, cudaStream_t st);
+// Copy each stream's used payload words into one contiguous buffer.
+void launch_pack_payload(const uint32_t* src, const uint64_t* src_base, const uint64_t* dst_base,
+                         const uint64_t* count, int nstreams, uint32_t* dst, cudaStream_t st);
+template <typename T>
+void launch_unpred_move(bool gather, const UnpredWork* work, int nwork, const StreamDesc* sd, const uint16_t* codes,
+                        T* dense, T* list, cudaStream_t st);
+
+}  // namespace stz

@@ -1,0 +1,65 @@
+// Host-side launchers of the level kernels (levels.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+
+#include <cuda_runtime.h>
+
+#include "stz_internal.h"
+
+namespace stz {
+
+template <typename T>
+struct LevelEncodeArgs {
+    const T* field;     // input field (device)
+    size_t fsx, fsy;    // field row / plane strides
+    int stride;         // sampling stride of this level's fine grid (1 = finest)
+    const T* coarse;    // decoded coarse grid (geo.dx x dy x dz)
+    LevelGeom geo;
+    int predictor;      // 0 = dynamic lines (FD5), 1 = plain cubic
+    uint16_t* codes;        // 7 x n, chunk-major per stream
+    T* unpred_dense;        // 7 x n, written where the code is 0
+    uint32_t* unpred_cnt;   // 7 x (nchunks + 1)
+    uint32_t* hist_full;    // 7 x 2*radius
+    uint32_t* hist_outside; // 7
+    T* decoded;             // decoded fine grid (2dx x 2dy x 2dz) or null on the finest level
+    QuantParams qp;
+};
+
+template <typename T>
+struct LevelDecodeArgs {
+    const T* coarse;
+    LevelGeom geo;
+    int predictor;
+    QuantParams qp;
+    const uint16_t* codes;
+    const T* unpred_dense;
+    T* out;  // fine grid (2dx x 2dy x 2dz)
+};
+
+template <typename T>
+void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st);
+template <typename T>
+void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st);
+template <typename T>
+void launch_subsample(const T* field, int nx, int ny, int nz, int s, T* out, cudaStream_t st);
+template <typename T>
+void launch_minmax(const T* p, size_t n, double* out2, cudaStream_t st);
+double minmax_key_to_double(unsigned long long k);
+
+template <typename T>
+void launch_split(const T* full, int nx, int ny, int nz, T* subs, cudaStream_t st);
+template <typename T>
+void launch_merge(const T* subs, int hx, int hy, int hz, T* full, cudaStream_t st);
+template <typename T>
+void launch_quantize(const T* d, size_t n, QuantParams qp, int* q, T* unpred, uint32_t* tile_cnt, uint64_t* tile_off,
+                     cudaStream_t st);
+template <typename T>
+void launch_dequantize(const int* q, size_t n, QuantParams qp, const T* unpred, T* out, uint32_t* tile_cnt,
+                       uint64_t* tile_off, cudaStream_t st);
+template <typename T>
+void launch_block_op(int mode, int predictor, int block, const T* src, const T* ref, T* dst, int dx, int dy, int dz,
+                     int x0, int x1, int y0, int y1, int z0, int z1, cudaStream_t st);
+
+}  // namespace stz

@@ -1,0 +1,61 @@
+// Internal shared definitions of the STZ B200 library (host + device).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace stz {
+
+// Longest canonical Huffman code of the container format.
+constexpr int kMaxCodeLen = 24;
+// Fast decode table width (bits) of the GPU decoder.
+constexpr int kLutBits = 12;
+// Histogram window (bins around the radius) kept in shared memory and copied
+// to the host for codebook construction; codes outside it take a slow path.
+constexpr int kHistWindow = 4096;
+// Threads of one entropy-coding CTA; a CTA covers 128 / C chunks of a stream.
+constexpr int kCoderThreads = 128;
+
+// Quantizer constants of one level (FD5:1208-1210): eb, 1/eb computed once on
+// the host (recip = 1.0 / eb), radius.
+struct QuantParams {
+    double eb;
+    double recip;
+    int radius;
+};
+
+// One refinement level: the 7 residual sub-blocks of size (dx,dy,dz) predicted
+// from the decoded coarse grid of the same size.
+struct LevelGeom {
+    int dx, dy, dz;
+    int C;              // marker chunk edge
+    int ncx, ncy, ncz;  // chunks per axis
+    size_t n;           // dx*dy*dz
+    __host__ __device__ int nchunks() const { return ncx * ncy * ncz; }
+};
+
+// One residual stream (level k, block b) as the entropy coder sees it.
+struct StreamDesc {
+    uint64_t code_off;    // element offset of the stream's codes / unpred_dense
+    uint64_t chunk_base;  // offset into per-chunk arrays (unpred counts, word offsets: +stream index)
+    uint64_t sub_base;    // offset into per-sub-chunk arrays (nchunks * C)
+    uint64_t word_base;   // payload word offset of the stream
+    uint64_t word_cap;    // payload words reserved for the stream
+    uint32_t C, ncx, ncy, ncz;
+    uint32_t nchunks;
+    uint32_t cb_off;      // offset of the canonical list (sym/len) in the codebook arrays
+    uint32_t n_used;      // symbols in the codebook
+    uint32_t radius;
+};
+
+// One CTA of the chunk coders: `count` chunks of stream `stream` whose ids are
+// chunk_ids[first .. first + count).
+struct CtaWork {
+    uint32_t stream;
+    uint32_t first;
+    uint32_t count;
+    uint32_t pad;
+};
+
+}  // namespace stz

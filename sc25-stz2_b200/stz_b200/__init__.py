@@ -1,0 +1,403 @@
+"""Python binding of the B200-native STZ library (libstz_b200.so) via ctypes.
+
+The library is the product; this module only marshals arguments. It loads
+the in-tree build (sc25-stz2_b200/lib/libstz_b200.so) and raises if it is
+missing: there is no CPU fallback.
+
+    ctx = Context(0)
+    s = ctx.compress(field, eb=1e-3, eb_mode="rel")        # numpy or torch (CPU/CUDA)
+    full = ctx.decompress(s)                                  # numpy array
+    half = ctx.decompress(s, level=1)
+    box = ctx.decompress_box(s, (0, 0, 0), (63, 63, 63))
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libstz_b200.so")
+
+STZ_F32, STZ_F64 = 0, 1
+_STATUS = {
+    0: "ok", 1: "invalid argument", 2: "unsupported dimensions", 3: "CUDA error", 4: "out of memory",
+    5: "invalid stream", 6: "zstd error", 7: "out of range", 8: "unsupported",
+}
+
+
+class StzError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("eb", C.c_double), ("eb_mode", C.c_int), ("bound_mode", C.c_int),
+        ("mult_base", C.c_double), ("mult_low", C.c_double), ("mult_high", C.c_double),
+        ("radius", C.c_int), ("chunk_high", C.c_int), ("chunk_low", C.c_int),
+        ("zstd_level", C.c_int), ("predictor", C.c_int), ("threads", C.c_int),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("dtype", C.c_int), ("predictor", C.c_int), ("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
+        ("n_levels", C.c_int), ("radius", C.c_int), ("chunk_high", C.c_int), ("chunk_low", C.c_int),
+        ("eb", C.c_double), ("mult_base", C.c_double), ("mult_low", C.c_double), ("mult_high", C.c_double),
+        ("max_error", C.c_double), ("stream_bytes", C.c_size_t), ("raw_payload_bytes", C.c_size_t),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libstz_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libstz_b200.so not built: {path} is missing (run sc25-stz2_b200/build.py)")
+    lib = C.CDLL(path)
+    vp, sz, i64p = C.c_void_p, C.c_size_t, C.POINTER(C.c_int64)
+    lib.stz_last_error.restype = C.c_char_p
+    lib.stz_status_string.restype = C.c_char_p
+    lib.stz_default_opts.argtypes = [C.POINTER(Opts)]
+    lib.stz_context_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.stz_context_destroy.argtypes = [vp]
+    lib.stz_context_sync.argtypes = [vp]
+    for f in (lib.stz_compress, lib.stz_compress_dev):
+        f.argtypes = [vp, vp, C.c_int, sz, sz, sz, C.POINTER(Opts), C.POINTER(vp)]
+    for f in (lib.stz_decompress_full, lib.stz_decompress_full_dev):
+        f.argtypes = [vp, vp, vp]
+    for f in (lib.stz_decompress_level, lib.stz_decompress_level_dev):
+        f.argtypes = [vp, vp, C.c_int, vp, C.POINTER(sz)]
+    for f in (lib.stz_decompress_box, lib.stz_decompress_box_dev):
+        f.argtypes = [vp, vp, i64p, i64p, vp, C.POINTER(sz)]
+    lib.stz_stream_bytes.argtypes = [vp, C.POINTER(vp), C.POINTER(sz)]
+    lib.stz_stream_parse.argtypes = [vp, vp, sz, C.POINTER(vp)]
+    lib.stz_stream_info.argtypes = [vp, C.POINTER(Info)]
+    lib.stz_stream_upload.argtypes = [vp, vp]
+    lib.stz_stream_free.argtypes = [vp]
+    lib.stz_stream_free.restype = None
+    lib.stz_split_dev.argtypes = [vp, C.c_int, vp, sz, sz, sz, vp]
+    lib.stz_merge_dev.argtypes = [vp, C.c_int, vp, sz, sz, sz, vp]
+    for f in (lib.stz_preprocess_block_dev, lib.stz_depreprocess_block_dev, lib.stz_depreprocess_block_to_full_dev):
+        f.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp] + [C.c_int] * 5
+    lib.stz_depreprocess_block_roi_dev.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp] + [C.c_int] * 9
+    lib.stz_quantize_dev.argtypes = [vp, C.c_int, vp, sz, C.c_double, C.c_int, vp, vp, C.POINTER(sz)]
+    lib.stz_dequantize_dev.argtypes = [vp, C.c_int, vp, sz, C.c_double, C.c_int, vp, vp]
+    lib.stz_plan_box.argtypes = [sz, sz, sz, C.c_int, C.c_int, i64p, i64p, i64p, sz, C.POINTER(sz)]
+    lib.stz_debug_stream_codes.argtypes = [vp, vp, C.c_int, C.c_int, vp, sz, C.POINTER(sz)]
+    lib.stz_debug_codebook.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
+    lib.stz_context_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.stz_profile_enable.argtypes = [vp, C.c_int]
+    lib.stz_profile_reset.argtypes = [vp]
+    lib.stz_profile_count.argtypes = [vp, C.POINTER(C.c_int)]
+    lib.stz_profile_entry.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_uint64)]
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise StzError(status, _lib.stz_last_error().decode(errors="replace"))
+
+
+def default_opts(**kw) -> Opts:
+    lib = load_library()
+    o = Opts()
+    lib.stz_default_opts(C.byref(o))
+    modes = {"abs": 0, "rel": 1}
+    bounds = {"pointwise": 0, "reference": 1}
+    preds = {"dynamic": 0, "cubic": 1}
+    for k, v in kw.items():
+        if k == "eb_mode" and isinstance(v, str):
+            v = modes[v]
+        elif k == "bound_mode" and isinstance(v, str):
+            v = bounds[v]
+        elif k == "predictor" and isinstance(v, str):
+            v = preds[v]
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+def _dtype_code(dt) -> int:
+    dt = np.dtype(dt)
+    if dt == np.float32:
+        return STZ_F32
+    if dt == np.float64:
+        return STZ_F64
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _np_dtype(code: int):
+    return np.float64 if code == STZ_F64 else np.float32
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+@dataclass
+class StreamInfo:
+    dtype: type
+    predictor: int
+    shape: tuple  # (nz, ny, nx)
+    n_levels: int
+    radius: int
+    chunk_high: int
+    chunk_low: int
+    eb: float
+    mults: tuple
+    max_error: float
+    stream_bytes: int
+    raw_payload_bytes: int
+
+
+class Stream:
+    """A compressed field (library-owned)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.stz_stream_free(self._h)
+            self._h = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def to_bytes(self) -> bytes:
+        p, n = C.c_void_p(), C.c_size_t()
+        _check(_lib.stz_stream_bytes(self._h, C.byref(p), C.byref(n)))
+        return C.string_at(p, n.value)
+
+    def __len__(self) -> int:
+        p, n = C.c_void_p(), C.c_size_t()
+        _check(_lib.stz_stream_bytes(self._h, C.byref(p), C.byref(n)))
+        return n.value
+
+    def info(self) -> StreamInfo:
+        i = Info()
+        _check(_lib.stz_stream_info(self._h, C.byref(i)))
+        return StreamInfo(_np_dtype(i.dtype), i.predictor, (i.nz, i.ny, i.nx), i.n_levels, i.radius, i.chunk_high,
+                          i.chunk_low, i.eb, (i.mult_base, i.mult_low, i.mult_high), i.max_error, i.stream_bytes,
+                          i.raw_payload_bytes)
+
+
+class Context:
+    """One CUDA device + stream of the library."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self._c = C.c_void_p()
+        _check(self.lib.stz_context_create(int(device), C.byref(self._c)))
+        self.device = device
+
+    def close(self):
+        if self._c.value:
+            self.lib.stz_context_destroy(self._c)
+            self._c = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def sync(self):
+        _check(self.lib.stz_context_sync(self._c))
+
+    def cuda_stream(self) -> int:
+        """cudaStream_t of the context (as an integer handle)."""
+        p = C.c_void_p()
+        _check(self.lib.stz_context_stream(self._c, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, on: bool = True) -> None:
+        _check(self.lib.stz_profile_enable(self._c, 1 if on else 0))
+
+    def profile_reset(self) -> None:
+        _check(self.lib.stz_profile_reset(self._c))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (total ms, launches)} since the last reset."""
+        n = C.c_int()
+        _check(self.lib.stz_profile_count(self._c, C.byref(n)))
+        out = {}
+        for i in range(n.value):
+            name, ms, k = C.c_char_p(), C.c_double(), C.c_uint64()
+            _check(self.lib.stz_profile_entry(self._c, i, C.byref(name), C.byref(ms), C.byref(k)))
+            out[name.value.decode()] = (ms.value, k.value)
+        return out
+
+    # ---- codec -------------------------------------------------------------
+    def compress(self, field, opts: Opts | None = None, **kw) -> Stream:
+        """Compress a 3-D array (z, y, x) — numpy, or torch on CPU or CUDA."""
+        o = opts if opts is not None else default_opts(**kw)
+        h = C.c_void_p()
+        if _is_torch(field):
+            import torch
+
+            if field.dim() != 3 or not field.is_contiguous():
+                raise ValueError("field must be a contiguous 3-D tensor (z, y, x)")
+            code = {torch.float32: STZ_F32, torch.float64: STZ_F64}[field.dtype]
+            nz, ny, nx = field.shape
+            fn = self.lib.stz_compress_dev if field.is_cuda else self.lib.stz_compress
+            _check(fn(self._c, C.c_void_p(field.data_ptr()), code, nx, ny, nz, C.byref(o), C.byref(h)))
+        else:
+            a = np.ascontiguousarray(field)
+            if a.ndim != 3:
+                raise ValueError("field must be 3-D (z, y, x)")
+            nz, ny, nx = a.shape
+            _check(self.lib.stz_compress(self._c, a.ctypes.data_as(C.c_void_p), _dtype_code(a.dtype), nx, ny, nz,
+                                         C.byref(o), C.byref(h)))
+        return Stream(h.value)
+
+    def parse(self, data: bytes) -> Stream:
+        h = C.c_void_p()
+        buf = C.create_string_buffer(data, len(data))
+        _check(self.lib.stz_stream_parse(self._c, buf, len(data), C.byref(h)))
+        return Stream(h.value)
+
+    def upload(self, s: Stream) -> None:
+        _check(self.lib.stz_stream_upload(self._c, s.handle))
+
+    def decompress(self, s: Stream, level: int = 0, out=None):
+        """Full (level 0) or progressive decode. out: torch CUDA tensor for the
+        device path, else a numpy array is returned."""
+        inf = s.info()
+        nz, ny, nx = inf.shape
+        shape = (nz >> level, ny >> level, nx >> level)
+        dims = (C.c_size_t * 3)()
+        if out is not None and _is_torch(out) and out.is_cuda:
+            if tuple(out.shape) != shape:
+                raise ValueError(f"out must have shape {shape}")
+            _check(self.lib.stz_decompress_level_dev(self._c, s.handle, level, C.c_void_p(out.data_ptr()), dims))
+            return out
+        res = np.empty(shape, dtype=inf.dtype) if out is None else out
+        _check(self.lib.stz_decompress_level(self._c, s.handle, level, res.ctypes.data_as(C.c_void_p), dims))
+        return res
+
+    def decompress_box(self, s: Stream, lo, hi, out=None):
+        """Box / slice decode; lo, hi are inclusive (x, y, z) corners."""
+        inf = s.info()
+        a = (C.c_int64 * 3)(*[int(v) for v in lo])
+        b = (C.c_int64 * 3)(*[int(v) for v in hi])
+        nz, ny, nx = inf.shape
+        dims = [nx, ny, nz]
+        ext = []
+        for ax in range(3):
+            if a[ax] == b[ax]:
+                ext.append(1)
+            else:
+                lo_ = max(0, min(a[ax], b[ax]))
+                hi_ = min(dims[ax] - 1, max(a[ax], b[ax]))
+                ext.append(max(hi_, lo_) - lo_ + 1)
+        shape = (ext[2], ext[1], ext[0])
+        od = (C.c_size_t * 3)()
+        if out is not None and _is_torch(out) and out.is_cuda:
+            _check(self.lib.stz_decompress_box_dev(self._c, s.handle, a, b, C.c_void_p(out.data_ptr()), od))
+            return out
+        res = np.empty(shape, dtype=inf.dtype)
+        _check(self.lib.stz_decompress_box(self._c, s.handle, a, b, res.ctypes.data_as(C.c_void_p), od))
+        return res
+
+    def stream_codes(self, s: Stream, level_from_coarse: int, block: int) -> np.ndarray:
+        inf = s.info()
+        n = C.c_size_t()
+        cap = int(np.prod(inf.shape))
+        buf = np.empty(cap, dtype=np.uint16)
+        _check(self.lib.stz_debug_stream_codes(self._c, s.handle, level_from_coarse, block,
+                                               buf.ctypes.data_as(C.c_void_p), cap, C.byref(n)))
+        return buf[: n.value].copy()
+
+    # ---- reference function boundary (torch CUDA tensors) ------------------
+    def _p(self, t):
+        return C.c_void_p(t.data_ptr())
+
+    def split(self, full, subs):
+        nz, ny, nx = full.shape
+        _check(self.lib.stz_split_dev(self._c, _tcode(full), self._p(full), nx, ny, nz, self._p(subs)))
+
+    def merge(self, subs, full):
+        _, hz, hy, hx = subs.shape
+        _check(self.lib.stz_merge_dev(self._c, _tcode(full), self._p(subs), hx, hy, hz, self._p(full)))
+
+    def preprocess_block(self, block, sub, ref, diff, z0=0, z1=None, predictor=0):
+        dz, dy, dx = ref.shape
+        _check(self.lib.stz_preprocess_block_dev(self._c, _tcode(ref), predictor, block, self._p(sub), self._p(ref),
+                                                 self._p(diff), dx, dy, dz, z0, dz if z1 is None else z1))
+
+    def depreprocess_block(self, block, de, ref, out, z0=0, z1=None, predictor=0):
+        dz, dy, dx = ref.shape
+        _check(self.lib.stz_depreprocess_block_dev(self._c, _tcode(ref), predictor, block, self._p(de), self._p(ref),
+                                                   self._p(out), dx, dy, dz, z0, dz if z1 is None else z1))
+
+    def depreprocess_block_to_full(self, block, de, ref, full, z0=0, z1=None, predictor=0):
+        dz, dy, dx = ref.shape
+        _check(self.lib.stz_depreprocess_block_to_full_dev(self._c, _tcode(ref), predictor, block, self._p(de),
+                                                           self._p(ref), self._p(full), dx, dy, dz, z0,
+                                                           dz if z1 is None else z1))
+
+    def depreprocess_block_roi(self, block, de, ref, out, end, start, predictor=0):
+        dz, dy, dx = ref.shape
+        _check(self.lib.stz_depreprocess_block_roi_dev(self._c, _tcode(ref), predictor, block, self._p(de),
+                                                       self._p(ref), self._p(out), dx, dy, dz, *end, *start))
+
+    def quantize(self, data, eb, radius, q, unpred) -> int:
+        n = C.c_size_t()
+        _check(self.lib.stz_quantize_dev(self._c, _tcode(data), self._p(data), data.numel(), eb, radius, self._p(q),
+                                         self._p(unpred), C.byref(n)))
+        return n.value
+
+    def dequantize(self, q, eb, radius, unpred, out):
+        _check(self.lib.stz_dequantize_dev(self._c, _tcode(out), self._p(q), q.numel(), eb, radius, self._p(unpred),
+                                           self._p(out)))
+
+
+def _tcode(t) -> int:
+    import torch
+
+    return {torch.float32: STZ_F32, torch.float64: STZ_F64}[t.dtype]
+
+
+def plan_box(dims_xyz, chunk_high, chunk_low, a, b) -> np.ndarray:
+    """ROI planner record (host-only, no GPU needed)."""
+    lib = load_library()
+    cap = 1 << 20
+    out = np.zeros(cap, dtype=np.int64)
+    n = C.c_size_t()
+    aa = (C.c_int64 * 3)(*[int(v) for v in a])
+    bb = (C.c_int64 * 3)(*[int(v) for v in b])
+    _check(lib.stz_plan_box(*[int(d) for d in dims_xyz], chunk_high, chunk_low, aa, bb,
+                            out.ctypes.data_as(C.POINTER(C.c_int64)), cap, C.byref(n)))
+    return out[: n.value].copy()
+
+
+def codebook(hist: np.ndarray):
+    """Canonical codebook of the container format (host-only)."""
+    lib = load_library()
+    h = np.ascontiguousarray(hist, dtype=np.uint32)
+    sym = np.zeros(len(h), dtype=np.uint16)
+    ln = np.zeros(len(h), dtype=np.uint8)
+    n = C.c_int()
+    _check(lib.stz_debug_codebook(h.ctypes.data_as(C.c_void_p), len(h), sym.ctypes.data_as(C.c_void_p),
+                                  ln.ctypes.data_as(C.c_void_p), C.byref(n)))
+    return sym[: n.value].copy(), ln[: n.value].copy()

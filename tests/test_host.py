@@ -1,0 +1,123 @@
+"""CPU checks of the product library's host side: it loads, exports every
+declared entry point, and its host logic (codebook, planner) agrees with the
+oracle's independent implementation. No GPU calls."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+import stz_b200
+from conftest import ROOT
+
+
+def test_library_exports_every_declared_symbol():
+    lib = stz_b200.load_library()
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for dirpath, _, files in os.walk(inc):
+        for fn in files:
+            if fn.endswith(".h"):
+                names |= set(re.findall(r"\b(stz_[a-z0-9_]+)\s*\(", open(os.path.join(dirpath, fn)).read()))
+    assert names, "no declarations found"
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_has_no_oracle_dependency():
+    with open(stz_b200.LIB_PATH, "rb") as f:
+        blob = f.read()
+    assert b"stzo_" not in blob and b"fd5ref_" not in blob
+
+
+def test_default_opts_are_reference_defaults():
+    o = stz_b200.default_opts()
+    assert (o.mult_base, o.mult_low, o.mult_high) == (0.7, 2.7, 8.2)
+    assert (o.radius, o.chunk_high, o.chunk_low, o.zstd_level) == (32768, 32, 16, 3)
+
+
+def _hists():
+    rng = np.random.default_rng(1)
+    yield np.bincount(rng.geometric(0.3, 5000), minlength=64).astype(np.uint32)
+    h = np.zeros(4096, np.uint32)
+    h[2048] = 10**7
+    h[2047] = h[2049] = 1000
+    h[100] = 1
+    yield h
+    fib = [1, 1]
+    while len(fib) < 40:
+        fib.append(fib[-1] + fib[-2])
+    yield np.array(fib, dtype=np.uint32)  # forces the length limit
+    h = np.zeros(65536, np.uint32)
+    h[32768] = 5
+    yield h  # single symbol
+    yield rng.integers(0, 3, 65536).astype(np.uint32)
+    yield np.ones(3000, np.uint32)
+
+
+def test_codebook_matches_oracle():
+    for h in _hists():
+        s1, l1 = stz_b200.codebook(h)
+        s2, l2 = po.codebook(h)
+        assert np.array_equal(s1, s2) and np.array_equal(l1, l2)
+        assert l1.max() <= 24
+        if len(l1) > 1:
+            assert (2.0 ** -l1.astype(np.float64)).sum() <= 1.0  # Kraft
+
+
+def test_codebook_is_optimal_without_length_limit():
+    rng = np.random.default_rng(4)
+    h = rng.integers(1, 1000, 300).astype(np.uint32)
+    s, l = stz_b200.codebook(h)
+    # Huffman cost equals the sum of merged weights
+    import heapq
+
+    heap = list(h.astype(np.int64))
+    heapq.heapify(heap)
+    cost = 0
+    while len(heap) > 1:
+        a, b = heapq.heappop(heap), heapq.heappop(heap)
+        cost += a + b
+        heapq.heappush(heap, a + b)
+    assert int((h[s].astype(np.int64) * l).sum()) == cost
+
+
+def test_planner_matches_oracle():
+    rng = np.random.default_rng(2)
+    for dims, ch, cl in [((256, 256, 256), 32, 16), ((384, 384, 256), 32, 16), ((64, 32, 128), 8, 4)]:
+        for _ in range(200):
+            a = rng.integers(-9, np.array(dims) + 9)
+            b = rng.integers(-9, np.array(dims) + 9)
+            if rng.random() < 0.25:
+                ax = rng.integers(0, 3)
+                b[ax] = a[ax]
+            assert np.array_equal(stz_b200.plan_box(dims, ch, cl, a, b), po.plan(dims, ch, cl, a, b))
+
+
+def test_planner_rejects_bad_dims():
+    with pytest.raises(stz_b200.StzError) as e:
+        stz_b200.plan_box((30, 32, 32), 8, 4, (0, 0, 0), (1, 1, 1))
+    assert e.value.status == 2
+
+
+def test_fields_generators():
+    from stz_b200 import fields
+
+    g = fields.grf((32, 32, 32), 3.0, 1)
+    assert g.dtype == np.float32 and abs(float(g.mean())) < 1e-5 and abs(float(g.std()) - 1) < 1e-4
+    ln = fields.lognormal((16, 16, 16), 1)
+    assert (ln > 0).all()
+    fr = fields.fronts((8, 8, 16), 1)
+    assert fr.dtype == np.float64 and fr.shape == (8, 8, 16)
+
+
+def test_ctypes_structs_match_header():
+    """Opts/Info layouts agree with include/stz/stz.h (field order and types)."""
+    hdr = open(os.path.join(ROOT, "include", "stz", "stz.h")).read()
+    for struct, cls in (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info)):
+        body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (struct, struct), hdr, re.S).group(1)
+        fields = re.findall(r"^\s*(?:int|double|size_t)\s+([a-z0-9_, ]+);", body, re.M)
+        names = [n.strip() for f in fields for n in f.split(",")]
+        assert names == [f[0] for f in cls._fields_], struct

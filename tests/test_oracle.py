@@ -1,0 +1,113 @@
+"""CPU checks of the oracle against the reference: golden vectors produced by
+the reference's own compiled functions (tests/golden/make_golden.py), and,
+where the reference build is present, live comparisons with it."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import GOLDEN_CASES
+
+
+def _levels(golden, name):
+    return int(golden[f"{name}_K"])
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_CASES))
+def test_level_encode_matches_reference_golden(golden, name):
+    """Predictor + quantizer + closed loop of every level, bit for bit."""
+    f = golden[f"{name}_field"]
+    K = _levels(golden, name)
+    coarse = golden[f"{name}_coarsest"]
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = np.ascontiguousarray(f[::s, ::s, ::s])
+        q, u, c, dec = po.level_encode(fine, coarse, float(golden[f"{name}_L{k}_eb"]))
+        assert np.array_equal(q.astype(np.uint16), golden[f"{name}_L{k}_codes"]), (name, k)
+        assert np.array_equal(c, golden[f"{name}_L{k}_counts"])
+        assert np.array_equal(u.view(np.uint8), golden[f"{name}_L{k}_unpred"].view(np.uint8))
+        if k < K:
+            # compressor-side grid equals the reference decoder's grid bit for bit
+            assert np.array_equal(dec.view(np.uint8), golden[f"{name}_L{k}_decoded"].view(np.uint8))
+        coarse = golden[f"{name}_L{k}_decoded"]
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_CASES))
+def test_codec_matches_reference_golden(golden, name):
+    """Whole container round trip: codes per stream and the decoded field equal
+    the reference decoder's output on the same quant codes."""
+    f = golden[f"{name}_field"]
+    K = _levels(golden, name)
+    ch, cl = GOLDEN_CASES[name]
+    eb = float(golden[f"{name}_eb"])
+    stream = po.compress(f, eb, chunk_high=ch, chunk_low=cl)
+    for k in range(1, K + 1):
+        dz, dy, dx = (np.array(f.shape) >> (K - k + 1))
+        C = po.oracle().stzo_level_chunk(f.shape[2], f.shape[1], f.shape[0], k, ch, cl)
+        for b in range(7):
+            want = po.chunk_major(golden[f"{name}_L{k}_codes"][b], (dz, dy, dx), C)
+            assert np.array_equal(po.stream_codes(stream, k, b), want), (name, k, b)
+    out = po.decompress(stream)
+    assert np.array_equal(out.view(np.uint8), golden[f"{name}_L{K}_decoded"].view(np.uint8))
+    for lvl in range(1, K + 1):
+        part = po.decompress(stream, lvl)
+        want = golden[f"{name}_L{K - lvl}_decoded"] if lvl < K else golden[f"{name}_coarsest"]
+        assert np.array_equal(part.view(np.uint8), want.view(np.uint8)), (name, lvl)
+
+
+def test_planner_matches_reference_golden(golden):
+    q, offs, rec = golden["plan_queries"], golden["plan_offsets"], golden["plan_records"]
+    for i, row in enumerate(q):
+        dims, ch, cl, a, b = row[:3], row[3], row[4], row[5:8], row[8:11]
+        got = po.plan(dims, ch, cl, a, b)
+        assert np.array_equal(got, rec[offs[i]:offs[i + 1]]), i
+
+
+def test_error_bound_and_progressive_levels():
+    from stz_b200 import fields
+
+    f = fields.grf((64, 64, 64), 11.0 / 3.0, 3, np.float32)
+    E = 1e-3 * (float(f.max()) - float(f.min()))
+    eb = E / 8.2 * (1 - 1e-6)
+    s = po.compress(f, eb)
+    out = po.decompress(s)
+    assert np.abs(out.astype(np.float64) - f).max() <= 8.2 * eb * (1 + 1e-6)
+    half = po.decompress(s, 1)
+    assert np.abs(half.astype(np.float64) - f[::2, ::2, ::2]).max() <= 2.7 * eb * (1 + 1e-5)
+
+
+def test_box_equals_full_crop():
+    from stz_b200 import fields
+
+    f = fields.fronts((32, 32, 64), 4, np.float64)
+    s = po.compress(f, 1e-4, chunk_high=8, chunk_low=4)
+    full = po.decompress(s)
+    for lo, hi in [((0, 0, 0), (63, 31, 31)), ((5, 7, 3), (40, 20, 30)), ((10, 0, 0), (10, 31, 31))]:
+        box = po.decompress_box(s, lo, hi)
+        sl = tuple(slice(min(a, b), max(a, b) + 1) for a, b in zip(lo[::-1], hi[::-1]))
+        assert np.array_equal(box, full[sl])
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_oracle_matches_reference_live(dtype):
+    rng = np.random.default_rng(9)
+    for dims in [(7, 5, 3), (12, 8, 20), (2, 2, 2), (33, 17, 9)]:
+        dz, dy, dx = dims
+        fine = (rng.standard_normal((2 * dz, 2 * dy, 2 * dx)) * 10).astype(dtype)
+        coarse = rng.standard_normal(dims).astype(dtype)
+        for eb in (1e-1, 1e-5):
+            a = po.level_encode(fine, coarse, eb)
+            b = po.level_encode(fine, coarse, eb, use_ref=True)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+            assert np.array_equal(a[1].view(np.uint8), b[1].view(np.uint8))
+            assert np.array_equal(a[3].view(np.uint8), b[3].view(np.uint8))
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_planner_matches_reference_live():
+    rng = np.random.default_rng(17)
+    for dims, ch, cl in [((128, 64, 64), 16, 8), ((64, 64, 64), 32, 16)]:
+        for _ in range(300):
+            a = rng.integers(-5, np.array(dims) + 5)
+            b = rng.integers(-5, np.array(dims) + 5)
+            assert np.array_equal(po.plan(dims, ch, cl, a, b), po.plan(dims, ch, cl, a, b, use_ref=True))
