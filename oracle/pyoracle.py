@@ -75,8 +75,28 @@ def oracle() -> C.CDLL:
     return _orc
 
 
+RD_SO = os.path.join(HERE, "_ref", "libstzrd_ref.so")
+_rd = None
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def rd_available() -> bool:
+    return os.path.exists(RD_SO)
+
+
+def rd() -> C.CDLL:
+    """The reference's plain tricubic variant (src/stz-rd.cpp) compiled from source."""
+    global _rd
+    if _rd is None:
+        L = C.CDLL(RD_SO)
+        for suf in ("f32", "f64"):
+            getattr(L, "rdref_preprocess_block_" + suf).argtypes = [ci, vp, vp, vp, ci, ci, ci]
+            getattr(L, "rdref_depreprocess_block_" + suf).argtypes = [ci, vp, vp, vp] + [ci] * 9
+        _rd = L
+    return _rd
 
 
 def ref() -> C.CDLL:

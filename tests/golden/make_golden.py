@@ -75,6 +75,24 @@ def main():
         arrays[f"{name}_rel"] = np.float64(rel)
         for k, v in hierarchy(f, rel).items():
             arrays[f"{name}_{k}"] = v
+    # plain tricubic predictor of src/stz-rd.cpp (= src/float.cpp / double.cpp):
+    # diff = sub - P for every block on a random reference grid with a flat half
+    R = po.rd()
+    rng = np.random.default_rng(8)
+    for dt, suf in ((np.float32, "f32"), (np.float64, "f64")):
+        dims = (9, 10, 12)
+        ref = rng.standard_normal(dims).astype(dt)
+        ref[:4] = 0.001
+        sub = rng.standard_normal(dims).astype(dt)
+        arrays[f"plain_{suf}_ref"] = ref
+        arrays[f"plain_{suf}_sub"] = sub
+        diffs = []
+        for b in range(7):
+            d = np.zeros(dims, dt)
+            getattr(R, "rdref_preprocess_block_" + suf)(b, po._p(sub), po._p(ref), po._p(d), dims[2], dims[1], dims[0])
+            diffs.append(d)
+        arrays[f"plain_{suf}_diff"] = np.stack(diffs)
+
     rng = np.random.default_rng(5)
     plans, offs, queries = [], [0], []
     for dims, ch, cl in [((256, 256, 256), 32, 16), ((384, 384, 256), 32, 16)]:

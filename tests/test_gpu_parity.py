@@ -285,3 +285,13 @@ def test_errors(ctx):
     except stz_b200.StzError:
         pass
     ctx.sync()
+
+
+@pytest.mark.parametrize("suf", ["f32", "f64"])
+def test_plain_cubic_kernel_matches_reference_golden(ctx, golden, suf):
+    ref, sub, diff = golden[f"plain_{suf}_ref"], golden[f"plain_{suf}_sub"], golden[f"plain_{suf}_diff"]
+    tr, ts = torch.from_numpy(ref).cuda(), torch.from_numpy(sub).cuda()
+    for b in range(7):
+        out = torch.zeros_like(tr)
+        ctx.preprocess_block(b, ts, tr, out, predictor=1)
+        assert np.array_equal(bits(out), bits(diff[b])), b

@@ -111,3 +111,15 @@ def test_planner_matches_reference_live():
             a = rng.integers(-5, np.array(dims) + 5)
             b = rng.integers(-5, np.array(dims) + 5)
             assert np.array_equal(po.plan(dims, ch, cl, a, b), po.plan(dims, ch, cl, a, b, use_ref=True))
+
+
+@pytest.mark.parametrize("suf", ["f32", "f64"])
+def test_plain_cubic_predictor_matches_reference_golden(golden, suf):
+    """Plain tricubic stencils of src/stz-rd.cpp (= src/float.cpp/double.cpp)."""
+    ref, sub, diff = golden[f"plain_{suf}_ref"], golden[f"plain_{suf}_sub"], golden[f"plain_{suf}_diff"]
+    dz, dy, dx = ref.shape
+    fn = getattr(po.oracle(), "stzo_predict_plain_" + suf)
+    for b in range(7):
+        P = np.array([[[fn(b, po._p(ref), x, y, z, dx, dy, dz) for x in range(dx)] for y in range(dy)]
+                      for z in range(dz)], dtype=ref.dtype)
+        assert np.array_equal((sub - P).view(np.uint8), diff[b].view(np.uint8)), b
