@@ -17,7 +17,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -32,7 +35,43 @@
 
 namespace {
 thread_local std::string g_err;
-}
+
+// Host phase timer, printed to stderr when STZ_TRACE is set.
+struct Trace {
+    const char* name;
+    std::chrono::steady_clock::time_point t0;
+    bool on;
+    explicit Trace(const char* n) : name(n), on(std::getenv("STZ_TRACE") != nullptr)
+    {
+        if (on) t0 = std::chrono::steady_clock::now();
+    }
+    ~Trace()
+    {
+        if (on)
+            std::fprintf(stderr, "[stz] %-28s %8.3f ms\n", name,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
+// Lap timer: mark(name) prints the time since the previous mark (STZ_TRACE).
+struct Lap {
+    const char* scope;
+    std::chrono::steady_clock::time_point t;
+    bool on;
+    explicit Lap(const char* s) : scope(s), on(std::getenv("STZ_TRACE") != nullptr)
+    {
+        if (on) t = std::chrono::steady_clock::now();
+    }
+    void mark(const char* what)
+    {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[stz] %s: %-24s %8.3f ms\n", scope, what,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+}  // namespace
 
 #define STZ_FAIL(code, msg)    \
     do {                       \
@@ -195,7 +234,12 @@ struct Prepared {
     std::vector<std::vector<uint64_t>> unpred_prefix;  // per stream, per chunk: list offset
     std::vector<uint64_t> ulist_off;                   // per stream: element offset in the unpred list
     uint64_t total_codes = 0, total_unpred = 0;
-    DevBuf stage;
+    // device buffers: owned by a resident stream, borrowed from the context
+    // for one-off decodes (no allocation per call)
+    DevBuf own_stage, own_coarsest, own_base;
+    DevBuf* stage = &own_stage;
+    DevBuf* coarsest = &own_coarsest;
+    DevBuf* base = &own_base;
     StreamDesc* d_sd = nullptr;
     uint16_t* d_sym = nullptr;
     uint8_t* d_len = nullptr;
@@ -203,9 +247,7 @@ struct Prepared {
     uint64_t* d_choff = nullptr;
     uint8_t* d_ulist = nullptr;
     uint32_t* d_payload = nullptr;
-    DevBuf coarsest;
-    DevBuf base;          // cached decoded base grid (level K-2 output) for box queries
-    bool base_valid = false;
+    bool base_valid = false;  // *base holds the decoded base grid (level K-2 output) for box queries
 };
 
 }  // namespace stz
@@ -267,6 +309,14 @@ struct stz_context {
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
         tiles;
     PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small;
+    // device buffers lent to one-off decodes
+    DevBuf p_stage, p_coarsest, p_base;
+    void borrow(Prepared& p)
+    {
+        p.stage = &p_stage;
+        p.coarsest = &p_coarsest;
+        p.base = &p_base;
+    }
 };
 
 struct stz_stream {
@@ -326,6 +376,7 @@ template <typename T>
 stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int nz, const stz_opts& o,
                          stz_stream** out)
 {
+    Lap lap("compress");
     cudaStream_t st = ctx->st;
     const Geometry g = make_geometry(nx, ny, nz, o.chunk_high, o.chunk_low, o.radius);
     const int K = g.K, R2 = 2 * o.radius;
@@ -342,6 +393,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     STZ_CUDA(cudaMemcpyAsync(ctx->h_small.p, ctx->minmax.p, 16, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    lap.mark("value range");
     const unsigned long long* mk = ctx->h_small.as<unsigned long long>();
     const double lo = minmax_key_to_double(mk[0]), hi = minmax_key_to_double(mk[1]);
     double E = o.eb;
@@ -426,6 +478,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    lap.mark("levels + histograms");
 
     // codebooks
     std::vector<std::vector<uint16_t>> syms(nstreams);
@@ -492,6 +545,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const uint32_t* d_ids = (const uint32_t*)(dstage + o_ids);
     const UnpredWork* d_uw = (const UnpredWork*)(dstage + o_uw);
 
+    lap.mark("codebooks + upload");
     // entropy coding
     STZ_CUDA(ctx->ctab.ensure((size_t)nstreams * R2 * 4));
     STZ_CUDA(ctx->sub_bits.ensure(g.total_sub * 4));
@@ -540,6 +594,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     if (total_unpred)
         STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    lap.mark("entropy coding + tables");
     const uint64_t* words = (const uint64_t*)(ht + t_words);
 
     // pack payloads contiguously and copy them back
@@ -565,6 +620,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(ctx->h_payload.ensure(std::max<uint64_t>(packed_total, 1) * 4));
     STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.p, ctx->packed.p, packed_total * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    lap.mark("pack + payload copy");
 
     // container
     FileHeader h;
@@ -598,6 +654,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     auto* so = new (std::nothrow) stz_stream();
     if (!so) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
     so->bytes = write_container(h, coarsest.data(), levels, parts, *ctx->pool);
+    lap.mark("zstd frames + container");
     so->raw_payload_bytes = packed_total * 4;
     const std::string pe = parse_stream(so->bytes.data(), so->bytes.size(), so->dir);
     if (!pe.empty()) {
@@ -611,6 +668,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
 // ---- decode preparation -------------------------------------------------------
 stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
 {
+    Lap lap("prepare");
     const ParsedStream& ps = s->dir;
     const FileHeader& h = ps.h;
     const size_t elem = h.elem();
@@ -630,6 +688,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         else if (!parse_stream_header(raw.data(), raw.size(), nch, L.C, elem, p.hdr[i])) bad = 2;
     });
     if (bad) STZ_FAIL(STZ_ERR_FORMAT, bad == 1 ? "stream header frame does not decode" : "bad stream header");
+    lap.mark("header frames");
     // layout
     uint64_t codes = 0, chunks = 0, subs = 0, words = 0, syms = 0, unp = 0;
     p.ulist_off.assign(nstreams + 1, 0);
@@ -713,6 +772,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         std::memcpy(hs + o_ch + 8 * d.chunk_base, H.chunk_word_off.data(), 8 * H.chunk_word_off.size());
         if (H.n_unpred) std::memcpy(hs + o_ul + p.ulist_off[i] * elem, H.unpred.data(), H.unpred.size());
     }
+    lap.mark("layout + tables");
     // payload frames straight into the staging buffer
     struct Job {
         const uint8_t* src;
@@ -735,9 +795,12 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         if (!decode_frame(jobs[j].src, jobs[j].stored, jobs[j].raw, jobs[j].dst)) bad = 3;
     });
     if (bad) STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
-    STZ_CUDA(p.stage.ensure(total));
-    STZ_CUDA(cudaMemcpyAsync(p.stage.p, hs, total, cudaMemcpyHostToDevice, ctx->st));
-    uint8_t* ds = p.stage.as<uint8_t>();
+    lap.mark("payload frames");
+    STZ_CUDA(p.stage->ensure(total));
+    lap.mark("stage alloc");
+    STZ_CUDA(cudaMemcpyAsync(p.stage->p, hs, total, cudaMemcpyHostToDevice, ctx->st));
+    lap.mark("h2d issue");
+    uint8_t* ds = p.stage->as<uint8_t>();
     p.d_sd = (StreamDesc*)(ds + o_sd);
     p.d_sym = (uint16_t*)(ds + o_sym);
     p.d_len = ds + o_len;
@@ -746,9 +809,11 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
     p.d_ulist = ds + o_ul;
     p.d_payload = (uint32_t*)(ds + o_pl);
     const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
-    STZ_CUDA(p.coarsest.ensure(n0 * elem));
-    STZ_CUDA(cudaMemcpyAsync(p.coarsest.p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
+    STZ_CUDA(p.coarsest->ensure(n0 * elem));
+    STZ_CUDA(cudaMemcpyAsync(p.coarsest->p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
+    lap.mark("coarsest copy");
     STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned staging buffer is reused by the next call
+    lap.mark("host->device");
     return STZ_OK;
 }
 
@@ -822,7 +887,7 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
     const FileHeader& h = ps.h;
     const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
     if (kdec == 0) {
-        STZ_CUDA(cudaMemcpyAsync(out_dev, p.coarsest.p, n0 * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
+        STZ_CUDA(cudaMemcpyAsync(out_dev, p.coarsest->p, n0 * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
         return STZ_OK;
     }
     std::vector<CtaWork> work;
@@ -840,7 +905,7 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
     for (int k = 1; k < kdec; ++k) gmax = std::max(gmax, 8 * (size_t)ps.lv[k].dx * ps.lv[k].dy * ps.lv[k].dz);
     STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
     STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
-    const T* coarse = p.coarsest.as<T>();
+    const T* coarse = p.coarsest->as<T>();
     int cur = 0;
     for (int k = 1; k <= kdec; ++k) {
         LevelDecodeArgs<T> a;
@@ -869,9 +934,14 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     const int kdec = K - level;
     if (s->resident && s->resident->kmax >= kdec) return decode_levels<T>(ctx, s, *s->resident, kdec, out_dev);
     Prepared p;
-    STZ_TRY(prepare(ctx, s, kdec, p));
+    ctx->borrow(p);
+    {
+        Trace t("decompress: prepare");
+        STZ_TRY(prepare(ctx, s, kdec, p));
+    }
+    Trace t("decompress: decode");
     STZ_TRY(decode_levels<T>(ctx, s, p, kdec, out_dev));
-    STZ_CUDA(cudaStreamSynchronize(ctx->st));  // p's device buffers are freed on return
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
     return STZ_OK;
 }
 
@@ -893,6 +963,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     Prepared local;
     Prepared* p = s->resident.get();
     if (!p || p->kmax < K) {
+        ctx->borrow(local);
         STZ_TRY(prepare(ctx, s, K, local));
         p = &local;
     }
@@ -901,8 +972,8 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     const LevelGeom low = level_geom(ps, K - 1), high = level_geom(ps, K);
     const size_t nbase = low.n;
     if (!p->base_valid) {
-        STZ_CUDA(p->base.ensure(nbase * elem));
-        STZ_TRY(decode_levels<T>(ctx, s, *p, K - 2, p->base.as<T>()));
+        STZ_CUDA(p->base->ensure(nbase * elem));
+        STZ_TRY(decode_levels<T>(ctx, s, *p, K - 2, p->base->as<T>()));
         p->base_valid = true;
     }
     // entropy-decode the planned chunks of the low and high levels
@@ -939,7 +1010,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     const T* ud = p->total_unpred ? ctx->unpred_dense.as<T>() : nullptr;
     if (total) {
         KScope ks(ctx, "k_roi_mid");
-        launch_roi_mid<T>(ctx->boxes.as<RoiBox>(), (int)boxes.size(), total, p->base.as<T>(), low,
+        launch_roi_mid<T>(ctx->boxes.as<RoiBox>(), (int)boxes.size(), total, p->base->as<T>(), low,
                           qparams(ps, K - 1), h.predictor, ctx->codes.as<uint16_t>() + p->sd[(size_t)(K - 2) * 7].code_off,
                           ud ? ud + p->sd[(size_t)(K - 2) * 7].code_off : nullptr, ctx->mid.as<T>(), ctx->st);
     }
@@ -1404,6 +1475,7 @@ stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int k, 
     *n_out = n;
     if (n > cap) STZ_FAIL(STZ_ERR_RANGE, "output capacity too small");
     Prepared p;
+    ctx->borrow(p);
     STZ_TRY(prepare(ctx, s, k, p));
     const uint32_t si = (uint32_t)((k - 1) * 7 + block);
     std::vector<CtaWork> work;

@@ -4,19 +4,54 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 #include "stz_internal.h"
 
 // libzstd 1.5.5 is present as a runtime library only; public prototypes (zstd.h).
 extern "C" {
-size_t ZSTD_compress(void* dst, size_t dstCapacity, const void* src, size_t srcSize, int compressionLevel);
-size_t ZSTD_decompress(void* dst, size_t dstCapacity, const void* src, size_t compressedSize);
+typedef struct ZSTD_CCtx_s ZSTD_CCtx;
+typedef struct ZSTD_DCtx_s ZSTD_DCtx;
 size_t ZSTD_compressBound(size_t srcSize);
 unsigned ZSTD_isError(size_t code);
+ZSTD_CCtx* ZSTD_createCCtx(void);
+size_t ZSTD_freeCCtx(ZSTD_CCtx* cctx);
+size_t ZSTD_compressCCtx(ZSTD_CCtx* cctx, void* dst, size_t dstCapacity, const void* src, size_t srcSize,
+                         int compressionLevel);
+ZSTD_DCtx* ZSTD_createDCtx(void);
+size_t ZSTD_freeDCtx(ZSTD_DCtx* dctx);
+size_t ZSTD_decompressDCtx(ZSTD_DCtx* dctx, void* dst, size_t dstCapacity, const void* src, size_t srcSize);
 }
 
 namespace stz {
+
+namespace {
+// One zstd context per host thread, reused across frames (ZSTD_compress /
+// ZSTD_decompress build a fresh one per call; the bytes are the same).
+struct ZstdContexts {
+    ZSTD_CCtx* c = nullptr;
+    ZSTD_DCtx* d = nullptr;
+    ~ZstdContexts()
+    {
+        if (c) ZSTD_freeCCtx(c);
+        if (d) ZSTD_freeDCtx(d);
+    }
+};
+thread_local ZstdContexts tl_zstd;
+
+size_t zstd_compress(void* dst, size_t cap, const void* src, size_t n, int level)
+{
+    if (!tl_zstd.c) tl_zstd.c = ZSTD_createCCtx();
+    return ZSTD_compressCCtx(tl_zstd.c, dst, cap, src, n, level);
+}
+
+size_t zstd_decompress(void* dst, size_t cap, const void* src, size_t n)
+{
+    if (!tl_zstd.d) tl_zstd.d = ZSTD_createDCtx();
+    return ZSTD_decompressDCtx(tl_zstd.d, dst, cap, src, n);
+}
+}  // namespace
 
 // ---- thread pool ------------------------------------------------------------
 ThreadPool::ThreadPool(int threads)
@@ -296,7 +331,7 @@ bool decode_frame(const uint8_t* src, uint64_t stored, uint64_t raw, uint8_t* ds
         if (raw) std::memcpy(dst, src, raw);
         return true;
     }
-    const size_t r = ZSTD_decompress(dst, raw, src, stored);
+    const size_t r = zstd_decompress(dst, raw, src, stored);
     return !ZSTD_isError(r) && r == raw;
 }
 
@@ -373,30 +408,40 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
     struct Frame {
         const uint8_t* src;
         size_t n;
-        std::vector<uint8_t> out;
-        bool raw = false;
+        std::unique_ptr<uint8_t[]> out;
+        size_t stored = 0;
+        bool raw = true;
+        const uint8_t* bytes() const { return raw ? src : out.get(); }
     };
     std::vector<Frame> frames;
     std::vector<size_t> first(parts.size());
     for (size_t i = 0; i < parts.size(); ++i) {
         first[i] = frames.size();
-        frames.push_back({parts[i].hdr.data(), parts[i].hdr.size(), {}});
+        frames.push_back({parts[i].hdr.data(), parts[i].hdr.size(), nullptr});
         for (int L = 0; L < parts[i].layers; ++L) {
             const uint64_t w0 = parts[i].chunk_word_off[(size_t)L * parts[i].chunks_per_layer];
             const uint64_t w1 = parts[i].chunk_word_off[(size_t)(L + 1) * parts[i].chunks_per_layer];
-            frames.push_back({(const uint8_t*)(parts[i].words + w0), (size_t)(4 * (w1 - w0)), {}});
+            frames.push_back({(const uint8_t*)(parts[i].words + w0), (size_t)(4 * (w1 - w0)), nullptr});
         }
     }
+    // largest frames first, so the pool's tail is short
+    std::vector<size_t> order(frames.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return frames[a].n > frames[b].n; });
     const int level = h.zstd_level;
-    pool.parallel_for(frames.size(), [&](size_t i) {
-        Frame& f = frames[i];
+    pool.parallel_for(frames.size(), [&](size_t k) {
+        Frame& f = frames[order[k]];
         f.raw = true;
+        f.stored = f.n;
         if (level > 0 && f.n > 0) {
-            f.out.resize(ZSTD_compressBound(f.n));
-            const size_t c = ZSTD_compress(f.out.data(), f.out.size(), f.src, f.n, level);
+            const size_t cap = ZSTD_compressBound(f.n);
+            f.out.reset(new uint8_t[cap]);
+            const size_t c = zstd_compress(f.out.get(), cap, f.src, f.n, level);
             if (!ZSTD_isError(c) && c < f.n) {
-                f.out.resize(c);
+                f.stored = c;
                 f.raw = false;
+            } else {
+                f.out.reset();
             }
         }
     });
@@ -434,22 +479,21 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
             const StreamParts& p = parts[si];
             w.u32((uint32_t)p.layers);
             const Frame& hf = frames[first[si]];
-            w.u64(hf.raw ? hf.n : hf.out.size());
+            w.u64(hf.stored);
             w.u64(hf.n);
-            for (int L2 = 0; L2 < p.layers; ++L2) {
-                const Frame& f = frames[first[si] + 1 + L2];
-                w.u64(f.raw ? f.n : f.out.size());
-            }
+            for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames[first[si] + 1 + L2].stored);
             for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames[first[si] + 1 + L2].n);
         }
     }
-    size_t total = out.size();
-    for (auto& f : frames) total += f.raw ? f.n : f.out.size();
-    out.reserve(total);
-    for (auto& f : frames) {
-        if (f.raw) w.put(f.src, f.n);
-        else w.put(f.out.data(), f.out.size());
-    }
+    // frames in order after the directory, copied in parallel
+    std::vector<size_t> off(frames.size() + 1);
+    off[0] = out.size();
+    for (size_t i = 0; i < frames.size(); ++i) off[i + 1] = off[i] + frames[i].stored;
+    out.resize(off.back());
+    uint8_t* base = out.data();
+    pool.parallel_for(frames.size(), [&](size_t i) {
+        if (frames[i].stored) std::memcpy(base + off[i], frames[i].bytes(), frames[i].stored);
+    });
     return out;
 }
 

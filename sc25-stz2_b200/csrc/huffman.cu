@@ -71,7 +71,19 @@ __global__ void __launch_bounds__(kCoderThreads) k_sub_bits(const CtaWork* __res
     const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
     uint32_t bits = 0;
-    for (size_t j = 0; j < plane; ++j) bits += __ldg(tab + __ldg(src + j)) & 31u;
+    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
+        // 8 codes per 16-byte load: one request per lane instead of eight
+        const uint4* v = reinterpret_cast<const uint4*>(src);
+        for (size_t j = 0; j < plane / 8; ++j) {
+            const uint4 q = __ldg(v + j);
+            const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                bits += (__ldg(tab + (u[k] & 0xffffu)) & 31u) + (__ldg(tab + (u[k] >> 16)) & 31u);
+        }
+    } else {
+        for (size_t j = 0; j < plane; ++j) bits += __ldg(tab + __ldg(src + j)) & 31u;
+    }
     sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
 }
 
@@ -173,8 +185,8 @@ __global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restr
     uint32_t wi = first_w;
     uint64_t acc = 0;      // pending bits, right-aligned
     int nacc = b0 & 31;    // leading bits of the first word belong to the previous plane (zeros here)
-    for (size_t j = 0; j < plane; ++j) {
-        const uint32_t e = __ldg(tab + __ldg(src + j));
+    auto put = [&](uint32_t code) {
+        const uint32_t e = __ldg(tab + code);
         const int l = e & 31;
         acc = (acc << l) | (e >> 5);
         nacc += l;
@@ -185,6 +197,16 @@ __global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restr
             else out[wi] = word;
             ++wi;
         }
+    };
+    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
+        const uint4* v = reinterpret_cast<const uint4*>(src);
+        for (size_t j = 0; j < plane / 8; ++j) {
+            const uint4 q = __ldg(v + j);
+            put(q.x & 0xffffu), put(q.x >> 16), put(q.y & 0xffffu), put(q.y >> 16);
+            put(q.z & 0xffffu), put(q.z >> 16), put(q.w & 0xffffu), put(q.w >> 16);
+        }
+    } else {
+        for (size_t j = 0; j < plane; ++j) put(__ldg(src + j));
     }
     if (nacc > 0) atomicOr(out + wi, (uint32_t)(acc << (32 - nacc)));
 }
@@ -225,13 +247,18 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
         }
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) {
-        const uint32_t l = cb_len[s.cb_off + i];
-        if (l == 0 || l > (uint32_t)kLutBits) continue;
-        const uint32_t code = first_code[l] + (i - first_idx[l]);
-        const uint32_t e = (uint32_t)cb_sym[s.cb_off + i] | (l << 16);
-        const uint32_t lo = code << (kLutBits - l), hi = (code + 1) << (kLutBits - l);
-        for (uint32_t j = lo; j < hi; ++j) lut[j] = e;
+    // every table entry finds its code: the shortest length whose canonical
+    // range holds the entry's prefix (entries of no code stay 0: slow path)
+    for (uint32_t j = threadIdx.x; j < (1u << kLutBits); j += blockDim.x) {
+        uint32_t e = 0;
+        for (uint32_t l = 1; l <= (uint32_t)kLutBits; ++l) {
+            const uint32_t v = (j >> (kLutBits - l)) - first_code[l];
+            if (v < cnt[l]) {
+                e = (uint32_t)cb_sym[s.cb_off + first_idx[l] + v] | (l << 16);
+                break;
+            }
+        }
+        lut[j] = e;
     }
     __syncthreads();
 
@@ -243,7 +270,12 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
     uint16_t* dst = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
     if (s.n_used == 1) {
         const uint16_t v = cb_sym[s.cb_off];
-        for (size_t j = 0; j < plane; ++j) dst[j] = v;
+        if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
+            const uint32_t v2 = (uint32_t)v | ((uint32_t)v << 16);
+            for (size_t j = 0; j < plane / 8; ++j) reinterpret_cast<uint4*>(dst)[j] = make_uint4(v2, v2, v2, v2);
+        } else {
+            for (size_t j = 0; j < plane; ++j) dst[j] = v;
+        }
         return;
     }
     const uint64_t cw = chunk_word_off[s.chunk_base + c];
@@ -257,7 +289,7 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
     uint64_t buf = (((uint64_t)rd(wi) << 32) | rd(wi + 1)) << (b0 & 31);
     int avail = 64 - (int)(b0 & 31);
     wi += 2;
-    for (size_t j = 0; j < plane; ++j) {
+    auto next = [&]() -> uint32_t {
         if (avail < 32) {
             buf |= (uint64_t)rd(wi) << (32 - avail);
             avail += 32;
@@ -282,7 +314,25 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
         }
         buf <<= l;
         avail -= (int)l;
-        dst[j] = (uint16_t)sym;
+        return sym;
+    };
+    if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
+        // 8 symbols per 16-byte store; all lanes decode in lockstep
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (size_t j = 0; j < plane / 8; ++j) {
+            uint4 v;
+            v.x = next();
+            v.x |= next() << 16;
+            v.y = next();
+            v.y |= next() << 16;
+            v.z = next();
+            v.z |= next() << 16;
+            v.w = next();
+            v.w |= next() << 16;
+            d4[j] = v;
+        }
+    } else {
+        for (size_t j = 0; j < plane; ++j) dst[j] = (uint16_t)next();
     }
 }
 

@@ -1,0 +1,266 @@
+// Level encode / decode kernels (included by levels.cu inside its anonymous
+// namespace, after the tile, histogram and chunk-index helpers).
+//
+// Each level runs as two launches that together cover every coarse point once:
+//   * the interior kernel: points with 1 <= x,y,z <= dim-3, where every block
+//     uses its interior stencil; 32x8x8 bricks with the coarse halo staged in
+//     shared memory, no boundary branches, so no warp ever runs both the
+//     interior and the boundary form of the predictor;
+//   * the shell kernel: the remaining points (index 0, dim-2, dim-1 on some
+//     axis), thread per point, predictor taps read from global memory (L2).
+
+// Shell enumeration: group 1 = boundary z planes (all x, y); group 2 =
+// interior z, boundary y rows (all x); group 3 = interior z and y, boundary x.
+struct Shell {
+    int dx, dy, dz;
+    int nbx, nby, nbz, nix, niy, niz;
+    uint64_t g1, g2, g3;
+    __host__ __device__ static int nb(int d) { return d < 3 ? d : 3; }
+    __host__ __device__ static int ni(int d) { return d > 3 ? d - 3 : 0; }
+    __host__ static Shell make(int dx, int dy, int dz)
+    {
+        Shell s;
+        s.dx = dx, s.dy = dy, s.dz = dz;
+        s.nbx = nb(dx), s.nby = nb(dy), s.nbz = nb(dz);
+        s.nix = ni(dx), s.niy = ni(dy), s.niz = ni(dz);
+        if (s.nix == 0 || s.niy == 0 || s.niz == 0) {  // no interior: every point is shell
+            s.nbz = dz, s.niz = 0;
+        }
+        s.g1 = (uint64_t)s.nbz * dy * dx;
+        s.g2 = (uint64_t)s.niz * s.nby * dx;
+        s.g3 = (uint64_t)s.niz * s.niy * s.nbx;
+        return s;
+    }
+    uint64_t total() const { return g1 + g2 + g3; }
+    // k-th boundary index of an axis of size d: 0, d-2, d-1 (all when d < 4)
+    __device__ static int bval(int k, int d) { return d < 4 ? k : (k == 0 ? 0 : d - 3 + k); }
+    __device__ void point(uint64_t i, int& x, int& y, int& z) const
+    {
+        if (i < g1) {
+            const uint64_t plane = (uint64_t)dy * dx;
+            const int kz = (int)(i / plane);
+            z = nbz == dz ? kz : bval(kz, dz);
+            const uint64_t r = i - (uint64_t)kz * plane;
+            y = (int)(r / dx), x = (int)(r - (uint64_t)y * dx);
+        } else if (i < g1 + g2) {
+            const uint64_t j = i - g1, plane = (uint64_t)nby * dx;
+            z = 1 + (int)(j / plane);
+            const uint64_t r = j - (uint64_t)(z - 1) * plane;
+            y = bval((int)(r / dx), dy), x = (int)(r % dx);
+        } else {
+            const uint64_t j = i - g1 - g2, plane = (uint64_t)niy * nbx;
+            z = 1 + (int)(j / plane);
+            const uint64_t r = j - (uint64_t)(z - 1) * plane;
+            y = 1 + (int)(r / nbx), x = bval((int)(r % nbx), dx);
+        }
+    }
+};
+
+template <typename T>
+struct EncodeIO {
+    const T* __restrict__ field;
+    size_t fsx, fsy;
+    int s;  // sampling stride of the fine grid
+    uint16_t* __restrict__ codes;
+    T* __restrict__ unpred_dense;
+    uint32_t* __restrict__ unpred_cnt;
+    T* __restrict__ G;  // decoded fine grid (coarser levels only)
+};
+
+// One coarse point of the encoder: fine values, 7 predictions, residuals,
+// codes, unpredictable values, decoded fine cell.
+template <typename T, int PRED, bool FINEST, bool INTERIOR, class Acc>
+__device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
+                                             const QuantParams& qp, const ChunkIndex& ci, int x, int y, int z,
+                                             int (&q)[7])
+{
+    using A = Ar<T>;
+    using T2 = typename V2<T>::type;
+    T o[8];
+    if constexpr (FINEST) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int pz = k >> 1, py = k & 1;
+            const T2 t = __ldg(reinterpret_cast<const T2*>(io.field + (size_t)(2 * z + pz) * io.fsy +
+                                                           (size_t)(2 * y + py) * io.fsx + 2 * (size_t)x));
+            o[2 * k] = t.x;
+            o[2 * k + 1] = t.y;
+        }
+    } else {
+        const int s = io.s;
+#pragma unroll
+        for (int si = 1; si < 8; ++si) {
+            const int px = si & 1, py = (si >> 1) & 1, pz = si >> 2;
+            o[si] = __ldg(io.field + (size_t)(s * (2 * z + pz)) * io.fsy + (size_t)(s * (2 * y + py)) * io.fsx +
+                          (size_t)s * (2 * x + px));
+        }
+    }
+    T p[7];
+    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    int chunk;
+    const size_t cm = ci.at(z, chunk);
+    const size_t n = geo.n;
+    T v[8];
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const T d = A::sub(o[b + 1], p[b]);
+        const int code = quantize(d, qp);
+        q[b] = code;
+        io.codes[(size_t)b * n + cm] = (uint16_t)code;
+        if (code == 0) {
+            io.unpred_dense[(size_t)b * n + cm] = d;
+            atomicAdd(&io.unpred_cnt[(size_t)b * (geo.nchunks() + 1) + chunk], 1u);
+        }
+        if constexpr (!FINEST) v[b + 1] = A::add(code ? recover<T>(code, qp) : d, p[b]);
+    }
+    if constexpr (!FINEST) {
+        v[0] = r(0);
+        const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int pz = k >> 1, py = k & 1;
+            T2 t;
+            t.x = v[2 * k];
+            t.y = v[2 * k + 1];
+            *reinterpret_cast<T2*>(io.G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
+        }
+    }
+}
+
+template <typename T, int PRED, bool FINEST>
+__global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
+                                                         QuantParams qp, HistArgs hist)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* tile = reinterpret_cast<T*>(smem_raw);
+    __shared__ uint32_t sh[7][kSmemBins];
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    for (int i = tid; i < 7 * kSmemBins; i += BX * BY) (&sh[0][0])[i] = 0;
+    const int wlo = max(0, qp.radius - kSmemBins / 2);
+    const int wn = min(kSmemBins, 2 * qp.radius - wlo);
+    const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
+    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
+    load_tile(tile, R, dx, dy, dz, x0, y0, z0);
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    const bool valid = x <= dx - 3 && y <= dy - 3;
+    ChunkIndex ci;
+    ci.init(geo, x, y);
+    uint32_t center[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int z1 = min(z0 + BZ, dz - 2);
+    for (int z = z0; z < z1; ++z) {
+        int q[7] = {-1, -1, -1, -1, -1, -1, -1};
+        if (valid) {
+            const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+            encode_point<T, PRED, FINEST, true>(r, io, geo, qp, ci, x, y, z, q);
+        }
+#pragma unroll
+        for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b], center[b]);
+    }
+    hist_flush_center(sh, wlo, wn, hist, center);
+    __syncthreads();
+    for (int i = tid; i < 7 * kSmemBins; i += BX * BY) {
+        const int b = i / kSmemBins, w = i % kSmemBins;
+        const uint32_t c = sh[b][w];
+        if (c) atomicAdd(&hist.full[(size_t)b * 2 * hist.radius + wlo + w], c);
+    }
+}
+
+template <typename T, int PRED, bool FINEST>
+__global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
+                                                            QuantParams qp, HistArgs hist, Shell sh)
+{
+    uint32_t center[7] = {0, 0, 0, 0, 0, 0, 0};
+    const uint64_t total = sh.g1 + sh.g2 + sh.g3;
+    const long long sx = geo.dx, sy = (long long)geo.dx * geo.dy;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < total; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = base + threadIdx.x;
+        int q[7] = {-1, -1, -1, -1, -1, -1, -1};
+        if (i < total) {
+            int x, y, z;
+            sh.point(i, x, y, z);
+            ChunkIndex ci;
+            ci.init(geo, x, y);
+            const GlobalAt<T> r{R + (size_t)z * sy + (size_t)y * sx + x, sx, sy};
+            encode_point<T, PRED, FINEST, false>(r, io, geo, qp, ci, x, y, z, q);
+        }
+#pragma unroll
+        for (int b = 0; b < 7; ++b) hist_warp(nullptr, 0, 0, hist, b, q[b], center[b]);
+    }
+    hist_flush_center(nullptr, 0, 0, hist, center);
+}
+
+// One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
+template <typename T, int PRED, bool INTERIOR, class Acc>
+__device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp,
+                                             const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
+                                             T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z)
+{
+    using A = Ar<T>;
+    using T2 = typename V2<T>::type;
+    int chunk;
+    const size_t cm = ci.at(z, chunk);
+    const size_t n = geo.n;
+    int q[7];
+#pragma unroll
+    for (int b = 0; b < 7; ++b) q[b] = __ldg(codes + (size_t)b * n + cm);
+    T p[7];
+    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    T v[8];
+    v[0] = r(0);
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const T dq = q[b] ? recover<T>(q[b], qp) : __ldg(unpred_dense + (size_t)b * n + cm);
+        v[b + 1] = A::add(dq, p[b]);
+    }
+    const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int pz = k >> 1, py = k & 1;
+        T2 t;
+        t.x = v[2 * k];
+        t.y = v[2 * k + 1];
+        *reinterpret_cast<T2*>(G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
+    }
+}
+
+template <typename T, int PRED>
+__global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
+                                                         const uint16_t* __restrict__ codes,
+                                                         const T* __restrict__ unpred_dense, T* __restrict__ G)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* tile = reinterpret_cast<T*>(smem_raw);
+    const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
+    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
+    load_tile(tile, R, dx, dy, dz, x0, y0, z0);
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x > dx - 3 || y > dy - 3) return;
+    ChunkIndex ci;
+    ci.init(geo, x, y);
+    const int z1 = min(z0 + BZ, dz - 2);
+    for (int z = z0; z < z1; ++z) {
+        const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+        decode_point<T, PRED, true>(r, geo, qp, codes, unpred_dense, G, ci, x, y, z);
+    }
+}
+
+template <typename T, int PRED>
+__global__ void __launch_bounds__(256) k_level_decode_shell(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
+                                                            const uint16_t* __restrict__ codes,
+                                                            const T* __restrict__ unpred_dense, T* __restrict__ G,
+                                                            Shell sh)
+{
+    const uint64_t total = sh.g1 + sh.g2 + sh.g3;
+    const long long sx = geo.dx, sy = (long long)geo.dx * geo.dy;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        sh.point(i, x, y, z);
+        ChunkIndex ci;
+        ci.init(geo, x, y);
+        const GlobalAt<T> r{R + (size_t)z * sy + (size_t)y * sx + x, sx, sy};
+        decode_point<T, PRED, false>(r, geo, qp, codes, unpred_dense, G, ci, x, y, z);
+    }
+}

@@ -1,14 +1,17 @@
 // Level kernels of the STZ hierarchy on B200.
 //
-// Encode (one launch per level): each thread owns one coarse point (x,y,z) of
-// a level and handles all 8 parity positions of the 2x2x2 cell above it. It
-// reads the original fine values straight from the input field (the
-// hierarchical split, FD5:107-139, is never materialised: level k reads the
-// field at stride 2^(K-k)), predicts the 7 odd-parity sub-blocks from the
-// decoded coarse grid (FD5:1005-1047 / 690-748), quantizes the residuals
-// (FD5:1204-1253), writes the codes in chunk-major order for the entropy
-// coder, builds the per-stream code histogram, and, for every level but the
-// finest, writes the decoded fine grid the next level predicts from (the
+// Encode (one launch per level): a CTA covers a 32 x 8 x 8 brick of coarse
+// points of a level; each thread owns one (x, y) column of it and handles all
+// 8 parity positions of the 2x2x2 cell above each coarse point. The brick's
+// coarse-grid halo (x-1..x+2 on every axis, the reach of the cubic stencils)
+// is staged once in shared memory, so every stencil tap is one shared load
+// with a compile-time offset. Per point the kernel reads the original fine
+// values straight from the input field (the hierarchical split, FD5:107-139,
+// is never materialised: level k reads the field at stride 2^(K-k)), predicts
+// the 7 odd-parity sub-blocks (FD5:1005-1047, 690-748), quantizes the
+// residuals (FD5:1204-1253), writes the codes in chunk-major order for the
+// entropy coder, builds the per-stream code histogram, and, on every level but
+// the finest, writes the decoded fine grid the next level predicts from (the
 // encoder's closed loop, FD5:2195-2230).
 //
 // Decode (one launch per level): the same traversal, x' = recover(q) + P
@@ -19,6 +22,7 @@
 // Standalone kernels mirror the reference's per-function boundary (split,
 // merge, zslab preprocess/depreprocess, ROI depreprocess, quantize,
 // dequantize) for callers that drive the stages themselves.
+#include <algorithm>
 #include <cstring>
 
 #include <cuda_runtime.h>
@@ -40,16 +44,61 @@ struct V2<double> {
     using type = double2;
 };
 
-__device__ __forceinline__ size_t chunk_major(const LevelGeom& g, int x, int y, int z, int& chunk)
+// Brick of coarse points per CTA and its halo tile.
+constexpr int BX = 32, BY = 8, BZ = 8;
+constexpr int TSX = BX + 3, TSY = BY + 3, TSZ = BZ + 3;
+constexpr int TPLANE = TSX * TSY;
+constexpr int TELEMS = TPLANE * TSZ;
+
+template <typename T>
+constexpr size_t tile_bytes()
 {
-    const int C = g.C;
-    const int cx = x / C, cy = y / C, cz = z / C;
-    chunk = (cz * g.ncy + cy) * g.ncx + cx;
-    const int lx = x - cx * C, ly = y - cy * C, lz = z - cz * C;
-    return (size_t)chunk * C * C * C + (size_t)(lz * C + ly) * C + lx;
+    return sizeof(T) * TELEMS;
 }
 
-constexpr int kSmemBins = 1024;
+// Stage the coarse grid on [x0-1, x0+BX+1] x [y0-1, y0+BY+1] x [z0-1, z0+BZ+1]
+// (zero outside the grid; the predictors never read those positions).
+template <typename T>
+__device__ __forceinline__ void load_tile(T* tile, const T* __restrict__ R, int dx, int dy, int dz, int x0, int y0,
+                                          int z0)
+{
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    for (int i = tid; i < TELEMS; i += BX * BY) {
+        const int tz = i / TPLANE, rem = i - tz * TPLANE;
+        const int ty = rem / TSX, tx = rem - ty * TSX;
+        const int gx = x0 - 1 + tx, gy = y0 - 1 + ty, gz = z0 - 1 + tz;
+        T v = T(0);
+        if (gx >= 0 && gx < dx && gy >= 0 && gy < dy && gz >= 0 && gz < dz)
+            v = __ldg(R + ((size_t)gz * dy + gy) * dx + gx);
+        tile[i] = v;
+    }
+}
+
+// The 7 predictions of one coarse point.
+template <int PRED, typename T, class Acc>
+__device__ __forceinline__ void predict7(const Acc& r, bool interior, int x, int y, int z, int dx, int dy, int dz,
+                                         T (&p)[7])
+{
+    if (interior) {
+        p[0] = predict_interior_at<PRED, 0, T>(r);
+        p[1] = predict_interior_at<PRED, 1, T>(r);
+        p[2] = predict_interior_at<PRED, 2, T>(r);
+        p[3] = predict_interior_at<PRED, 3, T>(r);
+        p[4] = predict_interior_at<PRED, 4, T>(r);
+        p[5] = predict_interior_at<PRED, 5, T>(r);
+        p[6] = predict_interior_at<PRED, 6, T>(r);
+    } else {
+        p[0] = predict_at<PRED, 0, T>(r, x, y, z, dx, dy, dz);
+        p[1] = predict_at<PRED, 1, T>(r, x, y, z, dx, dy, dz);
+        p[2] = predict_at<PRED, 2, T>(r, x, y, z, dx, dy, dz);
+        p[3] = predict_at<PRED, 3, T>(r, x, y, z, dx, dy, dz);
+        p[4] = predict_at<PRED, 4, T>(r, x, y, z, dx, dy, dz);
+        p[5] = predict_at<PRED, 5, T>(r, x, y, z, dx, dy, dz);
+        p[6] = predict_at<PRED, 6, T>(r, x, y, z, dx, dy, dz);
+    }
+}
+
+constexpr int kSmemBins = 512;
 
 struct HistArgs {
     uint32_t* full;     // 7 x 2r bins
@@ -67,141 +116,53 @@ __device__ __forceinline__ void hist_add(uint32_t (*sh)[kSmemBins], int wlo, int
     if (off < -kHistWindow / 2 || off >= kHistWindow / 2) atomicAdd(&h.outside[b], cnt);
 }
 
-// Warp-aggregated histogram update: one atomic per distinct code in the warp.
-__device__ __forceinline__ void hist_warp(uint32_t (*sh)[kSmemBins], int wlo, int wn, const HistArgs& h, int b, int key)
+// Histogram of one stream: codes equal to the radius (the dominant bin of a
+// well-predicted level) are counted in a register per thread; any other code
+// goes through a warp-aggregated atomic (one per distinct code in the warp).
+// `key` < 0 marks a lane without a code.
+__device__ __forceinline__ void hist_warp(uint32_t (*sh)[kSmemBins], int wlo, int wn, const HistArgs& h, int b, int key,
+                                          uint32_t& center)
 {
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int k0 = __shfl_sync(full, key, 0);
-    if (__all_sync(full, key == k0)) {
-        if (lane == 0 && k0 >= 0) hist_add(sh, wlo, wn, h, b, k0, 32u);
-        return;
-    }
-    const unsigned peers = __match_any_sync(full, key);
-    if (key >= 0 && lane == __ffs(peers) - 1) hist_add(sh, wlo, wn, h, b, key, (uint32_t)__popc(peers));
+    center += key == h.radius;
+    const int k = key == h.radius ? -1 : key;
+    if (!__any_sync(full, k >= 0)) return;
+    const unsigned peers = __match_any_sync(full, k);
+    if (k >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) hist_add(sh, wlo, wn, h, b, k, (uint32_t)__popc(peers));
 }
 
-template <typename T, int PRED, bool FINEST>
-__global__ void __launch_bounds__(256) k_level_encode(const T* __restrict__ field, size_t fsx, size_t fsy, int s,
-                                                      Grid<T> R, LevelGeom geo, QuantParams qp,
-                                                      uint16_t* __restrict__ codes, T* __restrict__ unpred_dense,
-                                                      uint32_t* __restrict__ unpred_cnt, HistArgs hist,
-                                                      T* __restrict__ G, size_t gsx, size_t gsy, int zper)
+// Flush the per-thread dominant-bin counters: warp sum, one atomic per warp.
+__device__ __forceinline__ void hist_flush_center(uint32_t (*sh)[kSmemBins], int wlo, int wn, const HistArgs& h,
+                                                  const uint32_t (&center)[7])
 {
-    using A = Ar<T>;
-    using T2 = typename V2<T>::type;
-    __shared__ uint32_t sh[7][kSmemBins];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int i = tid; i < 7 * kSmemBins; i += blockDim.x * blockDim.y) (&sh[0][0])[i] = 0;
-    const int wlo = max(0, qp.radius - kSmemBins / 2);
-    const int wn = min(kSmemBins, 2 * qp.radius - wlo);
-    __syncthreads();
-
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const bool valid = x < geo.dx && y < geo.dy;
-    const int z0 = blockIdx.z * zper, z1 = min(z0 + zper, geo.dz);
-    const size_t n = geo.n;
-    const int nch1 = geo.nchunks() + 1;
-
-    for (int z = z0; z < z1; ++z) {
-        T o[8];
-        T v[8];
-        int q[7];
-        if (valid) {
-            if constexpr (FINEST) {
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int pz = r >> 1, py = r & 1;
-                    const T2 t = *reinterpret_cast<const T2*>(field + (size_t)(2 * z + pz) * fsy +
-                                                              (size_t)(2 * y + py) * fsx + 2 * (size_t)x);
-                    o[2 * r] = t.x;
-                    o[2 * r + 1] = t.y;
-                }
-            } else {
-#pragma unroll
-                for (int si = 1; si < 8; ++si) {
-                    const int px = si & 1, py = (si >> 1) & 1, pz = si >> 2;
-                    o[si] = __ldg(field + (size_t)(s * (2 * z + pz)) * fsy + (size_t)(s * (2 * y + py)) * fsx +
-                                  (size_t)s * (2 * x + px));
-                }
-            }
-            int chunk;
-            const size_t cm = chunk_major(geo, x, y, z, chunk);
-#pragma unroll
-            for (int b = 0; b < 7; ++b) {
-                const T p = predict<PRED>(b, R, x, y, z);
-                const T d = A::sub(o[b + 1], p);
-                T dec;
-                const int code = quantize(d, qp, dec);
-                q[b] = code;
-                codes[(size_t)b * n + cm] = (uint16_t)code;
-                if (code == 0) {
-                    unpred_dense[(size_t)b * n + cm] = d;
-                    atomicAdd(&unpred_cnt[(size_t)b * nch1 + chunk], 1u);
-                }
-                if (G) v[b + 1] = A::add(code ? recover<T>(code, qp) : d, p);
-            }
-            if (G) {
-                v[0] = R.at((size_t)z * R.sy + (size_t)y * R.sx + x);
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int pz = r >> 1, py = r & 1;
-                    T2 t;
-                    t.x = v[2 * r];
-                    t.y = v[2 * r + 1];
-                    *reinterpret_cast<T2*>(G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int b = 0; b < 7; ++b) q[b] = -1;
-        }
-#pragma unroll
-        for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b]);
-    }
-    __syncthreads();
-    for (int i = tid; i < 7 * kSmemBins; i += blockDim.x * blockDim.y) {
-        const int b = i / kSmemBins, w = i % kSmemBins;
-        const uint32_t c = sh[b][w];
-        if (c) atomicAdd(&hist.full[(size_t)b * 2 * hist.radius + wlo + w], c);
+    for (int b = 0; b < 7; ++b) {
+        uint32_t c = center[b];
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) hist_add(sh, wlo, wn, h, b, h.radius, c);
     }
 }
 
-template <typename T, int PRED>
-__global__ void __launch_bounds__(256) k_level_decode(Grid<T> R, LevelGeom geo, QuantParams qp,
-                                                      const uint16_t* __restrict__ codes,
-                                                      const T* __restrict__ unpred_dense, T* __restrict__ G,
-                                                      size_t gsx, size_t gsy, int zper)
-{
-    using A = Ar<T>;
-    using T2 = typename V2<T>::type;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= geo.dx || y >= geo.dy) return;
-    const int z0 = blockIdx.z * zper, z1 = min(z0 + zper, geo.dz);
-    const size_t n = geo.n;
-    for (int z = z0; z < z1; ++z) {
-        int chunk;
-        const size_t cm = chunk_major(geo, x, y, z, chunk);
-        T v[8];
-        v[0] = R.at((size_t)z * R.sy + (size_t)y * R.sx + x);
-#pragma unroll
-        for (int b = 0; b < 7; ++b) {
-            const int code = __ldg(codes + (size_t)b * n + cm);
-            const T dq = code ? recover<T>(code, qp) : __ldg(unpred_dense + (size_t)b * n + cm);
-            v[b + 1] = A::add(dq, predict<PRED>(b, R, x, y, z));
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int pz = r >> 1, py = r & 1;
-            T2 t;
-            t.x = v[2 * r];
-            t.y = v[2 * r + 1];
-            *reinterpret_cast<T2*>(G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
-        }
+// Chunk-major position of coarse point (x, y, z): the x/y parts are fixed per
+// thread, the z part changes per plane.
+struct ChunkIndex {
+    int C, ncx, ncy;
+    int cx, lx, cy, ly;
+    __device__ __forceinline__ void init(const LevelGeom& g, int x, int y)
+    {
+        C = g.C, ncx = g.ncx, ncy = g.ncy;
+        cx = x / C, lx = x - cx * C;
+        cy = y / C, ly = y - cy * C;
     }
-}
+    __device__ __forceinline__ size_t at(int z, int& chunk) const
+    {
+        const int cz = z / C, lz = z - cz * C;
+        chunk = (cz * ncy + cy) * ncx + cx;
+        return (size_t)chunk * C * C * C + (size_t)((lz * C + ly) * C + lx);
+    }
+};
+
+#include "level_kernels.cuh"
 
 // Coarsest grid of the hierarchy: every 2^K-th point of the field.
 template <typename T>
@@ -215,15 +176,23 @@ __global__ void k_subsample(const T* __restrict__ field, size_t fsx, size_t fsy,
     }
 }
 
-// Value range (max - min in double) of a field, as computeRange (FD5:92-104).
+// Value range of a field (max and min, as computeRange FD5:92-104, NaN
+// ignored). Reduces in T (exact), then converts.
 template <typename T>
 __global__ void k_minmax(const T* __restrict__ p, size_t n, double* out)
 {
-    double lo = __longlong_as_double(0x7fefffffffffffffll), hi = -lo;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double v = (double)p[i];
-        lo = fmin(lo, v);
-        hi = fmax(hi, v);
+    T lo = T(INFINITY), hi = T(-INFINITY);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        const T a = __ldg(p + i), b = __ldg(p + i + stride), c = __ldg(p + i + 2 * stride), d = __ldg(p + i + 3 * stride);
+        lo = fmin(lo, fmin(fmin(a, b), fmin(c, d)));
+        hi = fmax(hi, fmax(fmax(a, b), fmax(c, d)));
+    }
+    for (; i < n; i += stride) {
+        const T a = __ldg(p + i);
+        lo = fmin(lo, a);
+        hi = fmax(hi, a);
     }
     for (int o = 16; o; o >>= 1) {
         lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -231,18 +200,19 @@ __global__ void k_minmax(const T* __restrict__ p, size_t n, double* out)
     }
     __shared__ double slo[32], shi[32];
     const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) slo[w] = lo, shi[w] = hi;
+    if ((threadIdx.x & 31) == 0) slo[w] = (double)lo, shi[w] = (double)hi;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) lo = fmin(lo, slo[i]), hi = fmax(hi, shi[i]);
-        // doubles compare as signed integers after a sign-magnitude fix-up
+        double l = slo[0], h = shi[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) l = fmin(l, slo[k]), h = fmax(h, shi[k]);
+        // doubles compare as unsigned integers after a sign-magnitude fix-up
         unsigned long long* u = reinterpret_cast<unsigned long long*>(out);
         auto key = [](double d) {
             long long b = __double_as_longlong(d);
             return (unsigned long long)(b < 0 ? ~b : (b | 0x8000000000000000ll));
         };
-        atomicMin(&u[0], key(lo));
-        atomicMax(&u[1], key(hi));
+        atomicMin(&u[0], key(l));
+        atomicMax(&u[1], key(h));
     }
 }
 
@@ -304,16 +274,7 @@ __global__ void k_block_op(int mode, int block, const T* __restrict__ src, Grid<
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
         const int x = x0 + (int)(i % ex), y = y0 + (int)((i / ex) % ey), z = z0 + (int)(i / ((size_t)ex * ey));
         const size_t idx = (size_t)z * R.sy + (size_t)y * R.sx + x;
-        T p;
-        switch (block) {
-        case 0: p = predict<PRED>(0, R, x, y, z); break;
-        case 1: p = predict<PRED>(1, R, x, y, z); break;
-        case 2: p = predict<PRED>(2, R, x, y, z); break;
-        case 3: p = predict<PRED>(3, R, x, y, z); break;
-        case 4: p = predict<PRED>(4, R, x, y, z); break;
-        case 5: p = predict<PRED>(5, R, x, y, z); break;
-        default: p = predict<PRED>(6, R, x, y, z); break;
-        }
+        const T p = predict<PRED>(block, R, x, y, z);
         if (mode == 0) dst[idx] = A::sub(src[idx], p);
         else if (mode == 1) dst[idx] = A::add(src[idx], p);
         else
@@ -329,8 +290,7 @@ __global__ void k_quantize(const T* __restrict__ d, size_t n, QuantParams qp, in
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     int code = 1;
     if (i < n) {
-        T dec;
-        code = quantize(d[i], qp, dec);
+        code = quantize(d[i], qp);
         q[i] = code;
     }
     const int c = __syncthreads_count(code == 0);
@@ -396,7 +356,6 @@ __global__ void k_quantize_unpred(const T* __restrict__ d, size_t n, const int* 
     if (f) unpred[off[blockIdx.x] + r] = d[i];
 }
 
-template <typename T>
 __global__ void k_dequant_count(const int* __restrict__ q, size_t n, uint32_t* __restrict__ tile_cnt)
 {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -433,21 +392,37 @@ Grid<T> make_grid(const T* p, int dx, int dy, int dz)
     return g;
 }
 
+// Dynamic shared memory above the 48 KB default needs an opt-in per kernel.
+template <class K>
+void allow_smem(K kernel, size_t bytes)
+{
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 }  // namespace
 
 template <typename T>
 void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
 {
     const LevelGeom& g = a.geo;
-    const int zper = 8;
-    dim3 blk(32, 8, 1);
-    dim3 grd((g.dx + 31) / 32, (g.dy + 7) / 8, (g.dz + zper - 1) / zper);
-    const Grid<T> R = make_grid(a.coarse, g.dx, g.dy, g.dz);
+    const Shell shell = Shell::make(g.dx, g.dy, g.dz);
+    dim3 blk(BX, BY, 1);
+    dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + BZ - 1) / BZ);
+    const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
     HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
-    const size_t gsx = 2 * (size_t)g.dx, gsy = 4 * (size_t)g.dx * g.dy;
-#define STZ_ENC(P, F)                                                                                            \
-    k_level_encode<T, P, F><<<grd, blk, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, R, g, a.qp, a.codes,          \
-                                                 a.unpred_dense, a.unpred_cnt, h, a.decoded, gsx, gsy, zper)
+    const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
+    const size_t sm = tile_bytes<T>();
+    const uint64_t ns = shell.total();
+    const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
+#define STZ_ENC(P, F)                                                                                              \
+    do {                                                                                                           \
+        if (interior) {                                                                                            \
+            auto kern = k_level_encode<T, P, F>;                                                                   \
+            allow_smem(kern, sm);                                                                                  \
+            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h);                                                  \
+        }                                                                                                          \
+        if (ns) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);                \
+    } while (0)
     const bool finest = a.stride == 1;
     if (a.predictor == 1) {
         if (finest) STZ_ENC(1, true);
@@ -463,15 +438,25 @@ template <typename T>
 void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
 {
     const LevelGeom& g = a.geo;
-    const int zper = 8;
-    dim3 blk(32, 8, 1);
-    dim3 grd((g.dx + 31) / 32, (g.dy + 7) / 8, (g.dz + zper - 1) / zper);
-    const Grid<T> R = make_grid(a.coarse, g.dx, g.dy, g.dz);
-    const size_t gsx = 2 * (size_t)g.dx, gsy = 4 * (size_t)g.dx * g.dy;
-    if (a.predictor == 1)
-        k_level_decode<T, 1><<<grd, blk, 0, st>>>(R, g, a.qp, a.codes, a.unpred_dense, a.out, gsx, gsy, zper);
-    else
-        k_level_decode<T, 0><<<grd, blk, 0, st>>>(R, g, a.qp, a.codes, a.unpred_dense, a.out, gsx, gsy, zper);
+    const Shell shell = Shell::make(g.dx, g.dy, g.dz);
+    dim3 blk(BX, BY, 1);
+    dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + BZ - 1) / BZ);
+    const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
+    const size_t sm = tile_bytes<T>();
+    const uint64_t ns = shell.total();
+    const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
+#define STZ_DEC(P)                                                                                                 \
+    do {                                                                                                           \
+        if (interior) {                                                                                            \
+            auto kern = k_level_decode<T, P>;                                                                      \
+            allow_smem(kern, sm);                                                                                  \
+            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out);                         \
+        }                                                                                                          \
+        if (ns) k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
+    } while (0)
+    if (a.predictor == 1) STZ_DEC(1);
+    else STZ_DEC(0);
+#undef STZ_DEC
 }
 
 template <typename T>
@@ -488,7 +473,7 @@ void launch_minmax(const T* p, size_t n, double* out2, cudaStream_t st)
     // out2 holds order-preserving keys; init to (max key, min key)
     const unsigned long long init[2] = {~0ull, 0ull};
     cudaMemcpyAsync(out2, init, sizeof(init), cudaMemcpyHostToDevice, st);
-    k_minmax<T><<<grid_for(n, 256), 256, 0, st>>>(p, n, out2);
+    k_minmax<T><<<148 * 8, 256, 0, st>>>(p, n, out2);
 }
 
 double minmax_key_to_double(unsigned long long k)
@@ -543,7 +528,7 @@ void launch_dequantize(const int* q, size_t n, QuantParams qp, const T* unpred, 
 {
     const size_t tiles = (n + 1023) / 1024;
     if (!tiles) return;
-    k_dequant_count<T><<<(unsigned)tiles, 1024, 0, st>>>(q, n, tile_cnt);
+    k_dequant_count<<<(unsigned)tiles, 1024, 0, st>>>(q, n, tile_cnt);
     k_scan_tiles<<<1, 1024, 0, st>>>(tile_cnt, tiles, tile_off);
     k_dequantize<T><<<(unsigned)tiles, 1024, 0, st>>>(q, n, qp, tile_off, unpred, out);
 }

@@ -6,6 +6,11 @@
 // issuing every floating-point operation as explicit round-to-nearest PTX:
 // f32 ops carry .ftz (flush subnormal inputs and results, as FTZ/DAZ do on the
 // host), and nothing can be contracted into an FMA or reassociated.
+//
+// Predictors read the coarse grid through an accessor `a(off)` relative to the
+// predicted point, with row / plane strides a.sx / a.sy: SmemTile has
+// compile-time strides (every tap is one shared-memory load with an immediate
+// offset), GlobalGrid runtime strides.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -109,13 +114,29 @@ __device__ __forceinline__ double d_mul(double a, double b)
     return r;
 }
 
-// Strided view of the coarse (decoded) grid a level predicts from.
+// Strided view of a coarse (decoded) grid in global memory.
 template <typename T>
 struct Grid {
     const T* __restrict__ p;
     int dx, dy, dz;
     size_t sx, sy;  // row and plane strides (elements)
     __device__ __forceinline__ T at(size_t i) const { return __ldg(p + i); }
+};
+
+// Accessor on a global grid, positioned at one point.
+template <typename T>
+struct GlobalAt {
+    const T* __restrict__ p;
+    long long sx, sy;
+    __device__ __forceinline__ T operator()(long long off) const { return __ldg(p + off); }
+};
+
+// Accessor on a shared-memory tile with compile-time strides.
+template <typename T, int SX, int SY>
+struct TileAt {
+    const T* p;
+    static constexpr int sx = SX, sy = SY;
+    __device__ __forceinline__ T operator()(int off) const { return p[off]; }
 };
 
 // cubic_line_pred (FD5:141-146): -(1/16)a + (9/16)b + (9/16)c - (1/16)d.
@@ -161,172 +182,219 @@ __device__ __forceinline__ T blend4(T p0, T v0, T p1, T v1, T p2, T v2, T p3, T 
     return A::div(num, den);
 }
 
-// FD5 "dynamic lines" predictor for sub-block `block` (= sub_index - 1) at
-// coarse point (x,y,z): predict_block_const<Block> (FD5:690-748) with
-// predict_dynamic_lines_const (FD5:624-688) in the interior.
-template <typename T>
-__device__ __forceinline__ T predict_dynamic(int block, const Grid<T>& g, int x, int y, int z)
+// Interior form of the FD5 "dynamic lines" predictor (predict_interior_const,
+// FD5:828-840, with predict_dynamic_lines_const FD5:624-688). BLOCK = sub_index-1.
+template <int BLOCK, typename T, class Acc>
+__device__ __forceinline__ T dynamic_interior(const Acc& r)
 {
-    using A = Ar<T>;
-    const size_t sx = g.sx, sy = g.sy;
-    const size_t i = (size_t)z * sy + (size_t)y * sx + x;
-    const int dx = g.dx, dy = g.dy, dz = g.dz;
+    const auto sx = r.sx, sy = r.sy;
     T p0, v0, p1, v1, p2, v2, p3, v3;
-    switch (block) {
-    case 0:
-        if (x == dx - 1) return g.at(i);
-        if (x == dx - 2 || x == 0) return A::mul(T(0.5f), A::add(g.at(i), g.at(i + 1)));
-        return cubic(g.at(i - 1), g.at(i), g.at(i + 1), g.at(i + 2));
-    case 1:
-        if (y == dy - 1) return g.at(i);
-        if (y == dy - 2 || y == 0) return A::mul(T(0.5f), A::add(g.at(i), g.at(i + sx)));
-        return cubic(g.at(i - sx), g.at(i), g.at(i + sx), g.at(i + 2 * sx));
-    case 2:
-        if (x == dx - 1 || y == dy - 1) return g.at(i);
-        if (y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
-            return A::mul(T(0.25f), A::add(A::add(A::add(g.at(i), g.at(i + sx + 1)), g.at(i + sx)), g.at(i + 1)));
-        line_pv(g.at(i - sx - 1), g.at(i), g.at(i + sx + 1), g.at(i + 2 * sx + 2), p0, v0);
-        line_pv(g.at(i - sx + 2), g.at(i + 1), g.at(i + sx), g.at(i + 2 * sx - 1), p1, v1);
+    if constexpr (BLOCK == 0) {
+        return cubic(r(-1), r(0), r(1), r(2));
+    } else if constexpr (BLOCK == 1) {
+        return cubic(r(-sx), r(0), r(sx), r(2 * sx));
+    } else if constexpr (BLOCK == 3) {
+        return cubic(r(-sy), r(0), r(sy), r(2 * sy));
+    } else if constexpr (BLOCK == 2) {
+        line_pv(r(-sx - 1), r(0), r(sx + 1), r(2 * sx + 2), p0, v0);
+        line_pv(r(-sx + 2), r(1), r(sx), r(2 * sx - 1), p1, v1);
         return blend2(p0, v0, p1, v1);
-    case 3:
-        if (z == dz - 1) return g.at(i);
-        if (z == dz - 2 || z == 0) return A::mul(T(0.5f), A::add(g.at(i), g.at(i + sy)));
-        return cubic(g.at(i - sy), g.at(i), g.at(i + sy), g.at(i + 2 * sy));
-    case 4:
-        if (x == dx - 1 || z == dz - 1) return g.at(i);
-        if (z == dz - 2 || z == 0 || x == dx - 2 || x == 0)
-            return A::mul(T(0.25f), A::add(A::add(A::add(g.at(i), g.at(i + sy + 1)), g.at(i + 1)), g.at(i + sy)));
-        line_pv(g.at(i - sy - 1), g.at(i), g.at(i + sy + 1), g.at(i + 2 * sy + 2), p0, v0);
-        line_pv(g.at(i - sy + 2), g.at(i + 1), g.at(i + sy), g.at(i + 2 * sy - 1), p1, v1);
+    } else if constexpr (BLOCK == 4) {
+        line_pv(r(-sy - 1), r(0), r(sy + 1), r(2 * sy + 2), p0, v0);
+        line_pv(r(-sy + 2), r(1), r(sy), r(2 * sy - 1), p1, v1);
         return blend2(p0, v0, p1, v1);
-    case 5:
-        if (z == dz - 1 || y == dy - 1) return g.at(i);
-        if (y == dy - 2 || y == 0 || z == dz - 2 || z == 0)
-            return A::mul(T(0.25f), A::add(A::add(A::add(g.at(i), g.at(i + sy + sx)), g.at(i + sy)), g.at(i + sx)));
-        line_pv(g.at(i - sy - sx), g.at(i), g.at(i + sy + sx), g.at(i + 2 * sy + 2 * sx), p0, v0);
-        line_pv(g.at(i - sy + 2 * sx), g.at(i + sx), g.at(i + sy), g.at(i + 2 * sy - sx), p1, v1);
+    } else if constexpr (BLOCK == 5) {
+        line_pv(r(-sy - sx), r(0), r(sy + sx), r(2 * sy + 2 * sx), p0, v0);
+        line_pv(r(-sy + 2 * sx), r(sx), r(sy), r(2 * sy - sx), p1, v1);
         return blend2(p0, v0, p1, v1);
-    default:
-        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return g.at(i);
-        if (z == dz - 2 || z == 0 || y == dy - 2 || y == 0 || x == dx - 2 || x == 0) {
-            T s = A::add(g.at(i), g.at(i + sy + sx + 1));
-            s = A::add(s, g.at(i + sy + sx));
-            s = A::add(s, g.at(i + sy + 1));
-            s = A::add(s, g.at(i + sx + 1));
-            s = A::add(s, g.at(i + 1));
-            s = A::add(s, g.at(i + sx));
-            s = A::add(s, g.at(i + sy));
-            return A::mul(T(0.125f), s);
-        }
-        line_pv(g.at(i - sy - sx - 1), g.at(i), g.at(i + sy + sx + 1), g.at(i + 2 * sy + 2 * sx + 2), p0, v0);
-        line_pv(g.at(i - sy - sx + 2), g.at(i + 1), g.at(i + sy + sx), g.at(i + 2 * sy + 2 * sx - 1), p1, v1);
-        line_pv(g.at(i - sy + 2 * sx - 1), g.at(i + sx), g.at(i + sy + 1), g.at(i + 2 * sy - sx + 2), p2, v2);
-        line_pv(g.at(i + 2 * sy - sx - 1), g.at(i + sy), g.at(i + sx + 1), g.at(i - sy + 2 * sx + 2), p3, v3);
+    } else {
+        line_pv(r(-sy - sx - 1), r(0), r(sy + sx + 1), r(2 * sy + 2 * sx + 2), p0, v0);
+        line_pv(r(-sy - sx + 2), r(1), r(sy + sx), r(2 * sy + 2 * sx - 1), p1, v1);
+        line_pv(r(-sy + 2 * sx - 1), r(sx), r(sy + 1), r(2 * sy - sx + 2), p2, v2);
+        line_pv(r(2 * sy - sx - 1), r(sy), r(sx + 1), r(-sy + 2 * sx + 2), p3, v3);
         return blend4(p0, v0, p1, v1, p2, v2, p3, v3);
     }
 }
 
-// Sum of w*tap over a tap list, left to right, then minus v*tap for the rest:
-// the fixed-stencil expressions of src/float.cpp keep that order.
-template <typename T>
-__device__ __forceinline__ T plain2(const Grid<T>& g, size_t i, T wp, size_t a0, size_t a1, size_t a2, size_t a3,
-                                    T wn, size_t b0, size_t b1, size_t b2, size_t b3)
+// Full FD5 predictor with its boundary rules (predict_block_const,
+// FD5:690-748): last index copies the reference, index 0 / dim-2 average the
+// 2 / 4 / 8 forward neighbours, the rest is the interior form.
+template <int BLOCK, typename T, class Acc>
+__device__ __forceinline__ T dynamic_block(const Acc& r, int x, int y, int z, int dx, int dy, int dz)
 {
     using A = Ar<T>;
-    T s = A::add(A::mul(wp, g.at(a0)), A::mul(wp, g.at(a1)));
-    s = A::add(s, A::mul(wp, g.at(a2)));
-    s = A::add(s, A::mul(wp, g.at(a3)));
-    s = A::sub(s, A::mul(wn, g.at(b0)));
-    s = A::sub(s, A::mul(wn, g.at(b1)));
-    s = A::sub(s, A::mul(wn, g.at(b2)));
-    s = A::sub(s, A::mul(wn, g.at(b3)));
+    const auto sx = r.sx, sy = r.sy;
+    if constexpr (BLOCK == 0) {
+        if (x == dx - 1) return r(0);
+        if (x == dx - 2 || x == 0) return A::mul(T(0.5f), A::add(r(0), r(1)));
+    } else if constexpr (BLOCK == 1) {
+        if (y == dy - 1) return r(0);
+        if (y == dy - 2 || y == 0) return A::mul(T(0.5f), A::add(r(0), r(sx)));
+    } else if constexpr (BLOCK == 3) {
+        if (z == dz - 1) return r(0);
+        if (z == dz - 2 || z == 0) return A::mul(T(0.5f), A::add(r(0), r(sy)));
+    } else if constexpr (BLOCK == 2) {
+        if (x == dx - 1 || y == dy - 1) return r(0);
+        if (y == dy - 2 || y == 0 || x == dx - 2 || x == 0)
+            return A::mul(T(0.25f), A::add(A::add(A::add(r(0), r(sx + 1)), r(sx)), r(1)));
+    } else if constexpr (BLOCK == 4) {
+        if (x == dx - 1 || z == dz - 1) return r(0);
+        if (z == dz - 2 || z == 0 || x == dx - 2 || x == 0)
+            return A::mul(T(0.25f), A::add(A::add(A::add(r(0), r(sy + 1)), r(1)), r(sy)));
+    } else if constexpr (BLOCK == 5) {
+        if (z == dz - 1 || y == dy - 1) return r(0);
+        if (y == dy - 2 || y == 0 || z == dz - 2 || z == 0)
+            return A::mul(T(0.25f), A::add(A::add(A::add(r(0), r(sy + sx)), r(sy)), r(sx)));
+    } else {
+        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return r(0);
+        if (z == dz - 2 || z == 0 || y == dy - 2 || y == 0 || x == dx - 2 || x == 0) {
+            T s = A::add(r(0), r(sy + sx + 1));
+            s = A::add(s, r(sy + sx));
+            s = A::add(s, r(sy + 1));
+            s = A::add(s, r(sx + 1));
+            s = A::add(s, r(1));
+            s = A::add(s, r(sx));
+            s = A::add(s, r(sy));
+            return A::mul(T(0.125f), s);
+        }
+    }
+    return dynamic_interior<BLOCK, T>(r);
+}
+
+// Sum of w*tap over four taps, then minus v*tap for four more: the fixed
+// stencil expressions of src/float.cpp keep that order.
+template <typename T, class Acc, class O>
+__device__ __forceinline__ T plain2(const Acc& r, T wp, O a0, O a1, O a2, O a3, T wn, O b0, O b1, O b2, O b3)
+{
+    using A = Ar<T>;
+    T s = A::add(A::mul(wp, r(a0)), A::mul(wp, r(a1)));
+    s = A::add(s, A::mul(wp, r(a2)));
+    s = A::add(s, A::mul(wp, r(a3)));
+    s = A::sub(s, A::mul(wn, r(b0)));
+    s = A::sub(s, A::mul(wn, r(b1)));
+    s = A::sub(s, A::mul(wn, r(b2)));
+    s = A::sub(s, A::mul(wn, r(b3)));
     return s;
 }
 
-// Plain tricubic-family predictor of src/float.cpp:84-273 (src/stz-rd.cpp
-// templated copy): fixed weights, boundary averages as sums of scaled taps.
-template <typename T>
-__device__ __forceinline__ T predict_plain(int block, const Grid<T>& g, int x, int y, int z)
+// Plain tricubic-family predictor of src/float.cpp:84-273 (templated copy in
+// src/stz-rd.cpp): fixed weights, boundary averages as sums of scaled taps.
+template <int BLOCK, typename T, class Acc>
+__device__ __forceinline__ T plain_block(const Acc& r, int x, int y, int z, int dx, int dy, int dz)
 {
     using A = Ar<T>;
-    const size_t sx = g.sx, sy = g.sy;
-    const size_t i = (size_t)z * sy + (size_t)y * sx + x;
-    const int dx = g.dx, dy = g.dy, dz = g.dz;
-    switch (block) {
-    case 0:
-        if (x == dx - 1) return g.at(i);
-        if (x == dx - 2 || x == 0) return A::add(A::mul(T(0.5f), g.at(i)), A::mul(T(0.5f), g.at(i + 1)));
-        return cubic(g.at(i - 1), g.at(i), g.at(i + 1), g.at(i + 2));
-    case 1:
-        if (y == dy - 1) return g.at(i);
-        if (y == dy - 2 || y == 0) return A::add(A::mul(T(0.5f), g.at(i)), A::mul(T(0.5f), g.at(i + sx)));
-        return cubic(g.at(i - sx), g.at(i), g.at(i + sx), g.at(i + 2 * sx));
-    case 2:
-        if (x == dx - 1 || y == dy - 1) return g.at(i);
+    const auto sx = r.sx, sy = r.sy;
+    using O = decltype(sx + 0);
+    if constexpr (BLOCK == 0) {
+        if (x == dx - 1) return r(0);
+        if (x == dx - 2 || x == 0) return A::add(A::mul(T(0.5f), r(0)), A::mul(T(0.5f), r(1)));
+        return cubic(r(-1), r(0), r(1), r(2));
+    } else if constexpr (BLOCK == 1) {
+        if (y == dy - 1) return r(0);
+        if (y == dy - 2 || y == 0) return A::add(A::mul(T(0.5f), r(0)), A::mul(T(0.5f), r(sx)));
+        return cubic(r(-sx), r(0), r(sx), r(2 * sx));
+    } else if constexpr (BLOCK == 3) {
+        if (z == dz - 1) return r(0);
+        if (z == dz - 2 || z == 0) return A::add(A::mul(T(0.5f), r(0)), A::mul(T(0.5f), r(sy)));
+        return cubic(r(-sy), r(0), r(sy), r(2 * sy));
+    } else if constexpr (BLOCK == 2) {
+        if (x == dx - 1 || y == dy - 1) return r(0);
         if (y == dy - 2 || y == 0 || x == dx - 2 || x == 0) {
-            T s = A::add(A::mul(T(0.25f), g.at(i)), A::mul(T(0.25f), g.at(i + sx + 1)));
-            s = A::add(s, A::mul(T(0.25f), g.at(i + sx)));
-            return A::add(s, A::mul(T(0.25f), g.at(i + 1)));
+            T s = A::add(A::mul(T(0.25f), r(0)), A::mul(T(0.25f), r(sx + 1)));
+            s = A::add(s, A::mul(T(0.25f), r(sx)));
+            return A::add(s, A::mul(T(0.25f), r(1)));
         }
-        return plain2(g, i, T(0.28125f), i, i + sx + 1, i + sx, i + 1, T(0.03125f), i - sx - 1, i + 2 * sx + 2,
-                      i + 2 * sx - 1, i - sx + 2);
-    case 3:
-        if (z == dz - 1) return g.at(i);
-        if (z == dz - 2 || z == 0) return A::add(A::mul(T(0.5f), g.at(i)), A::mul(T(0.5f), g.at(i + sy)));
-        return cubic(g.at(i - sy), g.at(i), g.at(i + sy), g.at(i + 2 * sy));
-    case 4:
-        if (x == dx - 1 || z == dz - 1) return g.at(i);
+        return plain2<T>(r, T(0.28125f), O(0), O(sx + 1), O(sx), O(1), T(0.03125f), O(-sx - 1), O(2 * sx + 2),
+                         O(2 * sx - 1), O(-sx + 2));
+    } else if constexpr (BLOCK == 4) {
+        if (x == dx - 1 || z == dz - 1) return r(0);
         if (z == dz - 2 || z == 0 || x == dx - 2 || x == 0) {
-            T s = A::add(A::mul(T(0.25f), g.at(i)), A::mul(T(0.25f), g.at(i + sy + 1)));
-            s = A::add(s, A::mul(T(0.25f), g.at(i + 1)));
-            return A::add(s, A::mul(T(0.25f), g.at(i + sy)));
+            T s = A::add(A::mul(T(0.25f), r(0)), A::mul(T(0.25f), r(sy + 1)));
+            s = A::add(s, A::mul(T(0.25f), r(1)));
+            return A::add(s, A::mul(T(0.25f), r(sy)));
         }
-        return plain2(g, i, T(0.28125f), i, i + sy + 1, i + 1, i + sy, T(0.03125f), i - sy - 1, i + 2 - sy,
-                      i + 2 * sy - 1, i + 2 * sy + 2);
-    case 5:
-        if (z == dz - 1 || y == dy - 1) return g.at(i);
+        return plain2<T>(r, T(0.28125f), O(0), O(sy + 1), O(1), O(sy), T(0.03125f), O(-sy - 1), O(2 - sy),
+                         O(2 * sy - 1), O(2 * sy + 2));
+    } else if constexpr (BLOCK == 5) {
+        if (z == dz - 1 || y == dy - 1) return r(0);
         if (y == dy - 2 || y == 0 || z == dz - 2 || z == 0) {
-            T s = A::add(A::mul(T(0.25f), g.at(i)), A::mul(T(0.25f), g.at(i + sy + sx)));
-            s = A::add(s, A::mul(T(0.25f), g.at(i + sy)));
-            return A::add(s, A::mul(T(0.25f), g.at(i + sx)));
+            T s = A::add(A::mul(T(0.25f), r(0)), A::mul(T(0.25f), r(sy + sx)));
+            s = A::add(s, A::mul(T(0.25f), r(sy)));
+            return A::add(s, A::mul(T(0.25f), r(sx)));
         }
-        return plain2(g, i, T(0.28125f), i, i + sy + sx, i + sy, i + sx, T(0.03125f), i - sy - sx,
-                      i + 2 * sy + 2 * sx, i + 2 * sy - sx, i + 2 * sx - sy);
-    default: {
-        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return g.at(i);
-        const size_t t[8] = {i, i + sy + sx + 1, i + sy + sx, i + sy + 1, i + sx + 1, i + 1, i + sx, i + sy};
+        return plain2<T>(r, T(0.28125f), O(0), O(sy + sx), O(sy), O(sx), T(0.03125f), O(-sy - sx), O(2 * sy + 2 * sx),
+                         O(2 * sy - sx), O(2 * sx - sy));
+    } else {
+        if (x == dx - 1 || y == dy - 1 || z == dz - 1) return r(0);
         if (z == dz - 2 || z == 0 || y == dy - 2 || y == 0 || x == dx - 2 || x == 0) {
-            T s = A::add(A::mul(T(0.125f), g.at(t[0])), A::mul(T(0.125f), g.at(t[1])));
-#pragma unroll
-            for (int k = 2; k < 8; ++k) s = A::add(s, A::mul(T(0.125f), g.at(t[k])));
-            return s;
+            T s = A::add(A::mul(T(0.125f), r(0)), A::mul(T(0.125f), r(sy + sx + 1)));
+            s = A::add(s, A::mul(T(0.125f), r(sy + sx)));
+            s = A::add(s, A::mul(T(0.125f), r(sy + 1)));
+            s = A::add(s, A::mul(T(0.125f), r(sx + 1)));
+            s = A::add(s, A::mul(T(0.125f), r(1)));
+            s = A::add(s, A::mul(T(0.125f), r(sx)));
+            return A::add(s, A::mul(T(0.125f), r(sy)));
         }
-        T s = A::add(A::mul(T(0.140625f), g.at(t[0])), A::mul(T(0.140625f), g.at(t[1])));
-#pragma unroll
-        for (int k = 2; k < 8; ++k) s = A::add(s, A::mul(T(0.140625f), g.at(t[k])));
-        const size_t u[8] = {i - sy - sx - 1,     i + 2 * sy + 2 * sx + 2, i + 2 * sy - sx + 2, i + 2 * sy + 2 * sx - 1,
-                             i - sy + 2 * sx + 2, i + 2 * sy - sx - 1,     i - sy + 2 * sx - 1, i - sy - sx + 2};
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s = A::sub(s, A::mul(T(0.015625f), g.at(u[k])));
-        return s;
-    }
+        T s = A::add(A::mul(T(0.140625f), r(0)), A::mul(T(0.140625f), r(sy + sx + 1)));
+        s = A::add(s, A::mul(T(0.140625f), r(sy + sx)));
+        s = A::add(s, A::mul(T(0.140625f), r(sy + 1)));
+        s = A::add(s, A::mul(T(0.140625f), r(sx + 1)));
+        s = A::add(s, A::mul(T(0.140625f), r(1)));
+        s = A::add(s, A::mul(T(0.140625f), r(sx)));
+        s = A::add(s, A::mul(T(0.140625f), r(sy)));
+        s = A::sub(s, A::mul(T(0.015625f), r(-sy - sx - 1)));
+        s = A::sub(s, A::mul(T(0.015625f), r(2 * sy + 2 * sx + 2)));
+        s = A::sub(s, A::mul(T(0.015625f), r(2 * sy - sx + 2)));
+        s = A::sub(s, A::mul(T(0.015625f), r(2 * sy + 2 * sx - 1)));
+        s = A::sub(s, A::mul(T(0.015625f), r(-sy + 2 * sx + 2)));
+        s = A::sub(s, A::mul(T(0.015625f), r(2 * sy - sx - 1)));
+        s = A::sub(s, A::mul(T(0.015625f), r(-sy + 2 * sx - 1)));
+        return A::sub(s, A::mul(T(0.015625f), r(-sy - sx + 2)));
     }
 }
 
+// Predictor dispatch: PRED 0 = FD5 dynamic lines, 1 = plain tricubic.
+template <int PRED, int BLOCK, typename T, class Acc>
+__device__ __forceinline__ T predict_at(const Acc& r, int x, int y, int z, int dx, int dy, int dz)
+{
+    if constexpr (PRED == 1) return plain_block<BLOCK, T>(r, x, y, z, dx, dy, dz);
+    else return dynamic_block<BLOCK, T>(r, x, y, z, dx, dy, dz);
+}
+
+// Interior-only form (caller guarantees 1 <= x,y,z <= dim-3 on every axis).
+template <int PRED, int BLOCK, typename T, class Acc>
+__device__ __forceinline__ T predict_interior_at(const Acc& r)
+{
+    if constexpr (PRED == 1) return plain_block<BLOCK, T>(r, 1, 1, 1, 1 << 30, 1 << 30, 1 << 30);
+    else return dynamic_interior<BLOCK, T>(r);
+}
+
+// Runtime-block predictor on a global grid (boundary-kernel and ROI paths).
 template <int PRED, typename T>
 __device__ __forceinline__ T predict(int block, const Grid<T>& g, int x, int y, int z)
 {
-    if constexpr (PRED == 1) return predict_plain(block, g, x, y, z);
-    else return predict_dynamic(block, g, x, y, z);
+    const GlobalAt<T> r{g.p + (size_t)z * g.sy + (size_t)y * g.sx + x, (long long)g.sx, (long long)g.sy};
+    switch (block) {
+    case 0: return predict_at<PRED, 0, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    case 1: return predict_at<PRED, 1, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    case 2: return predict_at<PRED, 2, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    case 3: return predict_at<PRED, 3, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    case 4: return predict_at<PRED, 4, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    case 5: return predict_at<PRED, 5, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    default: return predict_at<PRED, 6, T>(r, x, y, z, g.dx, g.dy, g.dz);
+    }
 }
 
 // quantize_range_nodec for one residual (FD5:1216-1229). Returns the shifted
-// code, 0 when unpredictable. dec receives the decompressed residual.
+// code, 0 when unpredictable. The half == 0 case (|d|/eb < 1) is taken first:
+// there the decompressed value is +-0 and the check reduces to |d| <= eb.
 template <typename T>
-__device__ __forceinline__ int quantize(T d, const QuantParams& qp, T& dec)
+__device__ __forceinline__ int quantize(T d, const QuantParams& qp)
 {
     using A = Ar<T>;
-    const double ad = d_mul(fabs(A::to_f64(d)), qp.recip);
+    const double dd = fabs(A::to_f64(d));
+    const double ad = d_mul(dd, qp.recip);
+    if (ad < 1.0) return dd <= qp.eb ? qp.radius : 0;
     const bool in_range = ad < (double)(2 * qp.radius - 1);
     const double adc = in_range ? ad : 0.0;
     const int half = (__double2int_rz(adc) + 1) >> 1;
@@ -335,7 +403,6 @@ __device__ __forceinline__ int quantize(T d, const QuantParams& qp, T& dec)
     const T dk = neg ? A::neg(mag) : mag;
     const T derr = A::sub(dk, d);
     const bool ok = in_range && (fabs(A::to_f64(derr)) <= qp.eb);
-    dec = dk;
     if (!ok) return 0;
     return neg ? qp.radius - half : qp.radius + half;
 }
