@@ -208,6 +208,25 @@ stz_status stz_quantize_dev(stz_context* ctx, stz_dtype dtype, const void* data,
 stz_status stz_dequantize_dev(stz_context* ctx, stz_dtype dtype, const int32_t* q, size_t n, double eb, int radius,
                               const void* unpred, void* out);
 
+/* stz_quantize_noalloc_dev: the quantizer of stz_quantize_dev (same results,
+ * bit for bit) for callers that cannot allocate device memory — code running
+ * inside another framework's memory pool or arena, latency-critical loops that
+ * must not hit the device-wide synchronization of cudaMalloc/cudaFree, hosts
+ * that reserve all GPU memory up front. It needs no context: work runs on the
+ * caller's CUDA stream (`stream` is a cudaStream_t; NULL = default stream) on
+ * the current device, and its scratch is a fixed array inside the library
+ * image (about 0.8 MB per GPU that loads the library, kept until the process
+ * exits), so at most STZ_NOALLOC_MAX_VALUES values per call; larger n returns
+ * STZ_ERR_RANGE. The first call on a device looks up that array's device
+ * address; make it before any stream capture. All calls share the one array:
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * must be serialized by the caller. The call waits for its stream to finish
+ * and returns the number of unpredictable values in *n_unpred.
+ * This entry point has no counterpart in the reference. */
+#define STZ_NOALLOC_MAX_VALUES ((size_t)65536 * 1024)
+stz_status stz_quantize_noalloc_dev(stz_dtype dtype, const void* data, size_t n, double eb, int radius, int32_t* q,
+                                    void* unpred, size_t* n_unpred, void* stream);
+
 /* ROI planner (FD5:1578-1839) for a query [a, b] on a field of dims
  * (nx,ny,nz), as a flat int64 record:
  *   query x.b x.e y.b y.e z.b z.e is_slice,

@@ -96,6 +96,8 @@ struct Lap {
 
 namespace stz {
 
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 // Grow-only device buffer.
 struct DevBuf {
     void* p = nullptr;

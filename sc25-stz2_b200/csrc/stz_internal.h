@@ -2,10 +2,14 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
 namespace stz {
+
+// Message returned by stz_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 
 // Longest canonical Huffman code of the container format.
 constexpr int kMaxCodeLen = 24;

@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_plan_box.argtypes = [sz, sz, sz, C.c_int, C.c_int, i64p, i64p, i64p, sz, C.POINTER(sz)]
     lib.stz_debug_stream_codes.argtypes = [vp, vp, C.c_int, C.c_int, vp, sz, C.POINTER(sz)]
     lib.stz_debug_codebook.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
+    lib.stz_quantize_noalloc_dev.argtypes = [C.c_int, vp, sz, C.c_double, C.c_int, vp, vp, C.POINTER(sz), vp]
     lib.stz_context_stream.argtypes = [vp, C.POINTER(vp)]
     lib.stz_profile_enable.argtypes = [vp, C.c_int]
     lib.stz_profile_reset.argtypes = [vp]
@@ -370,6 +371,21 @@ class Context:
     def dequantize(self, q, eb, radius, unpred, out):
         _check(self.lib.stz_dequantize_dev(self._c, _tcode(out), self._p(q), q.numel(), eb, radius, self._p(unpred),
                                            self._p(out)))
+
+
+def quantize_noalloc(data, eb: float, radius: int, q, unpred, stream: int = 0) -> int:
+    """Quantize CUDA tensors without any device allocation (no context needed):
+    same results as Context.quantize, on the caller's stream, at most
+    STZ_NOALLOC_MAX_VALUES values per call. Returns the unpredictable count."""
+    lib = load_library()
+    n = C.c_size_t()
+    _check(lib.stz_quantize_noalloc_dev(_tcode(data), C.c_void_p(data.data_ptr()), data.numel(), eb, radius,
+                                        C.c_void_p(q.data_ptr()), C.c_void_p(unpred.data_ptr()), C.byref(n),
+                                        C.c_void_p(stream)))
+    return n.value
+
+
+NOALLOC_MAX_VALUES = 65536 * 1024
 
 
 def _tcode(t) -> int:
