@@ -98,6 +98,22 @@ namespace stz {
 
 void set_last_error(const std::string& msg) { g_err = msg; }
 
+QuantParams make_quant_params(double eb, int radius)
+{
+    QuantParams q;
+    q.eb = eb;
+    q.recip = 1.0 / eb;
+    q.radius = radius;
+    // largest float / double t with t <= eb and t * recip < 1 in double
+    float f = (float)eb;
+    while (f > 0.f && ((double)f > eb || (double)f * q.recip >= 1.0)) f = std::nextafter(f, 0.f);
+    double d = eb;
+    while (d > 0.0 && d * q.recip >= 1.0) d = std::nextafter(d, 0.0);
+    q.tlo32 = f > 0.f ? f : 0.f;
+    q.tlo64 = d > 0.0 ? d : 0.0;
+    return q;
+}
+
 // Grow-only device buffer.
 struct DevBuf {
     void* p = nullptr;
@@ -456,9 +472,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         a.hist_full = ctx->hist.as<uint32_t>() + (size_t)(k - 1) * 7 * R2;
         a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
         a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
-        a.qp.eb = ebk[k];
-        a.qp.recip = 1.0 / ebk[k];
-        a.qp.radius = o.radius;
+        a.qp = make_quant_params(ebk[k], o.radius);
         {
             KScope ks(ctx, k == K ? "k_level_encode[finest]" : "k_level_encode[coarser]");
             launch_level_encode<T>(a, st);
@@ -782,7 +796,9 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         uint8_t* dst;
     };
     std::vector<Job> jobs;
+    std::vector<size_t> stream_first_job(nstreams + 1);
     for (int i = 0; i < nstreams; ++i) {
+        stream_first_job[i] = jobs.size();
         const StreamDir& d = ps.lv[i / 7 + 1].s[i % 7];
         const uint8_t* src = bytes + d.data_off + d.hdr_stored;
         uint8_t* dst = hs + o_pl + 4 * p.sd[i].word_base;
@@ -793,15 +809,30 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         }
         std::memset(dst, 0, 16);  // read-ahead padding of the decoder
     }
-    ctx->pool->parallel_for(jobs.size(), [&](size_t j) {
-        if (!decode_frame(jobs[j].src, jobs[j].stored, jobs[j].raw, jobs[j].dst)) bad = 3;
-    });
-    if (bad) STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
-    lap.mark("payload frames");
+    stream_first_job[nstreams] = jobs.size();
+    // Tables first, then the payload in batches of whole streams: each
+    // batch's host->device copy runs while the next batch is being
+    // zstd-decoded.
     STZ_CUDA(p.stage->ensure(total));
-    lap.mark("stage alloc");
-    STZ_CUDA(cudaMemcpyAsync(p.stage->p, hs, total, cudaMemcpyHostToDevice, ctx->st));
-    lap.mark("h2d issue");
+    STZ_CUDA(cudaMemcpyAsync(p.stage->p, hs, o_pl, cudaMemcpyHostToDevice, ctx->st));
+    const size_t min_batch = 2 * (size_t)ctx->pool->size();
+    for (int s0 = 0; s0 < nstreams;) {
+        int s1 = s0 + 1;
+        while (s1 < nstreams && stream_first_job[s1] - stream_first_job[s0] < min_batch) ++s1;
+        const size_t j0 = stream_first_job[s0], j1 = stream_first_job[s1];
+        ctx->pool->parallel_for(j1 - j0, [&](size_t j) {
+            if (!decode_frame(jobs[j0 + j].src, jobs[j0 + j].stored, jobs[j0 + j].raw, jobs[j0 + j].dst)) bad = 3;
+        });
+        if (bad) {
+            cudaStreamSynchronize(ctx->st);
+            STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
+        }
+        const size_t b0 = o_pl + 4 * p.sd[s0].word_base;
+        const size_t b1 = s1 < nstreams ? o_pl + 4 * p.sd[s1].word_base : total;
+        STZ_CUDA(cudaMemcpyAsync(p.stage->as<uint8_t>() + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st));
+        s0 = s1;
+    }
+    lap.mark("payload frames + h2d");
     uint8_t* ds = p.stage->as<uint8_t>();
     p.d_sd = (StreamDesc*)(ds + o_sd);
     p.d_sym = (uint16_t*)(ds + o_sym);
@@ -1403,7 +1434,7 @@ stz_status stz_quantize_dev(stz_context* ctx, stz_dtype dtype, const void* data,
     STZ_CUDA(ctx->tiles.ensure(align256(tiles * 4) + (tiles + 1) * 8));
     uint32_t* cnt = ctx->tiles.as<uint32_t>();
     uint64_t* off = (uint64_t*)(ctx->tiles.as<uint8_t>() + align256(tiles * 4));
-    QuantParams qp{eb, 1.0 / eb, radius};
+    const QuantParams qp = make_quant_params(eb, radius);
     {
         KScope ks(ctx, "k_quantize", 3);
         if (dtype == STZ_F64) launch_quantize<double>((const double*)data, n, qp, q, (double*)unpred, cnt, off, ctx->st);
@@ -1428,7 +1459,7 @@ stz_status stz_dequantize_dev(stz_context* ctx, stz_dtype dtype, const int32_t* 
     STZ_CUDA(ctx->tiles.ensure(align256(tiles * 4) + (tiles + 1) * 8));
     uint32_t* cnt = ctx->tiles.as<uint32_t>();
     uint64_t* off = (uint64_t*)(ctx->tiles.as<uint8_t>() + align256(tiles * 4));
-    QuantParams qp{eb, 1.0 / eb, radius};
+    const QuantParams qp = make_quant_params(eb, radius);
     KScope ks(ctx, "k_dequantize", 3);
     if (dtype == STZ_F64) launch_dequantize<double>(q, n, qp, (const double*)unpred, (double*)out, cnt, off, ctx->st);
     else launch_dequantize<float>(q, n, qp, (const float*)unpred, (float*)out, cnt, off, ctx->st);

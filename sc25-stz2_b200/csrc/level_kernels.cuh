@@ -71,8 +71,8 @@ struct EncodeIO {
 // codes, unpredictable values, decoded fine cell.
 template <typename T, int PRED, bool FINEST, bool INTERIOR, class Acc>
 __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
-                                             const QuantParams& qp, const ChunkIndex& ci, int x, int y, int z,
-                                             int (&q)[7])
+                                             const QuantParams& qp, const T* lut, const ChunkIndex& ci, int x, int y,
+                                             int z, int (&q)[7])
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -111,7 +111,7 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
             io.unpred_dense[(size_t)b * n + cm] = d;
             atomicAdd(&io.unpred_cnt[(size_t)b * (geo.nchunks() + 1) + chunk], 1u);
         }
-        if constexpr (!FINEST) v[b + 1] = A::add(code ? recover<T>(code, qp) : d, p[b]);
+        if constexpr (!FINEST) v[b + 1] = A::add(code ? recover_lut(lut, code, qp) : d, p[b]);
     }
     if constexpr (!FINEST) {
         v[0] = r(0);
@@ -134,8 +134,10 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ uint32_t sh[7][kSmemBins];
+    __shared__ T lut[2 * kRecW];
     const int tid = threadIdx.y * BX + threadIdx.x;
     for (int i = tid; i < 7 * kSmemBins; i += BX * BY) (&sh[0][0])[i] = 0;
+    if constexpr (!FINEST) build_recover_lut(lut, qp, tid, BX * BY);
     const int wlo = max(0, qp.radius - kSmemBins / 2);
     const int wn = min(kSmemBins, 2 * qp.radius - wlo);
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};
         if (valid) {
             const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-            encode_point<T, PRED, FINEST, true>(r, io, geo, qp, ci, x, y, z, q);
+            encode_point<T, PRED, FINEST, true>(r, io, geo, qp, lut, ci, x, y, z, q);
         }
 #pragma unroll
         for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b], center[b]);
@@ -170,6 +172,9 @@ template <typename T, int PRED, bool FINEST>
 __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                             QuantParams qp, HistArgs hist, Shell sh)
 {
+    __shared__ T lut[2 * kRecW];
+    if constexpr (!FINEST) build_recover_lut(lut, qp, threadIdx.x, blockDim.x);
+    __syncthreads();
     uint32_t center[7] = {0, 0, 0, 0, 0, 0, 0};
     const uint64_t total = sh.g1 + sh.g2 + sh.g3;
     const long long sx = geo.dx, sy = (long long)geo.dx * geo.dy;
@@ -182,7 +187,7 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
             ChunkIndex ci;
             ci.init(geo, x, y);
             const GlobalAt<T> r{R + (size_t)z * sy + (size_t)y * sx + x, sx, sy};
-            encode_point<T, PRED, FINEST, false>(r, io, geo, qp, ci, x, y, z, q);
+            encode_point<T, PRED, FINEST, false>(r, io, geo, qp, lut, ci, x, y, z, q);
         }
 #pragma unroll
         for (int b = 0; b < 7; ++b) hist_warp(nullptr, 0, 0, hist, b, q[b], center[b]);
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
 
 // One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
 template <typename T, int PRED, bool INTERIOR, class Acc>
-__device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp,
+__device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp, const T* lut,
                                              const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
                                              T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z)
 {
@@ -210,7 +215,7 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     v[0] = r(0);
 #pragma unroll
     for (int b = 0; b < 7; ++b) {
-        const T dq = q[b] ? recover<T>(q[b], qp) : __ldg(unpred_dense + (size_t)b * n + cm);
+        const T dq = q[b] ? recover_lut(lut, q[b], qp) : __ldg(unpred_dense + (size_t)b * n + cm);
         v[b + 1] = A::add(dq, p[b]);
     }
     const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
@@ -231,6 +236,8 @@ __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
+    __shared__ T lut[2 * kRecW];
+    build_recover_lut(lut, qp, threadIdx.y * BX + threadIdx.x, BX * BY);
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
     const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
     load_tile(tile, R, dx, dy, dz, x0, y0, z0);
@@ -242,7 +249,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R
     const int z1 = min(z0 + BZ, dz - 2);
     for (int z = z0; z < z1; ++z) {
         const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-        decode_point<T, PRED, true>(r, geo, qp, codes, unpred_dense, G, ci, x, y, z);
+        decode_point<T, PRED, true>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z);
     }
 }
 
@@ -252,6 +259,9 @@ __global__ void __launch_bounds__(256) k_level_decode_shell(const T* __restrict_
                                                             const T* __restrict__ unpred_dense, T* __restrict__ G,
                                                             Shell sh)
 {
+    __shared__ T lut[2 * kRecW];
+    build_recover_lut(lut, qp, threadIdx.x, blockDim.x);
+    __syncthreads();
     const uint64_t total = sh.g1 + sh.g2 + sh.g3;
     const long long sx = geo.dx, sy = (long long)geo.dx * geo.dy;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
@@ -261,6 +271,6 @@ __global__ void __launch_bounds__(256) k_level_decode_shell(const T* __restrict_
         ChunkIndex ci;
         ci.init(geo, x, y);
         const GlobalAt<T> r{R + (size_t)z * sy + (size_t)y * sx + x, sx, sy};
-        decode_point<T, PRED, false>(r, geo, qp, codes, unpred_dense, G, ci, x, y, z);
+        decode_point<T, PRED, false>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z);
     }
 }

@@ -146,21 +146,47 @@ __device__ __forceinline__ void hist_flush_center(uint32_t (*sh)[kSmemBins], int
 // Chunk-major position of coarse point (x, y, z): the x/y parts are fixed per
 // thread, the z part changes per plane.
 struct ChunkIndex {
-    int C, ncx, ncy;
+    int C, lc, ncx, ncy;  // lc = log2(C) for power-of-two edges, else -1
     int cx, lx, cy, ly;
     __device__ __forceinline__ void init(const LevelGeom& g, int x, int y)
     {
         C = g.C, ncx = g.ncx, ncy = g.ncy;
-        cx = x / C, lx = x - cx * C;
-        cy = y / C, ly = y - cy * C;
+        lc = (C & (C - 1)) == 0 ? __ffs(C) - 1 : -1;
+        if (lc >= 0) {
+            cx = x >> lc, lx = x & (C - 1);
+            cy = y >> lc, ly = y & (C - 1);
+        } else {
+            cx = x / C, lx = x - cx * C;
+            cy = y / C, ly = y - cy * C;
+        }
     }
     __device__ __forceinline__ size_t at(int z, int& chunk) const
     {
+        if (lc >= 0) {
+            const int cz = z >> lc, lz = z & (C - 1);
+            chunk = (cz * ncy + cy) * ncx + cx;
+            return ((size_t)chunk << (3 * lc)) + (size_t)((((lz << lc) + ly) << lc) + lx);
+        }
         const int cz = z / C, lz = z - cz * C;
         chunk = (cz * ncy + cy) * ncx + cx;
         return (size_t)chunk * C * C * C + (size_t)((lz * C + ly) * C + lx);
     }
 };
+
+// Recover table for the codes around the radius (the reference's recover LUT,
+// FD5:1528-1535): one shared load instead of int->double->T conversions.
+constexpr int kRecW = 256;
+template <typename T>
+__device__ __forceinline__ void build_recover_lut(T* lut, const QuantParams& qp, int tid, int nthreads)
+{
+    for (int i = tid; i < 2 * kRecW; i += nthreads) lut[i] = recover<T>(qp.radius - kRecW + i, qp);
+}
+template <typename T>
+__device__ __forceinline__ T recover_lut(const T* lut, int q, const QuantParams& qp)
+{
+    const unsigned i = (unsigned)(q - qp.radius + kRecW);
+    return i < 2u * kRecW ? lut[i] : recover<T>(q, qp);
+}
 
 #include "level_kernels.cuh"
 
@@ -392,11 +418,12 @@ Grid<T> make_grid(const T* p, int dx, int dy, int dz)
     return g;
 }
 
-// Dynamic shared memory above the 48 KB default needs an opt-in per kernel.
+// The kernel's dynamic shared memory (its static arrays come on top; above 48
+// KB in total the launch needs this opt-in).
 template <class K>
 void allow_smem(K kernel, size_t bytes)
 {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 }  // namespace

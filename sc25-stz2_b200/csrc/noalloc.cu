@@ -98,7 +98,7 @@ extern "C" stz_status stz_quantize_noalloc_dev(stz_dtype dtype, const void* data
     uint32_t* cnt = static_cast<uint32_t*>(base);
     uint64_t* off = reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(base) + kCntBytes);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const stz::QuantParams qp{eb, 1.0 / eb, radius};
+    const stz::QuantParams qp = stz::make_quant_params(eb, radius);
     if (dtype == STZ_F64)
         stz::launch_quantize<double>(static_cast<const double*>(data), n, qp, q, static_cast<double*>(unpred), cnt, off, st);
     else

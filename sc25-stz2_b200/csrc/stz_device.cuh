@@ -392,6 +392,11 @@ template <typename T>
 __device__ __forceinline__ int quantize(T d, const QuantParams& qp)
 {
     using A = Ar<T>;
+    if constexpr (sizeof(T) == 4) {
+        if (fabsf(d) < qp.tlo32) return qp.radius;
+    } else {
+        if (fabs(d) < qp.tlo64) return qp.radius;
+    }
     const double dd = fabs(A::to_f64(d));
     const double ad = d_mul(dd, qp.recip);
     if (ad < 1.0) return dd <= qp.eb ? qp.radius : 0;

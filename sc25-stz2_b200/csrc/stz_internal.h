@@ -27,7 +27,15 @@ struct QuantParams {
     double eb;
     double recip;
     int radius;
+    // |d| < tlo (in the residual's own type) guarantees code == radius: tlo is
+    // the largest value <= eb with fl(tlo * recip) < 1. Zero disables the
+    // shortcut (it is only an early exit; the full path gives the same code).
+    float tlo32 = 0.f;
+    double tlo64 = 0.0;
 };
+
+// Quantizer constants with the fast-path thresholds filled in.
+QuantParams make_quant_params(double eb, int radius);
 
 // One refinement level: the 7 residual sub-blocks of size (dx,dy,dz) predicted
 // from the decoded coarse grid of the same size.
