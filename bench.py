@@ -52,6 +52,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2025)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--once", action="store_true",
+                   help="one compress + one full decompress of the workload, no timing (profiler captures)")
     return p.parse_args()
 
 
@@ -268,6 +270,16 @@ def main():
     out = torch.empty_like(field)
     opts = stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd)
     stream = torch.cuda.ExternalStream(ctx.cuda_stream(), device=f"cuda:{local}")
+    if args.once:
+        s = ctx.compress(field, opts=opts)
+        ctx.decompress(s, out=out)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"once": True, "field": [n, n, n], "stream_bytes": len(s)}))
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     def step():
         s = ctx.compress(field, opts=opts)
