@@ -58,7 +58,9 @@ def parse_args():
 
 
 def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    from stz_b200.replicas import rank_env
+
+    return rank_env()
 
 
 # ---- clocks ---------------------------------------------------------------------
@@ -251,21 +253,16 @@ def main():
         run_reference(args)
         return
     import torch
-    import torch.distributed as dist
 
     import stz_b200
-    from stz_b200 import fields
+    from stz_b200 import fields, replicas
 
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    replicas.init("nccl", timeout_s=120, device=torch.device("cuda", local))
     n = args.size
     ctx = stz_b200.Context(local)
-    field = fields.lognormal((n, n, n), args.seed + rank, np.float32, device=f"cuda:{local}")
+    field = fields.lognormal((n, n, n), replicas.replica_seed(args.seed, rank), np.float32, device=f"cuda:{local}")
     nbytes = field.numel() * field.element_size()
     out = torch.empty_like(field)
     opts = stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd)
@@ -277,8 +274,7 @@ def main():
         if rank == 0:
             print(json.dumps({"once": True, "field": [n, n, n], "stream_bytes": len(s)}))
         ctx.close()
-        if world > 1:
-            dist.destroy_process_group()
+        replicas.finalize()
         return
 
     def step():
@@ -300,8 +296,7 @@ def main():
     time.sleep(0.3)
     ctx.profile(True)
     ctx.profile_reset()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
     ev[0].record(stream)
@@ -313,17 +308,14 @@ def main():
     torch.cuda.synchronize()
     prof = ctx.profile_read()
     ctx.profile(False)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     clk = clocks.stop()
     comp_ms = sum(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(args.steps))
     dec_ms = sum(ev[2 * i + 1].elapsed_time(ev[2 * i + 2]) for i in range(args.steps))
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * 2 * nbytes * args.steps / (total_ms / 1e3) / 1e9
+    total_ms = replicas.max_over_ranks(ev[0].elapsed_time(ev[-1]), device="cuda")
+    comp_ms = replicas.max_over_ranks(comp_ms, device="cuda")
+    dec_ms = replicas.max_over_ranks(dec_ms, device="cuda")
+    value = replicas.aggregate_gbs(2 * nbytes * args.steps, world, total_ms)
     launches = int(sum(v[1] for v in prof.values()))
 
     # end to end through the host-buffer API
@@ -333,8 +325,7 @@ def main():
         host_out = np.empty((n, n, n), np.float32)
         s = ctx.compress(host_field, opts=opts)
         ctx.decompress(s, out=host_out)
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -343,13 +334,9 @@ def main():
             ctx.decompress(s, out=host_out)
         e1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
         inf = s.info()
-        e2e = {"value": world * 2 * nbytes * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+        e2e = {"value": replicas.aggregate_gbs(2 * nbytes * args.steps, world, e2e_ms), "unit": "GB/s",
                "h2d_bytes_per_step": nbytes + inf.raw_payload_bytes,
                "d2h_bytes_per_step": nbytes + inf.raw_payload_bytes}
         assert np.array_equal(host_out.view(np.uint32), out.cpu().numpy().view(np.uint32))
@@ -395,16 +382,15 @@ def main():
             "config": {"workload": "512^3 f32 lognormal, rel eb 1e-3, compress + full decompress",
                        "field": [n, n, n], "rel_eb": args.rel, "zstd_level": args.zstd,
                        "l2": "inputs larger than L2 (512 MiB field per step)", "parallelism": f"replicas x{world}"},
-            "compress_gbs": world * nbytes * args.steps / (comp_ms / 1e3) / 1e9,
-            "decompress_gbs": world * nbytes * args.steps / (dec_ms / 1e3) / 1e9,
+            "compress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, comp_ms),
+            "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
             "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         }
         print(json.dumps(res))
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 if __name__ == "__main__":
