@@ -30,69 +30,13 @@
 #include "huffman.h"
 #include "levels.h"
 #include "roi.h"
+#include "runtime.h"
 #include "stz/stz.h"
 #include "stz_internal.h"
 
 namespace {
 thread_local std::string g_err;
-
-// Host phase timer, printed to stderr when STZ_TRACE is set.
-struct Trace {
-    const char* name;
-    std::chrono::steady_clock::time_point t0;
-    bool on;
-    explicit Trace(const char* n) : name(n), on(std::getenv("STZ_TRACE") != nullptr)
-    {
-        if (on) t0 = std::chrono::steady_clock::now();
-    }
-    ~Trace()
-    {
-        if (on)
-            std::fprintf(stderr, "[stz] %-28s %8.3f ms\n", name,
-                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-    }
-};
-
-// Lap timer: mark(name) prints the time since the previous mark (STZ_TRACE).
-struct Lap {
-    const char* scope;
-    std::chrono::steady_clock::time_point t;
-    bool on;
-    explicit Lap(const char* s) : scope(s), on(std::getenv("STZ_TRACE") != nullptr)
-    {
-        if (on) t = std::chrono::steady_clock::now();
-    }
-    void mark(const char* what)
-    {
-        if (!on) return;
-        const auto now = std::chrono::steady_clock::now();
-        std::fprintf(stderr, "[stz] %s: %-24s %8.3f ms\n", scope, what,
-                     std::chrono::duration<double, std::milli>(now - t).count());
-        t = now;
-    }
-};
 }  // namespace
-
-#define STZ_FAIL(code, msg)    \
-    do {                       \
-        g_err = (msg);         \
-        return (code);         \
-    } while (0)
-
-#define STZ_CUDA(x)                                                                         \
-    do {                                                                                    \
-        cudaError_t e_ = (x);                                                               \
-        if (e_ != cudaSuccess) {                                                            \
-            g_err = std::string(#x) + ": " + cudaGetErrorString(e_);                        \
-            return e_ == cudaErrorMemoryAllocation ? STZ_ERR_NOMEM : STZ_ERR_CUDA;          \
-        }                                                                                   \
-    } while (0)
-
-#define STZ_TRY(x)                  \
-    do {                            \
-        stz_status s_ = (x);        \
-        if (s_ != STZ_OK) return s_; \
-    } while (0)
 
 namespace stz {
 
@@ -113,68 +57,6 @@ QuantParams make_quant_params(double eb, int radius)
     q.tlo64 = d > 0.0 ? d : 0.0;
     return q;
 }
-
-// Grow-only device buffer.
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf()
-    {
-        if (p) cudaFree(p);
-    }
-    cudaError_t ensure(size_t bytes)
-    {
-        if (bytes <= cap && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        const size_t b = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e == cudaSuccess) cap = b;
-        else p = nullptr;
-        return e;
-    }
-    template <class T>
-    T* as() const
-    {
-        return (T*)p;
-    }
-};
-
-// Grow-only pinned host buffer.
-struct PinBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    PinBuf() = default;
-    PinBuf(const PinBuf&) = delete;
-    PinBuf& operator=(const PinBuf&) = delete;
-    ~PinBuf()
-    {
-        if (p) cudaFreeHost(p);
-    }
-    cudaError_t ensure(size_t bytes)
-    {
-        if (bytes <= cap && p) return cudaSuccess;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        const size_t b = std::max<size_t>(bytes, 4096);
-        cudaError_t e = cudaHostAlloc(&p, b, cudaHostAllocDefault);
-        if (e == cudaSuccess) cap = b;
-        else p = nullptr;
-        return e;
-    }
-    template <class T>
-    T* as() const
-    {
-        return (T*)p;
-    }
-};
-
-static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Shape of the hierarchy for given dims and options.
 struct Geometry {
@@ -224,9 +106,8 @@ static Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_
     return g;
 }
 
-// CTA work items for chunk lists: groups of up to kCoderThreads / C chunks.
-static void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, const uint32_t* chunks,
-                     size_t n, int C)
+void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, const uint32_t* chunks,
+              size_t n, int C)
 {
     const size_t G = std::max(1, kCoderThreads / C);
     for (size_t i = 0; i < n; i += G) {
@@ -236,137 +117,12 @@ static void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uin
     }
 }
 
-static void add_all_chunks(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, uint32_t nchunks,
-                           int C)
+void add_all_chunks(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, uint32_t nchunks, int C)
 {
     std::vector<uint32_t> all(nchunks);
     for (uint32_t i = 0; i < nchunks; ++i) all[i] = i;
     add_work(work, ids, stream, all.data(), all.size(), C);
 }
-
-// Device-resident decode inputs of levels 1..kmax of one stream object.
-struct Prepared {
-    int kmax = 0;
-    std::vector<StreamDesc> sd;
-    std::vector<StreamHeader> hdr;
-    std::vector<std::vector<uint64_t>> unpred_prefix;  // per stream, per chunk: list offset
-    std::vector<uint64_t> ulist_off;                   // per stream: element offset in the unpred list
-    uint64_t total_codes = 0, total_unpred = 0;
-    // device buffers: owned by a resident stream, borrowed from the context
-    // for one-off decodes (no allocation per call)
-    DevBuf own_stage, own_coarsest, own_base;
-    DevBuf* stage = &own_stage;
-    DevBuf* coarsest = &own_coarsest;
-    DevBuf* base = &own_base;
-    StreamDesc* d_sd = nullptr;
-    uint16_t* d_sym = nullptr;
-    uint8_t* d_len = nullptr;
-    uint32_t* d_sub = nullptr;
-    uint64_t* d_choff = nullptr;
-    uint8_t* d_ulist = nullptr;
-    uint32_t* d_payload = nullptr;
-    bool base_valid = false;  // *base holds the decoded base grid (level K-2 output) for box queries
-};
-
-}  // namespace stz
-
-using namespace stz;
-
-struct stz_context {
-    int device = 0;
-    cudaStream_t st = nullptr;
-    std::unique_ptr<ThreadPool> pool;
-    // kernel profiling (stz_profile_*)
-    struct ProfRec {
-        const char* name;
-        cudaEvent_t a, b;
-    };
-    bool prof_on = false;
-    std::vector<ProfRec> pending;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::string> prof_names;
-    std::vector<double> prof_ms;
-    std::vector<uint64_t> prof_launches;
-    size_t prof_slot(const char* name)
-    {
-        for (size_t i = 0; i < prof_names.size(); ++i)
-            if (prof_names[i] == name) return i;
-        prof_names.emplace_back(name);
-        prof_ms.push_back(0.0);
-        prof_launches.push_back(0);
-        return prof_names.size() - 1;
-    }
-    cudaEvent_t event()
-    {
-        if (!ev_pool.empty()) {
-            cudaEvent_t e = ev_pool.back();
-            ev_pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e = nullptr;
-        cudaEventCreate(&e);
-        return e;
-    }
-    void flush_prof()
-    {
-        for (auto& r : pending) {
-            float ms = 0.f;
-            if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess)
-                prof_ms[prof_slot(r.name)] += ms;
-            ev_pool.push_back(r.a);
-            ev_pool.push_back(r.b);
-        }
-        pending.clear();
-    }
-    ~stz_context()
-    {
-        flush_prof();
-        for (auto e : ev_pool) cudaEventDestroy(e);
-    }
-    DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
-        stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
-        tiles;
-    PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small;
-    // device buffers lent to one-off decodes
-    DevBuf p_stage, p_coarsest, p_base;
-    void borrow(Prepared& p)
-    {
-        p.stage = &p_stage;
-        p.coarsest = &p_coarsest;
-        p.base = &p_base;
-    }
-};
-
-struct stz_stream {
-    std::vector<uint8_t> bytes;
-    ParsedStream dir;
-    size_t raw_payload_bytes = 0;
-    std::unique_ptr<Prepared> resident;
-};
-
-namespace {
-
-// Counts the launches of one kernel and, when profiling is on, brackets them
-// with events on the context's stream.
-struct KScope {
-    stz_context* c;
-    cudaEvent_t b = nullptr;
-    KScope(stz_context* ctx, const char* name, int launches = 1) : c(ctx)
-    {
-        c->prof_launches[c->prof_slot(name)] += (uint64_t)launches;
-        if (c->prof_on) {
-            if (c->pending.size() > 4096) c->flush_prof();
-            cudaEvent_t a = c->event();
-            b = c->event();
-            cudaEventRecord(a, c->st);
-            c->pending.push_back({name, a, b});
-        }
-    }
-    ~KScope()
-    {
-        if (b) cudaEventRecord(b, c->st);
-    }
-};
 
 int pool_threads(int requested)
 {
@@ -1069,7 +825,16 @@ stz_status enter(stz_context* ctx)
     return STZ_OK;
 }
 
-}  // namespace
+template stz_status decode_chunks<float>(stz_context*, const Prepared&, const std::vector<CtaWork>&,
+                                         const std::vector<uint32_t>&, const std::vector<UnpredWork>&);
+template stz_status decode_chunks<double>(stz_context*, const Prepared&, const std::vector<CtaWork>&,
+                                          const std::vector<uint32_t>&, const std::vector<UnpredWork>&);
+template stz_status decode_levels<float>(stz_context*, const stz_stream*, const Prepared&, int, float*);
+template stz_status decode_levels<double>(stz_context*, const stz_stream*, const Prepared&, int, double*);
+
+}  // namespace stz
+
+using namespace stz;
 
 extern "C" {
 
