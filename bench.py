@@ -54,6 +54,9 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--once", action="store_true",
                    help="one compress + one full decompress of the workload, no timing (profiler captures)")
+    p.add_argument("--no-serve", action="store_true", help="skip the request-server latency measurement")
+    p.add_argument("--serve-size", type=int, default=1024, help="edge of the resident serving field")
+    p.add_argument("--serve-seconds", type=float, default=2.0, help="length of each serving load run")
     return p.parse_args()
 
 
@@ -229,6 +232,137 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+# ---- serving -------------------------------------------------------------------------
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
+    """Open-loop Poisson load: a producer thread submits at the arrival times,
+    a consumer waits for each ticket and releases its output. Latency is the
+    server's own submit -> result-complete time."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    n = max(1, int(rate * seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    reqs = [gen(rng) for _ in range(n)]
+    tickets = [0] * n
+    ready = threading.Semaphore(0)
+    err = []
+
+    def producer():
+        t0 = time.perf_counter()
+        try:
+            for i in range(n):
+                while True:
+                    dt = arrivals[i] - (time.perf_counter() - t0)
+                    if dt <= 0:
+                        break
+                    time.sleep(min(dt, 2e-4))
+                r = reqs[i]
+                tickets[i] = srv.submit_box(sid, r[1], r[2]) if r[0] != "level" else srv.submit_level(sid, r[1])
+                ready.release()
+        except Exception as e:  # reported below
+            err.append(repr(e))
+            ready.release()
+
+    lat = {"box": [], "slice": [], "level": []}
+    batch_sizes, out_bytes = [], 0
+    th = threading.Thread(target=producer)
+    t0 = time.perf_counter()
+    th.start()
+    for i in range(n):
+        ready.acquire()
+        if err:
+            break
+        res = srv.wait(tickets[i])
+        srv.release(tickets[i])
+        if res.status != 0:
+            err.append(f"status {res.status}")
+            break
+        lat[reqs[i][0]].append(res.latency_ms)
+        batch_sizes.append(res.batch_size)
+        out_bytes += res.nbytes
+    wall = time.perf_counter() - t0
+    th.join()
+    if err:
+        return {"error": err[0]}
+    allv = [x for v in lat.values() for x in v]
+    out = {"offered_rps": rate, "requests": n, "achieved_rps": n / wall, "p50_ms": _pct(allv, 50),
+           "p99_ms": _pct(allv, 99), "mean_batch": float(np.mean(batch_sizes)), "out_gbs": out_bytes / wall / 1e9}
+    for k, v in lat.items():
+        if v:
+            out[k] = {"n": len(v), "p50_ms": _pct(v, 50), "p99_ms": _pct(v, 99)}
+    return out
+
+
+def serving_bench(args, ctx, local):
+    """Resident-stream request serving on a 1024^3 f32 GRF (P(k) ~ k^-3, rel
+    eb 1e-3): 64^3 boxes alone under Poisson load, the mixed workload (60%
+    boxes with edges U[16,256], 30% slices, 10% progressive levels 0-3), and
+    one-request-at-a-time decode of the same 64^3 boxes through the
+    single-request API as the unbatched baseline."""
+    import torch
+
+    import stz_b200
+    from stz_b200 import fields
+
+    n = args.serve_size
+    f = fields.grf((n, n, n), 3.0, args.seed + 1000, np.float32, device=f"cuda:{local}")
+    s = ctx.compress(f, opts=stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd))
+    del f
+    torch.cuda.empty_cache()
+    K = s.info().n_levels
+    dims = (n, n, n)
+    full_bytes = n * n * n * 4
+    srv = stz_b200.Server(local, arena_bytes=max(4 << 30, 5 * full_bytes), max_batch=64)
+    t0 = time.perf_counter()
+    sid = srv.add_stream(s)
+    add_s = time.perf_counter() - t0
+
+    def box64(rng):
+        lo = [int(rng.integers(0, d - 63)) for d in dims]
+        return ("box", lo, [v + 63 for v in lo])
+
+    def mixed(rng):
+        u = rng.random()
+        if u < 0.6:
+            e = [int(rng.integers(16, 257)) for _ in range(3)]
+            lo = [int(rng.integers(0, d - x + 1)) for d, x in zip(dims, e)]
+            return ("box", lo, [a + x - 1 for a, x in zip(lo, e)])
+        if u < 0.9:
+            ax = int(rng.integers(0, 3))
+            lo, hi = [0, 0, 0], [d - 1 for d in dims]
+            lo[ax] = hi[ax] = int(rng.integers(0, dims[ax]))
+            return ("slice", lo, hi)
+        return ("level", int(rng.integers(0, 4)))
+
+    res = {"field": f"{n}^3 f32 GRF k^-3, rel eb {args.rel}", "stream_bytes": len(s), "add_stream_s": add_s,
+           "shapes": srv.stats()}
+    sec = args.serve_seconds
+    serve_load(srv, sid, dims, K, 500, 0.2, box64, 1)  # warm-up
+    res["box64"] = [serve_load(srv, sid, dims, K, r, sec, box64, 10 + i) for i, r in enumerate((2000, 10000))]
+    res["mixed"] = serve_load(srv, sid, dims, K, 1000, sec, mixed, 20)
+    srv.close()
+    # unbatched baseline: the single-request API on the resident stream
+    ctx.upload(s)
+    out = torch.empty((64, 64, 64), dtype=torch.float32, device=f"cuda:{local}")
+    rng = np.random.default_rng(30)
+    lat = []
+    for i in range(220):
+        r = box64(rng)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.decompress_box(s, r[1], r[2], out=out)
+        torch.cuda.synchronize()
+        if i >= 20:
+            lat.append(1e3 * (time.perf_counter() - t))
+    res["box64_one_at_a_time"] = {"requests": len(lat), "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
+                                  "max_rps": 1e3 / float(np.mean(lat))}
+    return res
+
+
 # ---- our arm ---------------------------------------------------------------------------
 def algorithmic_bytes(kernel: str, N: int, elem: int, K: int, raw_payload: int) -> float | None:
     """Minimum HBM bytes one launch of `kernel` must move on the N-point field."""
@@ -373,6 +507,10 @@ def main():
                              "(not timed)",
                    "compress_s": r["compress_s"], "decompress_s": r["decompress_s"]}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = serving_bench(args, ctx, local)
+
     if rank == 0:
         res = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -386,6 +524,7 @@ def main():
             "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
             "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "serving": serving,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         }
         print(json.dumps(res))

@@ -238,6 +238,80 @@ stz_status stz_quantize_noalloc_dev(stz_dtype dtype, const void* data, size_t n,
 stz_status stz_plan_box(size_t nx, size_t ny, size_t nz, int chunk_high, int chunk_low, const int64_t a[3],
                         const int64_t b[3], int64_t* out, size_t cap, size_t* n_out);
 
+/* ---- request server ------------------------------------------------------------
+ * Serves box, slice and progressive-resolution requests against streams kept
+ * resident in HBM (tables, payload, decoded base). The reference answers one
+ * query per process run (run_typed, FD5:2460-2660, and the no-marker ROI
+ * baseline of src/stz-rd.cpp); this is the long-lived form of the same path.
+ *
+ * Continuous batching: a worker thread admits queued requests while their
+ * outputs fit in the output arena (device memory reserved at create) and a
+ * batch slot is free, plans them on the host, and runs each batch as one
+ * replay of a captured CUDA graph per stream: one persistent chunk-decode
+ * kernel over the union of the batch's marker chunks, one low-level kernel
+ * over all mid-grid regions and one high-level kernel over all outputs.
+ * Requests that arrive while a batch is on the GPU join the next batch.
+ * Results do not depend on the batch a request lands in.
+ * All functions are thread-safe. */
+typedef struct stz_server stz_server;
+
+typedef struct stz_server_opts {
+    size_t arena_bytes; /* device memory for request outputs; 0 = 1 GiB */
+    int max_batch;      /* requests per batch; 0 = 64 */
+    int slots;          /* batches in flight (pinned + device batch buffers); 0 = 2 */
+    int autotune;       /* 1 = time launch shapes on each added stream and keep the fastest */
+    int threads;        /* host threads for zstd on stream upload; 0 = all cores */
+} stz_server_opts;
+
+typedef enum stz_request_kind {
+    STZ_REQ_BOX = 0,   /* lo/hi: inclusive (x, y, z) corners, as stz_decompress_box */
+    STZ_REQ_LEVEL = 1  /* level: 0 = full resolution, l = every 2^l-th point, as stz_decompress_level */
+} stz_request_kind;
+
+typedef struct stz_request {
+    int stream_id;
+    int kind;
+    int64_t lo[3], hi[3];
+    int level;
+} stz_request;
+
+typedef struct stz_result {
+    stz_status status;
+    const void* out_dev; /* result on the server's device; valid until stz_server_release */
+    size_t dims[3];      /* x, y, z extents */
+    size_t bytes;
+    double queue_ms;     /* submit -> launch of its batch */
+    double latency_ms;   /* submit -> result complete on the device */
+    uint64_t batch;      /* id of the batch that served it */
+    int batch_size;      /* requests in that batch */
+} stz_result;
+
+typedef struct stz_server_stats {
+    uint64_t submitted, completed, batches;
+    int decode_grid, roi_block, roi_grid; /* launch shapes in use (autotuned or default) */
+    size_t arena_bytes, arena_in_use;
+} stz_server_stats;
+
+void stz_server_default_opts(stz_server_opts* o);
+stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server** out);
+/* Stops the worker after the batches in flight; pending requests fail with
+ * STZ_ERR_ARG. */
+void stz_server_destroy(stz_server* srv);
+/* Parse a container stream, upload its tables and payload, decode its base
+ * (levels up to quarter resolution) and capture its batch graphs. */
+stz_status stz_server_add_stream(stz_server* srv, const void* data, size_t size, int* stream_id);
+/* Queue a request; *ticket identifies it. A request whose output can never
+ * fit in the arena returns STZ_ERR_NOMEM here. */
+stz_status stz_server_submit(stz_server* srv, const stz_request* req, uint64_t* ticket);
+/* Wait up to timeout_ms (< 0: forever) for a ticket; STZ_ERR_RANGE on
+ * timeout. The result's own status is in res->status. */
+stz_status stz_server_wait(stz_server* srv, uint64_t ticket, double timeout_ms, stz_result* res);
+/* Copy a completed result to host memory (res.bytes bytes). */
+stz_status stz_server_copy_out(stz_server* srv, uint64_t ticket, void* host);
+/* Return a completed ticket's output memory to the arena. */
+stz_status stz_server_release(stz_server* srv, uint64_t ticket);
+stz_status stz_server_stats_get(stz_server* srv, stz_server_stats* st);
+
 /* ---- inspection (tests) --------------------------------------------------- */
 /* Quant codes of one residual stream in chunk-major order (the entropy
  * coder's symbol order). level_from_coarse is 1..n_levels. */

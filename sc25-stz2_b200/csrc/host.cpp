@@ -572,6 +572,14 @@ void merge_axis(AxisRange& d, AxisRange s)
 
 }  // namespace
 
+bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], AxisRange q[3])
+{
+    const int dims[3] = {nx, ny, nz};
+    bool is_slice = false;
+    for (int ax = 0; ax < 3; ++ax) q[ax] = normalize_axis(a[ax], b[ax], dims[ax], is_slice);
+    return is_slice;
+}
+
 QueryPlan plan_query(int nx, int ny, int nz, int chunk_high, int chunk_low, const int64_t a[3], const int64_t b[3])
 {
     QueryPlan p;

@@ -129,6 +129,8 @@ struct QueryPlan {
     std::vector<BlockPlan> low;
 };
 QueryPlan plan_query(int nx, int ny, int nz, int chunk_high, int chunk_low, const int64_t a[3], const int64_t b[3]);
+// The query box alone (make_query, FD5:1637-1644); returns is_slice.
+bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], AxisRange q[3]);
 void flatten_plan(const QueryPlan& p, std::vector<int64_t>& out);
 
 }  // namespace stz

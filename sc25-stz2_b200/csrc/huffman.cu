@@ -214,22 +214,21 @@ __global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restr
 // Decode: each thread decodes one plane with a 2^kLutBits-entry table in
 // shared memory (symbol | length << 16); longer codes fall back to the
 // canonical first-code test per length.
-__global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restrict__ work,
-                                                          const uint32_t* __restrict__ chunk_ids,
-                                                          const StreamDesc* __restrict__ sd,
-                                                          const uint16_t* __restrict__ cb_sym,
-                                                          const uint8_t* __restrict__ cb_len,
-                                                          const uint32_t* __restrict__ sub_off,
-                                                          const uint64_t* __restrict__ chunk_word_off,
-                                                          const uint32_t* __restrict__ payload,
-                                                          uint16_t* __restrict__ codes)
+struct DecodeSmem {
+    uint32_t lut[1 << kLutBits];
+    uint32_t cnt[kMaxCodeLen + 1];
+    uint32_t first_code[kMaxCodeLen + 1];
+    uint32_t first_idx[kMaxCodeLen + 1];
+};
+
+// Build the decode tables of stream s (all threads of the block).
+__device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_t* __restrict__ cb_sym,
+                              const uint8_t* __restrict__ cb_len)
 {
-    __shared__ uint32_t lut[1 << kLutBits];
-    __shared__ uint32_t cnt[kMaxCodeLen + 1];
-    __shared__ uint32_t first_code[kMaxCodeLen + 1];
-    __shared__ uint32_t first_idx[kMaxCodeLen + 1];
-    const CtaWork w = work[blockIdx.x];
-    const StreamDesc s = sd[w.stream];
+    uint32_t* lut = sm.lut;
+    uint32_t* cnt = sm.cnt;
+    uint32_t* first_code = sm.first_code;
+    uint32_t* first_idx = sm.first_idx;
     for (int i = threadIdx.x; i < (1 << kLutBits); i += blockDim.x) lut[i] = 0;
     if (threadIdx.x <= kMaxCodeLen) cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -261,11 +260,19 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
         lut[j] = e;
     }
     __syncthreads();
+}
 
+// Decode plane lz of chunk c of stream s (one thread).
+__device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t c, uint32_t lz,
+                             const uint16_t* __restrict__ cb_sym, const uint32_t* __restrict__ sub_off,
+                             const uint64_t* __restrict__ chunk_word_off, const uint32_t* __restrict__ payload,
+                             uint16_t* __restrict__ codes)
+{
+    const uint32_t* lut = sm.lut;
+    const uint32_t* cnt = sm.cnt;
+    const uint32_t* first_code = sm.first_code;
+    const uint32_t* first_idx = sm.first_idx;
     const uint32_t C = s.C;
-    const uint32_t t = threadIdx.x;
-    if (t / C >= w.count) return;
-    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
     const size_t plane = (size_t)C * C;
     uint16_t* dst = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
     if (s.n_used == 1) {
@@ -336,21 +343,71 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restr
     }
 }
 
+// One CTA per work item.
+__global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restrict__ work,
+                                                          const uint32_t* __restrict__ chunk_ids,
+                                                          const StreamDesc* __restrict__ sd,
+                                                          const uint16_t* __restrict__ cb_sym,
+                                                          const uint8_t* __restrict__ cb_len,
+                                                          const uint32_t* __restrict__ sub_off,
+                                                          const uint64_t* __restrict__ chunk_word_off,
+                                                          const uint32_t* __restrict__ payload,
+                                                          uint16_t* __restrict__ codes)
+{
+    __shared__ DecodeSmem sm;
+    const CtaWork w = work[blockIdx.x];
+    const StreamDesc s = sd[w.stream];
+    decode_tables(sm, s, cb_sym, cb_len);
+    const uint32_t t = threadIdx.x;
+    if (t / s.C >= w.count) return;
+    decode_plane(sm, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off, chunk_word_off, payload, codes);
+}
+
+// Persistent variant: a fixed grid walks the work list of a batch held in
+// device memory (BatchHdr at meta), so one captured launch serves any batch.
+// The tables are rebuilt only when the stream changes between consecutive
+// items.
+__global__ void __launch_bounds__(kCoderThreads) k_decode_dyn(const uint8_t* __restrict__ meta,
+                                                              const StreamDesc* __restrict__ sd,
+                                                              const uint16_t* __restrict__ cb_sym,
+                                                              const uint8_t* __restrict__ cb_len,
+                                                              const uint32_t* __restrict__ sub_off,
+                                                              const uint64_t* __restrict__ chunk_word_off,
+                                                              const uint32_t* __restrict__ payload,
+                                                              uint16_t* __restrict__ codes)
+{
+    __shared__ DecodeSmem sm;
+    const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
+    const uint32_t n = h->n_work;
+    const CtaWork* __restrict__ work = reinterpret_cast<const CtaWork*>(meta + h->o_work);
+    const uint32_t* __restrict__ chunk_ids = reinterpret_cast<const uint32_t*>(meta + h->o_ids);
+    uint32_t cur = 0xffffffffu;
+    for (uint32_t wi = blockIdx.x; wi < n; wi += gridDim.x) {
+        const CtaWork w = work[wi];
+        const StreamDesc s = sd[w.stream];
+        if (w.stream != cur) {
+            __syncthreads();  // every thread is done with the previous tables
+            decode_tables(sm, s, cb_sym, cb_len);
+            cur = w.stream;
+        }
+        const uint32_t t = threadIdx.x;
+        if (t / s.C < w.count)
+            decode_plane(sm, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off, chunk_word_off, payload,
+                         codes);
+    }
+}
+
 // Unpredictable values: for each listed chunk, walk its codes in order and
 // move the values between the dense per-position buffer and the chunk's slot
 // of the compact list (gather on encode, scatter on decode).
 template <typename T, bool GATHER>
-__global__ void __launch_bounds__(1024) k_unpred_move(const UnpredWork* __restrict__ work,
-                                                      const StreamDesc* __restrict__ sd,
-                                                      const uint16_t* __restrict__ codes, T* __restrict__ dense,
-                                                      T* __restrict__ list)
+__device__ void unpred_move_one(const UnpredWork& uw, const StreamDesc* __restrict__ sd,
+                                const uint16_t* __restrict__ codes, T* __restrict__ dense, T* __restrict__ list,
+                                uint32_t* wc, uint64_t& carry)
 {
-    const UnpredWork uw = work[blockIdx.x];
     const StreamDesc s = sd[uw.stream];
     const size_t vol = (size_t)s.C * s.C * s.C;
     const size_t base = s.code_off + (size_t)uw.chunk * vol;
-    __shared__ uint32_t wc[32];
-    __shared__ uint64_t carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (size_t b = 0; b < vol; b += blockDim.x) {
@@ -374,6 +431,34 @@ __global__ void __launch_bounds__(1024) k_unpred_move(const UnpredWork* __restri
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
+}
+
+template <typename T, bool GATHER>
+__global__ void __launch_bounds__(1024) k_unpred_move(const UnpredWork* __restrict__ work,
+                                                      const StreamDesc* __restrict__ sd,
+                                                      const uint16_t* __restrict__ codes, T* __restrict__ dense,
+                                                      T* __restrict__ list)
+{
+    __shared__ uint32_t wc[32];
+    __shared__ uint64_t carry;
+    unpred_move_one<T, GATHER>(work[blockIdx.x], sd, codes, dense, list, wc, carry);
+}
+
+// Persistent scatter (decode side) over the unpredictable-value list of a
+// batch held in device memory (BatchHdr at meta).
+template <typename T>
+__global__ void __launch_bounds__(1024) k_unpred_scatter_dyn(const uint8_t* __restrict__ meta,
+                                                             const StreamDesc* __restrict__ sd,
+                                                             const uint16_t* __restrict__ codes,
+                                                             T* __restrict__ dense, T* __restrict__ list)
+{
+    __shared__ uint32_t wc[32];
+    __shared__ uint64_t carry;
+    const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
+    const uint32_t n = h->n_uwork;
+    const UnpredWork* __restrict__ work = reinterpret_cast<const UnpredWork*>(meta + h->o_uwork);
+    for (uint32_t wi = blockIdx.x; wi < n; wi += gridDim.x)
+        unpred_move_one<T, false>(work[wi], sd, codes, dense, list, wc, carry);
 }
 
 __global__ void k_pack_payload(const uint32_t* __restrict__ src, const uint64_t* __restrict__ src_base,
@@ -444,5 +529,24 @@ template void launch_unpred_move<float>(bool, const UnpredWork*, int, const Stre
                                         float*, cudaStream_t);
 template void launch_unpred_move<double>(bool, const UnpredWork*, int, const StreamDesc*, const uint16_t*, double*,
                                          double*, cudaStream_t);
+
+void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* cb_sym,
+                       const uint8_t* cb_len, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                       const uint32_t* payload, uint16_t* codes, cudaStream_t st)
+{
+    k_decode_dyn<<<grid, kCoderThreads, 0, st>>>(meta, sd, cb_sym, cb_len, sub_off, chunk_word_off, payload, codes);
+}
+
+template <typename T>
+void launch_unpred_scatter_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* codes, T* dense,
+                               T* list, cudaStream_t st)
+{
+    k_unpred_scatter_dyn<T><<<grid, 1024, 0, st>>>(meta, sd, codes, dense, list);
+}
+
+template void launch_unpred_scatter_dyn<float>(int, const uint8_t*, const StreamDesc*, const uint16_t*, float*, float*,
+                                               cudaStream_t);
+template void launch_unpred_scatter_dyn<double>(int, const uint8_t*, const StreamDesc*, const uint16_t*, double*,
+                                                double*, cudaStream_t);
 
 }  // namespace stz

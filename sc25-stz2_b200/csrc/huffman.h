@@ -37,4 +37,14 @@ template <typename T>
 void launch_unpred_move(bool gather, const UnpredWork* work, int nwork, const StreamDesc* sd, const uint16_t* codes,
                         T* dense, T* list, cudaStream_t st);
 
+// Persistent variants for captured graphs: `grid` CTAs walk the lists of a
+// batch held in device memory (BatchHdr at meta: n_work/o_work/o_ids,
+// n_uwork/o_uwork).
+void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* cb_sym,
+                       const uint8_t* cb_len, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                       const uint32_t* payload, uint16_t* codes, cudaStream_t st);
+template <typename T>
+void launch_unpred_scatter_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* codes, T* dense,
+                               T* list, cudaStream_t st);
+
 }  // namespace stz

@@ -1,0 +1,858 @@
+// Request server (stz_server_* in stz/stz.h): streams resident in HBM,
+// continuous batching of box / slice / progressive-level requests, and a
+// batched decode replayed from captured CUDA graphs.
+//
+// The reference answers one query per process: it plans the query
+// (FD5:1578-1839), entropy-decodes the planned marker chunks
+// (SZ_decompress_nopred_marked_chunks, FD5:1841-1911), rebuilds the
+// half-resolution reference regions from the decoded base (FD5:2507-2538) and
+// then the box (FD5:2573-2605). Here the same steps run for a whole batch of
+// requests at once:
+//   host   : plan every request, take the union of their marker chunks
+//            (each chunk decoded once per batch), pack one batch record;
+//   device : one H2D copy of the record, then one graph replay per stream:
+//            k_decode_dyn (all chunks) -> k_unpred_scatter_dyn ->
+//            k_roi_mid_dyn (all mid regions) -> k_roi_req_dyn (all outputs).
+// Progressive levels >= 2 are strided samples of the resident decoded base
+// (the decoded grid of level l+1 is the even-parity sub-grid of level l);
+// levels 1 and 0 add full level decodes after the graph.
+//
+// Admission: a request is taken from the queue when its output fits in the
+// output arena and a batch slot (pinned + device record buffers) is free;
+// requests that arrive while batches run join the next batch.
+#include <cuda_runtime.h>
+
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "levels.h"
+#include "roi.h"
+#include "runtime.h"
+
+namespace stz {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+constexpr int kMaxSlots = 8;
+constexpr int kMaxRegionsPerBox = 8;  // 7 high reference regions + the sub-block-0 region
+
+double ms_between(Clock::time_point a, Clock::time_point b)
+{
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// First-fit allocator over [0, cap) in 256-byte units.
+class Arena {
+public:
+    void reset(size_t cap)
+    {
+        free_.clear();
+        cap_ = cap & ~(size_t)255;
+        used_ = 0;
+        if (cap_) free_[0] = cap_;
+    }
+    bool alloc(size_t bytes, size_t& off)
+    {
+        bytes = align256(std::max<size_t>(bytes, 1));
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            off = it->first;
+            const size_t rest = it->second - bytes;
+            free_.erase(it);
+            if (rest) free_[off + bytes] = rest;
+            used_ += bytes;
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes)
+    {
+        bytes = align256(std::max<size_t>(bytes, 1));
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    size_t capacity() const { return cap_; }
+    size_t used() const { return used_; }
+    bool fits_ever(size_t bytes) const { return align256(std::max<size_t>(bytes, 1)) <= cap_; }
+
+private:
+    std::map<size_t, size_t> free_;
+    size_t cap_ = 0, used_ = 0;
+};
+
+struct LaunchShape {
+    int decode_grid = 148 * 4;
+    int unpred_grid = 148 * 2;
+    int roi_block = 256;
+    int roi_grid = 148 * 8;
+};
+
+struct SrvStream {
+    int id = 0;
+    std::unique_ptr<stz_stream> s;
+    Prepared* p = nullptr;
+    int K = 0, dtype = 0, predictor = 0;
+    size_t elem = 4;
+    LevelGeom low, high;
+    QuantParams qlow, qhigh;
+    uint32_t low_s0 = 0, high_s0 = 0;  // index of block 0 of the low / high level among the streams
+    DevBuf codes, unpred, mid;
+    std::vector<uint32_t> stamp;  // per chunk of the 14 low/high streams: last batch that listed it
+    uint64_t stamp_off[15] = {};
+    uint32_t epoch = 0;
+    size_t meta_cap = 0;
+    DevBuf meta[kMaxSlots];
+    cudaGraphExec_t graph[kMaxSlots] = {};
+    LaunchShape shape;
+    ~SrvStream()
+    {
+        for (auto g : graph)
+            if (g) cudaGraphExecDestroy(g);
+    }
+    const StreamDesc& sd(uint32_t i) const { return p->sd[i]; }
+    const uint16_t* low_codes() const { return codes.as<uint16_t>() + sd(low_s0).code_off; }
+    const uint16_t* high_codes() const { return codes.as<uint16_t>() + sd(high_s0).code_off; }
+    template <typename T>
+    const T* low_unpred() const
+    {
+        return p->total_unpred ? unpred.as<T>() + sd(low_s0).code_off : nullptr;
+    }
+    template <typename T>
+    const T* high_unpred() const
+    {
+        return p->total_unpred ? unpred.as<T>() + sd(high_s0).code_off : nullptr;
+    }
+};
+
+struct Ticket {
+    stz_request req{};
+    SrvStream* ss = nullptr;
+    int state = 0;  // 0 queued, 1 in a batch, 2 done
+    stz_status status = STZ_OK;
+    std::string error;
+    size_t off = 0, bytes = 0;
+    size_t dims[3] = {0, 0, 0};
+    Clock::time_point t_submit, t_launch, t_done;
+    uint64_t batch = 0;
+    int batch_size = 0;
+};
+
+// A level request's full decodes, run after the batch graph.
+struct LevelJob {
+    SrvStream* ss;
+    int level;  // 0 or 1
+    void* out;
+};
+
+// Host-side record of one batch for one stream.
+struct Build {
+    std::vector<uint32_t> lists[14];
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    std::vector<UnpredWork> uw;
+    std::vector<RoiBox> mid;
+    std::vector<ReqDesc> req;
+    uint64_t mid_total = 0, req_total = 0;
+    std::vector<LevelJob> jobs;
+};
+
+struct BatchDone;
+
+}  // namespace
+}  // namespace stz
+
+using namespace stz;
+
+struct stz_server {
+    stz_context* ctx = nullptr;
+    stz_server_opts opts{};
+    DevBuf arena_buf;
+    Arena arena;
+    std::mutex mu;  // queue, tickets, slots, arena, stats
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint64_t> queue;
+    std::unordered_map<uint64_t, Ticket> tickets;
+    uint64_t next_ticket = 1;
+    std::vector<std::unique_ptr<SrvStream>> streams;
+    std::vector<bool> slot_busy;
+    PinBuf hmeta[kMaxSlots];
+    std::mutex exec_mu;  // GPU submission (worker batches vs stream upload / capture)
+    std::thread worker;
+    bool stop = false;
+    uint64_t submitted = 0, completed = 0, batches = 0;
+    LaunchShape last_shape;
+};
+
+namespace stz {
+namespace {
+
+struct BatchDone {
+    stz_server* S;
+    int slot;
+    std::vector<uint64_t> ids;
+};
+
+void CUDART_CB batch_done(void* arg)
+{
+    BatchDone* d = static_cast<BatchDone*>(arg);
+    stz_server* S = d->S;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        const auto now = Clock::now();
+        for (uint64_t id : d->ids) {
+            auto it = S->tickets.find(id);
+            if (it == S->tickets.end()) continue;
+            it->second.state = 2;
+            it->second.t_done = now;
+        }
+        S->slot_busy[d->slot] = false;
+        S->completed += d->ids.size();
+    }
+    S->cv_done.notify_all();
+    S->cv_work.notify_all();
+    delete d;
+}
+
+uint32_t chunk_count(const SrvStream& ss, int j) { return ss.sd(j < 7 ? ss.low_s0 + j : ss.high_s0 + j - 7).nchunks; }
+
+void list_chunk(SrvStream& ss, Build& b, int j, uint32_t c)
+{
+    uint32_t& st = ss.stamp[ss.stamp_off[j] + c];
+    if (st == ss.epoch) return;
+    st = ss.epoch;
+    b.lists[j].push_back(c);
+}
+
+void list_all(SrvStream& ss, Build& b, int j0, int j1)
+{
+    for (int j = j0; j < j1; ++j) {
+        const uint32_t n = chunk_count(ss, j);
+        for (uint32_t c = 0; c < n; ++c) list_chunk(ss, b, j, c);
+    }
+}
+
+// Plan one request into the batch record.
+void plan_request(SrvStream& ss, Build& b, const Ticket& t, void* out)
+{
+    const FileHeader& h = ss.s->dir.h;
+    const stz_request& r = t.req;
+    if (r.kind == STZ_REQ_BOX) {
+        const QueryPlan plan = plan_query(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low, r.lo, r.hi);
+        for (const BlockPlan& bp : plan.low)
+            for (int64_t c : bp.chunks) list_chunk(ss, b, bp.block, (uint32_t)c);
+        for (const BlockPlan& bp : plan.high)
+            for (int64_t c : bp.chunks) list_chunk(ss, b, 7 + bp.block, (uint32_t)c);
+        for (const auto& rg : plan.regions) {
+            if (rg[0].empty() || rg[1].empty() || rg[2].empty()) continue;
+            b.mid.push_back({rg[0].b, rg[0].e, rg[1].b, rg[1].e, rg[2].b, rg[2].e, b.mid_total});
+            b.mid_total += (uint64_t)(rg[0].e - rg[0].b + 1) * (rg[1].e - rg[1].b + 1) * (rg[2].e - rg[2].b + 1);
+        }
+        ReqDesc d{};
+        d.box = {plan.q[0].b, plan.q[0].e, plan.q[1].b, plan.q[1].e, plan.q[2].b, plan.q[2].e, 0};
+        d.start = b.req_total;
+        d.out = (uint64_t)(uintptr_t)out;
+        d.kind = kReqBox;
+        b.req.push_back(d);
+        b.req_total += (uint64_t)t.dims[0] * t.dims[1] * t.dims[2];
+        return;
+    }
+    if (r.level >= 2) {
+        ReqDesc d{};
+        d.box = {0, (int)t.dims[0] - 1, 0, (int)t.dims[1] - 1, 0, (int)t.dims[2] - 1, 0};
+        d.start = b.req_total;
+        d.out = (uint64_t)(uintptr_t)out;
+        d.kind = kReqSample;
+        d.shift = r.level - 2;
+        b.req.push_back(d);
+        b.req_total += (uint64_t)t.dims[0] * t.dims[1] * t.dims[2];
+        return;
+    }
+    list_all(ss, b, 0, 7);
+    if (r.level == 0) list_all(ss, b, 7, 14);
+    b.jobs.push_back({&ss, r.level, out});
+}
+
+// Work lists and the packed record (header + arrays) in host memory.
+size_t pack(SrvStream& ss, Build& b, uint8_t* dst)
+{
+    for (int j = 0; j < 14; ++j) {
+        if (b.lists[j].empty()) continue;
+        const uint32_t si = j < 7 ? ss.low_s0 + j : ss.high_s0 + j - 7;
+        std::sort(b.lists[j].begin(), b.lists[j].end());
+        add_work(b.work, b.ids, si, b.lists[j].data(), b.lists[j].size(), (int)ss.sd(si).C);
+        add_unpred_work(*ss.p, si, b.lists[j].data(), b.lists[j].size(), b.uw);
+    }
+    BatchHdr h{};
+    h.n_work = (uint32_t)b.work.size();
+    h.n_uwork = (uint32_t)b.uw.size();
+    h.n_mid = (uint32_t)b.mid.size();
+    h.n_req = (uint32_t)b.req.size();
+    h.mid_total = b.mid_total;
+    h.req_total = b.req_total;
+    size_t off = align16(sizeof(BatchHdr));
+    h.o_work = (uint32_t)off;
+    off = align16(off + b.work.size() * sizeof(CtaWork));
+    h.o_ids = (uint32_t)off;
+    off = align16(off + b.ids.size() * 4);
+    h.o_uwork = (uint32_t)off;
+    off = align16(off + b.uw.size() * sizeof(UnpredWork));
+    h.o_mid = (uint32_t)off;
+    off = align16(off + b.mid.size() * sizeof(RoiBox));
+    h.o_req = (uint32_t)off;
+    off = align16(off + b.req.size() * sizeof(ReqDesc));
+    if (off > ss.meta_cap) return 0;
+    std::memcpy(dst, &h, sizeof h);
+    if (!b.work.empty()) std::memcpy(dst + h.o_work, b.work.data(), b.work.size() * sizeof(CtaWork));
+    if (!b.ids.empty()) std::memcpy(dst + h.o_ids, b.ids.data(), b.ids.size() * 4);
+    if (!b.uw.empty()) std::memcpy(dst + h.o_uwork, b.uw.data(), b.uw.size() * sizeof(UnpredWork));
+    if (!b.mid.empty()) std::memcpy(dst + h.o_mid, b.mid.data(), b.mid.size() * sizeof(RoiBox));
+    if (!b.req.empty()) std::memcpy(dst + h.o_req, b.req.data(), b.req.size() * sizeof(ReqDesc));
+    return off;
+}
+
+// The batch kernels of one stream on the context's stream (captured into the
+// slot graphs, and run directly by the autotuner).
+template <typename T>
+void enqueue_kernels(const SrvStream& ss, const LaunchShape& sh, const uint8_t* meta, cudaStream_t st)
+{
+    const Prepared& p = *ss.p;
+    uint16_t* codes = ss.codes.as<uint16_t>();
+    launch_decode_dyn(sh.decode_grid, meta, p.d_sd, p.d_sym, p.d_len, p.d_sub, p.d_choff, p.d_payload, codes, st);
+    if (p.total_unpred)
+        launch_unpred_scatter_dyn<T>(sh.unpred_grid, meta, p.d_sd, codes, ss.unpred.as<T>(), (T*)p.d_ulist, st);
+    launch_roi_mid_dyn<T>(sh.roi_grid, sh.roi_block, meta, p.base->as<T>(), ss.low, ss.qlow, ss.predictor,
+                          ss.low_codes(), ss.low_unpred<T>(), ss.mid.as<T>(), st);
+    launch_roi_req_dyn<T>(sh.roi_grid, sh.roi_block, meta, ss.mid.as<T>(), p.base->as<T>(), ss.low, ss.high, ss.qhigh,
+                          ss.predictor, ss.high_codes(), ss.high_unpred<T>(), st);
+}
+
+template <typename T>
+void enqueue_level_job(const SrvStream& ss, const LevelJob& j, cudaStream_t st)
+{
+    LevelDecodeArgs<T> a;
+    a.coarse = ss.p->base->as<T>();
+    a.geo = ss.low;
+    a.predictor = ss.predictor;
+    a.qp = ss.qlow;
+    a.codes = ss.low_codes();
+    a.unpred_dense = ss.low_unpred<T>();
+    a.out = j.level == 1 ? (T*)j.out : ss.mid.as<T>();
+    launch_level_decode<T>(a, st);
+    if (j.level == 1) return;
+    a.coarse = ss.mid.as<T>();
+    a.geo = ss.high;
+    a.qp = ss.qhigh;
+    a.codes = ss.high_codes();
+    a.unpred_dense = ss.high_unpred<T>();
+    a.out = (T*)j.out;
+    launch_level_decode<T>(a, st);
+}
+
+stz_status capture_graphs(stz_server* S, SrvStream& ss)
+{
+    cudaStream_t st = S->ctx->st;
+    for (int k = 0; k < S->opts.slots; ++k) {
+        if (ss.graph[k]) {
+            cudaGraphExecDestroy(ss.graph[k]);
+            ss.graph[k] = nullptr;
+        }
+        STZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        if (ss.dtype == 1) enqueue_kernels<double>(ss, ss.shape, ss.meta[k].as<uint8_t>(), st);
+        else enqueue_kernels<float>(ss, ss.shape, ss.meta[k].as<uint8_t>(), st);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            STZ_FAIL(STZ_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t e2 = cudaGraphInstantiate(&ss.graph[k], g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) STZ_FAIL(STZ_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+    }
+    return STZ_OK;
+}
+
+// Time the batch kernels on a synthetic batch of 16 boxes (edge 64, clipped
+// to the field) for each candidate shape and keep the fastest.
+stz_status autotune(stz_server* S, SrvStream& ss)
+{
+    cudaStream_t st = S->ctx->st;
+    const FileHeader& h = ss.s->dir.h;
+    Build b;
+    ++ss.epoch;
+    std::vector<Ticket> tk(16);
+    uint64_t seed = 0x9e3779b97f4a7c15ull;
+    auto rnd = [&](int n) {
+        seed = seed * 6364136223846793005ull + 1442695040888963407ull;
+        return n > 0 ? (int)((seed >> 33) % (uint64_t)n) : 0;
+    };
+    size_t out_elems = 0;
+    const int dims[3] = {h.nx, h.ny, h.nz};
+    for (auto& t : tk) {
+        t.req.kind = STZ_REQ_BOX;
+        for (int a = 0; a < 3; ++a) {
+            const int e = std::min(64, dims[a]);
+            t.req.lo[a] = rnd(dims[a] - e + 1);
+            t.req.hi[a] = t.req.lo[a] + e - 1;
+            t.dims[a] = (size_t)e;
+        }
+        out_elems += t.dims[0] * t.dims[1] * t.dims[2];
+    }
+    DevBuf out;
+    STZ_CUDA(out.ensure(out_elems * ss.elem));
+    size_t o = 0;
+    for (auto& t : tk) {
+        plan_request(ss, b, t, out.as<uint8_t>() + o * ss.elem);
+        o += t.dims[0] * t.dims[1] * t.dims[2];
+    }
+    STZ_CUDA(S->hmeta[0].ensure(ss.meta_cap));
+    const size_t bytes = pack(ss, b, S->hmeta[0].as<uint8_t>());
+    if (!bytes) STZ_FAIL(STZ_ERR_RANGE, "tuning batch exceeds the batch record");
+    STZ_CUDA(cudaMemcpyAsync(ss.meta[0].p, S->hmeta[0].p, bytes, cudaMemcpyHostToDevice, st));
+    cudaEvent_t e0, e1;
+    STZ_CUDA(cudaEventCreate(&e0));
+    STZ_CUDA(cudaEventCreate(&e1));
+    auto time_shape = [&](const LaunchShape& sh) -> float {
+        float best = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(e0, st);
+            if (ss.dtype == 1) enqueue_kernels<double>(ss, sh, ss.meta[0].as<uint8_t>(), st);
+            else enqueue_kernels<float>(ss, sh, ss.meta[0].as<uint8_t>(), st);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep) best = std::min(best, ms);  // first run warms up
+        }
+        return best;
+    };
+    LaunchShape best = ss.shape;
+    float tbest = time_shape(best);
+    for (int dg : {148, 148 * 2, 148 * 4, 148 * 8}) {
+        LaunchShape c = best;
+        c.decode_grid = dg;
+        const float t = time_shape(c);
+        if (t < tbest) tbest = t, best = c;
+    }
+    for (int blk : {128, 256, 512})
+        for (int per_sm : {2, 4, 8, 16}) {
+            if (blk * per_sm > 2048) continue;
+            LaunchShape c = best;
+            c.roi_block = blk;
+            c.roi_grid = 148 * per_sm;
+            const float t = time_shape(c);
+            if (t < tbest) tbest = t, best = c;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    STZ_CUDA(cudaGetLastError());
+    STZ_CUDA(cudaStreamSynchronize(st));
+    ss.shape = best;
+    return STZ_OK;
+}
+
+template <typename T>
+cudaError_t enqueue_batch_stream(SrvStream& ss, int slot, const std::vector<LevelJob>& jobs, cudaStream_t st)
+{
+    const cudaError_t e = cudaGraphLaunch(ss.graph[slot], st);
+    if (e != cudaSuccess) return e;
+    for (const LevelJob& j : jobs) enqueue_level_job<T>(ss, j, st);
+    return cudaGetLastError();
+}
+
+// Plan, pack and enqueue one batch (worker thread, exec_mu held).
+stz_status launch_batch(stz_server* S, int slot, uint64_t bid, const std::vector<uint64_t>& ids)
+{
+    cudaStream_t st = S->ctx->st;
+    // group by stream, keep arrival order inside a group
+    std::vector<SrvStream*> order;
+    std::unordered_map<SrvStream*, std::vector<Ticket*>> groups;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        const auto now = Clock::now();
+        for (uint64_t id : ids) {
+            Ticket& t = S->tickets[id];
+            t.t_launch = now;
+            t.batch = bid;
+            t.batch_size = (int)ids.size();
+            if (!groups.count(t.ss)) order.push_back(t.ss);
+            groups[t.ss].push_back(&t);
+        }
+    }
+    uint8_t* arena = S->arena_buf.as<uint8_t>();
+    size_t hoff = 0;
+    // every group's record goes to its own region of the slot's pinned buffer
+    size_t need = 0;
+    for (SrvStream* ss : order) need += align256(ss->meta_cap);
+    STZ_CUDA(S->hmeta[slot].ensure(need));
+    for (SrvStream* ss : order) {
+        Build b;
+        ++ss->epoch;
+        if (ss->epoch == 0) {  // wrapped: clear the stamps
+            std::fill(ss->stamp.begin(), ss->stamp.end(), 0u);
+            ss->epoch = 1;
+        }
+        for (Ticket* t : groups[ss]) plan_request(*ss, b, *t, arena + t->off);
+        uint8_t* hm = S->hmeta[slot].as<uint8_t>() + hoff;
+        const size_t bytes = pack(*ss, b, hm);
+        if (!bytes) STZ_FAIL(STZ_ERR_RANGE, "batch record exceeds its buffer");
+        STZ_CUDA(cudaMemcpyAsync(ss->meta[slot].p, hm, bytes, cudaMemcpyHostToDevice, st));
+        if (ss->dtype == 1) STZ_CUDA((enqueue_batch_stream<double>(*ss, slot, b.jobs, st)));
+        else STZ_CUDA((enqueue_batch_stream<float>(*ss, slot, b.jobs, st)));
+        hoff += align256(ss->meta_cap);
+    }
+    auto* d = new BatchDone{S, slot, ids};
+    const cudaError_t e = cudaLaunchHostFunc(st, batch_done, d);
+    if (e != cudaSuccess) {
+        delete d;
+        STZ_FAIL(STZ_ERR_CUDA, std::string("cudaLaunchHostFunc: ") + cudaGetErrorString(e));
+    }
+    return STZ_OK;
+}
+
+void worker_main(stz_server* S)
+{
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        int slot = -1;
+        auto ready = [&]() {
+            if (S->stop) return true;
+            if (S->queue.empty()) return false;
+            slot = -1;
+            for (int k = 0; k < S->opts.slots; ++k)
+                if (!S->slot_busy[k]) {
+                    slot = k;
+                    break;
+                }
+            if (slot < 0) return false;
+            size_t off;
+            const Ticket& t = S->tickets[S->queue.front()];
+            if (!S->arena.alloc(t.bytes, off)) return false;
+            S->arena.release(off, t.bytes);
+            return true;
+        };
+        S->cv_work.wait(lk, ready);
+        if (S->stop) break;
+        // admit in arrival order while outputs fit
+        std::vector<uint64_t> ids;
+        while (!S->queue.empty() && (int)ids.size() < S->opts.max_batch) {
+            Ticket& t = S->tickets[S->queue.front()];
+            if (!S->arena.alloc(t.bytes, t.off)) break;
+            t.state = 1;
+            ids.push_back(S->queue.front());
+            S->queue.pop_front();
+        }
+        if (ids.empty()) continue;
+        S->slot_busy[slot] = true;
+        const uint64_t bid = ++S->batches;
+        lk.unlock();
+        stz_status st;
+        std::string err;
+        {
+            std::lock_guard<std::mutex> ex(S->exec_mu);
+            st = launch_batch(S, slot, bid, ids);
+            if (st != STZ_OK) err = stz_last_error();
+        }
+        lk.lock();
+        if (st != STZ_OK) {
+            // nothing of a failed batch is pending its callback: fail its
+            // requests and give back the slot (after the stream drains)
+            lk.unlock();
+            cudaStreamSynchronize(S->ctx->st);
+            lk.lock();
+            const auto now = Clock::now();
+            for (uint64_t id : ids) {
+                Ticket& t = S->tickets[id];
+                S->arena.release(t.off, t.bytes);  // a failed ticket holds no output
+                t.state = 2;
+                t.status = st;
+                t.error = err;
+                t.t_done = now;
+            }
+            S->slot_busy[slot] = false;
+            S->completed += ids.size();
+            S->cv_done.notify_all();
+        }
+    }
+}
+
+stz_status enter_server(stz_server* S)
+{
+    if (!S) STZ_FAIL(STZ_ERR_ARG, "server is null");
+    STZ_TRY(enter(S->ctx));
+    return STZ_OK;
+}
+
+template <typename T>
+stz_status decode_base(stz_context* ctx, SrvStream& ss)
+{
+    Prepared& p = *ss.p;
+    STZ_CUDA(p.base->ensure(ss.low.n * sizeof(T)));
+    STZ_TRY(decode_levels<T>(ctx, ss.s.get(), p, ss.K - 2, p.base->as<T>()));
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    p.base_valid = true;
+    return STZ_OK;
+}
+
+}  // namespace
+}  // namespace stz
+
+extern "C" {
+
+void stz_server_default_opts(stz_server_opts* o)
+{
+    if (!o) return;
+    o->arena_bytes = (size_t)1 << 30;
+    o->max_batch = 64;
+    o->slots = 2;
+    o->autotune = 1;
+    o->threads = 0;
+}
+
+stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server** out)
+{
+    if (!out) STZ_FAIL(STZ_ERR_ARG, "out is null");
+    *out = nullptr;
+    stz_server_opts o;
+    stz_server_default_opts(&o);
+    if (opts) {
+        if (opts->arena_bytes) o.arena_bytes = opts->arena_bytes;
+        if (opts->max_batch > 0) o.max_batch = opts->max_batch;
+        if (opts->slots > 0) o.slots = std::min(opts->slots, kMaxSlots);
+        o.autotune = opts->autotune;
+        o.threads = opts->threads;
+    }
+    std::unique_ptr<stz_server> S(new (std::nothrow) stz_server());
+    if (!S) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
+    S->opts = o;
+    STZ_TRY(stz_context_create(device, &S->ctx));
+    if (o.threads > 0) S->ctx->pool.reset(new ThreadPool(o.threads));
+    const cudaError_t e = S->arena_buf.ensure(o.arena_bytes);
+    if (e != cudaSuccess) {
+        stz_context_destroy(S->ctx);
+        STZ_FAIL(STZ_ERR_NOMEM, "output arena allocation failed");
+    }
+    S->arena.reset(o.arena_bytes);
+    S->slot_busy.assign(o.slots, false);
+    stz_server* raw = S.release();
+    raw->worker = std::thread(worker_main, raw);
+    *out = raw;
+    return STZ_OK;
+}
+
+void stz_server_destroy(stz_server* S)
+{
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    if (S->worker.joinable()) S->worker.join();
+    cudaSetDevice(S->ctx->device);
+    cudaStreamSynchronize(S->ctx->st);  // batches in flight and their callbacks
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (uint64_t id : S->queue) {
+            Ticket& t = S->tickets[id];
+            t.state = 2;
+            t.status = STZ_ERR_ARG;
+            t.error = "server stopped";
+        }
+        S->queue.clear();
+    }
+    S->cv_done.notify_all();
+    S->streams.clear();
+    stz_context* ctx = S->ctx;
+    delete S;
+    stz_context_destroy(ctx);
+}
+
+stz_status stz_server_add_stream(stz_server* S, const void* data, size_t size, int* stream_id)
+{
+    STZ_TRY(enter_server(S));
+    if (!data || !stream_id) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    std::lock_guard<std::mutex> ex(S->exec_mu);
+    STZ_CUDA(cudaStreamSynchronize(S->ctx->st));
+    std::unique_ptr<SrvStream> ss(new SrvStream());
+    stz_stream* parsed = nullptr;
+    STZ_TRY(stz_stream_parse(S->ctx, data, size, &parsed));
+    ss->s.reset(parsed);
+    const ParsedStream& ps = ss->s->dir;
+    const FileHeader& h = ps.h;
+    if (h.K < 2) STZ_FAIL(STZ_ERR_DIMS, "stream has fewer than two levels");
+    ss->K = h.K;
+    ss->dtype = h.dtype;
+    ss->elem = h.elem();
+    ss->predictor = h.predictor;
+    ss->low = level_geom(ps, h.K - 1);
+    ss->high = level_geom(ps, h.K);
+    ss->qlow = qparams(ps, h.K - 1);
+    ss->qhigh = qparams(ps, h.K);
+    ss->low_s0 = (uint32_t)(h.K - 2) * 7;
+    ss->high_s0 = (uint32_t)(h.K - 1) * 7;
+    ss->s->resident.reset(new Prepared());
+    ss->p = ss->s->resident.get();
+    STZ_TRY(prepare(S->ctx, ss->s.get(), h.K, *ss->p));
+    if (h.dtype == 1) STZ_TRY(decode_base<double>(S->ctx, *ss));
+    else STZ_TRY(decode_base<float>(S->ctx, *ss));
+    const Prepared& p = *ss->p;
+    STZ_CUDA(ss->codes.ensure(p.total_codes * 2));
+    if (p.total_unpred) STZ_CUDA(ss->unpred.ensure(p.total_codes * ss->elem));
+    STZ_CUDA(ss->mid.ensure(8 * ss->low.n * ss->elem));
+    // chunk stamps and the batch record capacity
+    uint64_t nch = 0;
+    for (int j = 0; j < 14; ++j) {
+        ss->stamp_off[j] = nch;
+        nch += chunk_count(*ss, j);
+    }
+    ss->stamp_off[14] = nch;
+    ss->stamp.assign(nch, 0u);
+    ss->meta_cap = align16(sizeof(BatchHdr)) + align16(nch * sizeof(CtaWork)) + align16(nch * 4) +
+                   align16(nch * sizeof(UnpredWork)) +
+                   align16((size_t)S->opts.max_batch * kMaxRegionsPerBox * sizeof(RoiBox)) +
+                   align16((size_t)S->opts.max_batch * sizeof(ReqDesc)) + 256;
+    for (int k = 0; k < S->opts.slots; ++k) STZ_CUDA(ss->meta[k].ensure(ss->meta_cap));
+    if (S->opts.autotune) STZ_TRY(autotune(S, *ss));
+    STZ_TRY(capture_graphs(S, *ss));
+    STZ_CUDA(cudaStreamSynchronize(S->ctx->st));
+    std::lock_guard<std::mutex> lk(S->mu);
+    ss->id = (int)S->streams.size();
+    S->last_shape = ss->shape;
+    *stream_id = ss->id;
+    S->streams.push_back(std::move(ss));
+    return STZ_OK;
+}
+
+stz_status stz_server_submit(stz_server* S, const stz_request* r, uint64_t* ticket)
+{
+    if (!S || !r || !ticket) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    Ticket t;
+    t.req = *r;
+    t.t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stop) STZ_FAIL(STZ_ERR_ARG, "server stopped");
+        if (r->stream_id < 0 || r->stream_id >= (int)S->streams.size()) STZ_FAIL(STZ_ERR_ARG, "no such stream");
+        t.ss = S->streams[r->stream_id].get();
+    }
+    const FileHeader& h = t.ss->s->dir.h;
+    if (r->kind == STZ_REQ_BOX) {
+        AxisRange q[3];
+        query_box(h.nx, h.ny, h.nz, r->lo, r->hi, q);
+        for (int a = 0; a < 3; ++a) t.dims[a] = (size_t)(q[a].e - q[a].b + 1);
+    } else if (r->kind == STZ_REQ_LEVEL) {
+        if (r->level < 0 || r->level > h.K) STZ_FAIL(STZ_ERR_RANGE, "level out of range");
+        t.dims[0] = (size_t)h.nx >> r->level;
+        t.dims[1] = (size_t)h.ny >> r->level;
+        t.dims[2] = (size_t)h.nz >> r->level;
+    } else {
+        STZ_FAIL(STZ_ERR_ARG, "unknown request kind");
+    }
+    t.bytes = t.dims[0] * t.dims[1] * t.dims[2] * h.elem();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (!S->arena.fits_ever(t.bytes)) STZ_FAIL(STZ_ERR_NOMEM, "request output exceeds the output arena");
+        const uint64_t id = S->next_ticket++;
+        S->tickets.emplace(id, std::move(t));
+        S->queue.push_back(id);
+        ++S->submitted;
+        *ticket = id;
+    }
+    S->cv_work.notify_one();
+    return STZ_OK;
+}
+
+stz_status stz_server_wait(stz_server* S, uint64_t ticket, double timeout_ms, stz_result* res)
+{
+    if (!S || !res) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->tickets.find(ticket);
+    if (it == S->tickets.end()) STZ_FAIL(STZ_ERR_ARG, "unknown ticket");
+    Ticket& t = it->second;
+    auto done = [&]() { return t.state == 2; };
+    if (timeout_ms < 0) S->cv_done.wait(lk, done);
+    else if (!S->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
+        STZ_FAIL(STZ_ERR_RANGE, "timed out");
+    res->status = t.status;
+    res->out_dev = t.status == STZ_OK ? S->arena_buf.as<uint8_t>() + t.off : nullptr;
+    for (int a = 0; a < 3; ++a) res->dims[a] = t.dims[a];
+    res->bytes = t.bytes;
+    res->queue_ms = ms_between(t.t_submit, t.t_launch);
+    res->latency_ms = ms_between(t.t_submit, t.t_done);
+    res->batch = t.batch;
+    res->batch_size = t.batch_size;
+    if (t.status != STZ_OK) set_last_error(t.error);
+    return STZ_OK;
+}
+
+stz_status stz_server_copy_out(stz_server* S, uint64_t ticket, void* host)
+{
+    STZ_TRY(enter_server(S));
+    if (!host) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    const void* src = nullptr;
+    size_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        auto it = S->tickets.find(ticket);
+        if (it == S->tickets.end()) STZ_FAIL(STZ_ERR_ARG, "unknown ticket");
+        if (it->second.state != 2) STZ_FAIL(STZ_ERR_ARG, "request not complete");
+        if (it->second.status != STZ_OK) STZ_FAIL(it->second.status, it->second.error);
+        src = S->arena_buf.as<uint8_t>() + it->second.off;
+        bytes = it->second.bytes;
+    }
+    STZ_CUDA(cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
+    return STZ_OK;
+}
+
+stz_status stz_server_release(stz_server* S, uint64_t ticket)
+{
+    if (!S) STZ_FAIL(STZ_ERR_ARG, "server is null");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        auto it = S->tickets.find(ticket);
+        if (it == S->tickets.end()) STZ_FAIL(STZ_ERR_ARG, "unknown ticket");
+        if (it->second.state != 2) STZ_FAIL(STZ_ERR_ARG, "request not complete");
+        if (it->second.status == STZ_OK) S->arena.release(it->second.off, it->second.bytes);
+        S->tickets.erase(it);
+    }
+    S->cv_work.notify_one();
+    return STZ_OK;
+}
+
+stz_status stz_server_stats_get(stz_server* S, stz_server_stats* st)
+{
+    if (!S || !st) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    std::lock_guard<std::mutex> lk(S->mu);
+    st->submitted = S->submitted;
+    st->completed = S->completed;
+    st->batches = S->batches;
+    st->decode_grid = S->last_shape.decode_grid;
+    st->roi_block = S->last_shape.roi_block;
+    st->roi_grid = S->last_shape.roi_grid;
+    st->arena_bytes = S->arena.capacity();
+    st->arena_in_use = S->arena.used();
+    return STZ_OK;
+}
+
+}  // extern "C"

@@ -70,4 +70,13 @@ struct CtaWork {
     uint32_t pad;
 };
 
+// Header of a request batch in device memory (request server). The arrays
+// (CtaWork, chunk ids, UnpredWork, RoiBox mid regions, ReqDesc outputs)
+// follow at the given byte offsets from the header's start.
+struct BatchHdr {
+    uint32_t n_work, n_uwork, n_mid, n_req;
+    uint64_t mid_total, req_total;  // points of all mid regions / all outputs
+    uint32_t o_work, o_ids, o_uwork, o_mid, o_req, pad;
+};
+
 }  // namespace stz

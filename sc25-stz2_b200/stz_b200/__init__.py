@@ -101,8 +101,41 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_profile_count.argtypes = [vp, C.POINTER(C.c_int)]
     lib.stz_profile_entry.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                       C.POINTER(C.c_uint64)]
+    lib.stz_server_default_opts.argtypes = [C.POINTER(ServerOpts)]
+    lib.stz_server_default_opts.restype = None
+    lib.stz_server_create.argtypes = [C.c_int, C.POINTER(ServerOpts), C.POINTER(vp)]
+    lib.stz_server_destroy.argtypes = [vp]
+    lib.stz_server_destroy.restype = None
+    lib.stz_server_add_stream.argtypes = [vp, vp, sz, C.POINTER(C.c_int)]
+    lib.stz_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
+    lib.stz_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(Result)]
+    lib.stz_server_copy_out.argtypes = [vp, C.c_uint64, vp]
+    lib.stz_server_release.argtypes = [vp, C.c_uint64]
+    lib.stz_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
     _lib = lib
     return lib
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("arena_bytes", C.c_size_t), ("max_batch", C.c_int), ("slots", C.c_int), ("autotune", C.c_int),
+                ("threads", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("stream_id", C.c_int), ("kind", C.c_int), ("lo", C.c_int64 * 3), ("hi", C.c_int64 * 3),
+                ("level", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("out_dev", C.c_void_p), ("dims", C.c_size_t * 3), ("bytes", C.c_size_t),
+                ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("batch", C.c_uint64),
+                ("batch_size", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("decode_grid", C.c_int), ("roi_block", C.c_int), ("roi_grid", C.c_int),
+                ("arena_bytes", C.c_size_t), ("arena_in_use", C.c_size_t)]
 
 
 def _check(status: int) -> None:
@@ -386,6 +419,103 @@ def quantize_noalloc(data, eb: float, radius: int, q, unpred, stream: int = 0) -
 
 
 NOALLOC_MAX_VALUES = 65536 * 1024
+
+REQ_BOX, REQ_LEVEL = 0, 1
+
+
+@dataclass
+class ServedResult:
+    ticket: int
+    status: int
+    out_dev: int  # device address (valid until release)
+    shape: tuple  # (nz, ny, nx)
+    nbytes: int
+    queue_ms: float
+    latency_ms: float
+    batch: int
+    batch_size: int
+
+
+class Server:
+    """Request server over streams resident on one GPU (stz_server_*):
+    box / slice / progressive-level requests, continuously batched."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0, max_batch: int = 0, slots: int = 0,
+                 autotune: bool = True, threads: int = 0):
+        self.lib = load_library()
+        o = ServerOpts()
+        self.lib.stz_server_default_opts(C.byref(o))
+        if arena_bytes:
+            o.arena_bytes = arena_bytes
+        if max_batch:
+            o.max_batch = max_batch
+        if slots:
+            o.slots = slots
+        o.autotune = 1 if autotune else 0
+        o.threads = threads
+        self._s = C.c_void_p()
+        _check(self.lib.stz_server_create(int(device), C.byref(o), C.byref(self._s)))
+
+    def close(self):
+        if self._s.value:
+            self.lib.stz_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_stream(self, data) -> int:
+        b = data.to_bytes() if isinstance(data, Stream) else bytes(data)
+        sid = C.c_int()
+        _check(self.lib.stz_server_add_stream(self._s, b, len(b), C.byref(sid)))
+        return sid.value
+
+    def _submit(self, r: Request) -> int:
+        t = C.c_uint64()
+        _check(self.lib.stz_server_submit(self._s, C.byref(r), C.byref(t)))
+        return t.value
+
+    def submit_box(self, stream_id: int, lo, hi) -> int:
+        """lo/hi: inclusive (x, y, z) corners; lo == hi on one axis makes a slice."""
+        r = Request()
+        r.stream_id, r.kind = stream_id, REQ_BOX
+        for a in range(3):
+            r.lo[a], r.hi[a] = int(lo[a]), int(hi[a])
+        return self._submit(r)
+
+    def submit_level(self, stream_id: int, level: int) -> int:
+        r = Request()
+        r.stream_id, r.kind, r.level = stream_id, REQ_LEVEL, int(level)
+        return self._submit(r)
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0) -> ServedResult:
+        r = Result()
+        _check(self.lib.stz_server_wait(self._s, ticket, timeout_ms, C.byref(r)))
+        return ServedResult(ticket, r.status, r.out_dev or 0, (r.dims[2], r.dims[1], r.dims[0]), r.bytes, r.queue_ms,
+                            r.latency_ms, r.batch, r.batch_size)
+
+    def copy_out(self, res: ServedResult, dtype=np.float32) -> np.ndarray:
+        out = np.empty(res.shape, dtype=dtype)
+        assert out.nbytes == res.nbytes, "dtype does not match the stream"
+        _check(self.lib.stz_server_copy_out(self._s, res.ticket, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def release(self, ticket: int) -> None:
+        _check(self.lib.stz_server_release(self._s, ticket))
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(self.lib.stz_server_stats_get(self._s, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
 
 
 def _tcode(t) -> int:

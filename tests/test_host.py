@@ -114,10 +114,24 @@ def test_fields_generators():
 
 
 def test_ctypes_structs_match_header():
-    """Opts/Info layouts agree with include/stz/stz.h (field order and types)."""
+    """ctypes layouts agree with include/stz/stz.h (field order)."""
     hdr = open(os.path.join(ROOT, "include", "stz", "stz.h")).read()
-    for struct, cls in (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info)):
+    for struct, cls in (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info),
+                        ("stz_server_opts", stz_b200.ServerOpts), ("stz_request", stz_b200.Request),
+                        ("stz_result", stz_b200.Result), ("stz_server_stats", stz_b200.ServerStats)):
         body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (struct, struct), hdr, re.S).group(1)
-        fields = re.findall(r"^\s*(?:int|double|size_t)\s+([a-z0-9_, ]+);", body, re.M)
-        names = [n.strip() for f in fields for n in f.split(",")]
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = re.findall(r"^\s*(?:const\s+)?(?:u?int64_t|int|double|size_t|stz_status|void)\b\s*\**\s*"
+                            r"([a-z0-9_, \[\]]+);", body, re.M)
+        names = [re.sub(r"\[\d+\]", "", n).strip() for f in fields for n in f.split(",")]
         assert names == [f[0] for f in cls._fields_], struct
+    # sizes that the C compiler and ctypes must agree on (x86-64 ABI)
+    assert ctypes.sizeof(stz_b200.Request) == 4 + 4 + 24 + 24 + 4 + 4
+    assert ctypes.sizeof(stz_b200.Result) == 4 + 4 + 8 + 24 + 8 + 8 + 8 + 8 + 4 + 4
+
+
+def test_server_default_opts():
+    lib = stz_b200.load_library()
+    o = stz_b200.ServerOpts()
+    lib.stz_server_default_opts(ctypes.byref(o))
+    assert o.arena_bytes == 1 << 30 and o.max_batch == 64 and o.slots == 2 and o.autotune == 1
