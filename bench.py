@@ -55,6 +55,7 @@ def parse_args():
     p.add_argument("--once", action="store_true",
                    help="one compress + one full decompress of the workload, no timing (profiler captures)")
     p.add_argument("--no-serve", action="store_true", help="skip the request-server latency measurement")
+    p.add_argument("--serve-only", action="store_true", help="only the request-server latency measurement")
     p.add_argument("--serve-size", type=int, default=1024, help="edge of the resident serving field")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="length of each serving load run")
     return p.parse_args()
@@ -268,7 +269,7 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
             ready.release()
 
     lat = {"box": [], "slice": [], "level": []}
-    batch_sizes, out_bytes = [], 0
+    batch_sizes, out_bytes, queue, order = [], 0, [], []
     th = threading.Thread(target=producer)
     t0 = time.perf_counter()
     th.start()
@@ -282,6 +283,8 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
             err.append(f"status {res.status}")
             break
         lat[reqs[i][0]].append(res.latency_ms)
+        order.append(res.latency_ms)
+        queue.append(res.queue_ms)
         batch_sizes.append(res.batch_size)
         out_bytes += res.nbytes
     wall = time.perf_counter() - t0
@@ -289,8 +292,12 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
     if err:
         return {"error": err[0]}
     allv = [x for v in lat.values() for x in v]
+    h = len(order) // 2
     out = {"offered_rps": rate, "requests": n, "achieved_rps": n / wall, "p50_ms": _pct(allv, 50),
-           "p99_ms": _pct(allv, 99), "mean_batch": float(np.mean(batch_sizes)), "out_gbs": out_bytes / wall / 1e9}
+           "p99_ms": _pct(allv, 99), "max_ms": max(allv), "queue_p50_ms": _pct(queue, 50),
+           "queue_p99_ms": _pct(queue, 99), "p99_first_half_ms": _pct(order[:h], 99),
+           "p99_second_half_ms": _pct(order[h:], 99), "mean_batch": float(np.mean(batch_sizes)),
+           "max_batch": int(max(batch_sizes)), "out_gbs": out_bytes / wall / 1e9}
     for k, v in lat.items():
         if v:
             out[k] = {"n": len(v), "p50_ms": _pct(v, 50), "p99_ms": _pct(v, 99)}
@@ -311,7 +318,11 @@ def serving_bench(args, ctx, local):
     n = args.serve_size
     f = fields.grf((n, n, n), 3.0, args.seed + 1000, np.float32, device=f"cuda:{local}")
     s = ctx.compress(f, opts=stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd))
-    del f
+    E = args.rel * (float(f.max()) - float(f.min()))
+    probe = ctx.decompress_box(s, (n // 3, n // 5, n // 7), (n // 3 + 63, n // 5 + 63, n // 7 + 63))
+    ref = f[n // 7:n // 7 + 64, n // 5:n // 5 + 64, n // 3:n // 3 + 64].cpu().numpy()
+    probe_err = float(np.abs(probe.astype(np.float64) - ref).max()) / E
+    del f, ref
     torch.cuda.empty_cache()
     K = s.info().n_levels
     dims = (n, n, n)
@@ -338,8 +349,8 @@ def serving_bench(args, ctx, local):
             return ("slice", lo, hi)
         return ("level", int(rng.integers(0, 4)))
 
-    res = {"field": f"{n}^3 f32 GRF k^-3, rel eb {args.rel}", "stream_bytes": len(s), "add_stream_s": add_s,
-           "shapes": srv.stats()}
+    res = {"field": f"{n}^3 f32 GRF k^-3, rel eb {args.rel}", "stream_bytes": len(s), "cr": full_bytes / len(s),
+           "probe_box_max_err_over_bound": probe_err, "add_stream_s": add_s, "shapes": srv.stats()}
     sec = args.serve_seconds
     serve_load(srv, sid, dims, K, 500, 0.2, box64, 1)  # warm-up
     res["box64"] = [serve_load(srv, sid, dims, K, r, sec, box64, 10 + i) for i, r in enumerate((2000, 10000))]
@@ -401,6 +412,12 @@ def main():
     out = torch.empty_like(field)
     opts = stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd)
     stream = torch.cuda.ExternalStream(ctx.cuda_stream(), device=f"cuda:{local}")
+    if args.serve_only:
+        if rank == 0:
+            print(json.dumps({"serving": serving_bench(args, ctx, local)}))
+        ctx.close()
+        replicas.finalize()
+        return
     if args.once:
         s = ctx.compress(field, opts=opts)
         ctx.decompress(s, out=out)

@@ -20,7 +20,12 @@
  *   - Dims are (nx, ny, nz) with x fastest (row-major z, y, x), as in the
  *     reference (FD5:113).
  *   - `_dev` entry points take CUDA device pointers on the context's device
- *     and run on the context's stream; others take host pointers.
+ *     and run on the context's stream; others take host pointers. The
+ *     context's stream does not wait for other streams: device inputs
+ *     written on another stream must be complete before the call (synchronize
+ *     the producing stream). compress / decompress / box calls return with
+ *     their outputs complete; the function-level boundary calls below are
+ *     asynchronous on the context's stream (stz_context_sync).
  *   - The library owns stz_stream objects; callers own every output buffer.
  *   - A context is used by one host thread at a time; streams are immutable
  *     after creation and can be shared for reading.

@@ -721,7 +721,11 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
 {
     const int K = s->dir.h.K;
     const int kdec = K - level;
-    if (s->resident && s->resident->kmax >= kdec) return decode_levels<T>(ctx, s, *s->resident, kdec, out_dev);
+    if (s->resident && s->resident->kmax >= kdec) {
+        STZ_TRY(decode_levels<T>(ctx, s, *s->resident, kdec, out_dev));
+        STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the output is complete on return
+        return STZ_OK;
+    }
     Prepared p;
     ctx->borrow(p);
     {
@@ -781,34 +785,72 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         add_work(work, ids, si, cs.data(), cs.size(), high.C);
         add_unpred_work(*p, si, cs.data(), cs.size(), uw);
     }
-    STZ_TRY(decode_chunks<T>(ctx, *p, work, ids, uw));
-    // mid grid on the reference regions
-    std::vector<RoiBox> boxes;
-    uint64_t total = 0;
-    for (const auto& r : plan.regions) {
-        if (r[0].empty() || r[1].empty() || r[2].empty()) continue;
-        RoiBox b{r[0].b, r[0].e, r[1].b, r[1].e, r[2].b, r[2].e, total};
-        total += (uint64_t)(r[0].e - r[0].b + 1) * (r[1].e - r[1].b + 1) * (r[2].e - r[2].b + 1);
-        boxes.push_back(b);
-    }
+    // ROI jobs: the mid grid on the bounding box of the reference regions,
+    // then the query box
     STZ_CUDA(ctx->mid.ensure(8 * nbase * elem));
-    STZ_CUDA(ctx->boxes.ensure(std::max<size_t>(boxes.size(), 1) * sizeof(RoiBox)));
-    STZ_CUDA(ctx->h_small.ensure(std::max<size_t>(boxes.size(), 1) * sizeof(RoiBox)));
-    if (!boxes.empty()) std::memcpy(ctx->h_small.p, boxes.data(), boxes.size() * sizeof(RoiBox));
-    STZ_CUDA(cudaMemcpyAsync(ctx->boxes.p, ctx->h_small.p, boxes.size() * sizeof(RoiBox), cudaMemcpyHostToDevice, ctx->st));
-    const T* ud = p->total_unpred ? ctx->unpred_dense.as<T>() : nullptr;
-    if (total) {
-        KScope ks(ctx, "k_roi_mid");
-        launch_roi_mid<T>(ctx->boxes.as<RoiBox>(), (int)boxes.size(), total, p->base->as<T>(), low,
-                          qparams(ps, K - 1), h.predictor, ctx->codes.as<uint16_t>() + p->sd[(size_t)(K - 2) * 7].code_off,
-                          ud ? ud + p->sd[(size_t)(K - 2) * 7].code_off : nullptr, ctx->mid.as<T>(), ctx->st);
+    std::vector<RoiJob> mj, rj;
+    int m0[3], m1[3];
+    if (region_bbox(plan, m0, m1)) {
+        const int o0[3] = {0, 0, 0};
+        mj.push_back(cells_job(m0, m1, ctx->mid.p, o0, 2 * (uint64_t)low.dx, 4 * (uint64_t)low.dx * low.dy, 0));
     }
-    const RoiBox qb{plan.q[0].b, plan.q[0].e, plan.q[1].b, plan.q[1].e, plan.q[2].b, plan.q[2].e, 0};
+    const int w0[3] = {plan.q[0].b, plan.q[1].b, plan.q[2].b}, w1[3] = {plan.q[0].e, plan.q[1].e, plan.q[2].e};
+    const uint64_t ex = (uint64_t)(w1[0] - w0[0] + 1), ey = (uint64_t)(w1[1] - w0[1] + 1);
+    rj.push_back(cells_job(w0, w1, out_dev, w0, ex, ex * ey, 0));
+    // one record (work lists + job lists), one copy, one synchronization
+    BatchHdr hd{};
+    hd.n_work = (uint32_t)work.size(), hd.n_uwork = (uint32_t)uw.size();
+    hd.n_mid = (uint32_t)mj.size(), hd.n_req = (uint32_t)rj.size();
+    hd.mid_total = mj.empty() ? 0 : job_units(mj[0]);
+    hd.req_total = job_units(rj[0]);
+    size_t off = align256(sizeof(BatchHdr));
+    hd.o_work = (uint32_t)off;
+    off = align256(off + work.size() * sizeof(CtaWork));
+    hd.o_ids = (uint32_t)off;
+    off = align256(off + ids.size() * 4);
+    hd.o_uwork = (uint32_t)off;
+    off = align256(off + uw.size() * sizeof(UnpredWork));
+    hd.o_mid = (uint32_t)off;
+    off = align256(off + mj.size() * sizeof(RoiJob));
+    hd.o_req = (uint32_t)off;
+    off = align256(off + rj.size() * sizeof(RoiJob));
+    STZ_CUDA(ctx->h_meta.ensure(off));
+    uint8_t* hm = ctx->h_meta.as<uint8_t>();
+    std::memcpy(hm, &hd, sizeof hd);
+    if (!work.empty()) std::memcpy(hm + hd.o_work, work.data(), work.size() * sizeof(CtaWork));
+    if (!ids.empty()) std::memcpy(hm + hd.o_ids, ids.data(), ids.size() * 4);
+    if (!uw.empty()) std::memcpy(hm + hd.o_uwork, uw.data(), uw.size() * sizeof(UnpredWork));
+    if (!mj.empty()) std::memcpy(hm + hd.o_mid, mj.data(), mj.size() * sizeof(RoiJob));
+    std::memcpy(hm + hd.o_req, rj.data(), rj.size() * sizeof(RoiJob));
+    STZ_CUDA(ctx->work.ensure(off));
+    STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hm, off, cudaMemcpyHostToDevice, ctx->st));
+    const uint8_t* dm = ctx->work.as<uint8_t>();
+    STZ_CUDA(ctx->codes.ensure(p->total_codes * 2));
+    if (p->total_unpred) STZ_CUDA(ctx->unpred_dense.ensure(p->total_codes * sizeof(T)));
+    if (!work.empty()) {
+        KScope ks(ctx, "k_decode");
+        launch_decode((const CtaWork*)(dm + hd.o_work), (const uint32_t*)(dm + hd.o_ids), (int)work.size(), p->d_sd,
+                      p->d_sym, p->d_len, p->d_sub, p->d_choff, p->d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+    }
+    if (!uw.empty()) {
+        KScope ks(ctx, "k_unpred_move");
+        launch_unpred_move<T>(false, (const UnpredWork*)(dm + hd.o_uwork), (int)uw.size(), p->d_sd,
+                              ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p->d_ulist, ctx->st);
+    }
+    const T* ud = p->total_unpred ? ctx->unpred_dense.as<T>() : nullptr;
+    const uint64_t lo_off = p->sd[(size_t)(K - 2) * 7].code_off, hi_off = p->sd[(size_t)(K - 1) * 7].code_off;
+    auto blocks = [](uint64_t n) { return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 16)); };
+    if (hd.mid_total) {
+        KScope ks(ctx, "k_roi_cells[low]");
+        launch_roi_cells<T>(blocks(hd.mid_total), 256, dm, 0, p->base->as<T>(), low, p->base->as<T>(), low,
+                            qparams(ps, K - 1), h.predictor, ctx->codes.as<uint16_t>() + lo_off,
+                            ud ? ud + lo_off : nullptr, ctx->st);
+    }
     {
-        KScope ks(ctx, "k_roi_box");
-        launch_roi_box<T>(qb, ctx->mid.as<T>(), high, qparams(ps, K), h.predictor,
-                          ctx->codes.as<uint16_t>() + p->sd[(size_t)(K - 1) * 7].code_off,
-                          ud ? ud + p->sd[(size_t)(K - 1) * 7].code_off : nullptr, out_dev, ctx->st);
+        KScope ks(ctx, "k_roi_cells[high]");
+        launch_roi_cells<T>(blocks(hd.req_total), 256, dm, 1, ctx->mid.as<T>(), high, p->base->as<T>(), low,
+                            qparams(ps, K), h.predictor, ctx->codes.as<uint16_t>() + hi_off,
+                            ud ? ud + hi_off : nullptr, ctx->st);
     }
     STZ_CUDA(cudaGetLastError());
     STZ_CUDA(cudaStreamSynchronize(ctx->st));

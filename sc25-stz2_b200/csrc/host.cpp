@@ -572,6 +572,20 @@ void merge_axis(AxisRange& d, AxisRange s)
 
 }  // namespace
 
+bool region_bbox(const QueryPlan& p, int lo[3], int hi[3])
+{
+    bool any = false;
+    for (const auto& rg : p.regions) {
+        if (rg[0].empty() || rg[1].empty() || rg[2].empty()) continue;
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = any ? std::min(lo[a], rg[a].b) : rg[a].b;
+            hi[a] = any ? std::max(hi[a], rg[a].e) : rg[a].e;
+        }
+        any = true;
+    }
+    return any;
+}
+
 bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], AxisRange q[3])
 {
     const int dims[3] = {nx, ny, nz};

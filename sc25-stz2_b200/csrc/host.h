@@ -131,6 +131,9 @@ struct QueryPlan {
 QueryPlan plan_query(int nx, int ny, int nz, int chunk_high, int chunk_low, const int64_t a[3], const int64_t b[3]);
 // The query box alone (make_query, FD5:1637-1644); returns is_slice.
 bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], AxisRange q[3]);
+// Bounding box (x, y, z, inclusive) of a plan's non-empty reference regions
+// on the half-resolution grid; false when there are none.
+bool region_bbox(const QueryPlan& p, int lo[3], int hi[3]);
 void flatten_plan(const QueryPlan& p, std::vector<int64_t>& out);
 
 }  // namespace stz

@@ -74,30 +74,6 @@ __device__ __forceinline__ void load_tile(T* tile, const T* __restrict__ R, int 
     }
 }
 
-// The 7 predictions of one coarse point.
-template <int PRED, typename T, class Acc>
-__device__ __forceinline__ void predict7(const Acc& r, bool interior, int x, int y, int z, int dx, int dy, int dz,
-                                         T (&p)[7])
-{
-    if (interior) {
-        p[0] = predict_interior_at<PRED, 0, T>(r);
-        p[1] = predict_interior_at<PRED, 1, T>(r);
-        p[2] = predict_interior_at<PRED, 2, T>(r);
-        p[3] = predict_interior_at<PRED, 3, T>(r);
-        p[4] = predict_interior_at<PRED, 4, T>(r);
-        p[5] = predict_interior_at<PRED, 5, T>(r);
-        p[6] = predict_interior_at<PRED, 6, T>(r);
-    } else {
-        p[0] = predict_at<PRED, 0, T>(r, x, y, z, dx, dy, dz);
-        p[1] = predict_at<PRED, 1, T>(r, x, y, z, dx, dy, dz);
-        p[2] = predict_at<PRED, 2, T>(r, x, y, z, dx, dy, dz);
-        p[3] = predict_at<PRED, 3, T>(r, x, y, z, dx, dy, dz);
-        p[4] = predict_at<PRED, 4, T>(r, x, y, z, dx, dy, dz);
-        p[5] = predict_at<PRED, 5, T>(r, x, y, z, dx, dy, dz);
-        p[6] = predict_at<PRED, 6, T>(r, x, y, z, dx, dy, dz);
-    }
-}
-
 constexpr int kSmemBins = 512;
 
 struct HistArgs {

@@ -1,23 +1,41 @@
 // Random-access box / slice reconstruction (the query path of FD5:2460-2640).
 //
 // After the planner has chosen the marker chunks a box needs and those chunks
-// are entropy-decoded, two kernels finish the query:
-//   k_roi_mid : rebuild the half-resolution ("mid") grid on the high level's
-//               reference regions: sub-block 0 from the decoded base, the other
-//               parities as recover(q) + P(base) on the low level (the
-//               reference's low ROI depreprocess FD5:2507-2516 and the
+// are entropy-decoded, two launches of one kernel finish the query:
+//   low level : rebuild the half-resolution ("mid") grid on the bounding box
+//               of the high level's reference regions from the decoded base
+//               (the reference's low ROI depreprocess FD5:2507-2516 and its
 //               reference gather FD5:2520-2538, fused);
-//   k_roi_box : each box point is either a mid-grid value (even parity) or
-//               recover(q) + P(mid) of its high sub-block (FD5:2573-2605,
-//               fused with the desplit).
-// Every value is computed with the same expression as the full decode, so a
-// box equals the full decode on the same coordinates bit for bit.
+//   high level: rebuild the query box from the mid grid (FD5:2573-2605, fused
+//               with the desplit).
+// A thread rebuilds one coarse cell: the coarse value (parity 0) and the 7
+// sub-block values recover(q) + P(coarse) of the 2x2x2 fine points the cell
+// predicts, with the same predictor and the same interior/boundary split as
+// the full level decode, so a box equals the full decode on the same
+// coordinates bit for bit. Cells on the window's edge also evaluate the
+// parities outside the window; those values are not written.
 #include <cuda_runtime.h>
 
 #include "roi.h"
 #include "stz_device.cuh"
 
 namespace stz {
+
+RoiJob cells_job(const int w0[3], const int w1[3], void* out, const int origin[3], uint64_t osx, uint64_t osy,
+                 uint64_t start)
+{
+    RoiJob j{};
+    j.cx0 = w0[0] >> 1, j.cy0 = w0[1] >> 1, j.cz0 = w0[2] >> 1;
+    j.ncx = (w1[0] >> 1) - j.cx0 + 1, j.ncy = (w1[1] >> 1) - j.cy0 + 1, j.ncz = (w1[2] >> 1) - j.cz0 + 1;
+    j.wx0 = w0[0], j.wx1 = w1[0], j.wy0 = w0[1], j.wy1 = w1[1], j.wz0 = w0[2], j.wz1 = w1[2];
+    j.ox = origin[0], j.oy = origin[1], j.oz = origin[2];
+    j.kind = kJobCells;
+    j.osx = osx, j.osy = osy;
+    j.start = start;
+    j.out = (uint64_t)(uintptr_t)out;
+    return j;
+}
+
 namespace {
 
 __device__ __forceinline__ size_t cm_index(const LevelGeom& g, int x, int y, int z)
@@ -28,226 +46,98 @@ __device__ __forceinline__ size_t cm_index(const LevelGeom& g, int x, int y, int
     return (size_t)chunk * C * C * C + (size_t)((z - cz * C) * C + (y - cy * C)) * C + (x - cx * C);
 }
 
-template <int PRED, typename T>
-__device__ __forceinline__ T predict_rt(int b, const Grid<T>& g, int x, int y, int z)
-{
-    switch (b) {
-    case 0: return predict<PRED>(0, g, x, y, z);
-    case 1: return predict<PRED>(1, g, x, y, z);
-    case 2: return predict<PRED>(2, g, x, y, z);
-    case 3: return predict<PRED>(3, g, x, y, z);
-    case 4: return predict<PRED>(4, g, x, y, z);
-    case 5: return predict<PRED>(5, g, x, y, z);
-    default: return predict<PRED>(6, g, x, y, z);
-    }
-}
-
-// Value at point (X, Y, Z) of the grid one level finer than `coarse`: the
-// coarse value itself at even parity, else recover(q) + P(coarse) of the
-// point's sub-block (the level's codes are chunk-major per sub-block).
-template <typename T, int PRED>
-__device__ __forceinline__ T finer_value(const Grid<T>& coarse, const LevelGeom& g, const QuantParams& qp,
-                                         const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
-                                         int X, int Y, int Z)
-{
-    const int si = ((Z & 1) << 2) | ((Y & 1) << 1) | (X & 1);
-    const int x = X >> 1, y = Y >> 1, z = Z >> 1;
-    if (si == 0) return coarse.at((size_t)z * coarse.sy + (size_t)y * coarse.sx + x);
-    const size_t k = (size_t)(si - 1) * g.n + cm_index(g, x, y, z);
-    const int q = codes[k];
-    const T dq = q ? recover<T>(q, qp) : unpred_dense[k];
-    return Ar<T>::add(dq, predict_rt<PRED>(si - 1, coarse, x, y, z));
-}
-
-// Index of the last box whose start <= t (starts ascending, boxes[0].start == 0).
-template <typename B>
-__device__ __forceinline__ int find_box(const B* __restrict__ boxes, int n, uint64_t t)
+// Index of the last entry whose start <= t (starts ascending, [0].start == 0).
+__device__ __forceinline__ int find_job(const RoiJob* __restrict__ jobs, int n, uint64_t t)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int m = (lo + hi + 1) >> 1;
-        if (boxes[m].start <= t) lo = m;
+        if (jobs[m].start <= t) lo = m;
         else hi = m - 1;
     }
     return lo;
 }
 
-__device__ __forceinline__ void box_point(const RoiBox& bx, uint64_t i, int& X, int& Y, int& Z)
-{
-    const int ex = bx.x1 - bx.x0 + 1, ey = bx.y1 - bx.y0 + 1;
-    X = bx.x0 + (int)(i % ex);
-    Y = bx.y0 + (int)((i / ex) % ey);
-    Z = bx.z0 + (int)(i / ((uint64_t)ex * ey));
-}
-
-// Boxes are given as inclusive ranges; `start` is the prefix sum of box
-// volumes so one launch covers all boxes.
 template <typename T, int PRED>
-__global__ void k_roi_mid(const RoiBox* __restrict__ boxes, int nbox, uint64_t total, Grid<T> base, LevelGeom low,
-                          QuantParams qp, const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
-                          T* __restrict__ mid, size_t msx, size_t msy)
+__global__ void __launch_bounds__(256) k_roi_cells(const uint8_t* __restrict__ meta, int list, Grid<T> coarse,
+                                                   LevelGeom g, Grid<T> base, QuantParams qp,
+                                                   const uint16_t* __restrict__ codes,
+                                                   const T* __restrict__ unpred_dense)
 {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-        const RoiBox bx = boxes[find_box(boxes, nbox, t)];
-        int X, Y, Z;
-        box_point(bx, t - bx.start, X, Y, Z);
-        mid[(size_t)Z * msy + (size_t)Y * msx + X] = finer_value<T, PRED>(base, low, qp, codes, unpred_dense, X, Y, Z);
-    }
-}
-
-template <typename T, int PRED>
-__global__ void k_roi_box(RoiBox box, Grid<T> mid, LevelGeom high, QuantParams qp, const uint16_t* __restrict__ codes,
-                          const T* __restrict__ unpred_dense, T* __restrict__ out)
-{
-    const int ex = box.x1 - box.x0 + 1, ey = box.y1 - box.y0 + 1;
-    const uint64_t total = (uint64_t)ex * ey * (box.z1 - box.z0 + 1);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        int X, Y, Z;
-        box_point(box, i, X, Y, Z);
-        out[i] = finer_value<T, PRED>(mid, high, qp, codes, unpred_dense, X, Y, Z);
-    }
-}
-
-// Batched, device-sized variants (request server): the mid-grid regions and
-// the outputs of every request of a batch, counts read from the batch header.
-template <typename T, int PRED>
-__global__ void k_roi_mid_dyn(const uint8_t* __restrict__ meta, Grid<T> base, LevelGeom low, QuantParams qp,
-                              const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
-                              T* __restrict__ mid, size_t msx, size_t msy)
-{
+    using A = Ar<T>;
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
-    const uint64_t total = h->mid_total;
-    const int nbox = (int)h->n_mid;
-    const RoiBox* boxes = reinterpret_cast<const RoiBox*>(meta + h->o_mid);
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-        const RoiBox bx = boxes[find_box(boxes, nbox, t)];
-        int X, Y, Z;
-        box_point(bx, t - bx.start, X, Y, Z);
-        mid[(size_t)Z * msy + (size_t)Y * msx + X] = finer_value<T, PRED>(base, low, qp, codes, unpred_dense, X, Y, Z);
-    }
-}
-
-template <typename T, int PRED>
-__global__ void k_roi_req_dyn(const uint8_t* __restrict__ meta, Grid<T> mid, Grid<T> base, LevelGeom high,
-                              QuantParams qp, const uint16_t* __restrict__ codes,
-                              const T* __restrict__ unpred_dense)
-{
-    const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
-    const uint64_t total = h->req_total;
-    const int nreq = (int)h->n_req;
-    const ReqDesc* reqs = reinterpret_cast<const ReqDesc*>(meta + h->o_req);
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-        const int ri = find_box(reqs, nreq, t);
-        const ReqDesc r = reqs[ri];
-        const uint64_t i = t - r.start;
-        int X, Y, Z;
-        box_point(r.box, i, X, Y, Z);
-        T v;
-        if (r.kind == kReqBox) {
-            v = finer_value<T, PRED>(mid, high, qp, codes, unpred_dense, X, Y, Z);
-        } else {
-            const int s = r.shift;
-            v = base.at(((size_t)Z << s) * base.sy + ((size_t)Y << s) * base.sx + ((size_t)X << s));
+    const int nj = (int)(list ? h->n_req : h->n_mid);
+    const uint64_t total = list ? h->req_total : h->mid_total;
+    const RoiJob* jobs = reinterpret_cast<const RoiJob*>(meta + (list ? h->o_req : h->o_mid));
+    const size_t n = g.n;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const RoiJob J = jobs[find_job(jobs, nj, t)];
+        const uint64_t u = t - J.start;
+        const int cx = J.cx0 + (int)(u % J.ncx);
+        const int cy = J.cy0 + (int)((u / J.ncx) % J.ncy);
+        const int cz = J.cz0 + (int)(u / ((uint64_t)J.ncx * J.ncy));
+        T* out = reinterpret_cast<T*>(J.out);
+        if (J.kind == kJobSample) {
+            const int s = J.shift;
+            out[(size_t)(cz - J.oz) * J.osy + (size_t)(cy - J.oy) * J.osx + (cx - J.ox)] =
+                base.at(((size_t)cz << s) * base.sy + ((size_t)cy << s) * base.sx + ((size_t)cx << s));
+            continue;
         }
-        reinterpret_cast<T*>(r.out)[i] = v;
+        const size_t cm = cm_index(g, cx, cy, cz);
+        int q[7];
+#pragma unroll
+        for (int b = 0; b < 7; ++b) q[b] = __ldg(codes + (size_t)b * n + cm);
+        const GlobalAt<T> r{coarse.p + (size_t)cz * coarse.sy + (size_t)cy * coarse.sx + cx, (long long)coarse.sx,
+                            (long long)coarse.sy};
+        const bool interior = cx >= 1 && cx <= g.dx - 3 && cy >= 1 && cy <= g.dy - 3 && cz >= 1 && cz <= g.dz - 3;
+        T p[7];
+        predict7<PRED>(r, interior, cx, cy, cz, g.dx, g.dy, g.dz, p);
+        T v[8];
+        v[0] = r(0);
+#pragma unroll
+        for (int b = 0; b < 7; ++b) {
+            const T dq = q[b] ? recover<T>(q[b], qp) : __ldg(unpred_dense + (size_t)b * n + cm);
+            v[b + 1] = A::add(dq, p[b]);
+        }
+#pragma unroll
+        for (int si = 0; si < 8; ++si) {
+            const int X = 2 * cx + (si & 1), Y = 2 * cy + ((si >> 1) & 1), Z = 2 * cz + (si >> 2);
+            if (X >= J.wx0 && X <= J.wx1 && Y >= J.wy0 && Y <= J.wy1 && Z >= J.wz0 && Z <= J.wz1)
+                out[(size_t)(Z - J.oz) * J.osy + (size_t)(Y - J.oy) * J.osx + (X - J.ox)] = v[si];
+        }
     }
 }
 
-int grid_blocks(uint64_t n)
+template <typename T>
+Grid<T> grid_of(const T* p, const LevelGeom& g)
 {
-    uint64_t g = (n + 255) / 256;
-    if (g > 148 * 16) g = 148 * 16;
-    return (int)(g ? g : 1);
+    Grid<T> G;
+    G.p = p;
+    G.dx = g.dx, G.dy = g.dy, G.dz = g.dz;
+    G.sx = (size_t)g.dx, G.sy = (size_t)g.dx * g.dy;
+    return G;
 }
 
 }  // namespace
 
 template <typename T>
-void launch_roi_mid(const RoiBox* boxes_dev, int nbox, uint64_t total, const T* base, const LevelGeom& low,
-                    QuantParams qp, int predictor, const uint16_t* codes, const T* unpred_dense, T* mid,
-                    cudaStream_t st)
+void launch_roi_cells(int grid, int block, const uint8_t* meta, int list, const T* coarse, const LevelGeom& geo,
+                      const T* base, const LevelGeom& base_geo, QuantParams qp, int predictor, const uint16_t* codes,
+                      const T* unpred_dense, cudaStream_t st)
 {
-    if (!total) return;
-    Grid<T> g;
-    g.p = base;
-    g.dx = low.dx, g.dy = low.dy, g.dz = low.dz;
-    g.sx = (size_t)low.dx, g.sy = (size_t)low.dx * low.dy;
-    const size_t msx = 2 * (size_t)low.dx, msy = 4 * (size_t)low.dx * low.dy;
+    const Grid<T> gc = grid_of(coarse, geo), gb = grid_of(base, base_geo);
     if (predictor == 1)
-        k_roi_mid<T, 1><<<grid_blocks(total), 256, 0, st>>>(boxes_dev, nbox, total, g, low, qp, codes, unpred_dense,
-                                                            mid, msx, msy);
+        k_roi_cells<T, 1><<<grid, block, 0, st>>>(meta, list, gc, geo, gb, qp, codes, unpred_dense);
     else
-        k_roi_mid<T, 0><<<grid_blocks(total), 256, 0, st>>>(boxes_dev, nbox, total, g, low, qp, codes, unpred_dense,
-                                                            mid, msx, msy);
+        k_roi_cells<T, 0><<<grid, block, 0, st>>>(meta, list, gc, geo, gb, qp, codes, unpred_dense);
 }
 
-template <typename T>
-void launch_roi_box(const RoiBox& box, const T* mid, const LevelGeom& high, QuantParams qp, int predictor,
-                    const uint16_t* codes, const T* unpred_dense, T* out, cudaStream_t st)
-{
-    const uint64_t total = (uint64_t)(box.x1 - box.x0 + 1) * (box.y1 - box.y0 + 1) * (box.z1 - box.z0 + 1);
-    Grid<T> g;
-    g.p = mid;
-    g.dx = high.dx, g.dy = high.dy, g.dz = high.dz;
-    g.sx = (size_t)high.dx, g.sy = (size_t)high.dx * high.dy;
-    if (predictor == 1)
-        k_roi_box<T, 1><<<grid_blocks(total), 256, 0, st>>>(box, g, high, qp, codes, unpred_dense, out);
-    else
-        k_roi_box<T, 0><<<grid_blocks(total), 256, 0, st>>>(box, g, high, qp, codes, unpred_dense, out);
-}
-
-template <typename T>
-void launch_roi_mid_dyn(int grid, int block, const uint8_t* meta, const T* base, const LevelGeom& low, QuantParams qp,
-                        int predictor, const uint16_t* codes, const T* unpred_dense, T* mid, cudaStream_t st)
-{
-    Grid<T> g;
-    g.p = base;
-    g.dx = low.dx, g.dy = low.dy, g.dz = low.dz;
-    g.sx = (size_t)low.dx, g.sy = (size_t)low.dx * low.dy;
-    const size_t msx = 2 * (size_t)low.dx, msy = 4 * (size_t)low.dx * low.dy;
-    if (predictor == 1)
-        k_roi_mid_dyn<T, 1><<<grid, block, 0, st>>>(meta, g, low, qp, codes, unpred_dense, mid, msx, msy);
-    else
-        k_roi_mid_dyn<T, 0><<<grid, block, 0, st>>>(meta, g, low, qp, codes, unpred_dense, mid, msx, msy);
-}
-
-template <typename T>
-void launch_roi_req_dyn(int grid, int block, const uint8_t* meta, const T* mid, const T* base, const LevelGeom& low,
-                        const LevelGeom& high, QuantParams qp, int predictor, const uint16_t* codes,
-                        const T* unpred_dense, cudaStream_t st)
-{
-    Grid<T> gm;
-    gm.p = mid;
-    gm.dx = high.dx, gm.dy = high.dy, gm.dz = high.dz;
-    gm.sx = (size_t)high.dx, gm.sy = (size_t)high.dx * high.dy;
-    Grid<T> gb;
-    gb.p = base;
-    gb.dx = low.dx, gb.dy = low.dy, gb.dz = low.dz;
-    gb.sx = (size_t)low.dx, gb.sy = (size_t)low.dx * low.dy;
-    if (predictor == 1)
-        k_roi_req_dyn<T, 1><<<grid, block, 0, st>>>(meta, gm, gb, high, qp, codes, unpred_dense);
-    else
-        k_roi_req_dyn<T, 0><<<grid, block, 0, st>>>(meta, gm, gb, high, qp, codes, unpred_dense);
-}
-
-template void launch_roi_mid_dyn<float>(int, int, const uint8_t*, const float*, const LevelGeom&, QuantParams, int,
-                                        const uint16_t*, const float*, float*, cudaStream_t);
-template void launch_roi_mid_dyn<double>(int, int, const uint8_t*, const double*, const LevelGeom&, QuantParams, int,
-                                         const uint16_t*, const double*, double*, cudaStream_t);
-template void launch_roi_req_dyn<float>(int, int, const uint8_t*, const float*, const float*, const LevelGeom&,
-                                        const LevelGeom&, QuantParams, int, const uint16_t*, const float*,
-                                        cudaStream_t);
-template void launch_roi_req_dyn<double>(int, int, const uint8_t*, const double*, const double*, const LevelGeom&,
-                                         const LevelGeom&, QuantParams, int, const uint16_t*, const double*,
-                                         cudaStream_t);
-
-template void launch_roi_mid<float>(const RoiBox*, int, uint64_t, const float*, const LevelGeom&, QuantParams, int,
-                                    const uint16_t*, const float*, float*, cudaStream_t);
-template void launch_roi_mid<double>(const RoiBox*, int, uint64_t, const double*, const LevelGeom&, QuantParams, int,
-                                     const uint16_t*, const double*, double*, cudaStream_t);
-template void launch_roi_box<float>(const RoiBox&, const float*, const LevelGeom&, QuantParams, int, const uint16_t*,
-                                    const float*, float*, cudaStream_t);
-template void launch_roi_box<double>(const RoiBox&, const double*, const LevelGeom&, QuantParams, int,
-                                     const uint16_t*, const double*, double*, cudaStream_t);
+template void launch_roi_cells<float>(int, int, const uint8_t*, int, const float*, const LevelGeom&, const float*,
+                                      const LevelGeom&, QuantParams, int, const uint16_t*, const float*,
+                                      cudaStream_t);
+template void launch_roi_cells<double>(int, int, const uint8_t*, int, const double*, const LevelGeom&,
+                                       const double*, const LevelGeom&, QuantParams, int, const uint16_t*,
+                                       const double*, cudaStream_t);
 
 }  // namespace stz

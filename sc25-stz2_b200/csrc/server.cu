@@ -39,7 +39,6 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr int kMaxSlots = 8;
-constexpr int kMaxRegionsPerBox = 8;  // 7 high reference regions + the sub-block-0 region
 
 double ms_between(Clock::time_point a, Clock::time_point b)
 {
@@ -169,8 +168,8 @@ struct Build {
     std::vector<CtaWork> work;
     std::vector<uint32_t> ids;
     std::vector<UnpredWork> uw;
-    std::vector<RoiBox> mid;
-    std::vector<ReqDesc> req;
+    std::vector<RoiJob> mid;  // low-level cells: mid-grid windows
+    std::vector<RoiJob> req;  // high-level cells of boxes, base samples of coarse levels
     uint64_t mid_total = 0, req_total = 0;
     std::vector<LevelJob> jobs;
 };
@@ -261,29 +260,28 @@ void plan_request(SrvStream& ss, Build& b, const Ticket& t, void* out)
             for (int64_t c : bp.chunks) list_chunk(ss, b, bp.block, (uint32_t)c);
         for (const BlockPlan& bp : plan.high)
             for (int64_t c : bp.chunks) list_chunk(ss, b, 7 + bp.block, (uint32_t)c);
-        for (const auto& rg : plan.regions) {
-            if (rg[0].empty() || rg[1].empty() || rg[2].empty()) continue;
-            b.mid.push_back({rg[0].b, rg[0].e, rg[1].b, rg[1].e, rg[2].b, rg[2].e, b.mid_total});
-            b.mid_total += (uint64_t)(rg[0].e - rg[0].b + 1) * (rg[1].e - rg[1].b + 1) * (rg[2].e - rg[2].b + 1);
+        int m0[3], m1[3];
+        if (region_bbox(plan, m0, m1)) {
+            const int o0[3] = {0, 0, 0};
+            b.mid.push_back(cells_job(m0, m1, ss.mid.p, o0, 2 * (uint64_t)ss.low.dx,
+                                      4 * (uint64_t)ss.low.dx * ss.low.dy, b.mid_total));
+            b.mid_total += job_units(b.mid.back());
         }
-        ReqDesc d{};
-        d.box = {plan.q[0].b, plan.q[0].e, plan.q[1].b, plan.q[1].e, plan.q[2].b, plan.q[2].e, 0};
-        d.start = b.req_total;
-        d.out = (uint64_t)(uintptr_t)out;
-        d.kind = kReqBox;
-        b.req.push_back(d);
-        b.req_total += (uint64_t)t.dims[0] * t.dims[1] * t.dims[2];
+        const int w0[3] = {plan.q[0].b, plan.q[1].b, plan.q[2].b}, w1[3] = {plan.q[0].e, plan.q[1].e, plan.q[2].e};
+        b.req.push_back(cells_job(w0, w1, out, w0, t.dims[0], (uint64_t)t.dims[0] * t.dims[1], b.req_total));
+        b.req_total += job_units(b.req.back());
         return;
     }
     if (r.level >= 2) {
-        ReqDesc d{};
-        d.box = {0, (int)t.dims[0] - 1, 0, (int)t.dims[1] - 1, 0, (int)t.dims[2] - 1, 0};
-        d.start = b.req_total;
-        d.out = (uint64_t)(uintptr_t)out;
-        d.kind = kReqSample;
-        d.shift = r.level - 2;
-        b.req.push_back(d);
-        b.req_total += (uint64_t)t.dims[0] * t.dims[1] * t.dims[2];
+        RoiJob j{};
+        j.ncx = (int)t.dims[0], j.ncy = (int)t.dims[1], j.ncz = (int)t.dims[2];
+        j.kind = kJobSample;
+        j.shift = r.level - 2;
+        j.osx = t.dims[0], j.osy = (uint64_t)t.dims[0] * t.dims[1];
+        j.start = b.req_total;
+        j.out = (uint64_t)(uintptr_t)out;
+        b.req.push_back(j);
+        b.req_total += job_units(j);
         return;
     }
     list_all(ss, b, 0, 7);
@@ -316,16 +314,16 @@ size_t pack(SrvStream& ss, Build& b, uint8_t* dst)
     h.o_uwork = (uint32_t)off;
     off = align16(off + b.uw.size() * sizeof(UnpredWork));
     h.o_mid = (uint32_t)off;
-    off = align16(off + b.mid.size() * sizeof(RoiBox));
+    off = align16(off + b.mid.size() * sizeof(RoiJob));
     h.o_req = (uint32_t)off;
-    off = align16(off + b.req.size() * sizeof(ReqDesc));
+    off = align16(off + b.req.size() * sizeof(RoiJob));
     if (off > ss.meta_cap) return 0;
     std::memcpy(dst, &h, sizeof h);
     if (!b.work.empty()) std::memcpy(dst + h.o_work, b.work.data(), b.work.size() * sizeof(CtaWork));
     if (!b.ids.empty()) std::memcpy(dst + h.o_ids, b.ids.data(), b.ids.size() * 4);
     if (!b.uw.empty()) std::memcpy(dst + h.o_uwork, b.uw.data(), b.uw.size() * sizeof(UnpredWork));
-    if (!b.mid.empty()) std::memcpy(dst + h.o_mid, b.mid.data(), b.mid.size() * sizeof(RoiBox));
-    if (!b.req.empty()) std::memcpy(dst + h.o_req, b.req.data(), b.req.size() * sizeof(ReqDesc));
+    if (!b.mid.empty()) std::memcpy(dst + h.o_mid, b.mid.data(), b.mid.size() * sizeof(RoiJob));
+    if (!b.req.empty()) std::memcpy(dst + h.o_req, b.req.data(), b.req.size() * sizeof(RoiJob));
     return off;
 }
 
@@ -339,10 +337,11 @@ void enqueue_kernels(const SrvStream& ss, const LaunchShape& sh, const uint8_t* 
     launch_decode_dyn(sh.decode_grid, meta, p.d_sd, p.d_sym, p.d_len, p.d_sub, p.d_choff, p.d_payload, codes, st);
     if (p.total_unpred)
         launch_unpred_scatter_dyn<T>(sh.unpred_grid, meta, p.d_sd, codes, ss.unpred.as<T>(), (T*)p.d_ulist, st);
-    launch_roi_mid_dyn<T>(sh.roi_grid, sh.roi_block, meta, p.base->as<T>(), ss.low, ss.qlow, ss.predictor,
-                          ss.low_codes(), ss.low_unpred<T>(), ss.mid.as<T>(), st);
-    launch_roi_req_dyn<T>(sh.roi_grid, sh.roi_block, meta, ss.mid.as<T>(), p.base->as<T>(), ss.low, ss.high, ss.qhigh,
-                          ss.predictor, ss.high_codes(), ss.high_unpred<T>(), st);
+    const T* base = p.base->as<T>();
+    launch_roi_cells<T>(sh.roi_grid, sh.roi_block, meta, 0, base, ss.low, base, ss.low, ss.qlow, ss.predictor,
+                        ss.low_codes(), ss.low_unpred<T>(), st);
+    launch_roi_cells<T>(sh.roi_grid, sh.roi_block, meta, 1, ss.mid.as<T>(), ss.high, base, ss.low, ss.qhigh,
+                        ss.predictor, ss.high_codes(), ss.high_unpred<T>(), st);
 }
 
 template <typename T>
@@ -453,9 +452,8 @@ stz_status autotune(stz_server* S, SrvStream& ss)
         const float t = time_shape(c);
         if (t < tbest) tbest = t, best = c;
     }
-    for (int blk : {128, 256, 512})
+    for (int blk : {128, 256})  // k_roi_cells is built for at most 256 threads
         for (int per_sm : {2, 4, 8, 16}) {
-            if (blk * per_sm > 2048) continue;
             LaunchShape c = best;
             c.roi_block = blk;
             c.roi_grid = 148 * per_sm;
@@ -729,9 +727,8 @@ stz_status stz_server_add_stream(stz_server* S, const void* data, size_t size, i
     ss->stamp_off[14] = nch;
     ss->stamp.assign(nch, 0u);
     ss->meta_cap = align16(sizeof(BatchHdr)) + align16(nch * sizeof(CtaWork)) + align16(nch * 4) +
-                   align16(nch * sizeof(UnpredWork)) +
-                   align16((size_t)S->opts.max_batch * kMaxRegionsPerBox * sizeof(RoiBox)) +
-                   align16((size_t)S->opts.max_batch * sizeof(ReqDesc)) + 256;
+                   align16(nch * sizeof(UnpredWork)) + 2 * align16((size_t)S->opts.max_batch * sizeof(RoiJob)) +
+                   256;
     for (int k = 0; k < S->opts.slots; ++k) STZ_CUDA(ss->meta[k].ensure(ss->meta_cap));
     if (S->opts.autotune) STZ_TRY(autotune(S, *ss));
     STZ_TRY(capture_graphs(S, *ss));

@@ -71,7 +71,7 @@ struct CtaWork {
 };
 
 // Header of a request batch in device memory (request server). The arrays
-// (CtaWork, chunk ids, UnpredWork, RoiBox mid regions, ReqDesc outputs)
+// (CtaWork, chunk ids, UnpredWork, low-level and high-level ROI job lists)
 // follow at the given byte offsets from the header's start.
 struct BatchHdr {
     uint32_t n_work, n_uwork, n_mid, n_req;

@@ -180,6 +180,18 @@ def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
 
 
+def _torch_sync(*ts) -> None:
+    """The library works on its own CUDA stream: finish the work torch has
+    queued on these tensors' devices before the library reads or writes them."""
+    done = set()
+    for t in ts:
+        if t is not None and _is_torch(t) and t.is_cuda and t.device not in done:
+            import torch
+
+            torch.cuda.current_stream(t.device).synchronize()
+            done.add(t.device)
+
+
 @dataclass
 class StreamInfo:
     dtype: type
@@ -293,6 +305,7 @@ class Context:
                 raise ValueError("field must be a contiguous 3-D tensor (z, y, x)")
             code = {torch.float32: STZ_F32, torch.float64: STZ_F64}[field.dtype]
             nz, ny, nx = field.shape
+            _torch_sync(field)
             fn = self.lib.stz_compress_dev if field.is_cuda else self.lib.stz_compress
             _check(fn(self._c, C.c_void_p(field.data_ptr()), code, nx, ny, nz, C.byref(o), C.byref(h)))
         else:
@@ -323,6 +336,7 @@ class Context:
         if out is not None and _is_torch(out) and out.is_cuda:
             if tuple(out.shape) != shape:
                 raise ValueError(f"out must have shape {shape}")
+            _torch_sync(out)
             _check(self.lib.stz_decompress_level_dev(self._c, s.handle, level, C.c_void_p(out.data_ptr()), dims))
             return out
         res = np.empty(shape, dtype=inf.dtype) if out is None else out
@@ -347,6 +361,7 @@ class Context:
         shape = (ext[2], ext[1], ext[0])
         od = (C.c_size_t * 3)()
         if out is not None and _is_torch(out) and out.is_cuda:
+            _torch_sync(out)
             _check(self.lib.stz_decompress_box_dev(self._c, s.handle, a, b, C.c_void_p(out.data_ptr()), od))
             return out
         res = np.empty(shape, dtype=inf.dtype)
@@ -363,7 +378,10 @@ class Context:
         return buf[: n.value].copy()
 
     # ---- reference function boundary (torch CUDA tensors) ------------------
+    # These entry points are asynchronous on the context's stream: inputs are
+    # made ready first (_p), and outputs are ready after ctx.sync().
     def _p(self, t):
+        _torch_sync(t)
         return C.c_void_p(t.data_ptr())
 
     def split(self, full, subs):
