@@ -56,6 +56,8 @@ def parse_args():
                    help="one compress + one full decompress of the workload, no timing (profiler captures)")
     p.add_argument("--no-serve", action="store_true", help="skip the request-server latency measurement")
     p.add_argument("--serve-only", action="store_true", help="only the request-server latency measurement")
+    p.add_argument("--serve-trace", default="",
+                   help="write per-request (arrival s, queue ms, latency ms, batch, batch size) arrays to this .npz")
     p.add_argument("--serve-size", type=int, default=1024, help="edge of the resident serving field")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="length of each serving load run")
     return p.parse_args()
@@ -269,7 +271,7 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
             ready.release()
 
     lat = {"box": [], "slice": [], "level": []}
-    batch_sizes, out_bytes, queue, order = [], 0, [], []
+    batch_sizes, out_bytes, queue, order, trace = [], 0, [], [], []
     th = threading.Thread(target=producer)
     t0 = time.perf_counter()
     th.start()
@@ -285,6 +287,7 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
         lat[reqs[i][0]].append(res.latency_ms)
         order.append(res.latency_ms)
         queue.append(res.queue_ms)
+        trace.append((arrivals[i], res.queue_ms, res.latency_ms, res.batch, res.batch_size))
         batch_sizes.append(res.batch_size)
         out_bytes += res.nbytes
     wall = time.perf_counter() - t0
@@ -301,6 +304,7 @@ def serve_load(srv, sid, dims_xyz, K, rate, seconds, gen, seed):
     for k, v in lat.items():
         if v:
             out[k] = {"n": len(v), "p50_ms": _pct(v, 50), "p99_ms": _pct(v, 99)}
+    out["_trace"] = trace
     return out
 
 
@@ -353,8 +357,17 @@ def serving_bench(args, ctx, local):
            "probe_box_max_err_over_bound": probe_err, "add_stream_s": add_s, "shapes": srv.stats()}
     sec = args.serve_seconds
     serve_load(srv, sid, dims, K, 500, 0.2, box64, 1)  # warm-up
-    res["box64"] = [serve_load(srv, sid, dims, K, r, sec, box64, 10 + i) for i, r in enumerate((2000, 10000))]
+    traces = {}
+    res["box64"] = []
+    for i, r in enumerate((2000, 10000)):
+        res["box64"].append(serve_load(srv, sid, dims, K, r, sec, box64, 10 + i))
+        traces[f"box64_{r}_batches"] = srv.batch_log()
     res["mixed"] = serve_load(srv, sid, dims, K, 1000, sec, mixed, 20)
+    traces["mixed_batches"] = srv.batch_log()
+    for name, r in (("box64_2k", res["box64"][0]), ("box64_10k", res["box64"][1]), ("mixed", res["mixed"])):
+        traces[name] = np.asarray(r.pop("_trace", []), dtype=np.float64)
+    if args.serve_trace:
+        np.savez(args.serve_trace, **traces)
     srv.close()
     # unbatched baseline: the single-request API on the resident stream
     ctx.upload(s)

@@ -256,8 +256,10 @@ stz_status stz_plan_box(size_t nx, size_t ny, size_t nz, int chunk_high, int chu
  * kernel over the union of the batch's marker chunks, one low-level kernel
  * over all mid-grid regions and one high-level kernel over all outputs.
  * Requests that arrive while a batch is on the GPU join the next batch.
- * Results do not depend on the batch a request lands in.
- * All functions are thread-safe. */
+ * Full-resolution and half-resolution requests (levels 0 and 1) run in a
+ * separate lane on a low-priority CUDA stream, so boxes and slices do not
+ * wait behind them. Results do not depend on the batch or lane a request
+ * lands in. All functions are thread-safe. */
 typedef struct stz_server stz_server;
 
 typedef struct stz_server_opts {
@@ -266,6 +268,8 @@ typedef struct stz_server_opts {
     int slots;          /* batches in flight (pinned + device batch buffers); 0 = 2 */
     int autotune;       /* 1 = time launch shapes on each added stream and keep the fastest */
     int threads;        /* host threads for zstd on stream upload; 0 = all cores */
+    size_t fast_reserve; /* arena bytes level 0/1 outputs may not take (kept for boxes,
+                            slices, coarse levels); (size_t)-1 = a quarter of the arena */
 } stz_server_opts;
 
 typedef enum stz_request_kind {
@@ -297,6 +301,21 @@ typedef struct stz_server_stats {
     size_t arena_bytes, arena_in_use;
 } stz_server_stats;
 
+/* One batch of the server's recent history (times in ms since the server was
+ * created; device_ms = CUDA-event time from the batch record's copy to its
+ * last kernel, -1 until known). */
+typedef struct stz_batch_record {
+    uint64_t batch;
+    int n_requests;
+    int lane;             /* 0 = fast (boxes, slices, levels >= 2), 1 = bulk (levels 1 and 0) */
+    int slot;
+    double t_start_ms;    /* worker took the batch */
+    double t_planned_ms;  /* host planning and packing done */
+    double t_launched_ms; /* all of the batch's GPU work enqueued */
+    double t_done_ms;     /* the completion thread saw its end event */
+    double device_ms;
+} stz_batch_record;
+
 void stz_server_default_opts(stz_server_opts* o);
 stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server** out);
 /* Stops the worker after the batches in flight; pending requests fail with
@@ -316,6 +335,9 @@ stz_status stz_server_copy_out(stz_server* srv, uint64_t ticket, void* host);
 /* Return a completed ticket's output memory to the arena. */
 stz_status stz_server_release(stz_server* srv, uint64_t ticket);
 stz_status stz_server_stats_get(stz_server* srv, stz_server_stats* st);
+/* The most recent batches (up to 4096 are kept), oldest first: up to cap
+ * records into out, the number written in *n. */
+stz_status stz_server_batch_log(stz_server* srv, stz_batch_record* out, size_t cap, size_t* n);
 
 /* ---- inspection (tests) --------------------------------------------------- */
 /* Quant codes of one residual stream in chunk-major order (the entropy

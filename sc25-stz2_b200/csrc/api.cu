@@ -744,10 +744,12 @@ template <typename T>
 stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[3], const int64_t hi[3], T* out_dev,
                               size_t odims[3])
 {
+    Lap lap("box");
     const ParsedStream& ps = s->dir;
     const FileHeader& h = ps.h;
     const int K = h.K;
     const QueryPlan plan = plan_query(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low, lo, hi);
+    lap.mark("plan");
     if (odims) {
         odims[0] = (size_t)(plan.q[0].e - plan.q[0].b + 1);
         odims[1] = (size_t)(plan.q[1].e - plan.q[1].b + 1);
@@ -785,6 +787,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         add_work(work, ids, si, cs.data(), cs.size(), high.C);
         add_unpred_work(*p, si, cs.data(), cs.size(), uw);
     }
+    lap.mark("work lists");
     // ROI jobs: the mid grid on the bounding box of the reference regions,
     // then the query box
     STZ_CUDA(ctx->mid.ensure(8 * nbase * elem));
@@ -824,6 +827,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     std::memcpy(hm + hd.o_req, rj.data(), rj.size() * sizeof(RoiJob));
     STZ_CUDA(ctx->work.ensure(off));
     STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hm, off, cudaMemcpyHostToDevice, ctx->st));
+    lap.mark("record + copy");
     const uint8_t* dm = ctx->work.as<uint8_t>();
     STZ_CUDA(ctx->codes.ensure(p->total_codes * 2));
     if (p->total_unpred) STZ_CUDA(ctx->unpred_dense.ensure(p->total_codes * sizeof(T)));
@@ -853,7 +857,9 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
                             ud ? ud + hi_off : nullptr, ctx->st);
     }
     STZ_CUDA(cudaGetLastError());
+    lap.mark("launches");
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    lap.mark("device");
     return STZ_OK;
 }
 

@@ -214,11 +214,19 @@ __global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restr
 // Decode: each thread decodes one plane with a 2^kLutBits-entry table in
 // shared memory (symbol | length << 16); longer codes fall back to the
 // canonical first-code test per length.
+// Symbols of codes longer than kLutBits kept in shared memory (the rest of a
+// longer tail is read from global memory).
+constexpr int kTailSyms = 4096;
+
+// lut entry: sym | len << 16 for codes of at most kLutBits bits; for a prefix
+// of longer codes, l_min << 24 with l_min the shortest code length under that
+// prefix (the canonical length search starts there); 0 for a prefix of no code.
 struct DecodeSmem {
     uint32_t lut[1 << kLutBits];
     uint32_t cnt[kMaxCodeLen + 1];
     uint32_t first_code[kMaxCodeLen + 1];
     uint32_t first_idx[kMaxCodeLen + 1];
+    uint16_t tail[kTailSyms];
 };
 
 // Build the decode tables of stream s (all threads of the block).
@@ -247,7 +255,8 @@ __device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_
     }
     __syncthreads();
     // every table entry finds its code: the shortest length whose canonical
-    // range holds the entry's prefix (entries of no code stay 0: slow path)
+    // range holds the entry's prefix; prefixes of longer codes record the
+    // shortest such length
     for (uint32_t j = threadIdx.x; j < (1u << kLutBits); j += blockDim.x) {
         uint32_t e = 0;
         for (uint32_t l = 1; l <= (uint32_t)kLutBits; ++l) {
@@ -257,8 +266,21 @@ __device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_
                 break;
             }
         }
+        if (!e) {
+            for (uint32_t l = kLutBits + 1; l <= (uint32_t)kMaxCodeLen; ++l) {
+                if (!cnt[l]) continue;
+                const uint32_t sh = l - kLutBits;
+                if (j >= (first_code[l] >> sh) && j <= ((first_code[l] + cnt[l] - 1) >> sh)) {
+                    e = l << 24;
+                    break;
+                }
+            }
+        }
         lut[j] = e;
     }
+    const uint32_t t0 = first_idx[kLutBits + 1];
+    for (uint32_t i = threadIdx.x; i < (uint32_t)kTailSyms && t0 + i < s.n_used; i += blockDim.x)
+        sm.tail[i] = cb_sym[s.cb_off + t0 + i];
     __syncthreads();
 }
 
@@ -290,37 +312,59 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
     // words of the stream left from this chunk's start; reads beyond read 0
     const uint64_t lim = s.word_cap > cw ? s.word_cap - cw : 0;
     auto rd = [&](uint64_t i) -> uint32_t { return i < lim ? __ldg(in + i) : 0u; };
-    const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
-    uint64_t wi = b0 >> 5;
-    // 64-bit window, MSB = next bit.
-    uint64_t buf = (((uint64_t)rd(wi) << 32) | rd(wi + 1)) << (b0 & 31);
-    int avail = 64 - (int)(b0 & 31);
-    wi += 2;
+    uint32_t pos = sub_off[s.sub_base + (size_t)c * C + lz];  // bit position from the chunk's first word
+    // The plane's payload lines are prefetched into L1 up front (its end is
+    // the next plane's start, or the chunk's end), so the loads below hit L1.
+    {
+        const uint64_t cwords = chunk_word_off[s.chunk_base + c + 1] - cw;
+        const uint64_t b1 = lz + 1 < C ? (uint64_t)sub_off[s.sub_base + (size_t)c * C + lz + 1] : 32 * cwords;
+        const uint64_t w1 = min(min((b1 + 31) >> 5, cwords) + 2, lim);
+        for (uint64_t w = (pos >> 5) & ~31u; w < w1; w += 32) asm volatile("prefetch.global.L1 [%0];" ::"l"(in + w));
+    }
+    // 64-bit bit reservoir, MSB = next bit, `avail` valid bits (>= kLutBits
+    // at every symbol start). The dependency chain of a symbol is only
+    // table index -> lookup -> length -> shift: the refill word is merged in
+    // (below the valid bits, from the length-independent `avail`) while the
+    // lookup is in flight, and the next word is loaded one refill ahead.
+    uint64_t wi = pos >> 5;
+    uint64_t buf = (((uint64_t)rd(wi) << 32) | rd(wi + 1)) << (pos & 31);
+    int avail = 64 - (int)(pos & 31);
+    uint32_t w = rd(wi + 2);
+    wi += 3;
     auto next = [&]() -> uint32_t {
-        if (avail < 32) {
-            buf |= (uint64_t)rd(wi) << (32 - avail);
-            avail += 32;
-            ++wi;
-        }
-        const uint32_t e = lut[buf >> (64 - kLutBits)];
-        uint32_t sym, l = e >> 16;
-        if (l) {
-            sym = e & 0xffffu;
-        } else {
-            // a corrupt stream still yields a symbol of this codebook (never
+        const uint32_t e = lut[(uint32_t)(buf >> (64 - kLutBits))];
+        const bool rf = avail < 32;
+        const uint64_t b2 = rf ? (buf | ((uint64_t)w << (32 - avail))) : buf;  // >= 32 valid bits
+        const int a2 = rf ? avail + 32 : avail;
+        if (rf) w = rd(wi++);
+        uint32_t sym = e & 0xffffu, l = (e >> 16) & 0xffu;
+        if (!l) {
+            // canonical search from the shortest length under this prefix; a
+            // corrupt stream still yields a symbol of this codebook (never
             // code 0 unless the stream has unpredictable values)
-            sym = cb_sym[s.cb_off];
-            for (l = kLutBits + 1; l <= (uint32_t)kMaxCodeLen; ++l) {
-                const uint32_t v = (uint32_t)(buf >> (64 - l));
+            l = e >> 24;
+            if (!l) l = kLutBits + 1;
+            for (; l <= (uint32_t)kMaxCodeLen; ++l) {
+                const uint32_t v = (uint32_t)(b2 >> (64 - l));
                 if (v - first_code[l] < cnt[l]) {
-                    sym = cb_sym[s.cb_off + first_idx[l] + (v - first_code[l])];
+                    const uint32_t idx = first_idx[l] + (v - first_code[l]);
+                    const uint32_t ti = idx - first_idx[kLutBits + 1];
+                    sym = ti < (uint32_t)kTailSyms ? sm.tail[ti] : cb_sym[s.cb_off + idx];
                     break;
                 }
             }
-            if (l > (uint32_t)kMaxCodeLen) l = 1;  // corrupt stream: keep going, the result is garbage
+            if (l > (uint32_t)kMaxCodeLen) {
+                sym = cb_sym[s.cb_off];
+                l = 1;  // corrupt stream: keep going, the result is garbage
+            }
         }
-        buf <<= l;
-        avail -= (int)l;
+        buf = b2 << l;
+        avail = a2 - (int)l;
+        if (avail < kLutBits) {  // only after a long code taken without a refill
+            buf |= (uint64_t)w << (32 - avail);
+            avail += 32;
+            w = rd(wi++);
+        }
         return sym;
     };
     if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {

@@ -12,19 +12,28 @@
 //            (each chunk decoded once per batch), pack one batch record;
 //   device : one H2D copy of the record, then one graph replay per stream:
 //            k_decode_dyn (all chunks) -> k_unpred_scatter_dyn ->
-//            k_roi_mid_dyn (all mid regions) -> k_roi_req_dyn (all outputs).
+//            k_roi_cells (the mid-grid windows) -> k_roi_cells (all outputs).
 // Progressive levels >= 2 are strided samples of the resident decoded base
-// (the decoded grid of level l+1 is the even-parity sub-grid of level l);
-// levels 1 and 0 add full level decodes after the graph.
+// (the decoded grid of level l+1 is the even-parity sub-grid of level l) and
+// ride in the same graph.
+//
+// Two lanes, each with its own CUDA stream, batch slots and completion
+// thread: the fast lane (boxes, slices, levels >= 2) on a high-priority
+// stream, and the bulk lane (full decodes of levels 1 and 0, whole-grid
+// outputs) on a low-priority stream, so small requests never queue behind a
+// full-resolution decode. Both lanes write the stream's shared decode
+// buffers (codes, mid grid) only with the values a full decode gives, so
+// their overlap cannot change a result.
 //
 // Admission: a request is taken from the queue when its output fits in the
-// output arena and a batch slot (pinned + device record buffers) is free;
-// requests that arrive while batches run join the next batch.
+// output arena and a slot of its lane is free; requests that arrive while
+// batches run join the next batch of their lane.
 #include <cuda_runtime.h>
 
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <list>
 #include <map>
 #include <mutex>
 #include <thread>
@@ -39,6 +48,9 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr int kMaxSlots = 8;
+constexpr size_t kLogSize = 4096;
+constexpr int kLaneFast = 0, kLaneBulk = 1, kLanes = 2;
+constexpr int kBulkSlots = 1, kBulkBatch = 8;
 
 double ms_between(Clock::time_point a, Clock::time_point b)
 {
@@ -91,7 +103,17 @@ public:
     }
     size_t capacity() const { return cap_; }
     size_t used() const { return used_; }
-    bool fits_ever(size_t bytes) const { return align256(std::max<size_t>(bytes, 1)) <= cap_; }
+    // An allocation of `bytes` that leaves at least `reserve` bytes unused
+    // could be made some day / now.
+    bool fits_ever(size_t bytes, size_t reserve = 0) const
+    {
+        return reserve <= cap_ && align256(std::max<size_t>(bytes, 1)) <= cap_ - reserve;
+    }
+    bool alloc_leaving(size_t bytes, size_t reserve, size_t& off)
+    {
+        if (!fits_ever(bytes, reserve) || used_ + align256(std::max<size_t>(bytes, 1)) > cap_ - reserve) return false;
+        return alloc(bytes, off);
+    }
 
 private:
     std::map<size_t, size_t> free_;
@@ -119,8 +141,8 @@ struct SrvStream {
     uint64_t stamp_off[15] = {};
     uint32_t epoch = 0;
     size_t meta_cap = 0;
-    DevBuf meta[kMaxSlots];
-    cudaGraphExec_t graph[kMaxSlots] = {};
+    DevBuf meta[kLanes][kMaxSlots];          // batch records on the device, per lane and slot
+    cudaGraphExec_t graph[kMaxSlots] = {};  // fast-lane batch kernels, per slot
     LaunchShape shape;
     ~SrvStream()
     {
@@ -145,6 +167,7 @@ struct SrvStream {
 struct Ticket {
     stz_request req{};
     SrvStream* ss = nullptr;
+    int lane = kLaneFast;
     int state = 0;  // 0 queued, 1 in a batch, 2 done
     stz_status status = STZ_OK;
     std::string error;
@@ -155,7 +178,7 @@ struct Ticket {
     int batch_size = 0;
 };
 
-// A level request's full decodes, run after the batch graph.
+// A level request's full decodes (bulk lane).
 struct LevelJob {
     SrvStream* ss;
     int level;  // 0 or 1
@@ -174,7 +197,31 @@ struct Build {
     std::vector<LevelJob> jobs;
 };
 
-struct BatchDone;
+// A launched batch waiting for its end event.
+struct InFlight {
+    int slot;
+    uint64_t batch;
+    std::vector<uint64_t> ids;
+};
+
+// One lane: a CUDA stream, its batch slots (pinned record buffers, events
+// bracketing each batch's GPU work) and the batches in flight on it.
+struct Lane {
+    cudaStream_t st = nullptr;
+    int slots = 0;
+    bool busy[kMaxSlots] = {};
+    PinBuf hmeta[kMaxSlots];
+    cudaEvent_t ev_a[kMaxSlots] = {}, ev_b[kMaxSlots] = {};
+    std::deque<InFlight> inflight;
+    std::condition_variable cv;
+    std::thread completer;
+    int free_slot() const
+    {
+        for (int k = 0; k < slots; ++k)
+            if (!busy[k]) return k;
+        return -1;
+    }
+};
 
 }  // namespace
 }  // namespace stz
@@ -186,49 +233,69 @@ struct stz_server {
     stz_server_opts opts{};
     DevBuf arena_buf;
     Arena arena;
-    std::mutex mu;  // queue, tickets, slots, arena, stats
+    std::mutex mu;  // queue, tickets, lane slots and in-flight lists, arena, stats
     std::condition_variable cv_work, cv_done;
-    std::deque<uint64_t> queue;
+    std::list<uint64_t> queue;
     std::unordered_map<uint64_t, Ticket> tickets;
     uint64_t next_ticket = 1;
     std::vector<std::unique_ptr<SrvStream>> streams;
-    std::vector<bool> slot_busy;
-    PinBuf hmeta[kMaxSlots];
+    Lane lanes[kLanes];
     std::mutex exec_mu;  // GPU submission (worker batches vs stream upload / capture)
-    std::thread worker;
-    bool stop = false;
+    std::thread worker;  // admits, plans and launches batches
+    bool stop = false, stop_completers = false;
     uint64_t submitted = 0, completed = 0, batches = 0;
     LaunchShape last_shape;
+    // batch history (ring)
+    Clock::time_point t0 = Clock::now();
+    std::vector<stz_batch_record> log = std::vector<stz_batch_record>(kLogSize);
+    double ms_now() const { return ms_between(t0, Clock::now()); }
+    stz_batch_record& rec(uint64_t batch) { return log[batch % kLogSize]; }
 };
 
 namespace stz {
 namespace {
 
-struct BatchDone {
-    stz_server* S;
-    int slot;
-    std::vector<uint64_t> ids;
-};
-
-void CUDART_CB batch_done(void* arg)
+// Completion thread of one lane: its batches finish in launch order (one
+// CUDA stream), so it waits on the oldest batch's end event, then publishes
+// its results and frees its slot. (A host-function callback in the stream
+// would hold back the next batch's kernels until the driver ran it.)
+void completer_main(stz_server* S, int lane)
 {
-    BatchDone* d = static_cast<BatchDone*>(arg);
-    stz_server* S = d->S;
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
+    cudaSetDevice(S->ctx->device);
+    Lane& L = S->lanes[lane];
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        L.cv.wait(lk, [&]() { return S->stop_completers || !L.inflight.empty(); });
+        if (L.inflight.empty()) break;  // stopping, nothing left in flight
+        const int slot = L.inflight.front().slot;
+        lk.unlock();
+        const cudaError_t e = cudaEventSynchronize(L.ev_b[slot]);
+        float ms = -1.f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, L.ev_a[slot], L.ev_b[slot]);
+        lk.lock();
+        InFlight f = std::move(L.inflight.front());
+        L.inflight.pop_front();
         const auto now = Clock::now();
-        for (uint64_t id : d->ids) {
+        stz_batch_record& r = S->rec(f.batch);
+        r.t_done_ms = ms_between(S->t0, now);
+        r.device_ms = ms;
+        for (uint64_t id : f.ids) {
             auto it = S->tickets.find(id);
             if (it == S->tickets.end()) continue;
-            it->second.state = 2;
-            it->second.t_done = now;
+            Ticket& t = it->second;
+            if (e != cudaSuccess) {
+                S->arena.release(t.off, t.bytes);
+                t.status = STZ_ERR_CUDA;
+                t.error = std::string("batch failed on the device: ") + cudaGetErrorString(e);
+            }
+            t.state = 2;
+            t.t_done = now;
         }
-        S->slot_busy[d->slot] = false;
-        S->completed += d->ids.size();
+        L.busy[f.slot] = false;
+        S->completed += f.ids.size();
+        S->cv_done.notify_all();
+        S->cv_work.notify_all();
     }
-    S->cv_done.notify_all();
-    S->cv_work.notify_all();
-    delete d;
 }
 
 uint32_t chunk_count(const SrvStream& ss, int j) { return ss.sd(j < 7 ? ss.low_s0 + j : ss.high_s0 + j - 7).nchunks; }
@@ -256,12 +323,22 @@ void plan_request(SrvStream& ss, Build& b, const Ticket& t, void* out)
     const stz_request& r = t.req;
     if (r.kind == STZ_REQ_BOX) {
         const QueryPlan plan = plan_query(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low, r.lo, r.hi);
-        for (const BlockPlan& bp : plan.low)
-            for (int64_t c : bp.chunks) list_chunk(ss, b, bp.block, (uint32_t)c);
         for (const BlockPlan& bp : plan.high)
             for (int64_t c : bp.chunks) list_chunk(ss, b, 7 + bp.block, (uint32_t)c);
         int m0[3], m1[3];
         if (region_bbox(plan, m0, m1)) {
+            // The mid grid is rebuilt on the regions' bounding box: decode the
+            // low chunks of every cell of that box (a superset of the
+            // planner's low chunks, FD5:1784-1830), so every mid value written
+            // is the full decode's value.
+            const int C = ss.low.C;
+            const int c0[3] = {(m0[0] >> 1) / C, (m0[1] >> 1) / C, (m0[2] >> 1) / C};
+            const int c1[3] = {(m1[0] >> 1) / C, (m1[1] >> 1) / C, (m1[2] >> 1) / C};
+            for (int blk = 0; blk < 7; ++blk)
+                for (int cz = c0[2]; cz <= c1[2]; ++cz)
+                    for (int cy = c0[1]; cy <= c1[1]; ++cy)
+                        for (int cx = c0[0]; cx <= c1[0]; ++cx)
+                            list_chunk(ss, b, blk, (uint32_t)((cz * ss.low.ncy + cy) * ss.low.ncx + cx));
             const int o0[3] = {0, 0, 0};
             b.mid.push_back(cells_job(m0, m1, ss.mid.p, o0, 2 * (uint64_t)ss.low.dx,
                                       4 * (uint64_t)ss.low.dx * ss.low.dy, b.mid_total));
@@ -374,9 +451,10 @@ stz_status capture_graphs(stz_server* S, SrvStream& ss)
             cudaGraphExecDestroy(ss.graph[k]);
             ss.graph[k] = nullptr;
         }
+        const uint8_t* meta = ss.meta[kLaneFast][k].as<uint8_t>();
         STZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        if (ss.dtype == 1) enqueue_kernels<double>(ss, ss.shape, ss.meta[k].as<uint8_t>(), st);
-        else enqueue_kernels<float>(ss, ss.shape, ss.meta[k].as<uint8_t>(), st);
+        if (ss.dtype == 1) enqueue_kernels<double>(ss, ss.shape, meta, st);
+        else enqueue_kernels<float>(ss, ss.shape, meta, st);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(st, &g);
         if (e != cudaSuccess) {
@@ -423,10 +501,12 @@ stz_status autotune(stz_server* S, SrvStream& ss)
         plan_request(ss, b, t, out.as<uint8_t>() + o * ss.elem);
         o += t.dims[0] * t.dims[1] * t.dims[2];
     }
-    STZ_CUDA(S->hmeta[0].ensure(ss.meta_cap));
-    const size_t bytes = pack(ss, b, S->hmeta[0].as<uint8_t>());
+    PinBuf& hm = S->lanes[kLaneFast].hmeta[0];
+    const uint8_t* meta = ss.meta[kLaneFast][0].as<uint8_t>();
+    STZ_CUDA(hm.ensure(ss.meta_cap));
+    const size_t bytes = pack(ss, b, hm.as<uint8_t>());
     if (!bytes) STZ_FAIL(STZ_ERR_RANGE, "tuning batch exceeds the batch record");
-    STZ_CUDA(cudaMemcpyAsync(ss.meta[0].p, S->hmeta[0].p, bytes, cudaMemcpyHostToDevice, st));
+    STZ_CUDA(cudaMemcpyAsync(ss.meta[kLaneFast][0].p, hm.p, bytes, cudaMemcpyHostToDevice, st));
     cudaEvent_t e0, e1;
     STZ_CUDA(cudaEventCreate(&e0));
     STZ_CUDA(cudaEventCreate(&e1));
@@ -434,8 +514,8 @@ stz_status autotune(stz_server* S, SrvStream& ss)
         float best = 1e30f;
         for (int rep = 0; rep < 4; ++rep) {
             cudaEventRecord(e0, st);
-            if (ss.dtype == 1) enqueue_kernels<double>(ss, sh, ss.meta[0].as<uint8_t>(), st);
-            else enqueue_kernels<float>(ss, sh, ss.meta[0].as<uint8_t>(), st);
+            if (ss.dtype == 1) enqueue_kernels<double>(ss, sh, meta, st);
+            else enqueue_kernels<float>(ss, sh, meta, st);
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -468,19 +548,31 @@ stz_status autotune(stz_server* S, SrvStream& ss)
     return STZ_OK;
 }
 
+// Bulk lane: every chunk of the levels the batch's full decodes need, then
+// the level decodes (hrec: host copy of the record at drec).
 template <typename T>
-cudaError_t enqueue_batch_stream(SrvStream& ss, int slot, const std::vector<LevelJob>& jobs, cudaStream_t st)
+cudaError_t enqueue_bulk(SrvStream& ss, const uint8_t* hrec, const uint8_t* drec, const std::vector<LevelJob>& jobs,
+                         cudaStream_t st)
 {
-    const cudaError_t e = cudaGraphLaunch(ss.graph[slot], st);
-    if (e != cudaSuccess) return e;
+    const BatchHdr* h = reinterpret_cast<const BatchHdr*>(hrec);
+    const Prepared& p = *ss.p;
+    uint16_t* codes = ss.codes.as<uint16_t>();
+    if (h->n_work)
+        launch_decode(reinterpret_cast<const CtaWork*>(drec + h->o_work),
+                      reinterpret_cast<const uint32_t*>(drec + h->o_ids), (int)h->n_work, p.d_sd, p.d_sym, p.d_len,
+                      p.d_sub, p.d_choff, p.d_payload, codes, st);
+    if (h->n_uwork)
+        launch_unpred_move<T>(false, reinterpret_cast<const UnpredWork*>(drec + h->o_uwork), (int)h->n_uwork, p.d_sd,
+                              codes, ss.unpred.as<T>(), (T*)p.d_ulist, st);
     for (const LevelJob& j : jobs) enqueue_level_job<T>(ss, j, st);
     return cudaGetLastError();
 }
 
-// Plan, pack and enqueue one batch (worker thread, exec_mu held).
-stz_status launch_batch(stz_server* S, int slot, uint64_t bid, const std::vector<uint64_t>& ids)
+// Plan, pack and enqueue one batch on a lane (worker thread, exec_mu held).
+stz_status launch_batch(stz_server* S, int lane, int slot, uint64_t bid, const std::vector<uint64_t>& ids)
 {
-    cudaStream_t st = S->ctx->st;
+    Lane& L = S->lanes[lane];
+    cudaStream_t st = L.st;
     // group by stream, keep arrival order inside a group
     std::vector<SrvStream*> order;
     std::unordered_map<SrvStream*, std::vector<Ticket*>> groups;
@@ -495,36 +587,89 @@ stz_status launch_batch(stz_server* S, int slot, uint64_t bid, const std::vector
             if (!groups.count(t.ss)) order.push_back(t.ss);
             groups[t.ss].push_back(&t);
         }
+        stz_batch_record& r = S->rec(bid);
+        r = stz_batch_record{};
+        r.batch = bid;
+        r.n_requests = (int)ids.size();
+        r.slot = slot;
+        r.lane = lane;
+        r.t_start_ms = ms_between(S->t0, now);
+        r.t_planned_ms = r.t_launched_ms = r.t_done_ms = r.device_ms = -1.0;
     }
     uint8_t* arena = S->arena_buf.as<uint8_t>();
-    size_t hoff = 0;
-    // every group's record goes to its own region of the slot's pinned buffer
+    // plan and pack every group into its own region of the slot's pinned buffer
     size_t need = 0;
     for (SrvStream* ss : order) need += align256(ss->meta_cap);
-    STZ_CUDA(S->hmeta[slot].ensure(need));
-    for (SrvStream* ss : order) {
-        Build b;
+    STZ_CUDA(L.hmeta[slot].ensure(need));
+    uint8_t* hbase = L.hmeta[slot].as<uint8_t>();
+    std::vector<Build> builds(order.size());
+    std::vector<size_t> bytes(order.size()), hoff(order.size());
+    size_t off = 0;
+    for (size_t g = 0; g < order.size(); ++g) {
+        SrvStream* ss = order[g];
         ++ss->epoch;
         if (ss->epoch == 0) {  // wrapped: clear the stamps
             std::fill(ss->stamp.begin(), ss->stamp.end(), 0u);
             ss->epoch = 1;
         }
-        for (Ticket* t : groups[ss]) plan_request(*ss, b, *t, arena + t->off);
-        uint8_t* hm = S->hmeta[slot].as<uint8_t>() + hoff;
-        const size_t bytes = pack(*ss, b, hm);
-        if (!bytes) STZ_FAIL(STZ_ERR_RANGE, "batch record exceeds its buffer");
-        STZ_CUDA(cudaMemcpyAsync(ss->meta[slot].p, hm, bytes, cudaMemcpyHostToDevice, st));
-        if (ss->dtype == 1) STZ_CUDA((enqueue_batch_stream<double>(*ss, slot, b.jobs, st)));
-        else STZ_CUDA((enqueue_batch_stream<float>(*ss, slot, b.jobs, st)));
-        hoff += align256(ss->meta_cap);
+        for (Ticket* t : groups[ss]) plan_request(*ss, builds[g], *t, arena + t->off);
+        hoff[g] = off;
+        bytes[g] = pack(*ss, builds[g], hbase + off);
+        if (!bytes[g]) STZ_FAIL(STZ_ERR_RANGE, "batch record exceeds its buffer");
+        off += align256(ss->meta_cap);
     }
-    auto* d = new BatchDone{S, slot, ids};
-    const cudaError_t e = cudaLaunchHostFunc(st, batch_done, d);
-    if (e != cudaSuccess) {
-        delete d;
-        STZ_FAIL(STZ_ERR_CUDA, std::string("cudaLaunchHostFunc: ") + cudaGetErrorString(e));
+    const double t_planned = S->ms_now();
+    STZ_CUDA(cudaEventRecord(L.ev_a[slot], st));
+    for (size_t g = 0; g < order.size(); ++g) {
+        SrvStream* ss = order[g];
+        DevBuf& drec = ss->meta[lane][slot];
+        STZ_CUDA(cudaMemcpyAsync(drec.p, hbase + hoff[g], bytes[g], cudaMemcpyHostToDevice, st));
+        if (lane == kLaneFast) STZ_CUDA(cudaGraphLaunch(ss->graph[slot], st));
+        else if (ss->dtype == 1)
+            STZ_CUDA((enqueue_bulk<double>(*ss, hbase + hoff[g], drec.as<uint8_t>(), builds[g].jobs, st)));
+        else STZ_CUDA((enqueue_bulk<float>(*ss, hbase + hoff[g], drec.as<uint8_t>(), builds[g].jobs, st)));
     }
+    STZ_CUDA(cudaEventRecord(L.ev_b[slot], st));
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->rec(bid).t_planned_ms = t_planned;
+        S->rec(bid).t_launched_ms = S->ms_now();
+        L.inflight.push_back(InFlight{slot, bid, ids});
+    }
+    L.cv.notify_one();
     return STZ_OK;
+}
+
+// Admit the next batch (mu held): for the first lane with a free slot and a
+// queued request, take that lane's requests in arrival order while their
+// outputs fit in the arena.
+bool admit(stz_server* S, int& lane, int& slot, std::vector<uint64_t>& ids)
+{
+    for (int ln = 0; ln < kLanes; ++ln) {
+        Lane& L = S->lanes[ln];
+        const int k = L.free_slot();
+        if (k < 0) continue;
+        const int cap = ln == kLaneFast ? S->opts.max_batch : kBulkBatch;
+        ids.clear();
+        for (auto it = S->queue.begin(); it != S->queue.end() && (int)ids.size() < cap;) {
+            Ticket& t = S->tickets[*it];
+            if (t.lane != ln) {
+                ++it;
+                continue;
+            }
+            const size_t reserve = ln == kLaneBulk ? S->opts.fast_reserve : 0;
+            if (!S->arena.alloc_leaving(t.bytes, reserve, t.off)) break;  // the lane keeps its arrival order
+            t.state = 1;
+            ids.push_back(*it);
+            it = S->queue.erase(it);
+        }
+        if (!ids.empty()) {
+            lane = ln;
+            slot = k;
+            return true;
+        }
+    }
+    return false;
 }
 
 void worker_main(stz_server* S)
@@ -532,51 +677,28 @@ void worker_main(stz_server* S)
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
-        int slot = -1;
-        auto ready = [&]() {
-            if (S->stop) return true;
-            if (S->queue.empty()) return false;
-            slot = -1;
-            for (int k = 0; k < S->opts.slots; ++k)
-                if (!S->slot_busy[k]) {
-                    slot = k;
-                    break;
-                }
-            if (slot < 0) return false;
-            size_t off;
-            const Ticket& t = S->tickets[S->queue.front()];
-            if (!S->arena.alloc(t.bytes, off)) return false;
-            S->arena.release(off, t.bytes);
-            return true;
-        };
-        S->cv_work.wait(lk, ready);
-        if (S->stop) break;
-        // admit in arrival order while outputs fit
+        int lane = 0, slot = -1;
         std::vector<uint64_t> ids;
-        while (!S->queue.empty() && (int)ids.size() < S->opts.max_batch) {
-            Ticket& t = S->tickets[S->queue.front()];
-            if (!S->arena.alloc(t.bytes, t.off)) break;
-            t.state = 1;
-            ids.push_back(S->queue.front());
-            S->queue.pop_front();
-        }
-        if (ids.empty()) continue;
-        S->slot_busy[slot] = true;
+        S->cv_work.wait(lk, [&]() { return S->stop || admit(S, lane, slot, ids); });
+        if (S->stop) break;
+        Lane& L = S->lanes[lane];
+        L.busy[slot] = true;
         const uint64_t bid = ++S->batches;
         lk.unlock();
         stz_status st;
         std::string err;
         {
             std::lock_guard<std::mutex> ex(S->exec_mu);
-            st = launch_batch(S, slot, bid, ids);
+            st = launch_batch(S, lane, slot, bid, ids);
             if (st != STZ_OK) err = stz_last_error();
         }
         lk.lock();
         if (st != STZ_OK) {
-            // nothing of a failed batch is pending its callback: fail its
-            // requests and give back the slot (after the stream drains)
+            // a batch that failed to launch never reached the completion
+            // thread: fail its requests and give back the slot (after the
+            // lane's stream drains)
             lk.unlock();
-            cudaStreamSynchronize(S->ctx->st);
+            cudaStreamSynchronize(L.st);
             lk.lock();
             const auto now = Clock::now();
             for (uint64_t id : ids) {
@@ -587,7 +709,7 @@ void worker_main(stz_server* S)
                 t.error = err;
                 t.t_done = now;
             }
-            S->slot_busy[slot] = false;
+            L.busy[slot] = false;
             S->completed += ids.size();
             S->cv_done.notify_all();
         }
@@ -625,6 +747,7 @@ void stz_server_default_opts(stz_server_opts* o)
     o->slots = 2;
     o->autotune = 1;
     o->threads = 0;
+    o->fast_reserve = (size_t)-1;
 }
 
 stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server** out)
@@ -639,7 +762,10 @@ stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server
         if (opts->slots > 0) o.slots = std::min(opts->slots, kMaxSlots);
         o.autotune = opts->autotune;
         o.threads = opts->threads;
+        o.fast_reserve = opts->fast_reserve;
     }
+    if (o.fast_reserve == (size_t)-1) o.fast_reserve = o.arena_bytes / 4;
+    o.fast_reserve = std::min(o.fast_reserve, o.arena_bytes);
     std::unique_ptr<stz_server> S(new (std::nothrow) stz_server());
     if (!S) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
     S->opts = o;
@@ -651,8 +777,31 @@ stz_status stz_server_create(int device, const stz_server_opts* opts, stz_server
         STZ_FAIL(STZ_ERR_NOMEM, "output arena allocation failed");
     }
     S->arena.reset(o.arena_bytes);
-    S->slot_busy.assign(o.slots, false);
+    // fast lane on the highest stream priority, bulk lane on the lowest
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    bool ok = true;
+    for (int ln = 0; ln < kLanes && ok; ++ln) {
+        Lane& L = S->lanes[ln];
+        L.slots = ln == kLaneFast ? o.slots : kBulkSlots;
+        ok = cudaStreamCreateWithPriority(&L.st, cudaStreamNonBlocking, ln == kLaneFast ? greatest : least) ==
+             cudaSuccess;
+        for (int k = 0; k < L.slots && ok; ++k)
+            ok = cudaEventCreate(&L.ev_a[k]) == cudaSuccess && cudaEventCreate(&L.ev_b[k]) == cudaSuccess;
+    }
+    if (!ok) {
+        for (Lane& L : S->lanes) {
+            for (int k = 0; k < kMaxSlots; ++k) {
+                if (L.ev_a[k]) cudaEventDestroy(L.ev_a[k]);
+                if (L.ev_b[k]) cudaEventDestroy(L.ev_b[k]);
+            }
+            if (L.st) cudaStreamDestroy(L.st);
+        }
+        stz_context_destroy(S->ctx);
+        STZ_FAIL(STZ_ERR_CUDA, "stream or event creation failed");
+    }
     stz_server* raw = S.release();
+    for (int ln = 0; ln < kLanes; ++ln) raw->lanes[ln].completer = std::thread(completer_main, raw, ln);
     raw->worker = std::thread(worker_main, raw);
     *out = raw;
     return STZ_OK;
@@ -667,8 +816,17 @@ void stz_server_destroy(stz_server* S)
     }
     S->cv_work.notify_all();
     if (S->worker.joinable()) S->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop_completers = true;  // they still drain the batches in flight
+    }
+    for (Lane& L : S->lanes) {
+        L.cv.notify_all();
+        if (L.completer.joinable()) L.completer.join();
+    }
     cudaSetDevice(S->ctx->device);
-    cudaStreamSynchronize(S->ctx->st);  // batches in flight and their callbacks
+    for (Lane& L : S->lanes) cudaStreamSynchronize(L.st);
+    cudaStreamSynchronize(S->ctx->st);
     {
         std::lock_guard<std::mutex> lk(S->mu);
         for (uint64_t id : S->queue) {
@@ -681,6 +839,13 @@ void stz_server_destroy(stz_server* S)
     }
     S->cv_done.notify_all();
     S->streams.clear();
+    for (Lane& L : S->lanes) {
+        for (int k = 0; k < kMaxSlots; ++k) {
+            if (L.ev_a[k]) cudaEventDestroy(L.ev_a[k]);
+            if (L.ev_b[k]) cudaEventDestroy(L.ev_b[k]);
+        }
+        if (L.st) cudaStreamDestroy(L.st);
+    }
     stz_context* ctx = S->ctx;
     delete S;
     stz_context_destroy(ctx);
@@ -729,7 +894,8 @@ stz_status stz_server_add_stream(stz_server* S, const void* data, size_t size, i
     ss->meta_cap = align16(sizeof(BatchHdr)) + align16(nch * sizeof(CtaWork)) + align16(nch * 4) +
                    align16(nch * sizeof(UnpredWork)) + 2 * align16((size_t)S->opts.max_batch * sizeof(RoiJob)) +
                    256;
-    for (int k = 0; k < S->opts.slots; ++k) STZ_CUDA(ss->meta[k].ensure(ss->meta_cap));
+    for (int ln = 0; ln < kLanes; ++ln)
+        for (int k = 0; k < S->lanes[ln].slots; ++k) STZ_CUDA(ss->meta[ln][k].ensure(ss->meta_cap));
     if (S->opts.autotune) STZ_TRY(autotune(S, *ss));
     STZ_TRY(capture_graphs(S, *ss));
     STZ_CUDA(cudaStreamSynchronize(S->ctx->st));
@@ -763,13 +929,15 @@ stz_status stz_server_submit(stz_server* S, const stz_request* r, uint64_t* tick
         t.dims[0] = (size_t)h.nx >> r->level;
         t.dims[1] = (size_t)h.ny >> r->level;
         t.dims[2] = (size_t)h.nz >> r->level;
+        if (r->level <= 1) t.lane = kLaneBulk;  // full level decodes
     } else {
         STZ_FAIL(STZ_ERR_ARG, "unknown request kind");
     }
     t.bytes = t.dims[0] * t.dims[1] * t.dims[2] * h.elem();
     {
         std::lock_guard<std::mutex> lk(S->mu);
-        if (!S->arena.fits_ever(t.bytes)) STZ_FAIL(STZ_ERR_NOMEM, "request output exceeds the output arena");
+        if (!S->arena.fits_ever(t.bytes, t.lane == kLaneBulk ? S->opts.fast_reserve : 0))
+            STZ_FAIL(STZ_ERR_NOMEM, "request output exceeds the output arena (less the fast-lane reserve)");
         const uint64_t id = S->next_ticket++;
         S->tickets.emplace(id, std::move(t));
         S->queue.push_back(id);
@@ -849,6 +1017,17 @@ stz_status stz_server_stats_get(stz_server* S, stz_server_stats* st)
     st->roi_grid = S->last_shape.roi_grid;
     st->arena_bytes = S->arena.capacity();
     st->arena_in_use = S->arena.used();
+    return STZ_OK;
+}
+
+stz_status stz_server_batch_log(stz_server* S, stz_batch_record* out, size_t cap, size_t* n)
+{
+    if (!S || !n || (!out && cap)) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    std::lock_guard<std::mutex> lk(S->mu);
+    const uint64_t last = S->batches;
+    const uint64_t cnt = std::min<uint64_t>({last, (uint64_t)kLogSize, (uint64_t)cap});
+    for (uint64_t i = 0; i < cnt; ++i) out[i] = S->rec(last - cnt + 1 + i);
+    *n = (size_t)cnt;
     return STZ_OK;
 }
 

@@ -112,13 +112,21 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_server_copy_out.argtypes = [vp, C.c_uint64, vp]
     lib.stz_server_release.argtypes = [vp, C.c_uint64]
     lib.stz_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
+    lib.stz_server_batch_log.argtypes = [vp, C.POINTER(BatchRecord), sz, C.POINTER(sz)]
     _lib = lib
     return lib
 
 
+class BatchRecord(C.Structure):
+    _fields_ = [("batch", C.c_uint64), ("n_requests", C.c_int), ("lane", C.c_int), ("slot", C.c_int),
+                ("t_start_ms", C.c_double),
+                ("t_planned_ms", C.c_double), ("t_launched_ms", C.c_double), ("t_done_ms", C.c_double),
+                ("device_ms", C.c_double)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_size_t), ("max_batch", C.c_int), ("slots", C.c_int), ("autotune", C.c_int),
-                ("threads", C.c_int)]
+                ("threads", C.c_int), ("fast_reserve", C.c_size_t)]
 
 
 class Request(C.Structure):
@@ -459,7 +467,7 @@ class Server:
     box / slice / progressive-level requests, continuously batched."""
 
     def __init__(self, device: int = 0, arena_bytes: int = 0, max_batch: int = 0, slots: int = 0,
-                 autotune: bool = True, threads: int = 0):
+                 autotune: bool = True, threads: int = 0, fast_reserve: int | None = None):
         self.lib = load_library()
         o = ServerOpts()
         self.lib.stz_server_default_opts(C.byref(o))
@@ -471,6 +479,8 @@ class Server:
             o.slots = slots
         o.autotune = 1 if autotune else 0
         o.threads = threads
+        if fast_reserve is not None:
+            o.fast_reserve = fast_reserve
         self._s = C.c_void_p()
         _check(self.lib.stz_server_create(int(device), C.byref(o), C.byref(self._s)))
 
@@ -534,6 +544,15 @@ class Server:
         s = ServerStats()
         _check(self.lib.stz_server_stats_get(self._s, C.byref(s)))
         return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def batch_log(self, cap: int = 4096) -> np.ndarray:
+        """Recent batches, oldest first: columns batch, n_requests, lane, slot,
+        t_start, t_planned, t_launched, t_done (ms since creation), device_ms."""
+        recs = (BatchRecord * cap)()
+        n = C.c_size_t()
+        _check(self.lib.stz_server_batch_log(self._s, recs, cap, C.byref(n)))
+        return np.array([[getattr(recs[i], f) for f, _ in BatchRecord._fields_] for i in range(n.value)],
+                        dtype=np.float64).reshape(-1, len(BatchRecord._fields_))
 
 
 def _tcode(t) -> int:

@@ -193,6 +193,25 @@ def test_stream_and_decode_match_oracle(ctx, case):
     assert np.array_equal(bits(ctx.decompress(s2)), bits(out))
 
 
+@pytest.mark.parametrize("rel", [3e-6, 1e-4])
+def test_wide_codebooks_decode_exactly(ctx, rel):
+    """White noise at a tight bound: thousands of distinct codes, many longer
+    than the decoder's table (the canonical long-code search and its shared
+    and global symbol tails), plus unpredictable values at 3e-6."""
+    rng = np.random.default_rng(77)
+    f = rng.uniform(-1, 1, (64, 64, 64)).astype(np.float32)
+    s = ctx.compress(f, eb=rel, eb_mode="rel", chunk_high=16, chunk_low=8)
+    b = s.to_bytes()
+    assert b == po.compress(f, s.info().eb, chunk_high=16, chunk_low=8)
+    K = s.info().n_levels
+    # the finest streams use > 7000 symbols, > 6000 of them with codes longer than 12 bits
+    assert max(len(np.unique(po.stream_codes(b, K, blk))) for blk in range(7)) > 7000
+    out = ctx.decompress(s)
+    assert np.array_equal(bits(out), bits(po.decompress(b)))
+    box = ctx.decompress_box(s, (5, 9, 13), (50, 40, 60))
+    assert np.array_equal(bits(box), bits(out[13:61, 9:41, 5:51]))
+
+
 def test_reference_bound_mode_matches_cli_semantics(ctx):
     f = make_field("grf", (32, 32, 32), np.float32, 2)
     s = ctx.compress(f, eb=1e-3, eb_mode="abs", bound_mode="reference", chunk_high=8, chunk_low=4)

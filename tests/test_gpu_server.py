@@ -179,12 +179,46 @@ def test_admission_by_output_memory(ctx):
         assert srv.stats()["arena_in_use"] == 0
 
 
+def test_fast_lane_reserve_admits_boxes_while_full_decodes_hold_memory(ctx):
+    """Full decodes (bulk lane) may not take the fast-lane reserve: with the
+    rest of the arena held by unreleased full decodes, a box is still served."""
+    from stz_b200 import Server, StzError
+
+    f = make_field("grf", (32, 32, 32), np.float32, 43)
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=8, chunk_low=4)
+    full = ctx.decompress(s)
+    with Server(0, arena_bytes=1 << 20, autotune=False, fast_reserve=256 << 10) as srv:
+        sid = srv.add_stream(s)
+        held = [srv.submit_level(sid, 0) for _ in range(6)]  # 6 x 128 KiB = the non-reserved 768 KiB
+        for t in held:
+            assert srv.wait(t, timeout_ms=20000).status == 0
+        extra = srv.submit_level(sid, 0)
+        with pytest.raises(StzError):
+            srv.wait(extra, timeout_ms=200)  # the reserve is not for full decodes
+        box = srv.submit_box(sid, (0, 0, 0), (31, 31, 31))  # 128 KiB from the reserve
+        res = srv.wait(box, timeout_ms=20000)
+        assert np.array_equal(bits(srv.copy_out(res, np.float32)), bits(full))
+        srv.release(box)
+        srv.release(held[0])
+        assert srv.wait(extra, timeout_ms=20000).status == 0
+        for t in held[1:] + [extra]:
+            srv.release(t)
+    # a full decode larger than the arena less the reserve is refused at submit
+    with Server(0, arena_bytes=1 << 20, autotune=False, fast_reserve=(1 << 20) - 4096) as srv2:
+        sid2 = srv2.add_stream(s)
+        with pytest.raises(StzError):
+            srv2.submit_level(sid2, 0)
+        t = srv2.submit_box(sid2, (0, 0, 0), (31, 31, 31))
+        assert srv2.wait(t, timeout_ms=20000).status == 0
+        srv2.release(t)
+
+
 def test_wait_times_out_and_bad_requests(ctx):
     from stz_b200 import Server, StzError
 
     f = make_field("grf", (32, 32, 32), np.float32, 41)
     s = ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=8, chunk_low=4)
-    with Server(0, arena_bytes=1 << 20, autotune=False) as srv:
+    with Server(0, arena_bytes=1 << 20, autotune=False, fast_reserve=0) as srv:
         sid = srv.add_stream(s)
         with pytest.raises(StzError):
             srv.submit_level(sid, 99)

@@ -135,3 +135,4 @@ def test_server_default_opts():
     o = stz_b200.ServerOpts()
     lib.stz_server_default_opts(ctypes.byref(o))
     assert o.arena_bytes == 1 << 30 and o.max_batch == 64 and o.slots == 2 and o.autotune == 1
+    assert o.fast_reserve == ctypes.c_size_t(-1).value  # a quarter of the arena
