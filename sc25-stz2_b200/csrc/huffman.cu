@@ -444,37 +444,53 @@ __global__ void __launch_bounds__(kCoderThreads) k_decode_dyn(const uint8_t* __r
 // Unpredictable values: for each listed chunk, walk its codes in order and
 // move the values between the dense per-position buffer and the chunk's slot
 // of the compact list (gather on encode, scatter on decode).
+// One pass: every thread owns a contiguous segment of the chunk's codes
+// (thread order = code order), counts its zeros, and a block-wide exclusive
+// prefix of the counts gives each segment's first rank in the list.
+// blockDim.x is a multiple of 32, at most 1024 (wc holds one count per warp).
 template <typename T, bool GATHER>
 __device__ void unpred_move_one(const UnpredWork& uw, const StreamDesc* __restrict__ sd,
                                 const uint16_t* __restrict__ codes, T* __restrict__ dense, T* __restrict__ list,
-                                uint32_t* wc, uint64_t& carry)
+                                uint32_t* wc)
 {
     const StreamDesc s = sd[uw.stream];
-    const size_t vol = (size_t)s.C * s.C * s.C;
+    const uint32_t vol = s.C * s.C * s.C;
     const size_t base = s.code_off + (size_t)uw.chunk * vol;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (size_t b = 0; b < vol; b += blockDim.x) {
-        const size_t i = b + threadIdx.x;
-        const bool f = i < vol && codes[base + i] == 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        if (lane == 0) wc[wid] = __popc(bal);
-        __syncthreads();
-        uint32_t before = 0, tot = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-            if (k < wid) before += wc[k];
-            tot += wc[k];
-        }
-        const uint64_t r = carry + before + __popc(bal & ((1u << lane) - 1u));
-        if (f && r < uw.count) {
-            if (GATHER) list[uw.list_off + r] = dense[base + i];
-            else dense[base + i] = list[uw.list_off + r];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
+    const uint32_t nt = blockDim.x, seg = (vol + nt - 1) / nt;
+    const uint32_t a = min(threadIdx.x * seg, vol), b = min(a + seg, vol);
+    uint32_t cnt = 0;
+    for (uint32_t i = a; i < b; ++i) cnt += codes[base + i] == 0 ? 1u : 0u;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(nt >> 5);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
     }
+    if (lane == 31) wc[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t v = lane < nw ? wc[lane] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < nw) wc[lane] = x - v;  // exclusive prefix over warps
+    }
+    __syncthreads();
+    uint64_t r = (uint64_t)wc[wid] + incl - cnt;
+    if (cnt)
+        for (uint32_t i = a; i < b; ++i) {
+            if (codes[base + i] != 0) continue;
+            if (r < uw.count) {
+                if (GATHER) list[uw.list_off + r] = dense[base + i];
+                else dense[base + i] = list[uw.list_off + r];
+            }
+            ++r;
+        }
+    __syncthreads();  // wc is reused by the block's next item
 }
 
 template <typename T, bool GATHER>
@@ -484,8 +500,7 @@ __global__ void __launch_bounds__(1024) k_unpred_move(const UnpredWork* __restri
                                                       T* __restrict__ list)
 {
     __shared__ uint32_t wc[32];
-    __shared__ uint64_t carry;
-    unpred_move_one<T, GATHER>(work[blockIdx.x], sd, codes, dense, list, wc, carry);
+    unpred_move_one<T, GATHER>(work[blockIdx.x], sd, codes, dense, list, wc);
 }
 
 // Persistent scatter (decode side) over the unpredictable-value list of a
@@ -497,12 +512,11 @@ __global__ void __launch_bounds__(1024) k_unpred_scatter_dyn(const uint8_t* __re
                                                              T* __restrict__ dense, T* __restrict__ list)
 {
     __shared__ uint32_t wc[32];
-    __shared__ uint64_t carry;
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
     const uint32_t n = h->n_uwork;
     const UnpredWork* __restrict__ work = reinterpret_cast<const UnpredWork*>(meta + h->o_uwork);
     for (uint32_t wi = blockIdx.x; wi < n; wi += gridDim.x)
-        unpred_move_one<T, false>(work[wi], sd, codes, dense, list, wc, carry);
+        unpred_move_one<T, false>(work[wi], sd, codes, dense, list, wc);
 }
 
 __global__ void k_pack_payload(const uint32_t* __restrict__ src, const uint64_t* __restrict__ src_base,
