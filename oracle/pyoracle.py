@@ -25,9 +25,33 @@ REFERENCE_SRC = "/root/reference/src"
 vp, sz, dbl, ci = C.c_void_p, C.c_size_t, C.c_double, C.c_int
 
 
+class Model(C.Structure):
+    """stzo_model: int8 MLP 14 -> 32 -> 32 -> 7 of one level (the container's
+    2112-byte layout)."""
+    _fields_ = [("s_in", dbl), ("s_out", dbl), ("w1", (C.c_int8 * 16) * 32), ("b1", C.c_int32 * 32),
+                ("m1", C.c_int32), ("sh1", C.c_int32), ("w2", (C.c_int8 * 32) * 32), ("b2", C.c_int32 * 32),
+                ("m2", C.c_int32), ("sh2", C.c_int32), ("w3", (C.c_int8 * 32) * 8), ("b3", C.c_int32 * 8)]
+
+
 class Params(C.Structure):
     _fields_ = [("dtype", ci), ("predictor", ci), ("radius", ci), ("chunk_high", ci), ("chunk_low", ci),
-                ("zstd_level", ci), ("eb", dbl), ("mult_base", dbl), ("mult_low", dbl), ("mult_high", dbl)]
+                ("zstd_level", ci), ("eb", dbl), ("mult_base", dbl), ("mult_low", dbl), ("mult_high", dbl),
+                ("model", C.POINTER(Model) * 2), ("learned_flags", C.c_uint32 * 2)]
+
+
+def model_record(m: Model) -> bytes:
+    return C.string_at(C.addressof(m), C.sizeof(m))
+
+
+def mlp_corr(m: Model, coarse: np.ndarray, x: int, y: int, z: int, eb: float) -> np.ndarray:
+    """Corrections of the 7 blocks at interior coarse point (x, y, z)."""
+    L = oracle()
+    a = np.ascontiguousarray(coarse)
+    dz, dy, dx = a.shape
+    out = np.zeros(7, dtype=a.dtype)
+    fn = L.stzo_mlp_corr_f64 if a.dtype == np.float64 else L.stzo_mlp_corr_f32
+    fn(C.byref(m), _p(a), x, y, z, dx, dy, dz, C.c_double(eb), _p(out))
+    return out
 
 
 def build(ref: bool = True) -> None:
@@ -146,11 +170,16 @@ def pointwise_eb(field: np.ndarray, rel: float, mults=(0.7, 2.7, 8.2)) -> float:
 
 # ---- whole-field codec -------------------------------------------------------
 def compress(field: np.ndarray, eb: float, predictor=0, radius=32768, chunk_high=32, chunk_low=16, zstd_level=3,
-             mults=(0.7, 2.7, 8.2)) -> bytes:
+             mults=(0.7, 2.7, 8.2), models=(None, None), flags=(0, 0)) -> bytes:
+    """models / flags: learned correction of levels K-1 and K (Model or None,
+    block bit masks)."""
     L = oracle()
     a = np.ascontiguousarray(field)
     nz, ny, nx = a.shape
     p = Params(1 if a.dtype == np.float64 else 0, predictor, radius, chunk_high, chunk_low, zstd_level, eb, *mults)
+    for i in range(2):
+        p.model[i] = C.pointer(models[i]) if models[i] is not None else C.POINTER(Model)()
+        p.learned_flags[i] = int(flags[i]) if models[i] is not None else 0
     out = C.POINTER(C.c_uint8)()
     n = L.stzo_compress(_p(a), nx, ny, nz, C.byref(p), C.byref(out))
     if n < 0:

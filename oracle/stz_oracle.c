@@ -35,6 +35,18 @@ size_t ZSTD_compressBound(size_t srcSize);
 unsigned ZSTD_isError(size_t code);
 
 /* ---- 2. typed code ------------------------------------------------------ */
+/* Learned correction: stencil of a coarse cell (x, y, z offsets) and the
+ * hidden layers' fixed-point requantization (stz_oracle.h, stzo_model). */
+static const int kStencil[14][3] = {{0, 0, 0},  {1, 0, 0},  {0, 1, 0},  {1, 1, 0}, {0, 0, 1},
+                                    {1, 0, 1},  {0, 1, 1},  {1, 1, 1},  {-1, 0, 0}, {0, -1, 0},
+                                    {0, 0, -1}, {2, 1, 1},  {1, 2, 1},  {1, 1, 2}};
+
+static int requant(int32_t acc, int32_t m, int32_t sh)
+{
+    const int64_t p = ((int64_t)acc * m + ((int64_t)1 << (sh - 1))) >> sh;
+    return p < 0 ? 0 : p > 127 ? 127 : (int)p;
+}
+
 #define T float
 #define SUF f32
 #include "stz_oracle_typed.h"
@@ -459,9 +471,21 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
     h.elem = p->dtype == 1 ? 8 : 4;
     h.c0[0] = nx >> h.K, h.c0[1] = ny >> h.K, h.c0[2] = nz >> h.K;
 
+    /* learned correction of levels K-1 and K: container version 2 */
+    const stzo_model* lm[64] = {0};
+    uint32_t lf[64] = {0};
+    int version = 1;
+    for (int i = 0; i < 2; ++i) {
+        const int k = h.K - 1 + i;
+        if (k >= 1 && p->model[i] && (p->learned_flags[i] & 0x7fu)) {
+            lm[k] = p->model[i];
+            lf[k] = p->learned_flags[i] & 0x7fu;
+            version = 2;
+        }
+    }
     buf_t dir = {0}, data = {0};
     bput(&dir, kMagic, 8);
-    bu32(&dir, 1);
+    bu32(&dir, (uint32_t)version);
     bu32(&dir, (uint32_t)h.dtype);
     bu32(&dir, (uint32_t)h.predictor);
     bu32(&dir, (uint32_t)nx);
@@ -502,17 +526,21 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
         void* Gn = k < h.K ? malloc(8 * n * h.elem) : NULL;
         int rc;
         if (h.dtype == 1)
-            rc = t_level_encode_f64((const double*)fine, (const double*)G, d[0], d[1], d[2], h.predictor,
-                                            ebk, h.radius, q, (double*)unpred, 7 * n, counts, (double*)Gn);
+            rc = t_level_encode_f64((const double*)fine, (const double*)G, d[0], d[1], d[2], h.predictor, ebk,
+                                    h.radius, q, (double*)unpred, 7 * n, counts, (double*)Gn, lm[k], lf[k]);
         else
-            rc = t_level_encode_f32((const float*)fine, (const float*)G, d[0], d[1], d[2], h.predictor,
-                                            ebk, h.radius, q, (float*)unpred, 7 * n, counts, (float*)Gn);
+            rc = t_level_encode_f32((const float*)fine, (const float*)G, d[0], d[1], d[2], h.predictor, ebk,
+                                    h.radius, q, (float*)unpred, 7 * n, counts, (float*)Gn, lm[k], lf[k]);
         (void)rc;
         bu32(&dir, (uint32_t)d[0]);
         bu32(&dir, (uint32_t)d[1]);
         bu32(&dir, (uint32_t)d[2]);
         bu32(&dir, (uint32_t)C);
         bf64(&dir, ebk);
+        if (version == 2) {
+            bu32(&dir, lf[k]);
+            if (lf[k]) bput(&dir, lm[k], sizeof(stzo_model));
+        }
         uint16_t* codes = (uint16_t*)malloc(2 * n);
         uint8_t* ucm = (uint8_t*)malloc(n * h.elem + 1);
         const int nch = (d[0] / C) * (d[1] / C) * (d[2] / C);
@@ -576,6 +604,8 @@ typedef struct {
     int d[64][3];
     int C[64];
     double ebk[64];
+    uint32_t lflags[64];     /* learned-correction blocks of the level (version 2) */
+    stzo_model lmodel[64];   /* its model when lflags != 0 */
     sdir_t s[64][7];
 } parsed_t;
 
@@ -595,7 +625,8 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
     char mg[8];
     rget(&r, mg, 8);
     if (r.err || memcmp(mg, kMagic, 8) != 0) return -10;
-    if (ru32(&r) != 1) return -11;
+    const uint32_t version = ru32(&r);
+    if (version != 1 && version != 2) return -11;
     hdr_t* h = &ps->h;
     h->dtype = (int)ru32(&r);
     h->predictor = (int)ru32(&r);
@@ -614,6 +645,11 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
         ps->d[k][0] = (int)ru32(&r), ps->d[k][1] = (int)ru32(&r), ps->d[k][2] = (int)ru32(&r);
         ps->C[k] = (int)ru32(&r);
         ps->ebk[k] = rf64(&r);
+        if (version == 2) {
+            ps->lflags[k] = ru32(&r);
+            if (ps->lflags[k] > 0x7f) return -16;
+            if (ps->lflags[k]) rget(&r, &ps->lmodel[k], sizeof(stzo_model));
+        }
         for (int b = 0; b < 7; ++b) {
             sdir_t* s = &ps->s[k][b];
             s->layers = (int)ru32(&r);
@@ -778,12 +814,13 @@ static int decode_level(const uint8_t* st, const parsed_t* ps, int k, const void
     }
     if (!rc) {
         size_t counts[7] = {0};
+        const stzo_model* M = ps->lflags[k] ? &ps->lmodel[k] : NULL;
         if (h->dtype == 1)
             t_level_decode_f64(q, (const double*)urm, counts, (const double*)G, dx, dy, dz, h->predictor,
-                                       ps->ebk[k], h->radius, (double*)Gn);
+                               ps->ebk[k], h->radius, (double*)Gn, M, ps->lflags[k]);
         else
             t_level_decode_f32(q, (const float*)urm, counts, (const float*)G, dx, dy, dz, h->predictor,
-                                       ps->ebk[k], h->radius, (float*)Gn);
+                               ps->ebk[k], h->radius, (float*)Gn, M, ps->lflags[k]);
     }
     free(urm);
     free(q);
@@ -1110,20 +1147,36 @@ long long stzo_quantize_f64(const double* d, size_t n, double eb, int radius, in
 int stzo_level_encode_f32(const float* fine, const float* coarse, int dx, int dy, int dz, int predictor, double eb,
                           int radius, int* q, float* unpred, size_t cap, size_t* counts, float* decoded)
 {
-    return t_level_encode_f32(fine, coarse, dx, dy, dz, predictor, eb, radius, q, unpred, cap, counts, decoded);
+    return t_level_encode_f32(fine, coarse, dx, dy, dz, predictor, eb, radius, q, unpred, cap, counts, decoded,
+                              NULL, 0);
 }
 int stzo_level_encode_f64(const double* fine, const double* coarse, int dx, int dy, int dz, int predictor, double eb,
                           int radius, int* q, double* unpred, size_t cap, size_t* counts, double* decoded)
 {
-    return t_level_encode_f64(fine, coarse, dx, dy, dz, predictor, eb, radius, q, unpred, cap, counts, decoded);
+    return t_level_encode_f64(fine, coarse, dx, dy, dz, predictor, eb, radius, q, unpred, cap, counts, decoded,
+                              NULL, 0);
 }
 void stzo_level_decode_f32(const int* q, const float* unpred, const size_t* counts, const float* coarse, int dx, int dy,
                            int dz, int predictor, double eb, int radius, float* out)
 {
-    t_level_decode_f32(q, unpred, counts, coarse, dx, dy, dz, predictor, eb, radius, out);
+    t_level_decode_f32(q, unpred, counts, coarse, dx, dy, dz, predictor, eb, radius, out, NULL, 0);
 }
 void stzo_level_decode_f64(const int* q, const double* unpred, const size_t* counts, const double* coarse, int dx,
                            int dy, int dz, int predictor, double eb, int radius, double* out)
 {
-    t_level_decode_f64(q, unpred, counts, coarse, dx, dy, dz, predictor, eb, radius, out);
+    t_level_decode_f64(q, unpred, counts, coarse, dx, dy, dz, predictor, eb, radius, out, NULL, 0);
+}
+void stzo_mlp_corr_f32(const stzo_model* m, const float* coarse, int x, int y, int z, int dx, int dy, int dz,
+                       double eb, float corr[7])
+{
+    ftz_on();
+    (void)dz;
+    mlp_corr_f32(m, coarse, x, y, z, dx, dy, (float)(1.0 / (eb * m->s_in)), (float)(m->s_out * eb), corr);
+}
+void stzo_mlp_corr_f64(const stzo_model* m, const double* coarse, int x, int y, int z, int dx, int dy, int dz,
+                       double eb, double corr[7])
+{
+    ftz_on();
+    (void)dz;
+    mlp_corr_f64(m, coarse, x, y, z, dx, dy, 1.0 / (eb * m->s_in), m->s_out * eb, corr);
 }

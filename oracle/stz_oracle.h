@@ -54,6 +54,33 @@ void stzo_level_decode_f32(const int* q, const float* unpred, const size_t* coun
 void stzo_level_decode_f64(const int* q, const double* unpred, const size_t* counts, const double* coarse,
                            int dx, int dy, int dz, int predictor, double eb, int radius, double* out);
 
+/* Learned correction of one level (this project's addition; the reference has
+ * none). An int8 MLP 14 -> 32 -> 32 -> 7 on the 14-point stencil of a coarse
+ * cell (the 8 cell corners, then (-1,0,0), (0,-1,0), (0,0,-1), (2,1,1),
+ * (1,2,1), (1,1,2)); inputs are the stencil values minus the corner mean,
+ * times rs = 1 / (eb * s_in), rounded to int8; hidden layers are ReLU with a
+ * fixed-point requantization a = clamp((acc * m + 2^(sh-1)) >> sh, 0, 127);
+ * output o is the correction (acc_o * (s_out * eb)) added to the base
+ * prediction of block o. Only interior cells (1 <= x,y,z <= dim-3) use it.
+ * The struct is also the byte layout stored in the container (2112 bytes,
+ * little endian). */
+typedef struct stzo_model {
+    double s_in, s_out;
+    int8_t w1[32][16]; /* inputs 14 and 15 are zero */
+    int32_t b1[32], m1, sh1;
+    int8_t w2[32][32];
+    int32_t b2[32], m2, sh2;
+    int8_t w3[8][32];  /* row 7 unused */
+    int32_t b3[8];
+} stzo_model;
+
+/* Corrections of the 7 blocks at interior coarse point (x,y,z) of a decoded
+ * coarse grid, for a level of eb `eb` (tests). */
+void stzo_mlp_corr_f32(const stzo_model* m, const float* coarse, int x, int y, int z, int dx, int dy, int dz,
+                       double eb, float corr[7]);
+void stzo_mlp_corr_f64(const stzo_model* m, const double* coarse, int x, int y, int z, int dx, int dy, int dz,
+                       double eb, double corr[7]);
+
 /* Whole-field codec in this project's container format (byte-identical to the
  * GPU path's output). dtype 0 = f32, 1 = f64. */
 typedef struct stzo_params {
@@ -65,6 +92,8 @@ typedef struct stzo_params {
     int zstd_level;     /* 0 = frames stored raw; FD5/SZ3 default 3 */
     double eb;          /* absolute eb handed to the level multipliers */
     double mult_base, mult_low, mult_high; /* FD5:2127-2129 defaults 0.7 / 2.7 / 8.2 */
+    const stzo_model* model[2];   /* learned correction of levels K-1 and K (NULL = none) */
+    uint32_t learned_flags[2];    /* blocks (bit b) of those levels that use it */
 } stzo_params;
 
 /* Returns stream size, or a negative error. *out is malloc'ed. */

@@ -182,6 +182,52 @@ static inline T FN(predict_any)(int predictor, int block, const T* r, int x, int
                           : FN(t_predict)(block, r, x, y, z, dx, dy, dz);
 }
 
+/* Learned correction of one interior coarse cell (stzo_model in
+ * stz_oracle.h; this project's addition). rs = (T)(1/(eb*s_in)),
+ * so = (T)(s_out*eb). */
+static inline int FN(to_i8)(T v)
+{
+    if (!(v == v)) return 0;
+    if (v >= (T)127) return 127;
+    if (v <= (T)-127) return -127;
+    return (int)rint((double)v);
+}
+
+static void FN(mlp_corr)(const stzo_model* M, const T* r, int x, int y, int z, int dx, int dy, T rs, T so, T corr[7])
+{
+    const size_t sy = (size_t)dx, sz = (size_t)dx * dy;
+    T v[14];
+    for (int i = 0; i < 14; ++i)
+        v[i] = r[(size_t)(z + kStencil[i][2]) * sz + (size_t)(y + kStencil[i][1]) * sy + (size_t)(x + kStencil[i][0])];
+    T m = v[0];
+    for (int i = 1; i < 8; ++i) m = m + v[i];
+    m = m * (T)0.125;
+    int xin[16] = {0};
+    for (int i = 0; i < 14; ++i) xin[i] = FN(to_i8)((v[i] - m) * rs);
+    int a1[32], a2[32];
+    for (int j = 0; j < 32; ++j) {
+        int32_t acc = M->b1[j];
+        for (int i = 0; i < 16; ++i) acc += (int32_t)M->w1[j][i] * xin[i];
+        a1[j] = requant(acc, M->m1, M->sh1);
+    }
+    for (int j = 0; j < 32; ++j) {
+        int32_t acc = M->b2[j];
+        for (int i = 0; i < 32; ++i) acc += (int32_t)M->w2[j][i] * a1[i];
+        a2[j] = requant(acc, M->m2, M->sh2);
+    }
+    for (int o = 0; o < 7; ++o) {
+        int32_t acc = M->b3[o];
+        for (int i = 0; i < 32; ++i) acc += (int32_t)M->w3[o][i] * a2[i];
+        corr[o] = (T)acc * so;
+    }
+}
+
+static inline int FN(learned_at)(const stzo_model* M, uint32_t flags, int b, int x, int y, int z, int dx, int dy,
+                                 int dz)
+{
+    return M && ((flags >> b) & 1u) && x >= 1 && x <= dx - 3 && y >= 1 && y <= dy - 3 && z >= 1 && z <= dz - 3;
+}
+
 /* One value of quantize_range_nodec, FD5:1216-1229 (the fallback loop
  * FD5:1232-1249 yields the same code for every input). Returns the shifted
  * code, 0 when unpredictable; *dec gets the decompressed residual. */
@@ -227,12 +273,14 @@ static long long FN(t_quantize)(const T* d, size_t n, double eb, int radius, int
  * reference's call sequence). The decoded fine grid uses the decoder's
  * recover values, so it equals what the decompressor rebuilds. */
 static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, int dz, int predictor, double eb,
-                          int radius, int* q, T* unpred, size_t cap, size_t* counts, T* decoded)
+                          int radius, int* q, T* unpred, size_t cap, size_t* counts, T* decoded,
+                          const stzo_model* M, uint32_t flags)
 {
     ftz_on();
     const size_t n = (size_t)dx * dy * dz;
     const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
     const double recip = 1.0 / eb;
+    const T rs = M ? (T)(1.0 / (eb * M->s_in)) : (T)0, so = M ? (T)(M->s_out * eb) : (T)0;
     size_t nu = 0;
     for (int b = 0; b < 7; ++b) {
         const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
@@ -242,7 +290,12 @@ static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, in
                 for (int x = 0; x < dx; ++x) {
                     const size_t i = ((size_t)z * dy + y) * dx + x;
                     const size_t fi = (2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px;
-                    const T p = FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                    T p = FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                    if (FN(learned_at)(M, flags, b, x, y, z, dx, dy, dz)) {
+                        T corr[7];
+                        FN(mlp_corr)(M, coarse, x, y, z, dx, dy, rs, so, corr);
+                        p = p + corr[b];
+                    }
                     const T d = fine[fi] - p;
                     T dec = 0;
                     const int code = FN(quant1)(d, eb, recip, radius, &dec);
@@ -271,11 +324,12 @@ static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, in
 
 /* Level decode: x' = dq + P (FD5:1049-1143), merged into the fine grid. */
 static void FN(t_level_decode)(const int* q, const T* unpred, const size_t* counts, const T* coarse, int dx, int dy,
-                           int dz, int predictor, double eb, int radius, T* out)
+                           int dz, int predictor, double eb, int radius, T* out, const stzo_model* M, uint32_t flags)
 {
     ftz_on();
     const size_t n = (size_t)dx * dy * dz;
     const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    const T rs = M ? (T)(1.0 / (eb * M->s_in)) : (T)0, so = M ? (T)(M->s_out * eb) : (T)0;
     size_t u = 0;
     for (int b = 0; b < 7; ++b) {
         const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
@@ -285,8 +339,13 @@ static void FN(t_level_decode)(const int* q, const T* unpred, const size_t* coun
                     const size_t i = ((size_t)z * dy + y) * dx + x;
                     const int code = q[(size_t)b * n + i];
                     const T dq = code ? FN(recover)(code, eb, radius) : unpred[u++];
-                    out[(2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px] =
-                        dq + FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                    T p = FN(predict_any)(predictor, b, coarse, x, y, z, dx, dy, dz);
+                    if (FN(learned_at)(M, flags, b, x, y, z, dx, dy, dz)) {
+                        T corr[7];
+                        FN(mlp_corr)(M, coarse, x, y, z, dx, dy, rs, so, corr);
+                        p = p + corr[b];
+                    }
+                    out[(2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px] = dq + p;
                 }
         (void)counts;
     }
