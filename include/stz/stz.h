@@ -87,14 +87,23 @@ typedef struct stz_opts {
     int zstd_level;       /* final lossless stage level (SZ3 default 3); 0 stores frames raw */
     int predictor;        /* stz_predictor */
     int threads;          /* host threads for zstd; 0 = all cores */
+    /* Learned correction (this library's addition; streams that use it are
+     * container version 2): an int8 MLP per level adds a correction to the
+     * predictions of the second-finest and finest levels. null = none. */
+    const struct stz_model* model;
+    /* -1: per level and block, use the correction where a sampled code-length
+     * estimate says it pays; >= 0: forced blocks, bits 0-6 for the
+     * second-finest level and bits 8-14 for the finest. */
+    int learned_flags;
 } stz_opts;
 
 /* Reference defaults: rel eb 1e-3, pointwise, multipliers 0.7/2.7/8.2,
- * radius 32768, chunks 32/16, zstd 3, dynamic predictor. */
+ * radius 32768, chunks 32/16, zstd 3, dynamic predictor, no learned model. */
 void stz_default_opts(stz_opts* opts);
 
 typedef struct stz_context stz_context;
 typedef struct stz_stream stz_stream;
+typedef struct stz_model stz_model;
 
 typedef struct stz_info {
     int dtype;            /* stz_dtype */
@@ -108,6 +117,7 @@ typedef struct stz_info {
     double max_error;     /* guaranteed max |x - x'| of a full decode */
     size_t stream_bytes;  /* serialized size */
     size_t raw_payload_bytes; /* entropy-coded bytes before zstd */
+    int learned_flags;    /* learned-correction blocks, encoded as stz_opts.learned_flags */
 } stz_info;
 
 const char* stz_status_string(stz_status s);
@@ -178,6 +188,16 @@ stz_status stz_stream_info(const stz_stream* s, stz_info* info);
  * the context's device, so later decodes skip zstd and the host->device copy. */
 stz_status stz_stream_upload(stz_context* ctx, stz_stream* s);
 void stz_stream_free(stz_stream* s);
+
+/* ---- learned correction models ---------------------------------------- *
+ * A model file holds up to two 2112-byte level records (second-finest,
+ * finest): "STZLMDL1", a u32 mask (bit 0 / bit 1: record present), then the
+ * present records in that order, little-endian. A record: f64 s_in, s_out;
+ * int8 w1[32][16]; i32 b1[32], m1, sh1; int8 w2[32][32]; i32 b2[32], m2, sh2;
+ * int8 w3[8][32]; i32 b3[8]. */
+stz_status stz_model_parse(const void* data, size_t size, stz_model** out);
+stz_status stz_model_bytes(const stz_model* m, const void** data, size_t* size);
+void stz_model_free(stz_model* m);
 
 /* ---- reference function boundary (device pointers) --------------------- *
  * The reference's own stage functions, one for one, for callers that drive

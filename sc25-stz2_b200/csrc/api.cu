@@ -142,7 +142,41 @@ stz_status check_opts(const stz_opts* o)
     if (o->radius < 1 || o->radius > 32768) STZ_FAIL(STZ_ERR_ARG, "radius must be in [1, 32768]");
     if (o->zstd_level < 0 || o->zstd_level > 22) STZ_FAIL(STZ_ERR_ARG, "zstd_level must be in [0, 22]");
     if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    if (o->learned_flags < -1 || (o->learned_flags >= 0 && (o->learned_flags & ~0x7f7f)))
+        STZ_FAIL(STZ_ERR_ARG, "learned_flags must be -1 or a mask of bits 0-6 and 8-14");
     return STZ_OK;
+}
+
+// Estimated coded bits of a sampled code histogram (kEvalBins bins, the last
+// one for far and unpredictable codes): ideal code lengths, plus the stored
+// value for every entry of the last bin.
+double sample_bits(const uint32_t* h, size_t elem)
+{
+    double n = 0, bits = 0;
+    for (int i = 0; i < kEvalBins; ++i) n += h[i];
+    if (n == 0) return 0;
+    for (int i = 0; i < kEvalBins; ++i)
+        if (h[i]) bits += h[i] * std::log2(n / h[i]);
+    return bits + (double)h[kEvalBins - 1] * 8.0 * (double)elem;
+}
+
+// Blocks of level k where the learned correction pays, from the sampled
+// histograms of both predictions: a block is flagged when its estimate
+// drops below 0.995 of the base one, and the level only when the saving
+// (scaled from the 1/8 sample) exceeds the model record it costs.
+uint32_t choose_learned_flags(const uint32_t* hist, size_t elem)
+{
+    uint32_t flags = 0;
+    double saved = 0;
+    for (int b = 0; b < 7; ++b) {
+        const double b0 = sample_bits(hist + (size_t)b * kEvalBins, elem);
+        const double b1 = sample_bits(hist + (size_t)(7 + b) * kEvalBins, elem);
+        if (b1 < 0.995 * b0) {
+            flags |= 1u << b;
+            saved += b0 - b1;
+        }
+    }
+    return 8.0 * saved > 8.0 * (double)(sizeof(LearnedModel) + 4) ? flags : 0u;
 }
 
 // ---- compress ----------------------------------------------------------------
@@ -211,6 +245,19 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     std::vector<T> coarsest(n0);
     STZ_CUDA(cudaMemcpyAsync(coarsest.data(), ctx->grid[cur].p, n0 * elem, cudaMemcpyDeviceToHost, st));
 
+    // learned models of levels K-1 (record 0) and K (record 1) on the device
+    const stz_model* M = o.model;
+    std::vector<uint32_t> lflags(K + 1, 0);
+    if (M && M->mask) {
+        STZ_CUDA(ctx->models.ensure(2 * sizeof(LearnedModel)));
+        STZ_CUDA(cudaMemcpyAsync(ctx->models.p, M->lv, 2 * sizeof(LearnedModel), cudaMemcpyHostToDevice, st));
+        STZ_CUDA(ctx->eval.ensure(2 * 7 * kEvalBins * 4));
+    }
+    auto level_model = [&](int k) -> int {  // record index of level k, -1 if none
+        const int i = k - (K - 1);
+        return (M && i >= 0 && i < 2 && (M->mask >> i & 1u)) ? i : -1;
+    };
+
     // levels, coarse to fine
     for (int k = 1; k <= K; ++k) {
         const StreamDesc& s0 = g.sd[(size_t)(k - 1) * 7];
@@ -229,6 +276,29 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
         a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
         a.qp = make_quant_params(ebk[k], o.radius);
+        if (const int mi = level_model(k); mi >= 0) {
+            const LearnedModel& lm = M->lv[mi];
+            a.learned.model = ctx->models.as<LearnedModel>() + mi;
+            a.learned.rs = (T)(1.0 / (ebk[k] * lm.s_in));
+            a.learned.so = (T)(lm.s_out * ebk[k]);
+            if (o.learned_flags >= 0) {
+                lflags[k] = (uint32_t)(o.learned_flags >> (mi == 0 ? 0 : 8)) & 0x7fu;
+            } else {
+                a.learned.flags = 0x7f;
+                STZ_CUDA(cudaMemsetAsync(ctx->eval.p, 0, 2 * 7 * kEvalBins * 4, st));
+                {
+                    KScope ks(ctx, "k_learned_eval");
+                    launch_learned_eval<T>(a, ctx->eval.as<uint32_t>(), st);
+                }
+                STZ_CUDA(ctx->h_hist.ensure(2 * 7 * kEvalBins * 4));
+                STZ_CUDA(cudaMemcpyAsync(ctx->h_hist.p, ctx->eval.p, 2 * 7 * kEvalBins * 4, cudaMemcpyDeviceToHost,
+                                         st));
+                STZ_CUDA(cudaStreamSynchronize(st));
+                lflags[k] = choose_learned_flags(ctx->h_hist.as<uint32_t>(), elem);
+            }
+            a.learned.flags = lflags[k];
+            if (!lflags[k]) a.learned = LearnedArgs<T>();
+        }
         {
             KScope ks(ctx, k == K ? "k_level_encode[finest]" : "k_level_encode[coarser]");
             launch_level_encode<T>(a, st);
@@ -407,6 +477,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         levels[k].dx = g.lv[k].dx, levels[k].dy = g.lv[k].dy, levels[k].dz = g.lv[k].dz;
         levels[k].C = g.lv[k].C;
         levels[k].eb = ebk[k];
+        levels[k].lflags = lflags[k];
+        if (lflags[k]) levels[k].model = M->lv[level_model(k)];
     }
     std::vector<StreamParts> parts(nstreams);
     const uint64_t* choff = (const uint64_t*)(ht + t_choff);
@@ -531,9 +603,16 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
     p.total_unpred = unp;
     const size_t o_sd = 0, o_sym = align256(nstreams * sizeof(StreamDesc)), o_len = align256(o_sym + syms * 2);
     const size_t o_sub = align256(o_len + syms), o_ch = align256(o_sub + subs * 4), o_ul = align256(o_ch + chunks * 8);
-    const size_t o_pl = align256(o_ul + unp * elem), total = align256(o_pl + words * 4);
+    // learned models of levels 0..kmax (index k), with the tables
+    const bool learned = stream_learned(ps);
+    const size_t o_md = align256(o_ul + unp * elem);
+    const size_t o_pl = align256(o_md + (learned ? (size_t)(kmax + 1) * sizeof(LearnedModel) : 0));
+    const size_t total = align256(o_pl + words * 4);
     STZ_CUDA(ctx->h_stage.ensure(total));
     uint8_t* hs = ctx->h_stage.as<uint8_t>();
+    if (learned)
+        for (int k = 0; k <= kmax; ++k)
+            std::memcpy(hs + o_md + k * sizeof(LearnedModel), &ps.lv[k].model, sizeof(LearnedModel));
     std::memcpy(hs + o_sd, p.sd.data(), nstreams * sizeof(StreamDesc));
     for (int i = 0; i < nstreams; ++i) {
         const StreamHeader& H = p.hdr[i];
@@ -596,6 +675,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
     p.d_sub = (uint32_t*)(ds + o_sub);
     p.d_choff = (uint64_t*)(ds + o_ch);
     p.d_ulist = ds + o_ul;
+    p.d_models = learned ? (LearnedModel*)(ds + o_md) : nullptr;
     p.d_payload = (uint32_t*)(ds + o_pl);
     const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
     STZ_CUDA(p.coarsest->ensure(n0 * elem));
@@ -705,6 +785,7 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
         a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
         a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
         a.out = k == kdec ? out_dev : ctx->grid[cur].as<T>();
+        a.learned = learned_args<T>(ps, k, p.d_models);
         {
             KScope ks(ctx, k == h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
             launch_level_decode<T>(a, ctx->st);
@@ -771,15 +852,35 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         STZ_TRY(decode_levels<T>(ctx, s, *p, K - 2, p->base->as<T>()));
         p->base_valid = true;
     }
+    // Mid-grid window: the planner's reference regions; with a learned
+    // correction on the finest level, also the full -1..+2 stencil of every
+    // query cell, and then the low chunks of the whole window in all blocks.
+    const bool learned_high = ps.lv[K].lflags != 0;
+    int m0[3], m1[3];
+    const bool have_mid = mid_window(plan, low.dx * 2, low.dy * 2, low.dz * 2, learned_high, m0, m1);
     // entropy-decode the planned chunks of the low and high levels
     std::vector<CtaWork> work;
     std::vector<uint32_t> ids;
     std::vector<UnpredWork> uw;
-    for (const BlockPlan& bp : plan.low) {
-        const uint32_t si = (uint32_t)((K - 2) * 7 + bp.block);
-        std::vector<uint32_t> cs(bp.chunks.begin(), bp.chunks.end());
-        add_work(work, ids, si, cs.data(), cs.size(), low.C);
-        add_unpred_work(*p, si, cs.data(), cs.size(), uw);
+    if (learned_high) {
+        std::vector<int64_t> wc;
+        if (have_mid) {
+            const int nc[3] = {low.ncx, low.ncy, low.ncz};
+            window_chunks(m0, m1, low.C, nc, wc);
+        }
+        std::vector<uint32_t> cs(wc.begin(), wc.end());
+        for (int b = 0; b < 7 && !cs.empty(); ++b) {
+            const uint32_t si = (uint32_t)((K - 2) * 7 + b);
+            add_work(work, ids, si, cs.data(), cs.size(), low.C);
+            add_unpred_work(*p, si, cs.data(), cs.size(), uw);
+        }
+    } else {
+        for (const BlockPlan& bp : plan.low) {
+            const uint32_t si = (uint32_t)((K - 2) * 7 + bp.block);
+            std::vector<uint32_t> cs(bp.chunks.begin(), bp.chunks.end());
+            add_work(work, ids, si, cs.data(), cs.size(), low.C);
+            add_unpred_work(*p, si, cs.data(), cs.size(), uw);
+        }
     }
     for (const BlockPlan& bp : plan.high) {
         const uint32_t si = (uint32_t)((K - 1) * 7 + bp.block);
@@ -792,8 +893,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     // then the query box
     STZ_CUDA(ctx->mid.ensure(8 * nbase * elem));
     std::vector<RoiJob> mj, rj;
-    int m0[3], m1[3];
-    if (region_bbox(plan, m0, m1)) {
+    if (have_mid) {
         const int o0[3] = {0, 0, 0};
         mj.push_back(cells_job(m0, m1, ctx->mid.p, o0, 2 * (uint64_t)low.dx, 4 * (uint64_t)low.dx * low.dy, 0));
     }
@@ -848,13 +948,13 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         KScope ks(ctx, "k_roi_cells[low]");
         launch_roi_cells<T>(blocks(hd.mid_total), 256, dm, 0, p->base->as<T>(), low, p->base->as<T>(), low,
                             qparams(ps, K - 1), h.predictor, ctx->codes.as<uint16_t>() + lo_off,
-                            ud ? ud + lo_off : nullptr, ctx->st);
+                            ud ? ud + lo_off : nullptr, ctx->st, learned_args<T>(ps, K - 1, p->d_models));
     }
     {
         KScope ks(ctx, "k_roi_cells[high]");
         launch_roi_cells<T>(blocks(hd.req_total), 256, dm, 1, ctx->mid.as<T>(), high, p->base->as<T>(), low,
                             qparams(ps, K), h.predictor, ctx->codes.as<uint16_t>() + hi_off,
-                            ud ? ud + hi_off : nullptr, ctx->st);
+                            ud ? ud + hi_off : nullptr, ctx->st, learned_args<T>(ps, K, p->d_models));
     }
     STZ_CUDA(cudaGetLastError());
     lap.mark("launches");
@@ -901,6 +1001,8 @@ void stz_default_opts(stz_opts* o)
     o->zstd_level = 3;
     o->predictor = STZ_PRED_DYNAMIC;
     o->threads = 0;
+    o->model = nullptr;
+    o->learned_flags = -1;
 }
 
 const char* stz_status_string(stz_status s)
@@ -1137,6 +1239,9 @@ stz_status stz_stream_info(const stz_stream* s, stz_info* info)
     info->max_error = h.eb * std::max({h.mult_base, h.mult_low, h.mult_high});
     info->stream_bytes = s->bytes.size();
     info->raw_payload_bytes = s->raw_payload_bytes;
+    info->learned_flags = 0;
+    if (h.K >= 2) info->learned_flags |= (int)s->dir.lv[h.K - 1].lflags;
+    if (h.K >= 1) info->learned_flags |= (int)s->dir.lv[h.K].lflags << 8;
     return STZ_OK;
 }
 
@@ -1151,6 +1256,46 @@ stz_status stz_stream_upload(stz_context* ctx, stz_stream* s)
 }
 
 void stz_stream_free(stz_stream* s) { delete s; }
+
+// ---- learned correction models ------------------------------------------------
+stz_status stz_model_parse(const void* data, size_t size, stz_model** out)
+{
+    if (!data || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    *out = nullptr;
+    const uint8_t* b = (const uint8_t*)data;
+    if (size < 12 || std::memcmp(b, "STZLMDL1", 8) != 0) STZ_FAIL(STZ_ERR_FORMAT, "not an STZ model file");
+    uint32_t mask;
+    std::memcpy(&mask, b + 8, 4);
+    if (mask == 0 || mask > 3) STZ_FAIL(STZ_ERR_FORMAT, "model mask must be 1, 2 or 3");
+    const size_t nrec = (size_t)(mask & 1u) + (mask >> 1 & 1u);
+    if (size != 12 + nrec * sizeof(LearnedModel)) STZ_FAIL(STZ_ERR_FORMAT, "model file size does not match its mask");
+    auto* m = new (std::nothrow) stz_model();
+    if (!m) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
+    m->mask = mask;
+    size_t off = 12;
+    for (int i = 0; i < 2; ++i)
+        if (mask >> i & 1u) {
+            std::memcpy(&m->lv[i], b + off, sizeof(LearnedModel));
+            off += sizeof(LearnedModel);
+            if (!learned_model_valid(m->lv[i])) {
+                delete m;
+                STZ_FAIL(STZ_ERR_FORMAT, "bad learned model record");
+            }
+        }
+    m->serialize();
+    *out = m;
+    return STZ_OK;
+}
+
+stz_status stz_model_bytes(const stz_model* m, const void** data, size_t* size)
+{
+    if (!m || !data || !size) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    *data = m->bytes.data();
+    *size = m->bytes.size();
+    return STZ_OK;
+}
+
+void stz_model_free(stz_model* m) { delete m; }
 
 // ---- reference function boundary ------------------------------------------------
 stz_status stz_split_dev(stz_context* ctx, stz_dtype dtype, const void* full, size_t nx, size_t ny, size_t nz,

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -245,6 +246,12 @@ std::string validate_dims(long long nx, long long ny, long long nz, int chunk_hi
 }
 
 // ---- container ------------------------------------------------------------------
+bool learned_model_valid(const LearnedModel& m)
+{
+    return std::isfinite(m.s_in) && m.s_in > 0 && std::isfinite(m.s_out) && m.s_out > 0 && m.sh1 >= 1 &&
+           m.sh1 <= 62 && m.sh2 >= 1 && m.sh2 <= 62;
+}
+
 namespace {
 
 const char kMagic[8] = {'S', 'T', 'Z', 'B', '2', '0', '0', 0};
@@ -341,7 +348,8 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     char mg[8];
     r.get(mg, 8);
     if (r.err || std::memcmp(mg, kMagic, 8) != 0) return "not an STZ-B200 stream (bad magic)";
-    if (r.u32() != 1) return "unsupported stream version";
+    const uint32_t version = r.u32();
+    if (version != 1 && version != 2) return "unsupported stream version";
     FileHeader& h = out.h;
     h.dtype = (int)r.u32();
     h.predictor = (int)r.u32();
@@ -372,6 +380,14 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
         if (r.err || L.dx != (h.nx >> sh) || L.dy != (h.ny >> sh) || L.dz != (h.nz >> sh) ||
             L.C != level_chunk(h.nx, h.ny, h.nz, h.K, k, h.chunk_high, h.chunk_low))
             return "bad level record";
+        if (version == 2) {
+            L.lflags = r.u32();
+            if (L.lflags > 0x7f) return "bad learned-correction flags";
+            if (L.lflags) {
+                r.get(&L.model, sizeof(LearnedModel));
+                if (!r.err && !learned_model_valid(L.model)) return "bad learned model record";
+            }
+        }
         for (int b = 0; b < 7; ++b) {
             StreamDir& s = L.s[b];
             s.layers = r.u32();
@@ -448,7 +464,9 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
     std::vector<uint8_t> out;
     Writer w{out};
     w.put(kMagic, 8);
-    w.u32(1);
+    bool learned = false;  // version 2 carries per-level learned corrections
+    for (int k = 1; k <= h.K; ++k) learned = learned || levels[k].lflags != 0;
+    w.u32(learned ? 2 : 1);
     w.u32((uint32_t)h.dtype);
     w.u32((uint32_t)h.predictor);
     w.u32((uint32_t)h.nx);
@@ -475,6 +493,10 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
         w.u32((uint32_t)L.dz);
         w.u32((uint32_t)L.C);
         w.f64(L.eb);
+        if (learned) {
+            w.u32(L.lflags);
+            if (L.lflags) w.put(&L.model, sizeof(LearnedModel));
+        }
         for (int b = 0; b < 7; ++b, ++si) {
             const StreamParts& p = parts[si];
             w.u32((uint32_t)p.layers);
@@ -584,6 +606,28 @@ bool region_bbox(const QueryPlan& p, int lo[3], int hi[3])
         any = true;
     }
     return any;
+}
+
+bool mid_window(const QueryPlan& p, int hx, int hy, int hz, bool learned, int lo[3], int hi[3])
+{
+    bool any = region_bbox(p, lo, hi);
+    if (!learned) return any;
+    const int hd[3] = {hx, hy, hz};
+    for (int a = 0; a < 3; ++a)
+        if (p.q[a].empty()) return any;
+    for (int a = 0; a < 3; ++a) {
+        const int b = std::max(0, (p.q[a].b >> 1) - 1), e = std::min(hd[a] - 1, (p.q[a].e >> 1) + 2);
+        lo[a] = any ? std::min(lo[a], b) : b;
+        hi[a] = any ? std::max(hi[a], e) : e;
+    }
+    return true;
+}
+
+void window_chunks(const int lo[3], const int hi[3], int C, const int nc[3], std::vector<int64_t>& out)
+{
+    AxisRange r[3];
+    for (int a = 0; a < 3; ++a) r[a] = AxisRange{lo[a] >> 1, hi[a] >> 1};
+    chunks_for_box(nc[0] * C, nc[1] * C, nc[2] * C, C, r, out);
 }
 
 bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], AxisRange q[3])

@@ -11,6 +11,8 @@
 #include <thread>
 #include <vector>
 
+#include "stz_internal.h"
+
 namespace stz {
 
 // ---- thread pool ----------------------------------------------------------
@@ -61,8 +63,13 @@ struct StreamDir {
 struct LevelDir {
     int dx = 0, dy = 0, dz = 0, C = 0;
     double eb = 0;
+    uint32_t lflags = 0;     // blocks with the learned correction (container version 2)
+    LearnedModel model{};    // its model when lflags != 0
     StreamDir s[7];
 };
+
+// A learned model record is usable: finite positive scales, shifts 1..62.
+bool learned_model_valid(const LearnedModel& m);
 
 struct ParsedStream {
     FileHeader h;
@@ -134,6 +141,14 @@ bool query_box(int nx, int ny, int nz, const int64_t a[3], const int64_t b[3], A
 // Bounding box (x, y, z, inclusive) of a plan's non-empty reference regions
 // on the half-resolution grid; false when there are none.
 bool region_bbox(const QueryPlan& p, int lo[3], int hi[3]);
+// Half-resolution window a query decodes: the region bbox, grown when the
+// finest level carries a learned correction (its stencil reaches -1..+2
+// around every coarse cell of the query on all three axes) to the cells
+// (q.b>>1)-1 .. (q.e>>1)+2, clamped to the grid. false when empty.
+bool mid_window(const QueryPlan& p, int hx, int hy, int hz, bool learned, int lo[3], int hi[3]);
+// Row-major ids (ascending) of the chunks (edge C, nc per axis) holding the
+// cells lo>>1 .. hi>>1 of a half-resolution window.
+void window_chunks(const int lo[3], const int hi[3], int C, const int nc[3], std::vector<int64_t>& out);
 void flatten_plan(const QueryPlan& p, std::vector<int64_t>& out);
 
 }  // namespace stz

@@ -67,12 +67,24 @@ struct EncodeIO {
     T* __restrict__ G;  // decoded fine grid (coarser levels only)
 };
 
+// Learned correction of the blocks la.flags selects (interior points only;
+// la.model in shared memory).
+template <typename T, class Acc>
+__device__ __forceinline__ void apply_learned(const Acc& r, const LearnedArgs<T>& la, T (&p)[7])
+{
+    T corr[7];
+    learned_corr<T>(*la.model, r, la.rs, la.so, corr);
+#pragma unroll
+    for (int b = 0; b < 7; ++b)
+        if ((la.flags >> b) & 1u) p[b] = Ar<T>::add(p[b], corr[b]);
+}
+
 // One coarse point of the encoder: fine values, 7 predictions, residuals,
 // codes, unpredictable values, decoded fine cell.
-template <typename T, int PRED, bool FINEST, bool INTERIOR, class Acc>
+template <typename T, int PRED, bool FINEST, bool INTERIOR, bool LEARNED = false, class Acc>
 __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
                                              const QuantParams& qp, const T* lut, const ChunkIndex& ci, int x, int y,
-                                             int z, int (&q)[7])
+                                             int z, int (&q)[7], const LearnedArgs<T>& la = LearnedArgs<T>())
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -97,6 +109,7 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     }
     T p[7];
     predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    if constexpr (LEARNED) apply_learned(r, la, p);
     int chunk;
     const size_t cm = ci.at(z, chunk);
     const size_t n = geo.n;
@@ -127,9 +140,9 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     }
 }
 
-template <typename T, int PRED, bool FINEST>
+template <typename T, int PRED, bool FINEST, bool LEARNED>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
-                                                         QuantParams qp, HistArgs hist)
+                                                         QuantParams qp, HistArgs hist, LearnedArgs<T> la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
@@ -138,6 +151,11 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     const int tid = threadIdx.y * BX + threadIdx.x;
     for (int i = tid; i < 7 * kSmemBins; i += BX * BY) (&sh[0][0])[i] = 0;
     if constexpr (!FINEST) build_recover_lut(lut, qp, tid, BX * BY);
+    if constexpr (LEARNED) {  // the model follows the tile in dynamic shared memory
+        LearnedModel* smodel = reinterpret_cast<LearnedModel*>(smem_raw + kTileBytesAligned<T>);
+        learned_load(smodel, la.model, tid, BX * BY);
+        la.model = smodel;
+    }
     const int wlo = max(0, qp.radius - kSmemBins / 2);
     const int wn = min(kSmemBins, 2 * qp.radius - wlo);
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
@@ -154,7 +172,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};
         if (valid) {
             const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-            encode_point<T, PRED, FINEST, true>(r, io, geo, qp, lut, ci, x, y, z, q);
+            encode_point<T, PRED, FINEST, true, LEARNED>(r, io, geo, qp, lut, ci, x, y, z, q, la);
         }
 #pragma unroll
         for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b], center[b]);
@@ -196,10 +214,11 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
 }
 
 // One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
-template <typename T, int PRED, bool INTERIOR, class Acc>
+template <typename T, int PRED, bool INTERIOR, bool LEARNED = false, class Acc>
 __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp, const T* lut,
                                              const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
-                                             T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z)
+                                             T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z,
+                                             const LearnedArgs<T>& la = LearnedArgs<T>())
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -211,6 +230,7 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     for (int b = 0; b < 7; ++b) q[b] = __ldg(codes + (size_t)b * n + cm);
     T p[7];
     predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    if constexpr (LEARNED) apply_learned(r, la, p);
     T v[8];
     v[0] = r(0);
 #pragma unroll
@@ -229,15 +249,21 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     }
 }
 
-template <typename T, int PRED>
+template <typename T, int PRED, bool LEARNED>
 __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
-                                                         const T* __restrict__ unpred_dense, T* __restrict__ G)
+                                                         const T* __restrict__ unpred_dense, T* __restrict__ G,
+                                                         LearnedArgs<T> la)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ T lut[2 * kRecW];
     build_recover_lut(lut, qp, threadIdx.y * BX + threadIdx.x, BX * BY);
+    if constexpr (LEARNED) {  // the model follows the tile in dynamic shared memory
+        LearnedModel* smodel = reinterpret_cast<LearnedModel*>(smem_raw + kTileBytesAligned<T>);
+        learned_load(smodel, la.model, threadIdx.y * BX + threadIdx.x, BX * BY);
+        la.model = smodel;
+    }
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
     const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
     load_tile(tile, R, dx, dy, dz, x0, y0, z0);
@@ -249,7 +275,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R
     const int z1 = min(z0 + BZ, dz - 2);
     for (int z = z0; z < z1; ++z) {
         const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-        decode_point<T, PRED, true>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z);
+        decode_point<T, PRED, true, LEARNED>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z, la);
     }
 }
 

@@ -55,6 +55,9 @@ constexpr size_t tile_bytes()
 {
     return sizeof(T) * TELEMS;
 }
+// Offset of the learned model behind the tile in dynamic shared memory.
+template <typename T>
+constexpr size_t kTileBytesAligned = (sizeof(T) * TELEMS + 15) & ~(size_t)15;
 
 // Stage the coarse grid on [x0-1, x0+BX+1] x [y0-1, y0+BY+1] x [z0-1, z0+BZ+1]
 // (zero outside the grid; the predictors never read those positions).
@@ -394,6 +397,51 @@ Grid<T> make_grid(const T* p, int dx, int dy, int dz)
     return g;
 }
 
+// Code histograms of the sampled interior points without (hist[0]) and with
+// (hist[1]) the learned correction; thread per sample point.
+template <typename T, int PRED>
+__global__ void __launch_bounds__(256) k_learned_eval(const T* __restrict__ field, size_t fsx, size_t fsy, int s,
+                                                      const T* __restrict__ R, LevelGeom geo, QuantParams qp,
+                                                      LearnedArgs<T> la, int sx, int sy, int sz,
+                                                      uint32_t* __restrict__ hist)
+{
+    __shared__ __align__(16) LearnedModel model;
+    __shared__ uint32_t h[2][7][kEvalBins];
+    for (int i = threadIdx.x; i < 2 * 7 * kEvalBins; i += blockDim.x) (&h[0][0][0])[i] = 0;
+    learned_load(&model, la.model, threadIdx.x, blockDim.x);
+    __syncthreads();
+    using A = Ar<T>;
+    const uint64_t total = (uint64_t)sx * sy * sz;
+    const long long gx = geo.dx, gy = (long long)geo.dx * geo.dy;
+    const int lo = qp.radius - kEvalHalf;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i % sx), iy = (int)((i / sx) % sy), iz = (int)(i / ((uint64_t)sx * sy));
+        const int x = 1 + 2 * ix, y = 1 + 2 * iy, z = 1 + 2 * iz;
+        const GlobalAt<T> r{R + (size_t)z * gy + (size_t)y * gx + x, gx, gy};
+        T p[7], corr[7];
+        predict7<PRED>(r, true, x, y, z, geo.dx, geo.dy, geo.dz, p);
+        learned_corr<T>(model, r, la.rs, la.so, corr);
+#pragma unroll
+        for (int b = 0; b < 7; ++b) {
+            const int si = b + 1, px = si & 1, py = (si >> 1) & 1, pz = si >> 2;
+            const T o = __ldg(field + (size_t)s * (2 * z + pz) * fsy + (size_t)s * (2 * y + py) * fsx +
+                              (size_t)s * (2 * x + px));
+            const int c0 = quantize(A::sub(o, p[b]), qp);
+            const int c1 = quantize(A::sub(o, A::add(p[b], corr[b])), qp);
+            const int k0 = c0 == 0 ? kEvalBins - 1 : min(max(c0 - lo, -1), kEvalBins - 1);
+            const int k1 = c1 == 0 ? kEvalBins - 1 : min(max(c1 - lo, -1), kEvalBins - 1);
+            atomicAdd(&h[0][b][k0 < 0 ? kEvalBins - 1 : k0], 1u);
+            atomicAdd(&h[1][b][k1 < 0 ? kEvalBins - 1 : k1], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * 7 * kEvalBins; i += blockDim.x) {
+        const uint32_t c = (&h[0][0][0])[i];
+        if (c) atomicAdd(hist + i, c);
+    }
+}
+
 // The kernel's dynamic shared memory (its static arrays come on top; above 48
 // KB in total the launch needs this opt-in).
 template <class K>
@@ -414,15 +462,16 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
     HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
     const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
-    const size_t sm = tile_bytes<T>();
+    const bool learned = a.learned.model && a.learned.flags;
+    const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel) : tile_bytes<T>();
     const uint64_t ns = shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
         if (interior) {                                                                                            \
-            auto kern = k_level_encode<T, P, F>;                                                                   \
+            auto kern = learned ? k_level_encode<T, P, F, true> : k_level_encode<T, P, F, false>;                  \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h);                                                  \
+            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned);                                       \
         }                                                                                                          \
         if (ns) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);                \
     } while (0)
@@ -445,21 +494,39 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
     dim3 blk(BX, BY, 1);
     dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + BZ - 1) / BZ);
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
-    const size_t sm = tile_bytes<T>();
+    const bool learned = a.learned.model && a.learned.flags;
+    const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel) : tile_bytes<T>();
     const uint64_t ns = shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
 #define STZ_DEC(P)                                                                                                 \
     do {                                                                                                           \
         if (interior) {                                                                                            \
-            auto kern = k_level_decode<T, P>;                                                                      \
+            auto kern = learned ? k_level_decode<T, P, true> : k_level_decode<T, P, false>;                        \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out);                         \
+            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned);              \
         }                                                                                                          \
         if (ns) k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
     } while (0)
     if (a.predictor == 1) STZ_DEC(1);
     else STZ_DEC(0);
 #undef STZ_DEC
+}
+
+template <typename T>
+void launch_learned_eval(const LevelEncodeArgs<T>& a, uint32_t* hist, cudaStream_t st)
+{
+    const LevelGeom& g = a.geo;
+    const int sx = g.dx > 2 ? (g.dx - 2) / 2 : 0, sy = g.dy > 2 ? (g.dy - 2) / 2 : 0,
+              sz = g.dz > 2 ? (g.dz - 2) / 2 : 0;
+    const uint64_t total = (uint64_t)sx * sy * sz;
+    if (!total || !a.learned.model) return;
+    const int gs = (int)std::min<uint64_t>((total + 255) / 256, 148 * 8);
+    if (a.predictor == 1)
+        k_learned_eval<T, 1><<<gs, 256, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, a.coarse, g, a.qp, a.learned, sx,
+                                                  sy, sz, hist);
+    else
+        k_learned_eval<T, 0><<<gs, 256, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, a.coarse, g, a.qp, a.learned, sx,
+                                                  sy, sz, hist);
 }
 
 template <typename T>
@@ -539,6 +606,7 @@ void launch_dequantize(const int* q, size_t n, QuantParams qp, const T* unpred, 
 #define STZ_INST(T)                                                                                                 \
     template void launch_level_encode<T>(const LevelEncodeArgs<T>&, cudaStream_t);                                  \
     template void launch_level_decode<T>(const LevelDecodeArgs<T>&, cudaStream_t);                                  \
+    template void launch_learned_eval<T>(const LevelEncodeArgs<T>&, uint32_t*, cudaStream_t);                       \
     template void launch_subsample<T>(const T*, int, int, int, int, T*, cudaStream_t);                              \
     template void launch_minmax<T>(const T*, size_t, double*, cudaStream_t);                                        \
     template void launch_split<T>(const T*, int, int, int, T*, cudaStream_t);                                       \

@@ -25,6 +25,7 @@ struct LevelEncodeArgs {
     uint32_t* hist_outside; // 7
     T* decoded;             // decoded fine grid (2dx x 2dy x 2dz) or null on the finest level
     QuantParams qp;
+    LearnedArgs<T> learned; // learned correction (model null: none)
 };
 
 template <typename T>
@@ -36,12 +37,23 @@ struct LevelDecodeArgs {
     const uint16_t* codes;
     const T* unpred_dense;
     T* out;  // fine grid (2dx x 2dy x 2dz)
+    LearnedArgs<T> learned; // learned correction (model null: none)
 };
 
 template <typename T>
 void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st);
 template <typename T>
 void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st);
+
+// Learned-correction choice: on every second interior coarse point per axis
+// (1/8 of them) of a level, the codes of each block with the base prediction
+// (hist[0][b]) and with the correction a.learned adds (hist[1][b]); bins
+// radius-kEvalHalf .. radius+kEvalHalf exactly, every other code (and code 0)
+// in the last bin. hist: 2 x 7 x kEvalBins counters, zeroed by the caller.
+constexpr int kEvalHalf = 128;
+constexpr int kEvalBins = 2 * kEvalHalf + 2;
+template <typename T>
+void launch_learned_eval(const LevelEncodeArgs<T>& a, uint32_t* hist, cudaStream_t st);
 template <typename T>
 void launch_subsample(const T* field, int nx, int ny, int nz, int s, T* out, cudaStream_t st);
 template <typename T>

@@ -58,13 +58,18 @@ __device__ __forceinline__ int find_job(const RoiJob* __restrict__ jobs, int n, 
     return lo;
 }
 
-template <typename T, int PRED>
+template <typename T, int PRED, bool LEARNED>
 __global__ void __launch_bounds__(256) k_roi_cells(const uint8_t* __restrict__ meta, int list, Grid<T> coarse,
                                                    LevelGeom g, Grid<T> base, QuantParams qp,
                                                    const uint16_t* __restrict__ codes,
-                                                   const T* __restrict__ unpred_dense)
+                                                   const T* __restrict__ unpred_dense, LearnedArgs<T> la)
 {
     using A = Ar<T>;
+    __shared__ __align__(16) LearnedModel smodel;
+    if constexpr (LEARNED) {
+        learned_load(&smodel, la.model, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
     const int nj = (int)(list ? h->n_req : h->n_mid);
     const uint64_t total = list ? h->req_total : h->mid_total;
@@ -93,6 +98,15 @@ __global__ void __launch_bounds__(256) k_roi_cells(const uint8_t* __restrict__ m
         const bool interior = cx >= 1 && cx <= g.dx - 3 && cy >= 1 && cy <= g.dy - 3 && cz >= 1 && cz <= g.dz - 3;
         T p[7];
         predict7<PRED>(r, interior, cx, cy, cz, g.dx, g.dy, g.dz, p);
+        if constexpr (LEARNED) {
+            if (interior) {
+                T corr[7];
+                learned_corr<T>(smodel, r, la.rs, la.so, corr);
+#pragma unroll
+                for (int b = 0; b < 7; ++b)
+                    if ((la.flags >> b) & 1u) p[b] = A::add(p[b], corr[b]);
+            }
+        }
         T v[8];
         v[0] = r(0);
 #pragma unroll
@@ -124,20 +138,20 @@ Grid<T> grid_of(const T* p, const LevelGeom& g)
 template <typename T>
 void launch_roi_cells(int grid, int block, const uint8_t* meta, int list, const T* coarse, const LevelGeom& geo,
                       const T* base, const LevelGeom& base_geo, QuantParams qp, int predictor, const uint16_t* codes,
-                      const T* unpred_dense, cudaStream_t st)
+                      const T* unpred_dense, cudaStream_t st, const LearnedArgs<T>& la)
 {
     const Grid<T> gc = grid_of(coarse, geo), gb = grid_of(base, base_geo);
-    if (predictor == 1)
-        k_roi_cells<T, 1><<<grid, block, 0, st>>>(meta, list, gc, geo, gb, qp, codes, unpred_dense);
-    else
-        k_roi_cells<T, 0><<<grid, block, 0, st>>>(meta, list, gc, geo, gb, qp, codes, unpred_dense);
+    const bool learned = la.model && la.flags;
+    auto kern = predictor == 1 ? (learned ? k_roi_cells<T, 1, true> : k_roi_cells<T, 1, false>)
+                               : (learned ? k_roi_cells<T, 0, true> : k_roi_cells<T, 0, false>);
+    kern<<<grid, block, 0, st>>>(meta, list, gc, geo, gb, qp, codes, unpred_dense, la);
 }
 
 template void launch_roi_cells<float>(int, int, const uint8_t*, int, const float*, const LevelGeom&, const float*,
                                       const LevelGeom&, QuantParams, int, const uint16_t*, const float*,
-                                      cudaStream_t);
+                                      cudaStream_t, const LearnedArgs<float>&);
 template void launch_roi_cells<double>(int, int, const uint8_t*, int, const double*, const LevelGeom&,
                                        const double*, const LevelGeom&, QuantParams, int, const uint16_t*,
-                                       const double*, cudaStream_t);
+                                       const double*, cudaStream_t, const LearnedArgs<double>&);
 
 }  // namespace stz

@@ -42,9 +42,11 @@ inline uint64_t job_units(const RoiJob& j) { return (uint64_t)j.ncx * j.ncy * j.
 // coarse: the level's coarse grid (dims geo.dx x geo.dy x geo.dz); base: the
 // decoded base (dims base_geo) for kJobSample entries. A fixed grid walks the
 // units the header lists, so the launch can be captured once and replayed.
+// la: the level's learned correction (applied at interior cells of the
+// flagged blocks; the window must hold the -1..+2 stencil of every such cell).
 template <typename T>
 void launch_roi_cells(int grid, int block, const uint8_t* meta, int list, const T* coarse, const LevelGeom& geo,
                       const T* base, const LevelGeom& base_geo, QuantParams qp, int predictor, const uint16_t* codes,
-                      const T* unpred_dense, cudaStream_t st);
+                      const T* unpred_dense, cudaStream_t st, const LearnedArgs<T>& la = LearnedArgs<T>());
 
 }  // namespace stz

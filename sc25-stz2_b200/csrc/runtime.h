@@ -160,8 +160,31 @@ struct Prepared {
     uint64_t* d_choff = nullptr;
     uint8_t* d_ulist = nullptr;
     uint32_t* d_payload = nullptr;
+    LearnedModel* d_models = nullptr;  // per level k (index k), when the stream has learned corrections
     bool base_valid = false;  // *base holds the decoded base grid (level K-2 output) for box queries
 };
+
+// Learned-correction arguments of level k (none when the level has no flags).
+template <typename T>
+LearnedArgs<T> learned_args(const ParsedStream& ps, int k, const LearnedModel* d_models)
+{
+    LearnedArgs<T> a;
+    const LevelDir& L = ps.lv[k];
+    if (!L.lflags || !d_models) return a;
+    a.model = d_models + k;
+    a.flags = L.lflags;
+    a.rs = (T)(1.0 / (L.eb * L.model.s_in));
+    a.so = (T)(L.model.s_out * L.eb);
+    return a;
+}
+
+// Any level of the stream carries a learned correction.
+inline bool stream_learned(const ParsedStream& ps)
+{
+    for (size_t k = 1; k < ps.lv.size(); ++k)
+        if (ps.lv[k].lflags) return true;
+    return false;
+}
 
 // CTA work items for chunk lists: groups of up to kCoderThreads / C chunks.
 void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, const uint32_t* chunks,
@@ -223,7 +246,7 @@ struct stz_context {
     }
     stz::DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
-        tiles;
+        tiles, models, eval;
     stz::PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small;
     // device buffers lent to one-off decodes
     stz::DevBuf p_stage, p_coarsest, p_base;
@@ -240,6 +263,24 @@ struct stz_stream {
     stz::ParsedStream dir;
     size_t raw_payload_bytes = 0;
     std::unique_ptr<stz::Prepared> resident;
+};
+
+// Learned models of the second-finest (lv[0]) and finest (lv[1]) levels.
+struct stz_model {
+    uint32_t mask = 0;  // bit i: lv[i] present
+    stz::LearnedModel lv[2]{};
+    std::vector<uint8_t> bytes;  // serialized form, kept for stz_model_bytes
+    void serialize()
+    {
+        bytes.assign({'S', 'T', 'Z', 'L', 'M', 'D', 'L', '1'});
+        const uint8_t* m = (const uint8_t*)&mask;
+        bytes.insert(bytes.end(), m, m + 4);
+        for (int i = 0; i < 2; ++i)
+            if (mask >> i & 1u) {
+                const uint8_t* r = (const uint8_t*)&lv[i];
+                bytes.insert(bytes.end(), r, r + sizeof(stz::LearnedModel));
+            }
+    }
 };
 
 namespace stz {

@@ -326,11 +326,14 @@ void plan_request(SrvStream& ss, Build& b, const Ticket& t, void* out)
         for (const BlockPlan& bp : plan.high)
             for (int64_t c : bp.chunks) list_chunk(ss, b, 7 + bp.block, (uint32_t)c);
         int m0[3], m1[3];
-        if (region_bbox(plan, m0, m1)) {
-            // The mid grid is rebuilt on the regions' bounding box: decode the
-            // low chunks of every cell of that box (a superset of the
-            // planner's low chunks, FD5:1784-1830), so every mid value written
-            // is the full decode's value.
+        const bool learned_high = ss.s->dir.lv[ss.K].lflags != 0;
+        if (mid_window(plan, 2 * ss.low.dx, 2 * ss.low.dy, 2 * ss.low.dz, learned_high, m0, m1)) {
+            // The mid grid is rebuilt on the regions' bounding box (grown to
+            // the learned stencil of every query cell when the finest level
+            // has a learned correction): decode the low chunks of every cell
+            // of that box (a superset of the planner's low chunks,
+            // FD5:1784-1830), so every mid value written is the full decode's
+            // value.
             const int C = ss.low.C;
             const int c0[3] = {(m0[0] >> 1) / C, (m0[1] >> 1) / C, (m0[2] >> 1) / C};
             const int c1[3] = {(m1[0] >> 1) / C, (m1[1] >> 1) / C, (m1[2] >> 1) / C};
@@ -415,10 +418,11 @@ void enqueue_kernels(const SrvStream& ss, const LaunchShape& sh, const uint8_t* 
     if (p.total_unpred)
         launch_unpred_scatter_dyn<T>(sh.unpred_grid, meta, p.d_sd, codes, ss.unpred.as<T>(), (T*)p.d_ulist, st);
     const T* base = p.base->as<T>();
+    const ParsedStream& ps = ss.s->dir;
     launch_roi_cells<T>(sh.roi_grid, sh.roi_block, meta, 0, base, ss.low, base, ss.low, ss.qlow, ss.predictor,
-                        ss.low_codes(), ss.low_unpred<T>(), st);
+                        ss.low_codes(), ss.low_unpred<T>(), st, learned_args<T>(ps, ss.K - 1, p.d_models));
     launch_roi_cells<T>(sh.roi_grid, sh.roi_block, meta, 1, ss.mid.as<T>(), ss.high, base, ss.low, ss.qhigh,
-                        ss.predictor, ss.high_codes(), ss.high_unpred<T>(), st);
+                        ss.predictor, ss.high_codes(), ss.high_unpred<T>(), st, learned_args<T>(ps, ss.K, p.d_models));
 }
 
 template <typename T>
@@ -432,6 +436,7 @@ void enqueue_level_job(const SrvStream& ss, const LevelJob& j, cudaStream_t st)
     a.codes = ss.low_codes();
     a.unpred_dense = ss.low_unpred<T>();
     a.out = j.level == 1 ? (T*)j.out : ss.mid.as<T>();
+    a.learned = learned_args<T>(ss.s->dir, ss.K - 1, ss.p->d_models);
     launch_level_decode<T>(a, st);
     if (j.level == 1) return;
     a.coarse = ss.mid.as<T>();
@@ -440,6 +445,7 @@ void enqueue_level_job(const SrvStream& ss, const LevelJob& j, cudaStream_t st)
     a.codes = ss.high_codes();
     a.unpred_dense = ss.high_unpred<T>();
     a.out = (T*)j.out;
+    a.learned = learned_args<T>(ss.s->dir, ss.K, ss.p->d_models);
     launch_level_decode<T>(a, st);
 }
 

@@ -393,6 +393,83 @@ __device__ __forceinline__ void predict7(const Acc& r, bool interior, int x, int
     }
 }
 
+// ---- learned correction (LearnedModel in stz_internal.h) -------------------
+// Exact integer inference: the encoder, the decoder and the ROI path compute
+// the same 7 corrections bit for bit.
+__device__ __forceinline__ int learned_to_i8(float t)
+{
+    if (!(t == t)) return 0;
+    if (t >= 127.f) return 127;
+    if (t <= -127.f) return -127;
+    return __float2int_rn(t);
+}
+__device__ __forceinline__ int learned_to_i8(double t)
+{
+    if (!(t == t)) return 0;
+    if (t >= 127.0) return 127;
+    if (t <= -127.0) return -127;
+    return __double2int_rn(t);
+}
+__device__ __forceinline__ uint32_t learned_requant(int acc, int m, int sh)
+{
+    const long long p = ((long long)acc * m + (1ll << (sh - 1))) >> sh;
+    return p < 0 ? 0u : (p > 127 ? 127u : (uint32_t)p);
+}
+
+// The 7 corrections at a coarse point (accessor r positioned on it; the
+// stencil reaches -1..+2 on each axis). M is usually in shared memory.
+template <typename T, class Acc>
+__device__ __forceinline__ void learned_corr(const LearnedModel& M, const Acc& r, T rs, T so, T (&corr)[7])
+{
+    using A = Ar<T>;
+    constexpr int st[14][3] = STZ_LEARNED_STENCIL;
+    T v[14];
+#pragma unroll
+    for (int i = 0; i < 14; ++i) v[i] = r(st[i][2] * (long long)r.sy + st[i][1] * (long long)r.sx + st[i][0]);
+    T m = v[0];
+#pragma unroll
+    for (int i = 1; i < 8; ++i) m = A::add(m, v[i]);
+    m = A::mul(m, T(0.125));
+    uint32_t xw[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int i = 0; i < 14; ++i)
+        xw[i >> 2] |= ((uint32_t)learned_to_i8(A::mul(A::sub(v[i], m), rs)) & 0xffu) << (8 * (i & 3));
+    const int* w1 = reinterpret_cast<const int*>(&M.w1[0][0]);
+    const int* w2 = reinterpret_cast<const int*>(&M.w2[0][0]);
+    const int* w3 = reinterpret_cast<const int*>(&M.w3[0][0]);
+    uint32_t a1[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        int acc = M.b1[j];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) acc = __dp4a(w1[j * 4 + w], (int)xw[w], acc);
+        a1[j >> 2] |= learned_requant(acc, M.m1, M.sh1) << (8 * (j & 3));
+    }
+    uint32_t a2[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        int acc = M.b2[j];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) acc = __dp4a(w2[j * 8 + w], (int)a1[w], acc);
+        a2[j >> 2] |= learned_requant(acc, M.m2, M.sh2) << (8 * (j & 3));
+    }
+#pragma unroll
+    for (int o = 0; o < 7; ++o) {
+        int acc = M.b3[o];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) acc = __dp4a(w3[o * 8 + w], (int)a2[w], acc);
+        corr[o] = A::mul((T)acc, so);
+    }
+}
+
+// Copy a model into shared memory (all threads of the block; caller syncs).
+__device__ __forceinline__ void learned_load(LearnedModel* dst, const LearnedModel* src, int tid, int nthreads)
+{
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    for (int i = tid; i < (int)(sizeof(LearnedModel) / 16); i += nthreads) d[i] = s[i];
+}
+
 // Runtime-block predictor on a global grid (boundary-kernel and ROI paths).
 template <int PRED, typename T>
 __device__ __forceinline__ T predict(int block, const Grid<T>& g, int x, int y, int z)

@@ -21,6 +21,45 @@ constexpr int kHistWindow = 4096;
 // Threads of one entropy-coding CTA; a CTA covers 128 / C chunks of a stream.
 constexpr int kCoderThreads = 128;
 
+// Learned correction of one level (this project's addition; no reference
+// counterpart): an int8 MLP 14 -> 32 -> 32 -> 7 on the 14-point stencil of a
+// coarse cell (STZ_LEARNED_STENCIL). Inputs: stencil values minus the mean of
+// the 8 cell corners, times rs = 1 / (eb * s_in), rounded to int8 (clamped to
+// +-127). Hidden layers: int32 accumulation, ReLU and fixed-point
+// requantization a = clamp((acc * m + 2^(sh-1)) >> sh, 0, 127). Output o,
+// acc_o * (s_out * eb), is added to the base prediction of block o at interior
+// cells (1 <= x,y,z <= dim-3) of the blocks a per-level flag selects. The
+// struct is the 2112-byte little-endian record stored in the container.
+struct LearnedModel {
+    double s_in, s_out;
+    int8_t w1[32][16];  // columns 14, 15 are zero
+    int32_t b1[32], m1, sh1;
+    int8_t w2[32][32];
+    int32_t b2[32], m2, sh2;
+    int8_t w3[8][32];   // row 7 unused
+    int32_t b3[8];
+};
+static_assert(sizeof(LearnedModel) == 2112, "LearnedModel is a fixed on-disk record");
+
+// Stencil of the learned correction around coarse point (x, y, z): the 8
+// corners of the cell, then (-1,0,0), (0,-1,0), (0,0,-1), (2,1,1), (1,2,1),
+// (1,1,2) (x, y, z offsets).
+#define STZ_LEARNED_STENCIL                                                                                       \
+    {                                                                                                             \
+        {0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}, {-1, 0, 0},       \
+            {0, -1, 0}, {0, 0, -1}, {2, 1, 1}, {1, 2, 1}, {1, 1, 2}                                               \
+    }
+
+// What a level kernel needs to apply a learned correction (model == nullptr:
+// none). rs and so in the level's value type, computed on the host as
+// (T)(1 / (eb * s_in)) and (T)(s_out * eb).
+template <typename T>
+struct LearnedArgs {
+    const LearnedModel* model = nullptr;  // device memory
+    uint32_t flags = 0;                    // blocks (bit b) that use it
+    T rs = T(0), so = T(0);
+};
+
 // Quantizer constants of one level (FD5:1208-1210): eb, 1/eb computed once on
 // the host (recip = 1.0 / eb), radius.
 struct QuantParams {

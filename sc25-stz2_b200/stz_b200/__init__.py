@@ -40,6 +40,7 @@ class Opts(C.Structure):
         ("mult_base", C.c_double), ("mult_low", C.c_double), ("mult_high", C.c_double),
         ("radius", C.c_int), ("chunk_high", C.c_int), ("chunk_low", C.c_int),
         ("zstd_level", C.c_int), ("predictor", C.c_int), ("threads", C.c_int),
+        ("model", C.c_void_p), ("learned_flags", C.c_int),
     ]
 
 
@@ -49,6 +50,7 @@ class Info(C.Structure):
         ("n_levels", C.c_int), ("radius", C.c_int), ("chunk_high", C.c_int), ("chunk_low", C.c_int),
         ("eb", C.c_double), ("mult_base", C.c_double), ("mult_low", C.c_double), ("mult_high", C.c_double),
         ("max_error", C.c_double), ("stream_bytes", C.c_size_t), ("raw_payload_bytes", C.c_size_t),
+        ("learned_flags", C.c_int),
     ]
 
 
@@ -113,6 +115,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_server_release.argtypes = [vp, C.c_uint64]
     lib.stz_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
     lib.stz_server_batch_log.argtypes = [vp, C.POINTER(BatchRecord), sz, C.POINTER(sz)]
+    lib.stz_model_parse.argtypes = [vp, sz, C.POINTER(vp)]
+    lib.stz_model_bytes.argtypes = [vp, C.POINTER(vp), C.POINTER(sz)]
+    lib.stz_model_free.argtypes = [vp]
+    lib.stz_model_free.restype = None
     _lib = lib
     return lib
 
@@ -165,6 +171,9 @@ def default_opts(**kw) -> Opts:
             v = bounds[v]
         elif k == "predictor" and isinstance(v, str):
             v = preds[v]
+        elif k == "model":
+            o._model_ref = v  # the model must outlive the options that point at it
+            v = None if v is None else (v.handle.value if isinstance(v, Model) else v)
         if not hasattr(o, k):
             raise TypeError(f"unknown option {k}")
         setattr(o, k, v)
@@ -214,6 +223,37 @@ class StreamInfo:
     max_error: float
     stream_bytes: int
     raw_payload_bytes: int
+    learned_flags: int = 0  # bits 0-6: second-finest level's blocks, 8-14: finest level's
+
+
+class Model:
+    """Learned-correction models of the second-finest and finest levels
+    (library-owned; the "STZLMDL1" file format of stz_model_parse)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "Model":
+        lib = load_library()
+        h = C.c_void_p()
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(lib.stz_model_parse(buf, len(data), C.byref(h)))
+        return cls(h.value)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.stz_model_free(self._h)
+            self._h = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def to_bytes(self) -> bytes:
+        p, n = C.c_void_p(), C.c_size_t()
+        _check(_lib.stz_model_bytes(self._h, C.byref(p), C.byref(n)))
+        return C.string_at(p, n.value)
 
 
 class Stream:
@@ -246,7 +286,7 @@ class Stream:
         _check(_lib.stz_stream_info(self._h, C.byref(i)))
         return StreamInfo(_np_dtype(i.dtype), i.predictor, (i.nz, i.ny, i.nx), i.n_levels, i.radius, i.chunk_high,
                           i.chunk_low, i.eb, (i.mult_base, i.mult_low, i.mult_high), i.max_error, i.stream_bytes,
-                          i.raw_payload_bytes)
+                          i.raw_payload_bytes, i.learned_flags)
 
 
 class Context:

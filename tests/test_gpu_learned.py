@@ -1,0 +1,163 @@
+"""Learned correction (container version 2): the int8 MLP correction inside
+the level, ROI and server kernels, called through the C ABI, against the
+oracle's restatement. Streams must be identical byte for byte and every
+decode (full, progressive, box / slice, resident, served) bit for bit, for
+forced and automatically chosen block flags."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import stz_b200
+from conftest import model_file, random_model
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def bits(a):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
+
+
+def make_field(gen, shape, dtype, seed):
+    from stz_b200 import fields
+
+    if gen == "grf":
+        return fields.grf(shape, 11.0 / 3.0, seed, dtype)
+    if gen == "logn":
+        return fields.lognormal(shape, seed, dtype)
+    return fields.fronts(shape, seed, dtype)
+
+
+def crop(full, lo, hi):
+    """The box (lo, hi) of a (z, y, x) array with the planner's clamping."""
+    sl = []
+    for ax, n in zip((2, 1, 0), full.shape):
+        a_, b_ = lo[ax], hi[ax]
+        if a_ == b_:
+            v = max(0, min(a_, n - 1))
+            sl.append(slice(v, v + 1))
+        else:
+            sl.append(slice(max(0, min(a_, b_)), min(n - 1, max(a_, b_)) + 1))
+    return full[tuple(sl)]
+
+
+def queries(rng, dims_xyz, n):
+    nx, ny, nz = dims_xyz
+    q = [((0, 0, 0), (nx - 1, ny - 1, nz - 1)), ((1, 1, 1), (2, 2, 2)), ((nx - 3, 0, 5), (nx - 1, ny - 1, 5)),
+         ((7, 3, 0), (7, 3, nz - 1)), ((-4, 2, 3), (nx + 9, 2, nz // 2))]
+    for _ in range(n):
+        a = rng.integers(0, [nx, ny, nz])
+        b = np.minimum(a + rng.integers(0, 24, 3), [nx - 1, ny - 1, nz - 1])
+        q.append((tuple(int(v) for v in a), tuple(int(v) for v in b)))
+    return q
+
+
+CASES = [
+    # (generator, shape (z, y, x), dtype, rel eb, predictor, chunks, flags (second-finest, finest))
+    ("grf", (64, 64, 64), np.float32, 1e-3, 0, (16, 8), (0x7F, 0x7F)),
+    ("logn", (64, 64, 128), np.float32, 1e-4, 1, (16, 8), (0x15, 0x6A)),
+    ("fronts", (32, 48, 64), np.float64, 1e-6, 0, (8, 4), (0x00, 0x7F)),
+    ("grf", (32, 32, 32), np.float64, 1e-5, 1, (8, 4), (0x41, 0x00)),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}-{np.dtype(c[2]).name}-p{c[4]}-{c[6][0]:x}-{c[6][1]:x}"
+                                             for c in CASES])
+def test_forced_flags_match_oracle(ctx, case):
+    gen, shape, dtype, rel, pred, (ch, cl), flags = case
+    f = make_field(gen, shape, dtype, 31)
+    rng = np.random.default_rng(5)
+    m0, m1 = random_model(rng), random_model(rng)
+    model = stz_b200.Model.from_bytes(model_file((m0, m1)))
+    lf = flags[0] | flags[1] << 8
+    s = ctx.compress(f, eb=rel, eb_mode="rel", predictor=pred, chunk_high=ch, chunk_low=cl, model=model,
+                     learned_flags=lf)
+    inf = s.info()
+    assert inf.learned_flags == lf
+    ref = po.compress(f, inf.eb, predictor=pred, chunk_high=ch, chunk_low=cl, models=(m0, m1), flags=flags)
+    assert s.to_bytes() == ref
+    plain = po.compress(f, inf.eb, predictor=pred, chunk_high=ch, chunk_low=cl)
+    assert ref != plain  # the correction changed the residuals
+    out = ctx.decompress(s)
+    assert np.array_equal(bits(out), bits(po.decompress(ref)))
+    E = rel * (float(f.max()) - float(f.min()))
+    assert np.abs(out.astype(np.float64) - f.astype(np.float64)).max() <= E
+    for lvl in (1, 2):
+        assert np.array_equal(bits(ctx.decompress(s, level=lvl)), bits(po.decompress(ref, lvl)))
+    # boxes and slices: the learned stencil reaches -1..+2 around every cell
+    for lo, hi in queries(np.random.default_rng(2), (shape[2], shape[1], shape[0]), 10):
+        assert np.array_equal(bits(ctx.decompress_box(s, lo, hi)), bits(crop(out, lo, hi))), (lo, hi)
+    # a parsed copy, and the resident path
+    s2 = ctx.parse(ref)
+    assert s2.info().learned_flags == lf
+    assert np.array_equal(bits(ctx.decompress(s2)), bits(out))
+    ctx.upload(s2)
+    assert np.array_equal(bits(ctx.decompress(s2)), bits(out))
+    assert np.array_equal(bits(ctx.decompress(s2, level=1)), bits(po.decompress(ref, 1)))
+    lo, hi = (3, 5, 7), (40, 30, 20)
+    assert np.array_equal(bits(ctx.decompress_box(s2, lo, hi)), bits(crop(out, lo, hi)))
+
+
+def test_single_level_models(ctx):
+    """A model file with only the finest (or only the second-finest) record."""
+    f = make_field("grf", (32, 32, 64), np.float32, 3)
+    rng = np.random.default_rng(8)
+    m = random_model(rng)
+    for recs, flags in (((None, m), (0, 0x7F)), ((m, None), (0x7F, 0))):
+        model = stz_b200.Model.from_bytes(model_file(recs))
+        s = ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=8, chunk_low=4, model=model, learned_flags=0x7F7F)
+        assert s.info().learned_flags == flags[0] | flags[1] << 8
+        ref = po.compress(f, s.info().eb, chunk_high=8, chunk_low=4, models=recs, flags=(0x7F, 0x7F))
+        assert s.to_bytes() == ref
+        assert np.array_equal(bits(ctx.decompress(s)), bits(po.decompress(ref)))
+
+
+def test_automatic_flags_reproduce_in_oracle(ctx):
+    """Whatever blocks the sampled estimate picks, the stream is the oracle's
+    for those flags; a correction far off the residuals is never picked."""
+    f = make_field("grf", (64, 64, 64), np.float32, 12)
+    rng = np.random.default_rng(21)
+    m0, m1 = random_model(rng), random_model(rng)
+    model = stz_b200.Model.from_bytes(model_file((m0, m1)))
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=16, chunk_low=8, model=model)
+    lf = s.info().learned_flags
+    ref = po.compress(f, s.info().eb, chunk_high=16, chunk_low=8, models=(m0, m1), flags=(lf & 0x7F, lf >> 8))
+    assert s.to_bytes() == ref
+    # a constant correction of ~10^4 error bounds on every block
+    bad = random_model(rng, s_out=50.0)
+    for o in range(7):
+        for i in range(32):
+            bad.w3[o][i] = 0
+        bad.b3[o] = 200
+    model = stz_b200.Model.from_bytes(model_file((bad, bad)))
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=16, chunk_low=8, model=model)
+    assert s.info().learned_flags == 0
+    assert s.to_bytes() == ctx.compress(f, eb=1e-3, eb_mode="rel", chunk_high=16, chunk_low=8).to_bytes()
+
+
+def test_served_requests_equal_single_decodes(ctx):
+    from stz_b200 import Server
+
+    f = make_field("fronts", (64, 64, 64), np.float64, 4)
+    rng = np.random.default_rng(6)
+    m0, m1 = random_model(rng), random_model(rng)
+    model = stz_b200.Model.from_bytes(model_file((m0, m1)))
+    s = ctx.compress(f, eb=1e-5, eb_mode="rel", chunk_high=16, chunk_low=8, model=model, learned_flags=0x7F7F)
+    full = ctx.decompress(s)
+    srv = Server(0, arena_bytes=128 << 20, max_batch=16)
+    try:
+        sid = srv.add_stream(s)
+        reqs = [("box", lo, hi) for lo, hi in queries(np.random.default_rng(3), (64, 64, 64), 14)]
+        reqs += [("level", 0), ("level", 1), ("level", 2)]
+        tickets = [srv.submit_box(sid, r[1], r[2]) if r[0] == "box" else srv.submit_level(sid, r[1]) for r in reqs]
+        for r, t in zip(reqs, tickets):
+            res = srv.wait(t)
+            assert res.status == 0, r
+            got = srv.copy_out(res, np.float64)
+            want = crop(full, r[1], r[2]) if r[0] == "box" else ctx.decompress(s, level=r[1])
+            assert np.array_equal(bits(got), bits(want)), r
+            srv.release(t)
+    finally:
+        srv.close()

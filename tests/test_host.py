@@ -10,7 +10,7 @@ import pytest
 
 import pyoracle as po
 import stz_b200
-from conftest import ROOT
+from conftest import ROOT, random_model
 
 
 def test_library_exports_every_declared_symbol():
@@ -36,6 +36,60 @@ def test_default_opts_are_reference_defaults():
     o = stz_b200.default_opts()
     assert (o.mult_base, o.mult_low, o.mult_high) == (0.7, 2.7, 8.2)
     assert (o.radius, o.chunk_high, o.chunk_low, o.zstd_level) == (32768, 32, 16, 3)
+    assert o.model is None and o.learned_flags == -1
+
+
+def test_struct_offsets_match_the_c_compiler(tmp_path):
+    """Field offsets of the option / info structs as gcc lays them out."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "stz/stz.h"', "int main(void) {"]
+    for struct, cls in (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info)):
+        lines.append('printf("%%zu\\n", sizeof(%s));' % struct)
+        for f, _ in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (struct, f))
+    lines.append("return 0; }")
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for cls in (stz_b200.Opts, stz_b200.Info):
+        want.append(ctypes.sizeof(cls))
+        want += [getattr(cls, f).offset for f, _ in cls._fields_]
+    assert got == want
+
+
+def _random_model_record(rng, s_in=4.0, s_out=0.05, sh=(9, 9)):
+    return po.model_record(random_model(rng, s_in=s_in, s_out=s_out, sh=sh))
+
+
+def test_model_bytes_round_trip_and_validation():
+    rng = np.random.default_rng(11)
+    r0, r1 = _random_model_record(rng), _random_model_record(rng)
+    for mask, recs in ((1, [r0]), (2, [r1]), (3, [r0, r1])):
+        data = b"STZLMDL1" + np.uint32(mask).tobytes() + b"".join(recs)
+        m = stz_b200.Model.from_bytes(data)
+        assert m.to_bytes() == data
+    good = b"STZLMDL1" + np.uint32(3).tobytes() + r0 + r1
+    bad_cases = [
+        b"STZLMDL0" + good[8:],                              # magic
+        good[:-1],                                           # truncated
+        b"STZLMDL1" + np.uint32(0).tobytes(),                # empty mask
+        b"STZLMDL1" + np.uint32(4).tobytes() + r0,           # unknown record bit
+        b"STZLMDL1" + np.uint32(1).tobytes() + _random_model_record(rng, s_in=0.0),  # scale must be > 0
+        b"STZLMDL1" + np.uint32(1).tobytes() + _random_model_record(rng, s_out=float("nan")),
+        b"STZLMDL1" + np.uint32(2).tobytes() + _random_model_record(rng, sh=(0, 9)),  # shift out of range
+        b"STZLMDL1" + np.uint32(2).tobytes() + _random_model_record(rng, sh=(9, 63)),
+    ]
+    for data in bad_cases:
+        with pytest.raises(stz_b200.StzError) as e:
+            stz_b200.Model.from_bytes(data)
+        assert e.value.status == 5
 
 
 def _hists():
@@ -121,7 +175,7 @@ def test_ctypes_structs_match_header():
                         ("stz_result", stz_b200.Result), ("stz_server_stats", stz_b200.ServerStats)):
         body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (struct, struct), hdr, re.S).group(1)
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
-        fields = re.findall(r"^\s*(?:const\s+)?(?:u?int64_t|int|double|size_t|stz_status|void)\b\s*\**\s*"
+        fields = re.findall(r"^\s*(?:const\s+)?(?:struct\s+\w+|u?int64_t|int|double|size_t|stz_status|void)\b\s*\**\s*"
                             r"([a-z0-9_, \[\]]+);", body, re.M)
         names = [re.sub(r"\[\d+\]", "", n).strip() for f in fields for n in f.split(",")]
         assert names == [f[0] for f in cls._fields_], struct
