@@ -199,6 +199,59 @@ stz_status stz_model_parse(const void* data, size_t size, stz_model** out);
 stz_status stz_model_bytes(const stz_model* m, const void** data, size_t* size);
 void stz_model_free(stz_model* m);
 
+/* ---- training (on the GPU) --------------------------------------------- *
+ * Pairs come from the compressor itself: for the second-finest and finest
+ * levels, the decoded coarse grid the level predicts from (its 14-point cell
+ * stencil, minus the mean of the 8 corners, in units of the level's eb) and
+ * the true fine values minus the plain prediction (in eb). Each level's MLP
+ * is trained with BF16 operands and FP32 accumulation (forward, backward and
+ * Adam are this library's kernels; a training run is replayed from CUDA
+ * graphs), then quantization-aware trained and exported to int8. */
+typedef struct stz_train_opts {
+    int epochs;          /* float epochs (default 8) */
+    int qat_epochs;      /* quantization-aware epochs (default 3) */
+    int batch;           /* samples per Adam step, a multiple of 128 (default 4096) */
+    double lr;           /* Adam step size (default 2e-3; QAT uses lr / 8), cosine decay */
+    double huber_delta;  /* loss: Huber on the residual, in eb (default 2) */
+    int sample_step;     /* pairs from every n-th interior coarse cell per axis (default 2) */
+    size_t max_pairs;    /* pairs kept per level (default 1 << 23) */
+    uint64_t seed;       /* initialisation and shuffling (default 1) */
+} stz_train_opts;
+void stz_default_train_opts(stz_train_opts* t);
+
+typedef struct stz_train_stats {
+    size_t pairs[2];       /* (second-finest, finest) */
+    double loss_zero[2];   /* mean Huber loss per residual without a correction, eb^2 */
+    double loss_float[2];  /* after the float epochs */
+    double loss_qat[2];    /* after quantization-aware training (fake-quantized forward) */
+    double loss_int8[2];   /* exported int8 model, integer inference on the stored features */
+    double s_in[2], s_t[2];/* input and target scales */
+    double train_ms;       /* device time of the fit */
+} stz_train_stats;
+
+typedef struct stz_trainer stz_trainer;
+/* opts: the compressor options the pairs are generated with (eb, eb_mode,
+ * predictor, multipliers...); its model field is ignored. */
+stz_status stz_trainer_create(stz_context* ctx, const stz_opts* opts, const stz_train_opts* topts,
+                              stz_trainer** out);
+/* Adds the pairs of one field (device memory, x fastest). */
+stz_status stz_trainer_add_field_dev(stz_trainer* t, const void* field_dev, stz_dtype dtype, size_t nx, size_t ny,
+                                     size_t nz);
+/* Trains both levels and returns the int8 model (free with stz_model_free). */
+stz_status stz_trainer_fit(stz_trainer* t, stz_model** out);
+stz_status stz_trainer_stats(const stz_trainer* t, stz_train_stats* st);
+void stz_trainer_free(stz_trainer* t);
+
+/* One forward + backward pass of the training kernels over n samples, for
+ * gradient checks: params (1864 floats: W1[32][16], b1[32], W2[32][32],
+ * b2[32], W3[8][32], b3[8]) as the master weights, x n x 16 features in eb
+ * (rounded to BF16 as stored), t n x 8 targets in eb; s_in, s_t the scales,
+ * qat 0/1 with activation scales sa[2]. Writes the mean loss (normalised
+ * units) and the 1864 gradients. */
+stz_status stz_debug_mlp_grad(stz_context* ctx, const float* params, const float* x, const float* t, size_t n,
+                              double s_in, double s_t, double huber_delta, int qat, const double sa[2], float* grad,
+                              double* loss);
+
 /* ---- reference function boundary (device pointers) --------------------- *
  * The reference's own stage functions, one for one, for callers that drive
  * the stages themselves. Block = sub_index - 1 (0..6); dims are the block's.  */

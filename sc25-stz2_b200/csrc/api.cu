@@ -58,17 +58,7 @@ QuantParams make_quant_params(double eb, int radius)
     return q;
 }
 
-// Shape of the hierarchy for given dims and options.
-struct Geometry {
-    int nx = 0, ny = 0, nz = 0, K = 0, radius = 0, chunk_high = 0, chunk_low = 0;
-    int c0[3] = {0, 0, 0};
-    std::vector<LevelGeom> lv;  // 1..K
-    std::vector<StreamDesc> sd; // stream (k-1)*7+b
-    uint64_t total_codes = 0, total_chunk_slots = 0, total_sub = 0, total_words = 0;
-    size_t n_fine_max = 0;      // largest intermediate decoded grid (elements)
-};
-
-static Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_low, int radius)
+Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_low, int radius)
 {
     Geometry g;
     g.nx = nx, g.ny = ny, g.nz = nz;
@@ -179,6 +169,48 @@ uint32_t choose_learned_flags(const uint32_t* hist, size_t elem)
     return 8.0 * saved > 8.0 * (double)(sizeof(LearnedModel) + 4) ? flags : 0u;
 }
 
+// ---- error bounds ----------------------------------------------------------------
+template <typename T>
+stz_status level_error_bounds(stz_context* ctx, const T* field, size_t N, const stz_opts& o, int K, double& eb,
+                              std::vector<double>& ebk)
+{
+    cudaStream_t st = ctx->st;
+    // value range as computeRange (FD5:92-104)
+    STZ_CUDA(ctx->minmax.ensure(16));
+    STZ_CUDA(ctx->h_small.ensure(64));
+    {
+        KScope ks(ctx, "k_minmax");
+        launch_minmax<T>(field, N, ctx->minmax.as<double>(), st);
+    }
+    STZ_CUDA(cudaMemcpyAsync(ctx->h_small.p, ctx->minmax.p, 16, cudaMemcpyDeviceToHost, st));
+    STZ_CUDA(cudaStreamSynchronize(st));
+    const unsigned long long* mk = ctx->h_small.as<unsigned long long>();
+    const double lo = minmax_key_to_double(mk[0]), hi = minmax_key_to_double(mk[1]);
+    double E = o.eb;
+    if (o.eb_mode == STZ_EB_REL) {
+        E = o.eb * (hi - lo);
+        if (!(E > 0) || !std::isfinite(E)) E = o.eb;  // constant (or non-finite) field: bound taken as absolute
+    }
+    // The quantizer bounds each residual by eb, but the reconstruction
+    // dq + P is rounded once more in T, so the reference overshoots its bound
+    // by up to ~1.5 ulp of the largest magnitude. The pointwise mode leaves
+    // 4 ulp of slack so that max|x - x'| <= E holds when checked in FP64.
+    eb = E;
+    if (o.bound_mode == STZ_BOUND_POINTWISE) {
+        const double ulp = sizeof(T) == 4 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
+        const double slack = 4.0 * std::max(std::fabs(lo), std::fabs(hi)) * ulp;
+        const double Eb = (std::isfinite(slack) && E > 2.0 * slack) ? E - slack : 0.5 * E;
+        eb = Eb / std::max({o.mult_base, o.mult_low, o.mult_high});
+    }
+    ebk.assign(K + 1, 0.0);
+    for (int k = 1; k <= K; ++k) ebk[k] = (k == K ? o.mult_high : k == K - 1 ? o.mult_low : o.mult_base) * eb;
+    return STZ_OK;
+}
+template stz_status level_error_bounds<float>(stz_context*, const float*, size_t, const stz_opts&, int, double&,
+                                              std::vector<double>&);
+template stz_status level_error_bounds<double>(stz_context*, const double*, size_t, const stz_opts&, int, double&,
+                                               std::vector<double>&);
+
 // ---- compress ----------------------------------------------------------------
 template <typename T>
 stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int nz, const stz_opts& o,
@@ -191,37 +223,10 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const int nstreams = 7 * K;
     const size_t N = (size_t)nx * ny * nz;
     const size_t elem = sizeof(T);
-
-    // error bound: value range as computeRange (FD5:92-104)
-    STZ_CUDA(ctx->minmax.ensure(16));
-    STZ_CUDA(ctx->h_small.ensure(64));
-    {
-        KScope ks(ctx, "k_minmax");
-        launch_minmax<T>(field, N, ctx->minmax.as<double>(), st);
-    }
-    STZ_CUDA(cudaMemcpyAsync(ctx->h_small.p, ctx->minmax.p, 16, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaStreamSynchronize(st));
+    double eb = 0;
+    std::vector<double> ebk;
+    STZ_TRY(level_error_bounds<T>(ctx, field, N, o, K, eb, ebk));
     lap.mark("value range");
-    const unsigned long long* mk = ctx->h_small.as<unsigned long long>();
-    const double lo = minmax_key_to_double(mk[0]), hi = minmax_key_to_double(mk[1]);
-    double E = o.eb;
-    if (o.eb_mode == STZ_EB_REL) {
-        E = o.eb * (hi - lo);
-        if (!(E > 0) || !std::isfinite(E)) E = o.eb;  // constant (or non-finite) field: bound taken as absolute
-    }
-    // The quantizer bounds each residual by eb, but the reconstruction
-    // dq + P is rounded once more in T, so the reference overshoots its bound
-    // by up to ~1.5 ulp of the largest magnitude. The pointwise mode leaves
-    // 4 ulp of slack so that max|x - x'| <= E holds when checked in FP64.
-    double eb = E;
-    if (o.bound_mode == STZ_BOUND_POINTWISE) {
-        const double ulp = sizeof(T) == 4 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
-        const double slack = 4.0 * std::max(std::fabs(lo), std::fabs(hi)) * ulp;
-        const double Eb = (std::isfinite(slack) && E > 2.0 * slack) ? E - slack : 0.5 * E;
-        eb = Eb / std::max({o.mult_base, o.mult_low, o.mult_high});
-    }
-    std::vector<double> ebk(K + 1);
-    for (int k = 1; k <= K; ++k) ebk[k] = (k == K ? o.mult_high : k == K - 1 ? o.mult_low : o.mult_base) * eb;
 
     // buffers
     STZ_CUDA(ctx->grid[0].ensure(g.n_fine_max * elem));

@@ -186,6 +186,23 @@ inline bool stream_learned(const ParsedStream& ps)
     return false;
 }
 
+// Shape of the hierarchy for given dims and options.
+struct Geometry {
+    int nx = 0, ny = 0, nz = 0, K = 0, radius = 0, chunk_high = 0, chunk_low = 0;
+    int c0[3] = {0, 0, 0};
+    std::vector<LevelGeom> lv;  // 1..K
+    std::vector<StreamDesc> sd; // stream (k-1)*7+b
+    uint64_t total_codes = 0, total_chunk_slots = 0, total_sub = 0, total_words = 0;
+    size_t n_fine_max = 0;      // largest intermediate decoded grid (elements)
+};
+Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_low, int radius);
+
+// Absolute eb the level multipliers apply to (value range on the GPU for a
+// relative bound, pointwise slack) and the per-level bounds ebk[1..K].
+template <typename T>
+stz_status level_error_bounds(stz_context* ctx, const T* field, size_t N, const stz_opts& o, int K, double& eb,
+                              std::vector<double>& ebk);
+
 // CTA work items for chunk lists: groups of up to kCoderThreads / C chunks.
 void add_work(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint32_t stream, const uint32_t* chunks,
               size_t n, int C);
@@ -308,6 +325,8 @@ struct KScope {
 };
 
 int pool_threads(int requested);
+// Validates compressor options (STZ_ERR_ARG with a message).
+stz_status check_opts(const stz_opts* o);
 size_t dtype_size(int dtype);
 // Make ctx current on this thread and clear the thread's last error.
 stz_status enter(stz_context* ctx);

@@ -115,12 +115,34 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_server_release.argtypes = [vp, C.c_uint64]
     lib.stz_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
     lib.stz_server_batch_log.argtypes = [vp, C.POINTER(BatchRecord), sz, C.POINTER(sz)]
+    lib.stz_default_train_opts.argtypes = [C.POINTER(TrainOpts)]
+    lib.stz_default_train_opts.restype = None
+    lib.stz_trainer_create.argtypes = [vp, C.POINTER(Opts), C.POINTER(TrainOpts), C.POINTER(vp)]
+    lib.stz_trainer_add_field_dev.argtypes = [vp, vp, C.c_int, sz, sz, sz]
+    lib.stz_trainer_fit.argtypes = [vp, C.POINTER(vp)]
+    lib.stz_trainer_stats.argtypes = [vp, C.POINTER(TrainStats)]
+    lib.stz_trainer_free.argtypes = [vp]
+    lib.stz_trainer_free.restype = None
+    lib.stz_debug_mlp_grad.argtypes = [vp, vp, vp, vp, sz, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       C.POINTER(C.c_double), vp, C.POINTER(C.c_double)]
     lib.stz_model_parse.argtypes = [vp, sz, C.POINTER(vp)]
     lib.stz_model_bytes.argtypes = [vp, C.POINTER(vp), C.POINTER(sz)]
     lib.stz_model_free.argtypes = [vp]
     lib.stz_model_free.restype = None
     _lib = lib
     return lib
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("qat_epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double),
+                ("huber_delta", C.c_double), ("sample_step", C.c_int), ("max_pairs", C.c_size_t),
+                ("seed", C.c_uint64)]
+
+
+class TrainStats(C.Structure):
+    _fields_ = [("pairs", C.c_size_t * 2), ("loss_zero", C.c_double * 2), ("loss_float", C.c_double * 2),
+                ("loss_qat", C.c_double * 2), ("loss_int8", C.c_double * 2), ("s_in", C.c_double * 2),
+                ("s_t", C.c_double * 2), ("train_ms", C.c_double)]
 
 
 class BatchRecord(C.Structure):
@@ -624,3 +646,81 @@ def codebook(hist: np.ndarray):
     _check(lib.stz_debug_codebook(h.ctypes.data_as(C.c_void_p), len(h), sym.ctypes.data_as(C.c_void_p),
                                   ln.ctypes.data_as(C.c_void_p), C.byref(n)))
     return sym[: n.value].copy(), ln[: n.value].copy()
+
+
+class Trainer:
+    """GPU training of the learned correction on pairs the compressor makes
+    from the given fields (stz_trainer_*)."""
+
+    def __init__(self, ctx: "Context", opts: Opts | None = None, train: TrainOpts | None = None, **kw):
+        self.lib = load_library()
+        self.ctx = ctx
+        self.opts = opts if opts is not None else default_opts(**kw)
+        self.train = train if train is not None else default_train_opts()
+        self._h = C.c_void_p()
+        _check(self.lib.stz_trainer_create(ctx._c, C.byref(self.opts), C.byref(self.train), C.byref(self._h)))
+
+    def add_field(self, field) -> None:
+        """field: a contiguous 3-D CUDA tensor (z, y, x), float32 or float64."""
+        import torch
+
+        if not (_is_torch(field) and field.is_cuda and field.dim() == 3 and field.is_contiguous()):
+            raise ValueError("field must be a contiguous 3-D CUDA tensor (z, y, x)")
+        code = {torch.float32: STZ_F32, torch.float64: STZ_F64}[field.dtype]
+        nz, ny, nx = field.shape
+        _torch_sync(field)
+        _check(self.lib.stz_trainer_add_field_dev(self._h, C.c_void_p(field.data_ptr()), code, nx, ny, nz))
+
+    def fit(self) -> Model:
+        h = C.c_void_p()
+        _check(self.lib.stz_trainer_fit(self._h, C.byref(h)))
+        return Model(h.value)
+
+    def stats(self) -> dict:
+        st = TrainStats()
+        _check(self.lib.stz_trainer_stats(self._h, C.byref(st)))
+        out = {}
+        for f, _ in TrainStats._fields_:
+            v = getattr(st, f)
+            out[f] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            self.lib.stz_trainer_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.stz_trainer_free(self._h)
+            self._h = C.c_void_p()
+
+
+def default_train_opts(**kw) -> TrainOpts:
+    lib = load_library()
+    t = TrainOpts()
+    lib.stz_default_train_opts(C.byref(t))
+    for k, v in kw.items():
+        if not hasattr(t, k):
+            raise TypeError(f"unknown training option {k}")
+        setattr(t, k, v)
+    return t
+
+
+def mlp_grad(ctx: "Context", params, x, t, s_in: float, s_t: float, huber_delta: float = 2.0, qat: bool = False,
+             sa=(1.0, 1.0)):
+    """One forward + backward of the training kernels (stz_debug_mlp_grad):
+    returns (mean loss, 1864 gradients)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    tt = np.ascontiguousarray(t, dtype=np.float32)
+    n = xx.shape[0]
+    if p.shape != (1864,) or xx.shape != (n, 16) or tt.shape != (n, 8):
+        raise ValueError("params (1864,), x (n, 16), t (n, 8)")
+    g = np.zeros(1864, np.float32)
+    loss = C.c_double()
+    sav = (C.c_double * 2)(*sa)
+    _check(ctx.lib.stz_debug_mlp_grad(ctx._c, p.ctypes.data_as(C.c_void_p), xx.ctypes.data_as(C.c_void_p),
+                                      tt.ctypes.data_as(C.c_void_p), n, s_in, s_t, huber_delta, int(qat), sav,
+                                      g.ctypes.data_as(C.c_void_p), C.byref(loss)))
+    return loss.value, g

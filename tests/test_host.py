@@ -47,7 +47,9 @@ def test_struct_offsets_match_the_c_compiler(tmp_path):
     if shutil.which("gcc") is None:
         pytest.skip("gcc not available")
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "stz/stz.h"', "int main(void) {"]
-    for struct, cls in (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info)):
+    structs = (("stz_opts", stz_b200.Opts), ("stz_info", stz_b200.Info), ("stz_train_opts", stz_b200.TrainOpts),
+               ("stz_train_stats", stz_b200.TrainStats))
+    for struct, cls in structs:
         lines.append('printf("%%zu\\n", sizeof(%s));' % struct)
         for f, _ in cls._fields_:
             lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (struct, f))
@@ -58,7 +60,7 @@ def test_struct_offsets_match_the_c_compiler(tmp_path):
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = []
-    for cls in (stz_b200.Opts, stz_b200.Info):
+    for _, cls in structs:
         want.append(ctypes.sizeof(cls))
         want += [getattr(cls, f).offset for f, _ in cls._fields_]
     assert got == want
