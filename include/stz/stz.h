@@ -248,6 +248,13 @@ void stz_trainer_free(stz_trainer* t);
  * (rounded to BF16 as stored), t n x 8 targets in eb; s_in, s_t the scales,
  * qat 0/1 with activation scales sa[2]. Writes the mean loss (normalised
  * units) and the 1864 gradients. */
+/* The exported int8 network on n rows of int8 inputs (16 per row, the last
+ * two zero), host buffers: out (n x 8 int32) receives the output
+ * accumulators of the 7 blocks (and a zero). tensor_cores = 1 runs the
+ * tcgen05 kind::i8 kernel, 0 the dp4a form of the level kernels. */
+stz_status stz_debug_learned_infer(stz_context* ctx, const int8_t* xq, size_t n, const void* model_record,
+                                   int tensor_cores, int32_t* out);
+
 stz_status stz_debug_mlp_grad(stz_context* ctx, const float* params, const float* x, const float* t, size_t n,
                               double s_in, double s_t, double huber_delta, int qat, const double sa[2], float* grad,
                               double* loss);

@@ -26,7 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall", "-I", C
 # Every FP operation of the predictor/quantizer is explicit PTX; these flags
 # make the remaining compiler-generated arithmetic follow the same rules.
 CUDA_FLAGS = ARCH + ["-fmad=false", "-ftz=true", "-prec-div=true", "-prec-sqrt=true", "-Xptxas", "-v"]
-SOURCES = ["levels.cu", "huffman.cu", "roi.cu", "api.cu", "server.cu", "noalloc.cu", "train.cu", "host.cpp"]
+SOURCES = ["levels.cu", "huffman.cu", "roi.cu", "api.cu", "server.cu", "noalloc.cu", "train.cu", "learned.cu", "host.cpp"]
 
 
 def _digest() -> str:

@@ -416,24 +416,11 @@ __device__ __forceinline__ uint32_t learned_requant(int acc, int m, int sh)
     return p < 0 ? 0u : (p > 127 ? 127u : (uint32_t)p);
 }
 
-// The 7 corrections at a coarse point (accessor r positioned on it; the
-// stencil reaches -1..+2 on each axis). M is usually in shared memory.
-template <typename T, class Acc>
-__device__ __forceinline__ void learned_corr(const LearnedModel& M, const Acc& r, T rs, T so, T (&corr)[7])
+// The integer network on packed int8 inputs (16 bytes, the last two zero):
+// the output accumulators of the 7 blocks.
+__device__ __forceinline__ void learned_mlp_int(const LearnedModel& M, const uint4& x, int (&acc3)[7])
 {
-    using A = Ar<T>;
-    constexpr int st[14][3] = STZ_LEARNED_STENCIL;
-    T v[14];
-#pragma unroll
-    for (int i = 0; i < 14; ++i) v[i] = r(st[i][2] * (long long)r.sy + st[i][1] * (long long)r.sx + st[i][0]);
-    T m = v[0];
-#pragma unroll
-    for (int i = 1; i < 8; ++i) m = A::add(m, v[i]);
-    m = A::mul(m, T(0.125));
-    uint32_t xw[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-    for (int i = 0; i < 14; ++i)
-        xw[i >> 2] |= ((uint32_t)learned_to_i8(A::mul(A::sub(v[i], m), rs)) & 0xffu) << (8 * (i & 3));
+    const uint32_t xw[4] = {x.x, x.y, x.z, x.w};
     const int* w1 = reinterpret_cast<const int*>(&M.w1[0][0]);
     const int* w2 = reinterpret_cast<const int*>(&M.w2[0][0]);
     const int* w3 = reinterpret_cast<const int*>(&M.w3[0][0]);
@@ -458,8 +445,40 @@ __device__ __forceinline__ void learned_corr(const LearnedModel& M, const Acc& r
         int acc = M.b3[o];
 #pragma unroll
         for (int w = 0; w < 8; ++w) acc = __dp4a(w3[o * 8 + w], (int)a2[w], acc);
-        corr[o] = A::mul((T)acc, so);
+        acc3[o] = acc;
     }
+}
+
+// The network's int8 inputs at a coarse point (accessor r positioned on it;
+// the stencil reaches -1..+2 on each axis): stencil values minus the mean of
+// the 8 cell corners, times rs, rounded and clamped, packed 4 per word.
+template <typename T, class Acc>
+__device__ __forceinline__ uint4 learned_inputs(const Acc& r, T rs)
+{
+    using A = Ar<T>;
+    constexpr int st[14][3] = STZ_LEARNED_STENCIL;
+    T v[14];
+#pragma unroll
+    for (int i = 0; i < 14; ++i) v[i] = r(st[i][2] * (long long)r.sy + st[i][1] * (long long)r.sx + st[i][0]);
+    T m = v[0];
+#pragma unroll
+    for (int i = 1; i < 8; ++i) m = A::add(m, v[i]);
+    m = A::mul(m, T(0.125));
+    uint32_t xw[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int i = 0; i < 14; ++i)
+        xw[i >> 2] |= ((uint32_t)learned_to_i8(A::mul(A::sub(v[i], m), rs)) & 0xffu) << (8 * (i & 3));
+    return make_uint4(xw[0], xw[1], xw[2], xw[3]);
+}
+
+// The 7 corrections at a coarse point. M is usually in shared memory.
+template <typename T, class Acc>
+__device__ __forceinline__ void learned_corr(const LearnedModel& M, const Acc& r, T rs, T so, T (&corr)[7])
+{
+    int acc3[7];
+    learned_mlp_int(M, learned_inputs<T>(r, rs), acc3);
+#pragma unroll
+    for (int o = 0; o < 7; ++o) corr[o] = Ar<T>::mul((T)acc3[o], so);
 }
 
 // Copy a model into shared memory (all threads of the block; caller syncs).

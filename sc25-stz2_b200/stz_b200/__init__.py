@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_trainer_free.restype = None
     lib.stz_debug_mlp_grad.argtypes = [vp, vp, vp, vp, sz, C.c_double, C.c_double, C.c_double, C.c_int,
                                        C.POINTER(C.c_double), vp, C.POINTER(C.c_double)]
+    lib.stz_debug_learned_infer.argtypes = [vp, vp, sz, vp, C.c_int, vp]
     lib.stz_model_parse.argtypes = [vp, sz, C.POINTER(vp)]
     lib.stz_model_bytes.argtypes = [vp, C.POINTER(vp), C.POINTER(sz)]
     lib.stz_model_free.argtypes = [vp]
@@ -724,3 +725,16 @@ def mlp_grad(ctx: "Context", params, x, t, s_in: float, s_t: float, huber_delta:
                                       tt.ctypes.data_as(C.c_void_p), n, s_in, s_t, huber_delta, int(qat), sav,
                                       g.ctypes.data_as(C.c_void_p), C.byref(loss)))
     return loss.value, g
+
+
+def learned_infer(ctx: "Context", xq, record: bytes, tensor_cores: bool = True) -> np.ndarray:
+    """The int8 network's output accumulators (n x 8 int32) for int8 input
+    rows xq (n x 16), through stz_debug_learned_infer."""
+    x = np.ascontiguousarray(xq, dtype=np.int8)
+    if x.ndim != 2 or x.shape[1] != 16 or len(record) != 2112:
+        raise ValueError("xq (n, 16) int8 and a 2112-byte model record")
+    out = np.zeros((x.shape[0], 8), np.int32)
+    rec = C.create_string_buffer(bytes(record), len(record))
+    _check(ctx.lib.stz_debug_learned_infer(ctx._c, x.ctypes.data_as(C.c_void_p), x.shape[0], rec,
+                                           int(tensor_cores), out.ctypes.data_as(C.c_void_p)))
+    return out

@@ -161,3 +161,35 @@ def test_served_requests_equal_single_decodes(ctx):
             srv.release(t)
     finally:
         srv.close()
+
+
+def _int_net(rec, x):
+    """The int8 network in numpy (int64): output accumulators of the 7 blocks."""
+    w1 = np.array(rec.w1, np.int64)
+    w2 = np.array(rec.w2, np.int64)
+    w3 = np.array(rec.w3, np.int64)[:7]
+
+    def rq(acc, m, sh):
+        return np.clip((acc * m + (1 << (sh - 1))) >> sh, 0, 127)
+
+    a1 = rq(x.astype(np.int64) @ w1.T + np.array(rec.b1, np.int64), rec.m1, rec.sh1)
+    a2 = rq(a1 @ w2.T + np.array(rec.b2, np.int64), rec.m2, rec.sh2)
+    return a2 @ w3.T + np.array(rec.b3, np.int64)[:7]
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 5000, 128 * 1200 + 77])
+def test_tensor_core_inference_matches_dp4a_and_numpy(ctx, n):
+    """tcgen05 kind::i8 (three MMAs per 128-row tile, TMEM accumulators) and
+    the per-thread dp4a network give identical integer outputs."""
+    rng = np.random.default_rng(n)
+    rec = random_model(rng, sh=(int(rng.integers(6, 12)), int(rng.integers(6, 12))))
+    x = rng.integers(-127, 128, (n, 16)).astype(np.int8)
+    x[:, 14:] = 0
+    record = po.model_record(rec)
+    tc = stz_b200.learned_infer(ctx, x, record, tensor_cores=True)
+    dp = stz_b200.learned_infer(ctx, x, record, tensor_cores=False)
+    assert np.array_equal(tc, dp)
+    assert not tc[:, 7].any()
+    assert np.array_equal(tc[:, :7].astype(np.int64), _int_net(rec, x))
+    # the hidden layers are not saturated throughout: the test sees real activations
+    assert len(np.unique(tc[:, 0])) > min(n, 50) // 2
