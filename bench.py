@@ -60,6 +60,14 @@ def parse_args():
                    help="write per-request (arrival s, queue ms, latency ms, batch, batch size) arrays to this .npz")
     p.add_argument("--serve-size", type=int, default=1024, help="edge of the resident serving field")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="length of each serving load run")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned-predictor measurement")
+    p.add_argument("--learned-only", action="store_true", help="only the learned-predictor measurement")
+    p.add_argument("--learn-train-seeds", type=int, default=6, help="training fields (cycling the 3 generators)")
+    p.add_argument("--learn-size", type=int, default=256, help="edge of the training fields")
+    p.add_argument("--learn-eval-seeds", type=int, default=3, help="held-out evaluation fields")
+    p.add_argument("--learn-eval-size", type=int, default=512, help="edge of the evaluation fields")
+    p.add_argument("--learn-full", action="store_true",
+                   help="the full protocol: 64 training seeds of 256^3, 8 held-out 512^3 seeds")
     return p.parse_args()
 
 
@@ -387,6 +395,122 @@ def serving_bench(args, ctx, local):
     return res
 
 
+def learned_bench(args, ctx, local, field):
+    """Learned correction: train on seeded 256^3 f32 fields cycling the three
+    generators (GRF k^-11/3, lognormal, GRF k^-5/3 + fronts) at rel eb 1e-3
+    with the library's GPU trainer; on held-out 512^3 seeds at rel eb 1e-3 and
+    1e-4 compare stream size (CR) and PSNR with and without the model (the
+    per-block flags choose); time compress + decompress of the benchmark field
+    with the learned kernels forced on every block of both levels."""
+    import torch
+
+    import stz_b200
+    from stz_b200 import fields
+
+    dev = f"cuda:{local}"
+    gens = ("grf", "logn", "fronts")
+
+    def gen_field(g, e, seed):
+        shape = (e, e, e)
+        if g == "grf":
+            return fields.grf(shape, 11.0 / 3.0, seed, np.float32, device=dev)
+        if g == "logn":
+            return fields.lognormal(shape, seed, np.float32, device=dev)
+        return fields.fronts(shape, seed, np.float32, device=dev)
+
+    ntrain = 64 if args.learn_full else args.learn_train_seeds
+    neval = 8 if args.learn_full else args.learn_eval_seeds
+    topts = stz_b200.default_train_opts()
+    tr = stz_b200.Trainer(ctx, train=topts, eb=1e-3, eb_mode="rel", zstd_level=args.zstd)
+    t0 = time.perf_counter()
+    for i in range(ntrain):
+        f = gen_field(gens[i % 3], args.learn_size, 5000 + i)
+        tr.add_field(f)
+        del f
+    torch.cuda.synchronize()
+    pairs_s = time.perf_counter() - t0
+    model = tr.fit()
+    st = tr.stats()
+    tr.close()
+    rows = []
+    for j in range(neval):
+        g = gens[j % 3]
+        f = gen_field(g, args.learn_eval_size, 9000 + j)
+        vr = float(f.max()) - float(f.min())
+        out = torch.empty_like(f)
+        for rel in (1e-3, 1e-4):
+            row = {"generator": g, "seed": 9000 + j, "rel_eb": rel}
+            for name, kw in (("plain", {}), ("learned", {"model": model})):
+                s = ctx.compress(f, eb=rel, eb_mode="rel", zstd_level=args.zstd, **kw)
+                ctx.decompress(s, out=out)
+                mse = float(((out.double() - f.double()) ** 2).mean())
+                row[name] = {"bytes": len(s), "cr": f.numel() * 4 / len(s),
+                             "psnr_db": 20 * np.log10(vr) - 10 * np.log10(max(mse, 1e-300)),
+                             "max_err_over_bound": float((out.double() - f.double()).abs().max()) / (rel * vr)}
+                if name == "learned":
+                    row["learned_flags"] = s.info().learned_flags
+            row["cr_gain"] = row["learned"]["cr"] / row["plain"]["cr"]
+            rows.append(row)
+        del f, out
+    torch.cuda.empty_cache()
+    # throughput with every block of both levels corrected
+    out = torch.empty_like(field)
+    stream = torch.cuda.ExternalStream(ctx.cuda_stream(), device=dev)
+    thr = {}
+    all_blocks = {"model": model, "learned_flags": 0x7F7F}
+    ref_bytes = None
+    for name, kw, path in (("plain", {}, "tc"), ("learned_all_blocks", all_blocks, "tc"),
+                           ("learned_all_blocks_dp4a", all_blocks, "dp4a")):
+        os.environ["STZ_LEARNED_PATH"] = path
+        o = stz_b200.default_opts(eb=args.rel, eb_mode="rel", zstd_level=args.zstd, **kw)
+        for _ in range(2):
+            s = ctx.compress(field, opts=o)
+            ctx.decompress(s, out=out)
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        steps = max(2, args.steps)
+        cms = dms = 0.0
+        ctx.profile(True)
+        ctx.profile_reset()
+        for _ in range(steps):
+            e[0].record(stream)
+            s = ctx.compress(field, opts=o)
+            e[1].record(stream)
+            ctx.decompress(s, out=out)
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            cms += e[0].elapsed_time(e[1])
+            dms += e[1].elapsed_time(e[2])
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        nb = field.numel() * 4
+        thr[name] = {"compress_gbs": nb * steps / cms / 1e6, "decompress_gbs": nb * steps / dms / 1e6,
+                     "cr": nb / len(s), "level_kernel_ms": {k: round(v[0] / steps, 4) for k, v in prof.items()
+                                                            if k.startswith("k_level")}}
+        if kw:  # both learned paths write the same stream
+            b = s.to_bytes()
+            thr[name]["same_stream_as_other_path"] = None if ref_bytes is None else b == ref_bytes
+            ref_bytes = b
+    os.environ.pop("STZ_LEARNED_PATH", None)
+    del out
+    gains = {}
+    for rel in (1e-3, 1e-4):
+        v = [r["cr_gain"] for r in rows if r["rel_eb"] == rel]
+        gains[str(rel)] = float(np.exp(np.mean(np.log(v)))) if v else None
+    return {"train": {"fields": ntrain, "edge": args.learn_size, "rel_eb": 1e-3, "pairs": st["pairs"],
+                      "pair_extraction_s": pairs_s, "fit_ms": st["train_ms"],
+                      "loss_zero": st["loss_zero"], "loss_float": st["loss_float"], "loss_qat": st["loss_qat"],
+                      "loss_int8": st["loss_int8"],
+                      "opts": {"epochs": topts.epochs, "qat_epochs": topts.qat_epochs, "batch": topts.batch,
+                               "lr": topts.lr, "huber_delta": topts.huber_delta, "sample_step": topts.sample_step}},
+            "eval": rows, "cr_gain_geomean": gains, "throughput": thr,
+            "throughput_ratio_learned_vs_plain": {
+                "compress": thr["learned_all_blocks"]["compress_gbs"] / thr["plain"]["compress_gbs"],
+                "decompress": thr["learned_all_blocks"]["decompress_gbs"] / thr["plain"]["decompress_gbs"],
+                "compress_dp4a": thr["learned_all_blocks_dp4a"]["compress_gbs"] / thr["plain"]["compress_gbs"],
+                "decompress_dp4a": thr["learned_all_blocks_dp4a"]["decompress_gbs"] / thr["plain"]["decompress_gbs"]}}
+
+
 # ---- our arm ---------------------------------------------------------------------------
 def algorithmic_bytes(kernel: str, N: int, elem: int, K: int, raw_payload: int) -> float | None:
     """Minimum HBM bytes one launch of `kernel` must move on the N-point field."""
@@ -428,6 +552,12 @@ def main():
     if args.serve_only:
         if rank == 0:
             print(json.dumps({"serving": serving_bench(args, ctx, local)}))
+        ctx.close()
+        replicas.finalize()
+        return
+    if args.learned_only:
+        if rank == 0:
+            print(json.dumps({"learned": learned_bench(args, ctx, local, field)}))
         ctx.close()
         replicas.finalize()
         return
@@ -540,6 +670,9 @@ def main():
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = serving_bench(args, ctx, local)
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_bench(args, ctx, local, field)
 
     if rank == 0:
         res = {
@@ -554,7 +687,7 @@ def main():
             "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
             "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-            "serving": serving,
+            "serving": serving, "learned": learned,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         }
         print(json.dumps(res))

@@ -281,6 +281,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
         a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
         a.qp = make_quant_params(ebk[k], o.radius);
+        a.learned.tensor_cores = learned_tensor_cores();
         if (const int mi = level_model(k); mi >= 0) {
             const LearnedModel& lm = M->lv[mi];
             a.learned.model = ctx->models.as<LearnedModel>() + mi;
@@ -302,7 +303,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
                 lflags[k] = choose_learned_flags(ctx->h_hist.as<uint32_t>(), elem);
             }
             a.learned.flags = lflags[k];
-            if (!lflags[k]) a.learned = LearnedArgs<T>();
+            if (!lflags[k]) a.learned.model = nullptr, a.learned.flags = 0;
         }
         {
             KScope ks(ctx, k == K ? "k_level_encode[finest]" : "k_level_encode[coarser]");
@@ -325,6 +326,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    if (M && M->mask && learned_tc_error_take(st))
+        STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
     lap.mark("levels + histograms");
 
     // codebooks
@@ -810,6 +813,8 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     if (s->resident && s->resident->kmax >= kdec) {
         STZ_TRY(decode_levels<T>(ctx, s, *s->resident, kdec, out_dev));
         STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the output is complete on return
+        if (stream_learned(s->dir) && learned_tc_error_take(ctx->st))
+            STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
         return STZ_OK;
     }
     Prepared p;
@@ -821,6 +826,8 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     Trace t("decompress: decode");
     STZ_TRY(decode_levels<T>(ctx, s, p, kdec, out_dev));
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    if (stream_learned(s->dir) && learned_tc_error_take(ctx->st))
+        STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
     return STZ_OK;
 }
 

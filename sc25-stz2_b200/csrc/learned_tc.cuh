@@ -16,6 +16,9 @@
 
 #include <cuda_runtime.h>
 
+#include "stz_device.cuh"
+#include "stz_internal.h"
+
 namespace stz {
 namespace tc {
 
@@ -125,6 +128,105 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8])
                  : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---- the int8 network for a block of NT x 128 threads ------------------------------
+// Thread t owns row t & 127 of tile t >> 7. Layers 1 and 2 are M = 128,
+// N = 32, K = 32 MMAs (inputs padded from 14 to 32), layer 3 N = 16 (7
+// outputs); tile t's accumulators use TMEM columns 32t .. 32t + 31.
+constexpr uint32_t kIdescN32 = idesc_i8_m128(32);
+constexpr uint32_t kIdescN16 = idesc_i8_m128(16);
+
+template <int NT>
+struct Net {
+    uint8_t A[NT][4096];  // this layer's inputs, K-major
+    uint8_t B1[1024], B2[1024], B3[512];
+    uint64_t mbar;
+    uint32_t tbase;
+};
+
+// Whole block (NT x 128 threads), after M is readable: weights into the B
+// operands, the mbarrier, TMEM columns. Ends with a block barrier.
+template <int NT>
+__device__ __forceinline__ void net_setup(Net<NT>& s, const LearnedModel& M, int tid)
+{
+    for (int i = tid; i < 32 * 32; i += NT * 128) {
+        const int r = i >> 5, k = i & 31;
+        s.B1[kmajor_off(r, k)] = (uint8_t)(k < 16 ? M.w1[r][k] : 0);
+        s.B2[kmajor_off(r, k)] = (uint8_t)M.w2[r][k];
+        if (r < 16) s.B3[kmajor_off(r, k)] = (uint8_t)(r < 8 ? M.w3[r][k] : 0);
+    }
+    if (tid == 0) {
+        mbar_init(smem_addr(&s.mbar), 1);
+        fence_mbar_init();
+    }
+    if (tid < 32) tmem_alloc(smem_addr(&s.tbase), 32 * NT);
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+}
+
+// Whole block: the network on this thread's packed inputs x. acc3 gets the
+// 7 output accumulators. false (on every thread) when an MMA did not
+// complete in time; the block must then stop issuing and tear down.
+template <int NT>
+__device__ __forceinline__ bool net_run(Net<NT>& s, const LearnedModel& M, const uint4& x, uint32_t& phase, int tid,
+                                        int (&acc3)[7])
+{
+    const int tile = tid >> 7, row = tid & 127;
+    uint8_t* A = s.A[tile];
+    const uint32_t taddr = s.tbase + ((uint32_t)(((tid >> 5) & 3) * 32) << 16) + (uint32_t)(32 * tile);
+    const uint32_t mb = smem_addr(&s.mbar);
+    *reinterpret_cast<uint4*>(A + kmajor_off(row, 0)) = x;
+    *reinterpret_cast<uint4*>(A + kmajor_off(row, 16)) = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll 1
+    for (int layer = 0; layer < 3; ++layer) {
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        if (tid == 0) {
+            const uint64_t bd = kmajor_desc(smem_addr(layer == 0 ? s.B1 : layer == 1 ? s.B2 : s.B3));
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+                mma_i8(s.tbase + 32u * t, kmajor_desc(smem_addr(s.A[t])), bd, layer < 2 ? kIdescN32 : kIdescN16, 0u);
+            mma_commit(mb);
+        }
+        const bool ok = mbar_wait(mb, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) return false;
+        fence_after_sync();
+        if (layer < 2) {
+            uint32_t acc[32];
+            tmem_ld32(taddr, acc);
+            tmem_wait_ld();
+            const int32_t* b = layer == 0 ? M.b1 : M.b2;
+            const int m = layer == 0 ? M.m1 : M.m2, sh = layer == 0 ? M.sh1 : M.sh2;
+            uint32_t w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int j = 0; j < 32; ++j) w[j >> 2] |= learned_requant((int)acc[j] + b[j], m, sh) << (8 * (j & 3));
+            *reinterpret_cast<uint4*>(A + kmajor_off(row, 0)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(A + kmajor_off(row, 16)) = make_uint4(w[4], w[5], w[6], w[7]);
+        } else {
+            uint32_t acc[8];
+            tmem_ld8(taddr, acc);
+            tmem_wait_ld();
+#pragma unroll
+            for (int o = 0; o < 7; ++o) acc3[o] = (int)acc[o] + M.b3[o];
+        }
+    }
+    return true;
+}
+
+// Whole block: release the TMEM columns (after the last net_run).
+template <int NT>
+__device__ __forceinline__ void net_teardown(Net<NT>& s, int tid)
+{
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (tid < 32) tmem_dealloc(s.tbase, 32 * NT);
+}
 
 }  // namespace tc
 }  // namespace stz

@@ -67,24 +67,49 @@ struct EncodeIO {
     T* __restrict__ G;  // decoded fine grid (coarser levels only)
 };
 
-// Learned correction of the blocks la.flags selects (interior points only;
-// la.model in shared memory).
-template <typename T, class Acc>
-__device__ __forceinline__ void apply_learned(const Acc& r, const LearnedArgs<T>& la, T (&p)[7])
+// Learned correction modes of the level kernels: none, the network per
+// thread with dp4a, or block-wide on the tensor cores (the same integers).
+constexpr int kLearnNone = 0, kLearnDp4a = 1, kLearnTc = 2;
+
+// p[b] += acc3[b] * so for the blocks la.flags selects.
+template <typename T>
+__device__ __forceinline__ void apply_corr(const LearnedArgs<T>& la, const int* acc3, T (&p)[7])
 {
-    T corr[7];
-    learned_corr<T>(*la.model, r, la.rs, la.so, corr);
 #pragma unroll
     for (int b = 0; b < 7; ++b)
-        if ((la.flags >> b) & 1u) p[b] = Ar<T>::add(p[b], corr[b]);
+        if ((la.flags >> b) & 1u) p[b] = Ar<T>::add(p[b], Ar<T>::mul((T)acc3[b], la.so));
+}
+
+// Learned correction of the blocks la.flags selects (interior points only;
+// la.model in shared memory): LM == kLearnDp4a evaluates the network here,
+// kLearnTc takes the accumulators the block computed (acc3).
+template <int LM, typename T, class Acc>
+__device__ __forceinline__ void apply_learned(const Acc& r, const LearnedArgs<T>& la, const int* acc3, T (&p)[7])
+{
+    if constexpr (LM == kLearnDp4a) {
+        int a[7];
+        learned_mlp_int(*la.model, learned_inputs<T>(r, la.rs), a);
+        apply_corr(la, a, p);
+    } else if constexpr (LM == kLearnTc) {
+        apply_corr(la, acc3, p);
+    }
+}
+
+// Shared-memory state of the block-wide network (instantiated only by the
+// kLearnTc kernels, which are the only callers).
+__device__ __forceinline__ tc::Net<2>* net_smem()
+{
+    __shared__ __align__(1024) tc::Net<2> net;
+    return &net;
 }
 
 // One coarse point of the encoder: fine values, 7 predictions, residuals,
 // codes, unpredictable values, decoded fine cell.
-template <typename T, int PRED, bool FINEST, bool INTERIOR, bool LEARNED = false, class Acc>
+template <typename T, int PRED, bool FINEST, bool INTERIOR, int LM = kLearnNone, class Acc>
 __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
                                              const QuantParams& qp, const T* lut, const ChunkIndex& ci, int x, int y,
-                                             int z, int (&q)[7], const LearnedArgs<T>& la = LearnedArgs<T>())
+                                             int z, int (&q)[7], const LearnedArgs<T>& la = LearnedArgs<T>(),
+                                             const int* acc3 = nullptr)
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -109,7 +134,7 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     }
     T p[7];
     predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
-    if constexpr (LEARNED) apply_learned(r, la, p);
+    apply_learned<LM>(r, la, acc3, p);
     int chunk;
     const size_t cm = ci.at(z, chunk);
     const size_t n = geo.n;
@@ -140,7 +165,7 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     }
 }
 
-template <typename T, int PRED, bool FINEST, bool LEARNED>
+template <typename T, int PRED, bool FINEST, int LM>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                          QuantParams qp, HistArgs hist, LearnedArgs<T> la)
 {
@@ -151,7 +176,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     const int tid = threadIdx.y * BX + threadIdx.x;
     for (int i = tid; i < 7 * kSmemBins; i += BX * BY) (&sh[0][0])[i] = 0;
     if constexpr (!FINEST) build_recover_lut(lut, qp, tid, BX * BY);
-    if constexpr (LEARNED) {  // the model follows the tile in dynamic shared memory
+    if constexpr (LM != kLearnNone) {  // the model follows the tile in dynamic shared memory
         LearnedModel* smodel = reinterpret_cast<LearnedModel*>(smem_raw + kTileBytesAligned<T>);
         learned_load(smodel, la.model, tid, BX * BY);
         la.model = smodel;
@@ -168,14 +193,27 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     ci.init(geo, x, y);
     uint32_t center[7] = {0, 0, 0, 0, 0, 0, 0};
     const int z1 = min(z0 + BZ, dz - 2);
+    [[maybe_unused]] uint32_t phase = 0;
+    [[maybe_unused]] bool tc_failed = false;
+    if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
     for (int z = z0; z < z1; ++z) {
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};
-        if (valid) {
-            const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-            encode_point<T, PRED, FINEST, true, LEARNED>(r, io, geo, qp, lut, ci, x, y, z, q, la);
+        const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+        int acc3[7];
+        if constexpr (LM == kLearnTc) {
+            const uint4 xin = valid ? learned_inputs<T>(r, la.rs) : make_uint4(0u, 0u, 0u, 0u);
+            if (!tc::net_run(*net_smem(), *la.model, xin, phase, tid, acc3)) {
+                tc_failed = true;
+                break;
+            }
         }
+        if (valid) encode_point<T, PRED, FINEST, true, LM>(r, io, geo, qp, lut, ci, x, y, z, q, la, acc3);
 #pragma unroll
         for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b], center[b]);
+    }
+    if constexpr (LM == kLearnTc) {
+        tc::net_teardown(*net_smem(), tid);
+        if (tc_failed && tid == 0) atomicOr(&g_learned_tc_error, 1u);
     }
     hist_flush_center(sh, wlo, wn, hist, center);
     __syncthreads();
@@ -214,11 +252,11 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
 }
 
 // One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
-template <typename T, int PRED, bool INTERIOR, bool LEARNED = false, class Acc>
+template <typename T, int PRED, bool INTERIOR, int LM = kLearnNone, class Acc>
 __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp, const T* lut,
                                              const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
                                              T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z,
-                                             const LearnedArgs<T>& la = LearnedArgs<T>())
+                                             const LearnedArgs<T>& la = LearnedArgs<T>(), const int* acc3 = nullptr)
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -230,7 +268,7 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     for (int b = 0; b < 7; ++b) q[b] = __ldg(codes + (size_t)b * n + cm);
     T p[7];
     predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
-    if constexpr (LEARNED) apply_learned(r, la, p);
+    apply_learned<LM>(r, la, acc3, p);
     T v[8];
     v[0] = r(0);
 #pragma unroll
@@ -249,7 +287,7 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     }
 }
 
-template <typename T, int PRED, bool LEARNED>
+template <typename T, int PRED, int LM>
 __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
                                                          const T* __restrict__ unpred_dense, T* __restrict__ G,
@@ -258,10 +296,11 @@ __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ T lut[2 * kRecW];
-    build_recover_lut(lut, qp, threadIdx.y * BX + threadIdx.x, BX * BY);
-    if constexpr (LEARNED) {  // the model follows the tile in dynamic shared memory
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    build_recover_lut(lut, qp, tid, BX * BY);
+    if constexpr (LM != kLearnNone) {  // the model follows the tile in dynamic shared memory
         LearnedModel* smodel = reinterpret_cast<LearnedModel*>(smem_raw + kTileBytesAligned<T>);
-        learned_load(smodel, la.model, threadIdx.y * BX + threadIdx.x, BX * BY);
+        learned_load(smodel, la.model, tid, BX * BY);
         la.model = smodel;
     }
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
@@ -269,13 +308,31 @@ __global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R
     load_tile(tile, R, dx, dy, dz, x0, y0, z0);
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x > dx - 3 || y > dy - 3) return;
+    const bool valid = x <= dx - 3 && y <= dy - 3;
+    if constexpr (LM != kLearnTc) {
+        if (!valid) return;
+    }
     ChunkIndex ci;
     ci.init(geo, x, y);
     const int z1 = min(z0 + BZ, dz - 2);
+    [[maybe_unused]] uint32_t phase = 0;
+    [[maybe_unused]] bool tc_failed = false;
+    if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
     for (int z = z0; z < z1; ++z) {
         const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-        decode_point<T, PRED, true, LEARNED>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z, la);
+        int acc3[7];
+        if constexpr (LM == kLearnTc) {
+            const uint4 xin = valid ? learned_inputs<T>(r, la.rs) : make_uint4(0u, 0u, 0u, 0u);
+            if (!tc::net_run(*net_smem(), *la.model, xin, phase, tid, acc3)) {
+                tc_failed = true;
+                break;
+            }
+        }
+        if (valid) decode_point<T, PRED, true, LM>(r, geo, qp, lut, codes, unpred_dense, G, ci, x, y, z, la, acc3);
+    }
+    if constexpr (LM == kLearnTc) {
+        tc::net_teardown(*net_smem(), tid);
+        if (tc_failed && tid == 0) atomicOr(&g_learned_tc_error, 1u);
     }
 }
 

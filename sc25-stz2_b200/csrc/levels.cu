@@ -27,10 +27,25 @@
 
 #include <cuda_runtime.h>
 
+#include "learned_tc.cuh"
 #include "levels.h"
 #include "stz_device.cuh"
 
 namespace stz {
+
+// Set by a level kernel whose tensor-core network gave up waiting on an MMA.
+__device__ uint32_t g_learned_tc_error;
+
+uint32_t learned_tc_error_take(cudaStream_t st)
+{
+    uint32_t v = 0;
+    const uint32_t zero = 0;
+    if (cudaMemcpyFromSymbolAsync(&v, g_learned_tc_error, 4, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess) return 1;
+    if (v) cudaMemcpyToSymbolAsync(g_learned_tc_error, &zero, 4, 0, cudaMemcpyHostToDevice, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 1;
+    return v;
+}
+
 namespace {
 
 template <typename T>
@@ -398,8 +413,9 @@ Grid<T> make_grid(const T* p, int dx, int dy, int dz)
 }
 
 // Code histograms of the sampled interior points without (hist[0]) and with
-// (hist[1]) the learned correction; thread per sample point.
-template <typename T, int PRED>
+// (hist[1]) the learned correction; thread per sample point, the network per
+// thread (dp4a) or block-wide on the tensor cores (LM).
+template <typename T, int PRED, int LM>
 __global__ void __launch_bounds__(256) k_learned_eval(const T* __restrict__ field, size_t fsx, size_t fsy, int s,
                                                       const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                       LearnedArgs<T> la, int sx, int sy, int sz,
@@ -407,36 +423,57 @@ __global__ void __launch_bounds__(256) k_learned_eval(const T* __restrict__ fiel
 {
     __shared__ __align__(16) LearnedModel model;
     __shared__ uint32_t h[2][7][kEvalBins];
-    for (int i = threadIdx.x; i < 2 * 7 * kEvalBins; i += blockDim.x) (&h[0][0][0])[i] = 0;
-    learned_load(&model, la.model, threadIdx.x, blockDim.x);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 2 * 7 * kEvalBins; i += blockDim.x) (&h[0][0][0])[i] = 0;
+    learned_load(&model, la.model, tid, blockDim.x);
     __syncthreads();
     using A = Ar<T>;
     const uint64_t total = (uint64_t)sx * sy * sz;
     const long long gx = geo.dx, gy = (long long)geo.dx * geo.dy;
     const int lo = qp.radius - kEvalHalf;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const int ix = (int)(i % sx), iy = (int)((i / sx) % sy), iz = (int)(i / ((uint64_t)sx * sy));
+    [[maybe_unused]] uint32_t phase = 0;
+    [[maybe_unused]] bool tc_failed = false;
+    if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), model, tid);
+    // uniform trip count per block (the tensor-core network is block-wide)
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < total; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = base + tid;
+        const bool valid = i < total;
+        const uint64_t ii = valid ? i : 0;
+        const int ix = (int)(ii % sx), iy = (int)((ii / sx) % sy), iz = (int)(ii / ((uint64_t)sx * sy));
         const int x = 1 + 2 * ix, y = 1 + 2 * iy, z = 1 + 2 * iz;
         const GlobalAt<T> r{R + (size_t)z * gy + (size_t)y * gx + x, gx, gy};
-        T p[7], corr[7];
+        int acc3[7];
+        if constexpr (LM == kLearnTc) {
+            const uint4 xin = valid ? learned_inputs<T>(r, la.rs) : make_uint4(0u, 0u, 0u, 0u);
+            if (!tc::net_run(*net_smem(), model, xin, phase, tid, acc3)) {
+                tc_failed = true;
+                break;
+            }
+        } else {
+            learned_mlp_int(model, learned_inputs<T>(r, la.rs), acc3);
+        }
+        if (!valid) continue;
+        T p[7];
         predict7<PRED>(r, true, x, y, z, geo.dx, geo.dy, geo.dz, p);
-        learned_corr<T>(model, r, la.rs, la.so, corr);
 #pragma unroll
         for (int b = 0; b < 7; ++b) {
             const int si = b + 1, px = si & 1, py = (si >> 1) & 1, pz = si >> 2;
             const T o = __ldg(field + (size_t)s * (2 * z + pz) * fsy + (size_t)s * (2 * y + py) * fsx +
                               (size_t)s * (2 * x + px));
             const int c0 = quantize(A::sub(o, p[b]), qp);
-            const int c1 = quantize(A::sub(o, A::add(p[b], corr[b])), qp);
+            const int c1 = quantize(A::sub(o, A::add(p[b], A::mul((T)acc3[b], la.so))), qp);
             const int k0 = c0 == 0 ? kEvalBins - 1 : min(max(c0 - lo, -1), kEvalBins - 1);
             const int k1 = c1 == 0 ? kEvalBins - 1 : min(max(c1 - lo, -1), kEvalBins - 1);
             atomicAdd(&h[0][b][k0 < 0 ? kEvalBins - 1 : k0], 1u);
             atomicAdd(&h[1][b][k1 < 0 ? kEvalBins - 1 : k1], 1u);
         }
     }
+    if constexpr (LM == kLearnTc) {
+        tc::net_teardown(*net_smem(), tid);
+        if (tc_failed && tid == 0) atomicOr(&g_learned_tc_error, 1u);
+    }
     __syncthreads();
-    for (int i = threadIdx.x; i < 2 * 7 * kEvalBins; i += blockDim.x) {
+    for (int i = tid; i < 2 * 7 * kEvalBins; i += blockDim.x) {
         const uint32_t c = (&h[0][0][0])[i];
         if (c) atomicAdd(hist + i, c);
     }
@@ -469,7 +506,9 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
         if (interior) {                                                                                            \
-            auto kern = learned ? k_level_encode<T, P, F, true> : k_level_encode<T, P, F, false>;                  \
+            auto kern = !learned                     ? k_level_encode<T, P, F, kLearnNone>                         \
+                        : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
+                                                 : k_level_encode<T, P, F, kLearnDp4a>;                        \
             allow_smem(kern, sm);                                                                                  \
             kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned);                                       \
         }                                                                                                          \
@@ -501,7 +540,9 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
 #define STZ_DEC(P)                                                                                                 \
     do {                                                                                                           \
         if (interior) {                                                                                            \
-            auto kern = learned ? k_level_decode<T, P, true> : k_level_decode<T, P, false>;                        \
+            auto kern = !learned                     ? k_level_decode<T, P, kLearnNone>                            \
+                        : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \
+                                                 : k_level_decode<T, P, kLearnDp4a>;                           \
             allow_smem(kern, sm);                                                                                  \
             kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned);              \
         }                                                                                                          \
@@ -521,12 +562,10 @@ void launch_learned_eval(const LevelEncodeArgs<T>& a, uint32_t* hist, cudaStream
     const uint64_t total = (uint64_t)sx * sy * sz;
     if (!total || !a.learned.model) return;
     const int gs = (int)std::min<uint64_t>((total + 255) / 256, 148 * 8);
-    if (a.predictor == 1)
-        k_learned_eval<T, 1><<<gs, 256, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, a.coarse, g, a.qp, a.learned, sx,
-                                                  sy, sz, hist);
-    else
-        k_learned_eval<T, 0><<<gs, 256, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, a.coarse, g, a.qp, a.learned, sx,
-                                                  sy, sz, hist);
+    const bool tcm = a.learned.tensor_cores;
+    auto kern = a.predictor == 1 ? (tcm ? k_learned_eval<T, 1, kLearnTc> : k_learned_eval<T, 1, kLearnDp4a>)
+                                 : (tcm ? k_learned_eval<T, 0, kLearnTc> : k_learned_eval<T, 0, kLearnDp4a>);
+    kern<<<gs, 256, 0, st>>>(a.field, a.fsx, a.fsy, a.stride, a.coarse, g, a.qp, a.learned, sx, sy, sz, hist);
 }
 
 template <typename T>

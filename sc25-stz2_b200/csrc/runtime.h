@@ -164,11 +164,21 @@ struct Prepared {
     bool base_valid = false;  // *base holds the decoded base grid (level K-2 output) for box queries
 };
 
+// Where the level kernels evaluate the learned network: block-wide on the
+// tensor cores (default) or per thread with dp4a (STZ_LEARNED_PATH=dp4a);
+// both give the same integers.
+inline bool learned_tensor_cores()
+{
+    const char* e = std::getenv("STZ_LEARNED_PATH");
+    return !(e && std::string(e) == "dp4a");
+}
+
 // Learned-correction arguments of level k (none when the level has no flags).
 template <typename T>
 LearnedArgs<T> learned_args(const ParsedStream& ps, int k, const LearnedModel* d_models)
 {
     LearnedArgs<T> a;
+    a.tensor_cores = learned_tensor_cores();
     const LevelDir& L = ps.lv[k];
     if (!L.lflags || !d_models) return a;
     a.model = d_models + k;

@@ -58,7 +58,14 @@ struct LearnedArgs {
     const LearnedModel* model = nullptr;  // device memory
     uint32_t flags = 0;                    // blocks (bit b) that use it
     T rs = T(0), so = T(0);
+    // Level kernels: evaluate the network block-wide on the tensor cores
+    // (tcgen05 kind::i8) instead of per thread with dp4a (same integers).
+    bool tensor_cores = true;
 };
+
+// Nonzero when a tensor-core MMA of the learned network did not complete in
+// time (a bounded wait gave up); read and cleared by learned_tc_error_take.
+uint32_t learned_tc_error_take(cudaStream_t st);
 
 // Quantizer constants of one level (FD5:1208-1210): eb, 1/eb computed once on
 // the host (recip = 1.0 / eb), radius.

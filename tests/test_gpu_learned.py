@@ -63,9 +63,14 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("path", ["tc", "dp4a"])
 @pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}-{np.dtype(c[2]).name}-p{c[4]}-{c[6][0]:x}-{c[6][1]:x}"
                                              for c in CASES])
-def test_forced_flags_match_oracle(ctx, case):
+def test_forced_flags_match_oracle(ctx, case, path, monkeypatch):
+    """Level kernels with the network on the tensor cores (tc, the default)
+    or per thread (dp4a); the ROI kernels always use dp4a, so the box checks
+    also compare the two forms."""
+    monkeypatch.setenv("STZ_LEARNED_PATH", path)
     gen, shape, dtype, rel, pred, (ch, cl), flags = case
     f = make_field(gen, shape, dtype, 31)
     rng = np.random.default_rng(5)
