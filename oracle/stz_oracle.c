@@ -323,6 +323,83 @@ typedef struct {
     int n_chunks, layers, chunks_per_layer;
 } enc_stream;
 
+/* Run symbols of a stream (this container's own rule, version 3): a maximal
+ * run of the centre code (= radius) inside a plane is coded with run
+ * symbols placed in consecutive code values the stream does not use,
+ * [run_base, run_base + run_n):
+ *   J  = min(14, floor(log2 plane)), D = min(32, 2^J), LD = log2 D;
+ *   slots 0 .. D-2      : runs of exactly 2 .. D centre codes;
+ *   slots D-1 .. run_n-1: runs of 2^k centre codes, k = LD+1 .. J;
+ *   run_n = D - 1 + (J - LD). The window is the highest free one in
+ *   [1, 2 * radius); none (or J = 0): run_n = 0, no runs. */
+static int run_geometry(int plane, int* D, int* LD)
+{
+    int J = 0;
+    while (J < 14 && ((size_t)2 << J) <= (size_t)plane) ++J;
+    *LD = J < 5 ? J : 5;
+    *D = 1 << *LD;
+    return J;
+}
+
+int stzo_run_slots(const uint32_t* hist, int nbins, int plane, uint32_t* run_base)
+{
+    int D, LD;
+    const int J = run_geometry(plane, &D, &LD);
+    *run_base = 0;
+    if (J == 0) return 0;
+    const int S = D - 1 + (J - LD);
+    for (int u0 = nbins - S; u0 >= 1; --u0) {
+        int free_ = 1;
+        for (int j = 0; j < S && free_; ++j) free_ = hist[u0 + j] == 0;
+        if (free_) {
+            *run_base = (uint32_t)u0;
+            return S;
+        }
+    }
+    return 0;
+}
+
+/* The symbols of one plane with runs. A run of r centre codes: while
+ * r > D, the largest 2^k <= r (k <= J) when k > LD, else D; then a direct
+ * symbol for 2 <= r <= D, or the centre code itself for r = 1. Returns the
+ * symbol count; out needs plane entries. */
+static size_t plane_symbols(const uint16_t* s, size_t plane, int radius, uint32_t run_base, int run_n, uint16_t* out)
+{
+    int D = 0, LD = 0;
+    const int J = run_geometry((int)plane, &D, &LD);
+    size_t m = 0, r = 0;
+    for (size_t j = 0; j <= plane; ++j) {
+        if (j < plane && run_n && s[j] == radius) {
+            ++r;
+            continue;
+        }
+        while (r > (size_t)D) {
+            int k = 0;
+            while (k < J && ((size_t)2 << k) <= r) ++k; /* k = min(floor(log2 r), J) */
+            if (k > LD) {
+                out[m++] = (uint16_t)(run_base + (uint32_t)(D - 1 + (k - LD - 1)));
+                r -= (size_t)1 << k;
+            } else {
+                out[m++] = (uint16_t)(run_base + (uint32_t)(D - 2));
+                r -= (size_t)D;
+            }
+        }
+        if (r >= 2) out[m++] = (uint16_t)(run_base + (uint32_t)(r - 2));
+        else if (r == 1) out[m++] = (uint16_t)radius;
+        r = 0;
+        if (j < plane) out[m++] = s[j];
+    }
+    return m;
+}
+
+/* Length of run symbol slot i (0 <= i < run_n) for planes of `plane` codes. */
+static size_t run_length(uint32_t i, int plane)
+{
+    int D, LD;
+    run_geometry(plane, &D, &LD);
+    return i < (uint32_t)(D - 1) ? (size_t)i + 2 : (size_t)1 << (i - (uint32_t)(D - 1) + (uint32_t)LD + 1);
+}
+
 /* Entropy-code one stream given chunk-major codes and chunk-major unpred
  * values (elem = sizeof(T)). */
 static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int dz, int C, int radius,
@@ -330,8 +407,25 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
                           enc_stream* es)
 {
     const int nbins = 2 * radius;
+    const int ncx = dx / C, ncy = dy / C, ncz = dz / C;
+    const int nch = ncx * ncy * ncz;
+    const size_t cvol = (size_t)C * C * C, plane = (size_t)C * C;
     uint32_t* hist = (uint32_t*)calloc((size_t)nbins, 4);
     for (size_t i = 0; i < n; ++i) hist[codes[i]]++;
+    uint32_t run_base = 0;
+    const int run_n = stzo_run_slots(hist, nbins, (int)plane, &run_base);
+    /* the symbol stream: runs inside every plane */
+    uint16_t* syms = (uint16_t*)malloc(2 * (n ? n : 1));
+    size_t* pstart = (size_t*)malloc(sizeof(size_t) * ((size_t)nch * C + 1));
+    size_t m = 0;
+    for (int c = 0; c < nch; ++c)
+        for (int lz = 0; lz < C; ++lz) {
+            pstart[(size_t)c * C + lz] = m;
+            m += plane_symbols(codes + (size_t)c * cvol + (size_t)lz * plane, plane, radius, run_base, run_n, syms + m);
+        }
+    pstart[(size_t)nch * C] = m;
+    memset(hist, 0, 4 * (size_t)nbins);
+    for (size_t i = 0; i < m; ++i) hist[syms[i]]++;
     uint16_t* sym = (uint16_t*)malloc(2 * (size_t)nbins);
     uint8_t* len = (uint8_t*)malloc((size_t)nbins);
     const int nu = stzo_codebook(hist, nbins, sym, len);
@@ -343,18 +437,15 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
         ctab[sym[i]] = code[i];
         ltab[sym[i]] = len[i];
     }
-    const int ncx = dx / C, ncy = dy / C, ncz = dz / C;
-    const int nch = ncx * ncy * ncz;
-    const size_t cvol = (size_t)C * C * C, plane = (size_t)C * C;
     uint32_t* sub_off = (uint32_t*)malloc(4 * (size_t)nch * C);
     uint64_t* choff = (uint64_t*)malloc(8 * ((size_t)nch + 1));
     choff[0] = 0;
     for (int c = 0; c < nch; ++c) {
         uint64_t bits = 0;
         for (int lz = 0; lz < C; ++lz) {
-            sub_off[(size_t)c * C + lz] = (uint32_t)bits;
-            const uint16_t* s = codes + (size_t)c * cvol + (size_t)lz * plane;
-            for (size_t j = 0; j < plane; ++j) bits += ltab[s[j]];
+            const size_t p = (size_t)c * C + lz;
+            sub_off[p] = (uint32_t)bits;
+            for (size_t i = pstart[p]; i < pstart[p + 1]; ++i) bits += ltab[syms[i]];
         }
         choff[c + 1] = choff[c] + (bits + 31) / 32;
     }
@@ -363,21 +454,24 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
     for (int c = 0; c < nch; ++c) {
         uint64_t bit = 0;
         uint32_t* cw = w + choff[c];
-        const uint16_t* s = codes + (size_t)c * cvol;
-        for (size_t j = 0; j < cvol; ++j) {
-            const int l = ltab[s[j]];
-            const uint32_t cd = ctab[s[j]];
+        for (size_t i = pstart[(size_t)c * C]; i < pstart[(size_t)(c + 1) * C]; ++i) {
+            const int l = ltab[syms[i]];
+            const uint32_t cd = ctab[syms[i]];
             for (int t = l - 1; t >= 0; --t) {
                 if ((cd >> t) & 1u) cw[bit >> 5] |= 1u << (31 - (bit & 31));
                 ++bit;
             }
         }
     }
+    free(pstart);
+    free(syms);
     /* raw stream header */
     memset(&es->hdr, 0, sizeof(es->hdr));
     bu32(&es->hdr, (uint32_t)nu);
     for (int i = 0; i < nu; ++i) bu16(&es->hdr, sym[i]);
     for (int i = 0; i < nu; ++i) bu8(&es->hdr, len[i]);
+    bu32(&es->hdr, run_base);
+    bu32(&es->hdr, (uint32_t)run_n);
     bu64(&es->hdr, nunpred);
     bput(&es->hdr, unpred, (size_t)nunpred * elem);
     for (int c = 0; c < nch; ++c) bu32(&es->hdr, unpred_count[c]);
@@ -474,13 +568,12 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
     /* learned correction of levels K-1 and K: container version 2 */
     const stzo_model* lm[64] = {0};
     uint32_t lf[64] = {0};
-    int version = 1;
+    const int version = 3; /* per-level learned fields, run symbols */
     for (int i = 0; i < 2; ++i) {
         const int k = h.K - 1 + i;
         if (k >= 1 && p->model[i] && (p->learned_flags[i] & 0x7fu)) {
             lm[k] = p->model[i];
             lf[k] = p->learned_flags[i] & 0x7fu;
-            version = 2;
         }
     }
     buf_t dir = {0}, data = {0};
@@ -537,10 +630,8 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
         bu32(&dir, (uint32_t)d[2]);
         bu32(&dir, (uint32_t)C);
         bf64(&dir, ebk);
-        if (version == 2) {
-            bu32(&dir, lf[k]);
-            if (lf[k]) bput(&dir, lm[k], sizeof(stzo_model));
-        }
+        bu32(&dir, lf[k]);
+        if (lf[k]) bput(&dir, lm[k], sizeof(stzo_model));
         uint16_t* codes = (uint16_t*)malloc(2 * n);
         uint8_t* ucm = (uint8_t*)malloc(n * h.elem + 1);
         const int nch = (d[0] / C) * (d[1] / C) * (d[2] / C);
@@ -604,7 +695,8 @@ typedef struct {
     int d[64][3];
     int C[64];
     double ebk[64];
-    uint32_t lflags[64];     /* learned-correction blocks of the level (version 2) */
+    int version;             /* 1: plain, 2: learned fields, 3: learned fields and run symbols */
+    uint32_t lflags[64];     /* learned-correction blocks of the level (version >= 2) */
     stzo_model lmodel[64];   /* its model when lflags != 0 */
     sdir_t s[64][7];
 } parsed_t;
@@ -626,7 +718,8 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
     rget(&r, mg, 8);
     if (r.err || memcmp(mg, kMagic, 8) != 0) return -10;
     const uint32_t version = ru32(&r);
-    if (version != 1 && version != 2) return -11;
+    if (version < 1 || version > 3) return -11;
+    ps->version = (int)version;
     hdr_t* h = &ps->h;
     h->dtype = (int)ru32(&r);
     h->predictor = (int)ru32(&r);
@@ -645,7 +738,7 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
         ps->d[k][0] = (int)ru32(&r), ps->d[k][1] = (int)ru32(&r), ps->d[k][2] = (int)ru32(&r);
         ps->C[k] = (int)ru32(&r);
         ps->ebk[k] = rf64(&r);
-        if (version == 2) {
+        if (version >= 2) {
             ps->lflags[k] = ru32(&r);
             if (ps->lflags[k] > 0x7f) return -16;
             if (ps->lflags[k]) rget(&r, &ps->lmodel[k], sizeof(stzo_model));
@@ -715,12 +808,23 @@ static int decode_stream(const uint8_t* st, const parsed_t* ps, int k, int b, ui
         po += s->lr[L];
     }
     const uint32_t* words = (const uint32_t*)praw;
+    int rc_hdr_bad = 0;
     rd_t r = {hraw, (size_t)s->hdr_raw, 0, 0};
     const int nu = (int)ru32(&r);
     uint16_t* sym = (uint16_t*)malloc(2 * (size_t)(nu + 1));
     uint8_t* len = (uint8_t*)malloc((size_t)nu + 1);
     rget(&r, sym, 2 * (size_t)nu);
     rget(&r, len, (size_t)nu);
+    uint32_t run_base = 0, run_n = 0;
+    if (ps->version >= 3) {
+        run_base = ru32(&r);
+        run_n = ru32(&r);
+        int D_, LD_;
+        const int J_ = run_geometry((int)plane, &D_, &LD_);
+        if (run_n && (J_ == 0 || run_n != (uint32_t)(D_ - 1 + (J_ - LD_)) || run_base < 1 ||
+                      run_base + run_n > (uint32_t)(2 * h->radius)))
+            rc_hdr_bad = 1;
+    }
     const uint64_t nunp = ru64(&r);
     rget(&r, unpred, (size_t)nunp * h->elem);
     *nunpred_out = nunp;
@@ -729,7 +833,7 @@ static int decode_stream(const uint8_t* st, const parsed_t* ps, int k, int b, ui
     for (int c = 0; c <= nch; ++c) choff[c] = ru64(&r);
     uint32_t* sub = (uint32_t*)malloc(4 * (size_t)nch * C);
     for (size_t i = 0; i < (size_t)nch * C; ++i) sub[i] = ru32(&r);
-    int rc = r.err ? -23 : 0;
+    int rc = (r.err || rc_hdr_bad) ? -23 : 0;
     /* canonical decode tables: count / first code / first index per length */
     uint32_t* code = (uint32_t*)malloc(4 * (size_t)(nu + 1));
     canonical_codes(len, nu, code);
@@ -744,26 +848,37 @@ static int decode_stream(const uint8_t* st, const parsed_t* ps, int k, int b, ui
         for (int lz = 0; lz < C && !rc; ++lz) {
             uint64_t bit = 32 * choff[c] + sub[(size_t)c * C + lz];
             uint16_t* out = codes + (size_t)c * cvol + (size_t)lz * plane;
-            for (size_t j = 0; j < plane; ++j) {
+            for (size_t j = 0; j < plane;) {
+                uint32_t sy = 0;
                 if (nu == 1) {
-                    out[j] = sym[0];
-                    continue;
-                }
-                uint32_t v = 0;
-                int l = 0, found = 0;
-                while (l < STZO_LMAX) {
-                    v = (v << 1) | ((words[bit >> 5] >> (31 - (bit & 31))) & 1u);
-                    ++bit;
-                    ++l;
-                    if (cnt[l] && v >= first_code[l] && v - first_code[l] < (uint32_t)cnt[l]) {
-                        out[j] = sym[first_idx[l] + (int)(v - first_code[l])];
-                        found = 1;
+                    sy = sym[0];
+                } else {
+                    uint32_t v = 0;
+                    int l = 0, found = 0;
+                    while (l < STZO_LMAX) {
+                        v = (v << 1) | ((words[bit >> 5] >> (31 - (bit & 31))) & 1u);
+                        ++bit;
+                        ++l;
+                        if (cnt[l] && v >= first_code[l] && v - first_code[l] < (uint32_t)cnt[l]) {
+                            sy = sym[first_idx[l] + (int)(v - first_code[l])];
+                            found = 1;
+                            break;
+                        }
+                    }
+                    if (!found) {
+                        rc = -24;
                         break;
                     }
                 }
-                if (!found) {
-                    rc = -24;
-                    break;
+                if (run_n && sy - run_base < run_n) { /* a run of centre codes */
+                    size_t rl = run_length(sy - run_base, (int)plane);
+                    if (rl > plane - j) {
+                        rc = -25;
+                        break;
+                    }
+                    for (; rl; --rl) out[j++] = (uint16_t)h->radius;
+                } else {
+                    out[j++] = (uint16_t)sy;
                 }
             }
         }

@@ -116,6 +116,10 @@ int stzo_level_chunk(int nx, int ny, int nz, int k, int chunk_high, int chunk_lo
 /* Canonical Huffman codebook of this project's format for one histogram of
  * 2*radius bins. Writes n_used symbols/lengths in canonical order. */
 int stzo_codebook(const uint32_t* hist, int nbins, uint16_t* sym, uint8_t* len);
+/* Run-symbol slots of a stream with code histogram hist (nbins = 2 * radius)
+ * and planes of `plane` codes: returns run_n (0: no runs), *run_base the first
+ * slot (direct run lengths 2..D, then powers of two; see stz_oracle.c). */
+int stzo_run_slots(const uint32_t* hist, int nbins, int plane, uint32_t* run_base);
 
 /* ROI planner restatement (FD5:1578-1839) with the same flat record layout as
  * fd5ref_plan in oracle/ref_shim.cpp. */

@@ -340,11 +340,61 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             STZ_CUDA(cudaMemcpy(fullh[s].data(), ctx->hist.as<uint32_t>() + (size_t)s * R2, (size_t)R2 * 4,
                                 cudaMemcpyDeviceToHost));
         }
-    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
-        if (h_out[s]) build_codebook(fullh[s].data(), R2, 0, syms[s], lens[s]);
-        else build_codebook(ctx->h_hist.as<uint32_t>() + s * (size_t)wn, wn, wlo, syms[s], lens[s]);
-    });
+    lap.mark("full histograms");
     std::vector<StreamDesc> sd = g.sd;
+    // work list over every chunk of every stream
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    // run symbols: slots in unused code values, then the symbol counts of the
+    // run-coded planes (one pass over the codes on the GPU)
+    bool any_runs = false;
+    for (int s = 0; s < nstreams; ++s) {
+        const uint32_t* hw = ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
+        auto count = [&](uint32_t c) -> uint64_t {
+            if (h_out[s]) return fullh[s][c];
+            return (c >= (uint32_t)wlo && c < (uint32_t)(wlo + wn)) ? hw[c - wlo] : 0;
+        };
+        sd[s].run_n = (uint32_t)run_slots(count, R2, (int)(sd[s].C * sd[s].C), sd[s].run_base);
+        any_runs = any_runs || sd[s].run_n;
+    }
+    std::vector<unsigned long long> rstats((size_t)nstreams * kRunStats, 0);
+    if (any_runs) {
+        const size_t r_sd = 0, r_work = align256(sd.size() * sizeof(StreamDesc));
+        const size_t r_ids = align256(r_work + work.size() * sizeof(CtaWork)), r_bytes = align256(r_ids + ids.size() * 4);
+        STZ_CUDA(ctx->h_stage.ensure(r_bytes));
+        uint8_t* hr = ctx->h_stage.as<uint8_t>();
+        std::memcpy(hr + r_sd, sd.data(), sd.size() * sizeof(StreamDesc));
+        std::memcpy(hr + r_work, work.data(), work.size() * sizeof(CtaWork));
+        std::memcpy(hr + r_ids, ids.data(), ids.size() * 4);
+        STZ_CUDA(ctx->work.ensure(r_bytes));
+        STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hr, r_bytes, cudaMemcpyHostToDevice, st));
+        STZ_CUDA(ctx->rstats.ensure(rstats.size() * 8));
+        STZ_CUDA(cudaMemsetAsync(ctx->rstats.p, 0, rstats.size() * 8, st));
+        const uint8_t* dw = ctx->work.as<uint8_t>();
+        {
+            KScope ks(ctx, "k_run_stats");
+            launch_run_stats((const CtaWork*)(dw + r_work), (const uint32_t*)(dw + r_ids), (int)work.size(),
+                             (const StreamDesc*)(dw + r_sd), ctx->codes.as<uint16_t>(),
+                             ctx->rstats.as<unsigned long long>(), st);
+        }
+        STZ_CUDA(cudaGetLastError());
+        STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
+        STZ_CUDA(cudaMemcpyAsync(ctx->h_rstats.p, ctx->rstats.p, rstats.size() * 8, cudaMemcpyDeviceToHost, st));
+        STZ_CUDA(cudaStreamSynchronize(st));
+        std::memcpy(rstats.data(), ctx->h_rstats.p, rstats.size() * 8);
+    }
+    lap.mark("run slots + run stats");
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        std::vector<std::pair<uint32_t, uint64_t>> set;
+        if (sd[s].run_n) {
+            set.push_back({(uint32_t)o.radius, rstats[s * kRunStats]});
+            for (uint32_t i = 0; i < sd[s].run_n; ++i) set.push_back({sd[s].run_base + i, rstats[s * kRunStats + 1 + i]});
+        }
+        if (h_out[s]) build_codebook_adjusted(fullh[s].data(), R2, 0, set, syms[s], lens[s]);
+        else build_codebook_adjusted(ctx->h_hist.as<uint32_t>() + s * (size_t)wn, wn, wlo, set, syms[s], lens[s]);
+    });
+    lap.mark("codebooks");
     uint32_t cb_total = 0;
     for (int s = 0; s < nstreams; ++s) {
         sd[s].cb_off = cb_total;
@@ -364,11 +414,6 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         unpred_off[s + 1] = acc;
     }
     const uint64_t total_unpred = unpred_off[nstreams];
-
-    // work list over every chunk of every stream
-    std::vector<CtaWork> work;
-    std::vector<uint32_t> ids;
-    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
 
     // upload: sd | cb_sym | cb_len | work | ids | uwork
     const size_t o_sd = 0, o_sym = align256(o_sd + sd.size() * sizeof(StreamDesc));
@@ -495,7 +540,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
         const StreamDesc& d = sd[s];
         StreamParts& p = parts[s];
-        append_stream_header(p.hdr, syms[s].data(), lens[s].data(), d.n_used, unpred_off[s + 1] - unpred_off[s],
+        append_stream_header(p.hdr, syms[s].data(), lens[s].data(), d.n_used, d.run_base, d.run_n,
+                             unpred_off[s + 1] - unpred_off[s],
                              ul + unpred_off[s] * elem, elem, h_ucnt + d.chunk_base, choff + d.chunk_base,
                              subo + d.sub_base, (int)d.nchunks, (int)d.C);
         p.words = ctx->h_payload.as<uint32_t>() + meta[nstreams + s];
@@ -537,7 +583,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         std::vector<uint8_t> raw(d.hdr_raw);
         const int nch = (L.dx / L.C) * (L.dy / L.C) * (L.dz / L.C);
         if (!decode_frame(bytes + d.data_off, d.hdr_stored, d.hdr_raw, raw.data())) bad = 1;
-        else if (!parse_stream_header(raw.data(), raw.size(), nch, L.C, elem, p.hdr[i])) bad = 2;
+        else if (!parse_stream_header(raw.data(), raw.size(), nch, L.C, elem, ps.version, p.hdr[i])) bad = 2;
     });
     if (bad) STZ_FAIL(STZ_ERR_FORMAT, bad == 1 ? "stream header frame does not decode" : "bad stream header");
     lap.mark("header frames");
@@ -563,6 +609,10 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         d.cb_off = (uint32_t)syms;
         d.n_used = (uint32_t)H.sym.size();
         syms += d.n_used;
+        d.run_base = H.run_base;
+        d.run_n = H.run_n;
+        if (d.run_n && (uint64_t)d.run_base + d.run_n > 2 * (uint64_t)h.radius)
+            STZ_FAIL(STZ_ERR_FORMAT, "run symbols outside the code range");
         uint64_t raw = 0;
         for (uint64_t v : L.s[i % 7].lr) raw += v;
         if (H.chunk_word_off.back() * 4 != raw) STZ_FAIL(STZ_ERR_FORMAT, "marker table does not match payload size");

@@ -3,12 +3,16 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <numeric>
 
 #include "stz_internal.h"
+#include "trace.h"
 
 // libzstd 1.5.5 is present as a runtime library only; public prototypes (zstd.h).
 extern "C" {
@@ -165,6 +169,13 @@ void min_redundancy_lengths(std::vector<uint64_t>& a)
 
 int build_codebook(const uint32_t* hist, int nbins, int base, std::vector<uint16_t>& sym, std::vector<uint8_t>& len)
 {
+    return build_codebook_adjusted(hist, nbins, base, {}, sym, len);
+}
+
+int build_codebook_adjusted(const uint32_t* hist, int nbins, int base,
+                            const std::vector<std::pair<uint32_t, uint64_t>>& set, std::vector<uint16_t>& sym,
+                            std::vector<uint8_t>& len)
+{
     struct Item {
         uint64_t w;
         uint32_t s;
@@ -172,6 +183,15 @@ int build_codebook(const uint32_t* hist, int nbins, int base, std::vector<uint16
     std::vector<Item> items;
     for (int i = 0; i < nbins; ++i)
         if (hist[i]) items.push_back({hist[i], (uint32_t)(i + base)});
+    if (!set.empty()) {  // items are in symbol order: replace or append the set's counts
+        for (const auto& o : set) {
+            auto it = std::lower_bound(items.begin(), items.end(), o.first,
+                                       [](const Item& x, uint32_t sym) { return x.s < sym; });
+            if (it != items.end() && it->s == o.first) it->w = o.second;
+            else items.insert(it, {o.second, o.first});
+        }
+        items.erase(std::remove_if(items.begin(), items.end(), [](const Item& x) { return x.w == 0; }), items.end());
+    }
     const int n = (int)items.size();
     sym.clear();
     len.clear();
@@ -245,6 +265,22 @@ std::string validate_dims(long long nx, long long ny, long long nz, int chunk_hi
     return "";
 }
 
+int run_slots(const std::function<uint64_t(uint32_t)>& count, int nbins, int plane, uint32_t& run_base)
+{
+    const int J = (int)run_slot_count((uint32_t)plane);
+    run_base = 0;
+    if (J == 0) return 0;
+    for (int u0 = nbins - J; u0 >= 1; --u0) {
+        bool free_ = true;
+        for (int j = 0; j < J && free_; ++j) free_ = count((uint32_t)(u0 + j)) == 0;
+        if (free_) {
+            run_base = (uint32_t)u0;
+            return J;
+        }
+    }
+    return 0;
+}
+
 // ---- container ------------------------------------------------------------------
 bool learned_model_valid(const LearnedModel& m)
 {
@@ -292,13 +328,16 @@ struct Reader {
 }  // namespace
 
 void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const uint8_t* len, uint32_t n_used,
-                          uint64_t n_unpred, const void* unpred, size_t elem, const uint32_t* unpred_count,
-                          const uint64_t* chunk_word_off, const uint32_t* sub_off, int nchunks, int C)
+                          uint32_t run_base, uint32_t run_n, uint64_t n_unpred, const void* unpred, size_t elem,
+                          const uint32_t* unpred_count, const uint64_t* chunk_word_off, const uint32_t* sub_off,
+                          int nchunks, int C)
 {
     Writer w{out};
     w.u32(n_used);
     w.put(sym, 2 * (size_t)n_used);
     w.put(len, n_used);
+    w.u32(run_base);
+    w.u32(run_n);
     w.u64(n_unpred);
     w.put(unpred, n_unpred * elem);
     w.put(unpred_count, 4 * (size_t)nchunks);
@@ -306,7 +345,8 @@ void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const 
     w.put(sub_off, 4 * (size_t)nchunks * C);
 }
 
-bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, StreamHeader& out)
+bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, int version,
+                         StreamHeader& out)
 {
     Reader r{raw, n};
     const uint32_t nu = r.u32();
@@ -315,6 +355,12 @@ bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_
     out.len.resize(nu);
     r.get(out.sym.data(), 2 * (size_t)nu);
     r.get(out.len.data(), nu);
+    out.run_base = out.run_n = 0;
+    if (version >= 3) {
+        out.run_base = r.u32();
+        out.run_n = r.u32();
+        if (out.run_n && (out.run_n != run_slot_count((uint32_t)C * C) || out.run_base < 1)) return false;
+    }
     out.n_unpred = r.u64();
     if (r.err || out.n_unpred > n) return false;
     out.unpred.resize(out.n_unpred * elem);
@@ -349,7 +395,8 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     r.get(mg, 8);
     if (r.err || std::memcmp(mg, kMagic, 8) != 0) return "not an STZ-B200 stream (bad magic)";
     const uint32_t version = r.u32();
-    if (version != 1 && version != 2) return "unsupported stream version";
+    if (version < 1 || version > 3) return "unsupported stream version";
+    out.version = (int)version;
     FileHeader& h = out.h;
     h.dtype = (int)r.u32();
     h.predictor = (int)r.u32();
@@ -380,7 +427,7 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
         if (r.err || L.dx != (h.nx >> sh) || L.dy != (h.ny >> sh) || L.dz != (h.nz >> sh) ||
             L.C != level_chunk(h.nx, h.ny, h.nz, h.K, k, h.chunk_high, h.chunk_low))
             return "bad level record";
-        if (version == 2) {
+        if (version >= 2) {
             L.lflags = r.u32();
             if (L.lflags > 0x7f) return "bad learned-correction flags";
             if (L.lflags) {
@@ -417,8 +464,8 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     return "";
 }
 
-std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
-                                     std::vector<StreamParts>& parts, ThreadPool& pool)
+Bytes write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
+                      std::vector<StreamParts>& parts, ThreadPool& pool)
 {
     // Frame list: per stream its header, then one frame per chunk z-layer.
     struct Frame {
@@ -445,7 +492,10 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
     std::iota(order.begin(), order.end(), 0);
     std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return frames[a].n > frames[b].n; });
     const int level = h.zstd_level;
+    Lap lap("container");
+    std::atomic<int64_t> busy_ns{0};
     pool.parallel_for(frames.size(), [&](size_t k) {
+        const auto t0 = std::chrono::steady_clock::now();
         Frame& f = frames[order[k]];
         f.raw = true;
         f.stored = f.n;
@@ -460,13 +510,21 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
                 f.out.reset();
             }
         }
+        if (lap.on)
+            busy_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0)
+                           .count();
     });
-    std::vector<uint8_t> out;
-    Writer w{out};
+    if (lap.on) {
+        size_t raw = 0, mx = 0;
+        for (const Frame& f : frames) raw += f.n, mx = std::max(mx, f.n);
+        std::fprintf(stderr, "[stz] container: %zu frames, %.2f MB raw, largest %.3f MB, zstd busy %.3f ms on %d threads\n",
+                     frames.size(), raw / 1e6, mx / 1e6, busy_ns.load() / 1e6, pool.size());
+    }
+    lap.mark("zstd frames");
+    std::vector<uint8_t> dir;
+    Writer w{dir};
     w.put(kMagic, 8);
-    bool learned = false;  // version 2 carries per-level learned corrections
-    for (int k = 1; k <= h.K; ++k) learned = learned || levels[k].lflags != 0;
-    w.u32(learned ? 2 : 1);
+    w.u32(3);  // per-level learned-correction fields, run symbols
     w.u32((uint32_t)h.dtype);
     w.u32((uint32_t)h.predictor);
     w.u32((uint32_t)h.nx);
@@ -493,10 +551,8 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
         w.u32((uint32_t)L.dz);
         w.u32((uint32_t)L.C);
         w.f64(L.eb);
-        if (learned) {
-            w.u32(L.lflags);
-            if (L.lflags) w.put(&L.model, sizeof(LearnedModel));
-        }
+        w.u32(L.lflags);
+        if (L.lflags) w.put(&L.model, sizeof(LearnedModel));
         for (int b = 0; b < 7; ++b, ++si) {
             const StreamParts& p = parts[si];
             w.u32((uint32_t)p.layers);
@@ -507,15 +563,20 @@ std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, 
             for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames[first[si] + 1 + L2].n);
         }
     }
-    // frames in order after the directory, copied in parallel
+    // the directory, then the frames in order, copied in parallel into an
+    // uninitialized buffer
     std::vector<size_t> off(frames.size() + 1);
-    off[0] = out.size();
+    off[0] = dir.size();
     for (size_t i = 0; i < frames.size(); ++i) off[i + 1] = off[i] + frames[i].stored;
+    Bytes out;
     out.resize(off.back());
+    std::memcpy(out.data(), dir.data(), dir.size());
+    lap.mark("directory");
     uint8_t* base = out.data();
     pool.parallel_for(frames.size(), [&](size_t i) {
         if (frames[i].stored) std::memcpy(base + off[i], frames[i].bytes(), frames[i].stored);
     });
+    lap.mark("frame copy");
     return out;
 }
 

@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -14,6 +15,33 @@
 #include "stz_internal.h"
 
 namespace stz {
+
+// Byte buffer whose resize leaves new bytes uninitialized (the container is
+// written in parallel right after; zero-filling first costs a single-threaded
+// pass over fresh pages).
+template <class T>
+struct DefaultInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInitAlloc<U>;
+    };
+    DefaultInitAlloc() = default;
+    template <class U>
+    DefaultInitAlloc(const DefaultInitAlloc<U>&) noexcept
+    {
+    }
+    template <class U>
+    void construct(U* p) noexcept
+    {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a)
+    {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+using Bytes = std::vector<uint8_t, DefaultInitAlloc<uint8_t>>;
 
 // ---- thread pool ----------------------------------------------------------
 class ThreadPool {
@@ -42,6 +70,19 @@ private:
 // output in canonical (length, symbol) order. A lone symbol gets length 0.
 // `base` is added to every histogram index (windowed histograms).
 int build_codebook(const uint32_t* hist, int nbins, int base, std::vector<uint16_t>& sym, std::vector<uint8_t>& len);
+// The same with the counts of the listed symbols set (symbols outside the
+// window [base, base + nbins) are added).
+int build_codebook_adjusted(const uint32_t* hist, int nbins, int base,
+                            const std::vector<std::pair<uint32_t, uint64_t>>& set, std::vector<uint16_t>& sym,
+                            std::vector<uint8_t>& len);
+
+// ---- run symbols (container version 3) ---------------------------------------
+// Runs of the centre code (= radius) inside a plane are coded with run
+// symbols (run_geometry) in run_n consecutive code values the stream does
+// not use, [run_base, run_base + run_n): the highest free window in
+// [1, nbins) (count(code) = the stream's code count). Returns run_n (0: no
+// runs).
+int run_slots(const std::function<uint64_t(uint32_t)>& count, int nbins, int plane, uint32_t& run_base);
 
 // ---- container ------------------------------------------------------------
 struct FileHeader {
@@ -72,6 +113,7 @@ struct LevelDir {
 bool learned_model_valid(const LearnedModel& m);
 
 struct ParsedStream {
+    int version = 0;  // 1: plain, 2: learned fields, 3: learned fields and run symbols
     FileHeader h;
     size_t coarsest_off = 0;
     std::vector<LevelDir> lv;  // index 1..K (0 unused)
@@ -86,6 +128,7 @@ struct StreamHeader {
     std::vector<uint32_t> unpred_count;
     std::vector<uint64_t> chunk_word_off;  // nchunks + 1
     std::vector<uint32_t> sub_off;         // nchunks * C
+    uint32_t run_base = 0, run_n = 0;      // run symbols (version 3)
 };
 
 // Levels of the hierarchy and chunk edge per level (shared rule with the
@@ -98,7 +141,8 @@ std::string validate_dims(long long nx, long long ny, long long nz, int chunk_hi
 // Parse the directory; returns "" on success, else an error message.
 std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out);
 bool decode_frame(const uint8_t* src, uint64_t stored, uint64_t raw, uint8_t* dst);
-bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, StreamHeader& out);
+bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, int version,
+                         StreamHeader& out);
 
 // Writer input for one residual stream.
 struct StreamParts {
@@ -109,13 +153,14 @@ struct StreamParts {
 };
 
 void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const uint8_t* len, uint32_t n_used,
-                          uint64_t n_unpred, const void* unpred, size_t elem, const uint32_t* unpred_count,
-                          const uint64_t* chunk_word_off, const uint32_t* sub_off, int nchunks, int C);
+                          uint32_t run_base, uint32_t run_n, uint64_t n_unpred, const void* unpred, size_t elem,
+                          const uint32_t* unpred_count, const uint64_t* chunk_word_off, const uint32_t* sub_off,
+                          int nchunks, int C);
 
 // Assemble the container: directory, coarsest grid, then every frame
 // (zstd-compressed in parallel on the pool).
-std::vector<uint8_t> write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
-                                     std::vector<StreamParts>& parts, ThreadPool& pool);
+Bytes write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
+                      std::vector<StreamParts>& parts, ThreadPool& pool);
 
 // ---- ROI planner (FD5:1578-1839) -------------------------------------------
 struct AxisRange {

@@ -13,6 +13,15 @@
 // is stored, so all planes of all chunks of all streams encode and decode
 // independently. Bits are packed MSB-first into 32-bit words; a chunk starts
 // on a word boundary.
+//
+// Runs: inside a plane, a maximal run of r centre codes (code == radius) is
+// coded with run symbols (run_geometry): while r > D, 2^k (the largest power
+// of two <= r, k <= J) when k > LD, else D codes; then one symbol for the
+// remaining 2..D codes, or the centre code itself for one. The run symbols
+// occupy run_n code values the stream does not use (StreamDesc::run_base),
+// so they share the codebook, the tables and the 16-bit symbol width with
+// the codes; a well-predicted stream (mostly centre codes) then costs well
+// under one bit per code.
 #include <cuda_runtime.h>
 
 #include "huffman.h"
@@ -53,6 +62,81 @@ __global__ void k_expand_codebook(const StreamDesc* __restrict__ sd, const uint1
     }
 }
 
+// Symbols of one plane with runs: f(sym) for each, in order.
+template <class F>
+__device__ __forceinline__ void plane_symbols(const uint16_t* __restrict__ src, size_t plane, const StreamDesc& s,
+                                              F&& f)
+{
+    const uint32_t R = s.radius, base = s.run_base;
+    uint32_t D, LD;
+    const uint32_t J = run_geometry((uint32_t)plane, D, LD);
+    uint32_t run = 0;
+    auto flush = [&]() {
+        while (run > D) {
+            const uint32_t k = min((uint32_t)(31 - __clz(run)), J);
+            if (k > LD) {
+                f(base + D - 1 + (k - LD - 1));
+                run -= 1u << k;
+            } else {
+                f(base + D - 2);
+                run -= D;
+            }
+        }
+        if (run >= 2) f(base + run - 2);
+        else if (run) f(R);
+        run = 0;
+    };
+    auto feed = [&](uint32_t q) {
+        if (q == R) {
+            ++run;
+        } else {
+            if (run) flush();
+            f(q);
+        }
+    };
+    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
+        const uint4* v = reinterpret_cast<const uint4*>(src);
+        for (size_t j = 0; j < plane / 8; ++j) {
+            const uint4 q = __ldg(v + j);
+            feed(q.x & 0xffffu), feed(q.x >> 16), feed(q.y & 0xffffu), feed(q.y >> 16);
+            feed(q.z & 0xffffu), feed(q.z >> 16), feed(q.w & 0xffffu), feed(q.w >> 16);
+        }
+    } else {
+        for (size_t j = 0; j < plane; ++j) feed(__ldg(src + j));
+    }
+    if (run) flush();
+}
+
+// Run-symbol counts of every listed plane (streams with runs).
+__global__ void __launch_bounds__(kCoderThreads) k_run_stats(const CtaWork* __restrict__ work,
+                                                             const uint32_t* __restrict__ chunk_ids,
+                                                             const StreamDesc* __restrict__ sd,
+                                                             const uint16_t* __restrict__ codes,
+                                                             unsigned long long* __restrict__ stats)
+{
+    __shared__ uint32_t cnt[kRunStats];
+    const CtaWork w = work[blockIdx.x];
+    const StreamDesc s = sd[w.stream];
+    if (s.run_n == 0) return;  // uniform per block
+    if (threadIdx.x < kRunStats) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t C = s.C, t = threadIdx.x;
+    if (t / C < w.count) {
+        const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
+        const size_t plane = (size_t)C * C;
+        const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+        uint32_t singles = 0;
+        plane_symbols(src, plane, s, [&](uint32_t sym) {
+            if (sym == s.radius) ++singles;
+            else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
+        });
+        if (singles) atomicAdd(&cnt[0], singles);
+    }
+    __syncthreads();
+    if (threadIdx.x < kRunStats && cnt[threadIdx.x])
+        atomicAdd(&stats[(size_t)w.stream * kRunStats + threadIdx.x], cnt[threadIdx.x]);
+}
+
 // Bits of every sub-chunk.
 __global__ void __launch_bounds__(kCoderThreads) k_sub_bits(const CtaWork* __restrict__ work,
                                                             const uint32_t* __restrict__ chunk_ids,
@@ -71,7 +155,9 @@ __global__ void __launch_bounds__(kCoderThreads) k_sub_bits(const CtaWork* __res
     const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
     uint32_t bits = 0;
-    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
+    if (s.run_n) {
+        plane_symbols(src, plane, s, [&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; });
+    } else if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
         // 8 codes per 16-byte load: one request per lane instead of eight
         const uint4* v = reinterpret_cast<const uint4*>(src);
         for (size_t j = 0; j < plane / 8; ++j) {
@@ -198,7 +284,9 @@ __global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restr
             ++wi;
         }
     };
-    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
+    if (s.run_n) {
+        plane_symbols(src, plane, s, put);
+    } else if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
         const uint4* v = reinterpret_cast<const uint4*>(src);
         for (size_t j = 0; j < plane / 8; ++j) {
             const uint4 q = __ldg(v + j);
@@ -298,7 +386,9 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
     const size_t plane = (size_t)C * C;
     uint16_t* dst = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
     if (s.n_used == 1) {
-        const uint16_t v = cb_sym[s.cb_off];
+        // a lone run symbol means the plane is all centre codes
+        const uint16_t v0 = cb_sym[s.cb_off];
+        const uint16_t v = (uint32_t)v0 - s.run_base < s.run_n ? (uint16_t)s.radius : v0;
         if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
             const uint32_t v2 = (uint32_t)v | ((uint32_t)v << 16);
             for (size_t j = 0; j < plane / 8; ++j) reinterpret_cast<uint4*>(dst)[j] = make_uint4(v2, v2, v2, v2);
@@ -367,7 +457,54 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
         }
         return sym;
     };
-    if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
+    if (s.run_n) {
+        // Runs expand to 2^k centre codes, clipped to the plane (a corrupt
+        // stream cannot write past it; every symbol yields at least one code,
+        // so the loop ends). Vector form: codes collect in a 128-bit shift
+        // register and leave as 16-byte stores; long runs store whole
+        // 8-code groups directly.
+        const uint32_t R = s.radius, base = s.run_base, J = s.run_n;
+        uint32_t D, LD;
+        run_geometry((uint32_t)plane, D, LD);
+        size_t j = 0;
+        if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
+            uint4* d4 = reinterpret_cast<uint4*>(dst);
+            uint64_t s0 = 0, s1 = 0;
+            uint32_t ns = 0;
+            auto push = [&](uint32_t v) {
+                s0 = (s0 >> 16) | (s1 << 48);
+                s1 = (s1 >> 16) | ((uint64_t)v << 48);
+                if (++ns == 8) {
+                    d4[j >> 3] = make_uint4((uint32_t)s0, (uint32_t)(s0 >> 32), (uint32_t)s1, (uint32_t)(s1 >> 32));
+                    ns = 0;
+                }
+                ++j;
+            };
+            const uint32_t r2 = R | (R << 16);
+            const uint4 rr = make_uint4(r2, r2, r2, r2);
+            while (j < plane) {
+                const uint32_t sym = next();
+                if (sym - base < J) {
+                    size_t n = min((size_t)run_length(sym - base, D, LD), plane - j);
+                    while (n && ns) push(R), --n;
+                    for (; n >= 8; n -= 8, j += 8) d4[j >> 3] = rr;
+                    while (n) push(R), --n;
+                } else {
+                    push(sym);
+                }
+            }
+        } else {
+            while (j < plane) {
+                const uint32_t sym = next();
+                if (sym - base < J) {
+                    const size_t n = min((size_t)run_length(sym - base, D, LD), plane - j);
+                    for (size_t i = 0; i < n; ++i) dst[j++] = (uint16_t)R;
+                } else {
+                    dst[j++] = (uint16_t)sym;
+                }
+            }
+        }
+    } else if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
         // 8 symbols per 16-byte store; all lanes decode in lockstep
         uint4* d4 = reinterpret_cast<uint4*>(dst);
         for (size_t j = 0; j < plane / 8; ++j) {
@@ -541,6 +678,12 @@ void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* 
                             uint32_t* ctab, cudaStream_t st)
 {
     if (nstreams) k_expand_codebook<<<nstreams, 256, 0, st>>>(sd, cb_sym, cb_len, ctab);
+}
+
+void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                      const uint16_t* codes, unsigned long long* stats, cudaStream_t st)
+{
+    if (nwork > 0) k_run_stats<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, stats);
 }
 
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,

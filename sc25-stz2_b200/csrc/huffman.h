@@ -20,6 +20,12 @@ struct UnpredWork {
 // Dense code table per stream (2*radius entries): code << 5 | length.
 void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
                             uint32_t* ctab, cudaStream_t st);
+// Run-symbol counts per stream (streams with run_n > 0): stats[s * kRunStats]
+// gets the centre codes left as single symbols, stats[s * kRunStats + 1 + i]
+// the uses of run slot i. stats must be zeroed.
+constexpr int kRunStats = 64;
+void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                      const uint16_t* codes, unsigned long long* stats, cudaStream_t st);
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                      const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st);
 void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,

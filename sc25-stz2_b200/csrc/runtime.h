@@ -15,6 +15,7 @@
 
 #include "host.h"
 #include "huffman.h"
+#include "trace.h"
 #include "stz/stz.h"
 #include "stz_internal.h"
 
@@ -40,42 +41,6 @@
     } while (0)
 
 namespace stz {
-
-// Host phase timer, printed to stderr when STZ_TRACE is set.
-struct Trace {
-    const char* name;
-    std::chrono::steady_clock::time_point t0;
-    bool on;
-    explicit Trace(const char* n) : name(n), on(std::getenv("STZ_TRACE") != nullptr)
-    {
-        if (on) t0 = std::chrono::steady_clock::now();
-    }
-    ~Trace()
-    {
-        if (on)
-            std::fprintf(stderr, "[stz] %-28s %8.3f ms\n", name,
-                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-    }
-};
-
-// Lap timer: mark(name) prints the time since the previous mark (STZ_TRACE).
-struct Lap {
-    const char* scope;
-    std::chrono::steady_clock::time_point t;
-    bool on;
-    explicit Lap(const char* s) : scope(s), on(std::getenv("STZ_TRACE") != nullptr)
-    {
-        if (on) t = std::chrono::steady_clock::now();
-    }
-    void mark(const char* what)
-    {
-        if (!on) return;
-        const auto now = std::chrono::steady_clock::now();
-        std::fprintf(stderr, "[stz] %s: %-24s %8.3f ms\n", scope, what,
-                     std::chrono::duration<double, std::milli>(now - t).count());
-        t = now;
-    }
-};
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -273,8 +238,8 @@ struct stz_context {
     }
     stz::DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
-        tiles, models, eval;
-    stz::PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small;
+        tiles, models, eval, rstats;
+    stz::PinBuf h_hist, h_meta, h_payload, h_stage, h_io, h_small, h_rstats;
     // device buffers lent to one-off decodes
     stz::DevBuf p_stage, p_coarsest, p_base;
     void borrow(stz::Prepared& p)
@@ -286,7 +251,7 @@ struct stz_context {
 };
 
 struct stz_stream {
-    std::vector<uint8_t> bytes;
+    stz::Bytes bytes;
     stz::ParsedStream dir;
     size_t raw_payload_bytes = 0;
     std::unique_ptr<stz::Prepared> resident;

@@ -104,8 +104,33 @@ struct StreamDesc {
     uint32_t nchunks;
     uint32_t cb_off;      // offset of the canonical list (sym/len) in the codebook arrays
     uint32_t n_used;      // symbols in the codebook
-    uint32_t radius;
+    uint32_t radius;      // also the centre code
+    uint32_t run_base;    // run symbols in code values [run_base, run_base + run_n)
+    uint32_t run_n;       // (0: no runs); see run_geometry
 };
+
+// Run symbols of a plane of `plane` codes (container version 3): J =
+// min(14, floor(log2 plane)), D = min(32, 2^J), LD = log2 D. Slot i < D - 1
+// stands for a run of i + 2 centre codes, slot D - 1 + m for 2^(LD + 1 + m)
+// (m < J - LD); run_n = D - 1 + J - LD slots. Returns J (0: no runs).
+__host__ __device__ inline uint32_t run_geometry(uint32_t plane, uint32_t& D, uint32_t& LD)
+{
+    uint32_t J = 0;
+    while (J < 14 && (2ull << J) <= plane) ++J;
+    LD = J < 5 ? J : 5;
+    D = 1u << LD;
+    return J;
+}
+__host__ __device__ inline uint32_t run_slot_count(uint32_t plane)
+{
+    uint32_t D, LD;
+    const uint32_t J = run_geometry(plane, D, LD);
+    return J ? D - 1 + J - LD : 0;
+}
+__host__ __device__ inline uint32_t run_length(uint32_t slot, uint32_t D, uint32_t LD)
+{
+    return slot < D - 1 ? slot + 2 : 1u << (slot - (D - 1) + LD + 1);
+}
 
 // One CTA of the chunk coders: `count` chunks of stream `stream` whose ids are
 // chunk_ids[first .. first + count).
