@@ -413,7 +413,18 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
     uint32_t* hist = (uint32_t*)calloc((size_t)nbins, 4);
     for (size_t i = 0; i < n; ++i) hist[codes[i]]++;
     uint32_t run_base = 0;
-    const int run_n = stzo_run_slots(hist, nbins, (int)plane, &run_base);
+    int run_n = stzo_run_slots(hist, nbins, (int)plane, &run_base);
+    /* runs only where they shorten the Huffman payload (else the decoder
+     * keeps its plain path): compare sum(count * length) of both codebooks */
+    uint64_t bits_plain = 0;
+    if (run_n) {
+        uint16_t* ps = (uint16_t*)malloc(2 * (size_t)nbins);
+        uint8_t* pl = (uint8_t*)malloc((size_t)nbins);
+        const int pn = stzo_codebook(hist, nbins, ps, pl);
+        for (int i = 0; i < pn; ++i) bits_plain += (uint64_t)hist[ps[i]] * pl[i];
+        free(ps);
+        free(pl);
+    }
     /* the symbol stream: runs inside every plane */
     uint16_t* syms = (uint16_t*)malloc(2 * (n ? n : 1));
     size_t* pstart = (size_t*)malloc(sizeof(size_t) * ((size_t)nch * C + 1));
@@ -424,11 +435,28 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
             m += plane_symbols(codes + (size_t)c * cvol + (size_t)lz * plane, plane, radius, run_base, run_n, syms + m);
         }
     pstart[(size_t)nch * C] = m;
-    memset(hist, 0, 4 * (size_t)nbins);
-    for (size_t i = 0; i < m; ++i) hist[syms[i]]++;
+    uint32_t* rhist = (uint32_t*)calloc((size_t)nbins, 4);
+    for (size_t i = 0; i < m; ++i) rhist[syms[i]]++;
     uint16_t* sym = (uint16_t*)malloc(2 * (size_t)nbins);
     uint8_t* len = (uint8_t*)malloc((size_t)nbins);
-    const int nu = stzo_codebook(hist, nbins, sym, len);
+    int nu = stzo_codebook(rhist, nbins, sym, len);
+    if (run_n) {
+        uint64_t bits_runs = 0;
+        for (int i = 0; i < nu; ++i) bits_runs += (uint64_t)rhist[sym[i]] * len[i];
+        if (bits_runs >= bits_plain) { /* plain coding: symbols = codes */
+            run_n = 0;
+            run_base = 0;
+            m = 0;
+            for (int c = 0; c < nch; ++c)
+                for (int lz = 0; lz < C; ++lz) {
+                    pstart[(size_t)c * C + lz] = m;
+                    m += plane_symbols(codes + (size_t)c * cvol + (size_t)lz * plane, plane, radius, 0, 0, syms + m);
+                }
+            pstart[(size_t)nch * C] = m;
+            nu = stzo_codebook(hist, nbins, sym, len);
+        }
+    }
+    free(rhist);
     uint32_t* code = (uint32_t*)malloc(4 * (size_t)(nu ? nu : 1));
     canonical_codes(len, nu, code);
     uint32_t* ctab = (uint32_t*)calloc((size_t)nbins, 4);

@@ -386,13 +386,37 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     lap.mark("run slots + run stats");
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        const uint32_t* hw = h_out[s] ? fullh[s].data() : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
+        const int hn = h_out[s] ? R2 : wn, hb = h_out[s] ? 0 : wlo;
+        auto code_count = [&](uint32_t c) -> uint64_t {
+            return c >= (uint32_t)hb && c < (uint32_t)(hb + hn) ? hw[c - hb] : 0;
+        };
+        build_codebook(hw, hn, hb, syms[s], lens[s]);
+        if (!sd[s].run_n) return;
+        // runs only where they shorten the Huffman payload (else the decoder
+        // keeps its plain path): sum(count * length) of both codebooks
+        uint64_t bits_plain = 0;
+        for (size_t i = 0; i < syms[s].size(); ++i) bits_plain += code_count(syms[s][i]) * lens[s][i];
         std::vector<std::pair<uint32_t, uint64_t>> set;
-        if (sd[s].run_n) {
-            set.push_back({(uint32_t)o.radius, rstats[s * kRunStats]});
-            for (uint32_t i = 0; i < sd[s].run_n; ++i) set.push_back({sd[s].run_base + i, rstats[s * kRunStats + 1 + i]});
+        set.push_back({(uint32_t)o.radius, rstats[s * kRunStats]});
+        for (uint32_t i = 0; i < sd[s].run_n; ++i) set.push_back({sd[s].run_base + i, rstats[s * kRunStats + 1 + i]});
+        std::vector<uint16_t> rs;
+        std::vector<uint8_t> rl;
+        build_codebook_adjusted(hw, hn, hb, set, rs, rl);
+        uint64_t bits_runs = 0;
+        for (size_t i = 0; i < rs.size(); ++i) {
+            uint64_t c = code_count(rs[i]);
+            for (const auto& e : set)
+                if (e.first == rs[i]) c = e.second;
+            bits_runs += c * rl[i];
         }
-        if (h_out[s]) build_codebook_adjusted(fullh[s].data(), R2, 0, set, syms[s], lens[s]);
-        else build_codebook_adjusted(ctx->h_hist.as<uint32_t>() + s * (size_t)wn, wn, wlo, set, syms[s], lens[s]);
+        if (bits_runs < bits_plain) {
+            syms[s].swap(rs);
+            lens[s].swap(rl);
+        } else {
+            sd[s].run_n = 0;
+            sd[s].run_base = 0;
+        }
     });
     lap.mark("codebooks");
     uint32_t cb_total = 0;

@@ -96,8 +96,13 @@ __device__ __forceinline__ void plane_symbols(const uint16_t* __restrict__ src, 
     };
     if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
         const uint4* v = reinterpret_cast<const uint4*>(src);
+        const uint32_t R2 = R | (R << 16);
         for (size_t j = 0; j < plane / 8; ++j) {
             const uint4 q = __ldg(v + j);
+            if (((q.x ^ R2) | (q.y ^ R2) | (q.z ^ R2) | (q.w ^ R2)) == 0) {  // 8 centre codes
+                run += 8;
+                continue;
+            }
             feed(q.x & 0xffffu), feed(q.x >> 16), feed(q.y & 0xffffu), feed(q.y >> 16);
             feed(q.z & 0xffffu), feed(q.z >> 16), feed(q.w & 0xffffu), feed(q.w >> 16);
         }
@@ -468,29 +473,41 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
         run_geometry((uint32_t)plane, D, LD);
         size_t j = 0;
         if (plane % 8 == 0 && ((uintptr_t)dst & 15) == 0) {
+            // 8 staged codes in (s0, s1), slot i at bits 16i; n copies of a
+            // code enter with one masked OR, a full stage leaves as one store
             uint4* d4 = reinterpret_cast<uint4*>(dst);
             uint64_t s0 = 0, s1 = 0;
             uint32_t ns = 0;
-            auto push = [&](uint32_t v) {
-                s0 = (s0 >> 16) | (s1 << 48);
-                s1 = (s1 >> 16) | ((uint64_t)v << 48);
-                if (++ns == 8) {
-                    d4[j >> 3] = make_uint4((uint32_t)s0, (uint32_t)(s0 >> 32), (uint32_t)s1, (uint32_t)(s1 >> 32));
+            auto low = [](uint32_t b) -> uint64_t { return b >= 64 ? ~0ull : (1ull << b) - 1; };
+            auto put = [&](uint32_t v, uint32_t n) {  // n <= 8 - ns copies of v
+                const uint64_t p = (uint64_t)(v | (v << 16)) * 0x0000000100000001ull;
+                const uint32_t a = 16 * ns, b = 16 * (ns + n);
+                s0 |= p & (low(min(b, 64u)) & ~low(min(a, 64u)));
+                s1 |= p & (low(b > 64 ? b - 64 : 0) & ~low(a > 64 ? a - 64 : 0));
+                ns += n;
+                j += n;
+                if (ns == 8) {
+                    d4[(j >> 3) - 1] =
+                        make_uint4((uint32_t)s0, (uint32_t)(s0 >> 32), (uint32_t)s1, (uint32_t)(s1 >> 32));
+                    s0 = s1 = 0;
                     ns = 0;
                 }
-                ++j;
             };
             const uint32_t r2 = R | (R << 16);
             const uint4 rr = make_uint4(r2, r2, r2, r2);
             while (j < plane) {
                 const uint32_t sym = next();
                 if (sym - base < J) {
-                    size_t n = min((size_t)run_length(sym - base, D, LD), plane - j);
-                    while (n && ns) push(R), --n;
+                    uint32_t n = (uint32_t)min((size_t)run_length(sym - base, D, LD), plane - j);
+                    if (ns) {
+                        const uint32_t k = min(n, 8u - ns);
+                        put(R, k);
+                        n -= k;
+                    }
                     for (; n >= 8; n -= 8, j += 8) d4[j >> 3] = rr;
-                    while (n) push(R), --n;
+                    if (n) put(R, n);
                 } else {
-                    push(sym);
+                    put(sym, 1);
                 }
             }
         } else {
