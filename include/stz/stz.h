@@ -429,6 +429,10 @@ stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int lev
  * reference's equivalent is SZ3-ncp HuffmanEncoder::preprocess_encode_fast
  * (call site FD5:1401-1402), whose format is not available. */
 stz_status stz_debug_codebook(const uint32_t* hist, int nbins, uint16_t* sym, uint8_t* len, int* n_used);
+/* Run-symbol slots (container version 3) of a stream with code histogram
+ * hist (nbins = 2 * radius) and planes of `plane` codes: *run_n slots from
+ * *run_base (0: no runs). Host only. */
+stz_status stz_debug_run_slots(const uint32_t* hist, int nbins, int plane, uint32_t* run_base, uint32_t* run_n);
 
 #ifdef __cplusplus
 }

@@ -249,6 +249,14 @@ def codebook(hist: np.ndarray):
     return sym[:n].copy(), ln[:n].copy()
 
 
+def run_slots(hist: np.ndarray, plane: int):
+    L = oracle()
+    h = np.ascontiguousarray(hist, dtype=np.uint32)
+    base = C.c_uint32()
+    n = L.stzo_run_slots(_p(h), len(h), int(plane), C.byref(base))
+    return base.value, n
+
+
 # ---- level functions -----------------------------------------------------------
 def level_encode(fine, coarse, eb, radius=32768, predictor=0, decoded=True, use_ref=False):
     """Codes (7, n) row-major per block, unpred values, counts, decoded fine grid."""

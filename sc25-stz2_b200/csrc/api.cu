@@ -1540,6 +1540,14 @@ stz_status stz_debug_codebook(const uint32_t* hist, int nbins, uint16_t* sym, ui
     return STZ_OK;
 }
 
+stz_status stz_debug_run_slots(const uint32_t* hist, int nbins, int plane, uint32_t* run_base, uint32_t* run_n)
+{
+    g_err.clear();
+    if (!hist || !run_base || !run_n || nbins <= 0 || nbins > 65536 || plane < 1) STZ_FAIL(STZ_ERR_ARG, "bad arguments");
+    *run_n = (uint32_t)run_slots([&](uint32_t c) -> uint64_t { return hist[c]; }, nbins, plane, *run_base);
+    return STZ_OK;
+}
+
 stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int k, int block, uint16_t* codes, size_t cap,
                                   size_t* n_out)
 {

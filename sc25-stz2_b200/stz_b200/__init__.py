@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_plan_box.argtypes = [sz, sz, sz, C.c_int, C.c_int, i64p, i64p, i64p, sz, C.POINTER(sz)]
     lib.stz_debug_stream_codes.argtypes = [vp, vp, C.c_int, C.c_int, vp, sz, C.POINTER(sz)]
     lib.stz_debug_codebook.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
+    lib.stz_debug_run_slots.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     lib.stz_quantize_noalloc_dev.argtypes = [C.c_int, vp, sz, C.c_double, C.c_int, vp, vp, C.POINTER(sz), vp]
     lib.stz_context_stream.argtypes = [vp, C.POINTER(vp)]
     lib.stz_profile_enable.argtypes = [vp, C.c_int]
@@ -647,6 +648,15 @@ def codebook(hist: np.ndarray):
     _check(lib.stz_debug_codebook(h.ctypes.data_as(C.c_void_p), len(h), sym.ctypes.data_as(C.c_void_p),
                                   ln.ctypes.data_as(C.c_void_p), C.byref(n)))
     return sym[: n.value].copy(), ln[: n.value].copy()
+
+
+def run_slots(hist: np.ndarray, plane: int):
+    """(run_base, run_n) of the container's run symbols for a code histogram."""
+    lib = load_library()
+    h = np.ascontiguousarray(hist, dtype=np.uint32)
+    base, n = C.c_uint32(), C.c_uint32()
+    _check(lib.stz_debug_run_slots(h.ctypes.data_as(C.c_void_p), len(h), int(plane), C.byref(base), C.byref(n)))
+    return base.value, n.value
 
 
 class Trainer:

@@ -314,3 +314,41 @@ def test_plain_cubic_kernel_matches_reference_golden(ctx, golden, suf):
         out = torch.zeros_like(tr)
         ctx.preprocess_block(b, ts, tr, out, predictor=1)
         assert np.array_equal(bits(out), bits(diff[b])), b
+
+
+# ---- run symbols (container version 3) ---------------------------------------------
+@pytest.mark.parametrize("case", ["constant", "noise_full_range", "ramp_spikes", "tiny_chunks"])
+def test_run_symbol_streams_match_oracle(ctx, case):
+    """Streams whose planes are one long run (single-symbol codebooks of run
+    symbols), streams whose code range is full (no free window: no runs),
+    mixed runs and spikes, and planes of 4 codes (2x2 chunks)."""
+    rng = np.random.default_rng(3)
+    kw = dict(chunk_high=8, chunk_low=4)
+    if case == "constant":
+        f = np.full((32, 32, 64), 2.5, np.float32)
+        rel, radius = 1e-3, 32768
+    elif case == "noise_full_range":
+        f = rng.uniform(-1, 1, (32, 32, 32)).astype(np.float32)
+        rel, radius = 1e-4, 64
+    elif case == "ramp_spikes":
+        f = np.fromfunction(lambda z, y, x: 0.01 * x + 0.003 * y * z, (64, 32, 32), dtype=np.float32)
+        idx = rng.integers(0, f.size, 300)
+        f.flat[idx] += rng.normal(0, 5, 300).astype(np.float32)
+        rel, radius = 1e-4, 256
+    else:
+        f = make_field("grf", (16, 16, 32), np.float32, 4)
+        rel, radius = 1e-3, 32768
+        kw = dict(chunk_high=2, chunk_low=1)
+    s = ctx.compress(f, eb=rel, eb_mode="rel", radius=radius, **kw)
+    b = s.to_bytes()
+    assert int.from_bytes(b[8:12], "little") == 3
+    assert b == po.compress(f, s.info().eb, radius=radius, **kw)
+    out = ctx.decompress(s)
+    assert np.array_equal(bits(out), bits(po.decompress(b)))
+    E = rel * max(float(f.max()) - float(f.min()), 0.0) or rel
+    assert np.abs(out.astype(np.float64) - f).max() <= E
+    nz, ny, nx = f.shape
+    for lo, hi in (((1, 2, 3), (nx - 3, ny - 2, nz - 1)), ((0, ny // 2, 0), (nx - 1, ny // 2, nz - 1))):
+        box = ctx.decompress_box(s, lo, hi)
+        want = out[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+        assert np.array_equal(bits(box), bits(want)), (lo, hi)

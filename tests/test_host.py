@@ -123,6 +123,33 @@ def test_codebook_matches_oracle():
             assert (2.0 ** -l1.astype(np.float64)).sum() <= 1.0  # Kraft
 
 
+def test_run_slots_match_oracle():
+    """Run-symbol slots: the highest window of unused codes, none when the
+    range is full, sized by the plane (direct lengths up to 32, then powers
+    of two)."""
+    rng = np.random.default_rng(9)
+    cases = []
+    for nbins in (16, 64, 4096, 65536):
+        for plane in (1, 2, 4, 16, 64, 256, 1024, 16384):
+            h = np.zeros(nbins, np.uint32)
+            h[nbins // 2] = 100
+            cases.append((h.copy(), plane))                       # top free
+            h[-3:] = 1
+            cases.append((h.copy(), plane))                       # top used: next window down
+            h2 = rng.integers(0, 3, nbins).astype(np.uint32)
+            cases.append((h2, plane))                             # scattered free codes
+            cases.append((np.ones(nbins, np.uint32), plane))      # none free
+    for h, plane in cases:
+        got = stz_b200.run_slots(h, plane)
+        assert got == po.run_slots(h, plane), (len(h), plane)
+        base, n = got
+        if n:
+            assert base >= 1 and base + n <= len(h) and not h[base:base + n].any()
+    assert stz_b200.run_slots(np.zeros(65536, np.uint32), 1024) == (65536 - 36, 36)
+    assert stz_b200.run_slots(np.zeros(65536, np.uint32), 64) == (65536 - 32, 32)
+    assert stz_b200.run_slots(np.zeros(65536, np.uint32), 1) == (0, 0)
+
+
 def test_codebook_is_optimal_without_length_limit():
     rng = np.random.default_rng(4)
     h = rng.integers(1, 1000, 300).astype(np.uint32)
