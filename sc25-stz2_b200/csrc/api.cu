@@ -345,7 +345,12 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     // work list over every chunk of every stream
     std::vector<CtaWork> work;
     std::vector<uint32_t> ids;
-    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    std::vector<size_t> wbeg(nstreams + 1);  // each stream's range of work items
+    for (int s = 0; s < nstreams; ++s) {
+        wbeg[s] = work.size();
+        add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    }
+    wbeg[nstreams] = work.size();
     // run symbols: slots in unused code values, then the symbol counts of the
     // run-coded planes (one pass over the codes on the GPU)
     bool any_runs = false;
@@ -488,12 +493,6 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
                             ctx->chunk_off.as<uint64_t>(), ctx->stream_words.as<uint64_t>(),
                             ctx->payload.as<uint32_t>(), st);
     }
-    {
-        KScope ks(ctx, "k_encode");
-        launch_encode(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), ctx->ctab.as<uint32_t>(),
-                      ctx->sub_off.as<uint32_t>(), ctx->sub_bits.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
-                      ctx->payload.as<uint32_t>(), st);
-    }
     if (!uwork.empty()) {
         KScope ks(ctx, "k_unpred_move");
         launch_unpred_move<T>(true, d_uw, (int)uwork.size(), d_sd, ctx->codes.as<uint16_t>(),
@@ -501,7 +500,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     STZ_CUDA(cudaGetLastError());
 
-    // tables to the host
+    // stream sizes and tables to the host (the payload is encoded next)
     const size_t t_words = 0, t_choff = align256(t_words + (size_t)nstreams * 8);
     const size_t t_sub = align256(t_choff + g.total_chunk_slots * 8);
     const size_t t_ul = align256(t_sub + g.total_sub * 4), t_bytes = align256(t_ul + total_unpred * elem);
@@ -513,10 +512,10 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     if (total_unpred)
         STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
-    lap.mark("entropy coding + tables");
+    lap.mark("code lengths + tables");
     const uint64_t* words = (const uint64_t*)(ht + t_words);
 
-    // pack payloads contiguously and copy them back
+    // packed payload layout
     std::vector<uint64_t> meta(3 * (size_t)nstreams);
     uint64_t packed_total = 0;
     for (int s = 0; s < nstreams; ++s) {
@@ -525,23 +524,79 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         meta[2 * (size_t)nstreams + s] = words[s];
         packed_total += words[s];
     }
-    STZ_CUDA(ctx->pack_meta.ensure(meta.size() * 8));
-    STZ_CUDA(ctx->h_small.ensure(meta.size() * 8));
-    std::memcpy(ctx->h_small.p, meta.data(), meta.size() * 8);
-    STZ_CUDA(cudaMemcpyAsync(ctx->pack_meta.p, ctx->h_small.p, meta.size() * 8, cudaMemcpyHostToDevice, st));
-    STZ_CUDA(ctx->packed.ensure(std::max<uint64_t>(packed_total, 1) * 4));
-    const uint64_t* pm = ctx->pack_meta.as<uint64_t>();
-    {
-        KScope ks(ctx, "k_pack_payload");
-        launch_pack_payload(ctx->payload.as<uint32_t>(), pm, pm + nstreams, pm + 2 * nstreams, nstreams,
-                            ctx->packed.as<uint32_t>(), st);
-    }
     STZ_CUDA(ctx->h_payload.ensure(std::max<uint64_t>(packed_total, 1) * 4));
-    STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.p, ctx->packed.p, packed_total * 4, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaStreamSynchronize(st));
-    lap.mark("pack + payload copy");
 
-    // container
+    // Encode, pack and copy back in groups: every stream of the coarser
+    // levels, then the finest level's streams two chunk z-layers at a time
+    // (all 7 streams per group, so every launch still fills the device); the
+    // host zstd-compresses a group's frames while the device encodes the next.
+    const int fin0 = std::max(0, nstreams - 7);
+    const int fin_layers = (int)sd[nstreams - 1].ncz;
+    const int lpg = std::max(1, (fin_layers + 3) / 4);  // layers per group
+    const size_t ngroups = 1 + (size_t)((fin_layers + lpg - 1) / lpg);
+    struct Piece {  // a word range of one stream's payload
+        int s;
+        uint64_t w0, w1;  // words from the stream's start
+    };
+    std::vector<std::vector<Piece>> pieces(ngroups);
+    std::vector<CtaWork> gwork;
+    std::vector<uint32_t> gids;
+    std::vector<size_t> gw(ngroups + 1, 0);
+    const uint64_t* choff_h = (const uint64_t*)(ht + t_choff);
+    for (int s = 0; s < fin0; ++s) {
+        add_all_chunks(gwork, gids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+        pieces[0].push_back({s, 0, words[s]});
+    }
+    for (size_t gi = 1; gi < ngroups; ++gi) {
+        gw[gi] = gwork.size();
+        const int L0 = (int)(gi - 1) * lpg, L1 = std::min(fin_layers, L0 + lpg);
+        for (int s = fin0; s < nstreams; ++s) {
+            const uint32_t cpl = sd[s].ncx * sd[s].ncy;
+            std::vector<uint32_t> cs;
+            for (uint32_t c = (uint32_t)L0 * cpl; c < (uint32_t)L1 * cpl; ++c) cs.push_back(c);
+            add_work(gwork, gids, (uint32_t)s, cs.data(), cs.size(), (int)sd[s].C);
+            const uint64_t* co = choff_h + sd[s].chunk_base;
+            pieces[gi].push_back({s, co[(size_t)L0 * cpl], co[(size_t)L1 * cpl]});
+        }
+    }
+    gw[0] = 0;
+    gw[ngroups] = gwork.size();
+    const size_t g_work = 0, g_ids = align256(gwork.size() * sizeof(CtaWork)), g_bytes = align256(g_ids + gids.size() * 4);
+    STZ_CUDA(ctx->h_meta2.ensure(g_bytes));
+    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_work, gwork.data(), gwork.size() * sizeof(CtaWork));
+    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_ids, gids.data(), gids.size() * 4);
+    STZ_CUDA(ctx->gwork.ensure(g_bytes));
+    STZ_CUDA(cudaMemcpyAsync(ctx->gwork.p, ctx->h_meta2.p, g_bytes, cudaMemcpyHostToDevice, st));
+    const CtaWork* d_gwork = (const CtaWork*)(ctx->gwork.as<uint8_t>() + g_work);
+    const uint32_t* d_gids = (const uint32_t*)(ctx->gwork.as<uint8_t>() + g_ids);
+    struct Events {
+        std::vector<cudaEvent_t> e;
+        ~Events()
+        {
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } ev;
+    ev.e.assign(ngroups, nullptr);
+    for (auto& x : ev.e) STZ_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    for (size_t gi = 0; gi < ngroups; ++gi) {
+        {
+            KScope ks(ctx, "k_encode");
+            launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
+                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->sub_bits.as<uint32_t>(),
+                          ctx->chunk_off.as<uint64_t>(), ctx->payload.as<uint32_t>(), st);
+        }
+        // the group's words straight from the stream buffers to their place in
+        // the packed host payload (one copy per piece)
+        for (const Piece& pc : pieces[gi])
+            if (pc.w1 > pc.w0)
+                STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.as<uint32_t>() + meta[nstreams + pc.s] + pc.w0,
+                                         ctx->payload.as<uint32_t>() + sd[pc.s].word_base + pc.w0,
+                                         (pc.w1 - pc.w0) * 4, cudaMemcpyDeviceToHost, st));
+        STZ_CUDA(cudaEventRecord(ev.e[gi], st));
+    }
+    STZ_CUDA(cudaGetLastError());
+
+    // container: stream headers from the tables while the device encodes
     FileHeader h;
     h.dtype = sizeof(T) == 8 ? 1 : 0;
     h.predictor = o.predictor;
@@ -573,10 +628,24 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         p.layers = (int)d.ncz;
         p.chunks_per_layer = (int)(d.ncx * d.ncy);
     });
+    lap.mark("stream headers");
+    ContainerWriter cw(h, parts, *ctx->pool);
+    std::atomic<int> ev_err{0};
+    cw.compress_groups(
+        ngroups,
+        [&](size_t st_, int layer) -> size_t {
+            if ((int)st_ < fin0 || layer < 0) return 0;  // coarser levels and every header: group 0
+            return 1 + (size_t)(layer / lpg);
+        },
+        [&](size_t gi) {
+            if (cudaEventSynchronize(ev.e[gi]) != cudaSuccess) ev_err = 1;
+        });
+    if (ev_err) STZ_CUDA(cudaStreamSynchronize(st));  // reports the device error
+    lap.mark("encode + copy + zstd");
     auto* so = new (std::nothrow) stz_stream();
     if (!so) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
-    so->bytes = write_container(h, coarsest.data(), levels, parts, *ctx->pool);
-    lap.mark("zstd frames + container");
+    so->bytes = cw.finish(coarsest.data(), levels);
+    lap.mark("container");
     so->raw_payload_bytes = packed_total * 4;
     const std::string pe = parse_stream(so->bytes.data(), so->bytes.size(), so->dir);
     if (!pe.empty()) {

@@ -6,7 +6,9 @@
 #include <chrono>
 #include <cstdio>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <functional>
 #include <memory>
 #include <numeric>
@@ -265,6 +267,70 @@ std::string validate_dims(long long nx, long long ny, long long nz, int chunk_hi
     return "";
 }
 
+namespace {
+struct BlockPool {
+    std::mutex mu;
+    std::vector<std::pair<void*, size_t>> free_;  // (block, capacity)
+    size_t bytes = 0;
+};
+BlockPool& block_pool()
+{
+    static BlockPool* p = new BlockPool();  // never destroyed: frees may come from static destructors
+    return *p;
+}
+// blocks below this size use malloc directly
+constexpr size_t kPoolMin = (size_t)1 << 20;
+constexpr size_t kPoolMaxBlocks = 4;
+constexpr size_t kPoolMaxBytes = (size_t)2 << 30;
+// header before each pooled block: its capacity (16 bytes keeps alignment)
+constexpr size_t kPoolHdr = 16;
+}  // namespace
+
+void* pooled_alloc(size_t bytes)
+{
+    if (bytes < kPoolMin) return std::malloc(bytes ? bytes : 1);
+    BlockPool& bp = block_pool();
+    {
+        std::lock_guard<std::mutex> lk(bp.mu);
+        size_t best = SIZE_MAX;
+        for (size_t i = 0; i < bp.free_.size(); ++i) {
+            const size_t cap = bp.free_[i].second;
+            if (cap >= bytes && cap <= 2 * bytes + kPoolMin && (best == SIZE_MAX || cap < bp.free_[best].second)) best = i;
+        }
+        if (best != SIZE_MAX) {
+            void* blk = bp.free_[best].first;
+            bp.bytes -= bp.free_[best].second;
+            bp.free_.erase(bp.free_.begin() + (long)best);
+            return static_cast<uint8_t*>(blk) + kPoolHdr;
+        }
+    }
+    void* blk = std::malloc(bytes + kPoolHdr);
+    if (!blk) return nullptr;
+    *static_cast<size_t*>(blk) = bytes;
+    return static_cast<uint8_t*>(blk) + kPoolHdr;
+}
+
+void pooled_free(void* p, size_t bytes)
+{
+    if (!p) return;
+    if (bytes < kPoolMin) {
+        std::free(p);
+        return;
+    }
+    void* blk = static_cast<uint8_t*>(p) - kPoolHdr;
+    const size_t cap = *static_cast<size_t*>(blk);
+    BlockPool& bp = block_pool();
+    {
+        std::lock_guard<std::mutex> lk(bp.mu);
+        if (bp.free_.size() < kPoolMaxBlocks && bp.bytes + cap <= kPoolMaxBytes) {
+            bp.free_.push_back({blk, cap});
+            bp.bytes += cap;
+            return;
+        }
+    }
+    std::free(blk);
+}
+
 int run_slots(const std::function<uint64_t(uint32_t)>& count, int nbins, int plane, uint32_t& run_base)
 {
     const int J = (int)run_slot_count((uint32_t)plane);
@@ -464,39 +530,53 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     return "";
 }
 
-Bytes write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
-                      std::vector<StreamParts>& parts, ThreadPool& pool)
+ContainerWriter::ContainerWriter(const FileHeader& h, std::vector<StreamParts>& parts, ThreadPool& pool)
+    : h_(h), parts_(parts), pool_(pool)
 {
-    // Frame list: per stream its header, then one frame per chunk z-layer.
-    struct Frame {
-        const uint8_t* src;
-        size_t n;
-        std::unique_ptr<uint8_t[]> out;
-        size_t stored = 0;
-        bool raw = true;
-        const uint8_t* bytes() const { return raw ? src : out.get(); }
-    };
-    std::vector<Frame> frames;
-    std::vector<size_t> first(parts.size());
+    // per stream its header, then one frame per chunk z-layer
+    first_.resize(parts.size() + 1);
     for (size_t i = 0; i < parts.size(); ++i) {
-        first[i] = frames.size();
-        frames.push_back({parts[i].hdr.data(), parts[i].hdr.size(), nullptr});
+        first_[i] = frames_.size();
+        frames_.push_back({parts[i].hdr.data(), parts[i].hdr.size()});
         for (int L = 0; L < parts[i].layers; ++L) {
             const uint64_t w0 = parts[i].chunk_word_off[(size_t)L * parts[i].chunks_per_layer];
             const uint64_t w1 = parts[i].chunk_word_off[(size_t)(L + 1) * parts[i].chunks_per_layer];
-            frames.push_back({(const uint8_t*)(parts[i].words + w0), (size_t)(4 * (w1 - w0)), nullptr});
+            frames_.push_back({(const uint8_t*)(parts[i].words + w0), (size_t)(4 * (w1 - w0))});
         }
     }
-    // largest frames first, so the pool's tail is short
-    std::vector<size_t> order(frames.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return frames[a].n > frames[b].n; });
-    const int level = h.zstd_level;
-    Lap lap("container");
-    std::atomic<int64_t> busy_ns{0};
-    pool.parallel_for(frames.size(), [&](size_t k) {
-        const auto t0 = std::chrono::steady_clock::now();
-        Frame& f = frames[order[k]];
+    first_[parts.size()] = frames_.size();
+}
+
+void ContainerWriter::compress_streams(size_t s0, size_t s1)
+{
+    compress_groups(1, [&](size_t s, int) -> size_t { return s >= s0 && s < s1 ? 0 : SIZE_MAX; }, [](size_t) {});
+}
+
+void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t(size_t, int)>& group_of_frame,
+                                      const std::function<void(size_t)>& wait_group)
+{
+    // group by group, largest frames first inside a group: the pool's threads
+    // move on to the next group's frames as soon as its bytes are ready
+    std::vector<std::vector<size_t>> by_group(ngroups);
+    for (size_t st = 0; st + 1 < first_.size(); ++st)
+        for (size_t i = first_[st]; i < first_[st + 1]; ++i) {
+            const size_t gi = group_of_frame(st, (int)(i - first_[st]) - 1);
+            if (gi < ngroups) by_group[gi].push_back(i);
+        }
+    std::vector<size_t> order, group_of;
+    for (size_t gi = 0; gi < ngroups; ++gi) {
+        auto& v = by_group[gi];
+        std::sort(v.begin(), v.end(), [&](size_t a, size_t c) { return frames_[a].n > frames_[c].n; });
+        order.insert(order.end(), v.begin(), v.end());
+        group_of.resize(order.size(), gi);
+    }
+    const int level = h_.zstd_level;
+    const bool trace = std::getenv("STZ_TRACE") != nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    pool_.parallel_for(order.size(), [&](size_t k) {
+        wait_group(group_of[k]);
+        const auto f0 = std::chrono::steady_clock::now();
+        Frame& f = frames_[order[k]];
         f.raw = true;
         f.stored = f.n;
         if (level > 0 && f.n > 0) {
@@ -510,17 +590,25 @@ Bytes write_container(const FileHeader& h, const void* coarsest, const std::vect
                 f.out.reset();
             }
         }
-        if (lap.on)
-            busy_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0)
-                           .count();
+        if (trace)
+            busy_ns_ += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - f0)
+                            .count();
     });
-    if (lap.on) {
+    if (trace)
+        wall_ns_ += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
+}
+
+Bytes ContainerWriter::finish(const void* coarsest, const std::vector<LevelDir>& levels)
+{
+    const FileHeader& h = h_;
+    if (std::getenv("STZ_TRACE")) {
         size_t raw = 0, mx = 0;
-        for (const Frame& f : frames) raw += f.n, mx = std::max(mx, f.n);
-        std::fprintf(stderr, "[stz] container: %zu frames, %.2f MB raw, largest %.3f MB, zstd busy %.3f ms on %d threads\n",
-                     frames.size(), raw / 1e6, mx / 1e6, busy_ns.load() / 1e6, pool.size());
+        for (const Frame& f : frames_) raw += f.n, mx = std::max(mx, f.n);
+        std::fprintf(stderr, "[stz] container: %zu frames, %.2f MB raw, largest %.3f MB, zstd busy %.3f ms on %d "
+                             "threads, %.3f ms in zstd calls\n",
+                     frames_.size(), raw / 1e6, mx / 1e6, busy_ns_.load() / 1e6, pool_.size(), wall_ns_ / 1e6);
     }
-    lap.mark("zstd frames");
+    Lap lap("container");
     std::vector<uint8_t> dir;
     Writer w{dir};
     w.put(kMagic, 8);
@@ -554,30 +642,37 @@ Bytes write_container(const FileHeader& h, const void* coarsest, const std::vect
         w.u32(L.lflags);
         if (L.lflags) w.put(&L.model, sizeof(LearnedModel));
         for (int b = 0; b < 7; ++b, ++si) {
-            const StreamParts& p = parts[si];
+            const StreamParts& p = parts_[si];
             w.u32((uint32_t)p.layers);
-            const Frame& hf = frames[first[si]];
+            const Frame& hf = frames_[first_[si]];
             w.u64(hf.stored);
             w.u64(hf.n);
-            for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames[first[si] + 1 + L2].stored);
-            for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames[first[si] + 1 + L2].n);
+            for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames_[first_[si] + 1 + L2].stored);
+            for (int L2 = 0; L2 < p.layers; ++L2) w.u64(frames_[first_[si] + 1 + L2].n);
         }
     }
-    // the directory, then the frames in order, copied in parallel into an
-    // uninitialized buffer
-    std::vector<size_t> off(frames.size() + 1);
+    // the directory, then the frames in order, copied in parallel
+    std::vector<size_t> off(frames_.size() + 1);
     off[0] = dir.size();
-    for (size_t i = 0; i < frames.size(); ++i) off[i + 1] = off[i] + frames[i].stored;
+    for (size_t i = 0; i < frames_.size(); ++i) off[i + 1] = off[i] + frames_[i].stored;
     Bytes out;
     out.resize(off.back());
     std::memcpy(out.data(), dir.data(), dir.size());
     lap.mark("directory");
     uint8_t* base = out.data();
-    pool.parallel_for(frames.size(), [&](size_t i) {
-        if (frames[i].stored) std::memcpy(base + off[i], frames[i].bytes(), frames[i].stored);
+    pool_.parallel_for(frames_.size(), [&](size_t i) {
+        if (frames_[i].stored) std::memcpy(base + off[i], frames_[i].bytes(), frames_[i].stored);
     });
     lap.mark("frame copy");
     return out;
+}
+
+Bytes write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
+                      std::vector<StreamParts>& parts, ThreadPool& pool)
+{
+    ContainerWriter w(h, parts, pool);
+    w.compress_streams(0, parts.size());
+    return w.finish(coarsest, levels);
 }
 
 // ---- ROI planner ------------------------------------------------------------------

@@ -2,6 +2,7 @@
 // stream container, the ROI planner and a small thread pool for zstd.
 #pragma once
 #include <array>
+#include <atomic>
 #include <condition_variable>
 #include <cstddef>
 #include <cstdint>
@@ -19,6 +20,12 @@ namespace stz {
 // Byte buffer whose resize leaves new bytes uninitialized (the container is
 // written in parallel right after; zero-filling first costs a single-threaded
 // pass over fresh pages).
+// Large byte blocks come from a small process-wide pool of recently freed
+// blocks (their pages stay mapped, so writing a new container does not fault
+// and zero fresh pages); the pool keeps at most 4 blocks and 2 GiB.
+void* pooled_alloc(size_t bytes);
+void pooled_free(void* p, size_t bytes);
+
 template <class T>
 struct DefaultInitAlloc : std::allocator<T> {
     template <class U>
@@ -30,6 +37,13 @@ struct DefaultInitAlloc : std::allocator<T> {
     DefaultInitAlloc(const DefaultInitAlloc<U>&) noexcept
     {
     }
+    T* allocate(size_t n)
+    {
+        void* p = pooled_alloc(n * sizeof(T));
+        if (!p) throw std::bad_alloc();
+        return static_cast<T*>(p);
+    }
+    void deallocate(T* p, size_t n) noexcept { pooled_free(p, n * sizeof(T)); }
     template <class U>
     void construct(U* p) noexcept
     {
@@ -157,8 +171,42 @@ void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const 
                           const uint32_t* unpred_count, const uint64_t* chunk_word_off, const uint32_t* sub_off,
                           int nchunks, int C);
 
-// Assemble the container: directory, coarsest grid, then every frame
-// (zstd-compressed in parallel on the pool).
+// The container in stages: the frame list of every stream (its header, one
+// frame per chunk z-layer of payload), zstd of the frames of a range of
+// streams on the pool (as soon as their bytes are on the host), then the
+// directory, the coarsest grid and every frame. `parts` stays alive and
+// unchanged until finish.
+class ContainerWriter {
+public:
+    ContainerWriter(const FileHeader& h, std::vector<StreamParts>& parts, ThreadPool& pool);
+    void compress_streams(size_t s0, size_t s1);
+    // The frames in group order on the pool: group_of_frame(stream, layer)
+    // (layer -1: the stream's header frame) gives a frame's group in
+    // [0, ngroups) (anything else: not compressed by this call); a thread
+    // calls wait_group(g) before each frame of group g.
+    void compress_groups(size_t ngroups, const std::function<size_t(size_t, int)>& group_of_frame,
+                         const std::function<void(size_t)>& wait_group);
+    Bytes finish(const void* coarsest, const std::vector<LevelDir>& levels);
+
+private:
+    struct Frame {
+        const uint8_t* src;
+        size_t n;
+        std::unique_ptr<uint8_t[]> out;
+        size_t stored = 0;
+        bool raw = true;
+        const uint8_t* bytes() const { return raw ? src : out.get(); }
+    };
+    FileHeader h_;
+    std::vector<StreamParts>& parts_;
+    ThreadPool& pool_;
+    std::vector<Frame> frames_;
+    std::vector<size_t> first_;  // first frame of each stream (+ end)
+    std::atomic<int64_t> busy_ns_{0};
+    int64_t wall_ns_ = 0;
+};
+
+// All stages at once.
 Bytes write_container(const FileHeader& h, const void* coarsest, const std::vector<LevelDir>& levels,
                       std::vector<StreamParts>& parts, ThreadPool& pool);
 
