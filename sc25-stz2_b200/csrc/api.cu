@@ -582,8 +582,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         {
             KScope ks(ctx, "k_encode");
             launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
-                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->sub_bits.as<uint32_t>(),
-                          ctx->chunk_off.as<uint64_t>(), ctx->payload.as<uint32_t>(), st);
+                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
+                          ctx->payload.as<uint32_t>(), st);
         }
         // the group's words straight from the stream buffers to their place in
         // the packed host payload (one copy per piece)

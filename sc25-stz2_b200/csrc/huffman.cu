@@ -62,62 +62,191 @@ __global__ void k_expand_codebook(const StreamDesc* __restrict__ sd, const uint1
     }
 }
 
-// Symbols of one plane with runs: f(sym) for each, in order.
+// ---- encode side: one warp per plane -----------------------------------------
+// Lane i of a warp owns the codes [a_i, b_i) of the plane (32 consecutive
+// segments of S = ceil(plane / 32) codes). A run of centre codes is coded by
+// the lane holding the literal that follows it, or, for a run that reaches
+// the plane's end, by the lane holding the plane's last code (`tail`): a
+// warp max-scan of the lanes' last literal positions gives every lane the
+// centre codes just before its segment (`lead`), which belong to the run
+// leading into its first literal. The lanes' bit counts, an exclusive warp
+// scan of them and the plane's bit offset place every lane's bits, so the
+// bitstream is the one a sequential pass over the plane writes.
+constexpr int kLaneThreads = 256;  // 8 warps per CTA, each one plane at a time
+constexpr int kPlaneSlices = 4;    // CTAs per work item (gridDim.y)
+
+// Symbols of a run of r centre codes (none for r = 0), in order: while
+// r > D, 2^k (the largest power of two <= r, k <= J) when k > LD, else D
+// codes; then the symbol of the remaining 2..D codes, or the centre code.
 template <class F>
-__device__ __forceinline__ void plane_symbols(const uint16_t* __restrict__ src, size_t plane, const StreamDesc& s,
-                                              F&& f)
+__device__ __forceinline__ void run_symbols(uint32_t r, uint32_t R, uint32_t base, uint32_t J, uint32_t D, uint32_t LD,
+                                            F&& f)
 {
-    const uint32_t R = s.radius, base = s.run_base;
-    uint32_t D, LD;
-    const uint32_t J = run_geometry((uint32_t)plane, D, LD);
-    uint32_t run = 0;
-    auto flush = [&]() {
-        while (run > D) {
-            const uint32_t k = min((uint32_t)(31 - __clz(run)), J);
-            if (k > LD) {
-                f(base + D - 1 + (k - LD - 1));
-                run -= 1u << k;
-            } else {
-                f(base + D - 2);
-                run -= D;
-            }
-        }
-        if (run >= 2) f(base + run - 2);
-        else if (run) f(R);
-        run = 0;
-    };
-    auto feed = [&](uint32_t q) {
-        if (q == R) {
-            ++run;
+    while (r > D) {
+        const uint32_t k = min((uint32_t)(31 - __clz(r)), J);
+        if (k > LD) {
+            f(base + D - 1 + (k - LD - 1));
+            r -= 1u << k;
         } else {
-            if (run) flush();
-            f(q);
+            f(base + D - 2);
+            r -= D;
         }
-    };
-    if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
-        const uint4* v = reinterpret_cast<const uint4*>(src);
-        const uint32_t R2 = R | (R << 16);
-        for (size_t j = 0; j < plane / 8; ++j) {
-            const uint4 q = __ldg(v + j);
-            if (((q.x ^ R2) | (q.y ^ R2) | (q.z ^ R2) | (q.w ^ R2)) == 0) {  // 8 centre codes
-                run += 8;
-                continue;
-            }
-            feed(q.x & 0xffffu), feed(q.x >> 16), feed(q.y & 0xffffu), feed(q.y >> 16);
-            feed(q.z & 0xffffu), feed(q.z >> 16), feed(q.w & 0xffffu), feed(q.w >> 16);
-        }
-    } else {
-        for (size_t j = 0; j < plane; ++j) feed(__ldg(src + j));
     }
-    if (run) flush();
+    if (r >= 2) f(base + r - 2);
+    else if (r) f(R);
 }
 
+// A warp's view of one plane.
+struct LaneSeg {
+    uint32_t P, a, b;  // plane size; this lane's codes [a, b)
+    bool vec;          // segments are whole 16-byte groups of 8 codes
+};
+
+__device__ __forceinline__ LaneSeg lane_seg(uint32_t C, const uint16_t* src)
+{
+    LaneSeg g;
+    g.P = C * C;
+    const uint32_t S = (g.P + 31) / 32, lane = threadIdx.x & 31;
+    g.a = min(lane * S, g.P);
+    g.b = min(g.a + S, g.P);
+    g.vec = g.P % 256 == 0 && ((uintptr_t)src & 15) == 0;
+    return g;
+}
+
+// The lane's codes in order (streams without runs): f(q) for each.
+template <class G>
+__device__ __forceinline__ void lane_codes(const uint16_t* __restrict__ src, const LaneSeg& g, G&& f)
+{
+    if (g.vec) {
+        const uint4* v = reinterpret_cast<const uint4*>(src + g.a);
+        for (uint32_t j = 0; j < (g.b - g.a) / 8; ++j) {
+            const uint4 q = __ldg(v + j);
+            f(q.x & 0xffffu), f(q.x >> 16), f(q.y & 0xffffu), f(q.y >> 16);
+            f(q.z & 0xffffu), f(q.z >> 16), f(q.w & 0xffffu), f(q.w >> 16);
+        }
+    } else {
+        for (uint32_t j = g.a; j < g.b; ++j) f(__ldg(src + j));
+    }
+}
+
+// Bits 0 and 1 set for the 16-bit halves of w equal to those of R2.
+__device__ __forceinline__ uint32_t pair_mask(uint32_t w, uint32_t R2)
+{
+    const uint32_t e = __vcmpeq2(w, R2);  // 0xffff per equal half
+    return (e & 1u) | ((e >> 15) & 2u);
+}
+
+// Literal mask of the n <= 32 codes at plane position p: bit i set when code
+// p + i is not the centre code R (with g.vec, p and n are multiples of 8).
+__device__ __forceinline__ uint32_t literal_mask(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t p,
+                                                 uint32_t n, uint32_t R)
+{
+    uint32_t m = 0;  // centre codes
+    if (g.vec) {
+        const uint4* v = reinterpret_cast<const uint4*>(src + p);
+        const uint32_t R2 = R | (R << 16);
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+            if (j < n / 8) {
+                const uint4 q = __ldg(v + j);
+                m |= (pair_mask(q.x, R2) | pair_mask(q.y, R2) << 2 | pair_mask(q.z, R2) << 4 |
+                      pair_mask(q.w, R2) << 6)
+                     << (8 * j);
+            }
+    } else {
+        for (uint32_t i = 0; i < n; ++i) m |= (uint32_t)(__ldg(src + p + i) == R) << i;
+    }
+    return ~m & (n == 32 ? ~0u : (1u << n) - 1);
+}
+
+// A lane's plane segment with runs, as 32-code blocks: the literal mask of
+// the first block is kept (most segments are one block), later ones are
+// rebuilt on each pass.
+struct RunLane {
+    uint32_t lit0 = 0;  // literal mask of the block at a
+    uint32_t lead = 0;  // centre codes between the last literal before a and a
+    bool tail = false;  // the lane holds the plane's last code
+
+    template <class F>
+    __device__ __forceinline__ void blocks(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t R, F&& fn) const
+    {
+        for (uint32_t p = g.a; p < g.b; p += 32) {
+            const uint32_t n = min(32u, g.b - p);
+            fn(p, n, p == g.a ? lit0 : literal_mask(src, g, p, n, R));
+        }
+    }
+
+    // Literal masks, then a warp max-scan of the lanes' last literal
+    // positions for lead.
+    __device__ __forceinline__ void init(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t R)
+    {
+        uint32_t last = 0;  // last literal + 1 (0: none)
+        for (uint32_t p = g.a; p < g.b; p += 32) {
+            const uint32_t n = min(32u, g.b - p);
+            const uint32_t lit = literal_mask(src, g, p, n, R);
+            if (p == g.a) lit0 = lit;
+            if (lit) last = p + 32 - __clz(lit);
+        }
+        const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, last, o);
+            if (lane >= (uint32_t)o) last = max(last, v);
+        }
+        uint32_t excl = __shfl_up_sync(0xffffffffu, last, 1);
+        if (lane == 0) excl = 0;
+        lead = g.a - excl;
+        tail = g.a < g.b && g.b == g.P;
+    }
+
+    // The lane's symbols in order: f(sym). Between consecutive literals of a
+    // block every code is a centre code, so the runs are the gaps.
+    template <class F>
+    __device__ __forceinline__ void symbols(const uint16_t* __restrict__ src, const LaneSeg& g, const StreamDesc& s,
+                                            F&& f) const
+    {
+        uint32_t D, LD;
+        const uint32_t J = run_geometry(g.P, D, LD);
+        uint32_t run = lead;
+        blocks(src, g, s.radius, [&](uint32_t p, uint32_t n, uint32_t lit) {
+            uint32_t i = 0;
+            while (lit) {
+                const uint32_t j = __ffs(lit) - 1;
+                run += j - i;
+                if (run) {
+                    run_symbols(run, s.radius, s.run_base, J, D, LD, f);
+                    run = 0;
+                }
+                f((uint32_t)__ldg(src + p + j));
+                i = j + 1;
+                lit &= lit - 1;
+            }
+            run += n - i;
+        });
+        if (tail && run) run_symbols(run, s.radius, s.run_base, J, D, LD, f);
+    }
+};
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Planes of a work item for this warp: CTA (x, y) of a grid with gridDim.y
+// slices takes every (8 * gridDim.y)-th plane, so short lists still spread
+// over many warps.
+#define STZ_WARP_PLANES(p, nplanes)                                                              \
+    for (uint32_t p = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5); p < (nplanes); \
+         p += (blockDim.x >> 5) * gridDim.y)
+
 // Run-symbol counts of every listed plane (streams with runs).
-__global__ void __launch_bounds__(kCoderThreads) k_run_stats(const CtaWork* __restrict__ work,
-                                                             const uint32_t* __restrict__ chunk_ids,
-                                                             const StreamDesc* __restrict__ sd,
-                                                             const uint16_t* __restrict__ codes,
-                                                             unsigned long long* __restrict__ stats)
+__global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __restrict__ work,
+                                                            const uint32_t* __restrict__ chunk_ids,
+                                                            const StreamDesc* __restrict__ sd,
+                                                            const uint16_t* __restrict__ codes,
+                                                            unsigned long long* __restrict__ stats)
 {
     __shared__ uint32_t cnt[kRunStats];
     const CtaWork w = work[blockIdx.x];
@@ -125,57 +254,56 @@ __global__ void __launch_bounds__(kCoderThreads) k_run_stats(const CtaWork* __re
     if (s.run_n == 0) return;  // uniform per block
     if (threadIdx.x < kRunStats) cnt[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t C = s.C, t = threadIdx.x;
-    if (t / C < w.count) {
-        const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
-        const size_t plane = (size_t)C * C;
-        const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
-        uint32_t singles = 0;
-        plane_symbols(src, plane, s, [&](uint32_t sym) {
+    const uint32_t C = s.C, P = C * C;
+    uint32_t singles = 0;
+    STZ_WARP_PLANES(p, w.count * C)
+    {
+        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src);
+        RunLane rl;
+        rl.init(src, g, s.radius);
+        rl.symbols(src, g, s, [&](uint32_t sym) {
             if (sym == s.radius) ++singles;
             else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
         });
-        if (singles) atomicAdd(&cnt[0], singles);
     }
+    singles = warp_sum(singles);
+    if ((threadIdx.x & 31) == 0 && singles) atomicAdd(&cnt[0], singles);
     __syncthreads();
     if (threadIdx.x < kRunStats && cnt[threadIdx.x])
         atomicAdd(&stats[(size_t)w.stream * kRunStats + threadIdx.x], cnt[threadIdx.x]);
 }
 
-// Bits of every sub-chunk.
-__global__ void __launch_bounds__(kCoderThreads) k_sub_bits(const CtaWork* __restrict__ work,
-                                                            const uint32_t* __restrict__ chunk_ids,
-                                                            const StreamDesc* __restrict__ sd,
-                                                            const uint16_t* __restrict__ codes,
-                                                            const uint32_t* __restrict__ ctab,
-                                                            uint32_t* __restrict__ sub_bits)
+// Bits of every plane.
+__global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __restrict__ work,
+                                                           const uint32_t* __restrict__ chunk_ids,
+                                                           const StreamDesc* __restrict__ sd,
+                                                           const uint16_t* __restrict__ codes,
+                                                           const uint32_t* __restrict__ ctab,
+                                                           uint32_t* __restrict__ sub_bits)
 {
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
-    const uint32_t C = s.C;
-    const uint32_t t = threadIdx.x;
-    if (t / C >= w.count) return;
-    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
-    const size_t plane = (size_t)C * C;
-    const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+    const uint32_t C = s.C, P = C * C;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
-    uint32_t bits = 0;
-    if (s.run_n) {
-        plane_symbols(src, plane, s, [&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; });
-    } else if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
-        // 8 codes per 16-byte load: one request per lane instead of eight
-        const uint4* v = reinterpret_cast<const uint4*>(src);
-        for (size_t j = 0; j < plane / 8; ++j) {
-            const uint4 q = __ldg(v + j);
-            const uint32_t u[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                bits += (__ldg(tab + (u[k] & 0xffffu)) & 31u) + (__ldg(tab + (u[k] >> 16)) & 31u);
+    STZ_WARP_PLANES(p, w.count * C)
+    {
+        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src);
+        uint32_t bits = 0;
+        auto add = [&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; };
+        if (s.run_n) {
+            RunLane rl;
+            rl.init(src, g, s.radius);
+            rl.symbols(src, g, s, add);
+        } else {
+            lane_codes(src, g, add);
         }
-    } else {
-        for (size_t j = 0; j < plane; ++j) bits += __ldg(tab + __ldg(src + j)) & 31u;
+        bits = warp_sum(bits);
+        if ((threadIdx.x & 31) == 0) sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
     }
-    sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
 }
 
 // Per stream: plane bit offsets inside each chunk, chunk word offsets (the
@@ -245,63 +373,73 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
     }
 }
 
-// Encode: each thread packs one plane MSB-first. Words shared with a
-// neighbouring plane (its first and last) are merged with atomicOr; words in
-// between belong to this plane alone and are stored directly.
-__global__ void __launch_bounds__(kCoderThreads) k_encode(const CtaWork* __restrict__ work,
-                                                          const uint32_t* __restrict__ chunk_ids,
-                                                          const StreamDesc* __restrict__ sd,
-                                                          const uint16_t* __restrict__ codes,
-                                                          const uint32_t* __restrict__ ctab,
-                                                          const uint32_t* __restrict__ sub_off,
-                                                          const uint32_t* __restrict__ sub_bits,
-                                                          const uint64_t* __restrict__ chunk_word_off,
-                                                          uint32_t* __restrict__ payload)
+// Encode: a warp packs one plane MSB-first, each lane its own bits from the
+// plane's offset plus the bits of the lanes before it. The plane's first and
+// last words (shared with its neighbours, cleared by k_scan_stream) and each
+// lane's first and last words are merged with atomicOr; the warp clears the
+// plane's inner words first, and words inside one lane's range are stored.
+__global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restrict__ work,
+                                                         const uint32_t* __restrict__ chunk_ids,
+                                                         const StreamDesc* __restrict__ sd,
+                                                         const uint16_t* __restrict__ codes,
+                                                         const uint32_t* __restrict__ ctab,
+                                                         const uint32_t* __restrict__ sub_off,
+                                                         const uint64_t* __restrict__ chunk_word_off,
+                                                         uint32_t* __restrict__ payload)
 {
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
-    const uint32_t C = s.C;
-    const uint32_t t = threadIdx.x;
-    if (t / C >= w.count) return;
-    const uint32_t c = chunk_ids[w.first + t / C], lz = t % C;
-    const size_t k = s.sub_base + (size_t)c * C + lz;
-    const uint32_t nb = sub_bits[k];
-    if (nb == 0) return;
-    const size_t plane = (size_t)C * C;
-    const uint16_t* src = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
+    const uint32_t C = s.C, P = C * C, lane = threadIdx.x & 31;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
-    uint32_t* out = payload + s.word_base + chunk_word_off[s.chunk_base + c];
-    const uint32_t b0 = sub_off[k];
-    const uint32_t first_w = b0 >> 5, last_w = (b0 + nb - 1) >> 5;
-    uint32_t wi = first_w;
-    uint64_t acc = 0;      // pending bits, right-aligned
-    int nacc = b0 & 31;    // leading bits of the first word belong to the previous plane (zeros here)
-    auto put = [&](uint32_t code) {
-        const uint32_t e = __ldg(tab + code);
-        const int l = e & 31;
-        acc = (acc << l) | (e >> 5);
-        nacc += l;
-        if (nacc >= 32) {
-            const uint32_t word = (uint32_t)(acc >> (nacc - 32));
-            nacc -= 32;
-            if (wi == first_w || wi == last_w) atomicOr(out + wi, word);
-            else out[wi] = word;
-            ++wi;
+    STZ_WARP_PLANES(p, w.count * C)
+    {
+        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src);
+        RunLane rl;
+        if (s.run_n) rl.init(src, g, s.radius);
+        auto each = [&](auto&& f) {
+            if (s.run_n) rl.symbols(src, g, s, f);
+            else lane_codes(src, g, f);
+        };
+        uint32_t bits = 0;
+        each([&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; });
+        uint32_t off = bits;  // inclusive scan -> this lane's first bit in the plane
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= (uint32_t)o) off += v;
         }
-    };
-    if (s.run_n) {
-        plane_symbols(src, plane, s, put);
-    } else if (plane % 8 == 0 && ((uintptr_t)src & 15) == 0) {
-        const uint4* v = reinterpret_cast<const uint4*>(src);
-        for (size_t j = 0; j < plane / 8; ++j) {
-            const uint4 q = __ldg(v + j);
-            put(q.x & 0xffffu), put(q.x >> 16), put(q.y & 0xffffu), put(q.y >> 16);
-            put(q.z & 0xffffu), put(q.z >> 16), put(q.w & 0xffffu), put(q.w >> 16);
+        const uint32_t nb = __shfl_sync(0xffffffffu, off, 31);
+        off -= bits;
+        if (nb == 0) continue;  // uniform per warp
+        uint32_t* out = payload + s.word_base + chunk_word_off[s.chunk_base + c];
+        const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
+        for (uint32_t x = (b0 >> 5) + 1 + lane; x < (b0 + nb - 1) >> 5; x += 32) out[x] = 0;
+        __syncwarp();
+        if (bits) {
+            const uint32_t pos = b0 + off;
+            const uint32_t first_w = pos >> 5, last_w = (pos + bits - 1) >> 5;
+            uint32_t wi = first_w;
+            uint64_t acc = 0;            // pending bits, right-aligned
+            int nacc = (int)(pos & 31);  // leading bits of the first word belong to earlier lanes (zeros here)
+            each([&](uint32_t sym) {
+                const uint32_t e = __ldg(tab + sym);
+                const int l = e & 31;
+                acc = (acc << l) | (e >> 5);
+                nacc += l;
+                if (nacc >= 32) {
+                    const uint32_t word = (uint32_t)(acc >> (nacc - 32));
+                    nacc -= 32;
+                    if (wi == first_w || wi == last_w) atomicOr(out + wi, word);
+                    else out[wi] = word;
+                    ++wi;
+                }
+            });
+            if (nacc > 0) atomicOr(out + wi, (uint32_t)(acc << (32 - nacc)));
         }
-    } else {
-        for (size_t j = 0; j < plane; ++j) put(__ldg(src + j));
+        __syncwarp();
     }
-    if (nacc > 0) atomicOr(out + wi, (uint32_t)(acc << (32 - nacc)));
 }
 
 // Decode: each thread decodes one plane with a 2^kLutBits-entry table in
@@ -479,6 +617,14 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
             uint64_t s0 = 0, s1 = 0;
             uint32_t ns = 0;
             auto low = [](uint32_t b) -> uint64_t { return b >= 64 ? ~0ull : (1ull << b) - 1; };
+            auto flush = [&]() {
+                if (ns == 8) {
+                    d4[(j >> 3) - 1] =
+                        make_uint4((uint32_t)s0, (uint32_t)(s0 >> 32), (uint32_t)s1, (uint32_t)(s1 >> 32));
+                    s0 = s1 = 0;
+                    ns = 0;
+                }
+            };
             auto put = [&](uint32_t v, uint32_t n) {  // n <= 8 - ns copies of v
                 const uint64_t p = (uint64_t)(v | (v << 16)) * 0x0000000100000001ull;
                 const uint32_t a = 16 * ns, b = 16 * (ns + n);
@@ -486,12 +632,14 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
                 s1 |= p & (low(b > 64 ? b - 64 : 0) & ~low(a > 64 ? a - 64 : 0));
                 ns += n;
                 j += n;
-                if (ns == 8) {
-                    d4[(j >> 3) - 1] =
-                        make_uint4((uint32_t)s0, (uint32_t)(s0 >> 32), (uint32_t)s1, (uint32_t)(s1 >> 32));
-                    s0 = s1 = 0;
-                    ns = 0;
-                }
+                flush();
+            };
+            auto put1 = [&](uint32_t v) {  // one code: a shift into its slot
+                if (ns < 4) s0 |= (uint64_t)v << (16 * ns);
+                else s1 |= (uint64_t)v << (16 * (ns - 4));
+                ++ns;
+                ++j;
+                flush();
             };
             const uint32_t r2 = R | (R << 16);
             const uint4 rr = make_uint4(r2, r2, r2, r2);
@@ -507,7 +655,7 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
                     for (; n >= 8; n -= 8, j += 8) d4[j >> 3] = rr;
                     if (n) put(R, n);
                 } else {
-                    put(sym, 1);
+                    put1(sym);
                 }
             }
         } else {
@@ -700,13 +848,13 @@ void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* 
 void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                       const uint16_t* codes, unsigned long long* stats, cudaStream_t st)
 {
-    if (nwork > 0) k_run_stats<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, stats);
+    if (nwork > 0) k_run_stats<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, stats);
 }
 
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                      const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st)
 {
-    if (nwork) k_sub_bits<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
+    if (nwork) k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
 }
 
 void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
@@ -717,12 +865,11 @@ void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub
 }
 
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint32_t* sub_bits,
-                   const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st)
+                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                   uint32_t* payload, cudaStream_t st)
 {
     if (nwork)
-        k_encode<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_off, sub_bits, chunk_word_off,
-                                                  payload);
+        k_encode<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_off, chunk_word_off, payload);
 }
 
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,

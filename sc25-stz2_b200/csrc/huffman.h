@@ -31,8 +31,8 @@ void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, 
 void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
                          uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload, cudaStream_t st);
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint32_t* sub_bits,
-                   const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st);
+                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                   uint32_t* payload, cudaStream_t st);
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                    const uint16_t* cb_sym, const uint8_t* cb_len, const uint32_t* sub_off,
                    const uint64_t* chunk_word_off, const uint32_t* payload, uint16_t* codes, cudaStream_t st);
