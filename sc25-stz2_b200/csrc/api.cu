@@ -657,7 +657,53 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
 }
 
 // ---- decode preparation -------------------------------------------------------
-stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
+namespace {
+// Checks one parsed stream header against its directory entry; nullptr when
+// it is consistent. Fills the stream's per-chunk unpredictable-value prefix.
+const char* check_stream(const FileHeader& h, const LevelDir& L, const StreamDir& sdir, const StreamHeader& H,
+                         std::vector<uint64_t>& pre)
+{
+    const uint32_t C = (uint32_t)L.C;
+    const uint32_t nchunks = (uint32_t)((L.dx / L.C) * (L.dy / L.C) * (L.dz / L.C));
+    const uint32_t n_used = (uint32_t)H.sym.size();
+    if (H.run_n && (uint64_t)H.run_base + H.run_n > 2 * (uint64_t)h.radius) return "run symbols outside the code range";
+    uint64_t raw = 0;
+    for (uint64_t v : sdir.lr) raw += v;
+    if (H.chunk_word_off.back() * 4 != raw) return "marker table does not match payload size";
+    if (n_used == 0 || (n_used == 1 && raw != 0)) return "bad codebook";
+    // codebook: symbols in range, sorted canonically, Kraft sum <= 1
+    uint64_t kraft = 0;
+    for (uint32_t j = 0; j < n_used; ++j) {
+        if (H.sym[j] >= 2 * h.radius) return "codebook symbol out of range";
+        if (j && (H.len[j] < H.len[j - 1] || (H.len[j] == H.len[j - 1] && H.sym[j] <= H.sym[j - 1])))
+            return "codebook not in canonical order";
+        if (n_used > 1) {
+            if (H.len[j] == 0) return "zero-length code";
+            kraft += 1ull << (kMaxCodeLen - H.len[j]);
+        }
+        if (H.sym[j] == 0 && H.n_unpred == 0) return "code 0 without unpredictable values";
+    }
+    if (kraft > (1ull << kMaxCodeLen)) return "codebook violates the Kraft inequality";
+    for (uint32_t c = 0; c < nchunks; ++c) {
+        if (H.chunk_word_off[c] > H.chunk_word_off[c + 1]) return "bad marker table";
+        const uint64_t cbits = 32 * (H.chunk_word_off[c + 1] - H.chunk_word_off[c]);
+        const uint32_t* so = H.sub_off.data() + (size_t)c * C;
+        for (uint32_t lz = 0; lz < C; ++lz)
+            if (so[lz] > cbits || (lz && so[lz] < so[lz - 1])) return "bad plane offsets";
+    }
+    pre.resize(nchunks + 1);
+    uint64_t acc = 0;
+    for (uint32_t c = 0; c < nchunks; ++c) {
+        pre[c] = acc;
+        acc += H.unpred_count[c];
+    }
+    pre[nchunks] = acc;
+    if (acc != H.n_unpred) return "unpredictable counts do not match";
+    return nullptr;
+}
+}  // namespace
+
+stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p, const BatchFn* on_batch)
 {
     Lap lap("prepare");
     const ParsedStream& ps = s->dir;
@@ -667,7 +713,9 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
     p.kmax = kmax;
     p.sd.assign(nstreams, StreamDesc{});
     p.hdr.assign(nstreams, StreamHeader{});
+    p.unpred_prefix.assign(nstreams, {});
     std::atomic<int> bad{0};
+    std::vector<const char*> why(nstreams, nullptr);
     const uint8_t* bytes = s->bytes.data();
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t i) {
         const int k = (int)i / 7 + 1, b = (int)i % 7;
@@ -677,13 +725,15 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         const int nch = (L.dx / L.C) * (L.dy / L.C) * (L.dz / L.C);
         if (!decode_frame(bytes + d.data_off, d.hdr_stored, d.hdr_raw, raw.data())) bad = 1;
         else if (!parse_stream_header(raw.data(), raw.size(), nch, L.C, elem, ps.version, p.hdr[i])) bad = 2;
+        else why[i] = check_stream(h, L, d, p.hdr[i], p.unpred_prefix[i]);
     });
     if (bad) STZ_FAIL(STZ_ERR_FORMAT, bad == 1 ? "stream header frame does not decode" : "bad stream header");
+    for (const char* w : why)
+        if (w) STZ_FAIL(STZ_ERR_FORMAT, w);
     lap.mark("header frames");
     // layout
     uint64_t codes = 0, chunks = 0, subs = 0, words = 0, syms = 0, unp = 0;
     p.ulist_off.assign(nstreams + 1, 0);
-    p.unpred_prefix.assign(nstreams, {});
     for (int i = 0; i < nstreams; ++i) {
         const int k = i / 7 + 1;
         const LevelDir& L = ps.lv[k];
@@ -704,49 +754,10 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         syms += d.n_used;
         d.run_base = H.run_base;
         d.run_n = H.run_n;
-        if (d.run_n && (uint64_t)d.run_base + d.run_n > 2 * (uint64_t)h.radius)
-            STZ_FAIL(STZ_ERR_FORMAT, "run symbols outside the code range");
-        uint64_t raw = 0;
-        for (uint64_t v : L.s[i % 7].lr) raw += v;
-        if (H.chunk_word_off.back() * 4 != raw) STZ_FAIL(STZ_ERR_FORMAT, "marker table does not match payload size");
-        if (d.n_used == 0 || (d.n_used == 1 && raw != 0)) STZ_FAIL(STZ_ERR_FORMAT, "bad codebook");
-        // codebook: symbols in range, sorted canonically, Kraft sum <= 1
-        {
-            uint64_t kraft = 0;
-            for (uint32_t j = 0; j < d.n_used; ++j) {
-                if (H.sym[j] >= 2 * h.radius) STZ_FAIL(STZ_ERR_FORMAT, "codebook symbol out of range");
-                if (j && (H.len[j] < H.len[j - 1] || (H.len[j] == H.len[j - 1] && H.sym[j] <= H.sym[j - 1])))
-                    STZ_FAIL(STZ_ERR_FORMAT, "codebook not in canonical order");
-                if (d.n_used > 1) {
-                    if (H.len[j] == 0) STZ_FAIL(STZ_ERR_FORMAT, "zero-length code");
-                    kraft += 1ull << (kMaxCodeLen - H.len[j]);
-                }
-                if (H.sym[j] == 0 && H.n_unpred == 0) STZ_FAIL(STZ_ERR_FORMAT, "code 0 without unpredictable values");
-            }
-            if (kraft > (1ull << kMaxCodeLen)) STZ_FAIL(STZ_ERR_FORMAT, "codebook violates the Kraft inequality");
-        }
-        for (uint32_t c = 0; c < d.nchunks; ++c) {
-            if (H.chunk_word_off[c] > H.chunk_word_off[c + 1]) STZ_FAIL(STZ_ERR_FORMAT, "bad marker table");
-            const uint64_t cbits = 32 * (H.chunk_word_off[c + 1] - H.chunk_word_off[c]);
-            for (uint32_t lz = 0; lz < d.C; ++lz) {
-                const uint32_t v = H.sub_off[(size_t)c * d.C + lz];
-                if (v > cbits || (lz && v < H.sub_off[(size_t)c * d.C + lz - 1]))
-                    STZ_FAIL(STZ_ERR_FORMAT, "bad plane offsets");
-            }
-        }
         d.word_base = words;
-        d.word_cap = raw / 4 + 4;
+        d.word_cap = H.chunk_word_off.back() + 4;
         words += d.word_cap;
         p.ulist_off[i] = unp;
-        auto& pre = p.unpred_prefix[i];
-        pre.resize(d.nchunks + 1);
-        uint64_t acc = 0;
-        for (uint32_t c = 0; c < d.nchunks; ++c) {
-            pre[c] = acc;
-            acc += H.unpred_count[c];
-        }
-        pre[d.nchunks] = acc;
-        if (acc != H.n_unpred) STZ_FAIL(STZ_ERR_FORMAT, "unpredictable counts do not match");
         unp += H.n_unpred;
     }
     p.ulist_off[nstreams] = unp;
@@ -765,7 +776,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         for (int k = 0; k <= kmax; ++k)
             std::memcpy(hs + o_md + k * sizeof(LearnedModel), &ps.lv[k].model, sizeof(LearnedModel));
     std::memcpy(hs + o_sd, p.sd.data(), nstreams * sizeof(StreamDesc));
-    for (int i = 0; i < nstreams; ++i) {
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t i) {
         const StreamHeader& H = p.hdr[i];
         const StreamDesc& d = p.sd[i];
         std::memcpy(hs + o_sym + 2 * (size_t)d.cb_off, H.sym.data(), 2 * H.sym.size());
@@ -773,7 +784,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         std::memcpy(hs + o_sub + 4 * d.sub_base, H.sub_off.data(), 4 * H.sub_off.size());
         std::memcpy(hs + o_ch + 8 * d.chunk_base, H.chunk_word_off.data(), 8 * H.chunk_word_off.size());
         if (H.n_unpred) std::memcpy(hs + o_ul + p.ulist_off[i] * elem, H.unpred.data(), H.unpred.size());
-    }
+    });
     lap.mark("layout + tables");
     // payload frames straight into the staging buffer
     struct Job {
@@ -796,15 +807,46 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         std::memset(dst, 0, 16);  // read-ahead padding of the decoder
     }
     stream_first_job[nstreams] = jobs.size();
-    // Tables first, then the payload in batches of whole streams: each
-    // batch's host->device copy runs while the next batch is being
-    // zstd-decoded.
-    STZ_CUDA(p.stage->ensure(total));
+    // Tables and the coarsest grid first, then the payload in batches of
+    // whole streams: each batch's host->device copy (and, with on_batch, its
+    // decoding) runs while the next batch is being zstd-decoded.
+    const size_t o_tab = align256(total), dev_total = o_tab + (size_t)nstreams * decode_tables_bytes();
+    STZ_CUDA(p.stage->ensure(dev_total));
     STZ_CUDA(cudaMemcpyAsync(p.stage->p, hs, o_pl, cudaMemcpyHostToDevice, ctx->st));
-    const size_t min_batch = 2 * (size_t)ctx->pool->size();
-    for (int s0 = 0; s0 < nstreams;) {
-        int s1 = s0 + 1;
-        while (s1 < nstreams && stream_first_job[s1] - stream_first_job[s0] < min_batch) ++s1;
+    uint8_t* ds = p.stage->as<uint8_t>();
+    p.d_sd = (StreamDesc*)(ds + o_sd);
+    p.d_sym = (uint16_t*)(ds + o_sym);
+    p.d_len = ds + o_len;
+    p.d_sub = (uint32_t*)(ds + o_sub);
+    p.d_choff = (uint64_t*)(ds + o_ch);
+    p.d_ulist = ds + o_ul;
+    p.d_models = learned ? (LearnedModel*)(ds + o_md) : nullptr;
+    p.d_payload = (uint32_t*)(ds + o_pl);
+    p.d_tables = ds + o_tab;
+    launch_build_tables(p.d_sd, nstreams, p.d_sym, p.d_len, p.d_tables, ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
+    STZ_CUDA(p.coarsest->ensure(n0 * elem));
+    STZ_CUDA(cudaMemcpyAsync(p.coarsest->p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
+    // batch ends: with on_batch, every level below kmax, then the finest
+    // level's streams in two halves; else batches of at least two frames per
+    // pool thread
+    std::vector<int> ends;
+    if (on_batch) {
+        if (kmax > 1) ends.push_back(7 * (kmax - 1));
+        ends.push_back(7 * (kmax - 1) + 4);
+        ends.push_back(nstreams);
+    } else {
+        const size_t min_batch = 2 * (size_t)ctx->pool->size();
+        for (int s0 = 0; s0 < nstreams;) {
+            int s1 = s0 + 1;
+            while (s1 < nstreams && stream_first_job[s1] - stream_first_job[s0] < min_batch) ++s1;
+            ends.push_back(s1);
+            s0 = s1;
+        }
+    }
+    int s0 = 0;
+    for (const int s1 : ends) {
         const size_t j0 = stream_first_job[s0], j1 = stream_first_job[s1];
         ctx->pool->parallel_for(j1 - j0, [&](size_t j) {
             if (!decode_frame(jobs[j0 + j].src, jobs[j0 + j].stored, jobs[j0 + j].raw, jobs[j0 + j].dst)) bad = 3;
@@ -815,23 +857,17 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p)
         }
         const size_t b0 = o_pl + 4 * p.sd[s0].word_base;
         const size_t b1 = s1 < nstreams ? o_pl + 4 * p.sd[s1].word_base : total;
-        STZ_CUDA(cudaMemcpyAsync(p.stage->as<uint8_t>() + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st));
+        STZ_CUDA(cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st));
+        if (on_batch) {
+            const stz_status st = (*on_batch)(s0, s1);
+            if (st != STZ_OK) {
+                cudaStreamSynchronize(ctx->st);
+                return st;
+            }
+        }
         s0 = s1;
     }
     lap.mark("payload frames + h2d");
-    uint8_t* ds = p.stage->as<uint8_t>();
-    p.d_sd = (StreamDesc*)(ds + o_sd);
-    p.d_sym = (uint16_t*)(ds + o_sym);
-    p.d_len = ds + o_len;
-    p.d_sub = (uint32_t*)(ds + o_sub);
-    p.d_choff = (uint64_t*)(ds + o_ch);
-    p.d_ulist = ds + o_ul;
-    p.d_models = learned ? (LearnedModel*)(ds + o_md) : nullptr;
-    p.d_payload = (uint32_t*)(ds + o_pl);
-    const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
-    STZ_CUDA(p.coarsest->ensure(n0 * elem));
-    STZ_CUDA(cudaMemcpyAsync(p.coarsest->p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
-    lap.mark("coarsest copy");
     STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned staging buffer is reused by the next call
     lap.mark("host->device");
     return STZ_OK;
@@ -857,7 +893,7 @@ stz_status decode_chunks(stz_context* ctx, const Prepared& p, const std::vector<
     if (!work.empty()) {
         KScope ks(ctx, "k_decode");
         launch_decode((const CtaWork*)(dw + o_w), (const uint32_t*)(dw + o_i), (int)work.size(), p.d_sd, p.d_sym,
-                      p.d_len, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+                      p.d_tables, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), ctx->st);
     }
     if (!uwork.empty()) {
         KScope ks(ctx, "k_unpred_move");
@@ -899,6 +935,113 @@ LevelGeom level_geom(const ParsedStream& ps, int k)
     return g;
 }
 
+// Launches of a decode of levels 1..kdec in batches of streams (in level
+// order): the chunks of a batch are entropy-decoded, then every level whose
+// seven streams are all decoded is reconstructed; the last one lands in out.
+template <typename T>
+struct DecodePipe {
+    stz_context* ctx;
+    const stz_stream* s;
+    const Prepared& p;
+    int kdec;
+    T* out;
+    bool planned = false;
+    std::vector<size_t> wfirst, ufirst;  // per stream: first work / unpredictable item (+ end)
+    size_t o_w = 0, o_i = 0, o_u = 0;
+    int next_level = 1, cur = 0;
+    const T* coarse = nullptr;
+
+    DecodePipe(stz_context* c, const stz_stream* st, const Prepared& pp, int k, T* o)
+        : ctx(c), s(st), p(pp), kdec(k), out(o)
+    {
+    }
+
+    // Work lists of every stream, uploaded once; buffers sized.
+    stz_status plan()
+    {
+        const ParsedStream& ps = s->dir;
+        const int nstreams = 7 * kdec;
+        std::vector<CtaWork> work;
+        std::vector<uint32_t> ids;
+        std::vector<UnpredWork> uw;
+        wfirst.assign(nstreams + 1, 0);
+        ufirst.assign(nstreams + 1, 0);
+        std::vector<uint32_t> all;
+        for (int i = 0; i < nstreams; ++i) {
+            const StreamDesc& d = p.sd[i];
+            wfirst[i] = work.size();
+            ufirst[i] = uw.size();
+            all.resize(d.nchunks);
+            for (uint32_t c = 0; c < d.nchunks; ++c) all[c] = c;
+            add_work(work, ids, (uint32_t)i, all.data(), all.size(), (int)d.C);
+            add_unpred_work(p, (uint32_t)i, all.data(), all.size(), uw);
+        }
+        wfirst[nstreams] = work.size();
+        ufirst[nstreams] = uw.size();
+        o_w = 0, o_i = align256(work.size() * sizeof(CtaWork));
+        o_u = align256(o_i + ids.size() * 4);
+        const size_t total = align256(o_u + uw.size() * sizeof(UnpredWork));
+        STZ_CUDA(ctx->h_meta.ensure(total));
+        uint8_t* hm = ctx->h_meta.as<uint8_t>();
+        std::memcpy(hm + o_w, work.data(), work.size() * sizeof(CtaWork));
+        std::memcpy(hm + o_i, ids.data(), ids.size() * 4);
+        if (!uw.empty()) std::memcpy(hm + o_u, uw.data(), uw.size() * sizeof(UnpredWork));
+        STZ_CUDA(ctx->work.ensure(total));
+        STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hm, total, cudaMemcpyHostToDevice, ctx->st));
+        STZ_CUDA(ctx->codes.ensure(p.total_codes * 2));
+        if (p.total_unpred) STZ_CUDA(ctx->unpred_dense.ensure(p.total_codes * sizeof(T)));
+        const FileHeader& h = ps.h;
+        size_t gmax = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
+        for (int k = 1; k < kdec; ++k) gmax = std::max(gmax, 8 * (size_t)ps.lv[k].dx * ps.lv[k].dy * ps.lv[k].dz);
+        STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
+        STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
+        coarse = p.coarsest->as<T>();
+        planned = true;
+        return STZ_OK;
+    }
+
+    // Streams [s0, s1) have their payload on the device (in stream order).
+    stz_status batch(int s0, int s1)
+    {
+        s1 = std::min(s1, 7 * kdec);
+        if (s0 >= s1) return STZ_OK;
+        if (!planned) STZ_TRY(plan());
+        const uint8_t* dw = ctx->work.as<uint8_t>();
+        const size_t w0 = wfirst[s0], w1 = wfirst[s1], u0 = ufirst[s0], u1 = ufirst[s1];
+        if (w1 > w0) {
+            KScope ks(ctx, "k_decode");
+            launch_decode((const CtaWork*)(dw + o_w) + w0, (const uint32_t*)(dw + o_i), (int)(w1 - w0), p.d_sd,
+                          p.d_sym, p.d_tables, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+        }
+        if (u1 > u0) {
+            KScope ks(ctx, "k_unpred_move");
+            launch_unpred_move<T>(false, (const UnpredWork*)(dw + o_u) + u0, (int)(u1 - u0), p.d_sd,
+                                  ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p.d_ulist, ctx->st);
+        }
+        const ParsedStream& ps = s->dir;
+        for (; next_level <= kdec && 7 * next_level <= s1; ++next_level) {
+            const int k = next_level;
+            LevelDecodeArgs<T> a;
+            a.coarse = coarse;
+            a.geo = level_geom(ps, k);
+            a.predictor = ps.h.predictor;
+            a.qp = qparams(ps, k);
+            a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
+            a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
+            a.out = k == kdec ? out : ctx->grid[cur].as<T>();
+            a.learned = learned_args<T>(ps, k, p.d_models);
+            {
+                KScope ks(ctx, k == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
+                launch_level_decode<T>(a, ctx->st);
+            }
+            coarse = a.out;
+            cur = 1 - cur;
+        }
+        STZ_CUDA(cudaGetLastError());
+        return STZ_OK;
+    }
+};
+
 // Reconstruct levels 1..kdec; the last one lands in out_dev.
 template <typename T>
 stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& p, int kdec, T* out_dev)
@@ -910,42 +1053,10 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
         STZ_CUDA(cudaMemcpyAsync(out_dev, p.coarsest->p, n0 * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
         return STZ_OK;
     }
-    std::vector<CtaWork> work;
-    std::vector<uint32_t> ids;
-    std::vector<UnpredWork> uw;
-    for (int i = 0; i < 7 * kdec; ++i) {
-        const StreamDesc& d = p.sd[i];
-        std::vector<uint32_t> all(d.nchunks);
-        for (uint32_t c = 0; c < d.nchunks; ++c) all[c] = c;
-        add_work(work, ids, (uint32_t)i, all.data(), all.size(), (int)d.C);
-        add_unpred_work(p, (uint32_t)i, all.data(), all.size(), uw);
-    }
-    STZ_TRY(decode_chunks<T>(ctx, p, work, ids, uw));
-    size_t gmax = n0;
-    for (int k = 1; k < kdec; ++k) gmax = std::max(gmax, 8 * (size_t)ps.lv[k].dx * ps.lv[k].dy * ps.lv[k].dz);
-    STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
-    STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
-    const T* coarse = p.coarsest->as<T>();
-    int cur = 0;
-    for (int k = 1; k <= kdec; ++k) {
-        LevelDecodeArgs<T> a;
-        a.coarse = coarse;
-        a.geo = level_geom(ps, k);
-        a.predictor = h.predictor;
-        a.qp = qparams(ps, k);
-        a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
-        a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
-        a.out = k == kdec ? out_dev : ctx->grid[cur].as<T>();
-        a.learned = learned_args<T>(ps, k, p.d_models);
-        {
-            KScope ks(ctx, k == h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
-            launch_level_decode<T>(a, ctx->st);
-        }
-        coarse = a.out;
-        cur = 1 - cur;
-    }
-    STZ_CUDA(cudaGetLastError());
-    return STZ_OK;
+    DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
+    STZ_TRY(pipe.plan());
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned work-list buffer is free for the caller
+    return pipe.batch(0, 7 * kdec);
 }
 
 template <typename T>
@@ -962,12 +1073,16 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     }
     Prepared p;
     ctx->borrow(p);
-    {
-        Trace t("decompress: prepare");
-        STZ_TRY(prepare(ctx, s, kdec, p));
+    if (kdec == 0) {
+        STZ_TRY(prepare(ctx, s, 0, p));
+        STZ_TRY(decode_levels<T>(ctx, s, p, 0, out_dev));
+    } else {
+        // each batch of streams is decoded while the host zstd-decodes the next
+        Trace t("decompress: prepare + decode");
+        DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
+        const BatchFn fn = [&](int s0, int s1) { return pipe.batch(s0, s1); };
+        STZ_TRY(prepare(ctx, s, kdec, p, &fn));
     }
-    Trace t("decompress: decode");
-    STZ_TRY(decode_levels<T>(ctx, s, p, kdec, out_dev));
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
     if (stream_learned(s->dir) && learned_tc_error_take(ctx->st))
         STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
@@ -1089,7 +1204,7 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
     if (!work.empty()) {
         KScope ks(ctx, "k_decode");
         launch_decode((const CtaWork*)(dm + hd.o_work), (const uint32_t*)(dm + hd.o_ids), (int)work.size(), p->d_sd,
-                      p->d_sym, p->d_len, p->d_sub, p->d_choff, p->d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+                      p->d_sym, p->d_tables, p->d_sub, p->d_choff, p->d_payload, ctx->codes.as<uint16_t>(), ctx->st);
     }
     if (!uw.empty()) {
         KScope ks(ctx, "k_unpred_move");

@@ -22,6 +22,8 @@
 // so they share the codebook, the tables and the 16-bit symbol width with
 // the codes; a well-predicted stream (mostly centre codes) then costs well
 // under one bit per code.
+#include <cstdlib>
+
 #include <cuda_runtime.h>
 
 #include "huffman.h"
@@ -442,17 +444,19 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
     }
 }
 
-// Decode: each thread decodes one plane with a 2^kLutBits-entry table in
-// shared memory (symbol | length << 16); longer codes fall back to the
-// canonical first-code test per length.
-// Symbols of codes longer than kLutBits kept in shared memory (the rest of a
-// longer tail is read from global memory).
+// Decode: a warp decodes one plane with a 2^kLutBits-entry table in shared
+// memory (symbol | length << 16); longer codes fall back to the canonical
+// first-code test per length.
+// Symbols of codes longer than kLutBits kept with the tables (the rest of a
+// longer tail is read from the codebook).
 constexpr int kTailSyms = 4096;
 
+// Decode tables of one stream, built once per prepared stream in device
+// memory (k_build_tables) and read by the decoders through L1.
 // lut entry: sym | len << 16 for codes of at most kLutBits bits; for a prefix
 // of longer codes, l_min << 24 with l_min the shortest code length under that
 // prefix (the canonical length search starts there); 0 for a prefix of no code.
-struct DecodeSmem {
+struct DecodeTables {
     uint32_t lut[1 << kLutBits];
     uint32_t cnt[kMaxCodeLen + 1];
     uint32_t first_code[kMaxCodeLen + 1];
@@ -460,15 +464,17 @@ struct DecodeSmem {
     uint16_t tail[kTailSyms];
 };
 
-// Build the decode tables of stream s (all threads of the block).
-__device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_t* __restrict__ cb_sym,
-                              const uint8_t* __restrict__ cb_len)
+// One CTA per stream.
+__global__ void __launch_bounds__(256) k_build_tables(const StreamDesc* __restrict__ sd,
+                                                      const uint16_t* __restrict__ cb_sym,
+                                                      const uint8_t* __restrict__ cb_len,
+                                                      DecodeTables* __restrict__ out)
 {
-    uint32_t* lut = sm.lut;
-    uint32_t* cnt = sm.cnt;
-    uint32_t* first_code = sm.first_code;
-    uint32_t* first_idx = sm.first_idx;
-    for (int i = threadIdx.x; i < (1 << kLutBits); i += blockDim.x) lut[i] = 0;
+    const StreamDesc s = sd[blockIdx.x];
+    DecodeTables& t = out[blockIdx.x];
+    __shared__ uint32_t cnt[kMaxCodeLen + 1];
+    __shared__ uint32_t first_code[kMaxCodeLen + 1];
+    __shared__ uint32_t first_idx[kMaxCodeLen + 1];
     if (threadIdx.x <= kMaxCodeLen) cnt[threadIdx.x] = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < s.n_used; i += blockDim.x) atomicAdd(&cnt[cb_len[s.cb_off + i]], 1u);
@@ -485,6 +491,11 @@ __device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_
         }
     }
     __syncthreads();
+    if (threadIdx.x <= kMaxCodeLen) {
+        t.cnt[threadIdx.x] = cnt[threadIdx.x];
+        t.first_code[threadIdx.x] = first_code[threadIdx.x];
+        t.first_idx[threadIdx.x] = first_idx[threadIdx.x];
+    }
     // every table entry finds its code: the shortest length whose canonical
     // range holds the entry's prefix; prefixes of longer codes record the
     // shortest such length
@@ -507,24 +518,86 @@ __device__ void decode_tables(DecodeSmem& sm, const StreamDesc& s, const uint16_
                 }
             }
         }
-        lut[j] = e;
+        t.lut[j] = e;
     }
     const uint32_t t0 = first_idx[kLutBits + 1];
     for (uint32_t i = threadIdx.x; i < (uint32_t)kTailSyms && t0 + i < s.n_used; i += blockDim.x)
-        sm.tail[i] = cb_sym[s.cb_off + t0 + i];
-    __syncthreads();
+        t.tail[i] = cb_sym[s.cb_off + t0 + i];
 }
 
-// Decode plane lz of chunk c of stream s (one thread).
-__device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t c, uint32_t lz,
+// The symbol whose code starts at the top of `bits` (MSB first, at least
+// kMaxCodeLen valid bits); its code length in l (>= 1). A prefix of no code
+// (corrupt stream) yields the codebook's first symbol with length 1, so
+// every step consumes a bit.
+__device__ __forceinline__ uint32_t lookup_symbol(const DecodeTables* __restrict__ t, const StreamDesc& s,
+                                                  const uint16_t* __restrict__ cb_sym, uint32_t bits, uint32_t& l)
+{
+    const uint32_t e = __ldg(&t->lut[bits >> (32 - kLutBits)]);
+    uint32_t sym = e & 0xffffu;
+    l = (e >> 16) & 0xffu;
+    if (!l) {
+        // canonical search from the shortest length under this prefix
+        l = e >> 24;
+        if (!l) l = kLutBits + 1;
+        for (; l <= (uint32_t)kMaxCodeLen; ++l) {
+            const uint32_t v = bits >> (32 - l), fc = __ldg(&t->first_code[l]);
+            if (v - fc < __ldg(&t->cnt[l])) {
+                const uint32_t fi = __ldg(&t->first_idx[l]);
+                const uint32_t idx = fi + (v - fc);
+                const uint32_t ti = idx - __ldg(&t->first_idx[kLutBits + 1]);
+                sym = ti < (uint32_t)kTailSyms ? __ldg(&t->tail[ti]) : cb_sym[s.cb_off + idx];
+                break;
+            }
+        }
+        if (l > (uint32_t)kMaxCodeLen) {
+            sym = cb_sym[s.cb_off];
+            l = 1;
+        }
+    }
+    return sym;
+}
+
+// Bits of one chunk's payload: 32 bits from any bit position. Plane bit
+// ranges are validated against the chunk's words, and every stream keeps at
+// least two words of zero padding after its payload, so a read at a position
+// below a plane's end stays inside the stream's buffer.
+struct ChunkBits {
+    const uint32_t* in;
+    __device__ __forceinline__ uint32_t peek(uint32_t pos) const
+    {
+        const uint32_t i = pos >> 5;
+        return __funnelshift_l(__ldg(in + i + 1), __ldg(in + i), pos & 31);
+    }
+};
+
+// Decode every code that starts in [pos, stop): f(sym) for each; returns the
+// position after the last one (the first code boundary >= stop, or pos).
+template <class F>
+__device__ __forceinline__ uint32_t decode_range(const DecodeTables* __restrict__ t, const StreamDesc& s,
+                                                 const uint16_t* __restrict__ cb_sym, const ChunkBits& cb,
+                                                 uint32_t pos, uint32_t stop, F&& f)
+{
+    while (pos < stop) {
+        uint32_t l;
+        const uint32_t sym = lookup_symbol(t, s, cb_sym, cb.peek(pos), l);
+        pos += l;
+        f(sym);
+    }
+    return pos;
+}
+
+// Decode plane lz of chunk c of stream s (one thread, sequentially): for
+// dense streams, where a plane holds many symbols and a warp per plane would
+// decode each one about three times.
+__device__ void decode_plane_seq(const DecodeTables* __restrict__ t, const StreamDesc& s, uint32_t c, uint32_t lz,
                              const uint16_t* __restrict__ cb_sym, const uint32_t* __restrict__ sub_off,
                              const uint64_t* __restrict__ chunk_word_off, const uint32_t* __restrict__ payload,
                              uint16_t* __restrict__ codes)
 {
-    const uint32_t* lut = sm.lut;
-    const uint32_t* cnt = sm.cnt;
-    const uint32_t* first_code = sm.first_code;
-    const uint32_t* first_idx = sm.first_idx;
+    const uint32_t* __restrict__ lut = t->lut;
+    const uint32_t* __restrict__ cnt = t->cnt;
+    const uint32_t* __restrict__ first_code = t->first_code;
+    const uint32_t* __restrict__ first_idx = t->first_idx;
     const uint32_t C = s.C;
     const size_t plane = (size_t)C * C;
     uint16_t* dst = codes + s.code_off + (size_t)c * plane * C + (size_t)lz * plane;
@@ -565,7 +638,7 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
     uint32_t w = rd(wi + 2);
     wi += 3;
     auto next = [&]() -> uint32_t {
-        const uint32_t e = lut[(uint32_t)(buf >> (64 - kLutBits))];
+        const uint32_t e = __ldg(lut + (uint32_t)(buf >> (64 - kLutBits)));
         const bool rf = avail < 32;
         const uint64_t b2 = rf ? (buf | ((uint64_t)w << (32 - avail))) : buf;  // >= 32 valid bits
         const int a2 = rf ? avail + 32 : avail;
@@ -582,7 +655,7 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
                 if (v - first_code[l] < cnt[l]) {
                     const uint32_t idx = first_idx[l] + (v - first_code[l]);
                     const uint32_t ti = idx - first_idx[kLutBits + 1];
-                    sym = ti < (uint32_t)kTailSyms ? sm.tail[ti] : cb_sym[s.cb_off + idx];
+                    sym = ti < (uint32_t)kTailSyms ? __ldg(&t->tail[ti]) : cb_sym[s.cb_off + idx];
                     break;
                 }
             }
@@ -689,57 +762,159 @@ __device__ void decode_plane(const DecodeSmem& sm, const StreamDesc& s, uint32_t
     }
 }
 
-// One CTA per work item.
-__global__ void __launch_bounds__(kCoderThreads) k_decode(const CtaWork* __restrict__ work,
-                                                          const uint32_t* __restrict__ chunk_ids,
-                                                          const StreamDesc* __restrict__ sd,
-                                                          const uint16_t* __restrict__ cb_sym,
-                                                          const uint8_t* __restrict__ cb_len,
-                                                          const uint32_t* __restrict__ sub_off,
-                                                          const uint64_t* __restrict__ chunk_word_off,
-                                                          const uint32_t* __restrict__ payload,
-                                                          uint16_t* __restrict__ codes)
+// Decode plane lz of chunk c of stream s (one warp; Weissenberger & Schmidt,
+// "Massively parallel Huffman decoding on GPUs", ICPP 2018: speculative
+// decoding from equal bit slices, then resynchronisation). The plane's bits
+// [b0, b1) are cut into 32 slices; lane i decodes the codes that start in
+// its slice, beginning at the slice start. A lane whose start is not where
+// its left neighbour's last code ends decodes again from there, until no
+// start moves (lane i is exact after i rounds; codes resynchronise within a
+// few symbols, so one or two rounds are usual). An exclusive scan of the
+// lanes' code counts (a run symbol counts its run) then places each lane's
+// output. With run symbols the plane is first filled with the centre code,
+// so a lane writes only its literals. Output past the plane (a corrupt
+// stream) is dropped.
+__device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const StreamDesc& s, uint32_t c, uint32_t lz,
+                                  const uint16_t* __restrict__ cb_sym, const uint32_t* __restrict__ sub_off,
+                                  const uint64_t* __restrict__ chunk_word_off, const uint32_t* __restrict__ payload,
+                                  uint16_t* __restrict__ codes)
 {
-    __shared__ DecodeSmem sm;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t C = s.C, P = C * C;
+    uint16_t* dst = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+    const bool vec = P % 8 == 0 && ((uintptr_t)dst & 15) == 0;
+    const uint32_t R = s.radius, base = s.run_base, J = s.run_n;
+    auto fill = [&](uint16_t v) {
+        if (vec) {
+            const uint32_t v2 = (uint32_t)v | ((uint32_t)v << 16);
+            for (uint32_t j = lane; j < P / 8; j += 32) reinterpret_cast<uint4*>(dst)[j] = make_uint4(v2, v2, v2, v2);
+        } else {
+            for (uint32_t j = lane; j < P; j += 32) dst[j] = v;
+        }
+    };
+    if (s.n_used == 1) {
+        // a lone run symbol means the plane is all centre codes
+        const uint16_t v0 = cb_sym[s.cb_off];
+        fill((uint32_t)v0 - base < J ? (uint16_t)R : v0);
+        return;
+    }
+    const uint64_t cw = chunk_word_off[s.chunk_base + c];
+    ChunkBits cb;
+    cb.in = payload + s.word_base + cw;
+    const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
+    const uint32_t b1 = lz + 1 < C ? sub_off[s.sub_base + (size_t)c * C + lz + 1]
+                                   : (uint32_t)(32 * (chunk_word_off[s.chunk_base + c + 1] - cw));
+    const uint32_t nb = b1 > b0 ? b1 - b0 : 0;
+    const uint32_t L = (nb + 31) / 32;
+    const uint32_t stop = b0 + min(nb, (lane + 1) * L);
+    uint32_t D, LD;
+    run_geometry(P, D, LD);
+    uint32_t start = b0 + min(nb, lane * L), cnt = 0;
+    auto count = [&](uint32_t sym) { cnt += sym - base < J ? run_length(sym - base, D, LD) : 1u; };
+    uint32_t end = decode_range(t, s, cb_sym, cb, start, stop, count);
+    for (int round = 0; round < 32; ++round) {
+        uint32_t prev = __shfl_up_sync(0xffffffffu, end, 1);
+        if (lane == 0) prev = b0;
+        const bool moved = prev != start;
+        if (!__any_sync(0xffffffffu, moved)) break;
+        if (moved) {
+            start = prev;
+            cnt = 0;
+            end = decode_range(t, s, cb_sym, cb, start, stop, count);
+        }
+    }
+    uint32_t q = cnt;  // inclusive scan -> first output position
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, q, o);
+        if (lane >= (uint32_t)o) q += v;
+    }
+    q -= cnt;
+    if (J) {
+        fill((uint16_t)R);
+        __syncwarp();
+        decode_range(t, s, cb_sym, cb, start, stop, [&](uint32_t sym) {
+            if (sym - base < J) {
+                q += run_length(sym - base, D, LD);
+            } else {
+                if (q < P) dst[q] = (uint16_t)sym;
+                ++q;
+            }
+        });
+    } else {
+        decode_range(t, s, cb_sym, cb, start, stop, [&](uint32_t sym) {
+            if (q < P) dst[q] = (uint16_t)sym;
+            ++q;
+        });
+    }
+}
+
+constexpr int kDecodeThreads = 256;  // 8 warps, each one plane
+constexpr int kDecodeSlices = 16;    // CTAs per work item (gridDim.y): short CTAs, every warp one plane
+constexpr uint32_t kSeqBits = 2048;  // mean payload bits per plane above which a stream decodes one thread per plane
+
+// A stream whose planes average more than seq_bits payload bits, with enough
+// planes to fill the device one thread per plane, is decoded one thread per
+// plane; sparser or smaller streams one warp per plane (a warp decodes each
+// symbol about three times, a thread once but with the full serial chain).
+constexpr uint64_t kSeqMinPlanes = 16384;
+constexpr int kSeqMinItems = 128;  // smaller launches (single requests) are latency-bound: warps only
+__device__ __forceinline__ bool decode_sequential(const StreamDesc& s, uint32_t seq_bits)
+{
+    const uint64_t planes = (uint64_t)s.nchunks * s.C;
+    return planes >= kSeqMinPlanes && 32 * (s.word_cap - 4) > (uint64_t)seq_bits * planes;
+}
+
+// Planes of the listed chunks; the tables of stream i at tabs[i]. Warp mode:
+// CTA (x, y) takes 8 planes of item x; sequential mode: CTA (x, 0) takes all
+// of them, one per thread (at most kDecodeThreads).
+__global__ void __launch_bounds__(kDecodeThreads) k_decode(const CtaWork* __restrict__ work,
+                                                           const uint32_t* __restrict__ chunk_ids,
+                                                           const StreamDesc* __restrict__ sd,
+                                                           const DecodeTables* __restrict__ tabs,
+                                                           const uint16_t* __restrict__ cb_sym,
+                                                           const uint32_t* __restrict__ sub_off,
+                                                           const uint64_t* __restrict__ chunk_word_off,
+                                                           const uint32_t* __restrict__ payload,
+                                                           uint16_t* __restrict__ codes, uint32_t seq_bits)
+{
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
-    decode_tables(sm, s, cb_sym, cb_len);
-    const uint32_t t = threadIdx.x;
-    if (t / s.C >= w.count) return;
-    decode_plane(sm, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off, chunk_word_off, payload, codes);
+    if (decode_sequential(s, seq_bits)) {
+        const uint32_t t = threadIdx.x;
+        if (blockIdx.y == 0 && t < w.count * s.C)
+            decode_plane_seq(tabs + w.stream, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off,
+                             chunk_word_off, payload, codes);
+        return;
+    }
+    STZ_WARP_PLANES(p, w.count * s.C)
+    decode_plane_warp(tabs + w.stream, s, chunk_ids[w.first + p / s.C], p % s.C, cb_sym, sub_off, chunk_word_off,
+                      payload, codes);
 }
 
 // Persistent variant: a fixed grid walks the work list of a batch held in
-// device memory (BatchHdr at meta), so one captured launch serves any batch.
-// The tables are rebuilt only when the stream changes between consecutive
-// items.
-__global__ void __launch_bounds__(kCoderThreads) k_decode_dyn(const uint8_t* __restrict__ meta,
-                                                              const StreamDesc* __restrict__ sd,
-                                                              const uint16_t* __restrict__ cb_sym,
-                                                              const uint8_t* __restrict__ cb_len,
-                                                              const uint32_t* __restrict__ sub_off,
-                                                              const uint64_t* __restrict__ chunk_word_off,
-                                                              const uint32_t* __restrict__ payload,
-                                                              uint16_t* __restrict__ codes)
+// device memory (BatchHdr at meta), so one captured launch serves any batch;
+// each item is cut into kDecodeSlices slices of 8 planes.
+__global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __restrict__ meta,
+                                                               const StreamDesc* __restrict__ sd,
+                                                               const DecodeTables* __restrict__ tabs,
+                                                               const uint16_t* __restrict__ cb_sym,
+                                                               const uint32_t* __restrict__ sub_off,
+                                                               const uint64_t* __restrict__ chunk_word_off,
+                                                               const uint32_t* __restrict__ payload,
+                                                               uint16_t* __restrict__ codes)
 {
-    __shared__ DecodeSmem sm;
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
     const uint32_t n = h->n_work;
     const CtaWork* __restrict__ work = reinterpret_cast<const CtaWork*>(meta + h->o_work);
     const uint32_t* __restrict__ chunk_ids = reinterpret_cast<const uint32_t*>(meta + h->o_ids);
-    uint32_t cur = 0xffffffffu;
-    for (uint32_t wi = blockIdx.x; wi < n; wi += gridDim.x) {
-        const CtaWork w = work[wi];
+    const uint32_t nw = blockDim.x >> 5, S = kDecodeSlices;
+    for (uint32_t u = blockIdx.x; u < n * S; u += gridDim.x) {
+        const CtaWork w = work[u / S];
         const StreamDesc s = sd[w.stream];
-        if (w.stream != cur) {
-            __syncthreads();  // every thread is done with the previous tables
-            decode_tables(sm, s, cb_sym, cb_len);
-            cur = w.stream;
-        }
-        const uint32_t t = threadIdx.x;
-        if (t / s.C < w.count)
-            decode_plane(sm, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off, chunk_word_off, payload,
-                         codes);
+        for (uint32_t p = (u % S) * nw + (threadIdx.x >> 5); p < w.count * s.C; p += nw * S)
+            decode_plane_warp(tabs + w.stream, s, chunk_ids[w.first + p / s.C], p % s.C, cb_sym, sub_off,
+                              chunk_word_off, payload, codes);
     }
 }
 
@@ -873,12 +1048,31 @@ void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, co
 }
 
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* cb_sym, const uint8_t* cb_len, const uint32_t* sub_off,
-                   const uint64_t* chunk_word_off, const uint32_t* payload, uint16_t* codes, cudaStream_t st)
+                   const uint16_t* cb_sym, const void* tables, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                   const uint32_t* payload, uint16_t* codes, cudaStream_t st)
 {
     if (nwork)
-        k_decode<<<nwork, kCoderThreads, 0, st>>>(work, chunk_ids, sd, cb_sym, cb_len, sub_off, chunk_word_off, payload,
-                                                  codes);
+        k_decode<<<dim3(nwork, kDecodeSlices), kDecodeThreads, 0, st>>>(
+            work, chunk_ids, sd, static_cast<const DecodeTables*>(tables), cb_sym, sub_off, chunk_word_off, payload,
+            codes, nwork >= kSeqMinItems ? decode_seq_bits() : 0xffffffffu);
+}
+
+size_t decode_tables_bytes() { return sizeof(DecodeTables); }
+
+uint32_t decode_seq_bits()
+{
+    static const uint32_t v = [] {
+        const char* e = std::getenv("STZ_DECODE_SEQ_BITS");
+        return e ? (uint32_t)std::strtoul(e, nullptr, 10) : kSeqBits;
+    }();
+    return v;
+}
+
+void launch_build_tables(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
+                         void* tables, cudaStream_t st)
+{
+    if (nstreams > 0)
+        k_build_tables<<<nstreams, 256, 0, st>>>(sd, cb_sym, cb_len, static_cast<DecodeTables*>(tables));
 }
 
 template <typename T>
@@ -896,10 +1090,11 @@ template void launch_unpred_move<double>(bool, const UnpredWork*, int, const Str
                                          double*, cudaStream_t);
 
 void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* cb_sym,
-                       const uint8_t* cb_len, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                       const void* tables, const uint32_t* sub_off, const uint64_t* chunk_word_off,
                        const uint32_t* payload, uint16_t* codes, cudaStream_t st)
 {
-    k_decode_dyn<<<grid, kCoderThreads, 0, st>>>(meta, sd, cb_sym, cb_len, sub_off, chunk_word_off, payload, codes);
+    k_decode_dyn<<<grid, kDecodeThreads, 0, st>>>(meta, sd, static_cast<const DecodeTables*>(tables), cb_sym, sub_off,
+                                                  chunk_word_off, payload, codes);
 }
 
 template <typename T>

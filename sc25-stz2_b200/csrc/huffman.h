@@ -34,8 +34,18 @@ void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, co
                    const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
                    uint32_t* payload, cudaStream_t st);
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* cb_sym, const uint8_t* cb_len, const uint32_t* sub_off,
-                   const uint64_t* chunk_word_off, const uint32_t* payload, uint16_t* codes, cudaStream_t st);
+                   const uint16_t* cb_sym, const void* tables, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                   const uint32_t* payload, uint16_t* codes, cudaStream_t st);
+// Decode tables of every stream (read by the decoders): decode_tables_bytes()
+// each, stream i at byte i * decode_tables_bytes() of `tables`.
+size_t decode_tables_bytes();
+// Mean payload bits per plane above which launch_decode decodes a stream one
+// thread per plane instead of one warp per plane, in launches of at least 128
+// work items and for streams of at least 16384 planes (STZ_DECODE_SEQ_BITS
+// overrides the built-in 2048).
+uint32_t decode_seq_bits();
+void launch_build_tables(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
+                         void* tables, cudaStream_t st);
 // Copy each stream's used payload words into one contiguous buffer.
 void launch_pack_payload(const uint32_t* src, const uint64_t* src_base, const uint64_t* dst_base,
                          const uint64_t* count, int nstreams, uint32_t* dst, cudaStream_t st);
@@ -47,7 +57,7 @@ void launch_unpred_move(bool gather, const UnpredWork* work, int nwork, const St
 // batch held in device memory (BatchHdr at meta: n_work/o_work/o_ids,
 // n_uwork/o_uwork).
 void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* cb_sym,
-                       const uint8_t* cb_len, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                       const void* tables, const uint32_t* sub_off, const uint64_t* chunk_word_off,
                        const uint32_t* payload, uint16_t* codes, cudaStream_t st);
 template <typename T>
 void launch_unpred_scatter_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, const uint16_t* codes, T* dense,

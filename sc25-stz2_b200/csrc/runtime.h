@@ -126,6 +126,7 @@ struct Prepared {
     uint8_t* d_ulist = nullptr;
     uint32_t* d_payload = nullptr;
     LearnedModel* d_models = nullptr;  // per level k (index k), when the stream has learned corrections
+    void* d_tables = nullptr;          // decode tables per stream (launch_build_tables)
     bool base_valid = false;  // *base holds the decoded base grid (level K-2 output) for box queries
 };
 
@@ -307,7 +308,11 @@ size_t dtype_size(int dtype);
 stz_status enter(stz_context* ctx);
 // Parse stream headers, lay out and upload the tables and payload of levels
 // 1..kmax (zstd frames decoded on the host pool) and the coarsest grid.
-stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p);
+// on_batch(s0, s1), when given, runs after the copy of the payload of streams
+// [s0, s1) is enqueued on ctx->st (batches in stream order, ending at the
+// level boundaries below kmax); prepare returns once the stream is idle.
+using BatchFn = std::function<stz_status(int, int)>;
+stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p, const BatchFn* on_batch = nullptr);
 // Entropy-decode the listed chunks into ctx->codes (and scatter their
 // unpredictable values into ctx->unpred_dense).
 template <typename T>

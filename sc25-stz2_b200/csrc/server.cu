@@ -414,7 +414,7 @@ void enqueue_kernels(const SrvStream& ss, const LaunchShape& sh, const uint8_t* 
 {
     const Prepared& p = *ss.p;
     uint16_t* codes = ss.codes.as<uint16_t>();
-    launch_decode_dyn(sh.decode_grid, meta, p.d_sd, p.d_sym, p.d_len, p.d_sub, p.d_choff, p.d_payload, codes, st);
+    launch_decode_dyn(sh.decode_grid, meta, p.d_sd, p.d_sym, p.d_tables, p.d_sub, p.d_choff, p.d_payload, codes, st);
     if (p.total_unpred)
         launch_unpred_scatter_dyn<T>(sh.unpred_grid, meta, p.d_sd, codes, ss.unpred.as<T>(), (T*)p.d_ulist, st);
     const T* base = p.base->as<T>();
@@ -565,7 +565,7 @@ cudaError_t enqueue_bulk(SrvStream& ss, const uint8_t* hrec, const uint8_t* drec
     uint16_t* codes = ss.codes.as<uint16_t>();
     if (h->n_work)
         launch_decode(reinterpret_cast<const CtaWork*>(drec + h->o_work),
-                      reinterpret_cast<const uint32_t*>(drec + h->o_ids), (int)h->n_work, p.d_sd, p.d_sym, p.d_len,
+                      reinterpret_cast<const uint32_t*>(drec + h->o_ids), (int)h->n_work, p.d_sd, p.d_sym, p.d_tables,
                       p.d_sub, p.d_choff, p.d_payload, codes, st);
     if (h->n_uwork)
         launch_unpred_move<T>(false, reinterpret_cast<const UnpredWork*>(drec + h->o_uwork), (int)h->n_uwork, p.d_sd,
