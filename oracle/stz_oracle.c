@@ -295,10 +295,22 @@ static double rf64(rd_t* r) { double v; rget(r, &v, 8); return v; }
 static const char kMagic[8] = {'S', 'T', 'Z', 'B', '2', '0', '0', 0};
 
 /* One zstd frame of the container: compressed when that is smaller, else the
- * raw bytes (a stored size equal to the raw size means raw). */
-static void put_frame(buf_t* data, const uint8_t* raw, size_t n, int level, uint64_t* stored)
+ * raw bytes (a stored size equal to the raw size means raw). A payload frame
+ * longer than ZSTD_PROBE bytes is tried only when zstd shrinks its first
+ * ZSTD_PROBE bytes (this container's own rule; Huffman payload is rarely
+ * compressible). */
+#define ZSTD_PROBE 4096
+static void put_frame(buf_t* data, const uint8_t* raw, size_t n, int level, int payload, uint64_t* stored)
 {
-    if (level > 0 && n > 0) {
+    int try_zstd = level > 0 && n > 0;
+    if (try_zstd && payload && n > ZSTD_PROBE) {
+        const size_t pcap = ZSTD_compressBound(ZSTD_PROBE);
+        uint8_t* tmp = (uint8_t*)malloc(pcap);
+        const size_t c = ZSTD_compress(tmp, pcap, raw, ZSTD_PROBE, level);
+        try_zstd = !ZSTD_isError(c) && c < ZSTD_PROBE;
+        free(tmp);
+    }
+    if (try_zstd) {
         const size_t cap = ZSTD_compressBound(n);
         uint8_t* tmp = (uint8_t*)malloc(cap);
         const size_t c = ZSTD_compress(tmp, cap, raw, n, level);
@@ -672,7 +684,7 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
             encode_stream(codes, n, d[0], d[1], d[2], C, h.radius, ucm, counts[b], ucount, h.elem, &es);
             uoff += counts[b];
             uint64_t hs;
-            put_frame(&data, es.hdr.p, es.hdr.n, h.zstd_level, &hs);
+            put_frame(&data, es.hdr.p, es.hdr.n, h.zstd_level, 0, &hs);
             bu32(&dir, (uint32_t)es.layers);
             bu64(&dir, hs);
             bu64(&dir, es.hdr.n);
@@ -682,7 +694,7 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
                 const uint64_t w0 = es.chunk_off[(size_t)L * es.chunks_per_layer];
                 const uint64_t w1 = es.chunk_off[(size_t)(L + 1) * es.chunks_per_layer];
                 lr[L] = 4 * (w1 - w0);
-                put_frame(&data, (const uint8_t*)(es.words + w0), (size_t)lr[L], h.zstd_level, &ls[L]);
+                put_frame(&data, (const uint8_t*)(es.words + w0), (size_t)lr[L], h.zstd_level, 1, &ls[L]);
             }
             for (int L = 0; L < es.layers; ++L) bu64(&dir, ls[L]);
             for (int L = 0; L < es.layers; ++L) bu64(&dir, lr[L]);

@@ -542,6 +542,7 @@ ContainerWriter::ContainerWriter(const FileHeader& h, std::vector<StreamParts>& 
             const uint64_t w0 = parts[i].chunk_word_off[(size_t)L * parts[i].chunks_per_layer];
             const uint64_t w1 = parts[i].chunk_word_off[(size_t)(L + 1) * parts[i].chunks_per_layer];
             frames_.push_back({(const uint8_t*)(parts[i].words + w0), (size_t)(4 * (w1 - w0))});
+            frames_.back().payload = true;
         }
     }
     first_[parts.size()] = frames_.size();
@@ -579,7 +580,15 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
         Frame& f = frames_[order[k]];
         f.raw = true;
         f.stored = f.n;
-        if (level > 0 && f.n > 0) {
+        bool try_zstd = level > 0 && f.n > 0;
+        if (try_zstd && f.payload && f.n > kZstdProbeBytes) {
+            // Huffman payload is rarely compressible: zstd the whole frame only
+            // when it shrinks the frame's first kZstdProbeBytes
+            uint8_t probe[kZstdProbeBytes + kZstdProbeBytes / 64 + 512];
+            const size_t c = zstd_compress(probe, sizeof(probe), f.src, kZstdProbeBytes, level);
+            try_zstd = !ZSTD_isError(c) && c < kZstdProbeBytes;
+        }
+        if (try_zstd) {
             const size_t cap = ZSTD_compressBound(f.n);
             f.out.reset(new uint8_t[cap]);
             const size_t c = zstd_compress(f.out.get(), cap, f.src, f.n, level);

@@ -171,6 +171,11 @@ void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const 
                           const uint32_t* unpred_count, const uint64_t* chunk_word_off, const uint32_t* sub_off,
                           int nchunks, int C);
 
+// A payload frame longer than this many bytes is zstd-compressed only when
+// zstd shrinks its first kZstdProbeBytes (stream headers and shorter frames
+// are always tried); a frame is stored compressed when that is smaller.
+constexpr size_t kZstdProbeBytes = 4096;
+
 // The container in stages: the frame list of every stream (its header, one
 // frame per chunk z-layer of payload), zstd of the frames of a range of
 // streams on the pool (as soon as their bytes are on the host), then the
@@ -192,6 +197,7 @@ private:
     struct Frame {
         const uint8_t* src;
         size_t n;
+        bool payload = false;  // a chunk z-layer of payload (else a stream header)
         std::unique_ptr<uint8_t[]> out;
         size_t stored = 0;
         bool raw = true;
