@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
         }
         if (valid) encode_point<T, PRED, FINEST, true, LM>(r, io, geo, qp, lut, ci, x, y, z, q, la, acc3);
 #pragma unroll
-        for (int b = 0; b < 7; ++b) hist_warp(sh, wlo, wn, hist, b, q[b], center[b]);
+        for (int b = 0; b < 7; ++b) hist_code(sh, wlo, wn, hist, b, q[b], center[b]);
     }
     if constexpr (LM == kLearnTc) {
         tc::net_teardown(*net_smem(), tid);
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
             encode_point<T, PRED, FINEST, false>(r, io, geo, qp, lut, ci, x, y, z, q);
         }
 #pragma unroll
-        for (int b = 0; b < 7; ++b) hist_warp(nullptr, 0, 0, hist, b, q[b], center[b]);
+        for (int b = 0; b < 7; ++b) hist_code(nullptr, 0, 0, hist, b, q[b], center[b]);
     }
     hist_flush_center(nullptr, 0, 0, hist, center);
 }
@@ -288,7 +288,7 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
 }
 
 template <typename T, int PRED, int LM>
-__global__ void __launch_bounds__(BX* BY) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
+__global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
                                                          const T* __restrict__ unpred_dense, T* __restrict__ G,
                                                          LearnedArgs<T> la)

@@ -112,17 +112,14 @@ __device__ __forceinline__ void hist_add(uint32_t (*sh)[kSmemBins], int wlo, int
 
 // Histogram of one stream: codes equal to the radius (the dominant bin of a
 // well-predicted level) are counted in a register per thread; any other code
-// goes through a warp-aggregated atomic (one per distinct code in the warp).
-// `key` < 0 marks a lane without a code.
-__device__ __forceinline__ void hist_warp(uint32_t (*sh)[kSmemBins], int wlo, int wn, const HistArgs& h, int b, int key,
+// is one atomic on the block's shared bins (such codes are few, so lanes
+// rarely collide; a warp-aggregated form cost more in match/vote
+// instructions than it saved). `key` < 0 marks a lane without a code.
+__device__ __forceinline__ void hist_code(uint32_t (*sh)[kSmemBins], int wlo, int wn, const HistArgs& h, int b, int key,
                                           uint32_t& center)
 {
-    const unsigned full = 0xffffffffu;
     center += key == h.radius;
-    const int k = key == h.radius ? -1 : key;
-    if (!__any_sync(full, k >= 0)) return;
-    const unsigned peers = __match_any_sync(full, k);
-    if (k >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) hist_add(sh, wlo, wn, h, b, k, (uint32_t)__popc(peers));
+    if (key >= 0 && key != h.radius) hist_add(sh, wlo, wn, h, b, key, 1u);
 }
 
 // Flush the per-thread dominant-bin counters: warp sum, one atomic per warp.
