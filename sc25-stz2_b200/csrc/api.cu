@@ -527,12 +527,15 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(ctx->h_payload.ensure(std::max<uint64_t>(packed_total, 1) * 4));
 
     // Encode, pack and copy back in groups: every stream of the coarser
-    // levels, then the finest level's streams two chunk z-layers at a time
-    // (all 7 streams per group, so every launch still fills the device); the
-    // host zstd-compresses a group's frames while the device encodes the next.
+    // levels, then the finest level's streams in two halves of their chunk
+    // z-layers (all 7 streams per group, so every launch still fills the
+    // device); the host zstd-compresses a group's frames while the device
+    // encodes the next (one, two, four or eight finest groups measured within
+    // noise of each other once payload frames skip zstd; two is the fewest
+    // launches that still overlap the copy back).
     const int fin0 = std::max(0, nstreams - 7);
     const int fin_layers = (int)sd[nstreams - 1].ncz;
-    const int lpg = std::max(1, (fin_layers + 3) / 4);  // layers per group
+    const int lpg = std::max(1, (fin_layers + 1) / 2);  // layers per group: two finest groups
     const size_t ngroups = 1 + (size_t)((fin_layers + lpg - 1) / lpg);
     struct Piece {  // a word range of one stream's payload
         int s;
@@ -845,6 +848,20 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
             s0 = s1;
         }
     }
+    // Payload copies go on the context's copy stream, so a batch's copy
+    // overlaps the decoding of the batch before it; ctx->st waits on each
+    // batch's event before decoding it (or, without on_batch, on the last).
+    struct Events {
+        std::vector<cudaEvent_t> e;
+        ~Events()
+        {
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } ev;
+    auto sync_both = [&]() {
+        cudaStreamSynchronize(ctx->st_copy);
+        cudaStreamSynchronize(ctx->st);
+    };
     int s0 = 0;
     for (const int s1 : ends) {
         const size_t j0 = stream_first_job[s0], j1 = stream_first_job[s1];
@@ -852,23 +869,33 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
             if (!decode_frame(jobs[j0 + j].src, jobs[j0 + j].stored, jobs[j0 + j].raw, jobs[j0 + j].dst)) bad = 3;
         });
         if (bad) {
-            cudaStreamSynchronize(ctx->st);
+            sync_both();
             STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
         }
         const size_t b0 = o_pl + 4 * p.sd[s0].word_base;
         const size_t b1 = s1 < nstreams ? o_pl + 4 * p.sd[s1].word_base : total;
-        STZ_CUDA(cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st));
+        cudaEvent_t e = nullptr;
+        cudaError_t ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (ce == cudaSuccess) ev.e.push_back(e);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st_copy);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e, ctx->st_copy);
+        if (ce == cudaSuccess && (on_batch || s1 == nstreams)) ce = cudaStreamWaitEvent(ctx->st, e, 0);
+        if (ce != cudaSuccess) {
+            sync_both();
+            STZ_CUDA(ce);
+        }
         if (on_batch) {
             const stz_status st = (*on_batch)(s0, s1);
             if (st != STZ_OK) {
-                cudaStreamSynchronize(ctx->st);
+                sync_both();
                 return st;
             }
         }
         s0 = s1;
     }
     lap.mark("payload frames + h2d");
-    STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned staging buffer is reused by the next call
+    STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));  // the pinned staging buffer is reused by the next call
+    STZ_CUDA(cudaStreamSynchronize(ctx->st));
     lap.mark("host->device");
     return STZ_OK;
 }
@@ -1305,6 +1332,10 @@ stz_status stz_context_create(int device, stz_context** out)
     if (!c) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
     c->device = device;
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        e = cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking);
+        if (e != cudaSuccess) cudaStreamDestroy(c->st);
+    }
     if (e != cudaSuccess) {
         delete c;
         STZ_FAIL(STZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
@@ -1319,7 +1350,9 @@ void stz_context_destroy(stz_context* ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->st);
+    cudaStreamSynchronize(ctx->st_copy);
     cudaStreamDestroy(ctx->st);
+    cudaStreamDestroy(ctx->st_copy);
     delete ctx;
 }
 

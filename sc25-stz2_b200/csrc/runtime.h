@@ -189,6 +189,7 @@ void add_all_chunks(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint
 struct stz_context {
     int device = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t st_copy = nullptr;  // payload host->device copies of decode preparation
     std::unique_ptr<stz::ThreadPool> pool;
     // kernel profiling (stz_profile_*)
     struct ProfRec {
