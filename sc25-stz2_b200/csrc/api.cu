@@ -307,6 +307,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         }
         {
             KScope ks(ctx, k == K ? "k_level_encode[finest]" : "k_level_encode[coarser]");
+            a.side = ctx->side();
             launch_level_encode<T>(a, st);
         }
         cur = 1 - cur;
@@ -1059,6 +1060,7 @@ struct DecodePipe {
             a.learned = learned_args<T>(ps, k, p.d_models);
             {
                 KScope ks(ctx, k == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
+                a.side = ctx->side();
                 launch_level_decode<T>(a, ctx->st);
             }
             coarse = a.out;
@@ -1332,11 +1334,15 @@ stz_status stz_context_create(int device, stz_context** out)
     if (!c) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");
     c->device = device;
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) {
-        e = cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking);
-        if (e != cudaSuccess) cudaStreamDestroy(c->st);
-    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        if (c->st) cudaStreamDestroy(c->st);
+        if (c->st_copy) cudaStreamDestroy(c->st_copy);
+        if (c->st_side) cudaStreamDestroy(c->st_side);
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
         delete c;
         STZ_FAIL(STZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
@@ -1351,8 +1357,12 @@ void stz_context_destroy(stz_context* ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->st);
     cudaStreamSynchronize(ctx->st_copy);
+    cudaStreamSynchronize(ctx->st_side);
     cudaStreamDestroy(ctx->st);
     cudaStreamDestroy(ctx->st_copy);
+    cudaStreamDestroy(ctx->st_side);
+    cudaEventDestroy(ctx->ev_fork);
+    cudaEventDestroy(ctx->ev_join);
     delete ctx;
 }
 

@@ -500,8 +500,15 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel) : tile_bytes<T>();
     const uint64_t ns = shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
+    const bool par = a.side.st && interior && ns;
+    cudaStream_t ss = par ? a.side.st : st;
+    if (par) {
+        cudaEventRecord(a.side.fork, st);
+        cudaStreamWaitEvent(ss, a.side.fork, 0);
+    }
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
+        if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
         if (interior) {                                                                                            \
             auto kern = !learned                     ? k_level_encode<T, P, F, kLearnNone>                         \
                         : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
@@ -509,7 +516,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
             allow_smem(kern, sm);                                                                                  \
             kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned);                                       \
         }                                                                                                          \
-        if (ns) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);                \
+        if (ns && !par) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);        \
     } while (0)
     const bool finest = a.stride == 1;
     if (a.predictor == 1) {
@@ -520,6 +527,10 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
         else STZ_ENC(0, false);
     }
 #undef STZ_ENC
+    if (par) {
+        cudaEventRecord(a.side.join, ss);
+        cudaStreamWaitEvent(st, a.side.join, 0);
+    }
 }
 
 template <typename T>
@@ -534,8 +545,16 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel) : tile_bytes<T>();
     const uint64_t ns = shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
+    const bool par = a.side.st && interior && ns;
+    cudaStream_t ss = par ? a.side.st : st;
+    if (par) {
+        cudaEventRecord(a.side.fork, st);
+        cudaStreamWaitEvent(ss, a.side.fork, 0);
+    }
 #define STZ_DEC(P)                                                                                                 \
     do {                                                                                                           \
+        if (ns && par)                                                                                             \
+            k_level_decode_shell<T, P><<<gs, 256, 0, ss>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
         if (interior) {                                                                                            \
             auto kern = !learned                     ? k_level_decode<T, P, kLearnNone>                            \
                         : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \
@@ -543,11 +562,16 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
             allow_smem(kern, sm);                                                                                  \
             kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned);              \
         }                                                                                                          \
-        if (ns) k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
+        if (ns && !par)                                                                                            \
+            k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
     } while (0)
     if (a.predictor == 1) STZ_DEC(1);
     else STZ_DEC(0);
 #undef STZ_DEC
+    if (par) {
+        cudaEventRecord(a.side.join, ss);
+        cudaStreamWaitEvent(st, a.side.join, 0);
+    }
 }
 
 template <typename T>

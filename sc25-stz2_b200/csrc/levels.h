@@ -26,6 +26,7 @@ struct LevelEncodeArgs {
     T* decoded;             // decoded fine grid (2dx x 2dy x 2dz) or null on the finest level
     QuantParams qp;
     LearnedArgs<T> learned; // learned correction (model null: none)
+    SideStream side;        // boundary-shell kernel placement
 };
 
 template <typename T>
@@ -38,6 +39,7 @@ struct LevelDecodeArgs {
     const T* unpred_dense;
     T* out;  // fine grid (2dx x 2dy x 2dz)
     LearnedArgs<T> learned; // learned correction (model null: none)
+    SideStream side;        // boundary-shell kernel placement
 };
 
 template <typename T>

@@ -190,6 +190,9 @@ struct stz_context {
     int device = 0;
     cudaStream_t st = nullptr;
     cudaStream_t st_copy = nullptr;  // payload host->device copies of decode preparation
+    cudaStream_t st_side = nullptr;  // boundary-shell kernels of level launches (SideStream)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    stz::SideStream side() const { return stz::SideStream{st_side, ev_fork, ev_join}; }
     std::unique_ptr<stz::ThreadPool> pool;
     // kernel profiling (stz_profile_*)
     struct ProfRec {

@@ -132,6 +132,15 @@ __host__ __device__ inline uint32_t run_length(uint32_t slot, uint32_t D, uint32
     return slot < D - 1 ? slot + 2 : 1u << (slot - (D - 1) + LD + 1);
 }
 
+// Where a level launch runs its boundary-shell kernel: on `st`, concurrently
+// with the interior kernel (forked from and joined back to the caller's
+// stream with the two events); st null: after the interior kernel on the
+// caller's stream. The two kernels write disjoint points.
+struct SideStream {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
 // One CTA of the chunk coders: `count` chunks of stream `stream` whose ids are
 // chunk_ids[first .. first + count).
 struct CtaWork {
