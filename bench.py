@@ -513,7 +513,7 @@ def learned_bench(args, ctx, local, field):
 
 # ---- our arm ---------------------------------------------------------------------------
 def algorithmic_bytes(kernel: str, N: int, elem: int, K: int, raw_payload: int) -> float | None:
-    """Minimum HBM bytes one launch of `kernel` must move on the N-point field."""
+    """Minimum HBM bytes all launches of `kernel` in one step must move on the N-point field."""
     fine_syms = 7 * N // 8
     all_syms = sum(7 * (N >> (3 * j)) // 8 for j in range(K))
     if kernel == "k_level_encode[finest]":
@@ -645,6 +645,9 @@ def main():
     alg = algorithmic_bytes(dname, field.numel(), 4, info.n_levels, info.raw_payload_bytes)
     roof = None
     if alg is not None and dl:
+        # alg covers one step; a kernel launched several times per step (the
+        # coder's stream batches) moves alg / (launches per step) per launch
+        alg = alg * args.steps / dl
         per_launch_s = dms / dl / 1e3
         achieved = alg / per_launch_s / 1e9
         traffic = None
