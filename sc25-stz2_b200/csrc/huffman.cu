@@ -65,8 +65,9 @@ __global__ void k_expand_codebook(const StreamDesc* __restrict__ sd, const uint1
 }
 
 // ---- encode side: one warp per plane -----------------------------------------
-// Lane i of a warp owns the codes [a_i, b_i) of the plane (32 consecutive
-// segments of S = ceil(plane / 32) codes). A run of centre codes is coded by
+// Lane i of a group of W lanes (W = 32 for planes of 1024 codes and more,
+// fewer for smaller planes, see lanes_per_plane) owns the codes [a_i, b_i) of
+// the plane (W consecutive segments of S = ceil(plane / W) codes). A run of centre codes is coded by
 // the lane holding the literal that follows it, or, for a run that reaches
 // the plane's end, by the lane holding the plane's last code (`tail`): a
 // warp max-scan of the lanes' last literal positions gives every lane the
@@ -98,21 +99,53 @@ __device__ __forceinline__ void run_symbols(uint32_t r, uint32_t R, uint32_t bas
     else if (r) f(R);
 }
 
-// A warp's view of one plane.
+// Lanes per plane: the largest power of two <= plane / 32, at most 32, so a
+// lane holds about 32 codes; a warp takes 32 / W planes at a time (small
+// planes of the coarser levels would otherwise leave each lane a few codes
+// and the per-plane lane scans would dominate).
+__host__ __device__ inline uint32_t lanes_per_plane(uint32_t P)
+{
+    uint32_t w = 1;
+    while (w < 32 && 2 * w <= P / 32) w *= 2;
+    return w;
+}
+
+// A lane group's view of one plane (a group without a plane has an empty
+// segment but still takes part in the group's shuffles).
 struct LaneSeg {
     uint32_t P, a, b;  // plane size; this lane's codes [a, b)
+    uint32_t W, lane;  // lanes of the group; this lane's index in it
     bool vec;          // segments are whole 16-byte groups of 8 codes
 };
 
-__device__ __forceinline__ LaneSeg lane_seg(uint32_t C, const uint16_t* src)
+__device__ __forceinline__ LaneSeg lane_seg(uint32_t C, const uint16_t* src, uint32_t W, bool active)
 {
     LaneSeg g;
     g.P = C * C;
-    const uint32_t S = (g.P + 31) / 32, lane = threadIdx.x & 31;
-    g.a = min(lane * S, g.P);
-    g.b = min(g.a + S, g.P);
-    g.vec = g.P % 256 == 0 && ((uintptr_t)src & 15) == 0;
+    g.W = W;
+    g.lane = threadIdx.x & (W - 1);
+    const uint32_t S = (g.P + W - 1) / W;
+    g.a = active ? min(g.lane * S, g.P) : 0;
+    g.b = active ? min(g.a + S, g.P) : 0;
+    g.vec = g.P % (8 * W) == 0 && ((uintptr_t)src & 15) == 0;
     return g;
+}
+
+// Sum over a lane group of width W (a power of two).
+__device__ __forceinline__ uint32_t group_sum(uint32_t v, uint32_t W)
+{
+    for (uint32_t o = W >> 1; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Inclusive prefix sum over a lane group of width W.
+__device__ __forceinline__ uint32_t group_scan(uint32_t v, uint32_t W, uint32_t lane)
+{
+    for (uint32_t o = 1; o < W; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, v, o, W);
+        if (lane >= o) v += u;
+    }
+    return v;
 }
 
 // The lane's codes in order (streams without runs): f(q) for each.
@@ -178,7 +211,7 @@ struct RunLane {
         }
     }
 
-    // Literal masks, then a warp max-scan of the lanes' last literal
+    // Literal masks, then a group max-scan of the lanes' last literal
     // positions for lead.
     __device__ __forceinline__ void init(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t R)
     {
@@ -189,14 +222,12 @@ struct RunLane {
             if (p == g.a) lit0 = lit;
             if (lit) last = p + 32 - __clz(lit);
         }
-        const uint32_t lane = threadIdx.x & 31;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, last, o);
-            if (lane >= (uint32_t)o) last = max(last, v);
+        for (uint32_t o = 1; o < g.W; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, last, o, g.W);
+            if (g.lane >= o) last = max(last, v);
         }
-        uint32_t excl = __shfl_up_sync(0xffffffffu, last, 1);
-        if (lane == 0) excl = 0;
+        uint32_t excl = __shfl_up_sync(0xffffffffu, last, 1, g.W);
+        if (g.lane == 0) excl = 0;
         lead = g.a - excl;
         tail = g.a < g.b && g.b == g.P;
     }
@@ -229,19 +260,18 @@ struct RunLane {
     }
 };
 
-__device__ __forceinline__ uint32_t warp_sum(uint32_t v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Planes of a work item for this warp: CTA (x, y) of a grid with gridDim.y
-// slices takes every (8 * gridDim.y)-th plane, so short lists still spread
-// over many warps.
-#define STZ_WARP_PLANES(p, nplanes)                                                              \
-    for (uint32_t p = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5); p < (nplanes); \
-         p += (blockDim.x >> 5) * gridDim.y)
+// Planes of a work item for this lane group: warp i of the grid's
+// (blockDim.x / 32) * gridDim.y warps on an item takes its planes
+// [i * G, i * G + G), then every (warps * G)-th group of G after that (G =
+// 32 / W planes per warp); p is this group's plane, valid when active (else
+// pe, a valid plane of the same warp, stands in for reads).
+#define STZ_GROUP_PLANES(nplanes, W)                                                                      \
+    for (uint32_t base_ = (blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / (W));            \
+         base_ < (nplanes); base_ += (blockDim.x >> 5) * gridDim.y * (32 / (W)))
+#define STZ_GROUP_PLANE(nplanes, W)                                     \
+    const uint32_t p = base_ + (threadIdx.x & 31) / (W);               \
+    const bool active = p < (nplanes);                                 \
+    const uint32_t pe = active ? p : base_
 
 // Run-symbol counts of every listed plane (streams with runs).
 __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __restrict__ work,
@@ -256,13 +286,14 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
     if (s.run_n == 0) return;  // uniform per block
     if (threadIdx.x < kRunStats) cnt[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t C = s.C, P = C * C;
+    const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     uint32_t singles = 0;
-    STZ_WARP_PLANES(p, w.count * C)
+    STZ_GROUP_PLANES(np, W)
     {
-        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        STZ_GROUP_PLANE(np, W);
+        const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
         const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
-        const LaneSeg g = lane_seg(C, src);
+        const LaneSeg g = lane_seg(C, src, W, active);
         RunLane rl;
         rl.init(src, g, s.radius);
         rl.symbols(src, g, s, [&](uint32_t sym) {
@@ -270,7 +301,7 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
             else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
         });
     }
-    singles = warp_sum(singles);
+    singles = group_sum(singles, 32);
     if ((threadIdx.x & 31) == 0 && singles) atomicAdd(&cnt[0], singles);
     __syncthreads();
     if (threadIdx.x < kRunStats && cnt[threadIdx.x])
@@ -287,13 +318,14 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
 {
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
-    const uint32_t C = s.C, P = C * C;
+    const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
-    STZ_WARP_PLANES(p, w.count * C)
+    STZ_GROUP_PLANES(np, W)
     {
-        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        STZ_GROUP_PLANE(np, W);
+        const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
         const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
-        const LaneSeg g = lane_seg(C, src);
+        const LaneSeg g = lane_seg(C, src, W, active);
         uint32_t bits = 0;
         auto add = [&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; };
         if (s.run_n) {
@@ -303,8 +335,8 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
         } else {
             lane_codes(src, g, add);
         }
-        bits = warp_sum(bits);
-        if ((threadIdx.x & 31) == 0) sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
+        bits = group_sum(bits, W);
+        if (active && g.lane == 0) sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
     }
 }
 
@@ -391,13 +423,14 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
 {
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
-    const uint32_t C = s.C, P = C * C, lane = threadIdx.x & 31;
+    const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
-    STZ_WARP_PLANES(p, w.count * C)
+    STZ_GROUP_PLANES(np, W)
     {
-        const uint32_t c = chunk_ids[w.first + p / C], lz = p % C;
+        STZ_GROUP_PLANE(np, W);
+        const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
         const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
-        const LaneSeg g = lane_seg(C, src);
+        const LaneSeg g = lane_seg(C, src, W, active);
         RunLane rl;
         if (s.run_n) rl.init(src, g, s.radius);
         auto each = [&](auto&& f) {
@@ -406,20 +439,15 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
         };
         uint32_t bits = 0;
         each([&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; });
-        uint32_t off = bits;  // inclusive scan -> this lane's first bit in the plane
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, off, o);
-            if (lane >= (uint32_t)o) off += v;
-        }
-        const uint32_t nb = __shfl_sync(0xffffffffu, off, 31);
+        uint32_t off = group_scan(bits, W, g.lane);  // inclusive -> this lane's first bit in the plane
+        const uint32_t nb = __shfl_sync(0xffffffffu, off, W - 1, W);
         off -= bits;
-        if (nb == 0) continue;  // uniform per warp
         uint32_t* out = payload + s.word_base + chunk_word_off[s.chunk_base + c];
         const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
-        for (uint32_t x = (b0 >> 5) + 1 + lane; x < (b0 + nb - 1) >> 5; x += 32) out[x] = 0;
+        if (active && nb)
+            for (uint32_t x = (b0 >> 5) + 1 + g.lane; x < (b0 + nb - 1) >> 5; x += W) out[x] = 0;
         __syncwarp();
-        if (bits) {
+        if (active && bits) {
             const uint32_t pos = b0 + off;
             const uint32_t first_w = pos >> 5, last_w = (pos + bits - 1) >> 5;
             uint32_t wi = first_w;
@@ -762,10 +790,12 @@ __device__ void decode_plane_seq(const DecodeTables* __restrict__ t, const Strea
     }
 }
 
-// Decode plane lz of chunk c of stream s (one warp; Weissenberger & Schmidt,
-// "Massively parallel Huffman decoding on GPUs", ICPP 2018: speculative
-// decoding from equal bit slices, then resynchronisation). The plane's bits
-// [b0, b1) are cut into 32 slices; lane i decodes the codes that start in
+// Decode plane lz of chunk c of stream s (one group of W lanes, see
+// lanes_per_plane; Weissenberger & Schmidt, "Massively parallel Huffman
+// decoding on GPUs", ICPP 2018: speculative decoding from equal bit slices,
+// then resynchronisation). A group without a plane (active false) takes part
+// in the shuffles only. The plane's bits [b0, b1) are cut into W slices;
+// lane i decodes the codes that start in
 // its slice, beginning at the slice start. A lane whose start is not where
 // its left neighbour's last code ends decodes again from there, until no
 // start moves (lane i is exact after i rounds; codes resynchronise within a
@@ -774,22 +804,24 @@ __device__ void decode_plane_seq(const DecodeTables* __restrict__ t, const Strea
 // output. With run symbols the plane is first filled with the centre code,
 // so a lane writes only its literals. Output past the plane (a corrupt
 // stream) is dropped.
-__device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const StreamDesc& s, uint32_t c, uint32_t lz,
+__device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const StreamDesc& s, uint32_t W, bool active,
+                                  uint32_t c, uint32_t lz,
                                   const uint16_t* __restrict__ cb_sym, const uint32_t* __restrict__ sub_off,
                                   const uint64_t* __restrict__ chunk_word_off, const uint32_t* __restrict__ payload,
                                   uint16_t* __restrict__ codes)
 {
-    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & (W - 1);
     const uint32_t C = s.C, P = C * C;
     uint16_t* dst = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
     const bool vec = P % 8 == 0 && ((uintptr_t)dst & 15) == 0;
     const uint32_t R = s.radius, base = s.run_base, J = s.run_n;
     auto fill = [&](uint16_t v) {
+        if (!active) return;
         if (vec) {
             const uint32_t v2 = (uint32_t)v | ((uint32_t)v << 16);
-            for (uint32_t j = lane; j < P / 8; j += 32) reinterpret_cast<uint4*>(dst)[j] = make_uint4(v2, v2, v2, v2);
+            for (uint32_t j = lane; j < P / 8; j += W) reinterpret_cast<uint4*>(dst)[j] = make_uint4(v2, v2, v2, v2);
         } else {
-            for (uint32_t j = lane; j < P; j += 32) dst[j] = v;
+            for (uint32_t j = lane; j < P; j += W) dst[j] = v;
         }
     };
     if (s.n_used == 1) {
@@ -804,8 +836,8 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
     const uint32_t b0 = sub_off[s.sub_base + (size_t)c * C + lz];
     const uint32_t b1 = lz + 1 < C ? sub_off[s.sub_base + (size_t)c * C + lz + 1]
                                    : (uint32_t)(32 * (chunk_word_off[s.chunk_base + c + 1] - cw));
-    const uint32_t nb = b1 > b0 ? b1 - b0 : 0;
-    const uint32_t L = (nb + 31) / 32;
+    const uint32_t nb = active && b1 > b0 ? b1 - b0 : 0;
+    const uint32_t L = (nb + W - 1) / W;
     const uint32_t stop = b0 + min(nb, (lane + 1) * L);
     uint32_t D, LD;
     run_geometry(P, D, LD);
@@ -813,7 +845,7 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
     auto count = [&](uint32_t sym) { cnt += sym - base < J ? run_length(sym - base, D, LD) : 1u; };
     uint32_t end = decode_range(t, s, cb_sym, cb, start, stop, count);
     for (int round = 0; round < 32; ++round) {
-        uint32_t prev = __shfl_up_sync(0xffffffffu, end, 1);
+        uint32_t prev = __shfl_up_sync(0xffffffffu, end, 1, W);
         if (lane == 0) prev = b0;
         const bool moved = prev != start;
         if (!__any_sync(0xffffffffu, moved)) break;
@@ -823,13 +855,7 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
             end = decode_range(t, s, cb_sym, cb, start, stop, count);
         }
     }
-    uint32_t q = cnt;  // inclusive scan -> first output position
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, q, o);
-        if (lane >= (uint32_t)o) q += v;
-    }
-    q -= cnt;
+    uint32_t q = group_scan(cnt, W, lane) - cnt;  // first output position
     if (J) {
         fill((uint16_t)R);
         __syncwarp();
@@ -837,13 +863,13 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
             if (sym - base < J) {
                 q += run_length(sym - base, D, LD);
             } else {
-                if (q < P) dst[q] = (uint16_t)sym;
+                if (active && q < P) dst[q] = (uint16_t)sym;
                 ++q;
             }
         });
     } else {
         decode_range(t, s, cb_sym, cb, start, stop, [&](uint32_t sym) {
-            if (q < P) dst[q] = (uint16_t)sym;
+            if (active && q < P) dst[q] = (uint16_t)sym;
             ++q;
         });
     }
@@ -887,9 +913,13 @@ __global__ void __launch_bounds__(kDecodeThreads) k_decode(const CtaWork* __rest
                              chunk_word_off, payload, codes);
         return;
     }
-    STZ_WARP_PLANES(p, w.count * s.C)
-    decode_plane_warp(tabs + w.stream, s, chunk_ids[w.first + p / s.C], p % s.C, cb_sym, sub_off, chunk_word_off,
-                      payload, codes);
+    const uint32_t W = lanes_per_plane(s.C * s.C), np = w.count * s.C;
+    STZ_GROUP_PLANES(np, W)
+    {
+        STZ_GROUP_PLANE(np, W);
+        decode_plane_warp(tabs + w.stream, s, W, active, chunk_ids[w.first + pe / s.C], pe % s.C, cb_sym, sub_off,
+                          chunk_word_off, payload, codes);
+    }
 }
 
 // Persistent variant: a fixed grid walks the work list of a batch held in
@@ -912,9 +942,14 @@ __global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __
     for (uint32_t u = blockIdx.x; u < n * S; u += gridDim.x) {
         const CtaWork w = work[u / S];
         const StreamDesc s = sd[w.stream];
-        for (uint32_t p = (u % S) * nw + (threadIdx.x >> 5); p < w.count * s.C; p += nw * S)
-            decode_plane_warp(tabs + w.stream, s, chunk_ids[w.first + p / s.C], p % s.C, cb_sym, sub_off,
+        const uint32_t W = lanes_per_plane(s.C * s.C), G = 32 / W, np = w.count * s.C;
+        for (uint32_t base = ((u % S) * nw + (threadIdx.x >> 5)) * G; base < np; base += nw * S * G) {
+            const uint32_t p = base + (threadIdx.x & 31) / W;
+            const bool active = p < np;
+            const uint32_t pe = active ? p : base;
+            decode_plane_warp(tabs + w.stream, s, W, active, chunk_ids[w.first + pe / s.C], pe % s.C, cb_sym, sub_off,
                               chunk_word_off, payload, codes);
+        }
     }
 }
 
