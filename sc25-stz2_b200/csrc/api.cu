@@ -387,18 +387,27 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         STZ_CUDA(cudaGetLastError());
         STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
         STZ_CUDA(cudaMemcpyAsync(ctx->h_rstats.p, ctx->rstats.p, rstats.size() * 8, cudaMemcpyDeviceToHost, st));
+    }
+    lap.mark("run slots + run stats launch");
+    // the plain codebooks while the device counts the run symbols
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        const uint32_t* hw = h_out[s] ? fullh[s].data() : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
+        const int hn = h_out[s] ? R2 : wn, hb = h_out[s] ? 0 : wlo;
+        build_codebook(hw, hn, hb, syms[s], lens[s]);
+    });
+    lap.mark("plain codebooks");
+    if (any_runs) {
         STZ_CUDA(cudaStreamSynchronize(st));
         std::memcpy(rstats.data(), ctx->h_rstats.p, rstats.size() * 8);
     }
-    lap.mark("run slots + run stats");
+    lap.mark("run stats wait");
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+        if (!sd[s].run_n) return;
         const uint32_t* hw = h_out[s] ? fullh[s].data() : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
         const int hn = h_out[s] ? R2 : wn, hb = h_out[s] ? 0 : wlo;
         auto code_count = [&](uint32_t c) -> uint64_t {
             return c >= (uint32_t)hb && c < (uint32_t)(hb + hn) ? hw[c - hb] : 0;
         };
-        build_codebook(hw, hn, hb, syms[s], lens[s]);
-        if (!sd[s].run_n) return;
         // runs only where they shorten the Huffman payload (else the decoder
         // keeps its plain path): sum(count * length) of both codebooks
         uint64_t bits_plain = 0;
@@ -424,7 +433,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             sd[s].run_base = 0;
         }
     });
-    lap.mark("codebooks");
+    lap.mark("run codebooks");
     uint32_t cb_total = 0;
     for (int s = 0; s < nstreams; ++s) {
         sd[s].cb_off = cb_total;
