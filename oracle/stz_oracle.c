@@ -516,7 +516,24 @@ static void encode_stream(const uint16_t* codes, size_t n, int dx, int dy, int d
     bput(&es->hdr, unpred, (size_t)nunpred * elem);
     for (int c = 0; c < nch; ++c) bu32(&es->hdr, unpred_count[c]);
     for (int c = 0; c <= nch; ++c) bu64(&es->hdr, choff[c]);
-    for (size_t i = 0; i < (size_t)nch * C; ++i) bu32(&es->hdr, sub_off[i]);
+    /* plane table (version 4): per chunk the bit counts of its first C - 1
+     * planes (the first starts at bit 0), 2 bytes each when all fit, else 4 */
+    {
+        uint32_t mx = 0;
+        for (int c = 0; c < nch; ++c)
+            for (int lz = 1; lz < C; ++lz) {
+                const uint32_t d = sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1];
+                if (d > mx) mx = d;
+            }
+        const int width = mx < 65536 ? 2 : 4;
+        bu8(&es->hdr, (uint8_t)width);
+        for (int c = 0; c < nch; ++c)
+            for (int lz = 1; lz < C; ++lz) {
+                const uint32_t d = sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1];
+                if (width == 2) bu16(&es->hdr, (uint16_t)d);
+                else bu32(&es->hdr, d);
+            }
+    }
     es->words = w;
     es->nwords = nw;
     es->chunk_off = choff;
@@ -608,7 +625,7 @@ long long stzo_compress(const void* field, int nx, int ny, int nz, const stzo_pa
     /* learned correction of levels K-1 and K: container version 2 */
     const stzo_model* lm[64] = {0};
     uint32_t lf[64] = {0};
-    const int version = 3; /* per-level learned fields, run symbols */
+    const int version = 4; /* per-level learned fields, run symbols, plane bit counts */
     for (int i = 0; i < 2; ++i) {
         const int k = h.K - 1 + i;
         if (k >= 1 && p->model[i] && (p->learned_flags[i] & 0x7fu)) {
@@ -758,7 +775,7 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
     rget(&r, mg, 8);
     if (r.err || memcmp(mg, kMagic, 8) != 0) return -10;
     const uint32_t version = ru32(&r);
-    if (version < 1 || version > 3) return -11;
+    if (version < 1 || version > 4) return -11;
     ps->version = (int)version;
     hdr_t* h = &ps->h;
     h->dtype = (int)ru32(&r);
@@ -872,7 +889,30 @@ static int decode_stream(const uint8_t* st, const parsed_t* ps, int k, int b, ui
     uint64_t* choff = (uint64_t*)malloc(8 * ((size_t)nch + 1));
     for (int c = 0; c <= nch; ++c) choff[c] = ru64(&r);
     uint32_t* sub = (uint32_t*)malloc(4 * (size_t)nch * C);
-    for (size_t i = 0; i < (size_t)nch * C; ++i) sub[i] = ru32(&r);
+    if (ps->version >= 4) {
+        uint8_t width = 0;
+        rget(&r, &width, 1);
+        if (width != 2 && width != 4) rc_hdr_bad = 1;
+        for (int c = 0; c < nch; ++c) {
+            uint64_t acc = 0;
+            sub[(size_t)c * C] = 0;
+            for (int lz = 1; lz < C; ++lz) {
+                uint32_t d = 0;
+                if (width == 2) {
+                    uint16_t d16 = 0;
+                    rget(&r, &d16, 2);
+                    d = d16;
+                } else {
+                    d = ru32(&r);
+                }
+                acc += d;
+                if (acc > 0xffffffffull) rc_hdr_bad = 1;
+                sub[(size_t)c * C + lz] = (uint32_t)acc;
+            }
+        }
+    } else {
+        for (size_t i = 0; i < (size_t)nch * C; ++i) sub[i] = ru32(&r);
+    }
     int rc = (r.err || rc_hdr_bad) ? -23 : 0;
     /* canonical decode tables: count / first code / first index per length */
     uint32_t* code = (uint32_t*)malloc(4 * (size_t)(nu + 1));

@@ -589,7 +589,10 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             for (cudaEvent_t x : e) cudaEventDestroy(x);
         }
     } ev;
-    ev.e.assign(ngroups, nullptr);
+    // ev.e[gi]: group gi's words are on the host; ev.e[ngroups + gi]: its
+    // encode is done. The copies run on the context's copy stream, so group
+    // gi's copy overlaps group gi + 1's encode.
+    ev.e.assign(2 * ngroups, nullptr);
     for (auto& x : ev.e) STZ_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     for (size_t gi = 0; gi < ngroups; ++gi) {
         {
@@ -598,14 +601,16 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
                           ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
                           ctx->payload.as<uint32_t>(), st);
         }
+        STZ_CUDA(cudaEventRecord(ev.e[ngroups + gi], st));
+        STZ_CUDA(cudaStreamWaitEvent(ctx->st_copy, ev.e[ngroups + gi], 0));
         // the group's words straight from the stream buffers to their place in
         // the packed host payload (one copy per piece)
         for (const Piece& pc : pieces[gi])
             if (pc.w1 > pc.w0)
                 STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.as<uint32_t>() + meta[nstreams + pc.s] + pc.w0,
                                          ctx->payload.as<uint32_t>() + sd[pc.s].word_base + pc.w0,
-                                         (pc.w1 - pc.w0) * 4, cudaMemcpyDeviceToHost, st));
-        STZ_CUDA(cudaEventRecord(ev.e[gi], st));
+                                         (pc.w1 - pc.w0) * 4, cudaMemcpyDeviceToHost, ctx->st_copy));
+        STZ_CUDA(cudaEventRecord(ev.e[gi], ctx->st_copy));
     }
     STZ_CUDA(cudaGetLastError());
 
@@ -653,7 +658,11 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         [&](size_t gi) {
             if (cudaEventSynchronize(ev.e[gi]) != cudaSuccess) ev_err = 1;
         });
-    if (ev_err) STZ_CUDA(cudaStreamSynchronize(st));  // reports the device error
+    if (ev_err) {  // reports the device error
+        STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));
+        STZ_CUDA(cudaStreamSynchronize(st));
+    }
+    STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));  // every group's copy (the payload buffer is reused next call)
     lap.mark("encode + copy + zstd");
     auto* so = new (std::nothrow) stz_stream();
     if (!so) STZ_FAIL(STZ_ERR_NOMEM, "out of host memory");

@@ -365,6 +365,8 @@ struct Writer {
         const uint8_t* c = (const uint8_t*)p;
         b.insert(b.end(), c, c + n);
     }
+    void u8(uint8_t v) { put(&v, 1); }
+    void u16(uint16_t v) { put(&v, 2); }
     void u32(uint32_t v) { put(&v, 4); }
     void i32(int32_t v) { put(&v, 4); }
     void u64(uint64_t v) { put(&v, 8); }
@@ -385,6 +387,8 @@ struct Reader {
         std::memcpy(dst, p + pos, k);
         pos += k;
     }
+    uint8_t u8() { uint8_t v; get(&v, 1); return v; }
+    uint16_t u16() { uint16_t v; get(&v, 2); return v; }
     uint32_t u32() { uint32_t v; get(&v, 4); return v; }
     int32_t i32() { int32_t v; get(&v, 4); return v; }
     uint64_t u64() { uint64_t v; get(&v, 8); return v; }
@@ -408,7 +412,20 @@ void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const 
     w.put(unpred, n_unpred * elem);
     w.put(unpred_count, 4 * (size_t)nchunks);
     w.put(chunk_word_off, 8 * ((size_t)nchunks + 1));
-    w.put(sub_off, 4 * (size_t)nchunks * C);
+    // plane table (version 4): per chunk the bit counts of its first C - 1
+    // planes (the first plane starts at bit 0), 2 bytes each when all fit
+    uint32_t mx = 0;
+    for (int c = 0; c < nchunks; ++c)
+        for (int lz = 1; lz < C; ++lz)
+            mx = std::max(mx, sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1]);
+    const uint8_t width = mx < 65536 ? 2 : 4;
+    w.u8(width);
+    for (int c = 0; c < nchunks; ++c)
+        for (int lz = 1; lz < C; ++lz) {
+            const uint32_t d = sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1];
+            if (width == 2) w.u16((uint16_t)d);
+            else w.u32(d);
+        }
 }
 
 bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_t elem, int version,
@@ -436,7 +453,22 @@ bool parse_stream_header(const uint8_t* raw, size_t n, int nchunks, int C, size_
     out.chunk_word_off.resize((size_t)nchunks + 1);
     r.get(out.chunk_word_off.data(), 8 * ((size_t)nchunks + 1));
     out.sub_off.resize((size_t)nchunks * C);
-    r.get(out.sub_off.data(), 4 * (size_t)nchunks * C);
+    if (version >= 4) {
+        // plane bit counts (all planes of a chunk but its last) -> offsets
+        const uint8_t width = r.u8();
+        if (width != 2 && width != 4) return false;
+        for (int c = 0; c < nchunks && !r.err; ++c) {
+            uint64_t acc = 0;
+            out.sub_off[(size_t)c * C] = 0;
+            for (int lz = 1; lz < C; ++lz) {
+                acc += width == 2 ? r.u16() : r.u32();
+                if (acc > 0xffffffffull) return false;
+                out.sub_off[(size_t)c * C + lz] = (uint32_t)acc;
+            }
+        }
+    } else {
+        r.get(out.sub_off.data(), 4 * (size_t)nchunks * C);
+    }
     if (r.err || r.pos != n) return false;
     for (uint8_t l : out.len)
         if (l > kMaxCodeLen) return false;
@@ -461,7 +493,7 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     r.get(mg, 8);
     if (r.err || std::memcmp(mg, kMagic, 8) != 0) return "not an STZ-B200 stream (bad magic)";
     const uint32_t version = r.u32();
-    if (version < 1 || version > 3) return "unsupported stream version";
+    if (version < 1 || version > 4) return "unsupported stream version";
     out.version = (int)version;
     FileHeader& h = out.h;
     h.dtype = (int)r.u32();
@@ -621,7 +653,7 @@ Bytes ContainerWriter::finish(const void* coarsest, const std::vector<LevelDir>&
     std::vector<uint8_t> dir;
     Writer w{dir};
     w.put(kMagic, 8);
-    w.u32(3);  // per-level learned-correction fields, run symbols
+    w.u32(4);  // per-level learned-correction fields, run symbols, plane bit counts
     w.u32((uint32_t)h.dtype);
     w.u32((uint32_t)h.predictor);
     w.u32((uint32_t)h.nx);

@@ -127,7 +127,7 @@ struct LevelDir {
 bool learned_model_valid(const LearnedModel& m);
 
 struct ParsedStream {
-    int version = 0;  // 1: plain, 2: learned fields, 3: learned fields and run symbols
+    int version = 0;  // 1: plain, 2: learned fields, 3: + run symbols, 4: + plane bit counts (not offsets)
     FileHeader h;
     size_t coarsest_off = 0;
     std::vector<LevelDir> lv;  // index 1..K (0 unused)

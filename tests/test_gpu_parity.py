@@ -316,7 +316,7 @@ def test_plain_cubic_kernel_matches_reference_golden(ctx, golden, suf):
         assert np.array_equal(bits(out), bits(diff[b])), b
 
 
-# ---- run symbols (container version 3) ---------------------------------------------
+# ---- run symbols (container version 3 and later) ---------------------------------
 @pytest.mark.parametrize("case", ["constant", "noise_full_range", "ramp_spikes", "tiny_chunks"])
 def test_run_symbol_streams_match_oracle(ctx, case):
     """Streams whose planes are one long run (single-symbol codebooks of run
@@ -341,7 +341,7 @@ def test_run_symbol_streams_match_oracle(ctx, case):
         kw = dict(chunk_high=2, chunk_low=1)
     s = ctx.compress(f, eb=rel, eb_mode="rel", radius=radius, **kw)
     b = s.to_bytes()
-    assert int.from_bytes(b[8:12], "little") == 3
+    assert int.from_bytes(b[8:12], "little") == 4
     assert b == po.compress(f, s.info().eb, radius=radius, **kw)
     out = ctx.decompress(s)
     assert np.array_equal(bits(out), bits(po.decompress(b)))
@@ -352,3 +352,38 @@ def test_run_symbol_streams_match_oracle(ctx, case):
         box = ctx.decompress_box(s, lo, hi)
         want = out[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
         assert np.array_equal(bits(box), bits(want)), (lo, hi)
+
+
+# ---- plane tables (container version 4) ----------------------------------------------
+def test_plane_table_layouts_decode_alike(ctx):
+    """The same stream with its plane tables as version-3 offsets, version-4
+    2-byte counts (what the writer chose) and version-4 4-byte counts decodes
+    to the same field, full and as a box."""
+    from stream_tools import rewrite_plane_tables
+
+    f = make_field("grf", (64, 64, 64), np.float32, 11)
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel")
+    b = s.to_bytes()
+    assert b == po.compress(f, s.info().eb)
+    want = ctx.decompress(s)
+    lo, hi = (5, 9, 13), (40, 33, 50)
+    wbox = ctx.decompress_box(s, lo, hi)
+    for v, w in ((3, 4), (4, 4)):
+        b2 = rewrite_plane_tables(b, v, w)
+        s2 = ctx.parse(b2)
+        assert np.array_equal(bits(ctx.decompress(s2)), bits(want)), (v, w)
+        assert np.array_equal(bits(ctx.decompress_box(s2, lo, hi)), bits(wbox)), (v, w)
+
+
+def test_wide_planes_use_four_byte_counts(ctx):
+    """128^3 marker chunks of noise: planes of 16384 codes need more than
+    65535 bits, so the writer stores 4-byte plane counts; the stream is the
+    oracle's and decodes to it."""
+    rng = np.random.default_rng(5)
+    f = rng.normal(0, 1, (256, 256, 256)).astype(np.float32)
+    kw = dict(chunk_high=128, chunk_low=16)
+    s = ctx.compress(f, eb=1e-4, eb_mode="rel", **kw)
+    b = s.to_bytes()
+    assert b == po.compress(f, s.info().eb, **kw)
+    out = ctx.decompress(s)
+    assert np.array_equal(bits(out), bits(po.decompress(b)))

@@ -123,3 +123,19 @@ def test_plain_cubic_predictor_matches_reference_golden(golden, suf):
         P = np.array([[[fn(b, po._p(ref), x, y, z, dx, dy, dz) for x in range(dx)] for y in range(dy)]
                       for z in range(dz)], dtype=ref.dtype)
         assert np.array_equal((sub - P).view(np.uint8), diff[b].view(np.uint8)), b
+
+
+def test_plane_table_layouts_oracle():
+    """Version-3 plane offsets and version-4 plane counts of either width
+    decode alike in the oracle (the writer emits version 4, 2-byte counts
+    here)."""
+    from stream_tools import rewrite_plane_tables
+
+    rng = np.random.default_rng(9)
+    f = np.cumsum(rng.normal(0, 1, (64, 64, 64)), axis=2).astype(np.float32)
+    b = po.compress(f, po.pointwise_eb(f, 1e-3))
+    assert int.from_bytes(b[8:12], "little") == 4
+    want = po.decompress(b)
+    for v, w in ((3, 4), (4, 2), (4, 4)):
+        got = po.decompress(rewrite_plane_tables(b, v, w))
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (v, w)
