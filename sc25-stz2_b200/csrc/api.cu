@@ -879,6 +879,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
     } ev;
     auto sync_both = [&]() {
         cudaStreamSynchronize(ctx->st_copy);
+        cudaStreamSynchronize(ctx->st_dec);
         cudaStreamSynchronize(ctx->st);
     };
     int s0 = 0;
@@ -898,13 +899,13 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
         if (ce == cudaSuccess) ev.e.push_back(e);
         if (ce == cudaSuccess) ce = cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st_copy);
         if (ce == cudaSuccess) ce = cudaEventRecord(e, ctx->st_copy);
-        if (ce == cudaSuccess && (on_batch || s1 == nstreams)) ce = cudaStreamWaitEvent(ctx->st, e, 0);
+        if (ce == cudaSuccess && !on_batch && s1 == nstreams) ce = cudaStreamWaitEvent(ctx->st, e, 0);
         if (ce != cudaSuccess) {
             sync_both();
             STZ_CUDA(ce);
         }
         if (on_batch) {
-            const stz_status st = (*on_batch)(s0, s1);
+            const stz_status st = (*on_batch)(s0, s1, e);
             if (st != STZ_OK) {
                 sync_both();
                 return st;
@@ -914,6 +915,7 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
     }
     lap.mark("payload frames + h2d");
     STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));  // the pinned staging buffer is reused by the next call
+    STZ_CUDA(cudaStreamSynchronize(ctx->st_dec));
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
     lap.mark("host->device");
     return STZ_OK;
@@ -996,10 +998,24 @@ struct DecodePipe {
     size_t o_w = 0, o_i = 0, o_u = 0;
     int next_level = 1, cur = 0;
     const T* coarse = nullptr;
+    std::vector<cudaEvent_t> events;  // ordering between ctx->st and ctx->st_dec
 
     DecodePipe(stz_context* c, const stz_stream* st, const Prepared& pp, int k, T* o)
         : ctx(c), s(st), p(pp), kdec(k), out(o)
     {
+    }
+    ~DecodePipe()
+    {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+    }
+    cudaError_t record(cudaStream_t on, cudaStream_t waiter)
+    {
+        cudaEvent_t e = nullptr;
+        cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (r != cudaSuccess) return r;
+        events.push_back(e);
+        r = cudaEventRecord(e, on);
+        return r == cudaSuccess ? cudaStreamWaitEvent(waiter, e, 0) : r;
     }
 
     // Work lists of every stream, uploaded once; buffers sized.
@@ -1042,29 +1058,37 @@ struct DecodePipe {
         STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
         STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
         coarse = p.coarsest->as<T>();
+        // the entropy decodes (ctx->st_dec) follow everything enqueued on
+        // ctx->st so far: tables, coarsest grid, work lists, earlier calls
+        STZ_CUDA(record(ctx->st, ctx->st_dec));
         planned = true;
         return STZ_OK;
     }
 
-    // Streams [s0, s1) have their payload on the device (in stream order).
-    stz_status batch(int s0, int s1)
+    // Streams [s0, s1): their payload is on the device once `copied` has
+    // completed (null: already). Entropy decode on ctx->st_dec, so it runs
+    // beside the level decodes of earlier batches on ctx->st.
+    stz_status batch(int s0, int s1, cudaEvent_t copied)
     {
         s1 = std::min(s1, 7 * kdec);
         if (s0 >= s1) return STZ_OK;
         if (!planned) STZ_TRY(plan());
+        cudaStream_t sd = ctx->st_dec;
+        if (copied) STZ_CUDA(cudaStreamWaitEvent(sd, copied, 0));
         const uint8_t* dw = ctx->work.as<uint8_t>();
         const size_t w0 = wfirst[s0], w1 = wfirst[s1], u0 = ufirst[s0], u1 = ufirst[s1];
         if (w1 > w0) {
-            KScope ks(ctx, "k_decode");
+            KScope ks(ctx, "k_decode", 1, sd);
             launch_decode((const CtaWork*)(dw + o_w) + w0, (const uint32_t*)(dw + o_i), (int)(w1 - w0), p.d_sd,
-                          p.d_sym, p.d_tables, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), ctx->st);
+                          p.d_sym, p.d_tables, p.d_sub, p.d_choff, p.d_payload, ctx->codes.as<uint16_t>(), sd);
         }
         if (u1 > u0) {
-            KScope ks(ctx, "k_unpred_move");
+            KScope ks(ctx, "k_unpred_move", 1, sd);
             launch_unpred_move<T>(false, (const UnpredWork*)(dw + o_u) + u0, (int)(u1 - u0), p.d_sd,
-                                  ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p.d_ulist, ctx->st);
+                                  ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p.d_ulist, sd);
         }
         const ParsedStream& ps = s->dir;
+        if (next_level <= kdec && 7 * next_level <= s1) STZ_CUDA(record(sd, ctx->st));
         for (; next_level <= kdec && 7 * next_level <= s1; ++next_level) {
             const int k = next_level;
             LevelDecodeArgs<T> a;
@@ -1103,7 +1127,7 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
     DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
     STZ_TRY(pipe.plan());
     STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned work-list buffer is free for the caller
-    return pipe.batch(0, 7 * kdec);
+    return pipe.batch(0, 7 * kdec, nullptr);
 }
 
 template <typename T>
@@ -1127,7 +1151,7 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
         // each batch of streams is decoded while the host zstd-decodes the next
         Trace t("decompress: prepare + decode");
         DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
-        const BatchFn fn = [&](int s0, int s1) { return pipe.batch(s0, s1); };
+        const BatchFn fn = [&](int s0, int s1, cudaEvent_t copied) { return pipe.batch(s0, s1, copied); };
         STZ_TRY(prepare(ctx, s, kdec, p, &fn));
     }
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
@@ -1354,12 +1378,14 @@ stz_status stz_context_create(int device, stz_context** out)
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st_dec, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         if (c->st) cudaStreamDestroy(c->st);
         if (c->st_copy) cudaStreamDestroy(c->st_copy);
         if (c->st_side) cudaStreamDestroy(c->st_side);
+        if (c->st_dec) cudaStreamDestroy(c->st_dec);
         if (c->ev_fork) cudaEventDestroy(c->ev_fork);
         delete c;
         STZ_FAIL(STZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
@@ -1376,6 +1402,8 @@ void stz_context_destroy(stz_context* ctx)
     cudaStreamSynchronize(ctx->st);
     cudaStreamSynchronize(ctx->st_copy);
     cudaStreamSynchronize(ctx->st_side);
+    cudaStreamSynchronize(ctx->st_dec);
+    cudaStreamDestroy(ctx->st_dec);
     cudaStreamDestroy(ctx->st);
     cudaStreamDestroy(ctx->st_copy);
     cudaStreamDestroy(ctx->st_side);

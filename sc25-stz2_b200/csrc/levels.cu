@@ -200,17 +200,31 @@ __global__ void k_minmax(const T* __restrict__ p, size_t n, double* out)
 {
     T lo = T(INFINITY), hi = T(-INFINITY);
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    for (; i + 3 * stride < n; i += 4 * stride) {
-        const T a = __ldg(p + i), b = __ldg(p + i + stride), c = __ldg(p + i + 2 * stride), d = __ldg(p + i + 3 * stride);
-        lo = fmin(lo, fmin(fmin(a, b), fmin(c, d)));
-        hi = fmax(hi, fmax(fmax(a, b), fmax(c, d)));
-    }
-    for (; i < n; i += stride) {
-        const T a = __ldg(p + i);
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    auto take = [&](T a) {
         lo = fmin(lo, a);
         hi = fmax(hi, a);
+    };
+    // elements before the first 16-byte boundary, then 16-byte vectors (four
+    // in flight per thread), then the tail
+    constexpr size_t V = 16 / sizeof(T);
+    const size_t h = min(n, ((16 - ((uintptr_t)p & 15)) & 15) / sizeof(T));
+    const size_t nv = (n - h) / V;
+    const uint4* __restrict__ pv = reinterpret_cast<const uint4*>(p + h);
+    auto take4 = [&](const uint4& q) {
+        const T* e = reinterpret_cast<const T*>(&q);
+#pragma unroll
+        for (size_t k = 0; k < V; ++k) take(e[k]);
+    };
+    size_t i = tid;
+    for (; i + 3 * stride < nv; i += 4 * stride) {
+        const uint4 a = __ldg(pv + i), b = __ldg(pv + i + stride), c = __ldg(pv + i + 2 * stride),
+                    d = __ldg(pv + i + 3 * stride);
+        take4(a), take4(b), take4(c), take4(d);
     }
+    for (; i < nv; i += stride) take4(__ldg(pv + i));
+    for (size_t j = tid; j < h; j += stride) take(__ldg(p + j));
+    for (size_t j = h + nv * V + tid; j < n; j += stride) take(__ldg(p + j));
     for (int o = 16; o; o >>= 1) {
         lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
         hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));

@@ -191,6 +191,7 @@ struct stz_context {
     cudaStream_t st = nullptr;
     cudaStream_t st_copy = nullptr;  // payload host->device copies of decode preparation
     cudaStream_t st_side = nullptr;  // boundary-shell kernels of level launches (SideStream)
+    cudaStream_t st_dec = nullptr;   // entropy decoding of full decodes, beside the level decodes
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     stz::SideStream side() const { return stz::SideStream{st_side, ev_fork, ev_join}; }
     std::unique_ptr<stz::ThreadPool> pool;
@@ -287,20 +288,22 @@ namespace stz {
 struct KScope {
     stz_context* c;
     cudaEvent_t b = nullptr;
-    KScope(stz_context* ctx, const char* name, int launches = 1) : c(ctx)
+    cudaStream_t s;
+    KScope(stz_context* ctx, const char* name, int launches = 1, cudaStream_t on = nullptr)
+        : c(ctx), s(on ? on : ctx->st)
     {
         c->prof_launches[c->prof_slot(name)] += (uint64_t)launches;
         if (c->prof_on) {
             if (c->pending.size() > 4096) c->flush_prof();
             cudaEvent_t a = c->event();
             b = c->event();
-            cudaEventRecord(a, c->st);
+            cudaEventRecord(a, s);
             c->pending.push_back({name, a, b});
         }
     }
     ~KScope()
     {
-        if (b) cudaEventRecord(b, c->st);
+        if (b) cudaEventRecord(b, s);
     }
 };
 
@@ -312,10 +315,12 @@ size_t dtype_size(int dtype);
 stz_status enter(stz_context* ctx);
 // Parse stream headers, lay out and upload the tables and payload of levels
 // 1..kmax (zstd frames decoded on the host pool) and the coarsest grid.
-// on_batch(s0, s1), when given, runs after the copy of the payload of streams
-// [s0, s1) is enqueued on ctx->st (batches in stream order, ending at the
-// level boundaries below kmax); prepare returns once the stream is idle.
-using BatchFn = std::function<stz_status(int, int)>;
+// on_batch(s0, s1, copied), when given, runs after the copy of the payload of
+// streams [s0, s1) is enqueued (batches in stream order, ending at the level
+// boundaries below kmax); `copied` is the event after that copy, and the
+// callback orders its own work after it. Without on_batch, ctx->st waits for
+// every copy. prepare returns once the context's streams are idle.
+using BatchFn = std::function<stz_status(int, int, cudaEvent_t)>;
 stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p, const BatchFn* on_batch = nullptr);
 // Entropy-decode the listed chunks into ctx->codes (and scatter their
 // unpredictable values into ctx->unpred_dense).
