@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
         uint64_t words = 0;
         if (c < s.nchunks) {
             uint32_t acc = 0;
-for (uint32_t lz = 0; lz < C; ++lz) {
+            for (uint32_t lz = 0; lz < C; ++lz) {
                 const size_t k = s.sub_base + (size_t)c * C + lz;
                 sub_off[k] = acc;
                 acc += sub_bits[k];
@@ -388,7 +388,7 @@ for (uint32_t lz = 0; lz < C; ++lz) {
         if (c < s.nchunks) {
             chunk_word_off[s.chunk_base + c] = pre;
             uint32_t* w = payload + s.word_base + pre;
-for (uint32_t lz = 0; lz < C; ++lz) {
+            for (uint32_t lz = 0; lz < C; ++lz) {
                 const size_t k = s.sub_base + (size_t)c * C + lz;
                 const uint32_t b0 = sub_off[k], nb = sub_bits[k];
                 if (nb) {
