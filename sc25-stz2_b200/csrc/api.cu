@@ -334,13 +334,25 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     // codebooks
     std::vector<std::vector<uint16_t>> syms(nstreams);
     std::vector<std::vector<uint8_t>> lens(nstreams);
-    std::vector<std::vector<uint32_t>> fullh(nstreams);
-    for (int s = 0; s < nstreams; ++s)
-        if (h_out[s]) {
-            fullh[s].resize(R2);
-            STZ_CUDA(cudaMemcpy(fullh[s].data(), ctx->hist.as<uint32_t>() + (size_t)s * R2, (size_t)R2 * 4,
-                                cudaMemcpyDeviceToHost));
+    // full histograms of the streams with codes outside the window: one
+    // pinned buffer, asynchronous copies, one wait
+    std::vector<const uint32_t*> fullh(nstreams, nullptr);
+    {
+        size_t nfull = 0;
+        for (int s = 0; s < nstreams; ++s) nfull += h_out[s] ? 1 : 0;
+        if (nfull) {
+            STZ_CUDA(ctx->h_fullh.ensure(nfull * (size_t)R2 * 4));
+            size_t k = 0;
+            for (int s = 0; s < nstreams; ++s)
+                if (h_out[s]) {
+                    uint32_t* dst = ctx->h_fullh.as<uint32_t>() + k++ * (size_t)R2;
+                    STZ_CUDA(cudaMemcpyAsync(dst, ctx->hist.as<uint32_t>() + (size_t)s * R2, (size_t)R2 * 4,
+                                             cudaMemcpyDeviceToHost, st));
+                    fullh[s] = dst;
+                }
+            STZ_CUDA(cudaStreamSynchronize(st));
         }
+    }
     lap.mark("full histograms");
     std::vector<StreamDesc> sd = g.sd;
     // work list over every chunk of every stream
@@ -358,7 +370,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     for (int s = 0; s < nstreams; ++s) {
         const uint32_t* hw = ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
         auto count = [&](uint32_t c) -> uint64_t {
-            if (h_out[s]) return fullh[s][c];
+            if (h_out[s]) return (uint64_t)fullh[s][c];
             return (c >= (uint32_t)wlo && c < (uint32_t)(wlo + wn)) ? hw[c - wlo] : 0;
         };
         sd[s].run_n = (uint32_t)run_slots(count, R2, (int)(sd[s].C * sd[s].C), sd[s].run_base);
@@ -391,7 +403,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     lap.mark("run slots + run stats launch");
     // the plain codebooks while the device counts the run symbols
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
-        const uint32_t* hw = h_out[s] ? fullh[s].data() : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
+        const uint32_t* hw = h_out[s] ? fullh[s] : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
         const int hn = h_out[s] ? R2 : wn, hb = h_out[s] ? 0 : wlo;
         build_codebook(hw, hn, hb, syms[s], lens[s]);
     });
@@ -403,7 +415,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     lap.mark("run stats wait");
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
         if (!sd[s].run_n) return;
-        const uint32_t* hw = h_out[s] ? fullh[s].data() : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
+        const uint32_t* hw = h_out[s] ? fullh[s] : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
         const int hn = h_out[s] ? R2 : wn, hb = h_out[s] ? 0 : wlo;
         auto code_count = [&](uint32_t c) -> uint64_t {
             return c >= (uint32_t)hb && c < (uint32_t)(hb + hn) ? hw[c - hb] : 0;
@@ -649,14 +661,17 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     lap.mark("stream headers");
     ContainerWriter cw(h, parts, *ctx->pool);
     std::atomic<int> ev_err{0};
+    // zstd groups: every stream header first (nothing to wait for), then
+    // the payload of encode group g after its copy (event g)
     cw.compress_groups(
-        ngroups,
+        ngroups + 1,
         [&](size_t st_, int layer) -> size_t {
-            if ((int)st_ < fin0 || layer < 0) return 0;  // coarser levels and every header: group 0
-            return 1 + (size_t)(layer / lpg);
+            if (layer < 0) return 0;
+            if ((int)st_ < fin0) return 1;  // coarser levels: encode group 0
+            return 2 + (size_t)(layer / lpg);
         },
-        [&](size_t gi) {
-            if (cudaEventSynchronize(ev.e[gi]) != cudaSuccess) ev_err = 1;
+        [&](size_t g) {
+            if (g > 0 && cudaEventSynchronize(ev.e[g - 1]) != cudaSuccess) ev_err = 1;
         });
     if (ev_err) {  // reports the device error
         STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));

@@ -366,7 +366,6 @@ struct Writer {
         b.insert(b.end(), c, c + n);
     }
     void u8(uint8_t v) { put(&v, 1); }
-    void u16(uint16_t v) { put(&v, 2); }
     void u32(uint32_t v) { put(&v, 4); }
     void i32(int32_t v) { put(&v, 4); }
     void u64(uint64_t v) { put(&v, 8); }
@@ -420,11 +419,19 @@ void append_stream_header(std::vector<uint8_t>& out, const uint16_t* sym, const 
             mx = std::max(mx, sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1]);
     const uint8_t width = mx < 65536 ? 2 : 4;
     w.u8(width);
+    const size_t at = out.size(), m = (size_t)nchunks * (C > 0 ? C - 1 : 0);
+    out.resize(at + m * width);
+    uint8_t* dst = out.data() + at;
     for (int c = 0; c < nchunks; ++c)
         for (int lz = 1; lz < C; ++lz) {
             const uint32_t d = sub_off[(size_t)c * C + lz] - sub_off[(size_t)c * C + lz - 1];
-            if (width == 2) w.u16((uint16_t)d);
-            else w.u32(d);
+            if (width == 2) {
+                const uint16_t v = (uint16_t)d;
+                std::memcpy(dst, &v, 2);
+            } else {
+                std::memcpy(dst, &d, 4);
+            }
+            dst += width;
         }
 }
 

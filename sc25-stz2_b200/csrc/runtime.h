@@ -245,7 +245,7 @@ struct stz_context {
     stz::DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
         tiles, models, eval, rstats, gwork;
-    stz::PinBuf h_hist, h_meta, h_meta2, h_payload, h_stage, h_io, h_small, h_rstats;
+    stz::PinBuf h_hist, h_meta, h_meta2, h_payload, h_stage, h_io, h_small, h_rstats, h_fullh;
     // device buffers lent to one-off decodes
     stz::DevBuf p_stage, p_coarsest, p_base;
     void borrow(stz::Prepared& p)
