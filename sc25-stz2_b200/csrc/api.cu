@@ -533,7 +533,67 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(ht + t_sub, ctx->sub_off.p, g.total_sub * 4, cudaMemcpyDeviceToHost, st));
     if (total_unpred)
         STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaStreamSynchronize(st));
+    struct Events {
+        std::vector<cudaEvent_t> e;
+        ~Events()
+        {
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } ev;
+    // Encode, pack and copy back in groups: every stream of the coarser
+    // levels, then the finest level's streams in two halves of their chunk
+    // z-layers (all 7 streams per group, so every launch still fills the
+    // device); the host zstd-compresses a group's frames while the device
+    // encodes the next (one, two, four or eight finest groups measured within
+    // noise of each other once payload frames skip zstd; two is the fewest
+    // launches that still overlap the copy back). The encodes are enqueued
+    // before the host waits for the tables; the copies once it has them.
+    const int fin0 = std::max(0, nstreams - 7);
+    const int fin_layers = (int)sd[nstreams - 1].ncz;
+    const int lpg = std::max(1, (fin_layers + 1) / 2);  // layers per group: two finest groups
+    const size_t ngroups = 1 + (size_t)((fin_layers + lpg - 1) / lpg);
+    // ev.e[gi]: group gi's words are on the host; ev.e[ngroups + gi]: its
+    // encode is done; ev.e[2 * ngroups]: the tables are on the host. The
+    // copies run on the context's copy stream, so group gi's copy overlaps
+    // group gi + 1's encode.
+    ev.e.assign(2 * ngroups + 1, nullptr);
+    for (auto& x : ev.e) STZ_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    STZ_CUDA(cudaEventRecord(ev.e[2 * ngroups], st));
+    std::vector<CtaWork> gwork;
+    std::vector<uint32_t> gids;
+    std::vector<size_t> gw(ngroups + 1, 0);
+    for (int s = 0; s < fin0; ++s) add_all_chunks(gwork, gids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    for (size_t gi = 1; gi < ngroups; ++gi) {
+        gw[gi] = gwork.size();
+        const int L0 = (int)(gi - 1) * lpg, L1 = std::min(fin_layers, L0 + lpg);
+        for (int s = fin0; s < nstreams; ++s) {
+            const uint32_t cpl = sd[s].ncx * sd[s].ncy;
+            std::vector<uint32_t> cs;
+            for (uint32_t c = (uint32_t)L0 * cpl; c < (uint32_t)L1 * cpl; ++c) cs.push_back(c);
+            add_work(gwork, gids, (uint32_t)s, cs.data(), cs.size(), (int)sd[s].C);
+        }
+    }
+    gw[0] = 0;
+    gw[ngroups] = gwork.size();
+    const size_t g_work = 0, g_ids = align256(gwork.size() * sizeof(CtaWork)), g_bytes = align256(g_ids + gids.size() * 4);
+    STZ_CUDA(ctx->h_meta2.ensure(g_bytes));
+    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_work, gwork.data(), gwork.size() * sizeof(CtaWork));
+    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_ids, gids.data(), gids.size() * 4);
+    STZ_CUDA(ctx->gwork.ensure(g_bytes));
+    STZ_CUDA(cudaMemcpyAsync(ctx->gwork.p, ctx->h_meta2.p, g_bytes, cudaMemcpyHostToDevice, st));
+    const CtaWork* d_gwork = (const CtaWork*)(ctx->gwork.as<uint8_t>() + g_work);
+    const uint32_t* d_gids = (const uint32_t*)(ctx->gwork.as<uint8_t>() + g_ids);
+    for (size_t gi = 0; gi < ngroups; ++gi) {
+        {
+            KScope ks(ctx, "k_encode");
+            launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
+                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
+                          ctx->payload.as<uint32_t>(), st);
+        }
+        STZ_CUDA(cudaEventRecord(ev.e[ngroups + gi], st));
+    }
+    STZ_CUDA(cudaGetLastError());
+    STZ_CUDA(cudaEventSynchronize(ev.e[2 * ngroups]));
     lap.mark("code lengths + tables");
     const uint64_t* words = (const uint64_t*)(ht + t_words);
 
@@ -547,73 +607,22 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         packed_total += words[s];
     }
     STZ_CUDA(ctx->h_payload.ensure(std::max<uint64_t>(packed_total, 1) * 4));
-
-    // Encode, pack and copy back in groups: every stream of the coarser
-    // levels, then the finest level's streams in two halves of their chunk
-    // z-layers (all 7 streams per group, so every launch still fills the
-    // device); the host zstd-compresses a group's frames while the device
-    // encodes the next (one, two, four or eight finest groups measured within
-    // noise of each other once payload frames skip zstd; two is the fewest
-    // launches that still overlap the copy back).
-    const int fin0 = std::max(0, nstreams - 7);
-    const int fin_layers = (int)sd[nstreams - 1].ncz;
-    const int lpg = std::max(1, (fin_layers + 1) / 2);  // layers per group: two finest groups
-    const size_t ngroups = 1 + (size_t)((fin_layers + lpg - 1) / lpg);
     struct Piece {  // a word range of one stream's payload
         int s;
         uint64_t w0, w1;  // words from the stream's start
     };
     std::vector<std::vector<Piece>> pieces(ngroups);
-    std::vector<CtaWork> gwork;
-    std::vector<uint32_t> gids;
-    std::vector<size_t> gw(ngroups + 1, 0);
     const uint64_t* choff_h = (const uint64_t*)(ht + t_choff);
-    for (int s = 0; s < fin0; ++s) {
-        add_all_chunks(gwork, gids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
-        pieces[0].push_back({s, 0, words[s]});
-    }
+    for (int s = 0; s < fin0; ++s) pieces[0].push_back({s, 0, words[s]});
     for (size_t gi = 1; gi < ngroups; ++gi) {
-        gw[gi] = gwork.size();
         const int L0 = (int)(gi - 1) * lpg, L1 = std::min(fin_layers, L0 + lpg);
         for (int s = fin0; s < nstreams; ++s) {
             const uint32_t cpl = sd[s].ncx * sd[s].ncy;
-            std::vector<uint32_t> cs;
-            for (uint32_t c = (uint32_t)L0 * cpl; c < (uint32_t)L1 * cpl; ++c) cs.push_back(c);
-            add_work(gwork, gids, (uint32_t)s, cs.data(), cs.size(), (int)sd[s].C);
             const uint64_t* co = choff_h + sd[s].chunk_base;
             pieces[gi].push_back({s, co[(size_t)L0 * cpl], co[(size_t)L1 * cpl]});
         }
     }
-    gw[0] = 0;
-    gw[ngroups] = gwork.size();
-    const size_t g_work = 0, g_ids = align256(gwork.size() * sizeof(CtaWork)), g_bytes = align256(g_ids + gids.size() * 4);
-    STZ_CUDA(ctx->h_meta2.ensure(g_bytes));
-    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_work, gwork.data(), gwork.size() * sizeof(CtaWork));
-    std::memcpy(ctx->h_meta2.as<uint8_t>() + g_ids, gids.data(), gids.size() * 4);
-    STZ_CUDA(ctx->gwork.ensure(g_bytes));
-    STZ_CUDA(cudaMemcpyAsync(ctx->gwork.p, ctx->h_meta2.p, g_bytes, cudaMemcpyHostToDevice, st));
-    const CtaWork* d_gwork = (const CtaWork*)(ctx->gwork.as<uint8_t>() + g_work);
-    const uint32_t* d_gids = (const uint32_t*)(ctx->gwork.as<uint8_t>() + g_ids);
-    struct Events {
-        std::vector<cudaEvent_t> e;
-        ~Events()
-        {
-            for (cudaEvent_t x : e) cudaEventDestroy(x);
-        }
-    } ev;
-    // ev.e[gi]: group gi's words are on the host; ev.e[ngroups + gi]: its
-    // encode is done. The copies run on the context's copy stream, so group
-    // gi's copy overlaps group gi + 1's encode.
-    ev.e.assign(2 * ngroups, nullptr);
-    for (auto& x : ev.e) STZ_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     for (size_t gi = 0; gi < ngroups; ++gi) {
-        {
-            KScope ks(ctx, "k_encode");
-            launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
-                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
-                          ctx->payload.as<uint32_t>(), st);
-        }
-        STZ_CUDA(cudaEventRecord(ev.e[ngroups + gi], st));
         STZ_CUDA(cudaStreamWaitEvent(ctx->st_copy, ev.e[ngroups + gi], 0));
         // the group's words straight from the stream buffers to their place in
         // the packed host payload (one copy per piece)
