@@ -121,6 +121,94 @@ int pool_threads(int requested)
     return (int)std::max(1u, std::min(h ? h : 1u, 64u));
 }
 
+namespace {
+constexpr size_t kXferChunk = 16ull << 20;
+
+bool host_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // an unknown pointer: pageable
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy of n bytes on the pool, in pieces of at least 1 MiB
+void pool_copy(ThreadPool& pool, void* dst, const void* src, size_t n)
+{
+    const size_t parts = std::max<size_t>(1, std::min<size_t>((size_t)pool.size(), n >> 20));
+    const size_t per = (n + parts - 1) / parts;
+    pool.parallel_for(parts, [&](size_t i) {
+        const size_t a = i * per, b = std::min(n, a + per);
+        if (a < b) std::memcpy((uint8_t*)dst + a, (const uint8_t*)src + a, b - a);
+    });
+}
+
+struct XferEvents {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~XferEvents()
+    {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+}  // namespace
+
+stz_status copy_to_host(stz_context* ctx, void* dst, const void* src_dev, size_t n)
+{
+    cudaStream_t st = ctx->st;
+    if (n <= kXferChunk || host_pinned(dst)) {
+        STZ_CUDA(cudaMemcpyAsync(dst, src_dev, n, cudaMemcpyDeviceToHost, st));
+        STZ_CUDA(cudaStreamSynchronize(st));
+        return STZ_OK;
+    }
+    XferEvents ev;
+    for (int b = 0; b < 2; ++b) {
+        STZ_CUDA(ctx->h_xfer[b].ensure(kXferChunk));
+        STZ_CUDA(cudaEventCreateWithFlags(&ev.e[b], cudaEventDisableTiming));
+    }
+    const size_t nch = (n + kXferChunk - 1) / kXferChunk;
+    auto issue = [&](size_t i) -> cudaError_t {
+        const size_t a = i * kXferChunk, len = std::min(kXferChunk, n - a);
+        cudaError_t e = cudaMemcpyAsync(ctx->h_xfer[i & 1].p, (const uint8_t*)src_dev + a, len, cudaMemcpyDeviceToHost, st);
+        return e == cudaSuccess ? cudaEventRecord(ev.e[i & 1], st) : e;
+    };
+    STZ_CUDA(issue(0));
+    for (size_t i = 0; i < nch; ++i) {
+        if (i + 1 < nch) STZ_CUDA(issue(i + 1));  // into the other chunk, free since chunk i - 1 was copied out
+        STZ_CUDA(cudaEventSynchronize(ev.e[i & 1]));
+        const size_t a = i * kXferChunk;
+        pool_copy(*ctx->pool, (uint8_t*)dst + a, ctx->h_xfer[i & 1].p, std::min(kXferChunk, n - a));
+    }
+    return STZ_OK;
+}
+
+stz_status copy_from_host(stz_context* ctx, void* dst_dev, const void* src, size_t n)
+{
+    cudaStream_t st = ctx->st;
+    if (n <= kXferChunk || host_pinned(src)) {
+        STZ_CUDA(cudaMemcpyAsync(dst_dev, src, n, cudaMemcpyHostToDevice, st));
+        STZ_CUDA(cudaStreamSynchronize(st));
+        return STZ_OK;
+    }
+    XferEvents ev;
+    for (int b = 0; b < 2; ++b) {
+        STZ_CUDA(ctx->h_xfer[b].ensure(kXferChunk));
+        STZ_CUDA(cudaEventCreateWithFlags(&ev.e[b], cudaEventDisableTiming));
+    }
+    const size_t nch = (n + kXferChunk - 1) / kXferChunk;
+    for (size_t i = 0; i < nch; ++i) {
+        if (i >= 2) STZ_CUDA(cudaEventSynchronize(ev.e[i & 1]));  // chunk i - 2's DMA has left this buffer
+        const size_t a = i * kXferChunk, len = std::min(kXferChunk, n - a);
+        pool_copy(*ctx->pool, ctx->h_xfer[i & 1].p, (const uint8_t*)src + a, len);
+        STZ_CUDA(cudaMemcpyAsync((uint8_t*)dst_dev + a, ctx->h_xfer[i & 1].p, len, cudaMemcpyHostToDevice, st));
+        STZ_CUDA(cudaEventRecord(ev.e[i & 1], st));
+    }
+    STZ_CUDA(cudaStreamSynchronize(st));  // the staging chunks are reused by the next call
+    return STZ_OK;
+}
+
 stz_status check_opts(const stz_opts* o)
 {
     if (!o) STZ_FAIL(STZ_ERR_ARG, "opts is null");
@@ -1513,7 +1601,7 @@ stz_status stz_compress(stz_context* ctx, const void* field, stz_dtype dtype, si
     if (!dm.empty()) STZ_FAIL(STZ_ERR_DIMS, dm);
     const size_t bytes = nx * ny * nz * dtype_size(dtype);
     STZ_CUDA(ctx->field.ensure(bytes));
-    STZ_CUDA(cudaMemcpyAsync(ctx->field.p, field, bytes, cudaMemcpyHostToDevice, ctx->st));
+    STZ_TRY(copy_from_host(ctx, ctx->field.p, field, bytes));
     return stz_compress_dev(ctx, ctx->field.p, dtype, nx, ny, nz, opts, out);
 }
 
@@ -1538,9 +1626,7 @@ stz_status stz_decompress_level(stz_context* ctx, const stz_stream* s, int level
     const size_t n = (size_t)(h.nx >> level) * (h.ny >> level) * (h.nz >> level) * h.elem();
     STZ_CUDA(ctx->out.ensure(n));
     STZ_TRY(stz_decompress_level_dev(ctx, s, level, ctx->out.p, od));
-    STZ_CUDA(cudaMemcpyAsync(out, ctx->out.p, n, cudaMemcpyDeviceToHost, ctx->st));
-    STZ_CUDA(cudaStreamSynchronize(ctx->st));
-    return STZ_OK;
+    return copy_to_host(ctx, out, ctx->out.p, n);
 }
 
 stz_status stz_decompress_full_dev(stz_context* ctx, const stz_stream* s, void* out)
@@ -1574,9 +1660,7 @@ stz_status stz_decompress_box(stz_context* ctx, const stz_stream* s, const int64
                      (plan.q[2].e - plan.q[2].b + 1) * h.elem();
     STZ_CUDA(ctx->out.ensure(n));
     STZ_TRY(stz_decompress_box_dev(ctx, s, lo, hi, ctx->out.p, od));
-    STZ_CUDA(cudaMemcpyAsync(out, ctx->out.p, n, cudaMemcpyDeviceToHost, ctx->st));
-    STZ_CUDA(cudaStreamSynchronize(ctx->st));
-    return STZ_OK;
+    return copy_to_host(ctx, out, ctx->out.p, n);
 }
 
 stz_status stz_stream_bytes(const stz_stream* s, const void** data, size_t* size)

@@ -246,6 +246,7 @@ struct stz_context {
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
         tiles, models, eval, rstats, gwork;
     stz::PinBuf h_hist, h_meta, h_meta2, h_payload, h_stage, h_io, h_small, h_rstats, h_fullh;
+    stz::PinBuf h_xfer[2];  // staging chunks of host <-> device copies of pageable caller buffers
     // device buffers lent to one-off decodes
     stz::DevBuf p_stage, p_coarsest, p_base;
     void borrow(stz::Prepared& p)
@@ -308,6 +309,12 @@ struct KScope {
 };
 
 int pool_threads(int requested);
+// Host <-> device copies of a caller's host buffer on ctx->st, complete on
+// return. A page-locked buffer takes one DMA; a pageable one goes through
+// two pinned chunks, the DMA of one chunk overlapping the host pool's copy
+// of the other (the driver's own staging of pageable memory is serial).
+stz_status copy_to_host(stz_context* ctx, void* dst, const void* src_dev, size_t n);
+stz_status copy_from_host(stz_context* ctx, void* dst_dev, const void* src, size_t n);
 // Validates compressor options (STZ_ERR_ARG with a message).
 stz_status check_opts(const stz_opts* o);
 size_t dtype_size(int dtype);
