@@ -370,6 +370,7 @@ def serving_bench(args, ctx, local):
     for i, r in enumerate((2000, 10000)):
         res["box64"].append(serve_load(srv, sid, dims, K, r, sec, box64, 10 + i))
         traces[f"box64_{r}_batches"] = srv.batch_log()
+    serve_load(srv, sid, dims, K, 200, 0.5, mixed, 2)  # warm-up of the bulk lane (level requests)
     res["mixed"] = serve_load(srv, sid, dims, K, 1000, sec, mixed, 20)
     traces["mixed_batches"] = srv.batch_log()
     for name, r in (("box64_2k", res["box64"][0]), ("box64_10k", res["box64"][1]), ("mixed", res["mixed"])):
