@@ -599,7 +599,9 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     {
         KScope ks(ctx, "k_scan_stream");
-        launch_scan_streams(d_sd, nstreams, ctx->sub_bits.as<uint32_t>(), ctx->sub_off.as<uint32_t>(),
+        uint32_t max_chunks = 0;
+        for (int s = 0; s < nstreams; ++s) max_chunks = std::max(max_chunks, sd[s].nchunks);
+        launch_scan_streams(d_sd, nstreams, max_chunks, ctx->sub_bits.as<uint32_t>(), ctx->sub_off.as<uint32_t>(),
                             ctx->chunk_off.as<uint64_t>(), ctx->stream_words.as<uint64_t>(),
                             ctx->payload.as<uint32_t>(), st);
     }

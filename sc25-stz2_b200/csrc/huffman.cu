@@ -340,12 +340,41 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
     }
 }
 
-// Per stream: plane bit offsets inside each chunk, chunk word offsets (the
-// marker table) and the stream's word count; boundary words of every plane are
-// cleared for the encoder's atomic ORs.
+// Plane bit offsets inside each chunk (one warp per chunk: a scan of the
+// planes' bit counts); the chunk's word count goes to chunk_word_off, which
+// k_scan_stream then turns into offsets. Block (s, y) takes chunks 32y..32y+31
+// of stream s.
+__global__ void __launch_bounds__(1024) k_plane_offsets(const StreamDesc* __restrict__ sd,
+                                                        const uint32_t* __restrict__ sub_bits,
+                                                        uint32_t* __restrict__ sub_off,
+                                                        uint64_t* __restrict__ chunk_word_off)
+{
+    const StreamDesc s = sd[blockIdx.x];
+    const uint32_t c = blockIdx.y * 32 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (c >= s.nchunks) return;  // uniform per warp
+    const size_t k0 = s.sub_base + (size_t)c * s.C;
+    uint64_t carry = 0;
+    for (uint32_t lz0 = 0; lz0 < s.C; lz0 += 32) {
+        const uint32_t lz = lz0 + lane;
+        const uint32_t bits = lz < s.C ? sub_bits[k0 + lz] : 0u;
+        uint32_t incl = bits;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        if (lz < s.C) sub_off[k0 + lz] = (uint32_t)(carry + incl - bits);
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) chunk_word_off[s.chunk_base + c] = (carry + 31) / 32;
+}
+
+// Per stream: chunk word counts -> word offsets (the marker table) and the
+// stream's word count; then the boundary words of every plane are cleared
+// for the encoder's atomic ORs.
 __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restrict__ sd,
                                                       const uint32_t* __restrict__ sub_bits,
-                                                      uint32_t* __restrict__ sub_off,
+                                                      const uint32_t* __restrict__ sub_off,
                                                       uint64_t* __restrict__ chunk_word_off,
                                                       uint64_t* __restrict__ stream_words,
                                                       uint32_t* __restrict__ payload)
@@ -358,16 +387,7 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
     __syncthreads();
     for (uint32_t base = 0; base < s.nchunks; base += blockDim.x) {
         const uint32_t c = base + threadIdx.x;
-        uint64_t words = 0;
-        if (c < s.nchunks) {
-            uint32_t acc = 0;
-            for (uint32_t lz = 0; lz < C; ++lz) {
-                const size_t k = s.sub_base + (size_t)c * C + lz;
-                sub_off[k] = acc;
-                acc += sub_bits[k];
-            }
-            words = (acc + 31u) / 32u;
-        }
+        const uint64_t words = c < s.nchunks ? chunk_word_off[s.chunk_base + c] : 0;
         uint64_t incl = words;
         for (int o = 1; o < 32; o <<= 1) {
             const uint64_t v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -385,18 +405,7 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
         }
         __syncthreads();
         const uint64_t pre = carry + ((threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0) + incl - words;
-        if (c < s.nchunks) {
-            chunk_word_off[s.chunk_base + c] = pre;
-            uint32_t* w = payload + s.word_base + pre;
-            for (uint32_t lz = 0; lz < C; ++lz) {
-                const size_t k = s.sub_base + (size_t)c * C + lz;
-                const uint32_t b0 = sub_off[k], nb = sub_bits[k];
-                if (nb) {
-                    w[b0 >> 5] = 0;
-                    w[(b0 + nb - 1) >> 5] = 0;
-                }
-            }
-        }
+        if (c < s.nchunks) chunk_word_off[s.chunk_base + c] = pre;
         __syncthreads();
         if (threadIdx.x == 0) carry += wsum[31];
         __syncthreads();
@@ -404,6 +413,17 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
     if (threadIdx.x == 0) {
         chunk_word_off[s.chunk_base + s.nchunks] = carry;
         stream_words[blockIdx.x] = carry;
+    }
+    __syncthreads();  // every chunk offset is written
+    const uint64_t np = (uint64_t)s.nchunks * C;
+    for (uint64_t p = threadIdx.x; p < np; p += blockDim.x) {
+        const size_t k = s.sub_base + p;
+        const uint32_t b0 = sub_off[k], nb = sub_bits[k];
+        if (nb) {
+            uint32_t* w = payload + s.word_base + chunk_word_off[s.chunk_base + p / C];
+            w[b0 >> 5] = 0;
+            w[(b0 + nb - 1) >> 5] = 0;
+        }
     }
 }
 
@@ -1067,11 +1087,13 @@ void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, 
     if (nwork) k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
 }
 
-void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
-                         uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload, cudaStream_t st)
+void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks, const uint32_t* sub_bits,
+                         uint32_t* sub_off, uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload,
+                         cudaStream_t st)
 {
-    if (nstreams)
-        k_scan_stream<<<nstreams, 1024, 0, st>>>(sd, sub_bits, sub_off, chunk_word_off, stream_words, payload);
+    if (!nstreams || !max_chunks) return;
+    k_plane_offsets<<<dim3(nstreams, (max_chunks + 31) / 32), 1024, 0, st>>>(sd, sub_bits, sub_off, chunk_word_off);
+    k_scan_stream<<<nstreams, 1024, 0, st>>>(sd, sub_bits, sub_off, chunk_word_off, stream_words, payload);
 }
 
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,

@@ -28,8 +28,12 @@ void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork,
                       const uint16_t* codes, unsigned long long* stats, cudaStream_t st);
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                      const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st);
-void launch_scan_streams(const StreamDesc* sd, int nstreams, const uint32_t* sub_bits, uint32_t* sub_off,
-                         uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload, cudaStream_t st);
+// Plane bit offsets, chunk word offsets and stream word counts from the
+// plane bit counts; clears every plane's boundary words (max_chunks: the
+// most chunks of any stream).
+void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks, const uint32_t* sub_bits,
+                         uint32_t* sub_off, uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload,
+                         cudaStream_t st);
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                    const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
                    uint32_t* payload, cudaStream_t st);
