@@ -6,7 +6,9 @@ version 3 (u32 plane bit offsets inside the chunk) or version 4 with
 `width`-byte plane bit counts (2 or 4). Header frames are stored raw after
 the rewrite (a stored size equal to the raw size); payload frames are copied
 unchanged. The directory layout is the one ContainerWriter::finish writes
-(sc25-stz2_b200/csrc/host.cpp)."""
+(sc25-stz2_b200/csrc/host.cpp).
+
+frame_sizes(stream) lists every frame's stored and raw size."""
 import ctypes
 import struct
 
@@ -103,3 +105,38 @@ def rewrite_plane_tables(b: bytes, version: int, width: int = 2) -> bytes:
             pos += sum(ls)
     assert pos == len(b)
     return bytes(d + frames)
+
+
+def frame_sizes(b: bytes):
+    """[(level, block, kind, stored, raw)] for every frame of a version 2-4
+    container; kind is "header" or "payload"."""
+    r = [8]
+
+    def take(fmt):
+        v = struct.unpack_from("<" + fmt, b, r[0])
+        r[0] += struct.calcsize("<" + fmt)
+        return v
+
+    version = take("I")[0]
+    assert version >= 2
+    dtype, _pred, _nx, _ny, _nz, K = take("6I")
+    elem = 8 if dtype == 1 else 4
+    take("3I")
+    take("i")
+    take("4d")
+    c0 = take("3I")
+    r[0] += c0[0] * c0[1] * c0[2] * elem
+    out = []
+    for k in range(1, K + 1):
+        take("4I")
+        take("d")
+        (lf,) = take("I")
+        r[0] += 2112 if lf else 0
+        for blk in range(7):
+            (L,) = take("I")
+            hs, hr = take("2Q")
+            ls = take(f"{L}Q")
+            lr = take(f"{L}Q")
+            out.append((k, blk, "header", hs, hr))
+            out += [(k, blk, "payload", a, c) for a, c in zip(ls, lr)]
+    return out

@@ -139,3 +139,23 @@ def test_plane_table_layouts_oracle():
     for v, w in ((3, 4), (4, 2), (4, 4)):
         got = po.decompress(rewrite_plane_tables(b, v, w))
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (v, w)
+
+
+def test_zstd_probe_rule():
+    """Payload frames longer than 4 KiB are zstd-compressed only when zstd
+    shrinks their first 4 KiB: Huffman payload of a noisy field is stored
+    raw, while a field tiled from one small block (payload bytes repeat
+    with the tile) keeps compressed payload frames. Stream headers are
+    always tried."""
+    from stream_tools import frame_sizes
+
+    rng = np.random.default_rng(4)
+    noisy = rng.normal(0, 1, (64, 64, 64)).astype(np.float32)
+    fr = frame_sizes(po.compress(noisy, po.pointwise_eb(noisy, 1e-3)))
+    big = [f for f in fr if f[2] == "payload" and f[4] > 4096]
+    assert big and all(st == rw for _, _, _, st, rw in big)
+    assert any(st < rw for _, _, kind, st, rw in fr if kind == "header")
+    tile = rng.normal(0, 1, (8, 8, 64)).astype(np.float32)
+    tiled = np.tile(tile, (8, 8, 1))
+    fr = frame_sizes(po.compress(tiled, po.pointwise_eb(tiled, 1e-3)))
+    assert any(st < rw for _, _, kind, st, rw in fr if kind == "payload" and rw > 4096)
