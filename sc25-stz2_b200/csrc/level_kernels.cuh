@@ -165,10 +165,11 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     }
 }
 
-template <typename T, int PRED, bool FINEST, int LM>
+template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                          QuantParams qp, HistArgs hist, LearnedArgs<T> la)
 {
+    static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ uint32_t sh[7][kSmemBins];
@@ -184,15 +185,15 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     const int wlo = max(0, qp.radius - kSmemBins / 2);
     const int wn = min(kSmemBins, 2 * qp.radius - wlo);
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
-    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
-    load_tile(tile, R, dx, dy, dz, x0, y0, z0);
+    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * ZB;
+    load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool valid = x <= dx - 3 && y <= dy - 3;
     ChunkIndex ci;
     ci.init(geo, x, y);
     uint32_t center[7] = {0, 0, 0, 0, 0, 0, 0};
-    const int z1 = min(z0 + BZ, dz - 2);
+    const int z1 = min(z0 + ZB, dz - 2);
     [[maybe_unused]] uint32_t phase = 0;
     [[maybe_unused]] bool tc_failed = false;
     if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
@@ -287,12 +288,13 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     }
 }
 
-template <typename T, int PRED, int LM>
+template <typename T, int PRED, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
                                                          const T* __restrict__ unpred_dense, T* __restrict__ G,
                                                          LearnedArgs<T> la)
 {
+    static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ T lut[2 * kRecW];
@@ -304,8 +306,8 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
         la.model = smodel;
     }
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
-    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * BZ;
-    load_tile(tile, R, dx, dy, dz, x0, y0, z0);
+    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * ZB;
+    load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool valid = x <= dx - 3 && y <= dy - 3;
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
     }
     ChunkIndex ci;
     ci.init(geo, x, y);
-    const int z1 = min(z0 + BZ, dz - 2);
+    const int z1 = min(z0 + ZB, dz - 2);
     [[maybe_unused]] uint32_t phase = 0;
     [[maybe_unused]] bool tc_failed = false;
     if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
