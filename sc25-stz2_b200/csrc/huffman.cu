@@ -9,10 +9,14 @@
 // word offset per chunk (the marker table), so any chunk decodes on its own.
 //
 // Parallel decomposition: every z-plane of a chunk (C^2 symbols, a
-// "sub-chunk") is one thread's sequential run; its bit offset inside the chunk
-// is stored, so all planes of all chunks of all streams encode and decode
-// independently. Bits are packed MSB-first into 32-bit words; a chunk starts
-// on a word boundary.
+// "sub-chunk") has its bit offset inside the chunk in the stream header, so
+// all planes of all chunks of all streams encode and decode independently.
+// Inside a plane, a group of lanes shares the work: the encode side splits
+// the codes into lane segments (runs are the gaps between literal masks),
+// the decoder splits the bits into lane slices and resynchronises them
+// (a dense stream in a large launch is decoded one thread per plane
+// instead). Bits are packed MSB-first into 32-bit words; a chunk starts on a
+// word boundary.
 //
 // Runs: inside a plane, a maximal run of r centre codes (code == radius) is
 // coded with run symbols (run_geometry): while r > D, 2^k (the largest power
