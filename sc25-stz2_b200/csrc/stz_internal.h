@@ -18,7 +18,9 @@ constexpr int kLutBits = 12;
 // Histogram window (bins around the radius) kept in shared memory and copied
 // to the host for codebook construction; codes outside it take a slow path.
 constexpr int kHistWindow = 4096;
-// Threads of one entropy-coding CTA; a CTA covers 128 / C chunks of a stream.
+// Planes of one coder work item: an item covers max(1, 128 / C) chunks of a
+// stream, i.e. up to 128 planes (the coder kernels split an item over
+// several CTAs, see huffman.cu).
 constexpr int kCoderThreads = 128;
 
 // Learned correction of one level (this project's addition; no reference
