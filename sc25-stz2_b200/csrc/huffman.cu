@@ -918,7 +918,7 @@ __device__ __forceinline__ bool decode_sequential(const StreamDesc& s, uint32_t 
 // Planes of the listed chunks; the tables of stream i at tabs[i]. Warp mode:
 // CTA (x, y) takes 8 planes of item x; sequential mode: CTA (x, 0) takes all
 // of them, one per thread (at most kDecodeThreads).
-__global__ void __launch_bounds__(kDecodeThreads) k_decode(const CtaWork* __restrict__ work,
+__global__ void __launch_bounds__(kDecodeThreads, 5) k_decode(const CtaWork* __restrict__ work,
                                                            const uint32_t* __restrict__ chunk_ids,
                                                            const StreamDesc* __restrict__ sd,
                                                            const DecodeTables* __restrict__ tabs,
