@@ -52,6 +52,7 @@ def parse_args():
     p.add_argument("--seed", type=int, default=2025)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the bit-identity check against oracle/_ref")
     p.add_argument("--once", action="store_true",
                    help="one compress + one full decompress of the workload, no timing (profiler captures)")
     p.add_argument("--no-serve", action="store_true", help="skip the request-server latency measurement")
@@ -180,6 +181,30 @@ def cpu_reference_round_trip(field: np.ndarray, rel: float, radius: int = 32768)
         coarse = po.ref_level_decode(dq, coarse, 1 if k == K else 0)
     t2 = time.perf_counter()
     return {"compress_s": t1 - t0, "decompress_s": t2 - t1, "unpred": int(unpred)}
+
+
+def reference_parity(ctx, stream, field_host: np.ndarray, decoded_host: np.ndarray) -> dict:
+    """Bit-identity of the measured stream with the reference's own code
+    (oracle/_ref FD5 level functions through the hierarchy, at the eb the
+    stream records): every level's quant codes of every block, and the decoded
+    field. Runs outside the timed region."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    if not po.ref_available():
+        return {"unavailable": "oracle/_ref missing"}
+    t0 = time.perf_counter()
+    ref = po.ref_round_trip(field_host, stream.info().eb)
+    codes_ok = True
+    for k in range(1, ref["K"] + 1):
+        for b in range(7):
+            codes_ok &= bool(np.array_equal(ctx.stream_codes(stream, k, b), ref["codes"][k - 1][b]))
+    u = np.uint64 if field_host.dtype == np.float64 else np.uint32
+    dec_ok = bool(np.array_equal(decoded_host.view(u), ref["grids"][ref["K"]].view(u)))
+    return {"codes": codes_ok, "decoded": dec_ok, "closed_loop": ref["closed_loop_ok"],
+            "unpred": int(sum(sum(c) for c in ref["unpred"])),
+            "against": "reference FD5 level functions compiled from source (oracle/_ref), same eb",
+            "check_s": round(time.perf_counter() - t0, 2)}
 
 
 def cpu_cores() -> int:
@@ -660,6 +685,10 @@ def main():
                 "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
                 "ms_per_launch": dms / dl, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = reference_parity(ctx, s, field.cpu().numpy(), out.cpu().numpy())
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_round_trip(field.cpu().numpy(), args.rel)
@@ -689,7 +718,7 @@ def main():
                        "l2": "inputs larger than L2 (512 MiB field per step)", "parallelism": f"replicas x{world}"},
             "compress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, comp_ms),
             "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
-            "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
+            "parity": parity, "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "serving": serving, "learned": learned,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},

@@ -302,11 +302,13 @@ stz_status stz_dequantize_dev(stz_context* ctx, stz_dtype dtype, const int32_t* 
  * the current device, and its scratch is a fixed array inside the library
  * image (about 0.8 MB per GPU that loads the library, kept until the process
  * exits), so at most STZ_NOALLOC_MAX_VALUES values per call; larger n returns
- * STZ_ERR_RANGE. The first call on a device looks up that array's device
- * address; make it before any stream capture. All calls share the one array:
- * calls that overlap on the GPU (other streams, other host threads) race and
- * must be serialized by the caller. The call waits for its stream to finish
- * and returns the number of unpredictable values in *n_unpred.
+ * STZ_ERR_RANGE. Every call looks up that array's device address in the
+ * current context (cudaGetSymbolAddress, a host-side lookup). All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialized by the caller. The call copies the
+ * unpredictable count back and waits for its stream to finish, so it must not
+ * be called while its stream, or the legacy default stream, is being captured
+ * into a CUDA graph. It returns that count in *n_unpred.
  * This entry point has no counterpart in the reference. */
 #define STZ_NOALLOC_MAX_VALUES ((size_t)65536 * 1024)
 stz_status stz_quantize_noalloc_dev(stz_dtype dtype, const void* data, size_t n, double eb, int radius, int32_t* q,

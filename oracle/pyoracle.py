@@ -20,7 +20,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "lib", "libstz_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfd5ref.so")
-REFERENCE_SRC = "/root/reference/src"
+# The reference's src/ directory, from the environment (no default: the
+# reference sources exist only where the caller says they are).
+REFERENCE_SRC = os.environ.get("STZ_REFERENCE_SRC", "")
 
 vp, sz, dbl, ci = C.c_void_p, C.c_size_t, C.c_double, C.c_int
 
@@ -54,11 +56,13 @@ def mlp_corr(m: Model, coarse: np.ndarray, x: int, y: int, z: int, eb: float) ->
     return out
 
 
-def build(ref: bool = True) -> None:
-    """Compile the oracle (and the reference shim when its sources exist)."""
+def build(ref: bool = True, reference_src: str | None = None) -> None:
+    """Compile the oracle, and the reference shim when `reference_src` (default
+    $STZ_REFERENCE_SRC) names a directory holding the reference's sources."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if ref and os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_SRC={REFERENCE_SRC}"], check=True)
+    src = reference_src if reference_src is not None else REFERENCE_SRC
+    if ref and src and os.path.isdir(src):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_SRC={src}"], check=True)
 
 
 _orc = None
@@ -296,6 +300,49 @@ def ref_dequantize(q: np.ndarray, eb: float, radius: int, unpred: np.ndarray, dt
     un = np.ascontiguousarray(unpred, dtype=dtype)
     getattr(ref(), "fd5ref_dequantize_" + _suf(dtype))(_p(q), q.size, eb, radius, _p(un), _p(out))
     return out
+
+
+def ref_round_trip(field: np.ndarray, eb: float, mults=(0.7, 2.7, 8.2), radius: int = 32768,
+                   chunk_high: int = 32, chunk_low: int = 16) -> dict:
+    """The reference's own FD5 level functions (oracle/_ref) driven through
+    this project's hierarchy, for full-size parity checks.
+
+    Encoder: per level k = 1..K the reference's predict + quantize of the 7
+    odd-parity blocks against the encoder's decoded coarser grid, with the
+    closed loop of FD5:2195-2230 (the decoded fine grid feeds level k + 1);
+    level eb = multiplier x eb (base / low / high, FD5:2120-2129). Decoder:
+    the reference's dequantize (recover LUT and row-major unpredictable
+    values, FD5:1528-1562) and level decode (FD5:2369-2394 for the coarser
+    levels, the fused to-full path FD5:2413-2451 for the finest).
+
+    Returns codes[k-1] as the container's chunk-major uint16 symbols per block
+    (7 arrays), unpred[k-1] counts per block, grids[j] = the decoder's grid
+    after j levels (grids[0] the raw coarsest grid, grids[K] the field), and
+    closed_loop_ok: every encoder-side decoded grid equals the decoder's."""
+    a = np.ascontiguousarray(field)
+    nz, ny, nx = a.shape
+    K = num_levels(nx, ny, nz)
+    S = 1 << K
+    coarsest = np.ascontiguousarray(a[::S, ::S, ::S])
+    enc_grid, dec_grid = coarsest, coarsest
+    grids, codes, unpred = [coarsest], [], []
+    closed_loop_ok = True
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = a if s == 1 else np.ascontiguousarray(a[::s, ::s, ::s])
+        ebk = (mults[2] if k == K else mults[1] if k == K - 1 else mults[0]) * eb
+        q, u, c, d = level_encode(fine, enc_grid, ebk, radius, decoded=k < K, use_ref=True)
+        dz, dy, dx = enc_grid.shape
+        C_ = oracle().stzo_level_chunk(nx, ny, nz, k, chunk_high, chunk_low)
+        codes.append([chunk_major(q[b], (dz, dy, dx), C_).astype(np.uint16) for b in range(7)])
+        unpred.append([int(v) for v in c])
+        dq = ref_dequantize(q.reshape(-1), ebk, radius, u, a.dtype)
+        dec_grid = ref_level_decode(dq, dec_grid, 1 if k == K else 0)
+        grids.append(dec_grid)
+        if k < K:
+            closed_loop_ok &= bool(np.array_equal(d.view(np.uint8), dec_grid.view(np.uint8)))
+            enc_grid = d
+    return {"K": K, "codes": codes, "unpred": unpred, "grids": grids, "closed_loop_ok": closed_loop_ok}
 
 
 def plan(dims_xyz, chunk_high, chunk_low, a, b, use_ref=False) -> np.ndarray:

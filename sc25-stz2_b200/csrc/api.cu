@@ -153,6 +153,19 @@ struct XferEvents {
             if (x) cudaEventDestroy(x);
     }
 };
+
+// On an early return (a failed CUDA call mid-loop), waits for the copies
+// already queued on the stream, so the next host-buffer call never refills a
+// staging chunk that a DMA still reads or writes. The wait's own status is
+// ignored: the caller already reports the first error.
+struct DrainOnExit {
+    cudaStream_t st;
+    bool done = false;
+    ~DrainOnExit()
+    {
+        if (!done) cudaStreamSynchronize(st);
+    }
+};
 }  // namespace
 
 stz_status copy_to_host(stz_context* ctx, void* dst, const void* src_dev, size_t n)
@@ -164,6 +177,7 @@ stz_status copy_to_host(stz_context* ctx, void* dst, const void* src_dev, size_t
         return STZ_OK;
     }
     XferEvents ev;
+    DrainOnExit drain{st};
     for (int b = 0; b < 2; ++b) {
         STZ_CUDA(ctx->h_xfer[b].ensure(kXferChunk));
         STZ_CUDA(cudaEventCreateWithFlags(&ev.e[b], cudaEventDisableTiming));
@@ -181,6 +195,7 @@ stz_status copy_to_host(stz_context* ctx, void* dst, const void* src_dev, size_t
         const size_t a = i * kXferChunk;
         pool_copy(*ctx->pool, (uint8_t*)dst + a, ctx->h_xfer[i & 1].p, std::min(kXferChunk, n - a));
     }
+    drain.done = true;  // every DMA was waited for above
     return STZ_OK;
 }
 
@@ -193,6 +208,7 @@ stz_status copy_from_host(stz_context* ctx, void* dst_dev, const void* src, size
         return STZ_OK;
     }
     XferEvents ev;
+    DrainOnExit drain{st};
     for (int b = 0; b < 2; ++b) {
         STZ_CUDA(ctx->h_xfer[b].ensure(kXferChunk));
         STZ_CUDA(cudaEventCreateWithFlags(&ev.e[b], cudaEventDisableTiming));
@@ -206,6 +222,7 @@ stz_status copy_from_host(stz_context* ctx, void* dst_dev, const void* src, size
         STZ_CUDA(cudaEventRecord(ev.e[i & 1], st));
     }
     STZ_CUDA(cudaStreamSynchronize(st));  // the staging chunks are reused by the next call
+    drain.done = true;
     return STZ_OK;
 }
 

@@ -15,7 +15,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "levels.h"
@@ -34,29 +33,19 @@ constexpr size_t kScratchBytes = kCntBytes + (kMaxTiles + 1) * sizeof(uint64_t);
 static_assert(STZ_NOALLOC_MAX_VALUES == kMaxTiles * kTile, "header limit and scratch size disagree");
 
 // The scratch itself. In host code this name is only a host-side stand-in:
-// the device address comes from cudaGetSymbolAddress, per device.
+// the device address comes from cudaGetSymbolAddress in the current context.
 static __device__ __align__(256) unsigned char g_quantize_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this set-up).
+// Device address of the scratch in the current context. Looked up on every
+// call: the lookup is a host-side table read once the module is loaded, and a
+// cached address would go stale after cudaDeviceReset (the module reloads,
+// possibly elsewhere) or belong to another context on the same device.
 cudaError_t scratch_address(void** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_quantize_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_quantize_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return cudaSuccess;
 }
 

@@ -104,6 +104,35 @@ def test_oracle_matches_reference_live(dtype):
 
 
 @pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("case", ["grf256_f32_1e-3", "fronts128x64x64_f64_1e-6"])
+def test_oracle_stream_matches_reference_at_size(case):
+    """The C restatement's whole-field codec against the reference's own level
+    functions through the hierarchy (pyoracle.ref_round_trip): codes of every
+    stream, the full decode and every progressive level, bit for bit. The
+    256^3 GRF is the benchmark's 256^3 configuration at full size."""
+    from stz_b200 import fields
+
+    if case.startswith("grf"):
+        f, rel = fields.grf((256, 256, 256), 11.0 / 3.0, 2025, np.float32), 1e-3
+    else:
+        f, rel = fields.fronts((64, 64, 128), 5, np.float64), 1e-6
+    eb = po.pointwise_eb(f, rel)
+    ref = po.ref_round_trip(f, eb)
+    assert ref["closed_loop_ok"]
+    stream = po.compress(f, eb)
+    K = ref["K"]
+    for k in range(1, K + 1):
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), ref["codes"][k - 1][b]), (k, b)
+    u = np.uint64 if f.dtype == np.float64 else np.uint32
+    assert np.array_equal(po.decompress(stream).view(u), ref["grids"][K].view(u))
+    for lvl in range(1, K + 1):
+        assert np.array_equal(po.decompress(stream, lvl).view(u), ref["grids"][K - lvl].view(u)), lvl
+    if rel == 1e-6:
+        assert sum(sum(c) for c in ref["unpred"]) > 0
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
 def test_planner_matches_reference_live():
     rng = np.random.default_rng(17)
     for dims, ch, cl in [((128, 64, 64), 16, 8), ((64, 64, 64), 32, 16)]:

@@ -37,10 +37,19 @@ def _regular(ctx, d, eb, radius):
     return q.cpu().numpy(), u[:n].cpu().numpy()
 
 
-def _noalloc(d, eb, radius, stream=0):
+def _noalloc(d, eb, radius, stream=None):
+    """Run the entry point on `stream` (a torch.cuda.Stream; None = the legacy
+    default stream). The outputs are filled on torch's current stream first,
+    so the caller's stream waits for that work before the call."""
     q = torch.full((d.numel(),), -7, dtype=torch.int32, device="cuda")
     u = torch.zeros_like(d)
-    n = stz_b200.quantize_noalloc(d, eb, radius, q, u, stream)
+    handle = 0
+    if stream is not None:
+        stream.wait_stream(torch.cuda.current_stream())
+        handle = stream.cuda_stream
+    else:
+        torch.cuda.current_stream().synchronize()
+    n = stz_b200.quantize_noalloc(d, eb, radius, q, u, handle)
     return q.cpu().numpy(), u[:n].cpu().numpy()
 
 
@@ -58,10 +67,25 @@ def test_noalloc_quantize_matches_regular_entry_point_twice_in_a_row():
         b = _data(300_001, np.float64, 2)
         want_q, want_u = _regular(ctx, b, 3e-4, 512)
         s = torch.cuda.Stream()
-        got_q, got_u = _noalloc(b, 3e-4, 512, s.cuda_stream)
+        got_q, got_u = _noalloc(b, 3e-4, 512, s)
         assert np.array_equal(got_q, want_q)
         assert got_u.size == want_u.size > 0
         assert np.array_equal(got_u.view(np.uint64), want_u.view(np.uint64))
+
+
+def test_noalloc_quantize_at_its_size_limit():
+    """Exactly STZ_NOALLOC_MAX_VALUES values: every tile slot of the fixed
+    scratch is used; twice in a row, on a caller-owned stream."""
+    n = stz_b200.NOALLOC_MAX_VALUES
+    with stz_b200.Context(0) as ctx:
+        d = _data(n, np.float32, 3)
+        want_q, want_u = _regular(ctx, d, 1e-2, 32768)
+        s = torch.cuda.Stream()
+        for _ in range(2):
+            got_q, got_u = _noalloc(d, 1e-2, 32768, s)
+            assert np.array_equal(got_q, want_q)
+            assert got_u.size == want_u.size > 0
+            assert np.array_equal(got_u.view(np.uint32), want_u.view(np.uint32))
 
 
 def test_noalloc_quantize_rejects_sizes_beyond_its_scratch():
