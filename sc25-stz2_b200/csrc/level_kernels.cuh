@@ -103,13 +103,13 @@ __device__ __forceinline__ tc::Net<2>* net_smem()
     return &net;
 }
 
-// One coarse point of the encoder: fine values, 7 predictions, residuals,
-// codes, unpredictable values, decoded fine cell.
-template <typename T, int PRED, bool FINEST, bool INTERIOR, int LM = kLearnNone, class Acc>
-__device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
-                                             const QuantParams& qp, const T* lut, const ChunkIndex& ci, int x, int y,
-                                             int z, int (&q)[7], const LearnedArgs<T>& la = LearnedArgs<T>(),
-                                             const int* acc3 = nullptr)
+// One coarse point of the encoder after its 7 predictions p: fine values,
+// residuals, codes, unpredictable values, decoded fine cell (r0 = the coarse
+// value at the point, which is the decoded cell's parity-0 value).
+template <typename T, bool FINEST>
+__device__ __forceinline__ void encode_residuals(const EncodeIO<T>& io, const LevelGeom& geo, const QuantParams& qp,
+                                                 const T* lut, const ChunkIndex& ci, int x, int y, int z,
+                                                 const T (&p)[7], T r0, int (&q)[7])
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -132,9 +132,6 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
                           (size_t)s * (2 * x + px));
         }
     }
-    T p[7];
-    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
-    apply_learned<LM>(r, la, acc3, p);
     int chunk;
     const size_t cm = ci.at(z, chunk);
     const size_t n = geo.n;
@@ -152,7 +149,7 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
         if constexpr (!FINEST) v[b + 1] = A::add(code ? recover_lut(lut, code, qp) : d, p[b]);
     }
     if constexpr (!FINEST) {
-        v[0] = r(0);
+        v[0] = r0;
         const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -163,6 +160,20 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
             *reinterpret_cast<T2*>(io.G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
         }
     }
+}
+
+// One coarse point of the encoder: fine values, 7 predictions, residuals,
+// codes, unpredictable values, decoded fine cell.
+template <typename T, int PRED, bool FINEST, bool INTERIOR, int LM = kLearnNone, class Acc>
+__device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
+                                             const QuantParams& qp, const T* lut, const ChunkIndex& ci, int x, int y,
+                                             int z, int (&q)[7], const LearnedArgs<T>& la = LearnedArgs<T>(),
+                                             const int* acc3 = nullptr)
+{
+    T p[7];
+    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    apply_learned<LM>(r, la, acc3, p);
+    encode_residuals<T, FINEST>(io, geo, qp, lut, ci, x, y, z, p, FINEST ? T(0) : r(0), q);
 }
 
 template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
@@ -252,12 +263,13 @@ __global__ void __launch_bounds__(256) k_level_encode_shell(EncodeIO<T> io, cons
     hist_flush_center(nullptr, 0, 0, hist, center);
 }
 
-// One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
-template <typename T, int PRED, bool INTERIOR, int LM = kLearnNone, class Acc>
-__device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp, const T* lut,
-                                             const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
-                                             T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z,
-                                             const LearnedArgs<T>& la = LearnedArgs<T>(), const int* acc3 = nullptr)
+// One coarse point of the decoder after its 7 predictions p: codes -> dq,
+// x' = dq + p, the merged fine cell (r0 = the coarse value at the point).
+template <typename T>
+__device__ __forceinline__ void decode_values(const LevelGeom& geo, const QuantParams& qp, const T* lut,
+                                              const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
+                                              T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z,
+                                              const T (&p)[7], T r0)
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -267,11 +279,8 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     int q[7];
 #pragma unroll
     for (int b = 0; b < 7; ++b) q[b] = __ldg(codes + (size_t)b * n + cm);
-    T p[7];
-    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
-    apply_learned<LM>(r, la, acc3, p);
     T v[8];
-    v[0] = r(0);
+    v[0] = r0;
 #pragma unroll
     for (int b = 0; b < 7; ++b) {
         const T dq = q[b] ? recover_lut(lut, q[b], qp) : __ldg(unpred_dense + (size_t)b * n + cm);
@@ -286,6 +295,19 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
         t.y = v[2 * k + 1];
         *reinterpret_cast<T2*>(G + (size_t)(2 * z + pz) * gsy + (size_t)(2 * y + py) * gsx + 2 * (size_t)x) = t;
     }
+}
+
+// One coarse point of the decoder: codes -> dq, + 7 predictions, merged cell.
+template <typename T, int PRED, bool INTERIOR, int LM = kLearnNone, class Acc>
+__device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo, const QuantParams& qp, const T* lut,
+                                             const uint16_t* __restrict__ codes, const T* __restrict__ unpred_dense,
+                                             T* __restrict__ G, const ChunkIndex& ci, int x, int y, int z,
+                                             const LearnedArgs<T>& la = LearnedArgs<T>(), const int* acc3 = nullptr)
+{
+    T p[7];
+    predict7<PRED>(r, INTERIOR, x, y, z, geo.dx, geo.dy, geo.dz, p);
+    apply_learned<LM>(r, la, acc3, p);
+    decode_values<T>(geo, qp, lut, codes, unpred_dense, G, ci, x, y, z, p, r(0));
 }
 
 template <typename T, int PRED, int LM, int ZB = kZSmall>
