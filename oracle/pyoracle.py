@@ -345,6 +345,57 @@ def ref_round_trip(field: np.ndarray, eb: float, mults=(0.7, 2.7, 8.2), radius: 
     return {"K": K, "codes": codes, "unpred": unpred, "grids": grids, "closed_loop_ok": closed_loop_ok}
 
 
+def ref_round_trip_plain(field: np.ndarray, eb: float, mults=(1.0, 2.5, 6.25), radius: int = 32768,
+                         chunk_high: int = 32, chunk_low: int = 16) -> dict:
+    """The plain tricubic pipeline of the reference's artifact programs
+    (src/float.cpp / src/double.cpp main: preprocess_block on each level's
+    7 odd-parity sub-blocks against the decoded coarser grid, the linear
+    quantizer at multiplier x eb with multipliers 1 / 2.5 / 6.25 for base /
+    low / high, float.cpp:598, 634, 706; decode by depreprocess_block and
+    merge_sub_blocks_to_full), with the predictor from src/stz-rd.cpp and the
+    quantizer, dequantizer and merge from FD5, all compiled from source
+    (oracle/_ref), driven through this project's hierarchy. Returns the same
+    record as ref_round_trip."""
+    a = np.ascontiguousarray(field)
+    nz, ny, nx = a.shape
+    K = num_levels(nx, ny, nz)
+    S = 1 << K
+    suf = _suf(a.dtype)
+    R, D = ref(), rd()
+    grid = np.ascontiguousarray(a[::S, ::S, ::S])
+    grids, codes, unpred = [grid], [], []
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = a if s == 1 else np.ascontiguousarray(a[::s, ::s, ::s])
+        ebk = (mults[2] if k == K else mults[1] if k == K - 1 else mults[0]) * eb
+        dz, dy, dx = grid.shape
+        n = dx * dy * dz
+        C_ = oracle().stzo_level_chunk(nx, ny, nz, k, chunk_high, chunk_low)
+        subs = np.empty((8, dz, dy, dx), a.dtype)
+        getattr(R, "fd5ref_slice_full_data_" + suf)(_p(fine), _p(subs), 2 * dx, 2 * dy, 2 * dz)
+        out = np.empty((8, dz, dy, dx), a.dtype)
+        out[0] = grid
+        lc, lu = [], []
+        for b in range(7):
+            diff = np.empty((dz, dy, dx), a.dtype)
+            getattr(D, "rdref_preprocess_block_" + suf)(b, _p(subs[b + 1]), _p(grid), _p(diff), dx, dy, dz)
+            q = np.empty(n, np.int32)
+            u = np.empty(n, a.dtype)
+            nu = getattr(R, "fd5ref_quantize_range_nodec_" + suf)(_p(diff), n, ebk, radius, _p(q), _p(u), n)
+            lc.append(chunk_major(q, (dz, dy, dx), C_).astype(np.uint16))
+            lu.append(int(nu))
+            dq = ref_dequantize(q, ebk, radius, u[:nu], a.dtype).reshape(dz, dy, dx)
+            getattr(D, "rdref_depreprocess_block_" + suf)(b, _p(dq), _p(grid), _p(out[b + 1]), dx, dy, dz, dx, dy,
+                                                           dz, 0, 0, 0)
+        nxt = np.empty((2 * dz, 2 * dy, 2 * dx), a.dtype)
+        getattr(R, "fd5ref_merge_sub_blocks_to_full_" + suf)(_p(out), _p(nxt), dx, dy, dz)
+        codes.append(lc)
+        unpred.append(lu)
+        grid = nxt
+        grids.append(grid)
+    return {"K": K, "codes": codes, "unpred": unpred, "grids": grids, "closed_loop_ok": True}
+
+
 def plan(dims_xyz, chunk_high, chunk_low, a, b, use_ref=False) -> np.ndarray:
     out = np.zeros(1 << 20, dtype=np.int64)
     fn = ref().fd5ref_plan if use_ref else oracle().stzo_plan

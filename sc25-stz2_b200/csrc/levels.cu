@@ -23,9 +23,7 @@
 // merge, zslab preprocess/depreprocess, ROI depreprocess, quantize,
 // dequantize) for callers that drive the stages themselves.
 #include <algorithm>
-#include <cstdlib>
 #include <cstring>
-#include <type_traits>
 
 #include <cuda_runtime.h>
 
@@ -193,7 +191,6 @@ __device__ __forceinline__ T recover_lut(const T* lut, int q, const QuantParams&
 }
 
 #include "level_kernels.cuh"
-#include "level_pair.cuh"
 
 // Coarsest grid of the hierarchy: every 2^K-th point of the field.
 template <typename T>
@@ -512,18 +509,6 @@ void allow_smem(K kernel, size_t bytes)
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// The paired f32 interior kernels (level_pair.cuh) are the default;
-// STZ_LEVEL_KERNEL=scalar selects the one-point-per-step kernels (same
-// results), for comparisons.
-bool pair_kernels_enabled()
-{
-    static const bool on = [] {
-        const char* e = std::getenv("STZ_LEVEL_KERNEL");
-        return !(e && std::strcmp(e, "scalar") == 0);
-    }();
-    return on;
-}
-
 }  // namespace
 
 template <typename T>
@@ -550,19 +535,10 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
         cudaEventRecord(a.side.fork, st);
         cudaStreamWaitEvent(ss, a.side.fork, 0);
     }
-    const bool pair = std::is_same<T, float>::value && !learned && pair_kernels_enabled();
-    const size_t psm = big ? pair_tile_bytes<kZBig>() : pair_tile_bytes<kZSmall>();
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
         if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
-        if constexpr (std::is_same<T, float>::value) {                                                             \
-            if (interior && pair) {                                                                                \
-                auto kern = big ? k_level_encode_pair<P, F, kZBig> : k_level_encode_pair<P, F, kZSmall>;          \
-                allow_smem(kern, psm);                                                                             \
-                kern<<<grd, blk, psm, st>>>(io, a.coarse, g, a.qp, h);                                             \
-            }                                                                                                      \
-        }                                                                                                          \
-        if (interior && !pair) {                                                                                   \
+        if (interior) {                                                                                            \
             auto kern = big                          ? k_level_encode<T, P, F, kLearnNone, kZBig>                  \
                         : !learned               ? k_level_encode<T, P, F, kLearnNone>                         \
                         : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
@@ -609,20 +585,11 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
         cudaEventRecord(a.side.fork, st);
         cudaStreamWaitEvent(ss, a.side.fork, 0);
     }
-    const bool pair = std::is_same<T, float>::value && !learned && pair_kernels_enabled();
-    const size_t psm = big ? pair_tile_bytes<kZBig>() : pair_tile_bytes<kZSmall>();
 #define STZ_DEC(P)                                                                                                 \
     do {                                                                                                           \
         if (ns && par)                                                                                             \
             k_level_decode_shell<T, P><<<gs, 256, 0, ss>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
-        if constexpr (std::is_same<T, float>::value) {                                                             \
-            if (interior && pair) {                                                                                \
-                auto kern = big ? k_level_decode_pair<P, kZBig> : k_level_decode_pair<P, kZSmall>;                \
-                allow_smem(kern, psm);                                                                             \
-                kern<<<grd, blk, psm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out);                   \
-            }                                                                                                      \
-        }                                                                                                          \
-        if (interior && !pair) {                                                                                   \
+        if (interior) {                                                                                            \
             auto kern = big                          ? k_level_decode<T, P, kLearnNone, kZBig>                     \
                         : !learned               ? k_level_decode<T, P, kLearnNone>                            \
                         : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \

@@ -1,6 +1,6 @@
 """Full-size parity against the reference's own code (oracle/_ref: the FD5
-level functions compiled unmodified from the reference's sources), on the
-benchmark configurations:
+level functions and src/stz-rd.cpp compiled unmodified from the reference's
+sources), on the benchmark configurations:
 
 * 256^3 f32 GRF k^-11/3, rel eb 1e-3;
 * 512^3 f32 lognormal exp(1.5 g), rel eb 1e-3 (the timed workload);
@@ -10,7 +10,12 @@ For each: every level's quant codes of every block (the GPU stream's symbols
 against the reference's quantize_range_nodec output in the container's
 chunk-major order), the unpredictable counts, the full decode and every
 progressive level, bit for bit. The reference runs at the eb the GPU stream
-records, through the same hierarchy (pyoracle.ref_round_trip)."""
+records, through the same hierarchy (pyoracle.ref_round_trip).
+
+The plain tricubic pipeline of src/float.cpp / src/double.cpp (predictor
+STZ_PRED_CUBIC, multipliers 1 / 2.5 / 6.25, float.cpp:598, 634, 706) is
+checked the same way against src/stz-rd.cpp's stencils and FD5's quantizer
+(pyoracle.ref_round_trip_plain)."""
 import numpy as np
 import pytest
 
@@ -26,11 +31,14 @@ def _bits(a):
     return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
 
 
-def _check_against_reference(ctx, s, field_host):
-    if not po.ref_available():
+def _check_against_reference(ctx, s, field_host, plain=False):
+    if not (po.ref_available() and po.rd_available()):
         pytest.skip("oracle/_ref (the reference build) is missing")
     inf = s.info()
-    ref = po.ref_round_trip(field_host, inf.eb)
+    if plain:
+        ref = po.ref_round_trip_plain(field_host, inf.eb, inf.mults)
+    else:
+        ref = po.ref_round_trip(field_host, inf.eb)
     K = ref["K"]
     assert ref["closed_loop_ok"]
     for k in range(1, K + 1):
@@ -74,3 +82,18 @@ def test_fronts_384_f64_matches_reference(ctx, rel):
         assert sum(sum(c) for c in ref["unpred"]) > 0
     E = rel * (float(fh.max()) - float(fh.min()))
     assert np.abs(out - fh).max() <= E
+
+
+@pytest.mark.parametrize("case", ["grf256_f32_1e-3", "fronts128_f64_1e-6"])
+def test_plain_cubic_pipeline_matches_reference(ctx, case):
+    from stz_b200 import fields
+
+    if case.startswith("grf"):
+        f, rel = fields.grf((256, 256, 256), 11.0 / 3.0, 2025), 1e-3
+    else:
+        f, rel = fields.fronts((128, 128, 128), 11, np.float64, device="cuda:0").cpu().numpy(), 1e-6
+    s = ctx.compress(f, eb=rel, eb_mode="rel", predictor=1, mult_base=1.0, mult_low=2.5, mult_high=6.25)
+    assert s.info().mults == (1.0, 2.5, 6.25)
+    ref, out = _check_against_reference(ctx, s, f, plain=True)
+    E = rel * (float(f.max()) - float(f.min()))
+    assert np.abs(out.astype(np.float64) - f).max() <= E

@@ -132,6 +132,32 @@ def test_oracle_stream_matches_reference_at_size(case):
         assert sum(sum(c) for c in ref["unpred"]) > 0
 
 
+@pytest.mark.skipif(not (po.ref_available() and po.rd_available()), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("case", ["grf64_f32_1e-3", "fronts64_f64_1e-6"])
+def test_oracle_plain_pipeline_matches_reference(case):
+    """The plain tricubic pipeline of src/float.cpp / src/double.cpp (stz-rd
+    stencils, multipliers 1 / 2.5 / 6.25): the oracle's stream against the
+    reference's functions through the hierarchy (pyoracle.ref_round_trip_plain)."""
+    from stz_b200 import fields
+
+    if case.startswith("grf"):
+        f, rel = fields.grf((64, 64, 64), 11.0 / 3.0, 7, np.float32), 1e-3
+    else:
+        f, rel = fields.fronts((64, 64, 64), 3, np.float64), 1e-6
+    mults = (1.0, 2.5, 6.25)
+    eb = po.pointwise_eb(f, rel, mults)
+    ref = po.ref_round_trip_plain(f, eb, mults)
+    stream = po.compress(f, eb, predictor=1, mults=mults)
+    K = ref["K"]
+    for k in range(1, K + 1):
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), ref["codes"][k - 1][b]), (k, b)
+    u = np.uint64 if f.dtype == np.float64 else np.uint32
+    assert np.array_equal(po.decompress(stream).view(u), ref["grids"][K].view(u))
+    if rel == 1e-6:
+        assert sum(sum(c) for c in ref["unpred"]) > 0
+
+
 @pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
 def test_planner_matches_reference_live():
     rng = np.random.default_rng(17)
