@@ -176,6 +176,78 @@ __device__ __forceinline__ void encode_point(const Acc& r, const EncodeIO<T>& io
     encode_residuals<T, FINEST>(io, geo, qp, lut, ci, x, y, z, p, FINEST ? T(0) : r(0), q);
 }
 
+// Interior point of the plain encoder (no learned correction), the same
+// values as encode_point. A residual under the quantizer's early-exit bound
+// is a centre code, counted in a register; only the others run the full
+// quantizer, and only they touch the shared histogram or, as code 0, the
+// unpredictable list (the histogram counts code 0 too, like hist_code). The
+// walk's chunk-major position, field row pointer fp and decoded-grid pointer
+// gp move along z with the thread instead of being recomputed per point.
+template <typename T, int PRED, bool FINEST, class Acc>
+__device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
+                                                const QuantParams& qp, const T* lut, const ZWalk& zw,
+                                                const T* __restrict__ fp, T* __restrict__ gp, uint32_t (*sh)[kSmemBins],
+                                                int wlo, int wn, const HistArgs& hist, uint32_t (&center)[7])
+{
+    using A = Ar<T>;
+    using T2 = typename V2<T>::type;
+    T p[7];
+    predict7_interior_only<PRED>(r, p);
+    T o[8];
+    if constexpr (FINEST) {
+        const size_t fsx = io.fsx, fsy = io.fsy;
+        const T2 t0 = __ldg(reinterpret_cast<const T2*>(fp));
+        const T2 t1 = __ldg(reinterpret_cast<const T2*>(fp + fsx));
+        const T2 t2 = __ldg(reinterpret_cast<const T2*>(fp + fsy));
+        const T2 t3 = __ldg(reinterpret_cast<const T2*>(fp + fsy + fsx));
+        o[1] = t0.y, o[2] = t1.x, o[3] = t1.y, o[4] = t2.x, o[5] = t2.y, o[6] = t3.x, o[7] = t3.y;
+    } else {
+        const size_t s = (size_t)io.s, sx = s * io.fsx, sy = s * io.fsy;
+#pragma unroll
+        for (int si = 1; si < 8; ++si) {
+            const int px = si & 1, py = (si >> 1) & 1, pz = si >> 2;
+            o[si] = __ldg(fp + (pz ? sy : 0) + (py ? sx : 0) + (px ? s : 0));
+        }
+    }
+    const size_t n = geo.n;
+    uint16_t* __restrict__ cp = io.codes + zw.cm;
+    T v[8];
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const T d = A::sub(o[b + 1], p[b]);
+        int code = qp.radius;
+        if (quantize_is_centre(d, qp)) {
+            ++center[b];
+        } else {
+            code = quantize_full(d, qp);
+            if (code == qp.radius) {
+                ++center[b];
+            } else {
+                hist_add(sh, wlo, wn, hist, b, code, 1u);
+                if (code == 0) {
+                    io.unpred_dense[(size_t)b * n + zw.cm] = d;
+                    atomicAdd(&io.unpred_cnt[(size_t)b * (geo.nchunks() + 1) + zw.chunk], 1u);
+                }
+            }
+        }
+        cp[(size_t)b * n] = (uint16_t)code;
+        if constexpr (!FINEST) v[b + 1] = A::add(code ? recover_lut(lut, code, qp) : d, p[b]);
+    }
+    if constexpr (!FINEST) {
+        v[0] = r(0);
+        const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
+        T2 t;
+        t.x = v[0], t.y = v[1];
+        *reinterpret_cast<T2*>(gp) = t;
+        t.x = v[2], t.y = v[3];
+        *reinterpret_cast<T2*>(gp + gsx) = t;
+        t.x = v[4], t.y = v[5];
+        *reinterpret_cast<T2*>(gp + gsy) = t;
+        t.x = v[6], t.y = v[7];
+        *reinterpret_cast<T2*>(gp + gsy + gsx) = t;
+    }
+}
+
 template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                          QuantParams qp, HistArgs hist, LearnedArgs<T> la)
@@ -208,7 +280,23 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     [[maybe_unused]] uint32_t phase = 0;
     [[maybe_unused]] bool tc_failed = false;
     if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
-    for (int z = z0; z < z1; ++z) {
+    if constexpr (LM == kLearnNone) {
+        ZWalk zw;
+        zw.init(geo, x, y, z0);
+        const size_t s = (size_t)io.s;
+        const T* fp = io.field + s * (2 * (size_t)z0) * io.fsy + s * (2 * (size_t)y) * io.fsx + s * 2 * (size_t)x;
+        const size_t fstep = 2 * s * io.fsy;
+        const size_t gsy = 4 * (size_t)geo.dx * geo.dy;
+        T* gp = FINEST ? nullptr : io.G + (2 * (size_t)z0) * gsy + (2 * (size_t)y) * 2 * geo.dx + 2 * (size_t)x;
+        for (int z = z0; z < z1; ++z) {
+            const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+            if (valid) encode_interior<T, PRED, FINEST>(r, io, geo, qp, lut, zw, fp, gp, sh, wlo, wn, hist, center);
+            zw.next();
+            fp += fstep;
+            if constexpr (!FINEST) gp += 2 * gsy;
+        }
+    }
+    for (int z = z0; z < z1 && LM != kLearnNone; ++z) {
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};
         const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
         int acc3[7];
@@ -310,6 +398,43 @@ __device__ __forceinline__ void decode_point(const Acc& r, const LevelGeom& geo,
     decode_values<T>(geo, qp, lut, codes, unpred_dense, G, ci, x, y, z, p, r(0));
 }
 
+// Interior point of the plain decoder (no learned correction), the same
+// values as decode_point, with the walk's chunk-major position and the output
+// pointer gp (the cell's first fine value) moving along z with the thread.
+template <typename T, int PRED, class Acc>
+__device__ __forceinline__ void decode_interior(const Acc& r, const LevelGeom& geo, const QuantParams& qp,
+                                                const T* lut, const uint16_t* __restrict__ codes,
+                                                const T* __restrict__ unpred_dense, const ZWalk& zw,
+                                                T* __restrict__ gp)
+{
+    using A = Ar<T>;
+    using T2 = typename V2<T>::type;
+    const size_t n = geo.n;
+    T p[7];
+    predict7_interior_only<PRED>(r, p);
+    const uint16_t* __restrict__ cp = codes + zw.cm;
+    int q[7];
+#pragma unroll
+    for (int b = 0; b < 7; ++b) q[b] = __ldg(cp + (size_t)b * n);
+    T v[8];
+    v[0] = r(0);
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const T dq = q[b] ? recover_lut(lut, q[b], qp) : __ldg(unpred_dense + (size_t)b * n + zw.cm);
+        v[b + 1] = A::add(dq, p[b]);
+    }
+    const size_t gsx = 2 * (size_t)geo.dx, gsy = 4 * (size_t)geo.dx * geo.dy;
+    T2 t;
+    t.x = v[0], t.y = v[1];
+    *reinterpret_cast<T2*>(gp) = t;
+    t.x = v[2], t.y = v[3];
+    *reinterpret_cast<T2*>(gp + gsx) = t;
+    t.x = v[4], t.y = v[5];
+    *reinterpret_cast<T2*>(gp + gsy) = t;
+    t.x = v[6], t.y = v[7];
+    *reinterpret_cast<T2*>(gp + gsy + gsx) = t;
+}
+
 template <typename T, int PRED, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
@@ -336,9 +461,22 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
     if constexpr (LM != kLearnTc) {
         if (!valid) return;
     }
+    const int z1 = min(z0 + ZB, dz - 2);
+    if constexpr (LM == kLearnNone) {
+        ZWalk zw;
+        zw.init(geo, x, y, z0);
+        const size_t gsy = 4 * (size_t)dx * dy;
+        T* gp = G + (2 * (size_t)z0) * gsy + (2 * (size_t)y) * 2 * dx + 2 * (size_t)x;
+        for (int z = z0; z < z1; ++z) {
+            const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+            decode_interior<T, PRED>(r, geo, qp, lut, codes, unpred_dense, zw, gp);
+            zw.next();
+            gp += 2 * gsy;
+        }
+        return;
+    }
     ChunkIndex ci;
     ci.init(geo, x, y);
-    const int z1 = min(z0 + ZB, dz - 2);
     [[maybe_unused]] uint32_t phase = 0;
     [[maybe_unused]] bool tc_failed = false;
     if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);

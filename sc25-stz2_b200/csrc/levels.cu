@@ -175,6 +175,38 @@ struct ChunkIndex {
     }
 };
 
+// The same position, advanced along z by one thread's walk down its column:
+// inside a chunk the next z is C*C codes further, at a chunk boundary the walk
+// jumps to the chunk above (ncx*ncy chunks on).
+struct ZWalk {
+    size_t cm;   // chunk-major position of (x, y, z)
+    int chunk;   // its chunk
+    int lz, C;
+    size_t plane, jump;
+    int chunk_step;
+    __device__ __forceinline__ void init(const LevelGeom& g, int x, int y, int z)
+    {
+        ChunkIndex ci;
+        ci.init(g, x, y);
+        cm = ci.at(z, chunk);
+        C = g.C;
+        lz = z % C;
+        plane = (size_t)C * C;
+        chunk_step = g.ncx * g.ncy;
+        jump = (size_t)chunk_step * C * C * C - (size_t)(C - 1) * C * C;
+    }
+    __device__ __forceinline__ void next()
+    {
+        if (++lz == C) {
+            lz = 0;
+            chunk += chunk_step;
+            cm += jump;
+        } else {
+            cm += plane;
+        }
+    }
+};
+
 // Recover table for the codes around the radius (the reference's recover LUT,
 // FD5:1528-1535): one shared load instead of int->double->T conversions.
 constexpr int kRecW = 256;

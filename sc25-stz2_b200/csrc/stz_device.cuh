@@ -369,6 +369,19 @@ __device__ __forceinline__ T predict_interior_at(const Acc& r)
     else return dynamic_interior<BLOCK, T>(r);
 }
 
+// The 7 interior predictions of one coarse point (1 <= x,y,z <= dim-3).
+template <int PRED, typename T, class Acc>
+__device__ __forceinline__ void predict7_interior_only(const Acc& r, T (&p)[7])
+{
+    p[0] = predict_interior_at<PRED, 0, T>(r);
+    p[1] = predict_interior_at<PRED, 1, T>(r);
+    p[2] = predict_interior_at<PRED, 2, T>(r);
+    p[3] = predict_interior_at<PRED, 3, T>(r);
+    p[4] = predict_interior_at<PRED, 4, T>(r);
+    p[5] = predict_interior_at<PRED, 5, T>(r);
+    p[6] = predict_interior_at<PRED, 6, T>(r);
+}
+
 // The 7 predictions of one coarse point (interior: 1 <= x,y,z <= dim-3).
 template <int PRED, typename T, class Acc>
 __device__ __forceinline__ void predict7(const Acc& r, bool interior, int x, int y, int z, int dx, int dy, int dz,
@@ -506,17 +519,32 @@ __device__ __forceinline__ T predict(int block, const Grid<T>& g, int x, int y, 
 }
 
 // quantize_range_nodec for one residual (FD5:1216-1229). Returns the shifted
-// code, 0 when unpredictable. The half == 0 case (|d|/eb < 1) is taken first:
-// there the decompressed value is +-0 and the check reduces to |d| <= eb.
+// code, 0 when unpredictable. quantize_is_centre is the early exit: |d| below
+// the precomputed threshold tlo guarantees the centre code (QuantParams).
+// quantize_full is the whole computation; its half == 0 case (|d|/eb < 1) is
+// taken first: there the decompressed value is +-0 and the check reduces to
+// |d| <= eb.
+template <typename T>
+__device__ __forceinline__ bool quantize_is_centre(T d, const QuantParams& qp)
+{
+    if constexpr (sizeof(T) == 4) return fabsf(d) < qp.tlo32;
+    else return fabs(d) < qp.tlo64;
+}
+
+template <typename T>
+__device__ __forceinline__ int quantize_full(T d, const QuantParams& qp);
+
 template <typename T>
 __device__ __forceinline__ int quantize(T d, const QuantParams& qp)
 {
+    if (quantize_is_centre(d, qp)) return qp.radius;
+    return quantize_full(d, qp);
+}
+
+template <typename T>
+__device__ __forceinline__ int quantize_full(T d, const QuantParams& qp)
+{
     using A = Ar<T>;
-    if constexpr (sizeof(T) == 4) {
-        if (fabsf(d) < qp.tlo32) return qp.radius;
-    } else {
-        if (fabs(d) < qp.tlo64) return qp.radius;
-    }
     const double dd = fabs(A::to_f64(d));
     const double ad = d_mul(dd, qp.recip);
     if (ad < 1.0) return dd <= qp.eb ? qp.radius : 0;
