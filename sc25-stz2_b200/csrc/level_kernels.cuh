@@ -56,6 +56,65 @@ struct Shell {
     }
 };
 
+// Boundary points owned by an interior CTA (plain kernels). Along an axis
+// of size d the interior indices [1, d-3] are split into bricks of B; the
+// first brick also owns index 0 and the last one indices d-2 and d-1, so a
+// CTA owns the contiguous range [a, b) around its interior range [i0, i1).
+// Its halo tile covers [i0-1, i0+B+1], which holds every tap of the owned
+// boundary points: their boundary rules read the point and its forward
+// neighbour, their other axes the usual -1..+2 stencil inside [i0, i1).
+struct OwnedAxis {
+    int a, i0, i1, b;
+    __device__ __forceinline__ static OwnedAxis make(int d, int blk, int nblk, int B)
+    {
+        OwnedAxis o;
+        o.i0 = 1 + blk * B;
+        o.i1 = min(o.i0 + B, d - 2);
+        o.a = blk == 0 ? 0 : o.i0;
+        o.b = blk == nblk - 1 ? d : o.i1;
+        return o;
+    }
+    __device__ __forceinline__ int n() const { return b - a; }
+    __device__ __forceinline__ int ni() const { return i1 - i0; }
+    __device__ __forceinline__ int nb() const { return (i0 - a) + (b - i1); }
+    // k-th owned boundary index (k < nb())
+    __device__ __forceinline__ int bnd(int k) const { return k < i0 - a ? a + k : i1 + (k - (i0 - a)); }
+};
+
+// The owned boundary points of this CTA as three disjoint boxes: z outside
+// the interior range (all owned x, y); z inside, y outside (all owned x); z
+// and y inside, x outside. f(x, y, z) for each, spread over the CTA's threads.
+template <class F>
+__device__ __forceinline__ void for_owned_boundary(const LevelGeom& g, int ZB, int tid, int nthreads, F&& f)
+{
+    const OwnedAxis X = OwnedAxis::make(g.dx, blockIdx.x, gridDim.x, BX);
+    const OwnedAxis Y = OwnedAxis::make(g.dy, blockIdx.y, gridDim.y, BY);
+    const OwnedAxis Z = OwnedAxis::make(g.dz, blockIdx.z, gridDim.z, ZB);
+    const int ga = X.n() * Y.n() * Z.nb();
+    const int gb = X.n() * Y.nb() * Z.ni();
+    const int gc = X.nb() * Y.ni() * Z.ni();
+    for (int i = tid; i < ga + gb + gc; i += nthreads) {
+        int x, y, z;
+        if (i < ga) {
+            const int nxy = X.n() * Y.n();
+            z = Z.bnd(i / nxy);
+            const int r = i % nxy;
+            y = Y.a + r / X.n(), x = X.a + r % X.n();
+        } else if (i < ga + gb) {
+            const int j = i - ga, nxy = X.n() * Y.nb();
+            z = Z.i0 + j / nxy;
+            const int r = j % nxy;
+            y = Y.bnd(r / X.n()), x = X.a + r % X.n();
+        } else {
+            const int j = i - ga - gb, nxy = X.nb() * Y.ni();
+            z = Z.i0 + j / nxy;
+            const int r = j % nxy;
+            y = Y.i0 + r / X.nb(), x = X.bnd(r % X.nb());
+        }
+        f(x, y, z);
+    }
+}
+
 template <typename T>
 struct EncodeIO {
     const T* __restrict__ field;
@@ -295,6 +354,19 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
             fp += fstep;
             if constexpr (!FINEST) gp += 2 * gsy;
         }
+        // the CTA's owned boundary points, predicted from the same tile
+        for_owned_boundary(geo, ZB, tid, BX * BY, [&](int bx, int by, int bz) {
+            const TileAt<T, TSX, TPLANE> r{tile + (bz - z0 + 1) * TPLANE + (by - y0 + 1) * TSX + (bx - x0 + 1)};
+            ChunkIndex bci;
+            bci.init(geo, bx, by);
+            int q[7];
+            encode_point<T, PRED, FINEST, false>(r, io, geo, qp, lut, bci, bx, by, bz, q);
+#pragma unroll
+            for (int b = 0; b < 7; ++b) {
+                if (q[b] == qp.radius) ++center[b];
+                else hist_add(sh, wlo, wn, hist, b, q[b], 1u);
+            }
+        });
     }
     for (int z = z0; z < z1 && LM != kLearnNone; ++z) {
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};
@@ -458,22 +530,31 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool valid = x <= dx - 3 && y <= dy - 3;
-    if constexpr (LM != kLearnTc) {
-        if (!valid) return;
-    }
     const int z1 = min(z0 + ZB, dz - 2);
     if constexpr (LM == kLearnNone) {
-        ZWalk zw;
-        zw.init(geo, x, y, z0);
-        const size_t gsy = 4 * (size_t)dx * dy;
-        T* gp = G + (2 * (size_t)z0) * gsy + (2 * (size_t)y) * 2 * dx + 2 * (size_t)x;
-        for (int z = z0; z < z1; ++z) {
-            const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-            decode_interior<T, PRED>(r, geo, qp, lut, codes, unpred_dense, zw, gp);
-            zw.next();
-            gp += 2 * gsy;
+        if (valid) {
+            ZWalk zw;
+            zw.init(geo, x, y, z0);
+            const size_t gsy = 4 * (size_t)dx * dy;
+            T* gp = G + (2 * (size_t)z0) * gsy + (2 * (size_t)y) * 2 * dx + 2 * (size_t)x;
+            for (int z = z0; z < z1; ++z) {
+                const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
+                decode_interior<T, PRED>(r, geo, qp, lut, codes, unpred_dense, zw, gp);
+                zw.next();
+                gp += 2 * gsy;
+            }
         }
+        // the CTA's owned boundary points, predicted from the same tile
+        for_owned_boundary(geo, ZB, tid, BX * BY, [&](int bx, int by, int bz) {
+            const TileAt<T, TSX, TPLANE> r{tile + (bz - z0 + 1) * TPLANE + (by - y0 + 1) * TSX + (bx - x0 + 1)};
+            ChunkIndex bci;
+            bci.init(geo, bx, by);
+            decode_point<T, PRED, false>(r, geo, qp, lut, codes, unpred_dense, G, bci, bx, by, bz);
+        });
         return;
+    }
+    if constexpr (LM != kLearnTc) {
+        if (!valid) return;
     }
     ChunkIndex ci;
     ci.init(geo, x, y);
