@@ -56,7 +56,7 @@ struct Shell {
     }
 };
 
-// Boundary points owned by an interior CTA (plain kernels). Along an axis
+// Boundary points owned by an interior CTA (plain decode kernels). Along an axis
 // of size d the interior indices [1, d-3] are split into bricks of B; the
 // first brick also owns index 0 and the last one indices d-2 and d-1, so a
 // CTA owns the contiguous range [a, b) around its interior range [i0, i1).
@@ -354,19 +354,6 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
             fp += fstep;
             if constexpr (!FINEST) gp += 2 * gsy;
         }
-        // the CTA's owned boundary points, predicted from the same tile
-        for_owned_boundary(geo, ZB, tid, BX * BY, [&](int bx, int by, int bz) {
-            const TileAt<T, TSX, TPLANE> r{tile + (bz - z0 + 1) * TPLANE + (by - y0 + 1) * TSX + (bx - x0 + 1)};
-            ChunkIndex bci;
-            bci.init(geo, bx, by);
-            int q[7];
-            encode_point<T, PRED, FINEST, false>(r, io, geo, qp, lut, bci, bx, by, bz, q);
-#pragma unroll
-            for (int b = 0; b < 7; ++b) {
-                if (q[b] == qp.radius) ++center[b];
-                else hist_add(sh, wlo, wn, hist, b, q[b], 1u);
-            }
-        });
     }
     for (int z = z0; z < z1 && LM != kLearnNone; ++z) {
         int q[7] = {-1, -1, -1, -1, -1, -1, -1};

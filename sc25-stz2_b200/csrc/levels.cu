@@ -559,10 +559,10 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
                               : tile_bytes<T>();
-    // plain kernels predict the boundary shell themselves (owned boundary
-    // points); the shell kernel serves learned levels and levels without an
-    // interior
-    const uint64_t ns = (interior && !learned) ? 0 : shell.total();
+    // the boundary shell runs beside the interior on the side stream (folding
+    // it into the interior CTAs, as the decoder does, left the finest encode
+    // level and slowed the coarser ones, whose shells are a large share)
+    const uint64_t ns = shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
     const bool par = a.side.st && interior && ns;
     cudaStream_t ss = par ? a.side.st : st;
@@ -612,6 +612,9 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
                               : tile_bytes<T>();
+    // plain decode kernels predict their owned boundary points themselves
+    // from the halo tile; the shell kernel serves learned levels and levels
+    // without an interior
     const uint64_t ns = (interior && !learned) ? 0 : shell.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
     const bool par = a.side.st && interior && ns;
