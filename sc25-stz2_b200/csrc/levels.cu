@@ -68,6 +68,11 @@ struct V2<double> {
 constexpr int BX = 32, BY = 8;
 constexpr int kZSmall = 8, kZBig = 16;
 constexpr size_t kZBigPoints = size_t(1) << 23;
+// Levels of at most 2^18 coarse points (64^3) take 2-plane bricks: four times
+// the CTAs and a quarter of each thread's serial chain, for levels that are
+// too small to fill the device with 8-plane bricks.
+constexpr int kZTiny = 2;
+constexpr size_t kZTinyPoints = size_t(1) << 18;
 constexpr int TSX = BX + 3, TSY = BY + 3;
 constexpr int TPLANE = TSX * TSY;
 template <int ZB>
@@ -550,14 +555,17 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     const Shell shell = Shell::make(g.dx, g.dy, g.dz);
     dim3 blk(BX, BY, 1);
     const bool learned = a.learned.model && a.learned.flags;
-    const bool big = !learned && (size_t)g.dx * g.dy * g.dz >= kZBigPoints;
-    const int zb = big ? kZBig : kZSmall;
+    const size_t npts = (size_t)g.dx * g.dy * g.dz;
+    const bool big = !learned && npts >= kZBigPoints;
+    const bool tiny = !learned && npts <= kZTinyPoints;
+    const int zb = big ? kZBig : tiny ? kZTiny : kZSmall;
     dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + zb - 1) / zb);
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
     HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
     const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
+                      : tiny  ? tile_bytes<T, kZTiny>()
                               : tile_bytes<T>();
     // the boundary shell runs beside the interior on the side stream (folding
     // it into the interior CTAs, as the decoder does, left the finest encode
@@ -575,6 +583,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
         if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
         if (interior) {                                                                                            \
             auto kern = big                          ? k_level_encode<T, P, F, kLearnNone, kZBig>                  \
+                        : tiny                   ? k_level_encode<T, P, F, kLearnNone, kZTiny>                 \
                         : !learned               ? k_level_encode<T, P, F, kLearnNone>                         \
                         : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
                                                  : k_level_encode<T, P, F, kLearnDp4a>;                        \
@@ -605,12 +614,15 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
     const Shell shell = Shell::make(g.dx, g.dy, g.dz);
     dim3 blk(BX, BY, 1);
     const bool learned = a.learned.model && a.learned.flags;
-    const bool big = !learned && (size_t)g.dx * g.dy * g.dz >= kZBigPoints;
-    const int zb = big ? kZBig : kZSmall;
+    const size_t npts = (size_t)g.dx * g.dy * g.dz;
+    const bool big = !learned && npts >= kZBigPoints;
+    const bool tiny = !learned && npts <= kZTinyPoints;
+    const int zb = big ? kZBig : tiny ? kZTiny : kZSmall;
     dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + zb - 1) / zb);
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
+                      : tiny  ? tile_bytes<T, kZTiny>()
                               : tile_bytes<T>();
     // plain decode kernels predict their owned boundary points themselves
     // from the halo tile; the shell kernel serves learned levels and levels
@@ -629,6 +641,7 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
             k_level_decode_shell<T, P><<<gs, 256, 0, ss>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
         if (interior) {                                                                                            \
             auto kern = big                          ? k_level_decode<T, P, kLearnNone, kZBig>                     \
+                        : tiny                   ? k_level_decode<T, P, kLearnNone, kZTiny>                    \
                         : !learned               ? k_level_decode<T, P, kLearnNone>                            \
                         : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \
                                                  : k_level_decode<T, P, kLearnDp4a>;                           \
