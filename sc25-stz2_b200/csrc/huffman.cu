@@ -827,16 +827,12 @@ __device__ void decode_plane_seq(const DecodeTables* __restrict__ t, const Strea
 // lanes' code counts (a run symbol counts its run) then places each lane's
 // output. With run symbols the plane is first filled with the centre code,
 // so a lane writes only its literals. Output past the plane (a corrupt
-// stream) is dropped. Each lane keeps the symbols of its latest pass over
-// its slice (the one that turns out final) in the warp's shared buffer `sbuf`
-// (kSymBuf per lane, lane-interleaved; a lane touches only its own entries);
-// a lane whose slice held more decodes them again for the output.
-constexpr uint32_t kSymBuf = 16;
+// stream) is dropped.
 __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const StreamDesc& s, uint32_t W, bool active,
                                   uint32_t c, uint32_t lz,
                                   const uint16_t* __restrict__ cb_sym, const uint32_t* __restrict__ sub_off,
                                   const uint64_t* __restrict__ chunk_word_off, const uint32_t* __restrict__ payload,
-                                  uint16_t* __restrict__ codes, uint16_t* __restrict__ sbuf)
+                                  uint16_t* __restrict__ codes)
 {
     const uint32_t lane = threadIdx.x & (W - 1);
     const uint32_t C = s.C, P = C * C;
@@ -869,13 +865,8 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
     const uint32_t stop = b0 + min(nb, (lane + 1) * L);
     uint32_t D, LD;
     run_geometry(P, D, LD);
-    uint32_t start = b0 + min(nb, lane * L), cnt = 0, ns = 0;
-    const uint32_t l32 = threadIdx.x & 31;
-    auto count = [&](uint32_t sym) {
-        cnt += sym - base < J ? run_length(sym - base, D, LD) : 1u;
-        if (ns < kSymBuf) sbuf[ns * 32 + l32] = (uint16_t)sym;
-        ++ns;
-    };
+    uint32_t start = b0 + min(nb, lane * L), cnt = 0;
+    auto count = [&](uint32_t sym) { cnt += sym - base < J ? run_length(sym - base, D, LD) : 1u; };
     uint32_t end = decode_range(t, s, cb_sym, cb, start, stop, count);
     for (int round = 0; round < 32; ++round) {
         uint32_t prev = __shfl_up_sync(0xffffffffu, end, 1, W);
@@ -885,23 +876,14 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
         if (moved) {
             start = prev;
             cnt = 0;
-            ns = 0;
             end = decode_range(t, s, cb_sym, cb, start, stop, count);
         }
     }
     uint32_t q = group_scan(cnt, W, lane) - cnt;  // first output position
-    // the lane's symbols again: from the buffer, or decoded once more
-    auto replay = [&](auto&& f) {
-        if (ns <= kSymBuf) {
-            for (uint32_t k = 0; k < ns; ++k) f((uint32_t)sbuf[k * 32 + l32]);
-        } else {
-            decode_range(t, s, cb_sym, cb, start, stop, f);
-        }
-    };
     if (J) {
         fill((uint16_t)R);
         __syncwarp();
-        replay([&](uint32_t sym) {
+        decode_range(t, s, cb_sym, cb, start, stop, [&](uint32_t sym) {
             if (sym - base < J) {
                 q += run_length(sym - base, D, LD);
             } else {
@@ -910,7 +892,7 @@ __device__ void decode_plane_warp(const DecodeTables* __restrict__ t, const Stre
             }
         });
     } else {
-        replay([&](uint32_t sym) {
+        decode_range(t, s, cb_sym, cb, start, stop, [&](uint32_t sym) {
             if (active && q < P) dst[q] = (uint16_t)sym;
             ++q;
         });
@@ -955,22 +937,18 @@ __global__ void __launch_bounds__(kDecodeThreads, 5) k_decode(const CtaWork* __r
                              chunk_word_off, payload, codes);
         return;
     }
-    __shared__ uint16_t sbuf[kDecodeThreads / 32][kSymBuf * 32];
     const uint32_t W = lanes_per_plane(s.C * s.C), np = w.count * s.C;
     STZ_GROUP_PLANES(np, W)
     {
         STZ_GROUP_PLANE(np, W);
         decode_plane_warp(tabs + w.stream, s, W, active, chunk_ids[w.first + pe / s.C], pe % s.C, cb_sym, sub_off,
-                          chunk_word_off, payload, codes, sbuf[threadIdx.x >> 5]);
+                          chunk_word_off, payload, codes);
     }
 }
 
 // Persistent variant: a fixed grid walks the work list of a batch held in
 // device memory (BatchHdr at meta), so one captured launch serves any batch;
-// each item is cut into kDecodeSlices slices of 8 planes. In a batch of at
-// least kSeqMinItems items, dense streams decode one thread per plane (the
-// first slice of each item takes all its planes), as k_decode does for large
-// launches: under heavy load the batches are large and throughput counts.
+// each item is cut into kDecodeSlices slices of 8 planes.
 __global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __restrict__ meta,
                                                                const StreamDesc* __restrict__ sd,
                                                                const DecodeTables* __restrict__ tabs,
@@ -978,32 +956,23 @@ __global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __
                                                                const uint32_t* __restrict__ sub_off,
                                                                const uint64_t* __restrict__ chunk_word_off,
                                                                const uint32_t* __restrict__ payload,
-                                                               uint16_t* __restrict__ codes, uint32_t seq_bits)
+                                                               uint16_t* __restrict__ codes)
 {
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
     const uint32_t n = h->n_work;
     const CtaWork* __restrict__ work = reinterpret_cast<const CtaWork*>(meta + h->o_work);
     const uint32_t* __restrict__ chunk_ids = reinterpret_cast<const uint32_t*>(meta + h->o_ids);
     const uint32_t nw = blockDim.x >> 5, S = kDecodeSlices;
-    __shared__ uint16_t sbuf[kDecodeThreads / 32][kSymBuf * 32];
-    const uint32_t sb = n >= (uint32_t)kSeqMinItems ? seq_bits : 0xffffffffu;
     for (uint32_t u = blockIdx.x; u < n * S; u += gridDim.x) {
         const CtaWork w = work[u / S];
         const StreamDesc s = sd[w.stream];
-        if (decode_sequential(s, sb)) {  // uniform per block
-            const uint32_t t = threadIdx.x;
-            if (u % S == 0 && t < w.count * s.C)
-                decode_plane_seq(tabs + w.stream, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off,
-                                 chunk_word_off, payload, codes);
-            continue;
-        }
         const uint32_t W = lanes_per_plane(s.C * s.C), G = 32 / W, np = w.count * s.C;
         for (uint32_t base = ((u % S) * nw + (threadIdx.x >> 5)) * G; base < np; base += nw * S * G) {
             const uint32_t p = base + (threadIdx.x & 31) / W;
             const bool active = p < np;
             const uint32_t pe = active ? p : base;
             decode_plane_warp(tabs + w.stream, s, W, active, chunk_ids[w.first + pe / s.C], pe % s.C, cb_sym, sub_off,
-                              chunk_word_off, payload, codes, sbuf[threadIdx.x >> 5]);
+                              chunk_word_off, payload, codes);
         }
     }
 }
@@ -1186,7 +1155,7 @@ void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, cons
                        const uint32_t* payload, uint16_t* codes, cudaStream_t st)
 {
     k_decode_dyn<<<grid, kDecodeThreads, 0, st>>>(meta, sd, static_cast<const DecodeTables*>(tables), cb_sym, sub_off,
-                                                  chunk_word_off, payload, codes, decode_seq_bits());
+                                                  chunk_word_off, payload, codes);
 }
 
 template <typename T>
