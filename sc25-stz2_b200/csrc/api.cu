@@ -432,6 +432,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, st));
     STZ_CUDA(cudaStreamSynchronize(st));
+    if (level_error_take()) STZ_FAIL(STZ_ERR_CUDA, "level kernel: a TMA tile load did not complete in time");
     if (M && M->mask && learned_tc_error_take(st))
         STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
     lap.mark("levels + histograms");
@@ -1269,6 +1270,7 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     if (s->resident && s->resident->kmax >= kdec) {
         STZ_TRY(decode_levels<T>(ctx, s, *s->resident, kdec, out_dev));
         STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the output is complete on return
+        if (level_error_take()) STZ_FAIL(STZ_ERR_CUDA, "level kernel: a TMA tile load did not complete in time");
         if (stream_learned(s->dir) && learned_tc_error_take(ctx->st))
             STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
         return STZ_OK;
@@ -1286,6 +1288,7 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
         STZ_TRY(prepare(ctx, s, kdec, p, &fn));
     }
     STZ_CUDA(cudaStreamSynchronize(ctx->st));
+    if (level_error_take()) STZ_FAIL(STZ_ERR_CUDA, "level kernel: a TMA tile load did not complete in time");
     if (stream_learned(s->dir) && learned_tc_error_take(ctx->st))
         STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
     return STZ_OK;
@@ -1522,6 +1525,17 @@ stz_status stz_context_create(int device, stz_context** out)
         STZ_FAIL(STZ_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
     c->pool.reset(new ThreadPool(pool_threads(0)));
+    e = level_error_init();
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->st);
+        cudaStreamDestroy(c->st_copy);
+        cudaStreamDestroy(c->st_side);
+        cudaStreamDestroy(c->st_dec);
+        cudaEventDestroy(c->ev_fork);
+        cudaEventDestroy(c->ev_join);
+        delete c;
+        STZ_FAIL(STZ_ERR_CUDA, std::string("level error word: ") + cudaGetErrorString(e));
+    }
     *out = c;
     return STZ_OK;
 }

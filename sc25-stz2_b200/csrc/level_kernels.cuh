@@ -309,10 +309,11 @@ __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>&
 
 template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
-                                                         QuantParams qp, HistArgs hist, LearnedArgs<T> la)
+                                                         QuantParams qp, HistArgs hist, LearnedArgs<T> la,
+                                                         const __grid_constant__ CUtensorMap tmap, int use_tma)
 {
     static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ uint32_t sh[7][kSmemBins];
     __shared__ T lut[2 * kRecW];
@@ -328,7 +329,8 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     const int wn = min(kSmemBins, 2 * qp.radius - wlo);
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
     const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * ZB;
-    load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
+    __shared__ __align__(8) uint64_t tile_bar;
+    stage_tile<T, ZB>(tile, R, use_tma ? &tmap : nullptr, dx, dy, dz, x0, y0, z0, &tile_bar);
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool valid = x <= dx - 3 && y <= dy - 3;
@@ -498,10 +500,11 @@ template <typename T, int PRED, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict__ R, LevelGeom geo, QuantParams qp,
                                                          const uint16_t* __restrict__ codes,
                                                          const T* __restrict__ unpred_dense, T* __restrict__ G,
-                                                         LearnedArgs<T> la)
+                                                         LearnedArgs<T> la, const __grid_constant__ CUtensorMap tmap,
+                                                         int use_tma)
 {
     static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ T lut[2 * kRecW];
     const int tid = threadIdx.y * BX + threadIdx.x;
@@ -513,7 +516,8 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
     }
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
     const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * ZB;
-    load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
+    __shared__ __align__(8) uint64_t tile_bar;
+    stage_tile<T, ZB>(tile, R, use_tma ? &tmap : nullptr, dx, dy, dz, x0, y0, z0, &tile_bar);
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     const bool valid = x <= dx - 3 && y <= dy - 3;

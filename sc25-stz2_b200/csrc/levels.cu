@@ -23,8 +23,11 @@
 // merge, zslab preprocess/depreprocess, ROI depreprocess, quantize,
 // dequantize) for callers that drive the stages themselves.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "learned_tc.cuh"
@@ -35,6 +38,38 @@ namespace stz {
 
 // Set by a level kernel whose tensor-core network gave up waiting on an MMA.
 __device__ uint32_t g_learned_tc_error;
+
+// A pinned, mapped host word that a level kernel sets when a TMA tile load
+// did not complete within its bounded wait (null until level_error_init). The
+// host reads it after the synchronizations it makes anyway.
+__device__ volatile uint32_t* g_tile_error;
+namespace {
+volatile uint32_t* g_tile_error_host = nullptr;
+std::mutex g_tile_error_mu;
+}  // namespace
+
+cudaError_t level_error_init()
+{
+    std::lock_guard<std::mutex> lk(g_tile_error_mu);
+    if (!g_tile_error_host) {
+        void* p = nullptr;
+        const cudaError_t e = cudaHostAlloc(&p, 64, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) return e;
+        std::memset(p, 0, 64);
+        g_tile_error_host = static_cast<volatile uint32_t*>(p);
+    }
+    void* d = nullptr;
+    cudaError_t e = cudaHostGetDevicePointer(&d, (void*)g_tile_error_host, 0);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_tile_error, &d, sizeof(d));
+    return e;
+}
+
+bool level_error_take()
+{
+    if (!g_tile_error_host || !*g_tile_error_host) return false;
+    *g_tile_error_host = 0;
+    return true;
+}
 
 uint32_t learned_tc_error_take(cudaStream_t st)
 {
@@ -73,7 +108,9 @@ constexpr size_t kZBigPoints = size_t(1) << 23;
 // too small to fill the device with 8-plane bricks.
 constexpr int kZTiny = 2;
 constexpr size_t kZTinyPoints = size_t(1) << 18;
-constexpr int TSX = BX + 3, TSY = BY + 3;
+// Tile rows hold BX + 3 values, padded to BX + 4 so a row is a multiple of
+// 16 bytes: the inner extent of the TMA box that stages the tile.
+constexpr int TSX = BX + 4, TSY = BY + 3;
 constexpr int TPLANE = TSX * TSY;
 template <int ZB>
 __host__ __device__ constexpr int tile_elems()
@@ -106,6 +143,53 @@ __device__ __forceinline__ void load_tile(T* tile, const T* __restrict__ R, int 
             v = __ldg(R + ((size_t)gz * dy + gy) * dx + gx);
         tile[i] = v;
     }
+}
+
+// TMA staging of the halo tile (sm_100a): one thread issues a 3-D bulk tensor
+// load of the box [x0-1, x0+BX+3) x [y0-1, y0+BY+2) x [z0-1, z0+ZB+2) of the
+// coarse grid into the tile, the tensor map filling zeros outside the grid;
+// the CTA waits on an mbarrier. The box's x origin x0 - 1 = BX * blockIdx.x
+// is a multiple of 16 bytes for any element size, as the TMA requires. The
+// wait is bounded: past kTileSpin tries the kernel flags the error (host word
+// g_tile_error), waits once more within the same bound and goes on; the
+// host then fails the call.
+constexpr int kTileSpin = 1 << 22;
+
+template <typename T, int ZB>
+__device__ __forceinline__ void tma_load_tile(T* tile, const CUtensorMap* map, int x0, int y0, int z0,
+                                              uint64_t* bar)
+{
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const uint32_t b = tc::smem_addr(bar);
+    if (tid == 0) {
+        tc::mbar_init(b, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        constexpr uint32_t bytes = (uint32_t)(sizeof(T) * tile_elems<ZB>());
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+            "%4}], [%5];" ::"r"(tc::smem_addr(tile)),
+            "l"(reinterpret_cast<uint64_t>(map)), "r"(x0 - 1), "r"(y0 - 1), "r"(z0 - 1), "r"(b)
+            : "memory");
+    }
+    bool done = false;
+    for (int i = 0; i < kTileSpin && !done; ++i) done = tc::mbar_try(b, 0);
+    if (!done) {
+        if (tid == 0 && g_tile_error) *g_tile_error = 1u;
+        for (int i = 0; i < kTileSpin && !done; ++i) done = tc::mbar_try(b, 0);
+    }
+}
+
+// The halo tile through the TMA (tmap non-null) or by the CTA's threads.
+template <typename T, int ZB>
+__device__ __forceinline__ void stage_tile(T* tile, const T* __restrict__ R, const CUtensorMap* tmap, int dx, int dy,
+                                           int dz, int x0, int y0, int z0, uint64_t* bar)
+{
+    if (tmap) tma_load_tile<T, ZB>(tile, tmap, x0, y0, z0, bar);
+    else load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
 }
 
 constexpr int kSmemBins = 512;
@@ -546,6 +630,57 @@ void allow_smem(K kernel, size_t bytes)
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled_fn()
+{
+    static const EncodeTiledFn f = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return f;
+}
+
+// TMA staging is the default; STZ_TILE_LOAD=threads loads the tile with the
+// CTA's threads (same tile, for comparisons).
+bool tma_tiles_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("STZ_TILE_LOAD");
+        return !(e && std::strcmp(e, "threads") == 0);
+    }();
+    return on;
+}
+
+// Tensor map of a coarse grid for the halo tile of zb-deep bricks; false when
+// the TMA cannot serve it (grid or row not 16-byte aligned, no driver entry
+// point), and the threads load the tile instead.
+template <typename T>
+bool make_tile_map(const T* R, int dx, int dy, int dz, int zb, CUtensorMap* m)
+{
+    if (!tma_tiles_enabled() || !R) return false;
+    if ((uintptr_t)R % 16 || ((size_t)dx * sizeof(T)) % 16) return false;
+    const EncodeTiledFn f = encode_tiled_fn();
+    if (!f) return false;
+    const cuuint64_t gdim[3] = {(cuuint64_t)dx, (cuuint64_t)dy, (cuuint64_t)dz};
+    const cuuint64_t gstride[2] = {(cuuint64_t)dx * sizeof(T), (cuuint64_t)dx * dy * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)TSX, (cuuint32_t)TSY, (cuuint32_t)(zb + 3)};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    return f(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)R, gdim,
+             gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 template <typename T>
@@ -578,6 +713,9 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
         cudaEventRecord(a.side.fork, st);
         cudaStreamWaitEvent(ss, a.side.fork, 0);
     }
+    alignas(64) CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    const int use_tma = interior && make_tile_map(a.coarse, g.dx, g.dy, g.dz, zb, &tmap) ? 1 : 0;
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
         if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
@@ -588,7 +726,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
                         : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
                                                  : k_level_encode<T, P, F, kLearnDp4a>;                        \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned);                                       \
+            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned, tmap, use_tma);                        \
         }                                                                                                          \
         if (ns && !par) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);        \
     } while (0)
@@ -635,6 +773,9 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
         cudaEventRecord(a.side.fork, st);
         cudaStreamWaitEvent(ss, a.side.fork, 0);
     }
+    alignas(64) CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    const int use_tma = interior && make_tile_map(a.coarse, g.dx, g.dy, g.dz, zb, &tmap) ? 1 : 0;
 #define STZ_DEC(P)                                                                                                 \
     do {                                                                                                           \
         if (ns && par)                                                                                             \
@@ -646,7 +787,7 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
                         : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \
                                                  : k_level_decode<T, P, kLearnDp4a>;                           \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned);              \
+            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned, tmap, use_tma); \
         }                                                                                                          \
         if (ns && !par)                                                                                            \
             k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \

@@ -272,6 +272,9 @@ void completer_main(stz_server* S, int lane)
         const cudaError_t e = cudaEventSynchronize(L.ev_b[slot]);
         float ms = -1.f;
         if (e == cudaSuccess) cudaEventElapsedTime(&ms, L.ev_a[slot], L.ev_b[slot]);
+        // a bulk-lane level decode whose TMA tile load gave up (the word is
+        // process-wide; the batch that sees it fails)
+        const bool tile_err = e == cudaSuccess && lane == kLaneBulk && level_error_take();
         lk.lock();
         InFlight f = std::move(L.inflight.front());
         L.inflight.pop_front();
@@ -283,10 +286,11 @@ void completer_main(stz_server* S, int lane)
             auto it = S->tickets.find(id);
             if (it == S->tickets.end()) continue;
             Ticket& t = it->second;
-            if (e != cudaSuccess) {
+            if (e != cudaSuccess || tile_err) {
                 S->arena.release(t.off, t.bytes);
                 t.status = STZ_ERR_CUDA;
-                t.error = std::string("batch failed on the device: ") + cudaGetErrorString(e);
+                t.error = tile_err ? std::string("batch failed on the device: a TMA tile load did not complete in time")
+                                   : std::string("batch failed on the device: ") + cudaGetErrorString(e);
             }
             t.state = 2;
             t.t_done = now;

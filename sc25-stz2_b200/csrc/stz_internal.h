@@ -69,6 +69,12 @@ struct LearnedArgs {
 // time (a bounded wait gave up); read and cleared by learned_tc_error_take.
 uint32_t learned_tc_error_take(cudaStream_t st);
 
+// The level kernels' TMA tile-load error word: level_error_init maps it for
+// the current device (once per context); level_error_take returns whether a
+// tile load gave up waiting since the last call, and clears it.
+cudaError_t level_error_init();
+bool level_error_take();
+
 // Quantizer constants of one level (FD5:1208-1210): eb, 1/eb computed once on
 // the host (recip = 1.0 / eb), radius.
 struct QuantParams {
