@@ -62,6 +62,7 @@ def parse_args():
     p.add_argument("--serve-size", type=int, default=1024, help="edge of the resident serving field")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="length of each serving load run")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-predictor measurement")
+    p.add_argument("--no-configs", action="store_true", help="skip the other BASELINE configurations")
     p.add_argument("--learned-only", action="store_true", help="only the learned-predictor measurement")
     p.add_argument("--learn-train-seeds", type=int, default=6, help="training fields (cycling the 3 generators)")
     p.add_argument("--learn-size", type=int, default=256, help="edge of the training fields")
@@ -469,6 +470,105 @@ def serving_bench(args, ctx, local):
     return res
 
 
+def configs_bench(args, ctx, local, field):
+    """The other BASELINE configurations, measured (device-resident fields and
+    outputs, CUDA events on the library's stream):
+    * 512^3 f32 lognormal at rel eb 1e-2 and 1e-4: compress and full
+      decompress GB/s, CR;
+    * progressive decompress of the rel 1e-3 stream at 1/8, 1/4 and 1/2
+      resolution (levels 3, 2, 1): ms and output GB/s;
+    * 384x384x256 f64 GRF k^-5/3 + 20 tanh fronts at rel eb 1e-6 and 1e-3:
+      100 boxes (edges U[16,128], random offsets) and 20 axis-aligned slices
+      through the single-request box API, p50/p99 ms per request, against
+      decoding the whole stream and cropping (what a decoder without marker
+      chunks must do, the no-marker ROI baseline of src/stz-rd.cpp)."""
+    import torch
+
+    import stz_b200
+    from stz_b200 import fields
+
+    dev = f"cuda:{local}"
+    stream = torch.cuda.ExternalStream(ctx.cuda_stream(), device=dev)
+    nbytes = field.numel() * field.element_size()
+    out = torch.empty_like(field)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, r
+
+    res = {"eb_sweep": [], "progressive": [], "fronts_384_f64": []}
+    for rel in (1e-2, 1e-3, 1e-4):
+        o = stz_b200.default_opts(eb=rel, eb_mode="rel", zstd_level=args.zstd)
+        cms, s = timed(lambda: ctx.compress(field, opts=o), 3)
+        dms, _ = timed(lambda: ctx.decompress(s, out=out), 3)
+        res["eb_sweep"].append({"rel_eb": rel, "compress_gbs": nbytes / cms / 1e6, "decompress_gbs": nbytes / dms / 1e6,
+                                "cr": nbytes / len(s)})
+        if rel == 1e-3:
+            for lvl in (3, 2, 1):
+                st = 1 << lvl
+                o_l = torch.empty((field.shape[0] // st, field.shape[1] // st, field.shape[2] // st),
+                                  dtype=field.dtype, device=dev)
+                lms, _ = timed(lambda: ctx.decompress(s, level=lvl, out=o_l), 5)
+                res["progressive"].append({"level": lvl, "resolution": f"1/{st}", "ms": lms,
+                                           "output_gbs": o_l.numel() * 4 / lms / 1e6,
+                                           "field_equiv_gbs": nbytes / lms / 1e6})
+    del out
+    torch.cuda.empty_cache()
+    nz, ny, nx = 256, 384, 384
+    f = fields.fronts((nz, ny, nx), 31, np.float64, device=dev)
+    dims = (nx, ny, nz)
+    for rel in (1e-6, 1e-3):
+        s = ctx.compress(f, eb=rel, eb_mode="rel")
+        ctx.upload(s)
+        rng = np.random.default_rng(int(1 / rel) % 1000)
+        reqs = []
+        for _ in range(100):
+            e = rng.integers(16, 129, 3)
+            lo = [int(rng.integers(0, d - x + 1)) for d, x in zip(dims, e)]
+            reqs.append(("box", lo, [a + int(x) - 1 for a, x in zip(lo, e)]))
+        for _ in range(20):
+            ax = int(rng.integers(0, 3))
+            lo, hi = [0, 0, 0], [d - 1 for d in dims]
+            lo[ax] = hi[ax] = int(rng.integers(0, dims[ax]))
+            reqs.append(("slice", lo, hi))
+        lat = {"box": [], "slice": []}
+        for kind, lo, hi in reqs[:5]:  # warm-up
+            ctx.decompress_box(s, lo, hi, out=torch.empty((hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1),
+                                                          dtype=f.dtype, device=dev))
+        for kind, lo, hi in reqs:
+            o_b = torch.empty((hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1), dtype=f.dtype, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.decompress_box(s, lo, hi, out=o_b)
+            torch.cuda.synchronize()
+            lat[kind].append(1e3 * (time.perf_counter() - t0))
+        full = torch.empty_like(f)
+        whole = []
+        for kind, lo, hi in reqs[:20]:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.decompress(s, out=full)
+            crop = full[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1].contiguous()
+            torch.cuda.synchronize()
+            whole.append(1e3 * (time.perf_counter() - t0))
+        del full, crop
+        res["fronts_384_f64"].append({
+            "rel_eb": rel, "cr": f.numel() * 8 / len(s),
+            "box_p50_ms": _pct(lat["box"], 50), "box_p99_ms": _pct(lat["box"], 99),
+            "slice_p50_ms": _pct(lat["slice"], 50), "slice_p99_ms": _pct(lat["slice"], 99),
+            "whole_stream_then_crop_p50_ms": _pct(whole, 50)})
+    del f
+    torch.cuda.empty_cache()
+    return res
+
+
 def learned_bench(args, ctx, local, field):
     """Learned correction: train on seeded 256^3 f32 fields cycling the three
     generators (GRF k^-11/3, lognormal, GRF k^-5/3 + fronts) at rel eb 1e-3
@@ -786,6 +886,10 @@ def main():
                           "Huffman, zstd 3, container, the GPU's stream byte for byte",
                 "compress_s": rp["compress_s"], "decompress_s": rp["decompress_s"]}
 
+    cfgs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        cfgs = configs_bench(args, ctx, local, field)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = serving_bench(args, ctx, local)
@@ -819,7 +923,7 @@ def main():
             "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
             "parity": parity, "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-            "serving": serving, "learned": learned,
+            "configs": cfgs, "serving": serving, "learned": learned,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         }
         print(json.dumps(res))

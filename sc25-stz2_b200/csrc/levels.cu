@@ -183,12 +183,14 @@ __device__ __forceinline__ void tma_load_tile(T* tile, const CUtensorMap* map, i
     }
 }
 
-// The halo tile through the TMA (tmap non-null) or by the CTA's threads.
+// The halo tile through the TMA (tmap non-null, and the tile's shared-memory
+// address 128-byte aligned as a bulk tensor destination wants) or by the
+// CTA's threads.
 template <typename T, int ZB>
 __device__ __forceinline__ void stage_tile(T* tile, const T* __restrict__ R, const CUtensorMap* tmap, int dx, int dy,
                                            int dz, int x0, int y0, int z0, uint64_t* bar)
 {
-    if (tmap) tma_load_tile<T, ZB>(tile, tmap, x0, y0, z0, bar);
+    if (tmap && (tc::smem_addr(tile) & 127u) == 0) tma_load_tile<T, ZB>(tile, tmap, x0, y0, z0, bar);
     else load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
 }
 
