@@ -857,6 +857,22 @@ const char* check_stream(const FileHeader& h, const LevelDir& L, const StreamDir
 }
 }  // namespace
 
+std::vector<DecodeBatch> decode_batches(const ParsedStream& ps, int kmax)
+{
+    std::vector<DecodeBatch> v;
+    if (kmax < 1) return v;
+    const int f0 = 7 * (kmax - 1);
+    if (kmax > 1) v.push_back({0, f0, 0, -1});
+    const int L = (int)ps.lv[kmax].s[0].layers;
+    if (L >= 2) {
+        v.push_back({f0, f0 + 7, 0, L / 2});
+        v.push_back({f0, f0 + 7, L / 2, L});
+    } else {
+        v.push_back({f0, f0 + 7, 0, -1});
+    }
+    return v;
+}
+
 stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p, const BatchFn* on_batch)
 {
     Lap lap("prepare");
@@ -982,23 +998,28 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
     const size_t n0 = (size_t)h.c0[0] * h.c0[1] * h.c0[2];
     STZ_CUDA(p.coarsest->ensure(n0 * elem));
     STZ_CUDA(cudaMemcpyAsync(p.coarsest->p, bytes + ps.coarsest_off, n0 * elem, cudaMemcpyHostToDevice, ctx->st));
-    // batch ends: with on_batch, every level below kmax, then the finest
-    // level's streams in two halves; else batches of at least two frames per
-    // pool thread
-    std::vector<int> ends;
+    // batches: with on_batch, decode_batches; else whole streams, at least
+    // two frames per pool thread
+    std::vector<DecodeBatch> batches;
     if (on_batch) {
-        if (kmax > 1) ends.push_back(7 * (kmax - 1));
-        ends.push_back(7 * (kmax - 1) + 4);
-        ends.push_back(nstreams);
+        batches = decode_batches(ps, kmax);
     } else {
         const size_t min_batch = 2 * (size_t)ctx->pool->size();
         for (int s0 = 0; s0 < nstreams;) {
             int s1 = s0 + 1;
             while (s1 < nstreams && stream_first_job[s1] - stream_first_job[s0] < min_batch) ++s1;
-            ends.push_back(s1);
+            batches.push_back({s0, s1, 0, -1});
             s0 = s1;
         }
     }
+    // bytes of each stream's payload before chunk layer l
+    auto layer_bytes = [&](int si, int l) -> size_t {
+        const StreamDir& d = ps.lv[si / 7 + 1].s[si % 7];
+        size_t b = 0;
+        for (int i = 0; i < l; ++i) b += d.lr[i];
+        return b;
+    };
+    auto stream_end = [&](int si) -> size_t { return si + 1 < nstreams ? o_pl + 4 * p.sd[si + 1].word_base : total; };
     // Payload copies go on the context's copy stream, so a batch's copy
     // overlaps the decoding of the batch before it; ctx->st waits on each
     // batch's event before decoding it (or, without on_batch, on the last).
@@ -1014,36 +1035,52 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
         cudaStreamSynchronize(ctx->st_dec);
         cudaStreamSynchronize(ctx->st);
     };
-    int s0 = 0;
-    for (const int s1 : ends) {
-        const size_t j0 = stream_first_job[s0], j1 = stream_first_job[s1];
-        ctx->pool->parallel_for(j1 - j0, [&](size_t j) {
-            if (!decode_frame(jobs[j0 + j].src, jobs[j0 + j].stored, jobs[j0 + j].raw, jobs[j0 + j].dst)) bad = 3;
+    std::vector<size_t> bjobs;
+    for (const DecodeBatch& B : batches) {
+        // the batch's frames: whole streams, or layers [l0, l1) of each
+        bjobs.clear();
+        for (int si = B.s0; si < B.s1; ++si) {
+            const size_t a = stream_first_job[si] + (B.l1 < 0 ? 0 : (size_t)B.l0);
+            const size_t b = B.l1 < 0 ? stream_first_job[si + 1] : stream_first_job[si] + (size_t)B.l1;
+            for (size_t j = a; j < b; ++j) bjobs.push_back(j);
+        }
+        ctx->pool->parallel_for(bjobs.size(), [&](size_t i) {
+            const Job& J = jobs[bjobs[i]];
+            if (!decode_frame(J.src, J.stored, J.raw, J.dst)) bad = 3;
         });
         if (bad) {
             sync_both();
             STZ_FAIL(STZ_ERR_ZSTD, "payload frame does not decode");
         }
-        const size_t b0 = o_pl + 4 * p.sd[s0].word_base;
-        const size_t b1 = s1 < nstreams ? o_pl + 4 * p.sd[s1].word_base : total;
         cudaEvent_t e = nullptr;
         cudaError_t ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
         if (ce == cudaSuccess) ev.e.push_back(e);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st_copy);
+        auto copy = [&](size_t b0, size_t b1) {
+            if (ce == cudaSuccess && b1 > b0)
+                ce = cudaMemcpyAsync(ds + b0, hs + b0, b1 - b0, cudaMemcpyHostToDevice, ctx->st_copy);
+        };
+        if (B.l1 < 0) {
+            copy(o_pl + 4 * p.sd[B.s0].word_base, stream_end(B.s1 - 1));
+        } else {
+            const int L = (int)ps.lv[B.s0 / 7 + 1].s[B.s0 % 7].layers;
+            for (int si = B.s0; si < B.s1; ++si) {
+                const size_t base = o_pl + 4 * p.sd[si].word_base;
+                copy(base + layer_bytes(si, B.l0), B.l1 >= L ? stream_end(si) : base + layer_bytes(si, B.l1));
+            }
+        }
         if (ce == cudaSuccess) ce = cudaEventRecord(e, ctx->st_copy);
-        if (ce == cudaSuccess && !on_batch && s1 == nstreams) ce = cudaStreamWaitEvent(ctx->st, e, 0);
+        if (ce == cudaSuccess && !on_batch && B.s1 == nstreams) ce = cudaStreamWaitEvent(ctx->st, e, 0);
         if (ce != cudaSuccess) {
             sync_both();
             STZ_CUDA(ce);
         }
         if (on_batch) {
-            const stz_status st = (*on_batch)(s0, s1, e);
+            const stz_status st = (*on_batch)(B, e);
             if (st != STZ_OK) {
                 sync_both();
                 return st;
             }
         }
-        s0 = s1;
     }
     lap.mark("payload frames + h2d");
     STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));  // the pinned staging buffer is reused by the next call
@@ -1125,15 +1162,18 @@ struct DecodePipe {
     const Prepared& p;
     int kdec;
     T* out;
+    std::vector<DecodeBatch> batches;
     bool planned = false;
-    std::vector<size_t> wfirst, ufirst;  // per stream: first work / unpredictable item (+ end)
+    size_t next_batch = 0;
+    std::vector<size_t> wfirst, ufirst;  // per batch: first work / unpredictable item (+ end)
     size_t o_w = 0, o_i = 0, o_u = 0;
     int next_level = 1, cur = 0;
+    int fin_bricks = 0, fin_done = 0;  // the finest level's z-bricks, and those launched
     const T* coarse = nullptr;
     std::vector<cudaEvent_t> events;  // ordering between ctx->st and ctx->st_dec
 
-    DecodePipe(stz_context* c, const stz_stream* st, const Prepared& pp, int k, T* o)
-        : ctx(c), s(st), p(pp), kdec(k), out(o)
+    DecodePipe(stz_context* c, const stz_stream* st, const Prepared& pp, int k, T* o, std::vector<DecodeBatch> b)
+        : ctx(c), s(st), p(pp), kdec(k), out(o), batches(std::move(b))
     {
     }
     ~DecodePipe()
@@ -1150,28 +1190,33 @@ struct DecodePipe {
         return r == cudaSuccess ? cudaStreamWaitEvent(waiter, e, 0) : r;
     }
 
-    // Work lists of every stream, uploaded once; buffers sized.
+    // Work lists of every batch, uploaded once; buffers sized.
     stz_status plan()
     {
         const ParsedStream& ps = s->dir;
-        const int nstreams = 7 * kdec;
         std::vector<CtaWork> work;
         std::vector<uint32_t> ids;
         std::vector<UnpredWork> uw;
-        wfirst.assign(nstreams + 1, 0);
-        ufirst.assign(nstreams + 1, 0);
-        std::vector<uint32_t> all;
-        for (int i = 0; i < nstreams; ++i) {
-            const StreamDesc& d = p.sd[i];
-            wfirst[i] = work.size();
-            ufirst[i] = uw.size();
-            all.resize(d.nchunks);
-            for (uint32_t c = 0; c < d.nchunks; ++c) all[c] = c;
-            add_work(work, ids, (uint32_t)i, all.data(), all.size(), (int)d.C);
-            add_unpred_work(p, (uint32_t)i, all.data(), all.size(), uw);
+        wfirst.assign(batches.size() + 1, 0);
+        ufirst.assign(batches.size() + 1, 0);
+        std::vector<uint32_t> cs;
+        for (size_t bi = 0; bi < batches.size(); ++bi) {
+            const DecodeBatch& B = batches[bi];
+            wfirst[bi] = work.size();
+            ufirst[bi] = uw.size();
+            for (int i = B.s0; i < B.s1; ++i) {
+                const StreamDesc& d = p.sd[i];
+                const uint32_t per_layer = d.ncx * d.ncy;
+                const uint32_t c0 = B.l1 < 0 ? 0 : (uint32_t)B.l0 * per_layer;
+                const uint32_t c1 = B.l1 < 0 ? d.nchunks : std::min(d.nchunks, (uint32_t)B.l1 * per_layer);
+                cs.resize(c1 > c0 ? c1 - c0 : 0);
+                for (uint32_t c = c0; c < c1; ++c) cs[c - c0] = c;
+                add_work(work, ids, (uint32_t)i, cs.data(), cs.size(), (int)d.C);
+                add_unpred_work(p, (uint32_t)i, cs.data(), cs.size(), uw);
+            }
         }
-        wfirst[nstreams] = work.size();
-        ufirst[nstreams] = uw.size();
+        wfirst[batches.size()] = work.size();
+        ufirst[batches.size()] = uw.size();
         o_w = 0, o_i = align256(work.size() * sizeof(CtaWork));
         o_u = align256(o_i + ids.size() * 4);
         const size_t total = align256(o_u + uw.size() * sizeof(UnpredWork));
@@ -1190,6 +1235,11 @@ struct DecodePipe {
         STZ_CUDA(ctx->grid[0].ensure(gmax * sizeof(T)));
         STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
         coarse = p.coarsest->as<T>();
+        // the finest level decodes by z-bricks as its chunk layers arrive
+        // (plain kernels only; else the whole level after the last batch)
+        fin_bricks = level_decode_bricks(level_geom(ps, kdec), learned_args<T>(ps, kdec, p.d_models).model != nullptr &&
+                                                                   learned_args<T>(ps, kdec, p.d_models).flags,
+                                         0, nullptr);
         // the entropy decodes (ctx->st_dec) follow everything enqueued on
         // ctx->st so far: tables, coarsest grid, work lists, earlier calls
         STZ_CUDA(record(ctx->st, ctx->st_dec));
@@ -1197,18 +1247,33 @@ struct DecodePipe {
         return STZ_OK;
     }
 
-    // Streams [s0, s1): their payload is on the device once `copied` has
-    // completed (null: already). Entropy decode on ctx->st_dec, so it runs
-    // beside the level decodes of earlier batches on ctx->st.
-    stz_status batch(int s0, int s1, cudaEvent_t copied)
+    LevelDecodeArgs<T> level_args(int k)
     {
-        s1 = std::min(s1, 7 * kdec);
-        if (s0 >= s1) return STZ_OK;
+        const ParsedStream& ps = s->dir;
+        LevelDecodeArgs<T> a;
+        a.coarse = coarse;
+        a.geo = level_geom(ps, k);
+        a.predictor = ps.h.predictor;
+        a.qp = qparams(ps, k);
+        a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
+        a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
+        a.out = k == kdec ? out : ctx->grid[cur].as<T>();
+        a.learned = learned_args<T>(ps, k, p.d_models);
+        a.side = ctx->side();
+        return a;
+    }
+
+    // The next batch's entropy decode on ctx->st_dec (after `copied`, null:
+    // already on the device), then on ctx->st every level it completes, and
+    // for a layer batch of the finest level the z-bricks its layers cover.
+    stz_status batch(const DecodeBatch& B, cudaEvent_t copied)
+    {
         if (!planned) STZ_TRY(plan());
+        const size_t bi = next_batch++;
         cudaStream_t sd = ctx->st_dec;
         if (copied) STZ_CUDA(cudaStreamWaitEvent(sd, copied, 0));
         const uint8_t* dw = ctx->work.as<uint8_t>();
-        const size_t w0 = wfirst[s0], w1 = wfirst[s1], u0 = ufirst[s0], u1 = ufirst[s1];
+        const size_t w0 = wfirst[bi], w1 = wfirst[bi + 1], u0 = ufirst[bi], u1 = ufirst[bi + 1];
         if (w1 > w0) {
             KScope ks(ctx, "k_decode", 1, sd);
             launch_decode((const CtaWork*)(dw + o_w) + w0, (const uint32_t*)(dw + o_i), (int)(w1 - w0), p.d_sd,
@@ -1220,25 +1285,43 @@ struct DecodePipe {
                                   ctx->codes.as<uint16_t>(), ctx->unpred_dense.as<T>(), (T*)p.d_ulist, sd);
         }
         const ParsedStream& ps = s->dir;
-        if (next_level <= kdec && 7 * next_level <= s1) STZ_CUDA(record(sd, ctx->st));
-        for (; next_level <= kdec && 7 * next_level <= s1; ++next_level) {
-            const int k = next_level;
-            LevelDecodeArgs<T> a;
-            a.coarse = coarse;
-            a.geo = level_geom(ps, k);
-            a.predictor = ps.h.predictor;
-            a.qp = qparams(ps, k);
-            a.codes = ctx->codes.as<uint16_t>() + p.sd[(size_t)(k - 1) * 7].code_off;
-            a.unpred_dense = p.total_unpred ? ctx->unpred_dense.as<T>() + p.sd[(size_t)(k - 1) * 7].code_off : nullptr;
-            a.out = k == kdec ? out : ctx->grid[cur].as<T>();
-            a.learned = learned_args<T>(ps, k, p.d_models);
+        const bool last = bi + 1 == batches.size();
+        const bool whole = B.l1 < 0 || B.l1 >= (int)ps.lv[kdec].s[0].layers;
+        const int s1 = whole ? B.s1 : B.s0;  // streams complete after this batch
+        int bricks_to = fin_done;
+        if (next_level == kdec && B.s0 == 7 * (kdec - 1) && fin_bricks && !last) {
+            const LevelGeom g = level_geom(ps, kdec);
+            level_decode_bricks(g, false, B.l1 * g.C, &bricks_to);
+        }
+        const bool finest_part = bricks_to > fin_done;
+        if ((next_level <= kdec && 7 * next_level <= s1) || finest_part) STZ_CUDA(record(sd, ctx->st));
+        for (; next_level < kdec && 7 * next_level <= s1; ++next_level) {
+            const LevelDecodeArgs<T> a = level_args(next_level);
             {
-                KScope ks(ctx, k == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
-                a.side = ctx->side();
+                KScope ks(ctx, next_level == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]");
                 launch_level_decode<T>(a, ctx->st);
             }
             coarse = a.out;
             cur = 1 - cur;
+        }
+        if (next_level == kdec) {
+            LevelDecodeArgs<T> a = level_args(kdec);
+            const char* nm = kdec == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]";
+            if (finest_part) {  // the bricks of the layers on the device so far
+                a.zb_lo = fin_done, a.zb_hi = bricks_to;
+                KScope ks(ctx, nm);
+                launch_level_decode<T>(a, ctx->st);
+                fin_done = bricks_to;
+            }
+            if (7 * kdec <= s1) {  // every layer decoded: the rest of the level
+                if (fin_bricks) a.zb_lo = fin_done, a.zb_hi = fin_bricks;
+                {
+                    KScope ks(ctx, nm);
+                    launch_level_decode<T>(a, ctx->st);
+                }
+                fin_done = fin_bricks;
+                ++next_level;
+            }
         }
         STZ_CUDA(cudaGetLastError());
         return STZ_OK;
@@ -1256,10 +1339,10 @@ stz_status decode_levels(stz_context* ctx, const stz_stream* s, const Prepared& 
         STZ_CUDA(cudaMemcpyAsync(out_dev, p.coarsest->p, n0 * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
         return STZ_OK;
     }
-    DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
+    DecodePipe<T> pipe(ctx, s, p, kdec, out_dev, {DecodeBatch{0, 7 * kdec, 0, -1}});
     STZ_TRY(pipe.plan());
     STZ_CUDA(cudaStreamSynchronize(ctx->st));  // the pinned work-list buffer is free for the caller
-    return pipe.batch(0, 7 * kdec, nullptr);
+    return pipe.batch(pipe.batches[0], nullptr);
 }
 
 template <typename T>
@@ -1283,8 +1366,8 @@ stz_status decompress_level_dev(stz_context* ctx, const stz_stream* s, int level
     } else {
         // each batch of streams is decoded while the host zstd-decodes the next
         Trace t("decompress: prepare + decode");
-        DecodePipe<T> pipe(ctx, s, p, kdec, out_dev);
-        const BatchFn fn = [&](int s0, int s1, cudaEvent_t copied) { return pipe.batch(s0, s1, copied); };
+        DecodePipe<T> pipe(ctx, s, p, kdec, out_dev, decode_batches(s->dir, kdec));
+        const BatchFn fn = [&](const DecodeBatch& B, cudaEvent_t copied) { return pipe.batch(B, copied); };
         STZ_TRY(prepare(ctx, s, kdec, p, &fn));
     }
     STZ_CUDA(cudaStreamSynchronize(ctx->st));

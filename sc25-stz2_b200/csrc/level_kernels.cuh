@@ -84,12 +84,15 @@ struct OwnedAxis {
 // The owned boundary points of this CTA as three disjoint boxes: z outside
 // the interior range (all owned x, y); z inside, y outside (all owned x); z
 // and y inside, x outside. f(x, y, z) for each, spread over the CTA's threads.
+// bz / nbz: the CTA's brick index along z and the level's brick count (a
+// launch may cover a range of z-bricks).
 template <class F>
-__device__ __forceinline__ void for_owned_boundary(const LevelGeom& g, int ZB, int tid, int nthreads, F&& f)
+__device__ __forceinline__ void for_owned_boundary(const LevelGeom& g, int ZB, int bz, int nbz, int tid, int nthreads,
+                                                   F&& f)
 {
     const OwnedAxis X = OwnedAxis::make(g.dx, blockIdx.x, gridDim.x, BX);
     const OwnedAxis Y = OwnedAxis::make(g.dy, blockIdx.y, gridDim.y, BY);
-    const OwnedAxis Z = OwnedAxis::make(g.dz, blockIdx.z, gridDim.z, ZB);
+    const OwnedAxis Z = OwnedAxis::make(g.dz, bz, nbz, ZB);
     const int ga = X.n() * Y.n() * Z.nb();
     const int gb = X.n() * Y.nb() * Z.ni();
     const int gc = X.nb() * Y.ni() * Z.ni();
@@ -501,7 +504,7 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
                                                          const uint16_t* __restrict__ codes,
                                                          const T* __restrict__ unpred_dense, T* __restrict__ G,
                                                          LearnedArgs<T> la, const __grid_constant__ CUtensorMap tmap,
-                                                         int use_tma)
+                                                         int use_tma, int zoff, int nzb)
 {
     static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -515,7 +518,8 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
         la.model = smodel;
     }
     const int dx = geo.dx, dy = geo.dy, dz = geo.dz;
-    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + blockIdx.z * ZB;
+    const int bz = blockIdx.z + zoff;  // this launch covers z-bricks [zoff, zoff + gridDim.z) of nzb
+    const int x0 = 1 + blockIdx.x * BX, y0 = 1 + blockIdx.y * BY, z0 = 1 + bz * ZB;
     __shared__ __align__(8) uint64_t tile_bar;
     stage_tile<T, ZB>(tile, R, use_tma ? &tmap : nullptr, dx, dy, dz, x0, y0, z0, &tile_bar);
     __syncthreads();
@@ -536,11 +540,11 @@ __global__ void __launch_bounds__(BX* BY, 4) k_level_decode(const T* __restrict_
             }
         }
         // the CTA's owned boundary points, predicted from the same tile
-        for_owned_boundary(geo, ZB, tid, BX * BY, [&](int bx, int by, int bz) {
-            const TileAt<T, TSX, TPLANE> r{tile + (bz - z0 + 1) * TPLANE + (by - y0 + 1) * TSX + (bx - x0 + 1)};
+        for_owned_boundary(geo, ZB, bz, nzb, tid, BX * BY, [&](int px, int py, int pz) {
+            const TileAt<T, TSX, TPLANE> r{tile + (pz - z0 + 1) * TPLANE + (py - y0 + 1) * TSX + (px - x0 + 1)};
             ChunkIndex bci;
-            bci.init(geo, bx, by);
-            decode_point<T, PRED, false>(r, geo, qp, lut, codes, unpred_dense, G, bci, bx, by, bz);
+            bci.init(geo, px, py);
+            decode_point<T, PRED, false>(r, geo, qp, lut, codes, unpred_dense, G, bci, px, py, pz);
         });
         return;
     }

@@ -760,6 +760,14 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
     const int zb = big ? kZBig : tiny ? kZTiny : kZSmall;
     dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + zb - 1) / zb);
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
+    const int nzb = (int)grd.z;
+    int zoff = 0;
+    if (!learned && interior && a.zb_hi >= 0) {  // a range of z-bricks
+        zoff = std::min(std::max(a.zb_lo, 0), nzb);
+        const int zhi = std::min(std::max(a.zb_hi, zoff), nzb);
+        if (zhi == zoff) return;
+        grd.z = (unsigned)(zhi - zoff);
+    }
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
                       : tiny  ? tile_bytes<T, kZTiny>()
@@ -789,7 +797,8 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
                         : a.learned.tensor_cores ? k_level_decode<T, P, kLearnTc>                              \
                                                  : k_level_decode<T, P, kLearnDp4a>;                           \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned, tmap, use_tma); \
+            kern<<<grd, blk, sm, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, a.learned, tmap, use_tma,   \
+                                       zoff, nzb);                                                                 \
         }                                                                                                          \
         if (ns && !par)                                                                                            \
             k_level_decode_shell<T, P><<<gs, 256, 0, st>>>(a.coarse, g, a.qp, a.codes, a.unpred_dense, a.out, shell); \
@@ -801,6 +810,21 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
         cudaEventRecord(a.side.join, ss);
         cudaStreamWaitEvent(st, a.side.join, 0);
     }
+}
+
+int level_decode_bricks(const LevelGeom& g, bool learned, int zlim, int* below)
+{
+    const Shell shell = Shell::make(g.dx, g.dy, g.dz);
+    const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
+    if (learned || !interior) {
+        if (below) *below = 0;
+        return 0;
+    }
+    const size_t npts = (size_t)g.dx * g.dy * g.dz;
+    const int zb = npts >= kZBigPoints ? kZBig : npts <= kZTinyPoints ? kZTiny : kZSmall;
+    const int n = (shell.niz + zb - 1) / zb;
+    if (below) *below = std::max(0, std::min(n - 1, (zlim - 1) / zb));
+    return n;
 }
 
 template <typename T>

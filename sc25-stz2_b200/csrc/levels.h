@@ -40,7 +40,18 @@ struct LevelDecodeArgs {
     T* out;  // fine grid (2dx x 2dy x 2dz)
     LearnedArgs<T> learned; // learned correction (model null: none)
     SideStream side;        // boundary-shell kernel placement
+    // z-bricks [zb_lo, zb_hi) only (zb_hi < 0: the whole level); see
+    // level_decode_bricks
+    int zb_lo = 0, zb_hi = -1;
 };
+
+// The plain decode kernel's z-bricks of a level (0 when a level decode
+// cannot be split: learned correction, or no interior). Brick b < n - 1
+// reconstructs fine planes from coarse z in [1 + b*ZB, 1 + (b+1)*ZB), the
+// first also z = 0 and the last up to dz - 1; *below = the bricks whose
+// coarse z stay below zlim (they need only codes of chunk layers under
+// zlim / C).
+int level_decode_bricks(const LevelGeom& g, bool learned, int zlim, int* below);
 
 template <typename T>
 void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st);

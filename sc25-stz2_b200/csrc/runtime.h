@@ -320,14 +320,23 @@ stz_status check_opts(const stz_opts* o);
 size_t dtype_size(int dtype);
 // Make ctx current on this thread and clear the thread's last error.
 stz_status enter(stz_context* ctx);
+// A batch of the pipelined decode: streams [s0, s1), their chunk z-layers
+// [l0, l1) (l1 < 0: every layer).
+struct DecodeBatch {
+    int s0, s1, l0, l1;
+};
+// The batches of a decode of levels 1..kmax: every stream of the levels
+// below kmax, then the finest level's 7 streams in two halves of their chunk
+// z-layers (one batch when they have a single layer).
+std::vector<DecodeBatch> decode_batches(const ParsedStream& ps, int kmax);
 // Parse stream headers, lay out and upload the tables and payload of levels
 // 1..kmax (zstd frames decoded on the host pool) and the coarsest grid.
-// on_batch(s0, s1, copied), when given, runs after the copy of the payload of
-// streams [s0, s1) is enqueued (batches in stream order, ending at the level
-// boundaries below kmax); `copied` is the event after that copy, and the
-// callback orders its own work after it. Without on_batch, ctx->st waits for
-// every copy. prepare returns once the context's streams are idle.
-using BatchFn = std::function<stz_status(int, int, cudaEvent_t)>;
+// on_batch(b, copied), when given, runs for each batch of
+// decode_batches(kmax) in order, after the copy of its payload is enqueued;
+// `copied` is the event after that copy, and the callback orders its own
+// work after it. Without on_batch, ctx->st waits for every copy. prepare
+// returns once the context's streams are idle.
+using BatchFn = std::function<stz_status(const DecodeBatch&, cudaEvent_t)>;
 stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p, const BatchFn* on_batch = nullptr);
 // Entropy-decode the listed chunks into ctx->codes (and scatter their
 // unpredictable values into ctx->unpred_dense).
