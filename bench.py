@@ -836,24 +836,30 @@ def main():
     if os.path.exists(PEAKS_FILE):
         peaks = json.load(open(PEAKS_FILE))
     peak = peaks.get("hbm_gbs", FALLBACK_HBM)
-    dom = max(prof.items(), key=lambda kv: kv[1][0])
-    dname, (dms, dl) = dom
-    alg = algorithmic_bytes(dname, field.numel(), 4, info.n_levels, info.raw_payload_bytes)
-    roof = None
-    if alg is not None and dl:
+    traffic_tab = json.load(open(TRAFFIC_FILE)) if os.path.exists(TRAFFIC_FILE) else {}
+
+    def roofline_of(name):
+        dms, dl = prof[name]
+        alg = algorithmic_bytes(name, field.numel(), 4, info.n_levels, info.raw_payload_bytes)
+        if alg is None or not dl:
+            return None
         # alg covers one step; a kernel launched several times per step (the
-        # coder's stream batches) moves alg / (launches per step) per launch
+        # coder's stream batches, the finest decode's z-halves) moves
+        # alg / (launches per step) per launch
         alg = alg * args.steps / dl
         per_launch_s = dms / dl / 1e3
         achieved = alg / per_launch_s / 1e9
-        traffic = None
-        if os.path.exists(TRAFFIC_FILE):
-            tr = json.load(open(TRAFFIC_FILE)).get(dname)
-            if tr:
-                traffic = tr.get("dram_bytes_per_launch")
-        roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
-                "ms_per_launch": dms / dl, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+        tr = traffic_tab.get(name) or {}
+        return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": tr.get("dram_bytes_per_launch"), "algorithmic_bytes": alg,
+                "ms_per_launch": dms / dl, "launches_per_step": dl / args.steps,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # the dominant kernel (most time per step) and every kernel with a
+    # roofline, so a change of the top kernel does not hide the others
+    dname = max(prof.items(), key=lambda kv: kv[1][0])[0]
+    roof = roofline_of(dname)
+    rooflines = {k: r for k in prof for r in [roofline_of(k)] if r}
 
     parity = None
     if rank == 0 and not args.no_parity:
@@ -922,7 +928,10 @@ def main():
             "compress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, comp_ms),
             "decompress_gbs": replicas.aggregate_gbs(nbytes * args.steps, world, dec_ms),
             "parity": parity, "cr": cr, "max_err_over_bound": max_err / E, "stream_bytes": len(s),
-            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+            "rooflines": {k: {kk: r[kk] for kk in ("frac", "achieved", "ms_per_launch", "launches_per_step", "traffic")}
+                          for k, r in rooflines.items()},
+            "cpu_baseline": cpu, "clocks": clk,
             "configs": cfgs, "serving": serving, "learned": learned,
             "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
         }

@@ -426,6 +426,11 @@ stz_status stz_server_batch_log(stz_server* srv, stz_batch_record* out, size_t c
  * coder's symbol order). level_from_coarse is 1..n_levels. */
 stz_status stz_debug_stream_codes(stz_context* ctx, const stz_stream* s, int level_from_coarse, int block,
                                   uint16_t* codes, size_t cap, size_t* n_out);
+/* The f32 quantizer table of the plain level encoders for (eb, radius), host
+ * only: 64 entries of 4 floats {S_h, S_h+1, lo_h, hi_h} (see QuantTable in
+ * the sources), the float 0.5 / eb and whether the table is used. It
+ * restates quantize_range_nodec (FD5:1216-1229) for |d| < S_64. */
+stz_status stz_debug_quant_table(double eb, int radius, float* entries, float* r2, int* on);
 /* Canonical codebook the container format derives from a histogram of nbins
  * code counts (host only): n_used symbols and lengths in canonical order. The
  * reference's equivalent is SZ3-ncp HuffmanEncoder::preprocess_encode_fast

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -56,6 +57,83 @@ QuantParams make_quant_params(double eb, int radius)
     q.tlo32 = f > 0.f ? f : 0.f;
     q.tlo64 = d > 0.0 ? d : 0.0;
     return q;
+}
+
+namespace {
+// Host mirrors of the device's f32 quantizer operations.
+float ftz32(float x) { return std::fabs(x) < FLT_MIN ? std::copysign(0.0f, x) : x; }
+float next_up(float x) { return std::nextafter(x, INFINITY); }
+float next_down(float x) { return std::nextafter(x, 0.0f); }
+// The least float a >= 0 with pred(a), pred monotone (false then true),
+// searched from guess g; +inf when none below FLT_MAX.
+template <class P>
+float least_true(float g, P pred)
+{
+    if (!(g >= 0.0f) || !std::isfinite(g)) g = 0.0f;
+    int steps = 0;
+    if (pred(g)) {
+        while (g > 0.0f && pred(next_down(g)) && ++steps < 256) g = next_down(g);
+        if (steps < 256) return g;
+    } else {
+        while (g < FLT_MAX && !pred(g) && ++steps < 256) g = next_up(g);
+        if (steps < 256) return pred(g) ? g : INFINITY;
+    }
+    // far from the guess: bisection over the positive float bit patterns
+    uint32_t lo = 0, hi = 0x7f7fffffu;  // pred(hi) assumed; answer in [lo, hi]
+    auto f = [](uint32_t u) {
+        float x;
+        std::memcpy(&x, &u, 4);
+        return x;
+    };
+    if (!pred(f(hi))) return INFINITY;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (pred(f(mid))) hi = mid;
+        else lo = mid + 1;
+    }
+    return f(lo);
+}
+}  // namespace
+
+QuantTable make_quant_table(const QuantParams& qp)
+{
+    QuantTable t{};
+    const double eb = qp.eb, recip = qp.recip;
+    const int H = std::min(kQuantTableH, qp.radius - 2);  // every entry in range (ad < 2 radius - 1)
+    for (int h = 0; h < kQuantTableH; ++h) t.e[h] = make_float4(INFINITY, INFINITY, INFINITY, -INFINITY);
+    t.r2 = (float)(0.5 / eb);
+    t.on = 0;
+    if (!(eb >= 1e-30) || !(eb <= 1e30) || !std::isfinite(recip) || H < 1) return t;
+    // S_h for h = 0..H: least |d| with trunc(fl64(|d| * recip)) >= 2h - 1
+    std::vector<float> S(H + 1);
+    S[0] = 0.0f;
+    for (int h = 1; h <= H; ++h) {
+        const double m = 2.0 * h - 1.0;
+        S[h] = least_true((float)(m * eb), [&](float a) { return (double)a * recip >= m; });
+    }
+    for (int h = 0; h < H; ++h) {
+        if (!std::isfinite(S[h + 1])) break;
+        float lo, hi;
+        const float top = next_down(S[h + 1]);  // the interval's last float
+        if (h == 0) {
+            // half 0: the decompressed value is +-0, the check is |d| <= eb
+            lo = 0.0f;
+            const float hmax = least_true((float)eb, [&](float a) { return (double)a > eb; });
+            hi = std::min(top, next_down(hmax));
+        } else {
+            const float mag = ftz32((float)((double)(2 * h) * eb));
+            // |fl32(mag - a)| <= eb, fl32 flushed as the device's sub.rn.ftz
+            const float a1 = least_true(std::max(0.0f, (float)(mag - eb)),
+                                        [&](float a) { return (double)ftz32(mag - a) <= eb; });
+            const float a2n = least_true((float)(mag + eb), [&](float a) { return (double)ftz32(mag - a) < -eb; });
+            lo = std::max(S[h], a1);
+            hi = std::min(top, next_down(a2n));
+        }
+        if (lo > hi) lo = INFINITY, hi = -INFINITY;  // nothing in the interval passes
+        t.e[h] = make_float4(S[h], S[h + 1], lo, hi);
+    }
+    t.on = 1;
+    return t;
 }
 
 Geometry make_geometry(int nx, int ny, int nz, int chunk_high, int chunk_low, int radius)
@@ -2021,6 +2099,21 @@ stz_status stz_plan_box(size_t nx, size_t ny, size_t nz, int chunk_high, int chu
     *n_out = flat.size();
     if (flat.size() > cap) STZ_FAIL(STZ_ERR_RANGE, "output capacity too small");
     std::memcpy(out, flat.data(), flat.size() * 8);
+    return STZ_OK;
+}
+
+stz_status stz_debug_quant_table(double eb, int radius, float* entries, float* r2, int* on)
+{
+    g_err.clear();
+    if (!entries || !r2 || !on) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (!(eb > 0) || radius < 1) STZ_FAIL(STZ_ERR_ARG, "bad eb or radius");
+    const QuantTable t = make_quant_table(make_quant_params(eb, radius));
+    for (int h = 0; h < kQuantTableH; ++h) {
+        entries[4 * h] = t.e[h].x, entries[4 * h + 1] = t.e[h].y;
+        entries[4 * h + 2] = t.e[h].z, entries[4 * h + 3] = t.e[h].w;
+    }
+    *r2 = t.r2;
+    *on = t.on;
     return STZ_OK;
 }
 

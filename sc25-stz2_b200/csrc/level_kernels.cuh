@@ -249,7 +249,8 @@ template <typename T, int PRED, bool FINEST, class Acc>
 __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>& io, const LevelGeom& geo,
                                                 const QuantParams& qp, const T* lut, const ZWalk& zw,
                                                 const T* __restrict__ fp, T* __restrict__ gp, uint32_t (*sh)[kSmemBins],
-                                                int wlo, int wn, const HistArgs& hist, uint32_t (&center)[7])
+                                                int wlo, int wn, const HistArgs& hist, uint32_t (&center)[7],
+                                                const float4* qtab, float qr2)
 {
     using A = Ar<T>;
     using T2 = typename V2<T>::type;
@@ -281,7 +282,8 @@ __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>&
         if (quantize_is_centre(d, qp)) {
             ++center[b];
         } else {
-            code = quantize_full(d, qp);
+            if constexpr (sizeof(T) == 4) code = qtab ? quantize_table(d, qp, qtab, qr2) : quantize_full(d, qp);
+            else code = quantize_full(d, qp);
             if (code == qp.radius) {
                 ++center[b];
             } else {
@@ -313,7 +315,8 @@ __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>&
 template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
 __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                          QuantParams qp, HistArgs hist, LearnedArgs<T> la,
-                                                         const __grid_constant__ CUtensorMap tmap, int use_tma)
+                                                         const __grid_constant__ CUtensorMap tmap, int use_tma,
+                                                         const __grid_constant__ QuantTable qt)
 {
     static_assert(LM == kLearnNone || ZB == kZSmall, "learned kernels use the default tile depth");
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -345,6 +348,12 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
     [[maybe_unused]] bool tc_failed = false;
     if constexpr (LM == kLearnTc) tc::net_setup(*net_smem(), *la.model, tid);
     if constexpr (LM == kLearnNone) {
+        // the f32 quantizer table in shared memory (read after the tile's
+        // barrier below it in the kernel's order: staged before the walk)
+        __shared__ float4 qtab[kQuantTableH];
+        const bool use_qt = sizeof(T) == 4 && qt.on;
+        if (use_qt && tid < kQuantTableH) qtab[tid] = qt.e[tid];
+        __syncthreads();
         ZWalk zw;
         zw.init(geo, x, y, z0);
         const size_t s = (size_t)io.s;
@@ -354,7 +363,9 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
         T* gp = FINEST ? nullptr : io.G + (2 * (size_t)z0) * gsy + (2 * (size_t)y) * 2 * geo.dx + 2 * (size_t)x;
         for (int z = z0; z < z1; ++z) {
             const TileAt<T, TSX, TPLANE> r{tile + (z - z0 + 1) * TPLANE + (threadIdx.y + 1) * TSX + threadIdx.x + 1};
-            if (valid) encode_interior<T, PRED, FINEST>(r, io, geo, qp, lut, zw, fp, gp, sh, wlo, wn, hist, center);
+            if (valid)
+                encode_interior<T, PRED, FINEST>(r, io, geo, qp, lut, zw, fp, gp, sh, wlo, wn, hist, center,
+                                                 use_qt ? qtab : nullptr, qt.r2);
             zw.next();
             fp += fstep;
             if constexpr (!FINEST) gp += 2 * gsy;

@@ -26,6 +26,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -653,6 +654,17 @@ EncodeTiledFn encode_tiled_fn()
     return f;
 }
 
+// The f32 quantizer table is the default; STZ_QUANT_TABLE=0 sends every
+// non-centre residual through quantize_full (same codes), for comparisons.
+bool quant_table_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("STZ_QUANT_TABLE");
+        return !(e && std::strcmp(e, "0") == 0);
+    }();
+    return on;
+}
+
 // TMA staging is the default; STZ_TILE_LOAD=threads loads the tile with the
 // CTA's threads (same tile, for comparisons).
 bool tma_tiles_enabled()
@@ -718,6 +730,8 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     alignas(64) CUtensorMap tmap;
     std::memset(&tmap, 0, sizeof(tmap));
     const int use_tma = interior && make_tile_map(a.coarse, g.dx, g.dy, g.dz, zb, &tmap) ? 1 : 0;
+    QuantTable qt{};
+    if (std::is_same<T, float>::value && interior && !learned && quant_table_enabled()) qt = make_quant_table(a.qp);
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
         if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
@@ -728,7 +742,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
                         : a.learned.tensor_cores ? k_level_encode<T, P, F, kLearnTc>                           \
                                                  : k_level_encode<T, P, F, kLearnDp4a>;                        \
             allow_smem(kern, sm);                                                                                  \
-            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned, tmap, use_tma);                        \
+            kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned, tmap, use_tma, qt);                    \
         }                                                                                                          \
         if (ns && !par) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);        \
     } while (0)

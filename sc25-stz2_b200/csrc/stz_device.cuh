@@ -560,6 +560,20 @@ __device__ __forceinline__ int quantize_full(T d, const QuantParams& qp)
     return neg ? qp.radius - half : qp.radius + half;
 }
 
+// quantize_full of an f32 residual through the level's QuantTable (tab in
+// shared memory, r2 = 0.5 / eb in float): the table entry of the estimated
+// half index decides when |d| lies inside its interval, else quantize_full
+// itself does (interval edges, values beyond the table, NaN, inf).
+__device__ __forceinline__ int quantize_table(float d, const QuantParams& qp, const float4* tab, float r2)
+{
+    const float a = fabsf(d);
+    const int h = min(max(__float2int_rn(a * r2), 0), kQuantTableH - 1);
+    const float4 e = tab[h];
+    if (!(a >= e.x && a < e.y)) return quantize_full(d, qp);
+    const bool pass = a >= e.z && a <= e.w;
+    return pass ? (Ar<float>::is_neg(d) ? qp.radius - h : qp.radius + h) : 0;
+}
+
 // recover LUT entry (FD5:1531-1535): (T)(2*(q - radius)*eb).
 template <typename T>
 __device__ __forceinline__ T recover(int q, const QuantParams& qp)

@@ -91,6 +91,24 @@ struct QuantParams {
 // Quantizer constants with the fast-path thresholds filled in.
 QuantParams make_quant_params(double eb, int radius);
 
+// Exact f32 quantizer table of one eb (the plain level encoders): for half
+// index h < kQuantTableH, entry h = {S_h, S_{h+1}, lo_h, hi_h} on |d|: the
+// residuals with S_h <= |d| < S_{h+1} are the ones quantize_full puts at
+// half h (S_h = the least float with trunc(|d| / eb) >= 2h - 1, S_0 = 0), and
+// of those exactly lo_h <= |d| <= hi_h pass its error check (code radius +- h;
+// the others are unpredictable, code 0). Every threshold is found on the
+// host with the device's own operations (IEEE double products, float
+// subtraction flushed to zero), so the table reproduces quantize_full bit for
+// bit; |d| outside an entry's interval, or beyond the table, takes
+// quantize_full itself. r2 (~ 0.5 / eb in float) only estimates h.
+constexpr int kQuantTableH = 64;
+struct QuantTable {
+    float4 e[kQuantTableH];
+    float r2;
+    int on;  // 0: every residual takes quantize_full (eb out of the table's range)
+};
+QuantTable make_quant_table(const QuantParams& qp);
+
 // One refinement level: the 7 residual sub-blocks of size (dx,dy,dz) predicted
 // from the decoded coarse grid of the same size.
 struct LevelGeom {

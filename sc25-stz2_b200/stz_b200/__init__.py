@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.stz_plan_box.argtypes = [sz, sz, sz, C.c_int, C.c_int, i64p, i64p, i64p, sz, C.POINTER(sz)]
     lib.stz_debug_stream_codes.argtypes = [vp, vp, C.c_int, C.c_int, vp, sz, C.POINTER(sz)]
     lib.stz_debug_codebook.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
+    lib.stz_debug_quant_table.argtypes = [C.c_double, C.c_int, vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]
     lib.stz_debug_run_slots.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     lib.stz_quantize_noalloc_dev.argtypes = [C.c_int, vp, sz, C.c_double, C.c_int, vp, vp, C.POINTER(sz), vp]
     lib.stz_context_stream.argtypes = [vp, C.POINTER(vp)]
@@ -636,6 +637,16 @@ def plan_box(dims_xyz, chunk_high, chunk_low, a, b) -> np.ndarray:
     _check(lib.stz_plan_box(*[int(d) for d in dims_xyz], chunk_high, chunk_low, aa, bb,
                             out.ctypes.data_as(C.POINTER(C.c_int64)), cap, C.byref(n)))
     return out[: n.value].copy()
+
+
+def quant_table(eb: float, radius: int = 32768):
+    """The f32 quantizer table of the plain level encoders (host only):
+    (entries (64, 4) float32 {S_h, S_h+1, lo_h, hi_h}, r2, on)."""
+    lib = load_library()
+    e = np.zeros((64, 4), dtype=np.float32)
+    r2, on = C.c_float(), C.c_int()
+    _check(lib.stz_debug_quant_table(eb, radius, e.ctypes.data_as(C.c_void_p), C.byref(r2), C.byref(on)))
+    return e, np.float32(r2.value), bool(on.value)
 
 
 def codebook(hist: np.ndarray):
