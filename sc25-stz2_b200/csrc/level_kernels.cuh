@@ -85,16 +85,19 @@ struct OwnedAxis {
 // the interior range (all owned x, y); z inside, y outside (all owned x); z
 // and y inside, x outside. f(x, y, z) for each, spread over the CTA's threads.
 // bz / nbz: the CTA's brick index along z and the level's brick count (a
-// launch may cover a range of z-bricks).
-template <class F>
+// launch may cover a range of z-bricks). XCOLS: only the third box (the
+// x-boundary columns beside the interior; the encoders leave the other two
+// to the boundary-shell kernel, whose z-planes and y-rows it reads
+// coalesced, while a column point per thread is not).
+template <bool XCOLS = false, class F>
 __device__ __forceinline__ void for_owned_boundary(const LevelGeom& g, int ZB, int bz, int nbz, int tid, int nthreads,
                                                    F&& f)
 {
     const OwnedAxis X = OwnedAxis::make(g.dx, blockIdx.x, gridDim.x, BX);
     const OwnedAxis Y = OwnedAxis::make(g.dy, blockIdx.y, gridDim.y, BY);
     const OwnedAxis Z = OwnedAxis::make(g.dz, bz, nbz, ZB);
-    const int ga = X.n() * Y.n() * Z.nb();
-    const int gb = X.n() * Y.nb() * Z.ni();
+    const int ga = XCOLS ? 0 : X.n() * Y.n() * Z.nb();
+    const int gb = XCOLS ? 0 : X.n() * Y.nb() * Z.ni();
     const int gc = X.nb() * Y.ni() * Z.ni();
     for (int i = tid; i < ga + gb + gc; i += nthreads) {
         int x, y, z;
@@ -369,6 +372,23 @@ __global__ void __launch_bounds__(BX* BY) k_level_encode(EncodeIO<T> io, const T
             zw.next();
             fp += fstep;
             if constexpr (!FINEST) gp += 2 * gsy;
+        }
+        // the x-boundary columns beside this CTA's interior points, from the
+        // same tile (first and last CTAs along x; the shell kernel skips them)
+        if (blockIdx.x == 0 || blockIdx.x == gridDim.x - 1) {
+            const int bz = blockIdx.z;
+            for_owned_boundary<true>(geo, ZB, bz, (int)gridDim.z, tid, BX * BY, [&](int px, int py, int pz) {
+                const TileAt<T, TSX, TPLANE> rb{tile + (pz - z0 + 1) * TPLANE + (py - y0 + 1) * TSX + (px - x0 + 1)};
+                ChunkIndex bci;
+                bci.init(geo, px, py);
+                int q[7];
+                encode_point<T, PRED, FINEST, false>(rb, io, geo, qp, lut, bci, px, py, pz, q);
+#pragma unroll
+                for (int b = 0; b < 7; ++b) {
+                    if (q[b] == qp.radius) ++center[b];
+                    else hist_add(sh, wlo, wn, hist, b, q[b], 1u);
+                }
+            });
         }
     }
     for (int z = z0; z < z1 && LM != kLearnNone; ++z) {

@@ -717,9 +717,14 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
                       : tiny  ? tile_bytes<T, kZTiny>()
                               : tile_bytes<T>();
     // the boundary shell runs beside the interior on the side stream (folding
-    // it into the interior CTAs, as the decoder does, left the finest encode
-    // level and slowed the coarser ones, whose shells are a large share)
-    const uint64_t ns = shell.total();
+    // all of it into the interior CTAs, as the decoder does, left the finest
+    // encode level and slowed the coarser ones, whose shells are a large share
+    // and whose z-plane CTAs run last). Plain interior kernels take the
+    // x-boundary columns themselves: their owners are spread over the launch,
+    // and a column point per shell thread read the field and grid uncoalesced.
+    Shell shell_k = shell;
+    if (interior && !learned) shell_k.g3 = 0;
+    const uint64_t ns = shell_k.total();
     const int gs = (int)std::min<uint64_t>((ns + 255) / 256, 148 * 16);
     const bool par = a.side.st && interior && ns;
     cudaStream_t ss = par ? a.side.st : st;
@@ -734,7 +739,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     if (std::is_same<T, float>::value && interior && !learned && quant_table_enabled()) qt = make_quant_table(a.qp);
 #define STZ_ENC(P, F)                                                                                              \
     do {                                                                                                           \
-        if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell);         \
+        if (ns && par) k_level_encode_shell<T, P, F><<<gs, 256, 0, ss>>>(io, a.coarse, g, a.qp, h, shell_k);       \
         if (interior) {                                                                                            \
             auto kern = big                          ? k_level_encode<T, P, F, kLearnNone, kZBig>                  \
                         : tiny                   ? k_level_encode<T, P, F, kLearnNone, kZTiny>                 \
@@ -744,7 +749,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
             allow_smem(kern, sm);                                                                                  \
             kern<<<grd, blk, sm, st>>>(io, a.coarse, g, a.qp, h, a.learned, tmap, use_tma, qt);                    \
         }                                                                                                          \
-        if (ns && !par) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell);        \
+        if (ns && !par) k_level_encode_shell<T, P, F><<<gs, 256, 0, st>>>(io, a.coarse, g, a.qp, h, shell_k);      \
     } while (0)
     const bool finest = a.stride == 1;
     if (a.predictor == 1) {
