@@ -34,8 +34,38 @@ struct Shell {
     uint64_t total() const { return g1 + g2 + g3; }
     // k-th boundary index of an axis of size d: 0, d-2, d-1 (all when d < 4)
     __device__ static int bval(int k, int d) { return d < 4 ? k : (k == 0 ? 0 : d - 3 + k); }
+    // 32-bit index arithmetic when the shell and a plane fit (64-bit
+    // division is a long instruction sequence on the GPU)
+    __host__ __device__ bool small() const
+    {
+        return g1 + g2 + g3 < (1ull << 31) && (uint64_t)dx * dy < (1ull << 31);
+    }
+    __device__ void point32(uint32_t i, int& x, int& y, int& z) const
+    {
+        const uint32_t G1 = (uint32_t)g1, G2 = (uint32_t)g2, udx = (uint32_t)dx;
+        if (i < G1) {
+            const uint32_t plane = (uint32_t)dy * udx;
+            const uint32_t kz = i / plane, r = i - kz * plane;
+            z = nbz == dz ? (int)kz : bval((int)kz, dz);
+            y = (int)(r / udx), x = (int)(r - (uint32_t)y * udx);
+        } else if (i < G1 + G2) {
+            const uint32_t j = i - G1, plane = (uint32_t)nby * udx;
+            const uint32_t kz = j / plane, r = j - kz * plane;
+            z = 1 + (int)kz;
+            y = bval((int)(r / udx), dy), x = (int)(r % udx);
+        } else {
+            const uint32_t j = i - G1 - G2, plane = (uint32_t)niy * (uint32_t)nbx;
+            const uint32_t kz = j / plane, r = j - kz * plane;
+            z = 1 + (int)kz;
+            y = 1 + (int)(r / (uint32_t)nbx), x = bval((int)(r % (uint32_t)nbx), dx);
+        }
+    }
     __device__ void point(uint64_t i, int& x, int& y, int& z) const
     {
+        if (small()) {
+            point32((uint32_t)i, x, y, z);
+            return;
+        }
         if (i < g1) {
             const uint64_t plane = (uint64_t)dy * dx;
             const int kz = (int)(i / plane);
@@ -373,9 +403,11 @@ __global__ void __launch_bounds__(BX* BY, FINEST && LM == kLearnNone && sizeof(T
             fp += fstep;
             if constexpr (!FINEST) gp += 2 * gsy;
         }
-        // the x-boundary columns beside this CTA's interior points, from the
-        // same tile (first and last CTAs along x; the shell kernel skips them)
-        if (blockIdx.x == 0 || blockIdx.x == gridDim.x - 1) {
+        // the finest level's x-boundary columns beside this CTA's interior
+        // points, from the same tile (first and last CTAs along x; the shell
+        // kernel skips them there; on the coarser levels the extra registers
+        // and the serial tail cost more than the shell's uncoalesced reads)
+        if (FINEST && (blockIdx.x == 0 || blockIdx.x == gridDim.x - 1)) {
             const int bz = blockIdx.z;
             for_owned_boundary<true>(geo, ZB, bz, (int)gridDim.z, tid, BX * BY, [&](int px, int py, int pz) {
                 const TileAt<T, TSX, TPLANE> rb{tile + (pz - z0 + 1) * TPLANE + (py - y0 + 1) * TSX + (px - x0 + 1)};
