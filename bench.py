@@ -698,8 +698,10 @@ def algorithmic_bytes(kernel: str, N: int, elem: int, K: int, raw_payload: int) 
         return raw_payload + all_syms * 2  # read payload, write codes
     if kernel == "k_encode":
         return all_syms * 2 + raw_payload  # read codes, write payload
-    if kernel == "k_sub_bits":
+    if kernel == "k_sub_bits" or kernel == "k_run_stats":
         return all_syms * 2
+    if kernel == "k_minmax":
+        return N * elem
     return None
 
 

@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(BX* BY, LM == kLearnNone && sizeof(T) == 4 ? (
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     __shared__ uint32_t sh[7][kSmemBins];
-    __shared__ T lut[2 * kRecW];
+    __shared__ T lut[FINEST ? 1 : 2 * kRecW];  // the finest level writes no decoded grid
     const int tid = threadIdx.y * BX + threadIdx.x;
     for (int i = tid; i < 7 * kSmemBins; i += BX * BY) (&sh[0][0])[i] = 0;
     if constexpr (!FINEST) build_recover_lut(lut, qp, tid, BX * BY);

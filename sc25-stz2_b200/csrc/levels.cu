@@ -631,6 +631,9 @@ template <class K>
 void allow_smem(K kernel, size_t bytes)
 {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // the whole unified L1 / shared array as shared memory: five finest-encode
+    // CTAs (45.6 KB each) fit only in the largest carveout
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
