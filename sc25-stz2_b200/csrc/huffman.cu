@@ -948,7 +948,7 @@ __global__ void __launch_bounds__(kDecodeThreads, 5) k_decode(const CtaWork* __r
 
 // Persistent variant: a fixed grid walks the work list of a batch held in
 // device memory (BatchHdr at meta), so one captured launch serves any batch;
-// each item is cut into kDecodeSlices slices of 8 planes.
+// each warp-decoded item is cut into kDecodeSlices slices of 8 planes.
 __global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __restrict__ meta,
                                                                const StreamDesc* __restrict__ sd,
                                                                const DecodeTables* __restrict__ tabs,
@@ -956,16 +956,31 @@ __global__ void __launch_bounds__(kDecodeThreads) k_decode_dyn(const uint8_t* __
                                                                const uint32_t* __restrict__ sub_off,
                                                                const uint64_t* __restrict__ chunk_word_off,
                                                                const uint32_t* __restrict__ payload,
-                                                               uint16_t* __restrict__ codes)
+                                                               uint16_t* __restrict__ codes, uint32_t seq_bits)
 {
     const BatchHdr* h = reinterpret_cast<const BatchHdr*>(meta);
     const uint32_t n = h->n_work;
     const CtaWork* __restrict__ work = reinterpret_cast<const CtaWork*>(meta + h->o_work);
     const uint32_t* __restrict__ chunk_ids = reinterpret_cast<const uint32_t*>(meta + h->o_ids);
     const uint32_t nw = blockDim.x >> 5, S = kDecodeSlices;
+    // In a batch of at least kSeqMinItems items, dense streams decode one
+    // thread per plane (as k_decode does for large launches): a CTA takes
+    // whole items, striding over the items so every CTA gets some.
+    const uint32_t sb = n >= (uint32_t)kSeqMinItems ? seq_bits : 0xffffffffu;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const CtaWork w = work[i];
+        const StreamDesc s = sd[w.stream];
+        if (!decode_sequential(s, sb)) continue;  // uniform per block
+        const uint32_t t = threadIdx.x;
+        if (t < w.count * s.C)
+            decode_plane_seq(tabs + w.stream, s, chunk_ids[w.first + t / s.C], t % s.C, cb_sym, sub_off,
+                             chunk_word_off, payload, codes);
+    }
+    // the other items a warp per plane, kDecodeSlices slices per item
     for (uint32_t u = blockIdx.x; u < n * S; u += gridDim.x) {
         const CtaWork w = work[u / S];
         const StreamDesc s = sd[w.stream];
+        if (decode_sequential(s, sb)) continue;  // uniform per block
         const uint32_t W = lanes_per_plane(s.C * s.C), G = 32 / W, np = w.count * s.C;
         for (uint32_t base = ((u % S) * nw + (threadIdx.x >> 5)) * G; base < np; base += nw * S * G) {
             const uint32_t p = base + (threadIdx.x & 31) / W;
@@ -1155,7 +1170,7 @@ void launch_decode_dyn(int grid, const uint8_t* meta, const StreamDesc* sd, cons
                        const uint32_t* payload, uint16_t* codes, cudaStream_t st)
 {
     k_decode_dyn<<<grid, kDecodeThreads, 0, st>>>(meta, sd, static_cast<const DecodeTables*>(tables), cb_sym, sub_off,
-                                                  chunk_word_off, payload, codes);
+                                                  chunk_word_off, payload, codes, decode_seq_bits());
 }
 
 template <typename T>
