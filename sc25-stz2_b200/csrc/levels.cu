@@ -195,7 +195,10 @@ __device__ __forceinline__ void stage_tile(T* tile, const T* __restrict__ R, con
     else load_tile<T, ZB>(tile, R, dx, dy, dz, x0, y0, z0);
 }
 
-constexpr int kSmemBins = 512;
+// Shared histogram bins around the centre code per stream (codes outside go
+// to global atomics); 448 keeps five finest-encode CTAs within an SM's
+// shared memory.
+constexpr int kSmemBins = 448;
 
 struct HistArgs {
     uint32_t* full;     // 7 x 2r bins
