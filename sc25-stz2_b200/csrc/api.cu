@@ -422,13 +422,6 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemsetAsync(ctx->hist.p, 0, (size_t)nstreams * R2 * 4, st));
     STZ_CUDA(cudaMemsetAsync(ctx->hist_out.p, 0, (size_t)nstreams * 4, st));
     STZ_CUDA(cudaMemsetAsync(ctx->unpred_cnt.p, 0, g.total_chunk_slots * 4, st));
-    // literal bitmask: the level encoders mark every non-centre code, so the
-    // coder's passes read 1 bit per code instead of the codes (two words of
-    // padding for their 64-bit window reads)
-    const size_t lm_bytes = ((size_t)(g.total_codes + 31) / 32 + 2) * 4;
-    STZ_CUDA(ctx->lmask.ensure(lm_bytes));
-    STZ_CUDA(cudaMemsetAsync(ctx->lmask.p, 0, lm_bytes, st));
-    uint32_t* const lmask = ctx->lmask.as<uint32_t>();
 
     // coarsest grid
     const size_t n0 = (size_t)g.c0[0] * g.c0[1] * g.c0[2];
@@ -470,8 +463,6 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         a.hist_full = ctx->hist.as<uint32_t>() + (size_t)(k - 1) * 7 * R2;
         a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
         a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
-        a.lmask = lmask;
-        a.lbase = s0.code_off;
         a.qp = make_quant_params(ebk[k], o.radius);
         a.learned.tensor_cores = learned_tensor_cores();
         if (const int mi = level_model(k); mi >= 0) {
@@ -586,7 +577,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         {
             KScope ks(ctx, "k_run_stats");
             launch_run_stats((const CtaWork*)(dw + r_work), (const uint32_t*)(dw + r_ids), (int)work.size(),
-                             (const StreamDesc*)(dw + r_sd), ctx->codes.as<uint16_t>(), lmask,
+                             (const StreamDesc*)(dw + r_sd), ctx->codes.as<uint16_t>(),
                              ctx->rstats.as<unsigned long long>(), st);
         }
         STZ_CUDA(cudaGetLastError());
@@ -699,7 +690,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     {
         KScope ks(ctx, "k_sub_bits");
-        launch_sub_bits(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), lmask, ctx->ctab.as<uint32_t>(),
+        launch_sub_bits(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), ctx->ctab.as<uint32_t>(),
                         ctx->sub_bits.as<uint32_t>(), st);
     }
     {
@@ -781,7 +772,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     for (size_t gi = 0; gi < ngroups; ++gi) {
         {
             KScope ks(ctx, "k_encode");
-            launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(), lmask,
+            launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
                           ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
                           ctx->payload.as<uint32_t>(), st);
         }

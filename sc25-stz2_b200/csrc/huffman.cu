@@ -120,19 +120,11 @@ struct LaneSeg {
     uint32_t P, a, b;  // plane size; this lane's codes [a, b)
     uint32_t W, lane;  // lanes of the group; this lane's index in it
     bool vec;          // segments are whole 16-byte groups of 8 codes
-    // Literal bitmask of every code (bit i of word i >> 5 set when code i is
-    // not the centre code), written by the level encoders, and the global
-    // index of the plane's first code in it; null: compare the codes.
-    const uint32_t* lm;
-    uint64_t base;
 };
 
-__device__ __forceinline__ LaneSeg lane_seg(uint32_t C, const uint16_t* src, uint32_t W, bool active,
-                                            const uint32_t* lm = nullptr, uint64_t base = 0)
+__device__ __forceinline__ LaneSeg lane_seg(uint32_t C, const uint16_t* src, uint32_t W, bool active)
 {
     LaneSeg g;
-    g.lm = lm;
-    g.base = base;
     g.P = C * C;
     g.W = W;
     g.lane = threadIdx.x & (W - 1);
@@ -188,15 +180,6 @@ __device__ __forceinline__ uint32_t pair_mask(uint32_t w, uint32_t R2)
 __device__ __forceinline__ uint32_t literal_mask(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t p,
                                                  uint32_t n, uint32_t R)
 {
-    const uint32_t keep = n == 32 ? ~0u : (1u << n) - 1;
-    if (g.lm) {  // bits [base + p, base + p + n) of the literal bitmask
-        const uint64_t i = g.base + p;
-        const uint32_t* w = g.lm + (i >> 5);
-        const uint32_t sh = (uint32_t)(i & 31);
-        const uint32_t lo = __ldg(w);
-        const uint32_t v = sh ? __funnelshift_r(lo, __ldg(w + 1), sh) : lo;
-        return v & keep;
-    }
     uint32_t m = 0;  // centre codes
     if (g.vec) {
         const uint4* v = reinterpret_cast<const uint4*>(src + p);
@@ -212,7 +195,7 @@ __device__ __forceinline__ uint32_t literal_mask(const uint16_t* __restrict__ sr
     } else {
         for (uint32_t i = 0; i < n; ++i) m |= (uint32_t)(__ldg(src + p + i) == R) << i;
     }
-    return ~m & keep;
+    return ~m & (n == 32 ? ~0u : (1u << n) - 1);
 }
 
 // A lane's plane segment with runs, as 32-code blocks: the literal mask of
@@ -255,9 +238,7 @@ struct RunLane {
 
     // The lane's symbols in order: f(sym). Between consecutive literals of a
     // block every code is a centre code, so the runs are the gaps.
-    // LITERALS false: a literal reaches f as 0xffffffff (neither the centre
-    // code nor a run symbol) without its code being read.
-    template <bool LITERALS = true, class F>
+    template <class F>
     __device__ __forceinline__ void symbols(const uint16_t* __restrict__ src, const LaneSeg& g, const StreamDesc& s,
                                             F&& f) const
     {
@@ -273,7 +254,7 @@ struct RunLane {
                     run_symbols(run, s.radius, s.run_base, J, D, LD, f);
                     run = 0;
                 }
-                f(LITERALS ? (uint32_t)__ldg(src + p + j) : 0xffffffffu);
+                f((uint32_t)__ldg(src + p + j));
                 i = j + 1;
                 lit &= lit - 1;
             }
@@ -301,7 +282,6 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
                                                             const uint32_t* __restrict__ chunk_ids,
                                                             const StreamDesc* __restrict__ sd,
                                                             const uint16_t* __restrict__ codes,
-                                                            const uint32_t* __restrict__ lm,
                                                             unsigned long long* __restrict__ stats)
 {
     __shared__ uint32_t cnt[kRunStats];
@@ -316,13 +296,11 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
     {
         STZ_GROUP_PLANE(np, W);
         const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
-        const uint64_t pbase = s.code_off + (uint64_t)c * P * C + (uint64_t)lz * P;
-        const uint16_t* src = codes + pbase;
-        const LaneSeg g = lane_seg(C, src, W, active, lm, pbase);
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src, W, active);
         RunLane rl;
         rl.init(src, g, s.radius);
-        // only run symbols and centre singles are counted: no literal is read
-        rl.symbols<false>(src, g, s, [&](uint32_t sym) {
+        rl.symbols(src, g, s, [&](uint32_t sym) {
             if (sym == s.radius) ++singles;
             else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
         });
@@ -339,7 +317,6 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
                                                            const uint32_t* __restrict__ chunk_ids,
                                                            const StreamDesc* __restrict__ sd,
                                                            const uint16_t* __restrict__ codes,
-                                                           const uint32_t* __restrict__ lm,
                                                            const uint32_t* __restrict__ ctab,
                                                            uint32_t* __restrict__ sub_bits)
 {
@@ -351,9 +328,8 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
     {
         STZ_GROUP_PLANE(np, W);
         const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
-        const uint64_t pbase = s.code_off + (uint64_t)c * P * C + (uint64_t)lz * P;
-        const uint16_t* src = codes + pbase;
-        const LaneSeg g = lane_seg(C, src, W, active, lm, pbase);
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src, W, active);
         uint32_t bits = 0;
         auto add = [&](uint32_t sym) { bits += __ldg(tab + sym) & 31u; };
         if (s.run_n) {
@@ -464,7 +440,6 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
                                                          const uint32_t* __restrict__ chunk_ids,
                                                          const StreamDesc* __restrict__ sd,
                                                          const uint16_t* __restrict__ codes,
-                                                         const uint32_t* __restrict__ lm,
                                                          const uint32_t* __restrict__ ctab,
                                                          const uint32_t* __restrict__ sub_off,
                                                          const uint64_t* __restrict__ chunk_word_off,
@@ -478,9 +453,8 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
     {
         STZ_GROUP_PLANE(np, W);
         const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
-        const uint64_t pbase = s.code_off + (uint64_t)c * P * C + (uint64_t)lz * P;
-        const uint16_t* src = codes + pbase;
-        const LaneSeg g = lane_seg(C, src, W, active, lm, pbase);
+        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+        const LaneSeg g = lane_seg(C, src, W, active);
         RunLane rl;
         if (s.run_n) rl.init(src, g, s.radius);
         auto each = [&](auto&& f) {
@@ -1121,19 +1095,15 @@ void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* 
 }
 
 void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                      const uint16_t* codes, const uint32_t* lmask, unsigned long long* stats, cudaStream_t st)
+                      const uint16_t* codes, unsigned long long* stats, cudaStream_t st)
 {
-    if (nwork > 0)
-        k_run_stats<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, lmask, stats);
+    if (nwork > 0) k_run_stats<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, stats);
 }
 
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                     const uint16_t* codes, const uint32_t* lmask, const uint32_t* ctab, uint32_t* sub_bits,
-                     cudaStream_t st)
+                     const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st)
 {
-    if (nwork)
-        k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, lmask, ctab,
-                                                                        sub_bits);
+    if (nwork) k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
 }
 
 void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks, const uint32_t* sub_bits,
@@ -1146,12 +1116,11 @@ void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks
 }
 
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* codes, const uint32_t* lmask, const uint32_t* ctab, const uint32_t* sub_off,
-                   const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st)
+                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
+                   uint32_t* payload, cudaStream_t st)
 {
     if (nwork)
-        k_encode<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, lmask, ctab, sub_off,
-                                                                      chunk_word_off, payload);
+        k_encode<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_off, chunk_word_off, payload);
 }
 
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,

@@ -160,18 +160,6 @@ struct EncodeIO {
     T* __restrict__ unpred_dense;
     uint32_t* __restrict__ unpred_cnt;
     T* __restrict__ G;  // decoded fine grid (coarser levels only)
-    // Literal bitmask of the whole codes array (bit i of word i >> 5: code i
-    // is not the centre code), zeroed before the level encodes; lbase is the
-    // index of this level's first code in it. Null: not kept.
-    uint32_t* lmask;
-    uint64_t lbase;
-    __device__ __forceinline__ void mark_literal(size_t i) const
-    {
-        if (lmask) {
-            const uint64_t g = lbase + i;
-            atomicOr(lmask + (g >> 5), 1u << (g & 31));
-        }
-    }
 };
 
 // Learned correction modes of the level kernels: none, the network per
@@ -249,7 +237,6 @@ __device__ __forceinline__ void encode_residuals(const EncodeIO<T>& io, const Le
         const int code = quantize(d, qp);
         q[b] = code;
         io.codes[(size_t)b * n + cm] = (uint16_t)code;
-        if (code != qp.radius) io.mark_literal((size_t)b * n + cm);
         if (code == 0) {
             io.unpred_dense[(size_t)b * n + cm] = d;
             atomicAdd(&io.unpred_cnt[(size_t)b * (geo.nchunks() + 1) + chunk], 1u);
@@ -334,7 +321,6 @@ __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>&
                 ++center[b];
             } else {
                 hist_add(sh, wlo, wn, hist, b, code, 1u);
-                io.mark_literal((size_t)b * n + zw.cm);
                 if (code == 0) {
                     io.unpred_dense[(size_t)b * n + zw.cm] = d;
                     atomicAdd(&io.unpred_cnt[(size_t)b * (geo.nchunks() + 1) + zw.chunk], 1u);

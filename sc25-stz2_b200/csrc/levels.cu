@@ -717,8 +717,7 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
     dim3 grd((shell.nix + BX - 1) / BX, (shell.niy + BY - 1) / BY, (shell.niz + zb - 1) / zb);
     const bool interior = shell.nix > 0 && shell.niy > 0 && shell.niz > 0;
     HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
-    const EncodeIO<T> io{a.field, a.fsx, a.fsy,        a.stride, a.codes, a.unpred_dense,
-                         a.unpred_cnt, a.decoded, a.lmask, a.lbase};
+    const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
     const size_t sm = learned ? kTileBytesAligned<T> + sizeof(LearnedModel)
                       : big   ? tile_bytes<T, kZBig>()
                       : tiny  ? tile_bytes<T, kZTiny>()

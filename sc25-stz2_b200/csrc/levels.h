@@ -24,8 +24,6 @@ struct LevelEncodeArgs {
     uint32_t* hist_full;    // 7 x 2*radius
     uint32_t* hist_outside; // 7
     T* decoded;             // decoded fine grid (2dx x 2dy x 2dz) or null on the finest level
-    uint32_t* lmask = nullptr;  // literal bitmask of the codes array (null: none), see EncodeIO
-    uint64_t lbase = 0;         // index of this level's first code in it
     QuantParams qp;
     LearnedArgs<T> learned; // learned correction (model null: none)
     SideStream side;        // boundary-shell kernel placement

@@ -242,7 +242,6 @@ struct stz_context {
         flush_prof();
         for (auto e : ev_pool) cudaEventDestroy(e);
     }
-    stz::DevBuf lmask;  // literal bitmask of the codes (compress)
     stz::DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, pack_meta, out, mid, boxes,
         tiles, models, eval, rstats, gwork;
