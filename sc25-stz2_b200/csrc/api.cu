@@ -408,10 +408,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const size_t elem = sizeof(T);
     double eb = 0;
     std::vector<double> ebk;
-    STZ_TRY(level_error_bounds<T>(ctx, field, N, o, K, eb, ebk));
-    lap.mark("value range");
 
-    // buffers
+    // buffers, cleared ahead of the value range
     STZ_CUDA(ctx->grid[0].ensure(g.n_fine_max * elem));
     STZ_CUDA(ctx->grid[1].ensure(g.n_fine_max * elem));
     STZ_CUDA(ctx->codes.ensure(g.total_codes * 2));
@@ -422,6 +420,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemsetAsync(ctx->hist.p, 0, (size_t)nstreams * R2 * 4, st));
     STZ_CUDA(cudaMemsetAsync(ctx->hist_out.p, 0, (size_t)nstreams * 4, st));
     STZ_CUDA(cudaMemsetAsync(ctx->unpred_cnt.p, 0, g.total_chunk_slots * 4, st));
+    STZ_TRY(level_error_bounds<T>(ctx, field, N, o, K, eb, ebk));
+    lap.mark("value range");
 
     // coarsest grid
     const size_t n0 = (size_t)g.c0[0] * g.c0[1] * g.c0[2];
@@ -430,8 +430,47 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         KScope ks(ctx, "k_subsample");
         launch_subsample<T>(field, nx, ny, nz, 1 << K, ctx->grid[cur].as<T>(), st);
     }
-    std::vector<T> coarsest(n0);
-    STZ_CUDA(cudaMemcpyAsync(coarsest.data(), ctx->grid[cur].p, n0 * elem, cudaMemcpyDeviceToHost, st));
+    // to pinned memory, so the host goes on enqueueing (read after the levels)
+    STZ_CUDA(ctx->h_small.ensure(64 + n0 * elem));
+    STZ_CUDA(cudaMemcpyAsync(ctx->h_small.as<uint8_t>() + 64, ctx->grid[cur].p, n0 * elem, cudaMemcpyDeviceToHost, st));
+
+    std::vector<StreamDesc> sd = g.sd;
+    // work list over every chunk of every stream
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    // Run statistics of every stream whose planes can take run symbols: one
+    // pass over the codes right after the level encodes, while the histograms
+    // go to the host. The counts per run class depend only on the plane size
+    // and the codes, not on which free code values the stream's run symbols
+    // later take; here they are numbered from R2, above every code, so no
+    // literal is taken for one. Work list and counters are set up now.
+    std::vector<unsigned long long> rstats((size_t)nstreams * kRunStats, 0);
+    bool rs_any = false;
+    size_t r_sd = 0, r_work = 0, r_ids = 0;
+    {
+        std::vector<StreamDesc> rsd = sd;
+        for (auto& d : rsd) {
+            d.run_n = run_slot_count(d.C * d.C);
+            d.run_base = (uint32_t)R2;
+            rs_any = rs_any || d.run_n;
+        }
+        if (rs_any) {
+            r_work = align256(rsd.size() * sizeof(StreamDesc));
+            r_ids = align256(r_work + work.size() * sizeof(CtaWork));
+            const size_t r_bytes = align256(r_ids + ids.size() * 4);
+            STZ_CUDA(ctx->h_stage.ensure(r_bytes));
+            uint8_t* hr = ctx->h_stage.as<uint8_t>();
+            std::memcpy(hr + r_sd, rsd.data(), rsd.size() * sizeof(StreamDesc));
+            std::memcpy(hr + r_work, work.data(), work.size() * sizeof(CtaWork));
+            std::memcpy(hr + r_ids, ids.data(), ids.size() * 4);
+            STZ_CUDA(ctx->work.ensure(r_bytes));
+            STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hr, r_bytes, cudaMemcpyHostToDevice, st));
+            STZ_CUDA(ctx->rstats.ensure(rstats.size() * 8));
+            STZ_CUDA(cudaMemsetAsync(ctx->rstats.p, 0, rstats.size() * 8, st));
+            STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
+        }
+    }
 
     // learned models of levels K-1 (record 0) and K (record 1) on the device
     const stz_model* M = o.model;
@@ -497,19 +536,43 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     STZ_CUDA(cudaGetLastError());
 
-    // histogram windows + outside counts + unpred counts to the host
+    // histogram windows + outside counts + unpred counts to the host, on the
+    // copy stream, while ctx->st counts the run symbols
     const int wlo = std::max(0, o.radius - kHistWindow / 2);
     const int wn = std::min(kHistWindow, R2 - wlo);
     STZ_CUDA(ctx->h_hist.ensure((size_t)nstreams * wn * 4));
     const size_t meta_bytes = (size_t)nstreams * 4 + g.total_chunk_slots * 4;
     STZ_CUDA(ctx->h_meta.ensure(meta_bytes));
+    cudaStream_t sc = ctx->st_copy;
+    cudaEvent_t ev_lv = ctx->event(), ev_hist = ctx->event();
+    STZ_CUDA(cudaEventRecord(ev_lv, st));
+    STZ_CUDA(cudaStreamWaitEvent(sc, ev_lv, 0));
     STZ_CUDA(cudaMemcpy2DAsync(ctx->h_hist.p, (size_t)wn * 4, ctx->hist.as<uint32_t>() + wlo, (size_t)R2 * 4,
-                               (size_t)wn * 4, (size_t)nstreams, cudaMemcpyDeviceToHost, st));
+                               (size_t)wn * 4, (size_t)nstreams, cudaMemcpyDeviceToHost, sc));
     uint32_t* h_out = ctx->h_meta.as<uint32_t>();
     uint32_t* h_ucnt = h_out + nstreams;
-    STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaStreamSynchronize(st));
+    STZ_CUDA(cudaMemcpyAsync(h_out, ctx->hist_out.p, (size_t)nstreams * 4, cudaMemcpyDeviceToHost, sc));
+    STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, sc));
+    STZ_CUDA(cudaEventRecord(ev_hist, sc));
+    if (rs_any) {
+        const uint8_t* dw = ctx->work.as<uint8_t>();
+        {
+            KScope ks(ctx, "k_run_stats");
+            launch_run_stats((const CtaWork*)(dw + r_work), (const uint32_t*)(dw + r_ids), (int)work.size(),
+                             (const StreamDesc*)(dw + r_sd), ctx->codes.as<uint16_t>(),
+                             ctx->rstats.as<unsigned long long>(), st);
+        }
+        STZ_CUDA(cudaGetLastError());
+        STZ_CUDA(cudaMemcpyAsync(ctx->h_rstats.p, ctx->rstats.p, rstats.size() * 8, cudaMemcpyDeviceToHost, st));
+    }
+    {
+        const cudaError_t e = cudaEventSynchronize(ev_hist);
+        ctx->ev_pool.push_back(ev_lv);
+        ctx->ev_pool.push_back(ev_hist);
+        STZ_CUDA(e);
+    }
+    std::vector<T> coarsest(n0);
+    std::memcpy(coarsest.data(), ctx->h_small.as<uint8_t>() + 64, n0 * elem);
     if (level_error_take()) STZ_FAIL(STZ_ERR_CUDA, "level kernel: a TMA tile load did not complete in time");
     if (M && M->mask && learned_tc_error_take(st))
         STZ_FAIL(STZ_ERR_CUDA, "learned correction: a tensor-core MMA did not complete in time");
@@ -531,26 +594,16 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
                 if (h_out[s]) {
                     uint32_t* dst = ctx->h_fullh.as<uint32_t>() + k++ * (size_t)R2;
                     STZ_CUDA(cudaMemcpyAsync(dst, ctx->hist.as<uint32_t>() + (size_t)s * R2, (size_t)R2 * 4,
-                                             cudaMemcpyDeviceToHost, st));
+                                             cudaMemcpyDeviceToHost, ctx->st_copy));
                     fullh[s] = dst;
                 }
-            STZ_CUDA(cudaStreamSynchronize(st));
+            // on the copy stream: ctx->st is counting run symbols (the level
+            // encodes, all these copies need, are complete)
+            STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));
         }
     }
     lap.mark("full histograms");
-    std::vector<StreamDesc> sd = g.sd;
-    // work list over every chunk of every stream
-    std::vector<CtaWork> work;
-    std::vector<uint32_t> ids;
-    std::vector<size_t> wbeg(nstreams + 1);  // each stream's range of work items
-    for (int s = 0; s < nstreams; ++s) {
-        wbeg[s] = work.size();
-        add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
-    }
-    wbeg[nstreams] = work.size();
-    // run symbols: slots in unused code values, then the symbol counts of the
-    // run-coded planes (one pass over the codes on the GPU)
-    bool any_runs = false;
+    // run symbols: J slots in unused code values, else none
     for (int s = 0; s < nstreams; ++s) {
         const uint32_t* hw = ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
         auto count = [&](uint32_t c) -> uint64_t {
@@ -558,33 +611,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             return (c >= (uint32_t)wlo && c < (uint32_t)(wlo + wn)) ? hw[c - wlo] : 0;
         };
         sd[s].run_n = (uint32_t)run_slots(count, R2, (int)(sd[s].C * sd[s].C), sd[s].run_base);
-        any_runs = any_runs || sd[s].run_n;
     }
-    std::vector<unsigned long long> rstats((size_t)nstreams * kRunStats, 0);
-    if (any_runs) {
-        const size_t r_sd = 0, r_work = align256(sd.size() * sizeof(StreamDesc));
-        const size_t r_ids = align256(r_work + work.size() * sizeof(CtaWork)), r_bytes = align256(r_ids + ids.size() * 4);
-        STZ_CUDA(ctx->h_stage.ensure(r_bytes));
-        uint8_t* hr = ctx->h_stage.as<uint8_t>();
-        std::memcpy(hr + r_sd, sd.data(), sd.size() * sizeof(StreamDesc));
-        std::memcpy(hr + r_work, work.data(), work.size() * sizeof(CtaWork));
-        std::memcpy(hr + r_ids, ids.data(), ids.size() * 4);
-        STZ_CUDA(ctx->work.ensure(r_bytes));
-        STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hr, r_bytes, cudaMemcpyHostToDevice, st));
-        STZ_CUDA(ctx->rstats.ensure(rstats.size() * 8));
-        STZ_CUDA(cudaMemsetAsync(ctx->rstats.p, 0, rstats.size() * 8, st));
-        const uint8_t* dw = ctx->work.as<uint8_t>();
-        {
-            KScope ks(ctx, "k_run_stats");
-            launch_run_stats((const CtaWork*)(dw + r_work), (const uint32_t*)(dw + r_ids), (int)work.size(),
-                             (const StreamDesc*)(dw + r_sd), ctx->codes.as<uint16_t>(),
-                             ctx->rstats.as<unsigned long long>(), st);
-        }
-        STZ_CUDA(cudaGetLastError());
-        STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
-        STZ_CUDA(cudaMemcpyAsync(ctx->h_rstats.p, ctx->rstats.p, rstats.size() * 8, cudaMemcpyDeviceToHost, st));
-    }
-    lap.mark("run slots + run stats launch");
+    lap.mark("run slots");
     // the plain codebooks while the device counts the run symbols
     ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
         const uint32_t* hw = h_out[s] ? fullh[s] : ctx->h_hist.as<uint32_t>() + s * (size_t)wn;
@@ -592,7 +620,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         build_codebook(hw, hn, hb, syms[s], lens[s]);
     });
     lap.mark("plain codebooks");
-    if (any_runs) {
+    if (rs_any) {
         STZ_CUDA(cudaStreamSynchronize(st));
         std::memcpy(rstats.data(), ctx->h_rstats.p, rstats.size() * 8);
     }
@@ -884,6 +912,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         delete so;
         STZ_FAIL(STZ_ERR_FORMAT, "internal: written stream does not parse: " + pe);
     }
+    lap.mark("parse check");
     *out = so;
     return STZ_OK;
 }

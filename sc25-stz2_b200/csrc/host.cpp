@@ -613,9 +613,21 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
     const int level = h_.zstd_level;
     const bool trace = std::getenv("STZ_TRACE") != nullptr;
     const auto t0 = std::chrono::steady_clock::now();
+    // trace: per group, when its first frame got past the wait and when its
+    // last frame was done (microseconds from the start)
+    std::vector<std::atomic<int64_t>> g_first(ngroups), g_last(ngroups), g_max(ngroups), g_zn(ngroups);
+    for (size_t i = 0; i < ngroups; ++i) g_first[i] = INT64_MAX, g_last[i] = 0, g_max[i] = 0, g_zn[i] = 0;
+    auto since = [&](std::chrono::steady_clock::time_point t) {
+        return (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(t - t0).count();
+    };
     pool_.parallel_for(order.size(), [&](size_t k) {
         wait_group(group_of[k]);
         const auto f0 = std::chrono::steady_clock::now();
+        if (trace) {
+            int64_t v = since(f0), cur = g_first[group_of[k]].load();
+            while (v < cur && !g_first[group_of[k]].compare_exchange_weak(cur, v)) {
+            }
+        }
         Frame& f = frames_[order[k]];
         f.raw = true;
         f.stored = f.n;
@@ -638,12 +650,29 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
                 f.out.reset();
             }
         }
-        if (trace)
-            busy_ns_ += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - f0)
-                            .count();
+        if (trace) {
+            const auto f1 = std::chrono::steady_clock::now();
+            busy_ns_ += std::chrono::duration_cast<std::chrono::nanoseconds>(f1 - f0).count();
+            int64_t v = since(f1), cur = g_last[group_of[k]].load();
+            while (v > cur && !g_last[group_of[k]].compare_exchange_weak(cur, v)) {
+            }
+            const int64_t d = (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(f1 - f0).count();
+            cur = g_max[group_of[k]].load();
+            while (d > cur && !g_max[group_of[k]].compare_exchange_weak(cur, d)) {
+            }
+            if (!f.raw) ++g_zn[group_of[k]];
+        }
     });
-    if (trace)
+    if (trace) {
         wall_ns_ += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
+        for (size_t i = 0; i < ngroups; ++i)
+            if (g_last[i].load())
+                std::fprintf(stderr,
+                             "[stz] zstd group %zu: first frame at %.3f ms, last done at %.3f ms, longest frame "
+                             "%.3f ms, %lld of %zu frames compressed\n",
+                             i, g_first[i].load() / 1e3, g_last[i].load() / 1e3, g_max[i].load() / 1e3,
+                             (long long)g_zn[i].load(), by_group[i].size());
+    }
 }
 
 Bytes ContainerWriter::finish(const void* coarsest, const std::vector<LevelDir>& levels)

@@ -228,6 +228,18 @@ struct stz_context {
     }
     void flush_prof()
     {
+        // STZ_TIMELINE: every bracketed launch of this flush with its start and
+        // end relative to the first one's start (events of all the context's
+        // streams share the device clock).
+        static const bool timeline = std::getenv("STZ_TIMELINE") != nullptr;
+        if (timeline && !pending.empty() && cudaEventSynchronize(pending.back().b) == cudaSuccess)
+            for (auto& r : pending) {
+                float t0 = 0.f, t1 = 0.f;
+                if (cudaEventSynchronize(r.b) == cudaSuccess &&
+                    cudaEventElapsedTime(&t0, pending[0].a, r.a) == cudaSuccess &&
+                    cudaEventElapsedTime(&t1, pending[0].a, r.b) == cudaSuccess)
+                    std::fprintf(stderr, "[stz] timeline %-28s %9.4f %9.4f %8.4f\n", r.name, t0, t1, t1 - t0);
+            }
         for (auto& r : pending) {
             float ms = 0.f;
             if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess)
