@@ -195,6 +195,8 @@ void add_all_chunks(std::vector<CtaWork>& work, std::vector<uint32_t>& ids, uint
 int pool_threads(int requested)
 {
     if (requested > 0) return requested;
+    if (const char* e = std::getenv("STZ_POOL_THREADS"))
+        if (std::atoi(e) > 0) return std::min(std::atoi(e), 64);
     const unsigned h = std::thread::hardware_concurrency();
     return (int)std::max(1u, std::min(h ? h : 1u, 64u));
 }
@@ -771,7 +773,10 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     // copies run on the context's copy stream, so group gi's copy overlaps
     // group gi + 1's encode.
     ev.e.assign(2 * ngroups + 1, nullptr);
-    for (auto& x : ev.e) STZ_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    // the pool's threads wait on the copy events ev.e[0, ngroups) while others
+    // compress frames: those waits block instead of spinning on a core
+    for (size_t i = 0; i < ev.e.size(); ++i)
+        STZ_CUDA(cudaEventCreateWithFlags(&ev.e[i], cudaEventDisableTiming | (i < ngroups ? cudaEventBlockingSync : 0)));
     STZ_CUDA(cudaEventRecord(ev.e[2 * ngroups], st));
     std::vector<CtaWork> gwork;
     std::vector<uint32_t> gids;
@@ -797,12 +802,20 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(ctx->gwork.p, ctx->h_meta2.p, g_bytes, cudaMemcpyHostToDevice, st));
     const CtaWork* d_gwork = (const CtaWork*)(ctx->gwork.as<uint8_t>() + g_work);
     const uint32_t* d_gids = (const uint32_t*)(ctx->gwork.as<uint8_t>() + g_ids);
+    // the coarser levels' streams (group 0) are many small ones: packed back
+    // to back on the device, they go to the host in one transfer
+    if (fin0 > 0) STZ_CUDA(ctx->packed.ensure(sd[fin0].word_base * 4));
     for (size_t gi = 0; gi < ngroups; ++gi) {
         {
             KScope ks(ctx, "k_encode");
             launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
                           ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
                           ctx->payload.as<uint32_t>(), st);
+        }
+        if (gi == 0 && fin0 > 0) {
+            KScope ks(ctx, "k_pack_streams");
+            launch_pack_streams(d_sd, ctx->stream_words.as<uint64_t>(), 0, fin0, ctx->payload.as<uint32_t>(),
+                                ctx->packed.as<uint32_t>(), st);
         }
         STZ_CUDA(cudaEventRecord(ev.e[ngroups + gi], st));
     }
@@ -838,6 +851,14 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     for (size_t gi = 0; gi < ngroups; ++gi) {
         STZ_CUDA(cudaStreamWaitEvent(ctx->st_copy, ev.e[ngroups + gi], 0));
+        if (gi == 0 && fin0 > 0) {  // packed on the device, at the start of the host payload
+            const uint64_t n0 = meta[nstreams + fin0];
+            if (n0)
+                STZ_CUDA(cudaMemcpyAsync(ctx->h_payload.as<uint32_t>(), ctx->packed.p, n0 * 4, cudaMemcpyDeviceToHost,
+                                         ctx->st_copy));
+            STZ_CUDA(cudaEventRecord(ev.e[gi], ctx->st_copy));
+            continue;
+        }
         // the group's words straight from the stream buffers to their place in
         // the packed host payload (one copy per piece)
         for (const Piece& pc : pieces[gi])
@@ -884,6 +905,11 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     lap.mark("stream headers");
     ContainerWriter cw(h, parts, *ctx->pool);
     std::atomic<int> ev_err{0};
+    // a group's copy seen complete once: later frames of the group make no
+    // CUDA call (concurrent calls from the pool's threads serialize in the
+    // driver, and frames queued behind a finished copy waited on each other)
+    std::unique_ptr<std::atomic<int>[]> copied(new std::atomic<int>[ngroups]);
+    for (size_t i = 0; i < ngroups; ++i) copied[i].store(0);
     // zstd groups: every stream header first (nothing to wait for), then
     // the payload of encode group g after its copy (event g)
     cw.compress_groups(
@@ -894,7 +920,9 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             return 2 + (size_t)(layer / lpg);
         },
         [&](size_t g) {
-            if (g > 0 && cudaEventSynchronize(ev.e[g - 1]) != cudaSuccess) ev_err = 1;
+            if (g == 0 || copied[g - 1].load(std::memory_order_acquire)) return;
+            if (cudaEventSynchronize(ev.e[g - 1]) != cudaSuccess) ev_err = 1;
+            copied[g - 1].store(1, std::memory_order_release);
         });
     if (ev_err) {  // reports the device error
         STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));

@@ -620,9 +620,12 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
     auto since = [&](std::chrono::steady_clock::time_point t) {
         return (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(t - t0).count();
     };
+    std::vector<int64_t> j_take(trace ? order.size() : 0), j_go(j_take.size()), j_end(j_take.size());
     pool_.parallel_for(order.size(), [&](size_t k) {
+        if (trace) j_take[k] = since(std::chrono::steady_clock::now());
         wait_group(group_of[k]);
         const auto f0 = std::chrono::steady_clock::now();
+        if (trace) j_go[k] = since(f0);
         if (trace) {
             int64_t v = since(f0), cur = g_first[group_of[k]].load();
             while (v < cur && !g_first[group_of[k]].compare_exchange_weak(cur, v)) {
@@ -661,6 +664,7 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
             while (d > cur && !g_max[group_of[k]].compare_exchange_weak(cur, d)) {
             }
             if (!f.raw) ++g_zn[group_of[k]];
+            j_end[k] = since(f1);
         }
     });
     if (trace) {
@@ -672,6 +676,11 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
                              "%.3f ms, %lld of %zu frames compressed\n",
                              i, g_first[i].load() / 1e3, g_last[i].load() / 1e3, g_max[i].load() / 1e3,
                              (long long)g_zn[i].load(), by_group[i].size());
+        if (std::getenv("STZ_TRACE_JOBS"))
+            for (size_t k = 0; k < order.size(); ++k)
+                std::fprintf(stderr, "[stz] job %zu group %zu bytes %zu taken %lld started %lld done %lld us\n", k,
+                             group_of[k], frames_[order[k]].n, (long long)j_take[k], (long long)j_go[k],
+                             (long long)j_end[k]);
     }
 }
 

@@ -1070,22 +1070,23 @@ __global__ void __launch_bounds__(1024) k_unpred_scatter_dyn(const uint8_t* __re
         unpred_move_one<T, false>(work[wi], sd, codes, dense, list, wc);
 }
 
-__global__ void k_pack_payload(const uint32_t* __restrict__ src, const uint64_t* __restrict__ src_base,
-                               const uint64_t* __restrict__ dst_base, const uint64_t* __restrict__ count,
-                               uint32_t* __restrict__ dst)
+__global__ void k_pack_streams(const StreamDesc* __restrict__ sd, const uint64_t* __restrict__ stream_words, int s0,
+                               const uint32_t* __restrict__ payload, uint32_t* __restrict__ dst)
 {
-    const int s = blockIdx.y;
-    const uint64_t n = count[s], a = src_base[s], b = dst_base[s];
+    const int s = s0 + (int)blockIdx.y;
+    uint64_t b = 0;  // words of the streams before s in this group
+    for (int i = s0; i < s; ++i) b += stream_words[i];
+    const uint64_t n = stream_words[s], a = sd[s].word_base;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        dst[b + i] = src[a + i];
+        dst[b + i] = payload[a + i];
 }
 
 }  // namespace
 
-void launch_pack_payload(const uint32_t* src, const uint64_t* src_base, const uint64_t* dst_base,
-                         const uint64_t* count, int nstreams, uint32_t* dst, cudaStream_t st)
+void launch_pack_streams(const StreamDesc* sd, const uint64_t* stream_words, int s0, int s1, const uint32_t* payload,
+                         uint32_t* dst, cudaStream_t st)
 {
-    if (nstreams) k_pack_payload<<<dim3(64, nstreams), 256, 0, st>>>(src, src_base, dst_base, count, dst);
+    if (s1 > s0) k_pack_streams<<<dim3(16, s1 - s0), 256, 0, st>>>(sd, stream_words, s0, payload, dst);
 }
 
 void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,

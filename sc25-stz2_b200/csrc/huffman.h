@@ -50,9 +50,11 @@ size_t decode_tables_bytes();
 uint32_t decode_seq_bits();
 void launch_build_tables(const StreamDesc* sd, int nstreams, const uint16_t* cb_sym, const uint8_t* cb_len,
                          void* tables, cudaStream_t st);
-// Copy each stream's used payload words into one contiguous buffer.
-void launch_pack_payload(const uint32_t* src, const uint64_t* src_base, const uint64_t* dst_base,
-                         const uint64_t* count, int nstreams, uint32_t* dst, cudaStream_t st);
+// The payload words of streams [s0, s1) back to back in stream order into dst
+// (each stream's count from stream_words, as k_scan_stream leaves it), so a
+// group of small streams goes to the host in one transfer.
+void launch_pack_streams(const StreamDesc* sd, const uint64_t* stream_words, int s0, int s1, const uint32_t* payload,
+                         uint32_t* dst, cudaStream_t st);
 template <typename T>
 void launch_unpred_move(bool gather, const UnpredWork* work, int nwork, const StreamDesc* sd, const uint16_t* codes,
                         T* dense, T* list, cudaStream_t st);
