@@ -718,10 +718,15 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         KScope ks(ctx, "k_expand_codebook");
         launch_expand_codebook(d_sd, nstreams, d_sym, d_len, ctx->ctab.as<uint32_t>(), st);
     }
+    STZ_CUDA(ctx->rbits.ensure((size_t)nstreams * kRunBitsStride));
+    {
+        KScope ks(ctx, "k_run_bits");
+        launch_run_bits(d_sd, nstreams, ctx->ctab.as<uint32_t>(), ctx->rbits.as<uint8_t>(), st);
+    }
     {
         KScope ks(ctx, "k_sub_bits");
         launch_sub_bits(d_work, d_ids, (int)work.size(), d_sd, ctx->codes.as<uint16_t>(), ctx->ctab.as<uint32_t>(),
-                        ctx->sub_bits.as<uint32_t>(), st);
+                        ctx->rbits.as<uint8_t>(), ctx->sub_bits.as<uint32_t>(), st);
     }
     {
         KScope ks(ctx, "k_scan_stream");
@@ -809,8 +814,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         {
             KScope ks(ctx, "k_encode");
             launch_encode(d_gwork + gw[gi], d_gids, (int)(gw[gi + 1] - gw[gi]), d_sd, ctx->codes.as<uint16_t>(),
-                          ctx->ctab.as<uint32_t>(), ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(),
-                          ctx->payload.as<uint32_t>(), st);
+                          ctx->ctab.as<uint32_t>(), ctx->rbits.as<uint8_t>(), ctx->sub_bits.as<uint32_t>(),
+                          ctx->sub_off.as<uint32_t>(), ctx->chunk_off.as<uint64_t>(), ctx->payload.as<uint32_t>(), st);
         }
         if (gi == 0 && fin0 > 0) {
             KScope ks(ctx, "k_pack_streams");

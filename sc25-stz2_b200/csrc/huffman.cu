@@ -277,6 +277,77 @@ struct RunLane {
     const bool active = p < (nplanes);                                 \
     const uint32_t pe = active ? p : base_
 
+// ---- literal lists: the symbols of a run-coded plane in warp-wide rounds ----
+// A lane's literals vary in number from lane to lane, so a walk over each
+// lane's own literals leaves most of the warp idle. Instead the group first
+// lists the plane's literal positions in plane order in shared memory (a
+// group scan of the lanes' literal counts places each lane's), then visits
+// them in rounds of W: literal k (lane k mod W) with the run of centre codes
+// before it (the gap to literal k - 1), then the run after the last literal.
+// That is the symbol order of a sequential pass over the plane. Used where a
+// lane holds at most 32 codes (planes of up to 1024 codes).
+constexpr uint32_t kListPerWarp = 1024;  // list entries per warp: 32 / W groups of at most 32 W codes
+constexpr uint32_t kStagePerWarp = 832;  // staging words per warp: groups of at most (32 W * 24 + 63) / 32
+
+__device__ __forceinline__ bool lits_ok(uint32_t P, uint32_t W) { return (P + W - 1) / W <= 32; }
+
+// The group's literal positions into list[0, L) in plane order; returns L.
+__device__ __forceinline__ uint32_t plane_literals(const uint16_t* __restrict__ src, const LaneSeg& g, uint32_t R,
+                                                   uint16_t* list)
+{
+    const uint32_t n = g.b - g.a;
+    const uint32_t m = n ? literal_mask(src, g, g.a, n, R) : 0u;
+    const uint32_t c = __popc(m);
+    const uint32_t incl = group_scan(c, g.W, g.lane);
+    const uint32_t L = __shfl_sync(0xffffffffu, incl, g.W - 1, g.W);
+    uint32_t j = incl - c;
+    for (uint32_t mm = m; mm; mm &= mm - 1) list[j++] = (uint16_t)(g.a + (__ffs(mm) - 1));
+    __syncwarp();
+    return L;
+}
+
+// Rounds over the group's literals with a warp-uniform trip count (every lane
+// takes part in the shuffles f may make): f(valid, pos, run).
+template <class F>
+__device__ __forceinline__ void literal_rounds(const uint16_t* list, uint32_t L, const LaneSeg& g, F&& f)
+{
+    const uint32_t rounds = __reduce_max_sync(0xffffffffu, (L + g.W - 1) / g.W);
+    for (uint32_t t = 0; t < rounds; ++t) {
+        const uint32_t k = t * g.W + g.lane;
+        const bool valid = k < L;
+        uint32_t pos = 0, run = 0;
+        if (valid) {
+            pos = list[k];
+            run = pos - (k ? list[k - 1] + 1u : 0u);
+        }
+        f(valid, pos, run);
+    }
+}
+
+// Centre codes after the plane's last literal.
+__device__ __forceinline__ uint32_t tail_run(const uint16_t* list, uint32_t L, uint32_t P)
+{
+    return P - (L ? list[L - 1] + 1u : 0u);
+}
+
+// Bits of the run symbols of a run of r centre codes (r <= P), per stream:
+// rb[r], r = 0 .. kRunBitsStride - 1 (planes of up to 1024 codes).
+__global__ void k_run_bits(const StreamDesc* __restrict__ sd, const uint32_t* __restrict__ ctab,
+                           uint8_t* __restrict__ rbits)
+{
+    const StreamDesc s = sd[blockIdx.x];
+    const uint32_t P = s.C * s.C;
+    if (s.run_n == 0 || P >= kRunBitsStride) return;
+    const uint32_t* tab = ctab + (size_t)blockIdx.x * 2 * s.radius;
+    uint32_t D, LD;
+    const uint32_t J = run_geometry(P, D, LD);
+    for (uint32_t r = threadIdx.x; r <= P; r += blockDim.x) {
+        uint32_t b = 0;
+        run_symbols(r, s.radius, s.run_base, J, D, LD, [&](uint32_t sym) { b += __ldg(tab + sym) & 31u; });
+        rbits[(size_t)blockIdx.x * kRunBitsStride + r] = (uint8_t)b;
+    }
+}
+
 // Run-symbol counts of every listed plane (streams with runs).
 __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __restrict__ work,
                                                             const uint32_t* __restrict__ chunk_ids,
@@ -292,18 +363,39 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
     __syncthreads();
     const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     uint32_t singles = 0;
-    STZ_GROUP_PLANES(np, W)
-    {
-        STZ_GROUP_PLANE(np, W);
-        const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
-        const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
-        const LaneSeg g = lane_seg(C, src, W, active);
-        RunLane rl;
-        rl.init(src, g, s.radius);
-        rl.symbols(src, g, s, [&](uint32_t sym) {
-            if (sym == s.radius) ++singles;
-            else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
-        });
+    auto count = [&](uint32_t sym) {
+        if (sym == s.radius) ++singles;
+        else if (sym - s.run_base < s.run_n) atomicAdd(&cnt[sym - s.run_base + 1], 1u);
+    };
+    if (lits_ok(P, W)) {
+        __shared__ uint16_t lists[kLaneThreads / 32][kListPerWarp];
+        uint16_t* list = lists[threadIdx.x >> 5] + ((threadIdx.x & 31) / W) * 32 * W;
+        uint32_t D, LD;
+        const uint32_t J = run_geometry(P, D, LD);
+        STZ_GROUP_PLANES(np, W)
+        {
+            STZ_GROUP_PLANE(np, W);
+            const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
+            const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+            const LaneSeg g = lane_seg(C, src, W, active);
+            const uint32_t L = plane_literals(src, g, s.radius, list);
+            literal_rounds(list, L, g, [&](bool valid, uint32_t, uint32_t run) {
+                if (valid && run) run_symbols(run, s.radius, s.run_base, J, D, LD, count);
+            });
+            if (active && g.lane == 0) run_symbols(tail_run(list, L, P), s.radius, s.run_base, J, D, LD, count);
+            __syncwarp();  // the list is rewritten for the next plane
+        }
+    } else {
+        STZ_GROUP_PLANES(np, W)
+        {
+            STZ_GROUP_PLANE(np, W);
+            const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
+            const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+            const LaneSeg g = lane_seg(C, src, W, active);
+            RunLane rl;
+            rl.init(src, g, s.radius);
+            rl.symbols(src, g, s, count);
+        }
     }
     singles = group_sum(singles, 32);
     if ((threadIdx.x & 31) == 0 && singles) atomicAdd(&cnt[0], singles);
@@ -318,12 +410,35 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
                                                            const StreamDesc* __restrict__ sd,
                                                            const uint16_t* __restrict__ codes,
                                                            const uint32_t* __restrict__ ctab,
+                                                           const uint8_t* __restrict__ rbits,
                                                            uint32_t* __restrict__ sub_bits)
 {
     const CtaWork w = work[blockIdx.x];
     const StreamDesc s = sd[w.stream];
     const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
+    if (s.run_n && lits_ok(P, W)) {
+        __shared__ uint16_t lists[kLaneThreads / 32][kListPerWarp];
+        uint16_t* list = lists[threadIdx.x >> 5] + ((threadIdx.x & 31) / W) * 32 * W;
+        const uint8_t* rb = rbits + (size_t)w.stream * kRunBitsStride;
+        STZ_GROUP_PLANES(np, W)
+        {
+            STZ_GROUP_PLANE(np, W);
+            const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
+            const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+            const LaneSeg g = lane_seg(C, src, W, active);
+            const uint32_t L = plane_literals(src, g, s.radius, list);
+            uint32_t bits = 0;
+            literal_rounds(list, L, g, [&](bool valid, uint32_t pos, uint32_t run) {
+                if (valid) bits += __ldg(rb + run) + (__ldg(tab + __ldg(src + pos)) & 31u);
+            });
+            if (active && g.lane == 0) bits += __ldg(rb + tail_run(list, L, P));
+            bits = group_sum(bits, W);
+            if (active && g.lane == 0) sub_bits[s.sub_base + (size_t)c * C + lz] = bits;
+            __syncwarp();  // the list is rewritten for the next plane
+        }
+        return;
+    }
     STZ_GROUP_PLANES(np, W)
     {
         STZ_GROUP_PLANE(np, W);
@@ -441,6 +556,8 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
                                                          const StreamDesc* __restrict__ sd,
                                                          const uint16_t* __restrict__ codes,
                                                          const uint32_t* __restrict__ ctab,
+                                                         const uint8_t* __restrict__ rbits,
+                                                         const uint32_t* __restrict__ sub_bits,
                                                          const uint32_t* __restrict__ sub_off,
                                                          const uint64_t* __restrict__ chunk_word_off,
                                                          uint32_t* __restrict__ payload)
@@ -449,6 +566,75 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
     const StreamDesc s = sd[w.stream];
     const uint32_t C = s.C, P = C * C, W = lanes_per_plane(P), np = w.count * C;
     const uint32_t* tab = ctab + (size_t)w.stream * 2 * s.radius;
+    if (s.run_n && lits_ok(P, W)) {
+        // literal rounds: each literal's bits (its run's, then its own) placed
+        // by a group scan, written into a shared staging copy of the plane's
+        // words aligned as in the chunk; then the inner words are stored and
+        // the first and last (shared with the neighbouring planes) merged
+        __shared__ uint16_t lists[kLaneThreads / 32][kListPerWarp];
+        __shared__ uint32_t stage[kLaneThreads / 32][kStagePerWarp];
+        const uint32_t gi = (threadIdx.x & 31) / W;
+        uint16_t* list = lists[threadIdx.x >> 5] + gi * 32 * W;
+        uint32_t* stg = stage[threadIdx.x >> 5] + gi * (24 * W + 2);
+        const uint8_t* rb = rbits + (size_t)w.stream * kRunBitsStride;
+        uint32_t D, LD;
+        const uint32_t J = run_geometry(P, D, LD);
+        auto put = [&](uint32_t e, uint32_t& p) {  // e = code << 5 | length, MSB first at bit p
+            const uint32_t l = e & 31u, v = e >> 5, o = p & 31u, wi = p >> 5;
+            if (!l) return;
+            if (o + l <= 32) {
+                atomicOr(stg + wi, v << (32 - o - l));
+            } else {
+                atomicOr(stg + wi, v >> (o + l - 32));
+                atomicOr(stg + wi + 1, v << (64 - o - l));
+            }
+            p += l;
+        };
+        STZ_GROUP_PLANES(np, W)
+        {
+            STZ_GROUP_PLANE(np, W);
+            const uint32_t c = chunk_ids[w.first + pe / C], lz = pe % C;
+            const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
+            const LaneSeg g = lane_seg(C, src, W, active);
+            const uint32_t L = plane_literals(src, g, s.radius, list);
+            const size_t k = s.sub_base + (size_t)c * C + lz;
+            const uint32_t b0 = sub_off[k], nb = active ? sub_bits[k] : 0u;
+            const uint32_t nw = ((b0 & 31u) + nb + 31u) >> 5;
+            for (uint32_t x = g.lane; x < nw; x += W) stg[x] = 0;
+            __syncwarp();
+            uint32_t at = b0 & 31u;  // the group's next bit in the staging words
+            literal_rounds(list, L, g, [&](bool valid, uint32_t pos, uint32_t run) {
+                uint32_t ec = 0, len = 0;
+                if (valid) {
+                    ec = __ldg(tab + __ldg(src + pos));
+                    len = __ldg(rb + run) + (ec & 31u);
+                }
+                const uint32_t incl = group_scan(len, W, g.lane);
+                uint32_t p = at + incl - len;
+                at += __shfl_sync(0xffffffffu, incl, W - 1, W);
+                if (valid) {
+                    run_symbols(run, s.radius, s.run_base, J, D, LD, [&](uint32_t sym) { put(__ldg(tab + sym), p); });
+                    put(ec, p);
+                }
+            });
+            if (active && g.lane == 0) {
+                uint32_t p = at;
+                run_symbols(tail_run(list, L, P), s.radius, s.run_base, J, D, LD,
+                            [&](uint32_t sym) { put(__ldg(tab + sym), p); });
+            }
+            __syncwarp();
+            if (active && nb) {
+                uint32_t* out = payload + s.word_base + chunk_word_off[s.chunk_base + c] + (b0 >> 5);
+                for (uint32_t x = g.lane; x < nw; x += W) {
+                    const uint32_t v = stg[x];
+                    if (x == 0 || x == nw - 1) atomicOr(out + x, v);
+                    else out[x] = v;
+                }
+            }
+            __syncwarp();  // list and staging are rewritten for the next plane
+        }
+        return;
+    }
     STZ_GROUP_PLANES(np, W)
     {
         STZ_GROUP_PLANE(np, W);
@@ -1101,10 +1287,18 @@ void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork,
     if (nwork > 0) k_run_stats<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, stats);
 }
 
-void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                     const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st)
+void launch_run_bits(const StreamDesc* sd, int nstreams, const uint32_t* ctab, uint8_t* rbits, cudaStream_t st)
 {
-    if (nwork) k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_bits);
+    if (nstreams) k_run_bits<<<nstreams, 256, 0, st>>>(sd, ctab, rbits);
+}
+
+void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
+                     const uint16_t* codes, const uint32_t* ctab, const uint8_t* rbits, uint32_t* sub_bits,
+                     cudaStream_t st)
+{
+    if (nwork)
+        k_sub_bits<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, rbits,
+                                                                        sub_bits);
 }
 
 void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks, const uint32_t* sub_bits,
@@ -1117,11 +1311,12 @@ void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks
 }
 
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
-                   uint32_t* payload, cudaStream_t st)
+                   const uint16_t* codes, const uint32_t* ctab, const uint8_t* rbits, const uint32_t* sub_bits,
+                   const uint32_t* sub_off, const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st)
 {
     if (nwork)
-        k_encode<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, sub_off, chunk_word_off, payload);
+        k_encode<<<dim3(nwork, kPlaneSlices), kLaneThreads, 0, st>>>(work, chunk_ids, sd, codes, ctab, rbits, sub_bits,
+                                                                      sub_off, chunk_word_off, payload);
 }
 
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,

@@ -24,10 +24,18 @@ void launch_expand_codebook(const StreamDesc* sd, int nstreams, const uint16_t* 
 // gets the centre codes left as single symbols, stats[s * kRunStats + 1 + i]
 // the uses of run slot i. stats must be zeroed.
 constexpr int kRunStats = 64;
+// Per stream: the bits of a run of r centre codes, r < kRunBitsStride
+// (launch_run_bits; planes of up to 1024 codes).
+constexpr uint32_t kRunBitsStride = 1025;
 void launch_run_stats(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                       const uint16_t* codes, unsigned long long* stats, cudaStream_t st);
+// Bits of a run of r centre codes per stream (rbits: nstreams x
+// kRunBitsStride bytes), from the stream's code table (after
+// launch_expand_codebook); streams with runs and planes of up to 1024 codes.
+void launch_run_bits(const StreamDesc* sd, int nstreams, const uint32_t* ctab, uint8_t* rbits, cudaStream_t st);
 void launch_sub_bits(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                     const uint16_t* codes, const uint32_t* ctab, uint32_t* sub_bits, cudaStream_t st);
+                     const uint16_t* codes, const uint32_t* ctab, const uint8_t* rbits, uint32_t* sub_bits,
+                     cudaStream_t st);
 // Plane bit offsets, chunk word offsets and stream word counts from the
 // plane bit counts; clears every plane's boundary words (max_chunks: the
 // most chunks of any stream).
@@ -35,8 +43,8 @@ void launch_scan_streams(const StreamDesc* sd, int nstreams, uint32_t max_chunks
                          uint32_t* sub_off, uint64_t* chunk_word_off, uint64_t* stream_words, uint32_t* payload,
                          cudaStream_t st);
 void launch_encode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
-                   const uint16_t* codes, const uint32_t* ctab, const uint32_t* sub_off, const uint64_t* chunk_word_off,
-                   uint32_t* payload, cudaStream_t st);
+                   const uint16_t* codes, const uint32_t* ctab, const uint8_t* rbits, const uint32_t* sub_bits,
+                   const uint32_t* sub_off, const uint64_t* chunk_word_off, uint32_t* payload, cudaStream_t st);
 void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, const StreamDesc* sd,
                    const uint16_t* cb_sym, const void* tables, const uint32_t* sub_off, const uint64_t* chunk_word_off,
                    const uint32_t* payload, uint16_t* codes, cudaStream_t st);
