@@ -436,44 +436,6 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(ctx->h_small.ensure(64 + n0 * elem));
     STZ_CUDA(cudaMemcpyAsync(ctx->h_small.as<uint8_t>() + 64, ctx->grid[cur].p, n0 * elem, cudaMemcpyDeviceToHost, st));
 
-    std::vector<StreamDesc> sd = g.sd;
-    // work list over every chunk of every stream
-    std::vector<CtaWork> work;
-    std::vector<uint32_t> ids;
-    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
-    // Run statistics of every stream whose planes can take run symbols: one
-    // pass over the codes right after the level encodes, while the histograms
-    // go to the host. The counts per run class depend only on the plane size
-    // and the codes, not on which free code values the stream's run symbols
-    // later take; here they are numbered from R2, above every code, so no
-    // literal is taken for one. Work list and counters are set up now.
-    std::vector<unsigned long long> rstats((size_t)nstreams * kRunStats, 0);
-    bool rs_any = false;
-    size_t r_sd = 0, r_work = 0, r_ids = 0;
-    {
-        std::vector<StreamDesc> rsd = sd;
-        for (auto& d : rsd) {
-            d.run_n = run_slot_count(d.C * d.C);
-            d.run_base = (uint32_t)R2;
-            rs_any = rs_any || d.run_n;
-        }
-        if (rs_any) {
-            r_work = align256(rsd.size() * sizeof(StreamDesc));
-            r_ids = align256(r_work + work.size() * sizeof(CtaWork));
-            const size_t r_bytes = align256(r_ids + ids.size() * 4);
-            STZ_CUDA(ctx->h_stage.ensure(r_bytes));
-            uint8_t* hr = ctx->h_stage.as<uint8_t>();
-            std::memcpy(hr + r_sd, rsd.data(), rsd.size() * sizeof(StreamDesc));
-            std::memcpy(hr + r_work, work.data(), work.size() * sizeof(CtaWork));
-            std::memcpy(hr + r_ids, ids.data(), ids.size() * 4);
-            STZ_CUDA(ctx->work.ensure(r_bytes));
-            STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hr, r_bytes, cudaMemcpyHostToDevice, st));
-            STZ_CUDA(ctx->rstats.ensure(rstats.size() * 8));
-            STZ_CUDA(cudaMemsetAsync(ctx->rstats.p, 0, rstats.size() * 8, st));
-            STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
-        }
-    }
-
     // learned models of levels K-1 (record 0) and K (record 1) on the device
     const stz_model* M = o.model;
     std::vector<uint32_t> lflags(K + 1, 0);
@@ -538,6 +500,47 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     }
     STZ_CUDA(cudaGetLastError());
 
+    std::vector<StreamDesc> sd = g.sd;
+    // work list over every chunk of every stream
+    std::vector<CtaWork> work;
+    std::vector<uint32_t> ids;
+    for (int s = 0; s < nstreams; ++s) add_all_chunks(work, ids, (uint32_t)s, sd[s].nchunks, (int)sd[s].C);
+    // Run statistics of every stream whose planes can take run symbols: one
+    // pass over the codes right after the level encodes, while the histograms
+    // go to the host. The counts per run class depend only on the plane size
+    // and the codes, not on which free code values the stream's run symbols
+    // later take; here they are numbered from R2, above every code, so no
+    // literal is taken for one. Work list and counters go up on the copy
+    // stream while the device runs the levels.
+    std::vector<unsigned long long> rstats((size_t)nstreams * kRunStats, 0);
+    bool rs_any = false;
+    size_t r_sd = 0, r_work = 0, r_ids = 0;
+    cudaEvent_t ev_up = ctx->event();
+    {
+        std::vector<StreamDesc> rsd = sd;
+        for (auto& d : rsd) {
+            d.run_n = run_slot_count(d.C * d.C);
+            d.run_base = (uint32_t)R2;
+            rs_any = rs_any || d.run_n;
+        }
+        if (rs_any) {
+            r_work = align256(rsd.size() * sizeof(StreamDesc));
+            r_ids = align256(r_work + work.size() * sizeof(CtaWork));
+            const size_t r_bytes = align256(r_ids + ids.size() * 4);
+            STZ_CUDA(ctx->h_stage.ensure(r_bytes));
+            uint8_t* hr = ctx->h_stage.as<uint8_t>();
+            std::memcpy(hr + r_sd, rsd.data(), rsd.size() * sizeof(StreamDesc));
+            std::memcpy(hr + r_work, work.data(), work.size() * sizeof(CtaWork));
+            std::memcpy(hr + r_ids, ids.data(), ids.size() * 4);
+            STZ_CUDA(ctx->work.ensure(r_bytes));
+            STZ_CUDA(cudaMemcpyAsync(ctx->work.p, hr, r_bytes, cudaMemcpyHostToDevice, ctx->st_copy));
+            STZ_CUDA(ctx->rstats.ensure(rstats.size() * 8));
+            STZ_CUDA(cudaMemsetAsync(ctx->rstats.p, 0, rstats.size() * 8, ctx->st_copy));
+            STZ_CUDA(ctx->h_rstats.ensure(rstats.size() * 8));
+            STZ_CUDA(cudaEventRecord(ev_up, ctx->st_copy));
+        }
+    }
+
     // histogram windows + outside counts + unpred counts to the host, on the
     // copy stream, while ctx->st counts the run symbols
     const int wlo = std::max(0, o.radius - kHistWindow / 2);
@@ -557,6 +560,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     STZ_CUDA(cudaMemcpyAsync(h_ucnt, ctx->unpred_cnt.p, g.total_chunk_slots * 4, cudaMemcpyDeviceToHost, sc));
     STZ_CUDA(cudaEventRecord(ev_hist, sc));
     if (rs_any) {
+        STZ_CUDA(cudaStreamWaitEvent(st, ev_up, 0));
         const uint8_t* dw = ctx->work.as<uint8_t>();
         {
             KScope ks(ctx, "k_run_stats");
@@ -571,6 +575,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         const cudaError_t e = cudaEventSynchronize(ev_hist);
         ctx->ev_pool.push_back(ev_lv);
         ctx->ev_pool.push_back(ev_hist);
+        ctx->ev_pool.push_back(ev_up);
         STZ_CUDA(e);
     }
     std::vector<T> coarsest(n0);

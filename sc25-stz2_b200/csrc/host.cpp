@@ -198,9 +198,13 @@ int build_codebook_adjusted(const uint32_t* hist, int nbins, int base,
     sym.clear();
     len.clear();
     if (n == 0) return 0;
-    std::sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.w != y.w ? x.w < y.w : x.s < y.s; });
+    // (count, symbol) order as one 64-bit key per item (counts stay below
+    // 2^48), then (length, symbol) as one 32-bit key: plain integer sorts
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) key[i] = items[i].w << 16 | items[i].s;
+    std::sort(key.begin(), key.end());
     std::vector<uint64_t> a(n);
-    for (int i = 0; i < n; ++i) a[i] = items[i].w;
+    for (int i = 0; i < n; ++i) a[i] = key[i] >> 16;
     min_redundancy_lengths(a);
     if (n > 1) {
         const uint64_t cap = 1ull << kMaxCodeLen;
@@ -216,14 +220,14 @@ int build_codebook_adjusted(const uint32_t* hist, int nbins, int base,
             ++a[first_short];
         }
     }
-    std::vector<std::pair<uint8_t, uint16_t>> ls(n);
-    for (int i = 0; i < n; ++i) ls[i] = {(uint8_t)a[i], (uint16_t)items[i].s};
+    std::vector<uint32_t> ls(n);
+    for (int i = 0; i < n; ++i) ls[i] = (uint32_t)a[i] << 16 | (uint32_t)(key[i] & 0xffffu);
     std::sort(ls.begin(), ls.end());
     sym.resize(n);
     len.resize(n);
     for (int i = 0; i < n; ++i) {
-        len[i] = ls[i].first;
-        sym[i] = ls[i].second;
+        len[i] = (uint8_t)(ls[i] >> 16);
+        sym[i] = (uint16_t)(ls[i] & 0xffffu);
     }
     return n;
 }

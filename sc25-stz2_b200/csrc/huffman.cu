@@ -324,6 +324,28 @@ __device__ __forceinline__ void literal_rounds(const uint16_t* list, uint32_t L,
     }
 }
 
+// The same, two consecutive literals per lane per round (2 lane, 2 lane + 1
+// of the round's 2W): two independent load chains per lane.
+template <class F>
+__device__ __forceinline__ void literal_rounds2(const uint16_t* list, uint32_t L, const LaneSeg& g, F&& f)
+{
+    const uint32_t rounds = __reduce_max_sync(0xffffffffu, (L + 2 * g.W - 1) / (2 * g.W));
+    for (uint32_t t = 0; t < rounds; ++t) {
+        const uint32_t k = t * 2 * g.W + 2 * g.lane;
+        const bool v0 = k < L, v1 = k + 1 < L;
+        uint32_t pos0 = 0, run0 = 0, pos1 = 0, run1 = 0;
+        if (v0) {
+            pos0 = list[k];
+            run0 = pos0 - (k ? list[k - 1] + 1u : 0u);
+        }
+        if (v1) {
+            pos1 = list[k + 1];
+            run1 = pos1 - pos0 - 1u;
+        }
+        f(v0, pos0, run0, v1, pos1, run1);
+    }
+}
+
 // Centre codes after the plane's last literal.
 __device__ __forceinline__ uint32_t tail_run(const uint16_t* list, uint32_t L, uint32_t P)
 {
@@ -379,8 +401,9 @@ __global__ void __launch_bounds__(kLaneThreads) k_run_stats(const CtaWork* __res
             const uint16_t* src = codes + s.code_off + (size_t)c * P * C + (size_t)lz * P;
             const LaneSeg g = lane_seg(C, src, W, active);
             const uint32_t L = plane_literals(src, g, s.radius, list);
-            literal_rounds(list, L, g, [&](bool valid, uint32_t, uint32_t run) {
-                if (valid && run) run_symbols(run, s.radius, s.run_base, J, D, LD, count);
+            literal_rounds2(list, L, g, [&](bool v0, uint32_t, uint32_t run0, bool v1, uint32_t, uint32_t run1) {
+                if (v0 && run0) run_symbols(run0, s.radius, s.run_base, J, D, LD, count);
+                if (v1 && run1) run_symbols(run1, s.radius, s.run_base, J, D, LD, count);
             });
             if (active && g.lane == 0) run_symbols(tail_run(list, L, P), s.radius, s.run_base, J, D, LD, count);
             __syncwarp();  // the list is rewritten for the next plane
@@ -429,8 +452,10 @@ __global__ void __launch_bounds__(kLaneThreads) k_sub_bits(const CtaWork* __rest
             const LaneSeg g = lane_seg(C, src, W, active);
             const uint32_t L = plane_literals(src, g, s.radius, list);
             uint32_t bits = 0;
-            literal_rounds(list, L, g, [&](bool valid, uint32_t pos, uint32_t run) {
-                if (valid) bits += __ldg(rb + run) + (__ldg(tab + __ldg(src + pos)) & 31u);
+            literal_rounds2(list, L, g, [&](bool v0, uint32_t pos0, uint32_t run0, bool v1, uint32_t pos1, uint32_t run1) {
+                const uint32_t q0 = v0 ? __ldg(src + pos0) : 0u, q1 = v1 ? __ldg(src + pos1) : 0u;
+                if (v0) bits += __ldg(rb + run0) + (__ldg(tab + q0) & 31u);
+                if (v1) bits += __ldg(rb + run1) + (__ldg(tab + q1) & 31u);
             });
             if (active && g.lane == 0) bits += __ldg(rb + tail_run(list, L, P));
             bits = group_sum(bits, W);
@@ -534,15 +559,30 @@ __global__ void __launch_bounds__(1024) k_scan_stream(const StreamDesc* __restri
         stream_words[blockIdx.x] = carry;
     }
     __syncthreads();  // every chunk offset is written
+    // four planes per thread in flight (one block per stream: the loop is
+    // latency-bound)
     const uint64_t np = (uint64_t)s.nchunks * C;
-    for (uint64_t p = threadIdx.x; p < np; p += blockDim.x) {
-        const size_t k = s.sub_base + p;
-        const uint32_t b0 = sub_off[k], nb = sub_bits[k];
-        if (nb) {
-            uint32_t* w = payload + s.word_base + chunk_word_off[s.chunk_base + p / C];
-            w[b0 >> 5] = 0;
-            w[(b0 + nb - 1) >> 5] = 0;
+    for (uint64_t p0 = threadIdx.x; p0 < np; p0 += 4 * (uint64_t)blockDim.x) {
+        uint32_t b0[4], nb[4];
+        uint64_t cw[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint64_t p = p0 + (uint64_t)j * blockDim.x;
+            nb[j] = 0;
+            if (p < np) {
+                const size_t k = s.sub_base + p;
+                b0[j] = sub_off[k];
+                nb[j] = sub_bits[k];
+                cw[j] = chunk_word_off[s.chunk_base + p / C];
+            }
         }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (nb[j]) {
+                uint32_t* w = payload + s.word_base + cw[j];
+                w[b0[j] >> 5] = 0;
+                w[(b0[j] + nb[j] - 1) >> 5] = 0;
+            }
     }
 }
 
@@ -603,18 +643,29 @@ __global__ void __launch_bounds__(kLaneThreads) k_encode(const CtaWork* __restri
             for (uint32_t x = g.lane; x < nw; x += W) stg[x] = 0;
             __syncwarp();
             uint32_t at = b0 & 31u;  // the group's next bit in the staging words
-            literal_rounds(list, L, g, [&](bool valid, uint32_t pos, uint32_t run) {
-                uint32_t ec = 0, len = 0;
-                if (valid) {
-                    ec = __ldg(tab + __ldg(src + pos));
-                    len = __ldg(rb + run) + (ec & 31u);
+            literal_rounds2(list, L, g, [&](bool v0, uint32_t pos0, uint32_t run0, bool v1, uint32_t pos1, uint32_t run1) {
+                const uint32_t q0 = v0 ? __ldg(src + pos0) : 0u, q1 = v1 ? __ldg(src + pos1) : 0u;
+                uint32_t e0 = 0, e1 = 0, len0 = 0, len1 = 0;
+                if (v0) {
+                    e0 = __ldg(tab + q0);
+                    len0 = __ldg(rb + run0) + (e0 & 31u);
                 }
+                if (v1) {
+                    e1 = __ldg(tab + q1);
+                    len1 = __ldg(rb + run1) + (e1 & 31u);
+                }
+                const uint32_t len = len0 + len1;
                 const uint32_t incl = group_scan(len, W, g.lane);
                 uint32_t p = at + incl - len;
                 at += __shfl_sync(0xffffffffu, incl, W - 1, W);
-                if (valid) {
-                    run_symbols(run, s.radius, s.run_base, J, D, LD, [&](uint32_t sym) { put(__ldg(tab + sym), p); });
-                    put(ec, p);
+                auto sym_put = [&](uint32_t sym) { put(__ldg(tab + sym), p); };
+                if (v0) {
+                    run_symbols(run0, s.radius, s.run_base, J, D, LD, sym_put);
+                    put(e0, p);
+                }
+                if (v1) {
+                    run_symbols(run1, s.radius, s.run_base, J, D, LD, sym_put);
+                    put(e1, p);
                 }
             });
             if (active && g.lane == 0) {
