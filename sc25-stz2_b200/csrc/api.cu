@@ -1432,14 +1432,22 @@ struct DecodePipe {
         const ParsedStream& ps = s->dir;
         const bool last = bi + 1 == batches.size();
         const bool whole = B.l1 < 0 || B.l1 >= (int)ps.lv[kdec].s[0].layers;
-        const int s1 = whole ? B.s1 : B.s0;  // streams complete after this batch
-        int bricks_to = fin_done;
-        if (next_level == kdec && B.s0 == 7 * (kdec - 1) && fin_bricks && !last) {
-            const LevelGeom g = level_geom(ps, kdec);
-            level_decode_bricks(g, false, B.l1 * g.C, &bricks_to);
-        }
-        const bool finest_part = bricks_to > fin_done;
-        if ((next_level <= kdec && 7 * next_level <= s1) || finest_part) STZ_CUDA(record(sd, ctx->st));
+        // streams complete after this batch. The coarser levels of the first
+        // batch start after the second batch's entropy decode instead of
+        // beside it: its CTAs delayed theirs 3-4x, and the finest level's
+        // first bricks wait for both anyway (STZ_DECODE_DEFER=0: beside it)
+        static const bool defer = [] {
+            const char* e = std::getenv("STZ_DECODE_DEFER");
+            return !e || std::atoi(e) != 0;
+        }();
+        const int s1 = defer && bi == 0 && batches.size() > 1 ? 0 : whole ? B.s1 : B.s0;
+        bool waited = false;  // ctx->st waits for this batch's entropy decode
+        auto wait_decode = [&]() -> cudaError_t {
+            if (waited) return cudaSuccess;
+            waited = true;
+            return record(sd, ctx->st);
+        };
+        if (next_level < kdec && 7 * next_level <= s1) STZ_CUDA(wait_decode());
         for (; next_level < kdec && 7 * next_level <= s1; ++next_level) {
             const LevelDecodeArgs<T> a = level_args(next_level);
             {
@@ -1449,6 +1457,13 @@ struct DecodePipe {
             coarse = a.out;
             cur = 1 - cur;
         }
+        int bricks_to = fin_done;
+        if (next_level == kdec && B.s0 == 7 * (kdec - 1) && fin_bricks && !last) {
+            const LevelGeom g = level_geom(ps, kdec);
+            level_decode_bricks(g, false, B.l1 * g.C, &bricks_to);
+        }
+        const bool finest_part = bricks_to > fin_done;
+        if ((next_level == kdec && 7 * kdec <= s1) || finest_part) STZ_CUDA(wait_decode());
         if (next_level == kdec) {
             LevelDecodeArgs<T> a = level_args(kdec);
             const char* nm = kdec == ps.h.K ? "k_level_decode[finest]" : "k_level_decode[coarser]";
