@@ -754,11 +754,18 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const size_t t_ul = align256(t_sub + g.total_sub * 4), t_bytes = align256(t_ul + total_unpred * elem);
     STZ_CUDA(ctx->h_io.ensure(t_bytes));
     uint8_t* ht = ctx->h_io.as<uint8_t>();
-    STZ_CUDA(cudaMemcpyAsync(ht + t_words, ctx->stream_words.p, (size_t)nstreams * 8, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaMemcpyAsync(ht + t_choff, ctx->chunk_off.p, g.total_chunk_slots * 8, cudaMemcpyDeviceToHost, st));
-    STZ_CUDA(cudaMemcpyAsync(ht + t_sub, ctx->sub_off.p, g.total_sub * 4, cudaMemcpyDeviceToHost, st));
+    // on the copy stream, so the encode launches below do not wait for them
+    {
+        cudaEvent_t ev_scan = ctx->event();
+        STZ_CUDA(cudaEventRecord(ev_scan, st));
+        STZ_CUDA(cudaStreamWaitEvent(sc, ev_scan, 0));
+        ctx->ev_pool.push_back(ev_scan);  // the wait is enqueued: the event may be recorded again
+    }
+    STZ_CUDA(cudaMemcpyAsync(ht + t_words, ctx->stream_words.p, (size_t)nstreams * 8, cudaMemcpyDeviceToHost, sc));
+    STZ_CUDA(cudaMemcpyAsync(ht + t_choff, ctx->chunk_off.p, g.total_chunk_slots * 8, cudaMemcpyDeviceToHost, sc));
+    STZ_CUDA(cudaMemcpyAsync(ht + t_sub, ctx->sub_off.p, g.total_sub * 4, cudaMemcpyDeviceToHost, sc));
     if (total_unpred)
-        STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, st));
+        STZ_CUDA(cudaMemcpyAsync(ht + t_ul, ctx->ulist.p, total_unpred * elem, cudaMemcpyDeviceToHost, sc));
     struct Events {
         std::vector<cudaEvent_t> e;
         ~Events()
@@ -787,7 +794,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     // compress frames: those waits block instead of spinning on a core
     for (size_t i = 0; i < ev.e.size(); ++i)
         STZ_CUDA(cudaEventCreateWithFlags(&ev.e[i], cudaEventDisableTiming | (i < ngroups ? cudaEventBlockingSync : 0)));
-    STZ_CUDA(cudaEventRecord(ev.e[2 * ngroups], st));
+    STZ_CUDA(cudaEventRecord(ev.e[2 * ngroups], sc));
     std::vector<CtaWork> gwork;
     std::vector<uint32_t> gids;
     std::vector<size_t> gw(ngroups + 1, 0);
