@@ -907,7 +907,9 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const uint64_t* choff = (const uint64_t*)(ht + t_choff);
     const uint32_t* subo = (const uint32_t*)(ht + t_sub);
     const uint8_t* ul = ht + t_ul;
-    ctx->pool->parallel_for((size_t)nstreams, [&](size_t s) {
+    // finest streams first: their plane tables make them the largest
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t r) {
+        const size_t s = (size_t)nstreams - 1 - r;
         const StreamDesc& d = sd[s];
         StreamParts& p = parts[s];
         append_stream_header(p.hdr, syms[s].data(), lens[s].data(), d.n_used, d.run_base, d.run_n,
@@ -1039,7 +1041,8 @@ stz_status prepare(stz_context* ctx, const stz_stream* s, int kmax, Prepared& p,
     std::atomic<int> bad{0};
     std::vector<const char*> why(nstreams, nullptr);
     const uint8_t* bytes = s->bytes.data();
-    ctx->pool->parallel_for((size_t)nstreams, [&](size_t i) {
+    ctx->pool->parallel_for((size_t)nstreams, [&](size_t r) {
+        const size_t i = (size_t)nstreams - 1 - r;  // finest streams (largest headers) first
         const int k = (int)i / 7 + 1, b = (int)i % 7;
         const LevelDir& L = ps.lv[k];
         const StreamDir& d = L.s[b];
