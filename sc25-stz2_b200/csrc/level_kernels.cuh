@@ -346,7 +346,7 @@ __device__ __forceinline__ void encode_interior(const Acc& r, const EncodeIO<T>&
 }
 
 template <typename T, int PRED, bool FINEST, int LM, int ZB = kZSmall>
-__global__ void __launch_bounds__(BX* BY, LM == kLearnNone && sizeof(T) == 4 ? (FINEST ? 5 : 3) : 1) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
+__global__ void __launch_bounds__(BX* BY, LM == kLearnNone && sizeof(T) == 4 ? (FINEST ? 5 : 4) : 1) k_level_encode(EncodeIO<T> io, const T* __restrict__ R, LevelGeom geo,
                                                          QuantParams qp, HistArgs hist, LearnedArgs<T> la,
                                                          const __grid_constant__ CUtensorMap tmap, int use_tma,
                                                          const __grid_constant__ QuantTable qt)
