@@ -68,7 +68,9 @@ __global__ void k_expand_codebook(const StreamDesc* __restrict__ sd, const uint1
     }
 }
 
-// ---- encode side: one warp per plane -----------------------------------------
+// ---- encode side: a lane group per plane ----------------------------------------
+// (Planes of up to 1024 codes take the literal lists below; this segment form
+// serves larger planes.)
 // Lane i of a group of W lanes (W = 32 for planes of 1024 codes and more,
 // fewer for smaller planes, see lanes_per_plane) owns the codes [a_i, b_i) of
 // the plane (W consecutive segments of S = ceil(plane / W) codes). A run of centre codes is coded by
@@ -1155,8 +1157,9 @@ __device__ __forceinline__ uint32_t decode_group(const StreamDesc& s)
 
 // A stream whose planes average more than seq_bits payload bits, with enough
 // planes to fill the device one thread per plane, is decoded one thread per
-// plane; sparser or smaller streams one warp per plane (a warp decodes each
-// symbol about three times, a thread once but with the full serial chain).
+// plane; sparser or smaller streams a lane group per plane (decode_group: the
+// group decodes each symbol about three times, a thread once but with the
+// full serial chain).
 constexpr uint64_t kSeqMinPlanes = 16384;
 constexpr int kSeqMinItems = 128;  // smaller launches (single requests) are latency-bound: warps only
 __device__ __forceinline__ bool decode_sequential(const StreamDesc& s, uint32_t seq_bits)

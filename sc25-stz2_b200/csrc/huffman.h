@@ -52,7 +52,7 @@ void launch_decode(const CtaWork* work, const uint32_t* chunk_ids, int nwork, co
 // each, stream i at byte i * decode_tables_bytes() of `tables`.
 size_t decode_tables_bytes();
 // Mean payload bits per plane above which launch_decode decodes a stream one
-// thread per plane instead of one warp per plane, in launches of at least 128
+// thread per plane instead of a lane group per plane, in launches of at least 128
 // work items and for streams of at least 16384 planes (STZ_DECODE_SEQ_BITS
 // overrides the built-in 2048).
 uint32_t decode_seq_bits();
