@@ -907,21 +907,23 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     const uint64_t* choff = (const uint64_t*)(ht + t_choff);
     const uint32_t* subo = (const uint32_t*)(ht + t_sub);
     const uint8_t* ul = ht + t_ul;
-    // finest streams first: their plane tables make them the largest
-    ctx->pool->parallel_for((size_t)nstreams, [&](size_t r) {
-        const size_t s = (size_t)nstreams - 1 - r;
+    for (int s = 0; s < nstreams; ++s) {
         const StreamDesc& d = sd[s];
         StreamParts& p = parts[s];
-        append_stream_header(p.hdr, syms[s].data(), lens[s].data(), d.n_used, d.run_base, d.run_n,
-                             unpred_off[s + 1] - unpred_off[s],
-                             ul + unpred_off[s] * elem, elem, h_ucnt + d.chunk_base, choff + d.chunk_base,
-                             subo + d.sub_base, (int)d.nchunks, (int)d.C);
         p.words = ctx->h_payload.as<uint32_t>() + meta[nstreams + s];
         p.chunk_word_off = choff + d.chunk_base;
         p.layers = (int)d.ncz;
         p.chunks_per_layer = (int)(d.ncx * d.ncy);
-    });
-    lap.mark("stream headers");
+    }
+    // each stream header is built by the pool job that compresses it (the
+    // finest streams', the largest, first)
+    auto build_header = [&](size_t s) {
+        const StreamDesc& d = sd[s];
+        append_stream_header(parts[s].hdr, syms[s].data(), lens[s].data(), d.n_used, d.run_base, d.run_n,
+                             unpred_off[s + 1] - unpred_off[s], ul + unpred_off[s] * elem, elem,
+                             h_ucnt + d.chunk_base, choff + d.chunk_base, subo + d.sub_base, (int)d.nchunks,
+                             (int)d.C);
+    };
     ContainerWriter cw(h, parts, *ctx->pool);
     std::atomic<int> ev_err{0};
     // a group's copy seen complete once: later frames of the group make no
@@ -942,7 +944,8 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
             if (g == 0 || copied[g - 1].load(std::memory_order_acquire)) return;
             if (cudaEventSynchronize(ev.e[g - 1]) != cudaSuccess) ev_err = 1;
             copied[g - 1].store(1, std::memory_order_release);
-        });
+        },
+        build_header);
     if (ev_err) {  // reports the device error
         STZ_CUDA(cudaStreamSynchronize(ctx->st_copy));
         STZ_CUDA(cudaStreamSynchronize(st));

@@ -597,20 +597,25 @@ void ContainerWriter::compress_streams(size_t s0, size_t s1)
 }
 
 void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t(size_t, int)>& group_of_frame,
-                                      const std::function<void(size_t)>& wait_group)
+                                      const std::function<void(size_t)>& wait_group,
+                                      const std::function<void(size_t)>& build_header)
 {
-    // group by group, largest frames first inside a group: the pool's threads
-    // move on to the next group's frames as soon as its bytes are ready
+    // group by group, largest frames first inside a group (headers not built
+    // yet: later streams, the finer levels, first): the pool's threads move
+    // on to the next group's frames as soon as its bytes are ready
     std::vector<std::vector<size_t>> by_group(ngroups);
+    std::vector<size_t> stream_of(frames_.size(), SIZE_MAX);
     for (size_t st = 0; st + 1 < first_.size(); ++st)
         for (size_t i = first_[st]; i < first_[st + 1]; ++i) {
+            stream_of[i] = st;
             const size_t gi = group_of_frame(st, (int)(i - first_[st]) - 1);
             if (gi < ngroups) by_group[gi].push_back(i);
         }
     std::vector<size_t> order, group_of;
     for (size_t gi = 0; gi < ngroups; ++gi) {
         auto& v = by_group[gi];
-        std::sort(v.begin(), v.end(), [&](size_t a, size_t c) { return frames_[a].n > frames_[c].n; });
+        std::sort(v.begin(), v.end(),
+                  [&](size_t a, size_t c) { return frames_[a].n != frames_[c].n ? frames_[a].n > frames_[c].n : a > c; });
         order.insert(order.end(), v.begin(), v.end());
         group_of.resize(order.size(), gi);
     }
@@ -630,6 +635,12 @@ void ContainerWriter::compress_groups(size_t ngroups, const std::function<size_t
         wait_group(group_of[k]);
         const auto f0 = std::chrono::steady_clock::now();
         if (trace) j_go[k] = since(f0);
+        if (build_header && !frames_[order[k]].payload) {
+            const size_t st = stream_of[order[k]];
+            build_header(st);
+            frames_[order[k]].src = parts_[st].hdr.data();
+            frames_[order[k]].n = parts_[st].hdr.size();
+        }
         if (trace) {
             int64_t v = since(f0), cur = g_first[group_of[k]].load();
             while (v < cur && !g_first[group_of[k]].compare_exchange_weak(cur, v)) {

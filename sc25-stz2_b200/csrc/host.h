@@ -188,9 +188,12 @@ public:
     // The frames in group order on the pool: group_of_frame(stream, layer)
     // (layer -1: the stream's header frame) gives a frame's group in
     // [0, ngroups) (anything else: not compressed by this call); a thread
-    // calls wait_group(g) before each frame of group g.
+    // calls wait_group(g) before each frame of group g. build_header (may be
+    // empty): the job of stream s's header frame first calls it to fill
+    // parts[s].hdr, so each header is built and compressed by one job.
     void compress_groups(size_t ngroups, const std::function<size_t(size_t, int)>& group_of_frame,
-                         const std::function<void(size_t)>& wait_group);
+                         const std::function<void(size_t)>& wait_group,
+                         const std::function<void(size_t)>& build_header = nullptr);
     Bytes finish(const void* coarsest, const std::vector<LevelDir>& levels);
 
 private:
