@@ -519,6 +519,23 @@ def configs_bench(args, ctx, local, field):
                 res["progressive"].append({"level": lvl, "resolution": f"1/{st}", "ms": lms,
                                            "output_gbs": o_l.numel() * 4 / lms / 1e6,
                                            "field_equiv_gbs": nbytes / lms / 1e6})
+    # predictor modes on the same field and bound, at the multipliers of the
+    # reference's artifact programs (1 / 2.5 / 6.25, float.cpp and
+    # dependency.cpp): the staged predictor of src/dependency.cpp against the
+    # dynamic lines (FD5) and the plain cubic stencils (float.cpp)
+    res["predictors"] = []
+    for name in ("dynamic", "cubic", "staged"):
+        try:
+            o = stz_b200.default_opts(eb=1e-3, eb_mode="rel", zstd_level=args.zstd, predictor=name, mult_base=1.0,
+                                      mult_low=2.5, mult_high=6.25)
+            cms, s = timed(lambda: ctx.compress(field, opts=o), 3)
+            dms, _ = timed(lambda: ctx.decompress(s, out=out), 3)
+            res["predictors"].append({"predictor": name, "rel_eb": 1e-3, "mults": [1.0, 2.5, 6.25],
+                                      "compress_gbs": nbytes / cms / 1e6, "decompress_gbs": nbytes / dms / 1e6,
+                                      "cr": nbytes / len(s)})
+            del s
+        except Exception as e:  # recorded, so the rest of the line still comes out
+            res["predictors"].append({"predictor": name, "error": str(e)[:200]})
     del out
     torch.cuda.empty_cache()
     nz, ny, nx = 256, 384, 384

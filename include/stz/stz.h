@@ -71,7 +71,13 @@ typedef enum stz_bound_mode {
 
 typedef enum stz_predictor {
     STZ_PRED_DYNAMIC = 0, /* inverse-variance blend of cubic lines (FD5:624-748) */
-    STZ_PRED_CUBIC = 1    /* fixed tricubic-family stencils (src/float.cpp:84-273) */
+    STZ_PRED_CUBIC = 1,   /* fixed tricubic-family stencils (src/float.cpp:84-273) */
+    /* Staged: sub-blocks 1, 2, 4 from 1-D cubics on the coarse grid, then 3, 5,
+     * 6 and 7 from inverse-variance blends of 1-D cubics through the siblings
+     * decoded before them (src/dependency.cpp:90-330, stage order 659-704).
+     * No learned correction; boxes and slices decode the whole field and copy
+     * the box out; the request server does not take these streams. */
+    STZ_PRED_STAGED = 2
 } stz_predictor;
 
 typedef struct stz_opts {

@@ -127,6 +127,28 @@ def rd() -> C.CDLL:
     return _rd
 
 
+DEP_SO = os.path.join(HERE, "_ref", "libdep_ref.so")
+_dep = None
+
+
+def dep_available() -> bool:
+    return os.path.exists(DEP_SO)
+
+
+def dep() -> C.CDLL:
+    """The reference's staged-predictor experiment (src/dependency.cpp, float
+    only) compiled from source: its four stage functions."""
+    global _dep
+    if _dep is None:
+        L = C.CDLL(DEP_SO)
+        for f in ("depref_preprocess_block", "depref_depreprocess_block"):
+            getattr(L, f).argtypes = [ci, vp, vp, vp, ci, ci, ci]
+        for f in ("depref_preprocess_block_staged", "depref_depreprocess_block_staged"):
+            getattr(L, f).argtypes = [ci, vp, vp, vp, ci, ci, ci]
+        _dep = L
+    return _dep
+
+
 def ref() -> C.CDLL:
     global _ref
     if _ref is None:
@@ -389,6 +411,68 @@ def ref_round_trip_plain(field: np.ndarray, eb: float, mults=(1.0, 2.5, 6.25), r
                                                            dz, 0, 0, 0)
         nxt = np.empty((2 * dz, 2 * dy, 2 * dx), a.dtype)
         getattr(R, "fd5ref_merge_sub_blocks_to_full_" + suf)(_p(out), _p(nxt), dx, dy, dz)
+        codes.append(lc)
+        unpred.append(lu)
+        grid = nxt
+        grids.append(grid)
+    return {"K": K, "codes": codes, "unpred": unpred, "grids": grids, "closed_loop_ok": True}
+
+
+def ref_round_trip_staged(field: np.ndarray, eb: float, mults=(1.0, 2.5, 6.25), radius: int = 32768,
+                          chunk_high: int = 32, chunk_low: int = 16) -> dict:
+    """The staged pipeline of src/dependency.cpp (float only): per level,
+    blocks 0, 1, 3 through preprocess_block against the decoded coarser grid,
+    then 2, 4, 5 and last 6 through preprocess_block_staged against the
+    decoded siblings, each block's residuals quantized (FD5's
+    quantize_range_nodec at multiplier x eb, multipliers 1 / 2.5 / 6.25 as
+    dependency.cpp:602, 674) and its decoded values rebuilt by the matching
+    depreprocess function before the next stage reads them
+    (dependency.cpp:591-634, 659-704); merge_sub_blocks_to_full builds the next
+    level's grid. Stage functions from dependency.cpp, quantizer, dequantizer,
+    split and merge from FD5, all compiled from source (oracle/_ref), driven
+    through this project's hierarchy. Returns the same record as
+    ref_round_trip."""
+    a = np.ascontiguousarray(field)
+    if a.dtype != np.float32:
+        raise ValueError("src/dependency.cpp is float only")
+    nz, ny, nx = a.shape
+    K = num_levels(nx, ny, nz)
+    S = 1 << K
+    R, D = ref(), dep()
+    grid = np.ascontiguousarray(a[::S, ::S, ::S])
+    grids, codes, unpred = [grid], [], []
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = a if s == 1 else np.ascontiguousarray(a[::s, ::s, ::s])
+        ebk = (mults[2] if k == K else mults[1] if k == K - 1 else mults[0]) * eb
+        dz, dy, dx = grid.shape
+        n = dx * dy * dz
+        C_ = oracle().stzo_level_chunk(nx, ny, nz, k, chunk_high, chunk_low)
+        subs = np.empty((8, dz, dy, dx), a.dtype)
+        R.fd5ref_slice_full_data_f32(_p(fine), _p(subs), 2 * dx, 2 * dy, 2 * dz)
+        out = np.zeros((8, dz, dy, dx), a.dtype)
+        out[0] = grid
+        # ref_x, ref_y, ref_z, ref_xy, ref_xz, ref_yz: sub-blocks 1, 2, 4, 3, 5, 6
+        refs = (C.c_void_p * 6)(*[out[i].ctypes.data for i in (1, 2, 4, 3, 5, 6)])
+        lc, lu = [None] * 7, [0] * 7
+        for b in (0, 1, 3, 2, 4, 5, 6):
+            diff = np.empty((dz, dy, dx), a.dtype)
+            if b in (0, 1, 3):
+                D.depref_preprocess_block(b, _p(subs[b + 1]), _p(grid), _p(diff), dx, dy, dz)
+            else:
+                D.depref_preprocess_block_staged(b, _p(subs[b + 1]), refs, _p(diff), dx, dy, dz)
+            q = np.empty(n, np.int32)
+            u = np.empty(n, a.dtype)
+            nu = R.fd5ref_quantize_range_nodec_f32(_p(diff), n, ebk, radius, _p(q), _p(u), n)
+            lc[b] = chunk_major(q, (dz, dy, dx), C_).astype(np.uint16)
+            lu[b] = int(nu)
+            dq = ref_dequantize(q, ebk, radius, u[:nu], a.dtype).reshape(dz, dy, dx)
+            if b in (0, 1, 3):
+                D.depref_depreprocess_block(b, _p(dq), _p(grid), _p(out[b + 1]), dx, dy, dz)
+            else:
+                D.depref_depreprocess_block_staged(b, _p(dq), refs, _p(out[b + 1]), dx, dy, dz)
+        nxt = np.empty((2 * dz, 2 * dy, 2 * dx), a.dtype)
+        R.fd5ref_merge_sub_blocks_to_full_f32(_p(out), _p(nxt), dx, dy, dz)
         codes.append(lc)
         unpred.append(lu)
         grid = nxt

@@ -175,6 +175,94 @@ static T FN(t_predict_plain)(int block, const T* r, int x, int y, int z, int dx,
     }
 }
 
+/* Staged predictor of src/dependency.cpp (predictor 2). Blocks 0, 1, 3 (one
+ * odd axis) take a 1-D cubic along that axis of the coarse grid; blocks 2, 4, 5
+ * blend two 1-D cubics through the decoded blocks 0, 1, 3 by inverse
+ * variance; block 6 blends three through the decoded blocks 2, 4, 5. A line
+ * is addressed by the point c, its stride st along the axis, and the point's
+ * index pos on an axis of extent dim. */
+
+/* interp_axis, dependency.cpp:90-118 (W0..W3 = -1/16, 9/16, 9/16, -1/16). */
+static inline T FN(dep_line)(const T* c, ptrdiff_t st, int pos, int dim)
+{
+    if (pos == dim - 1) return c[0];
+    if (pos == dim - 2 || pos == 0) return 0.5f * (c[0] + c[st]);
+    return -0.0625f * c[-st] + 0.5625f * c[0] + 0.5625f * c[st] + -0.0625f * c[2 * st];
+}
+
+/* interp_axis_with_variance, dependency.cpp:162-243. The reference squares
+ * |b - a|; squaring b - a gives the same bits. */
+static inline void FN(dep_line_pv)(const T* c, ptrdiff_t st, int pos, int dim, T* p, T* v)
+{
+    const T eps = (T)1e-12f;
+    if (pos == dim - 1) {
+        *p = c[0];
+        *v = eps;
+        return;
+    }
+    if (pos == dim - 2 || pos == 0) {
+        const T a = c[0], b = c[st];
+        const T e = b - a;
+        *p = 0.5f * (a + b);
+        *v = e * e + eps;
+        return;
+    }
+    const T a = c[-st], b = c[0], cc = c[st], d = c[2 * st];
+    const T c0 = a - 2.0f * b + cc;
+    const T c1 = b - 2.0f * cc + d;
+    *p = -0.0625f * a + 0.5625f * b + 0.5625f * cc + -0.0625f * d;
+    *v = 0.5f * (c0 * c0 + c1 * c1) + eps;
+}
+
+/* inverse_variance_blend3, dependency.cpp:250-256 (blend2 above is
+ * inverse_variance_blend2, dependency.cpp:245-248, the same expression). */
+static inline T FN(blend3)(T p0, T v0, T p1, T v1, T p2, T v2)
+{
+    const T w0 = v1 * v2;
+    const T w1 = v0 * v2;
+    const T w2 = v0 * v1;
+    return (w0 * p0 + w1 * p1 + w2 * p2) / (w0 + w1 + w2);
+}
+
+/* Prediction of block b at coarse (x, y, z): stage-1 blocks from the coarse
+ * grid r (interp_axis on sub-block 0, preprocess_block dependency.cpp:333-383), the others
+ * from the decoded fine grid F of this level (2dx x 2dy x 2dz), in which
+ * sub-block s sits at parity (s & 1, s >> 1 & 1, s >> 2) and a step along an
+ * axis of a sub-block is two fine points (staged_prediction,
+ * dependency.cpp:258-292: ref_x, ref_y, ref_z, ref_xy, ref_xz, ref_yz are
+ * sub-blocks 1, 2, 4, 3, 5, 6). */
+static T FN(staged_pred)(int b, const T* r, const T* F, int x, int y, int z, int dx, int dy, int dz)
+{
+    const size_t cx = 1, cy = (size_t)dx, cz = (size_t)dx * dy;
+    const size_t i = (size_t)z * cz + (size_t)y * cy + x;
+    const ptrdiff_t fx = 2, fy = 4 * (ptrdiff_t)dx, fz = 8 * (ptrdiff_t)dx * dy;
+#define SIB(s) (F + (size_t)(2 * z + ((s) >> 2)) * (4 * (size_t)dx * dy) + (size_t)(2 * y + (((s) >> 1) & 1)) * (2 * (size_t)dx) + 2 * (size_t)x + ((s) & 1))
+    T p0, v0, p1, v1, p2, v2;
+    switch (b) {
+    case 0: return FN(dep_line)(r + i, (ptrdiff_t)cx, x, dx);
+    case 1: return FN(dep_line)(r + i, (ptrdiff_t)cy, y, dy);
+    case 3: return FN(dep_line)(r + i, (ptrdiff_t)cz, z, dz);
+    case 2:
+        FN(dep_line_pv)(SIB(1), fy, y, dy, &p0, &v0);
+        FN(dep_line_pv)(SIB(2), fx, x, dx, &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    case 4:
+        FN(dep_line_pv)(SIB(1), fz, z, dz, &p0, &v0);
+        FN(dep_line_pv)(SIB(4), fx, x, dx, &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    case 5:
+        FN(dep_line_pv)(SIB(2), fz, z, dz, &p0, &v0);
+        FN(dep_line_pv)(SIB(4), fy, y, dy, &p1, &v1);
+        return FN(blend2)(p0, v0, p1, v1);
+    default:
+        FN(dep_line_pv)(SIB(3), fz, z, dz, &p0, &v0);
+        FN(dep_line_pv)(SIB(5), fy, y, dy, &p1, &v1);
+        FN(dep_line_pv)(SIB(6), fx, x, dx, &p2, &v2);
+        return FN(blend3)(p0, v0, p1, v1, p2, v2);
+    }
+#undef SIB
+}
+
 static inline T FN(predict_any)(int predictor, int block, const T* r, int x, int y, int z, int dx, int dy,
                                 int dz)
 {
@@ -268,6 +356,99 @@ static long long FN(t_quantize)(const T* d, size_t n, double eb, int radius, int
     return (long long)nu;
 }
 
+/* Level step of the staged predictor: the blocks in the reference's stage
+ * order (compress dependency.cpp:659-704 and 591-634 for the
+ * second level, decompress 755-772): 0, 1, 3, then
+ * 2, 4, 5, then 6, each predicted from the decoded values of the stages
+ * before it (the encoder quantizes every residual and rebuilds the decoded
+ * value before the next stage reads it, as SZ_compress hands back the
+ * decoded residuals there). Codes and unpredictable values come out in block
+ * order, like the other predictors. decoded null: a scratch fine grid. */
+static const int FN(staged_order)[7] = {0, 1, 3, 2, 4, 5, 6};
+
+static int FN(t_level_encode_staged)(const T* fine, const T* coarse, int dx, int dy, int dz, double eb, int radius,
+                                     int* q, T* unpred, size_t cap, size_t* counts, T* decoded)
+{
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    const double recip = 1.0 / eb;
+    T* F = decoded ? decoded : (T*)malloc(8 * n * sizeof(T) + 1);
+    T* dres = (T*)malloc(7 * n * sizeof(T) + 1);
+    int rc = 0;
+    if (!F || !dres) {
+        rc = -1;
+        goto done;
+    }
+    for (int z = 0; z < dz; ++z)
+        for (int y = 0; y < dy; ++y)
+            for (int x = 0; x < dx; ++x)
+                F[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] = coarse[((size_t)z * dy + y) * dx + x];
+    for (int o = 0; o < 7; ++o) {
+        const int b = FN(staged_order)[o], s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const size_t i = ((size_t)z * dy + y) * dx + x;
+                    const size_t fi = (2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px;
+                    const T p = FN(staged_pred)(b, coarse, F, x, y, z, dx, dy, dz);
+                    const T d = fine[fi] - p;
+                    T dec = 0;
+                    const int code = FN(quant1)(d, eb, recip, radius, &dec);
+                    q[(size_t)b * n + i] = code;
+                    dres[(size_t)b * n + i] = d;
+                    F[fi] = (code ? FN(recover)(code, eb, radius) : d) + p;
+                }
+    }
+    {
+        size_t nu = 0;
+        for (int b = 0; b < 7 && !rc; ++b) {
+            size_t nb = 0;
+            for (size_t i = 0; i < n; ++i)
+                if (q[(size_t)b * n + i] == 0) {
+                    if (nu >= cap) {
+                        rc = -1;
+                        break;
+                    }
+                    unpred[nu++] = dres[(size_t)b * n + i];
+                    ++nb;
+                }
+            counts[b] = nb;
+        }
+    }
+done:
+    if (F != decoded) free(F);
+    free(dres);
+    return rc;
+}
+
+static void FN(t_level_decode_staged)(const int* q, const T* unpred, const T* coarse, int dx, int dy, int dz,
+                                      double eb, int radius, T* out)
+{
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    size_t first[7], u = 0;  /* each block's first unpredictable value */
+    for (int b = 0; b < 7; ++b) {
+        first[b] = u;
+        for (size_t i = 0; i < n; ++i) u += q[(size_t)b * n + i] == 0;
+    }
+    for (int z = 0; z < dz; ++z)
+        for (int y = 0; y < dy; ++y)
+            for (int x = 0; x < dx; ++x)
+                out[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] = coarse[((size_t)z * dy + y) * dx + x];
+    for (int o = 0; o < 7; ++o) {
+        const int b = FN(staged_order)[o], s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        size_t ub = first[b];
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const int code = q[(size_t)b * n + ((size_t)z * dy + y) * dx + x];
+                    const T dq = code ? FN(recover)(code, eb, radius) : unpred[ub++];
+                    const T p = FN(staged_pred)(b, coarse, out, x, y, z, dx, dy, dz);
+                    out[(2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px] = dq + p;
+                }
+    }
+}
+
 /* Level encode: residual of sub-block (block+1) against the predictor on the
  * decoded coarse grid (FD5 preprocess + quantize, see the fd5ref shim for the
  * reference's call sequence). The decoded fine grid uses the decoder's
@@ -277,6 +458,8 @@ static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, in
                           const stzo_model* M, uint32_t flags)
 {
     ftz_on();
+    if (predictor == 2)
+        return FN(t_level_encode_staged)(fine, coarse, dx, dy, dz, eb, radius, q, unpred, cap, counts, decoded);
     const size_t n = (size_t)dx * dy * dz;
     const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
     const double recip = 1.0 / eb;
@@ -327,6 +510,10 @@ static void FN(t_level_decode)(const int* q, const T* unpred, const size_t* coun
                            int dz, int predictor, double eb, int radius, T* out, const stzo_model* M, uint32_t flags)
 {
     ftz_on();
+    if (predictor == 2) {
+        FN(t_level_decode_staged)(q, unpred, coarse, dx, dy, dz, eb, radius, out);
+        return;
+    }
     const size_t n = (size_t)dx * dy * dz;
     const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
     const T rs = M ? (T)(1.0 / (eb * M->s_in)) : (T)0, so = M ? (T)(M->s_out * eb) : (T)0;

@@ -316,7 +316,10 @@ stz_status check_opts(const stz_opts* o)
     if (!(o->mult_base > 0) || !(o->mult_low > 0) || !(o->mult_high > 0)) STZ_FAIL(STZ_ERR_ARG, "multipliers must be > 0");
     if (o->radius < 1 || o->radius > 32768) STZ_FAIL(STZ_ERR_ARG, "radius must be in [1, 32768]");
     if (o->zstd_level < 0 || o->zstd_level > 22) STZ_FAIL(STZ_ERR_ARG, "zstd_level must be in [0, 22]");
-    if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC &&
+        o->predictor != STZ_PRED_STAGED) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    if (o->predictor == STZ_PRED_STAGED && o->model)
+        STZ_FAIL(STZ_ERR_ARG, "the staged predictor takes no learned correction");
     if (o->learned_flags < -1 || (o->learned_flags >= 0 && (o->learned_flags & ~0x7f7f)))
         STZ_FAIL(STZ_ERR_ARG, "learned_flags must be -1 or a mask of bits 0-6 and 8-14");
     return STZ_OK;
@@ -414,6 +417,11 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
     // buffers, cleared ahead of the value range
     STZ_CUDA(ctx->grid[0].ensure(g.n_fine_max * elem));
     STZ_CUDA(ctx->grid[1].ensure(g.n_fine_max * elem));
+    // the staged predictor's finest level keeps its decoded values too (its
+    // later stages predict from them): the grid level K would write, at
+    // full size
+    const bool staged = o.predictor == STZ_PRED_STAGED;
+    if (staged) STZ_CUDA(ctx->grid[K & 1].ensure(std::max(g.n_fine_max, N) * elem));
     STZ_CUDA(ctx->codes.ensure(g.total_codes * 2));
     STZ_CUDA(ctx->unpred_dense.ensure(g.total_codes * elem));
     STZ_CUDA(ctx->unpred_cnt.ensure(g.total_chunk_slots * 4));
@@ -465,7 +473,7 @@ stz_status compress_impl(stz_context* ctx, const T* field, int nx, int ny, int n
         a.unpred_cnt = ctx->unpred_cnt.as<uint32_t>() + s0.chunk_base;
         a.hist_full = ctx->hist.as<uint32_t>() + (size_t)(k - 1) * 7 * R2;
         a.hist_outside = ctx->hist_out.as<uint32_t>() + (size_t)(k - 1) * 7;
-        a.decoded = k < K ? ctx->grid[1 - cur].as<T>() : nullptr;
+        a.decoded = k < K || staged ? ctx->grid[1 - cur].as<T>() : nullptr;
         a.qp = make_quant_params(ebk[k], o.radius);
         a.learned.tensor_cores = learned_tensor_cores();
         if (const int mi = level_model(k); mi >= 0) {
@@ -1394,9 +1402,12 @@ struct DecodePipe {
         STZ_CUDA(ctx->grid[1].ensure(gmax * sizeof(T)));
         coarse = p.coarsest->as<T>();
         // the finest level decodes by z-bricks as its chunk layers arrive
-        // (plain kernels only; else the whole level after the last batch)
-        fin_bricks = level_decode_bricks(level_geom(ps, kdec), learned_args<T>(ps, kdec, p.d_models).model != nullptr &&
-                                                                   learned_args<T>(ps, kdec, p.d_models).flags,
+        // (plain kernels only; else the whole level after the last batch;
+        // the staged predictor's stages span the whole level)
+        fin_bricks = level_decode_bricks(level_geom(ps, kdec),
+                                         (learned_args<T>(ps, kdec, p.d_models).model != nullptr &&
+                                          learned_args<T>(ps, kdec, p.d_models).flags) ||
+                                             ps.h.predictor == STZ_PRED_STAGED,
                                          0, nullptr);
         // the entropy decodes (ctx->st_dec) follow everything enqueued on
         // ctx->st so far: tables, coarsest grid, work lists, earlier calls
@@ -1566,6 +1577,25 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         odims[0] = (size_t)(plan.q[0].e - plan.q[0].b + 1);
         odims[1] = (size_t)(plan.q[1].e - plan.q[1].b + 1);
         odims[2] = (size_t)(plan.q[2].e - plan.q[2].b + 1);
+    }
+    if (h.predictor == STZ_PRED_STAGED) {
+        // A staged block's value depends on siblings decoded before it along
+        // whole lines, beyond the planner's chunk halo: decode the field,
+        // then copy the box out (as a decoder without chunk markers does,
+        // src/stz-rd.cpp:591-596).
+        STZ_CUDA(ctx->staged_full.ensure((size_t)h.nx * h.ny * h.nz * sizeof(T)));
+        STZ_TRY(decompress_level_dev<T>(ctx, s, 0, ctx->staged_full.as<T>()));
+        const size_t ox = (size_t)(plan.q[0].e - plan.q[0].b + 1), oy = (size_t)(plan.q[1].e - plan.q[1].b + 1),
+                     oz = (size_t)(plan.q[2].e - plan.q[2].b + 1);
+        cudaMemcpy3DParms cp{};
+        cp.srcPtr = make_cudaPitchedPtr(ctx->staged_full.p, (size_t)h.nx * sizeof(T), (size_t)h.nx, (size_t)h.ny);
+        cp.srcPos = make_cudaPos((size_t)plan.q[0].b * sizeof(T), (size_t)plan.q[1].b, (size_t)plan.q[2].b);
+        cp.dstPtr = make_cudaPitchedPtr(out_dev, ox * sizeof(T), ox, oy);
+        cp.extent = make_cudaExtent(ox * sizeof(T), oy, oz);
+        cp.kind = cudaMemcpyDeviceToDevice;
+        STZ_CUDA(cudaMemcpy3DAsync(&cp, ctx->st));
+        STZ_CUDA(cudaStreamSynchronize(ctx->st));
+        return STZ_OK;
     }
     Prepared local;
     Prepared* p = s->resident.get();

@@ -318,6 +318,7 @@ __device__ __forceinline__ T recover_lut(const T* lut, int q, const QuantParams&
 }
 
 #include "level_kernels.cuh"
+#include "staged_kernels.cuh"
 
 // Coarsest grid of the hierarchy: every 2^K-th point of the field.
 template <typename T>
@@ -703,9 +704,35 @@ bool make_tile_map(const T* R, int dx, int dy, int dz, int zb, CUtensorMap* m)
 
 }  // namespace
 
+// Staged predictor: three dependent launches per level (staged_kernels.cuh);
+// a.decoded is the decoded fine grid, a scratch grid on the finest level.
+template <typename T>
+void launch_staged_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
+{
+    const HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
+    const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
+    const dim3 grd = staged_grid(a.geo), blk(kStagedTX, kStagedTY);
+    k_staged_encode<T, 1><<<grd, blk, 0, st>>>(io, a.decoded, a.coarse, a.geo, a.qp, h);
+    k_staged_encode<T, 2><<<grd, blk, 0, st>>>(io, a.decoded, a.coarse, a.geo, a.qp, h);
+    k_staged_encode<T, 3><<<grd, blk, 0, st>>>(io, a.decoded, a.coarse, a.geo, a.qp, h);
+}
+
+template <typename T>
+void launch_staged_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
+{
+    const dim3 grd = staged_grid(a.geo), blk(kStagedTX, kStagedTY);
+    k_staged_decode<T, 1><<<grd, blk, 0, st>>>(a.coarse, a.geo, a.qp, a.codes, a.unpred_dense, a.out);
+    k_staged_decode<T, 2><<<grd, blk, 0, st>>>(a.coarse, a.geo, a.qp, a.codes, a.unpred_dense, a.out);
+    k_staged_decode<T, 3><<<grd, blk, 0, st>>>(a.coarse, a.geo, a.qp, a.codes, a.unpred_dense, a.out);
+}
+
 template <typename T>
 void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
 {
+    if (a.predictor == 2) {
+        launch_staged_encode(a, st);
+        return;
+    }
     const LevelGeom& g = a.geo;
     const Shell shell = Shell::make(g.dx, g.dy, g.dz);
     dim3 blk(BX, BY, 1);
@@ -776,6 +803,10 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
 template <typename T>
 void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
 {
+    if (a.predictor == 2) {  // whole level (level_decode_bricks: none)
+        launch_staged_decode(a, st);
+        return;
+    }
     const LevelGeom& g = a.geo;
     const Shell shell = Shell::make(g.dx, g.dy, g.dz);
     dim3 blk(BX, BY, 1);

@@ -17,13 +17,14 @@ struct LevelEncodeArgs {
     int stride;         // sampling stride of this level's fine grid (1 = finest)
     const T* coarse;    // decoded coarse grid (geo.dx x dy x dz)
     LevelGeom geo;
-    int predictor;      // 0 = dynamic lines (FD5), 1 = plain cubic
+    int predictor;      // 0 = dynamic lines (FD5), 1 = plain cubic, 2 = staged (dependency.cpp)
     uint16_t* codes;        // 7 x n, chunk-major per stream
     T* unpred_dense;        // 7 x n, written where the code is 0
     uint32_t* unpred_cnt;   // 7 x (nchunks + 1)
     uint32_t* hist_full;    // 7 x 2*radius
     uint32_t* hist_outside; // 7
     T* decoded;             // decoded fine grid (2dx x 2dy x 2dz) or null on the finest level
+                            // (the staged predictor needs one there too: a scratch grid)
     QuantParams qp;
     LearnedArgs<T> learned; // learned correction (model null: none)
     SideStream side;        // boundary-shell kernel placement

@@ -256,7 +256,7 @@ struct stz_context {
     }
     stz::DevBuf field, grid[2], codes, unpred_dense, unpred_cnt, hist, hist_out, ctab, sub_bits, sub_off, chunk_off,
         stream_words, payload, sd, work, ids, uwork, ulist, cb_sym, cb_len, minmax, packed, rbits, out, mid, boxes,
-        tiles, models, eval, rstats, gwork;
+        tiles, models, eval, rstats, gwork, staged_full;
     stz::PinBuf h_hist, h_meta, h_meta2, h_payload, h_stage, h_io, h_small, h_rstats, h_fullh;
     stz::PinBuf h_xfer[2];  // staging chunks of host <-> device copies of pageable caller buffers
     // device buffers lent to one-off decodes

@@ -7,7 +7,8 @@ preprocess_block_zslab, quantize_range_nodec and, on coarser levels, the
 writeDec closed loop with depreprocess_block_zslab + merge), and the field is
 rebuilt with the reference decoder (recover LUT + depreprocess_block_zslab /
 depreprocess_block_zslab_to_full). Also records reference planner output for
-random queries.
+random queries, the plain tricubic stencils of src/stz-rd.cpp, and a staged
+pipeline of src/dependency.cpp's stage functions (oracle/_ref/libdep_ref.so).
 
     python tests/golden/make_golden.py        # needs the reference sources
 """
@@ -92,6 +93,20 @@ def main():
             getattr(R, "rdref_preprocess_block_" + suf)(b, po._p(sub), po._p(ref), po._p(d), dims[2], dims[1], dims[0])
             diffs.append(d)
         arrays[f"plain_{suf}_diff"] = np.stack(diffs)
+
+    # staged predictor of src/dependency.cpp (its stage functions, with FD5's
+    # quantizer, split and merge, through the hierarchy; chunks 8 / 4, level
+    # multipliers 1 / 2.5 / 6.25): each level's chunk-major codes per block
+    # and the decoded field
+    f = fields.grf((32, 32, 32), 3.0, 21, np.float32)
+    eb = po.pointwise_eb(f, 1e-3, (1.0, 2.5, 6.25))
+    st = po.ref_round_trip_staged(f, eb, (1.0, 2.5, 6.25), chunk_high=8, chunk_low=4)
+    arrays["staged_field"] = f
+    arrays["staged_eb"] = np.float64(eb)
+    arrays["staged_K"] = np.int64(st["K"])
+    for k in range(1, st["K"] + 1):
+        arrays[f"staged_L{k}_codes"] = np.stack(st["codes"][k - 1])
+    arrays["staged_decoded"] = st["grids"][st["K"]]
 
     rng = np.random.default_rng(5)
     plans, offs, queries = [], [0], []

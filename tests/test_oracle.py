@@ -158,6 +158,69 @@ def test_oracle_plain_pipeline_matches_reference(case):
         assert sum(sum(c) for c in ref["unpred"]) > 0
 
 
+@pytest.mark.skipif(not (po.ref_available() and po.dep_available()), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("case", ["grf64_1e-3", "logn64_1e-4", "ragged_112x80x48_1e-3"])
+def test_oracle_staged_pipeline_matches_reference(case):
+    """The staged predictor of src/dependency.cpp (predictor 2, multipliers
+    1 / 2.5 / 6.25): every level's codes of every block, and the full and
+    progressive decodes of the oracle's stream, against the reference's
+    stage functions in the reference's stage order
+    (pyoracle.ref_round_trip_staged)."""
+    from stz_b200 import fields
+
+    if case.startswith("grf"):
+        f, rel = fields.grf((64, 64, 64), 11.0 / 3.0, 7, np.float32), 1e-3
+    elif case.startswith("logn"):
+        f, rel = fields.lognormal((64, 64, 64), 5, np.float32), 1e-4
+    else:
+        f, rel = fields.grf((48, 80, 112), 3.0, 13, np.float32), 1e-3
+    mults = (1.0, 2.5, 6.25)
+    eb = po.pointwise_eb(f, rel, mults)
+    ref = po.ref_round_trip_staged(f, eb, mults, chunk_high=8, chunk_low=4)
+    stream = po.compress(f, eb, predictor=2, mults=mults, chunk_high=8, chunk_low=4)
+    K = ref["K"]
+    for k in range(1, K + 1):
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), ref["codes"][k - 1][b]), (k, b)
+    out = po.decompress(stream)
+    assert np.array_equal(out.view(np.uint32), ref["grids"][K].view(np.uint32))
+    for lvl in range(1, K + 1):
+        assert np.array_equal(po.decompress(stream, lvl).view(np.uint32), ref["grids"][K - lvl].view(np.uint32)), lvl
+    # this eb carries no slack for the final rounding of dq + P in float
+    # (the library's pointwise mode does): one ulp of the field's magnitude
+    E = rel * (float(f.max()) - float(f.min())) + float(np.spacing(np.abs(f).max()))
+    assert np.abs(out.astype(np.float64) - f).max() <= E
+
+
+def test_staged_pipeline_matches_reference_golden(golden):
+    """The oracle's staged stream against golden codes and decode produced by
+    src/dependency.cpp's stage functions (tests/golden/make_golden.py)."""
+    f = golden["staged_field"]
+    eb = float(golden["staged_eb"])
+    K = int(golden["staged_K"])
+    stream = po.compress(f, eb, predictor=2, mults=(1.0, 2.5, 6.25), chunk_high=8, chunk_low=4)
+    for k in range(1, K + 1):
+        want = golden[f"staged_L{k}_codes"]
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), want[b]), (k, b)
+    assert np.array_equal(po.decompress(stream).view(np.uint32), golden["staged_decoded"].view(np.uint32))
+
+
+def test_oracle_staged_f64_round_trip_and_box():
+    """The staged predictor in double (the same expressions in T): bound,
+    and boxes equal to the full decode's crop."""
+    from stz_b200 import fields
+
+    f = fields.fronts((64, 64, 64), 3, np.float64)
+    mults = (1.0, 2.5, 6.25)
+    eb = po.pointwise_eb(f, 1e-6, mults)
+    stream = po.compress(f, eb, predictor=2, mults=mults)
+    out = po.decompress(stream)
+    assert np.abs(out - f).max() <= 1e-6 * (float(f.max()) - float(f.min())) + float(np.spacing(np.abs(f).max()))
+    box = po.decompress_box(stream, (3, 5, 7), (40, 33, 20))
+    assert np.array_equal(box.view(np.uint64), out[7:21, 5:34, 3:41].view(np.uint64))
+
+
 @pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
 def test_planner_matches_reference_live():
     rng = np.random.default_rng(17)
