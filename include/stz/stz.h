@@ -291,6 +291,20 @@ stz_status stz_depreprocess_block_to_full_dev(stz_context* ctx, stz_dtype dtype,
 stz_status stz_depreprocess_block_roi_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* de,
                                           const void* ref, void* out, int dx, int dy, int dz, int end_x, int end_y,
                                           int end_z, int start_x, int start_y, int start_z);
+/* The staged predictor's stage functions of src/dependency.cpp on dense
+ * sub-blocks of dx*dy*dz values: diff = sub - P (preprocess) or out = de + P
+ * (depreprocess). Blocks 0, 1, 3 are preprocess_block / depreprocess_block
+ * (dependency.cpp:333-431): refs[0] is the coarse sub-block 0, the other
+ * entries are ignored. Blocks 2, 4, 5, 6 are preprocess_block_staged /
+ * depreprocess_block_staged (dependency.cpp:294-331): refs[0..5] are ref_x,
+ * ref_y, ref_z, ref_xy, ref_xz, ref_yz (the decoded sub-blocks 1, 2, 4, 3, 5,
+ * 6); an entry the block does not read may be null (2: ref_x, ref_y; 4:
+ * ref_x, ref_z; 5: ref_y, ref_z; 6: ref_xy, ref_xz, ref_yz). Asynchronous on
+ * the context's stream, like the other calls of this group. */
+stz_status stz_preprocess_block_staged_dev(stz_context* ctx, stz_dtype dtype, int block, const void* sub,
+                                           const void* const refs[6], void* diff, size_t dx, size_t dy, size_t dz);
+stz_status stz_depreprocess_block_staged_dev(stz_context* ctx, stz_dtype dtype, int block, const void* de,
+                                             const void* const refs[6], void* out, size_t dx, size_t dy, size_t dz);
 /* quantize_range_nodec (FD5:1204-1253): int32 codes, unpredictable values in
  * element order; *n_unpred receives their count. */
 stz_status stz_quantize_dev(stz_context* ctx, stz_dtype dtype, const void* data, size_t n, double eb, int radius,

@@ -2135,6 +2135,44 @@ static stz_status block_op(stz_context* ctx, int mode, stz_dtype dtype, int pred
     return STZ_OK;
 }
 
+static stz_status block_staged(stz_context* ctx, int mode, stz_dtype dtype, int block, const void* src,
+                               const void* const refs[6], void* dst, size_t dx, size_t dy, size_t dz)
+{
+    STZ_TRY(enter(ctx));
+    if (!src || !refs || !dst) STZ_FAIL(STZ_ERR_ARG, "null pointer");
+    if (dtype != STZ_F32 && dtype != STZ_F64) STZ_FAIL(STZ_ERR_ARG, "bad dtype");
+    if (block < 0 || block > 6) STZ_FAIL(STZ_ERR_RANGE, "block must be in [0, 6]");
+    if (!dx || !dy || !dz) STZ_FAIL(STZ_ERR_DIMS, "dims must be positive");
+    if (dx * dy * dz >= (size_t(1) << 40) || dx > INT32_MAX || dy > INT32_MAX || dz > INT32_MAX)
+        STZ_FAIL(STZ_ERR_DIMS, "dims too large");
+    // the refs each block's lines read (ref_x, ref_y, ref_z, ref_xy, ref_xz,
+    // ref_yz; blocks 0, 1, 3: the coarse sub-block 0 in refs[0])
+    static const unsigned kNeeds[7] = {0x01, 0x01, 0x03, 0x01, 0x05, 0x06, 0x38};
+    for (int k = 0; k < 6; ++k)
+        if ((kNeeds[block] >> k & 1u) && !refs[k]) STZ_FAIL(STZ_ERR_ARG, "a reference sub-block this block reads is null");
+    KScope ks(ctx, "k_block_staged");
+    if (dtype == STZ_F64)
+        launch_block_staged<double>(mode, block, (const double*)src, refs, (double*)dst, (int)dx, (int)dy, (int)dz,
+                                    ctx->st);
+    else
+        launch_block_staged<float>(mode, block, (const float*)src, refs, (float*)dst, (int)dx, (int)dy, (int)dz,
+                                   ctx->st);
+    STZ_CUDA(cudaGetLastError());
+    return STZ_OK;
+}
+
+stz_status stz_preprocess_block_staged_dev(stz_context* ctx, stz_dtype dtype, int block, const void* sub,
+                                           const void* const refs[6], void* diff, size_t dx, size_t dy, size_t dz)
+{
+    return block_staged(ctx, 0, dtype, block, sub, refs, diff, dx, dy, dz);
+}
+
+stz_status stz_depreprocess_block_staged_dev(stz_context* ctx, stz_dtype dtype, int block, const void* de,
+                                             const void* const refs[6], void* out, size_t dx, size_t dy, size_t dz)
+{
+    return block_staged(ctx, 1, dtype, block, de, refs, out, dx, dy, dz);
+}
+
 stz_status stz_preprocess_block_dev(stz_context* ctx, stz_dtype dtype, int predictor, int block, const void* sub,
                                     const void* ref, void* diff, int dx, int dy, int dz, int z0, int z1)
 {

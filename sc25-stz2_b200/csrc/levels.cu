@@ -952,6 +952,17 @@ void launch_block_op(int mode, int predictor, int block, const T* src, const T* 
 }
 
 template <typename T>
+void launch_block_staged(int mode, int block, const T* src, const void* const refs[6], T* dst, int dx, int dy, int dz,
+                         cudaStream_t st)
+{
+    const size_t m = (size_t)dx * dy * dz;
+    if (m == 0) return;
+    StagedRefs r;
+    for (int k = 0; k < 6; ++k) r.p[k] = refs[k];
+    k_block_staged<T><<<grid_for(m, 256), 256, 0, st>>>(mode, block, src, r, dst, dx, dy, dz);
+}
+
+template <typename T>
 void launch_quantize(const T* d, size_t n, QuantParams qp, int* q, T* unpred, uint32_t* tile_cnt, uint64_t* tile_off,
                      cudaStream_t st)
 {
@@ -983,6 +994,7 @@ void launch_dequantize(const int* q, size_t n, QuantParams qp, const T* unpred, 
     template void launch_merge<T>(const T*, int, int, int, T*, cudaStream_t);                                       \
     template void launch_block_op<T>(int, int, int, const T*, const T*, T*, int, int, int, int, int, int, int, int, \
                                      int, cudaStream_t);                                                            \
+    template void launch_block_staged<T>(int, int, const T*, const void* const*, T*, int, int, int, cudaStream_t);  \
     template void launch_quantize<T>(const T*, size_t, QuantParams, int*, T*, uint32_t*, uint64_t*, cudaStream_t);  \
     template void launch_dequantize<T>(const int*, size_t, QuantParams, const T*, T*, uint32_t*, uint64_t*,         \
                                        cudaStream_t);

@@ -78,6 +78,11 @@ template <typename T>
 void launch_split(const T* full, int nx, int ny, int nz, T* subs, cudaStream_t st);
 template <typename T>
 void launch_merge(const T* subs, int hx, int hy, int hz, T* full, cudaStream_t st);
+// dependency.cpp's per-block stage functions on dense sub-block arrays (mode
+// 0 preprocess, 1 depreprocess); refs as stz_preprocess_block_staged_dev.
+template <typename T>
+void launch_block_staged(int mode, int block, const T* src, const void* const refs[6], T* dst, int dx, int dy, int dz,
+                         cudaStream_t st);
 template <typename T>
 void launch_quantize(const T* d, size_t n, QuantParams qp, int* q, T* unpred, uint32_t* tile_cnt, uint64_t* tile_off,
                      cudaStream_t st);

@@ -230,3 +230,55 @@ inline dim3 staged_grid(const LevelGeom& g)
     return dim3((unsigned)((g.dx + kStagedTX - 1) / kStagedTX), (unsigned)((g.dy + kStagedTY - 1) / kStagedTY),
                 (unsigned)std::min(g.dz, 65535));
 }
+
+// The reference's per-block stage functions on dense sub-block arrays of
+// dx*dy*dz values (mode 0: diff = sub - P, mode 1: out = de + P). Blocks 0, 1,
+// 3 read refs.p[0], the coarse sub-block 0 (preprocess_block /
+// depreprocess_block, dependency.cpp:333-431); blocks 2, 4, 5, 6 read ref_x,
+// ref_y, ref_z, ref_xy, ref_xz, ref_yz = refs.p[0..5]
+// (preprocess_block_staged / depreprocess_block_staged,
+// dependency.cpp:294-331), each entry only where the block's lines need it.
+struct StagedRefs {
+    const void* p[6];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_block_staged(int mode, int block, const T* __restrict__ src, StagedRefs refs,
+                                                      T* __restrict__ dst, int dx, int dy, int dz)
+{
+    using A = Ar<T>;
+    const long long sy = dx, sz = (long long)dx * dy;
+    const size_t m = (size_t)sz * dz;
+    auto ref = [&](int k, size_t i) { return static_cast<const T*>(refs.p[k]) + i; };
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % (size_t)dx), y = (int)((i / (size_t)dx) % (size_t)dy), z = (int)(i / (size_t)sz);
+        T p, p0, v0, p1, v1, p2, v2;
+        switch (block) {
+        case 0: p = dep_line<T>(ref(0, i), 1, x, dx); break;
+        case 1: p = dep_line<T>(ref(0, i), sy, y, dy); break;
+        case 3: p = dep_line<T>(ref(0, i), sz, z, dz); break;
+        case 2:
+            dep_line_pv<T>(ref(0, i), sy, y, dy, p0, v0);
+            dep_line_pv<T>(ref(1, i), 1, x, dx, p1, v1);
+            p = dep_blend2(p0, v0, p1, v1);
+            break;
+        case 4:
+            dep_line_pv<T>(ref(0, i), sz, z, dz, p0, v0);
+            dep_line_pv<T>(ref(2, i), 1, x, dx, p1, v1);
+            p = dep_blend2(p0, v0, p1, v1);
+            break;
+        case 5:
+            dep_line_pv<T>(ref(1, i), sz, z, dz, p0, v0);
+            dep_line_pv<T>(ref(2, i), sy, y, dy, p1, v1);
+            p = dep_blend2(p0, v0, p1, v1);
+            break;
+        default:
+            dep_line_pv<T>(ref(3, i), sz, z, dz, p0, v0);
+            dep_line_pv<T>(ref(4, i), sy, y, dy, p1, v1);
+            dep_line_pv<T>(ref(5, i), 1, x, dx, p2, v2);
+            p = dep_blend3(p0, v0, p1, v1, p2, v2);
+            break;
+        }
+        dst[i] = mode == 0 ? A::sub(src[i], p) : A::add(src[i], p);
+    }
+}

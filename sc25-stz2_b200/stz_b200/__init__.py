@@ -91,6 +91,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     for f in (lib.stz_preprocess_block_dev, lib.stz_depreprocess_block_dev, lib.stz_depreprocess_block_to_full_dev):
         f.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp] + [C.c_int] * 5
     lib.stz_depreprocess_block_roi_dev.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp] + [C.c_int] * 9
+    for f in ("stz_preprocess_block_staged_dev", "stz_depreprocess_block_staged_dev"):
+        getattr(lib, f).argtypes = [vp, C.c_int, C.c_int, vp, C.POINTER(vp), vp, C.c_size_t, C.c_size_t, C.c_size_t]
     lib.stz_quantize_dev.argtypes = [vp, C.c_int, vp, sz, C.c_double, C.c_int, vp, vp, C.POINTER(sz)]
     lib.stz_dequantize_dev.argtypes = [vp, C.c_int, vp, sz, C.c_double, C.c_int, vp, vp]
     lib.stz_plan_box.argtypes = [sz, sz, sz, C.c_int, C.c_int, i64p, i64p, i64p, sz, C.POINTER(sz)]
@@ -485,6 +487,22 @@ class Context:
         dz, dy, dx = ref.shape
         _check(self.lib.stz_depreprocess_block_roi_dev(self._c, _tcode(ref), predictor, block, self._p(de),
                                                        self._p(ref), self._p(out), dx, dy, dz, *end, *start))
+
+    def _refs6(self, refs):
+        return (C.c_void_p * 6)(*[None if r is None else self._p(r).value for r in (list(refs) + [None] * 6)[:6]])
+
+    def preprocess_block_staged(self, block, sub, refs, diff):
+        """dependency.cpp's stage functions: blocks 0, 1, 3 take refs = [coarse
+        sub-block 0]; blocks 2, 4, 5, 6 take [ref_x, ref_y, ref_z, ref_xy,
+        ref_xz, ref_yz] (None where the block does not read one)."""
+        dz, dy, dx = sub.shape
+        _check(self.lib.stz_preprocess_block_staged_dev(self._c, _tcode(sub), block, self._p(sub), self._refs6(refs),
+                                                        self._p(diff), dx, dy, dz))
+
+    def depreprocess_block_staged(self, block, de, refs, out):
+        dz, dy, dx = de.shape
+        _check(self.lib.stz_depreprocess_block_staged_dev(self._c, _tcode(de), block, self._p(de), self._refs6(refs),
+                                                          self._p(out), dx, dy, dz))
 
     def quantize(self, data, eb, radius, q, unpred) -> int:
         n = C.c_size_t()

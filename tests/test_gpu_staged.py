@@ -103,3 +103,44 @@ def test_staged_refusals(ctx):
     with Server(0, arena_bytes=64 << 20, max_batch=8) as srv:
         with pytest.raises(StzError, match="staged"):
             srv.add_stream(s.to_bytes())
+
+
+@pytest.mark.parametrize("dims", [(9, 10, 12), (1, 2, 3), (4, 3, 5)])
+def test_stage_functions_match_reference(ctx, dims):
+    """stz_(de)preprocess_block_staged_dev against src/dependency.cpp's own
+    preprocess_block / depreprocess_block / preprocess_block_staged /
+    depreprocess_block_staged (oracle/_ref), every block, bit for bit, on
+    random sub-blocks with a flat region, including axes of extent 1-3 where
+    only the boundary forms run."""
+    if not po.dep_available():
+        pytest.skip("oracle/_ref (the reference build) is missing")
+    import ctypes as C
+
+    D = po.dep()
+    rng = np.random.default_rng(sum(dims))
+    dz, dy, dx = dims
+    arrs = [rng.standard_normal(dims).astype(np.float32) for _ in range(9)]
+    for a in arrs:
+        a[: max(1, dz // 2)] = np.float32(1e-3)
+    sub, coarse, rest = arrs[0], arrs[1], arrs[2:8]
+    dev = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    refs_ptr = (C.c_void_p * 6)(*[r.ctypes.data for r in rest])
+    for block in range(7):
+        one_axis = block in (0, 1, 3)
+        want = np.empty(dims, np.float32)
+        back = np.empty(dims, np.float32)
+        if one_axis:
+            D.depref_preprocess_block(block, po._p(sub), po._p(coarse), po._p(want), dx, dy, dz)
+            D.depref_depreprocess_block(block, po._p(want), po._p(coarse), po._p(back), dx, dy, dz)
+            refs = [dev(coarse)]
+        else:
+            D.depref_preprocess_block_staged(block, po._p(sub), refs_ptr, po._p(want), dx, dy, dz)
+            D.depref_depreprocess_block_staged(block, po._p(want), refs_ptr, po._p(back), dx, dy, dz)
+            refs = [dev(r) for r in rest]
+        sub_t, diff_t, out_t = dev(sub), torch.empty(dims, dtype=torch.float32, device="cuda"), None
+        ctx.preprocess_block_staged(block, sub_t, refs, diff_t)
+        out_t = torch.empty_like(diff_t)
+        ctx.depreprocess_block_staged(block, diff_t, refs, out_t)
+        ctx.sync()
+        assert np.array_equal(_bits(diff_t), _bits(want)), block
+        assert np.array_equal(_bits(out_t), _bits(back)), block
