@@ -522,9 +522,10 @@ def configs_bench(args, ctx, local, field):
     # predictor modes on the same field and bound, at the multipliers of the
     # reference's artifact programs (1 / 2.5 / 6.25, float.cpp and
     # dependency.cpp): the staged predictor of src/dependency.cpp against the
-    # dynamic lines (FD5) and the plain cubic stencils (float.cpp)
+    # dynamic lines (FD5) and the plain cubic stencils (float.cpp), and the
+    # 12-point truncated bicubic of src/stz2.cpp
     res["predictors"] = []
-    for name in ("dynamic", "cubic", "staged"):
+    for name in ("dynamic", "cubic", "staged", "truncated"):
         try:
             o = stz_b200.default_opts(eb=1e-3, eb_mode="rel", zstd_level=args.zstd, predictor=name, mult_base=1.0,
                                       mult_low=2.5, mult_high=6.25)

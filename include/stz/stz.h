@@ -77,7 +77,11 @@ typedef enum stz_predictor {
      * decoded before them (src/dependency.cpp:90-330, stage order 659-704).
      * No learned correction; boxes and slices decode the whole field and copy
      * the box out; the request server does not take these streams. */
-    STZ_PRED_STAGED = 2
+    STZ_PRED_STAGED = 2,
+    /* src/stz2.cpp: float.cpp's stencils with a 12-point truncated bicubic
+     * (no corner taps) for sub-blocks 3, 5, 6 and the one-axis interior cubic
+     * in double (stz2.cpp:82-309). The same restrictions as STZ_PRED_STAGED. */
+    STZ_PRED_TRUNCATED = 3
 } stz_predictor;
 
 typedef struct stz_opts {

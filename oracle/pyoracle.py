@@ -149,6 +149,26 @@ def dep() -> C.CDLL:
     return _dep
 
 
+STZ2_SO = os.path.join(HERE, "_ref", "libstz2_ref.so")
+_stz2 = None
+
+
+def stz2_available() -> bool:
+    return os.path.exists(STZ2_SO)
+
+
+def stz2() -> C.CDLL:
+    """The reference's 12-point truncated bicubic experiment (src/stz2.cpp,
+    float only) compiled from source: preprocess_block / depreprocess_block."""
+    global _stz2
+    if _stz2 is None:
+        L = C.CDLL(STZ2_SO)
+        for f in ("stz2ref_preprocess_block", "stz2ref_depreprocess_block"):
+            getattr(L, f).argtypes = [ci, vp, vp, vp, ci, ci, ci]
+        _stz2 = L
+    return _stz2
+
+
 def ref() -> C.CDLL:
     global _ref
     if _ref is None:
@@ -471,6 +491,56 @@ def ref_round_trip_staged(field: np.ndarray, eb: float, mults=(1.0, 2.5, 6.25), 
                 D.depref_depreprocess_block(b, _p(dq), _p(grid), _p(out[b + 1]), dx, dy, dz)
             else:
                 D.depref_depreprocess_block_staged(b, _p(dq), refs, _p(out[b + 1]), dx, dy, dz)
+        nxt = np.empty((2 * dz, 2 * dy, 2 * dx), a.dtype)
+        R.fd5ref_merge_sub_blocks_to_full_f32(_p(out), _p(nxt), dx, dy, dz)
+        codes.append(lc)
+        unpred.append(lu)
+        grid = nxt
+        grids.append(grid)
+    return {"K": K, "codes": codes, "unpred": unpred, "grids": grids, "closed_loop_ok": True}
+
+
+def ref_round_trip_trunc(field: np.ndarray, eb: float, mults=(1.0, 2.5, 6.25), radius: int = 32768,
+                         chunk_high: int = 32, chunk_low: int = 16) -> dict:
+    """The pipeline of src/stz2.cpp (float only): per level, its
+    preprocess_block on the 7 odd-parity sub-blocks against the decoded
+    coarser grid, FD5's quantize_range_nodec at multiplier x eb (multipliers
+    1 / 2.5 / 6.25, stz2.cpp:694, 766), its depreprocess_block on the
+    dequantized residuals, merge_sub_blocks_to_full; stz2.cpp's functions and
+    FD5's quantizer, dequantizer, split and merge compiled from source
+    (oracle/_ref), driven through this project's hierarchy. Returns the same
+    record as ref_round_trip."""
+    a = np.ascontiguousarray(field)
+    if a.dtype != np.float32:
+        raise ValueError("src/stz2.cpp is float only")
+    nz, ny, nx = a.shape
+    K = num_levels(nx, ny, nz)
+    S = 1 << K
+    R, D = ref(), stz2()
+    grid = np.ascontiguousarray(a[::S, ::S, ::S])
+    grids, codes, unpred = [grid], [], []
+    for k in range(1, K + 1):
+        s = 1 << (K - k)
+        fine = a if s == 1 else np.ascontiguousarray(a[::s, ::s, ::s])
+        ebk = (mults[2] if k == K else mults[1] if k == K - 1 else mults[0]) * eb
+        dz, dy, dx = grid.shape
+        n = dx * dy * dz
+        C_ = oracle().stzo_level_chunk(nx, ny, nz, k, chunk_high, chunk_low)
+        subs = np.empty((8, dz, dy, dx), a.dtype)
+        R.fd5ref_slice_full_data_f32(_p(fine), _p(subs), 2 * dx, 2 * dy, 2 * dz)
+        out = np.empty((8, dz, dy, dx), a.dtype)
+        out[0] = grid
+        lc, lu = [], []
+        for b in range(7):
+            diff = np.empty((dz, dy, dx), a.dtype)
+            D.stz2ref_preprocess_block(b, _p(subs[b + 1]), _p(grid), _p(diff), dx, dy, dz)
+            q = np.empty(n, np.int32)
+            u = np.empty(n, a.dtype)
+            nu = R.fd5ref_quantize_range_nodec_f32(_p(diff), n, ebk, radius, _p(q), _p(u), n)
+            lc.append(chunk_major(q, (dz, dy, dx), C_).astype(np.uint16))
+            lu.append(int(nu))
+            dq = ref_dequantize(q, ebk, radius, u[:nu], a.dtype).reshape(dz, dy, dx)
+            D.stz2ref_depreprocess_block(b, _p(dq), _p(grid), _p(out[b + 1]), dx, dy, dz)
         nxt = np.empty((2 * dz, 2 * dy, 2 * dx), a.dtype)
         R.fd5ref_merge_sub_blocks_to_full_f32(_p(out), _p(nxt), dx, dy, dz)
         codes.append(lc)

@@ -263,6 +263,43 @@ static T FN(staged_pred)(int b, const T* r, const T* F, int x, int y, int z, int
 #undef SIB
 }
 
+/* Predictor of src/stz2.cpp (predictor 3): the plain stencils above, except
+ * that the two-axis blocks 2, 4, 5 take a 12-point truncated bicubic inside
+ * (the 4 inner points at (9/16)^2, the 8 edge points at -(1/16)(9/16), no
+ * corners; stz2.cpp:122-155, 170-232) and that the one-axis interior cubic
+ * has double weights (stz2.cpp:86, 100-118), so the reference evaluates it,
+ * the residual and the rebuilt value in double and rounds once. Returns the
+ * prediction as a double; *wide = 1 for that double-evaluated case. */
+static double FN(t_predict_trunc)(int block, const T* r, int x, int y, int z, int dx, int dy, int dz, int* wide)
+{
+    const size_t sx = (size_t)dx, sy = (size_t)dx * (size_t)dy;
+    const size_t i = ((size_t)z * dy + y) * dx + x;
+    *wide = 0;
+    size_t st = 0, a1 = 0, a2 = 0; /* cubic stride; the 12-point form's two axes */
+    int pos = 0, dim = 0, inner = 0;
+    switch (block) {
+    case 0: st = 1, pos = x, dim = dx; break;
+    case 1: st = sx, pos = y, dim = dy; break;
+    case 3: st = sy, pos = z, dim = dz; break;
+    case 2: a1 = 1, a2 = sx, inner = x >= 1 && x < dx - 2 && y >= 1 && y < dy - 2; break;
+    case 4: a1 = 1, a2 = sy, inner = x >= 1 && x < dx - 2 && z >= 1 && z < dz - 2; break;
+    case 5: a1 = sx, a2 = sy, inner = y >= 1 && y < dy - 2 && z >= 1 && z < dz - 2; break;
+    default: break;
+    }
+    if (st && pos >= 1 && pos < dim - 2) {
+        *wide = 1;
+        return -0.0625 * (double)r[i - st] + 0.5625 * (double)r[i] + 0.5625 * (double)r[i + st] +
+               -0.0625 * (double)r[i + 2 * st];
+    }
+    if (inner) {
+        const T core = r[i] + r[i + a1] + r[i + a2] + r[i + a2 + a1];
+        const T edge = r[i - a1] + r[i + 2 * a1] + r[i + a2 - a1] + r[i + a2 + 2 * a1] + r[i - a2] + r[i - a2 + a1] +
+                       r[i + 2 * a2] + r[i + 2 * a2 + a1];
+        return (double)(T)(0.31640625f * core + -0.033203125f * edge);
+    }
+    return (double)FN(t_predict_plain)(block, r, x, y, z, dx, dy, dz);
+}
+
 static inline T FN(predict_any)(int predictor, int block, const T* r, int x, int y, int z, int dx, int dy,
                                 int dz)
 {
@@ -354,6 +391,77 @@ static long long FN(t_quantize)(const T* d, size_t n, double eb, int radius, int
         }
     }
     return (long long)nu;
+}
+
+/* Level step of predictor 3: as t_level_encode / t_level_decode, with the
+ * residual and the rebuilt value in double where the prediction is. */
+static int FN(t_level_encode_trunc)(const T* fine, const T* coarse, int dx, int dy, int dz, double eb, int radius,
+                                    int* q, T* unpred, size_t cap, size_t* counts, T* decoded)
+{
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    const double recip = 1.0 / eb;
+    size_t nu = 0;
+    for (int b = 0; b < 7; ++b) {
+        const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        size_t nb = 0;
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const size_t i = ((size_t)z * dy + y) * dx + x;
+                    const size_t fi = (2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px;
+                    int wide;
+                    const double pd = FN(t_predict_trunc)(b, coarse, x, y, z, dx, dy, dz, &wide);
+                    const T p = (T)pd;
+                    const T d = wide ? (T)((double)fine[fi] - pd) : fine[fi] - p;
+                    T dec = 0;
+                    const int code = FN(quant1)(d, eb, recip, radius, &dec);
+                    q[(size_t)b * n + i] = code;
+                    if (code == 0) {
+                        if (nu >= cap) return -1;
+                        unpred[nu++] = d;
+                        ++nb;
+                    }
+                    if (decoded) {
+                        const T dq = code ? FN(recover)(code, eb, radius) : d;
+                        decoded[fi] = wide ? (T)((double)dq + pd) : dq + p;
+                    }
+                }
+        counts[b] = nb;
+    }
+    if (decoded) {
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x)
+                    decoded[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] =
+                        coarse[((size_t)z * dy + y) * dx + x];
+    }
+    return 0;
+}
+
+static void FN(t_level_decode_trunc)(const int* q, const T* unpred, const T* coarse, int dx, int dy, int dz,
+                                     double eb, int radius, T* out)
+{
+    const size_t n = (size_t)dx * dy * dz;
+    const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
+    size_t u = 0;
+    for (int b = 0; b < 7; ++b) {
+        const int s = b + 1, px = s & 1, py = (s >> 1) & 1, pz = (s >> 2) & 1;
+        for (int z = 0; z < dz; ++z)
+            for (int y = 0; y < dy; ++y)
+                for (int x = 0; x < dx; ++x) {
+                    const int code = q[(size_t)b * n + ((size_t)z * dy + y) * dx + x];
+                    const T dq = code ? FN(recover)(code, eb, radius) : unpred[u++];
+                    int wide;
+                    const double pd = FN(t_predict_trunc)(b, coarse, x, y, z, dx, dy, dz, &wide);
+                    out[(2 * (size_t)z + pz) * fxy + (2 * (size_t)y + py) * fx + 2 * (size_t)x + px] =
+                        wide ? (T)((double)dq + pd) : dq + (T)pd;
+                }
+    }
+    for (int z = 0; z < dz; ++z)
+        for (int y = 0; y < dy; ++y)
+            for (int x = 0; x < dx; ++x)
+                out[(2 * (size_t)z) * fxy + (2 * (size_t)y) * fx + 2 * (size_t)x] = coarse[((size_t)z * dy + y) * dx + x];
 }
 
 /* Level step of the staged predictor: the blocks in the reference's stage
@@ -460,6 +568,8 @@ static int FN(t_level_encode)(const T* fine, const T* coarse, int dx, int dy, in
     ftz_on();
     if (predictor == 2)
         return FN(t_level_encode_staged)(fine, coarse, dx, dy, dz, eb, radius, q, unpred, cap, counts, decoded);
+    if (predictor == 3)
+        return FN(t_level_encode_trunc)(fine, coarse, dx, dy, dz, eb, radius, q, unpred, cap, counts, decoded);
     const size_t n = (size_t)dx * dy * dz;
     const size_t fx = 2 * (size_t)dx, fxy = 4 * (size_t)dx * dy;
     const double recip = 1.0 / eb;
@@ -512,6 +622,10 @@ static void FN(t_level_decode)(const int* q, const T* unpred, const size_t* coun
     ftz_on();
     if (predictor == 2) {
         FN(t_level_decode_staged)(q, unpred, coarse, dx, dy, dz, eb, radius, out);
+        return;
+    }
+    if (predictor == 3) {
+        FN(t_level_decode_trunc)(q, unpred, coarse, dx, dy, dz, eb, radius, out);
         return;
     }
     const size_t n = (size_t)dx * dy * dz;

@@ -316,10 +316,11 @@ stz_status check_opts(const stz_opts* o)
     if (!(o->mult_base > 0) || !(o->mult_low > 0) || !(o->mult_high > 0)) STZ_FAIL(STZ_ERR_ARG, "multipliers must be > 0");
     if (o->radius < 1 || o->radius > 32768) STZ_FAIL(STZ_ERR_ARG, "radius must be in [1, 32768]");
     if (o->zstd_level < 0 || o->zstd_level > 22) STZ_FAIL(STZ_ERR_ARG, "zstd_level must be in [0, 22]");
-    if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC &&
-        o->predictor != STZ_PRED_STAGED) STZ_FAIL(STZ_ERR_ARG, "bad predictor");
-    if (o->predictor == STZ_PRED_STAGED && o->model)
-        STZ_FAIL(STZ_ERR_ARG, "the staged predictor takes no learned correction");
+    if (o->predictor != STZ_PRED_DYNAMIC && o->predictor != STZ_PRED_CUBIC && o->predictor != STZ_PRED_STAGED &&
+        o->predictor != STZ_PRED_TRUNCATED)
+        STZ_FAIL(STZ_ERR_ARG, "bad predictor");
+    if (o->predictor >= STZ_PRED_STAGED && o->model)
+        STZ_FAIL(STZ_ERR_ARG, "the staged and truncated predictors take no learned correction");
     if (o->learned_flags < -1 || (o->learned_flags >= 0 && (o->learned_flags & ~0x7f7f)))
         STZ_FAIL(STZ_ERR_ARG, "learned_flags must be -1 or a mask of bits 0-6 and 8-14");
     return STZ_OK;
@@ -1403,11 +1404,11 @@ struct DecodePipe {
         coarse = p.coarsest->as<T>();
         // the finest level decodes by z-bricks as its chunk layers arrive
         // (plain kernels only; else the whole level after the last batch;
-        // the staged predictor's stages span the whole level)
+        // the staged and truncated predictors' kernels take whole levels)
         fin_bricks = level_decode_bricks(level_geom(ps, kdec),
                                          (learned_args<T>(ps, kdec, p.d_models).model != nullptr &&
                                           learned_args<T>(ps, kdec, p.d_models).flags) ||
-                                             ps.h.predictor == STZ_PRED_STAGED,
+                                             ps.h.predictor >= STZ_PRED_STAGED,
                                          0, nullptr);
         // the entropy decodes (ctx->st_dec) follow everything enqueued on
         // ctx->st so far: tables, coarsest grid, work lists, earlier calls
@@ -1578,10 +1579,11 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         odims[1] = (size_t)(plan.q[1].e - plan.q[1].b + 1);
         odims[2] = (size_t)(plan.q[2].e - plan.q[2].b + 1);
     }
-    if (h.predictor == STZ_PRED_STAGED) {
+    if (h.predictor >= STZ_PRED_STAGED) {
         // A staged block's value depends on siblings decoded before it along
-        // whole lines, beyond the planner's chunk halo: decode the field,
-        // then copy the box out (as a decoder without chunk markers does,
+        // whole lines, beyond the planner's chunk halo, and the ROI cell
+        // kernels carry the one-pass predictors only: decode the field, then
+        // copy the box out (as a decoder without chunk markers does,
         // src/stz-rd.cpp:591-596).
         STZ_CUDA(ctx->staged_full.ensure((size_t)h.nx * h.ny * h.nz * sizeof(T)));
         STZ_TRY(decompress_level_dev<T>(ctx, s, 0, ctx->staged_full.as<T>()));

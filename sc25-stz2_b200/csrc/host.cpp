@@ -518,7 +518,7 @@ std::string parse_stream(const uint8_t* data, size_t size, ParsedStream& out)
     h.c0[0] = (int)r.u32(), h.c0[1] = (int)r.u32(), h.c0[2] = (int)r.u32();
     if (r.err) return "truncated stream header";
     if (h.dtype != 0 && h.dtype != 1) return "bad dtype";
-    if (h.predictor < 0 || h.predictor > 2) return "bad predictor";
+    if (h.predictor < 0 || h.predictor > 3) return "bad predictor";
     if (h.radius < 1 || h.radius > 32768) return "bad radius";
     const std::string dm = validate_dims(h.nx, h.ny, h.nz, h.chunk_high, h.chunk_low);
     if (!dm.empty()) return dm;

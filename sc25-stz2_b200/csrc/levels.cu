@@ -319,6 +319,7 @@ __device__ __forceinline__ T recover_lut(const T* lut, int q, const QuantParams&
 
 #include "level_kernels.cuh"
 #include "staged_kernels.cuh"
+#include "trunc_kernels.cuh"
 
 // Coarsest grid of the hierarchy: every 2^K-th point of the field.
 template <typename T>
@@ -733,6 +734,12 @@ void launch_level_encode(const LevelEncodeArgs<T>& a, cudaStream_t st)
         launch_staged_encode(a, st);
         return;
     }
+    if (a.predictor == 3) {  // one global-tap pass (trunc_kernels.cuh)
+        const HistArgs h{a.hist_full, a.hist_outside, a.qp.radius};
+        const EncodeIO<T> io{a.field, a.fsx, a.fsy, a.stride, a.codes, a.unpred_dense, a.unpred_cnt, a.decoded};
+        k_trunc_encode<T><<<trunc_grid(a.geo), dim3(kTruncTX, kTruncTY), 0, st>>>(io, a.coarse, a.geo, a.qp, h);
+        return;
+    }
     const LevelGeom& g = a.geo;
     const Shell shell = Shell::make(g.dx, g.dy, g.dz);
     dim3 blk(BX, BY, 1);
@@ -805,6 +812,11 @@ void launch_level_decode(const LevelDecodeArgs<T>& a, cudaStream_t st)
 {
     if (a.predictor == 2) {  // whole level (level_decode_bricks: none)
         launch_staged_decode(a, st);
+        return;
+    }
+    if (a.predictor == 3) {  // whole level
+        k_trunc_decode<T><<<trunc_grid(a.geo), dim3(kTruncTX, kTruncTY), 0, st>>>(a.coarse, a.geo, a.qp, a.codes,
+                                                                                  a.unpred_dense, a.out);
         return;
     }
     const LevelGeom& g = a.geo;

@@ -17,7 +17,8 @@ struct LevelEncodeArgs {
     int stride;         // sampling stride of this level's fine grid (1 = finest)
     const T* coarse;    // decoded coarse grid (geo.dx x dy x dz)
     LevelGeom geo;
-    int predictor;      // 0 = dynamic lines (FD5), 1 = plain cubic, 2 = staged (dependency.cpp)
+    int predictor;      // 0 = dynamic lines (FD5), 1 = plain cubic, 2 = staged (dependency.cpp),
+                        // 3 = 12-point truncated bicubic (stz2.cpp)
     uint16_t* codes;        // 7 x n, chunk-major per stream
     T* unpred_dense;        // 7 x n, written where the code is 0
     uint32_t* unpred_cnt;   // 7 x (nchunks + 1)

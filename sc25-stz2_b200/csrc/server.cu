@@ -874,8 +874,9 @@ stz_status stz_server_add_stream(stz_server* S, const void* data, size_t size, i
     const ParsedStream& ps = ss->s->dir;
     const FileHeader& h = ps.h;
     if (h.K < 2) STZ_FAIL(STZ_ERR_DIMS, "stream has fewer than two levels");
-    if (h.predictor == STZ_PRED_STAGED)
-        STZ_FAIL(STZ_ERR_UNSUPPORTED, "the server's batched decodes take dynamic and cubic streams, not staged ones");
+    if (h.predictor >= STZ_PRED_STAGED)
+        STZ_FAIL(STZ_ERR_UNSUPPORTED,
+                 "the server's batched decodes take dynamic and cubic streams, not staged or truncated ones");
     ss->K = h.K;
     ss->dtype = h.dtype;
     ss->elem = h.elem();

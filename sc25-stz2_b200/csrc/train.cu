@@ -875,7 +875,8 @@ stz_status stz_trainer_create(stz_context* ctx, const stz_opts* opts, const stz_
     if (!ctx || !opts || !out) STZ_FAIL(STZ_ERR_ARG, "null pointer");
     *out = nullptr;
     STZ_TRY(check_opts(opts));
-    if (opts->predictor == STZ_PRED_STAGED) STZ_FAIL(STZ_ERR_UNSUPPORTED, "no learned correction for the staged predictor");
+    if (opts->predictor >= STZ_PRED_STAGED)
+        STZ_FAIL(STZ_ERR_UNSUPPORTED, "no learned correction for the staged and truncated predictors");
     stz_train_opts t;
     stz_default_train_opts(&t);
     if (topts) t = *topts;

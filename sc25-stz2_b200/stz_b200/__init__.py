@@ -190,7 +190,7 @@ def default_opts(**kw) -> Opts:
     lib.stz_default_opts(C.byref(o))
     modes = {"abs": 0, "rel": 1}
     bounds = {"pointwise": 0, "reference": 1}
-    preds = {"dynamic": 0, "cubic": 1, "staged": 2}
+    preds = {"dynamic": 0, "cubic": 1, "staged": 2, "truncated": 3}
     for k, v in kw.items():
         if k == "eb_mode" and isinstance(v, str):
             v = modes[v]

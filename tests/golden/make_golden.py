@@ -7,8 +7,9 @@ preprocess_block_zslab, quantize_range_nodec and, on coarser levels, the
 writeDec closed loop with depreprocess_block_zslab + merge), and the field is
 rebuilt with the reference decoder (recover LUT + depreprocess_block_zslab /
 depreprocess_block_zslab_to_full). Also records reference planner output for
-random queries, the plain tricubic stencils of src/stz-rd.cpp, and a staged
-pipeline of src/dependency.cpp's stage functions (oracle/_ref/libdep_ref.so).
+random queries, the plain tricubic stencils of src/stz-rd.cpp, a staged
+pipeline of src/dependency.cpp's stage functions (oracle/_ref/libdep_ref.so)
+and the pipeline of src/stz2.cpp's functions (oracle/_ref/libstz2_ref.so).
 
     python tests/golden/make_golden.py        # needs the reference sources
 """
@@ -107,6 +108,11 @@ def main():
     for k in range(1, st["K"] + 1):
         arrays[f"staged_L{k}_codes"] = np.stack(st["codes"][k - 1])
     arrays["staged_decoded"] = st["grids"][st["K"]]
+    # 12-point truncated bicubic of src/stz2.cpp, the same way
+    tr = po.ref_round_trip_trunc(f, eb, (1.0, 2.5, 6.25), chunk_high=8, chunk_low=4)
+    for k in range(1, tr["K"] + 1):
+        arrays[f"trunc_L{k}_codes"] = np.stack(tr["codes"][k - 1])
+    arrays["trunc_decoded"] = tr["grids"][tr["K"]]
 
     rng = np.random.default_rng(5)
     plans, offs, queries = [], [0], []

@@ -1,13 +1,16 @@
-"""Staged predictor (STZ_PRED_STAGED, src/dependency.cpp) on the GPU.
+"""The reference's experimental predictors on the GPU: the staged predictor
+(STZ_PRED_STAGED, src/dependency.cpp) and the 12-point truncated bicubic
+(STZ_PRED_TRUNCATED, src/stz2.cpp).
 
-* Small fields: the GPU stream is byte for byte the oracle's (whose staged
-  pipeline is itself pinned to the reference's stage functions, CPU tests),
+* Small fields: the GPU stream is byte for byte the oracle's (whose
+  pipelines are themselves pinned to the reference's functions, CPU tests),
   and so are the full decode, every progressive level and boxes/slices.
 * 256^3 f32 GRF: every level's codes of every block, the full decode and the
-  progressive levels against the reference's own stage functions compiled
-  from source (pyoracle.ref_round_trip_staged).
+  progressive levels against the reference's own functions compiled from
+  source (pyoracle.ref_round_trip_staged / ref_round_trip_trunc).
 * 512^3 f32 lognormal (the benchmark field): pointwise bound, box = crop.
-* What the mode refuses: a learned model, the request server."""
+* What the modes refuse: the request server.
+* dependency.cpp's stage functions at the function boundary."""
 import numpy as np
 import pytest
 
@@ -25,8 +28,12 @@ def _bits(a):
     return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
 
 
+PRED_ID = {"staged": 2, "truncated": 3}
+
+
+@pytest.mark.parametrize("pred", ["staged", "truncated"])
 @pytest.mark.parametrize("case", ["grf64_f32", "fronts64_f64", "ragged_112x80x48_f32", "logn64_f32_1e-4"])
-def test_staged_stream_is_the_oracles(ctx, case):
+def test_stream_is_the_oracles(ctx, case, pred):
     from stz_b200 import fields
 
     chunks = {}
@@ -39,10 +46,10 @@ def test_staged_stream_is_the_oracles(ctx, case):
     else:
         f, rel = fields.grf((48, 80, 112), 3.0, 13, np.float32), 1e-3
         chunks = dict(chunk_high=8, chunk_low=4)
-    s = ctx.compress(f, eb=rel, eb_mode="rel", predictor="staged", **MULTS, **chunks)
+    s = ctx.compress(f, eb=rel, eb_mode="rel", predictor=pred, **MULTS, **chunks)
     inf = s.info()
-    assert inf.predictor == 2
-    want = po.compress(f, inf.eb, predictor=2, mults=(1.0, 2.5, 6.25), **chunks)
+    assert inf.predictor == PRED_ID[pred]
+    want = po.compress(f, inf.eb, predictor=PRED_ID[pred], mults=(1.0, 2.5, 6.25), **chunks)
     assert s.to_bytes() == want
     out = ctx.decompress(s)
     assert np.array_equal(_bits(out), _bits(po.decompress(want)))
@@ -58,15 +65,17 @@ def test_staged_stream_is_the_oracles(ctx, case):
     assert np.array_equal(_bits(ctx.decompress(ctx.parse(s.to_bytes()))), _bits(out))
 
 
-def test_staged_256_matches_reference(ctx):
+@pytest.mark.parametrize("pred", ["staged", "truncated"])
+def test_256_matches_reference(ctx, pred):
     from stz_b200 import fields
 
-    if not (po.ref_available() and po.dep_available()):
+    if not (po.ref_available() and po.dep_available() and po.stz2_available()):
         pytest.skip("oracle/_ref (the reference build) is missing")
     f = fields.grf((256, 256, 256), 11.0 / 3.0, 2025)
-    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor="staged", **MULTS)
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor=pred, **MULTS)
     inf = s.info()
-    ref = po.ref_round_trip_staged(f, inf.eb, inf.mults)
+    trip = po.ref_round_trip_staged if pred == "staged" else po.ref_round_trip_trunc
+    ref = trip(f, inf.eb, inf.mults)
     K = ref["K"]
     for k in range(1, K + 1):
         for b in range(7):
@@ -78,11 +87,12 @@ def test_staged_256_matches_reference(ctx):
     assert np.abs(out.astype(np.float64) - f).max() <= 1e-3 * (float(f.max()) - float(f.min()))
 
 
-def test_staged_lognormal_512_bound_and_box(ctx):
+@pytest.mark.parametrize("pred", ["staged", "truncated"])
+def test_lognormal_512_bound_and_box(ctx, pred):
     from stz_b200 import fields
 
     f = fields.lognormal((512, 512, 512), 2025, np.float32, device="cuda:0")
-    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor="staged", **MULTS)
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor=pred, **MULTS)
     out = torch.empty_like(f)
     ctx.decompress(s, out=out)
     E = 1e-3 * (float(f.max()) - float(f.min()))
@@ -95,13 +105,14 @@ def test_staged_lognormal_512_bound_and_box(ctx):
     assert torch.equal(out.view(torch.int32), out2.view(torch.int32))
 
 
-def test_staged_refusals(ctx):
+@pytest.mark.parametrize("pred", ["staged", "truncated"])
+def test_server_refuses_the_stream(ctx, pred):
     from stz_b200 import Server, StzError, fields
 
     f = fields.grf((64, 64, 64), 11.0 / 3.0, 3, np.float32)
-    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor="staged")
+    s = ctx.compress(f, eb=1e-3, eb_mode="rel", predictor=pred)
     with Server(0, arena_bytes=64 << 20, max_batch=8) as srv:
-        with pytest.raises(StzError, match="staged"):
+        with pytest.raises(StzError, match=pred):
             srv.add_stream(s.to_bytes())
 
 

@@ -206,6 +206,46 @@ def test_staged_pipeline_matches_reference_golden(golden):
     assert np.array_equal(po.decompress(stream).view(np.uint32), golden["staged_decoded"].view(np.uint32))
 
 
+@pytest.mark.skipif(not (po.ref_available() and po.stz2_available()), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("case", ["grf64_1e-3", "logn64_1e-4", "ragged_112x80x48_1e-3"])
+def test_oracle_truncated_pipeline_matches_reference(case):
+    """The 12-point truncated bicubic predictor of src/stz2.cpp (predictor 3,
+    one-axis interior cubic in double): codes and decodes of the oracle's
+    stream against the reference's functions (pyoracle.ref_round_trip_trunc)."""
+    from stz_b200 import fields
+
+    if case.startswith("grf"):
+        f, rel = fields.grf((64, 64, 64), 11.0 / 3.0, 7, np.float32), 1e-3
+    elif case.startswith("logn"):
+        f, rel = fields.lognormal((64, 64, 64), 5, np.float32), 1e-4
+    else:
+        f, rel = fields.grf((48, 80, 112), 3.0, 13, np.float32), 1e-3
+    mults = (1.0, 2.5, 6.25)
+    eb = po.pointwise_eb(f, rel, mults)
+    ref = po.ref_round_trip_trunc(f, eb, mults, chunk_high=8, chunk_low=4)
+    stream = po.compress(f, eb, predictor=3, mults=mults, chunk_high=8, chunk_low=4)
+    K = ref["K"]
+    for k in range(1, K + 1):
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), ref["codes"][k - 1][b]), (k, b)
+    for lvl in range(0, K + 1):
+        assert np.array_equal(po.decompress(stream, lvl).view(np.uint32), ref["grids"][K - lvl].view(np.uint32)), lvl
+
+
+def test_truncated_pipeline_matches_reference_golden(golden):
+    """The oracle's predictor-3 stream against golden codes and decode made by
+    src/stz2.cpp's functions (tests/golden/make_golden.py)."""
+    f = golden["staged_field"]
+    eb = float(golden["staged_eb"])
+    K = int(golden["staged_K"])
+    stream = po.compress(f, eb, predictor=3, mults=(1.0, 2.5, 6.25), chunk_high=8, chunk_low=4)
+    for k in range(1, K + 1):
+        want = golden[f"trunc_L{k}_codes"]
+        for b in range(7):
+            assert np.array_equal(po.stream_codes(stream, k, b), want[b]), (k, b)
+    assert np.array_equal(po.decompress(stream).view(np.uint32), golden["trunc_decoded"].view(np.uint32))
+
+
 def test_oracle_staged_f64_round_trip_and_box():
     """The staged predictor in double (the same expressions in T): bound,
     and boxes equal to the full decode's crop."""
