@@ -2145,7 +2145,7 @@ static stz_status block_staged(stz_context* ctx, int mode, stz_dtype dtype, int 
     if (dtype != STZ_F32 && dtype != STZ_F64) STZ_FAIL(STZ_ERR_ARG, "bad dtype");
     if (block < 0 || block > 6) STZ_FAIL(STZ_ERR_RANGE, "block must be in [0, 6]");
     if (!dx || !dy || !dz) STZ_FAIL(STZ_ERR_DIMS, "dims must be positive");
-    if (dx * dy * dz >= (size_t(1) << 40) || dx > INT32_MAX || dy > INT32_MAX || dz > INT32_MAX)
+    if (dx > INT32_MAX || dy > INT32_MAX || dz > INT32_MAX || dx * dy > (size_t(1) << 40) / dz)
         STZ_FAIL(STZ_ERR_DIMS, "dims too large");
     // the refs each block's lines read (ref_x, ref_y, ref_z, ref_xy, ref_xz,
     // ref_yz; blocks 0, 1, 3: the coarse sub-block 0 in refs[0])
