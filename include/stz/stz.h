@@ -75,12 +75,15 @@ typedef enum stz_predictor {
     /* Staged: sub-blocks 1, 2, 4 from 1-D cubics on the coarse grid, then 3, 5,
      * 6 and 7 from inverse-variance blends of 1-D cubics through the siblings
      * decoded before them (src/dependency.cpp:90-330, stage order 659-704).
-     * No learned correction; boxes and slices decode the whole field and copy
-     * the box out; the request server does not take these streams. */
+     * No learned correction; boxes and slices decode the whole field (into a
+     * context buffer of the field's size) and copy the box out; the request
+     * server does not take these streams. Compress keeps the finest level's
+     * decoded values, a device scratch of the field's size. */
     STZ_PRED_STAGED = 2,
     /* src/stz2.cpp: float.cpp's stencils with a 12-point truncated bicubic
      * (no corner taps) for sub-blocks 3, 5, 6 and the one-axis interior cubic
-     * in double (stz2.cpp:82-309). The same restrictions as STZ_PRED_STAGED. */
+     * in double (stz2.cpp:82-309). No learned correction, boxes through the
+     * whole field, no request server, as STZ_PRED_STAGED (no compress scratch). */
     STZ_PRED_TRUNCATED = 3
 } stz_predictor;
 
