@@ -788,6 +788,7 @@ static int parse(const uint8_t* st, size_t size, parsed_t* ps)
     h->eb = rf64(&r), h->mb = rf64(&r), h->ml = rf64(&r), h->mh = rf64(&r);
     h->c0[0] = (int)ru32(&r), h->c0[1] = (int)ru32(&r), h->c0[2] = (int)ru32(&r);
     if (r.err || h->K < 1 || h->K >= 64 || (h->dtype != 0 && h->dtype != 1)) return -12;
+    if (h->predictor < 0 || h->predictor > 3) return -12; /* dynamic, cubic, staged, truncated */
     h->elem = h->dtype == 1 ? 8 : 4;
     ps->coarsest = st + r.pos;
     r.pos += (size_t)h->c0[0] * h->c0[1] * h->c0[2] * h->elem;

@@ -39,6 +39,27 @@ def test_default_opts_are_reference_defaults():
     assert o.model is None and o.learned_flags == -1
 
 
+def test_predictor_names_map_to_the_header_values():
+    import stz_b200
+
+    for name, v in (("dynamic", 0), ("cubic", 1), ("staged", 2), ("truncated", 3)):
+        assert stz_b200.default_opts(predictor=name).predictor == v
+
+
+def test_oracle_rejects_an_unknown_predictor():
+    """A stream header naming a predictor past the four known ones does not
+    decode (the library's parser rejects the same values)."""
+    import pyoracle as po
+
+    f = np.cumsum(np.random.default_rng(2).normal(0, 1, (64, 64, 64)), axis=2).astype(np.float32)
+    b = bytearray(po.compress(f, po.pointwise_eb(f, 1e-3), predictor=3))
+    assert int.from_bytes(b[16:20], "little") == 3  # magic, version, dtype, predictor
+    po.decompress(bytes(b))
+    b[16:20] = (4).to_bytes(4, "little")
+    with pytest.raises(ValueError):
+        po.decompress(bytes(b))
+
+
 def test_struct_offsets_match_the_c_compiler(tmp_path):
     """Field offsets of the option / info structs as gcc lays them out."""
     import shutil
