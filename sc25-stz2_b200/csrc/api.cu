@@ -1580,11 +1580,11 @@ stz_status decompress_box_dev(stz_context* ctx, stz_stream* s, const int64_t lo[
         odims[2] = (size_t)(plan.q[2].e - plan.q[2].b + 1);
     }
     if (h.predictor >= STZ_PRED_STAGED) {
-        // A staged block's value depends on siblings decoded before it along
-        // whole lines, beyond the planner's chunk halo, and the ROI cell
-        // kernels carry the one-pass predictors only: decode the field, then
-        // copy the box out (as a decoder without chunk markers does,
-        // src/stz-rd.cpp:591-596).
+        // The ROI cell kernels carry the one-pass predictors only, and a
+        // staged block also needs its siblings' decoded values up to two
+        // coarse points outside the box, whose codes can lie in chunks the
+        // planner does not pick: decode the field, then copy the box out (as
+        // a decoder without chunk markers does, src/stz-rd.cpp:591-596).
         STZ_CUDA(ctx->staged_full.ensure((size_t)h.nx * h.ny * h.nz * sizeof(T)));
         STZ_TRY(decompress_level_dev<T>(ctx, s, 0, ctx->staged_full.as<T>()));
         const size_t ox = (size_t)(plan.q[0].e - plan.q[0].b + 1), oy = (size_t)(plan.q[1].e - plan.q[1].b + 1),
